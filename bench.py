@@ -1,0 +1,326 @@
+"""Benchmark: RK45 (Cash-Karp, NR step control) steps/s of the 3-D quasi-dynamic
+boundary-integral model at N = 20,000 Nikkhoo-Walter triangles (curved
+megathrust, full reference layout: K is 60,000 x 40,000 FP64, 19.2 GB).
+
+One "step" is one accepted main-loop iteration of the reference
+(fortran/3d/src/ratestate.f90:307-326): f(y), yscal, RKQSm attempts until one
+is accepted.  `value` is accepted steps/s summed over GPUs with the state
+resident in HBM (device-resident loop, ucg_run); `e2e` is the same metric
+through the host-array ABI call (ucg_step: y host->device, step, y and dydt
+device->host every step).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Multi-GPU: replicas only (the path runs on one GPU; no inter-GPU collective).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "RK45 steps/s at N=20k (plain FP64, full layout)"
+YEAR = 3.15576e7
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=60)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--nx", type=int, default=100, help="along-strike cells (2 triangles each per row)")
+    p.add_argument("--nz", type=int, default=100, help="down-dip rows")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16"])
+    p.add_argument("--e2e-steps", type=int, default=None)
+    p.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU sample length")
+    return p.parse_args()
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(name):
+    """DRAM bytes per launch from a committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(name)
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            except Exception:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def reduce_max(x, world, args):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if args.impl == "ours" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---- CPU leg: the oracle restatement on a bounded row-block sample ----------------
+
+def cpu_step_rate(cfg, K_rows, threads, target_s):
+    """Steps/s of the oracle's main loop at full size, from a timed row-block
+    sample of its matrix-vector product (the step's dominant cost; the reference
+    distributes exactly these rows over MPI ranks) plus the O(N) remainder
+    timed on the full state."""
+    import oracle
+    n = K_rows.shape[1]
+    m_full = 3 * cfg["n_patch"]
+    v = np.random.default_rng(0).standard_normal(n)
+    # the sample must stream from DRAM like the full matrix: tile it past 256 MB
+    reps_rows = max(1, int(np.ceil(256e6 / K_rows.nbytes)))
+    if reps_rows > 1:
+        K_rows = np.tile(K_rows, (reps_rows, 1))
+    # time the sample matvec with the oracle's OpenMP row-block DGEMV
+    reps, t_mv = 0, 0.0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < target_s * 0.8 or reps < 2:
+        t1 = time.perf_counter()
+        oracle.dgemv_t(K_rows, v, threads)
+        t_mv += time.perf_counter() - t1
+        reps += 1
+    t_mv /= reps
+    rows = K_rows.shape[0]
+    t_full_mv = t_mv * m_full / rows
+    # O(N) remainder: the odefun elementwise parts, RK combinations, error norm
+    # and control, timed on the full state without the products
+    t_rest = oracle.rk_overhead_seconds(cfg)
+    step_s = 6.0 * t_full_mv + t_rest
+    sample = (f"{rows} of {m_full} receiver rows x {n} sources (row-block DGEMV, {reps} reps), "
+              f"extrapolated x{m_full / rows:.0f}; O(N) remainder timed in full")
+    return 1.0 / step_s, sample, t_full_mv
+
+
+# ---- arms ------------------------------------------------------------------------
+
+def run_reference(args, world, rank):
+    """The reference path on the host cores: the oracle restatement (the Fortran
+    drivers cannot be compiled here), all threads, same workload and metric."""
+    import oracle
+    from unicycle_b200 import configs
+    if rank != 0:
+        return None
+    cfg = configs.cfg2(nx=args.nx, nz=args.nz)
+    threads = os.cpu_count() or 1
+    oracle.build(ref=False)
+    i1, i2, i3, v = cfg["mesh"]["tri"]
+    M = oracle.Mesh(cfg["mu"], cfg["lam"], tri=(v, i1, i2, i3))
+    m_full = 3 * cfg["n_patch"]
+    rows = min(m_full, 3 * max(8, min(128, 4 * threads)))
+    t0 = time.perf_counter()
+    G = oracle.build_g_omp(M, 0, rows, threads)
+    t_asm = time.perf_counter() - t0
+    rate, sample, _ = cpu_step_rate(cfg, G, threads, args.cpu_seconds)
+    n = cfg["n_patch"]
+    return {"metric": METRIC, "value": rate, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 / rate, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cfg2 curved megathrust; random Dc)",
+            "impl": "reference",
+            "config": {"workload": f"megathrust {n} Nikkhoo-Walter triangles, full FP64 layout",
+                       "n_triangles": n, "K_shape": [3 * n, 2 * n], "precision": "fp64"},
+            "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": threads, "kind": "port",
+                             "sample": sample + f"; assembly sample {rows} rows in {t_asm:.1f} s"},
+            "assembly": {"mentries_per_s": rows * 2 * n / t_asm / 1e6, "sample_rows": rows},
+            "e2e": {"value": rate, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import unicycle_b200
+    from unicycle_b200 import configs
+
+    torch.cuda.set_device(local)
+    cfg = configs.cfg2(nx=args.nx, nz=args.nz)
+    n = cfg["n_patch"]
+    sim = unicycle_b200.Simulation(cfg["mu"], cfg["lam"], device=local)
+    i1, i2, i3, v = cfg["mesh"]["tri"]
+    sim.set_triangles(i1, i2, i3, v)
+    fr = cfg["friction"]
+    sim.set_friction(fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
+                     fr["damping"])
+    sim.set_tolerance(cfg["epsilon"])
+    stream = torch.cuda.ExternalStream(sim.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sim.buildG()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_asm = e0.elapsed_time(e1) / 1e3
+    mn = 6 * n * n
+    if args.precision != "fp64":
+        sim.set_precision(args.precision)
+    # warm-up
+    sim.set_state(cfg["y0"], 0.0, cfg["dt0"])
+    sim.run(1e300, args.warmup)
+    y_w, t_w, dt_w, acc_w, rej_w = sim.get_state()
+    launches0 = sim.launch_count
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0.record(stream)
+        steps = sim.run(1e300, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    elapsed = e0.elapsed_time(e1) / 1e3
+    launches = sim.launch_count - launches0
+    y_t, t_t, dt_t, acc_t, rej_t = sim.get_state()
+    elapsed_max = reduce_max(elapsed, world, args)
+    # roofline of the dominant kernel (traction product), timed live
+    ms_mv = sim.profile_traction(reps=10)
+    K_bytes = 8.0 * (3 * n) * (2 * n) if args.precision == "fp64" else 4.0 * (3 * n) * (2 * n) + 4.0 * 3 * n
+    alg_bytes = K_bytes + 8.0 * (2 * n + 3 * n)
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes / (ms_mv / 1e3) / 1e9
+    # end to end through the host-array ABI call
+    e2e_steps = args.e2e_steps or max(3, args.steps // 3)
+    y_h, t_h, dt_h = y_t.copy(), t_t, dt_t
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        t_h, y_h, dydt_h, dt_h, _, _ = sim.step(t_h, y_h, dt_h)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_elapsed = reduce_max(e0.elapsed_time(e1) / 1e3, world, args)
+    out = None
+    if rank == 0:
+        value = world * steps / elapsed_max
+        cpu = None
+        if world == 1:
+            K_rows = sim.copy_G(0, 3 * 128) if args.precision == "fp64" else None
+            if K_rows is not None:
+                rate, sample, _ = cpu_step_rate(cfg, K_rows, os.cpu_count() or 1, args.cpu_seconds)
+                cpu = {"value": rate, "unit": "steps/s", "cores": os.cpu_count() or 1, "kind": "port",
+                       "sample": sample}
+        out = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x2/f32",
+            "data": "synthetic (seeded cfg2 curved megathrust; random Dc)",
+            "config": {"workload": f"megathrust {n} Nikkhoo-Walter triangles, full FP64 layout",
+                       "n_triangles": n, "K_shape": [3 * n, 2 * n], "precision": args.precision,
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (K %.1f GB)" % (K_bytes / 1e9),
+                       "rtol": cfg["epsilon"]},
+            "sim_years_per_hour": (t_t - t_w) / YEAR / (elapsed / 3600.0),
+            "rejected_attempts": rej_t - rej_w,
+            "assembly": {"seconds": t_asm, "mentries_per_s": mn / t_asm / 1e6, "entries": mn},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": load_traffic("k_traction"),
+                         "kernel": "k_traction (FP64 K.v + rate-state epilogue)" if args.precision == "fp64"
+                         else "k_traction_split", "ms_per_launch": ms_mv, "peak_source": peak_kind,
+                         "bytes_per_launch": alg_bytes},
+            "e2e": {"value": world * e2e_steps / e2e_elapsed, "unit": "steps/s",
+                    "h2d_bytes_per_step": 8 * 7 * n, "d2h_bytes_per_step": 2 * 8 * 7 * n},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+    sim.close()
+    return out
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+    else:
+        out = run_ours(args, world, rank, local)
+    if out is not None and rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,188 @@
+/*
+ * ucg.h -- C ABI of libucg.so, the B200 (sm_100a) replacement for the 3-D
+ * quasi-dynamic boundary-integral hot path of Unicycle (fortran/3d).
+ *
+ * Plain C types only: pointers, sizes and doubles.  All arrays passed in are
+ * host memory owned by the caller and are copied during the call; the library
+ * owns every device allocation (matrix, state, Runge-Kutta scratch), one CUDA
+ * stream per context.  Every entry point returns an int status (UCG_OK = 0);
+ * none aborts the process.  One host thread per context.
+ *
+ * Coordinates are (north, east, down) in the length unit of the mesh, angles
+ * in radians, element orders rectangles -> triangles -> volumes, exactly as the
+ * reference's input deck and layout (fortran/3d/src/types.f90:125-223).
+ *
+ * Each entry point names the reference interface it replaces.
+ */
+#ifndef UCG_H
+#define UCG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ucg_ctx ucg_ctx;
+
+/* status codes */
+#define UCG_OK                0
+#define UCG_E_BADARG          1   /* invalid argument or size                  */
+#define UCG_E_CUDA            2   /* CUDA runtime error (message: ucg_last_error) */
+#define UCG_E_OOM             3   /* device allocation failed                  */
+#define UCG_E_STEP_UNDERFLOW  4   /* "stepsize underflow in RKQS" (ode45.f90:87-90) */
+#define UCG_E_NONFINITE       5   /* non-finite state or rate detected         */
+#define UCG_E_TIMEOUT         6   /* a bounded device wait gave up             */
+#define UCG_E_STATE           7   /* call out of order (e.g. odefun before assemble) */
+#define UCG_E_UNSUPPORTED     8   /* feature not available in this build       */
+#define UCG_E_NODEVICE        9   /* no CUDA device / extension unusable       */
+
+/* Okada (1992) interface precision (ucg_assemble) */
+#define UCG_OKADA_FP64     0   /* DC3D math and interface in binary64           */
+#define UCG_OKADA_REF32IO  1   /* the reference's REAL*4 DC3D interface (okada92.f90:121-160) */
+
+/* matrix storage for the traction product (ucg_set_precision) */
+#define UCG_PREC_FP64        0  /* K in binary64, FP64 matvec (the plain method) */
+#define UCG_PREC_SPLIT_BF16  1  /* K = diag(s)(hi + lo), bf16 hi/lo, FP32 accumulation */
+
+/* driver conventions (ucg_create flags) */
+#define UCG_DRIVER_RATESTATE      0  /* fortran/3d/src/ratestate.f90     */
+#define UCG_DRIVER_VISCOUSCYCLES  1  /* fortran/3d/src/viscouscycles.f90 */
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Create a context on CUDA device `device` for an elastic half-space with shear
+   modulus mu and Lame parameter lambda.  flags: UCG_DRIVER_*.
+   Replaces the module state set up by init()/initParallelism
+   (fortran/3d/src/ratestate.f90:788-899, 958-1739). */
+int ucg_create(ucg_ctx **ctx, int device, double mu, double lambda, int flags);
+void ucg_destroy(ucg_ctx *ctx);
+const char *ucg_strerror(int status);
+/* Last detailed error message of this context (CUDA error text etc.). */
+const char *ucg_last_error(ucg_ctx *ctx);
+
+/* ---- geometry (copied at the call) --------------------------------------- */
+
+/* n rectangles: x[3*i..3*i+2] upper-left corner (north, east, down), length L,
+   width W, strike and dip in radians.  Replaces in%rectangularPatch and
+   computeReferenceSystemOkada92 (fortran/3d/src/okada92.f90:59-87). */
+int ucg_set_rectangles(ucg_ctx *ctx, int n, const double *x, const double *L,
+                       const double *W, const double *strike, const double *dip);
+
+/* n triangles over nve vertices v[3*k..3*k+2]; i1,i2,i3 are 1-based vertex ids.
+   Replaces in%triangularPatch and computeReferenceSystemStuart97
+   (fortran/3d/src/stuart97.f90:44-101). */
+int ucg_set_triangles(ucg_ctx *ctx, int n, const int *i1, const int *i2, const int *i3,
+                      int nve, const double *v);
+
+/* n vertical cuboid strain volumes: corner x, length L, thickness T, width W,
+   strike.  Replaces in%strainVolume and computeReferenceSystemVerticalStrainVolume
+   (fortran/3d/src/strainvolume.f90:135-163). */
+int ucg_set_volumes(ucg_ctx *ctx, int n, const double *x, const double *L,
+                    const double *T, const double *W, const double *strike);
+
+/* ---- constitutive parameters -------------------------------------------- */
+
+/* Per patch (rectangles then triangles), the PATCH_ELEMENT_STRUCT fields
+   (fortran/3d/src/types.f90:35-40): Vpl, rake, mu0, sig, a, b, L, Vo, damping. */
+int ucg_set_friction(ucg_ctx *ctx, const double *Vpl, const double *rake,
+                     const double *mu0, const double *sig, const double *a,
+                     const double *b, const double *L, const double *Vo,
+                     const double *damping);
+
+/* Per volume: background strain rate e_bg[6*i..] (e11,e12,e13,e22,e23,e33) and
+   the steady-state nonlinear Maxwell fields ngammadot0m, npowerm used by
+   odefun (fortran/3d/src/viscouscycles.f90:938-995).  nonlinear_maxwell != 0
+   mirrors in%strainVolume%nNonlinearMaxwell > 0. */
+int ucg_set_rheology(ucg_ctx *ctx, const double *e_bg, const double *gammadot0m,
+                     const double *npowerm, int nonlinear_maxwell);
+
+/* ---- Green's functions ---------------------------------------------------- */
+
+/* Assemble the stress-interaction matrix on the device, FP64, one thread per
+   (receiver, source) pair.  Replaces buildG (fortran/3d/src/greens.f90:73-275).
+   okada_mode: UCG_OKADA_*. */
+int ucg_assemble(ucg_ctx *ctx, int okada_mode);
+
+/* Sizes of the reference layout G(n,m): n source DOFs, m receiver DOFs. */
+int ucg_dims(ucg_ctx *ctx, long *n, long *m);
+
+/* Copy G in the reference layout: G(c,k) at G[k*ld + c], ld >= n (Fortran
+   column-major, greens.f90:214-216,266-271).  Columns [k0,k1). */
+int ucg_copy_G(ucg_ctx *ctx, double *G, long ld, long k0, long k1);
+
+/* Select the storage of K used by the traction product (UCG_PREC_*).
+   Switching to split-BF16 builds the hi/lo pair from the assembled FP64 K. */
+int ucg_set_precision(ucg_ctx *ctx, int precision);
+
+/* Keep (keep != 0, default) or release the FP64 K after a split-BF16 copy
+   exists, freeing its HBM. */
+int ucg_keep_fp64(ucg_ctx *ctx, int keep);
+
+/* ---- state and right-hand side ------------------------------------------- */
+
+/* Length of the state vector: 7 per patch + 12 per volume
+   (fortran/3d/src/macros.f90:56-79). */
+long ucg_state_len(ucg_ctx *ctx);
+
+/* Reference initial state.  Replaces initStateVector
+   (fortran/3d/src/ratestate.f90:548-610, viscouscycles.f90:710-820).
+   Volume initial stress needs nGm, nQm, nRm, To (per volume); pass NULL when
+   there are no volumes. */
+int ucg_init_state(ucg_ctx *ctx, double *y, const double *nGm, const double *nQm,
+                   const double *nRm, const double *To);
+
+/* dydt = f(y) with host arrays.  Replaces odefun
+   (fortran/3d/src/ratestate.f90:624-778; viscouscycles.f90:834-1093).
+   vmax (may be NULL) receives max patch slip velocity. */
+int ucg_odefun(ucg_ctx *ctx, double t, const double *y, double *dydt, double *vmax);
+
+/* Integrator settings: the module globals `epsilon` and `maximumTimeStep` of
+   fortran/3d/src/ode45.f90:40-43. */
+int ucg_set_tolerance(ucg_ctx *ctx, double epsilon, double max_step);
+
+/* One RKQSm call with host arrays (fortran/3d/src/ode45.f90:51-108): attempts
+   Cash-Karp steps from (t, y) with derivative dydt and error scale yscal until
+   one is accepted.  On return y holds the accepted state, *t += *hdid.
+   Returns UCG_E_STEP_UNDERFLOW where the reference prints "stepsize underflow"
+   and stops.  *nrej (may be NULL) receives the number of rejected attempts. */
+int ucg_rkqs(ucg_ctx *ctx, double *t, double *y, const double *dydt, const double *yscal,
+             double htry, double *hdid, double *hnext, long *nrej);
+
+/* One iteration of the reference main loop (fortran/3d/src/ratestate.f90:307-326)
+   with host arrays: dydt = f(y), yscal = |y| + |dt_next*dydt| + 1e-30, RKQSm,
+   time += dt_done.  dydt receives f(y) at the start of the step (what export()
+   writes).  y is updated in place. */
+int ucg_step(ucg_ctx *ctx, double *time, double *y, double *dydt, double *dt_next,
+             double *dt_done, long *nrej);
+
+/* ---- device-resident integration ---------------------------------------- */
+
+/* Upload y as the device state with time and dt_next (ucg_set_state) or read
+   it back (ucg_get_state).  Counters: accepted steps and rejected attempts. */
+int ucg_set_state(ucg_ctx *ctx, const double *y, double time, double dt_next);
+int ucg_get_state(ucg_ctx *ctx, double *y, double *time, double *dt_next,
+                  long *accepted, long *rejected);
+
+/* March the device state with the reference main loop until time >= t_end or
+   max_steps accepted steps, without host round trips per step (attempts are
+   queued in batches; accept/reject, step size and the time update live on the
+   device).  *steps receives the accepted steps taken.  Returns
+   UCG_E_STEP_UNDERFLOW / UCG_E_NONFINITE as the device detects them. */
+int ucg_run(ucg_ctx *ctx, double t_end, long max_steps, long *steps);
+
+/* Number of kernel launches this context has issued (for launch accounting). */
+long ucg_launch_count(ucg_ctx *ctx);
+
+/* The context's CUDA stream (a cudaStream_t), so that callers can order their
+   own work or timing events with the library's.  No reference counterpart. */
+void *ucg_stream(ucg_ctx *ctx);
+
+/* Launch the traction-product kernel of one Runge-Kutta stage `reps` times on
+   the context stream between CUDA events and return the mean device time per
+   launch in *ms (a measurement aid for the roofline; the state must have been
+   stepped at least once).  No reference counterpart. */
+int ucg_profile_traction(ucg_ctx *ctx, int reps, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

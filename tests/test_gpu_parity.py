@@ -1,0 +1,262 @@
+"""GPU parity tests: the CUDA path through the C ABI against the oracle and the
+golden fixtures made from the reference's own C.
+
+Tolerances (FP64 paths):
+  K entries      |K - G_ref| <= 1e-12 * (max |G_ref| over the receiver's rows);
+                 entries >= 1% of the matrix maximum also <= 1e-12 relative
+  REF32IO mode   the REAL*4 interface rounds gradients to binary32, so a
+                 one-ulp flip of one gradient entry moves a stress by ~2mu*2^-24
+                 of the entry: |dK| <= 1e-6 * element scale and >= 90% of
+                 entries bit-identical to the oracle
+  odefun         |dydt - ref| <= 1e-10 * (component-type scale)
+  histories      log10 V, log10 theta within 1e-9 relative over 1000 accepted
+                 steps of the 512-patch strike-slip fault
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+
+
+def elem_scaled_err(G, ref, dof=3):
+    d = np.abs(G - ref)
+    em = np.abs(ref).reshape(-1, dof, ref.shape[1]).max(axis=(1, 2))
+    return np.max(d / np.repeat(em, dof)[:, None])
+
+
+def big_rel_err(G, ref, frac=1e-2):
+    big = np.abs(ref) > frac * np.abs(ref).max()
+    return np.max(np.abs(G[big] - ref[big]) / np.abs(ref[big]))
+
+
+@pytest.fixture(scope="module")
+def cfg1_small():
+    from unicycle_b200 import configs
+    return configs.cfg1(nx=16, nz=8)
+
+
+def _sim(ucg, cfg, mode=0):
+    from unicycle_b200 import configs
+    sim = ucg.Simulation(cfg["mu"], cfg["lam"])
+    configs.build(sim, cfg, okada_mode=mode)
+    return sim
+
+
+def test_okada_assembly_fp64(ucg, oracle_lib, cfg1_small):
+    sim = _sim(ucg, cfg1_small, 0)
+    K = sim.copy_G()
+    M = oracle_lib.Mesh(cfg1_small["mu"], cfg1_small["lam"], rect=cfg1_small["mesh"]["rect"])
+    G = M.build_g()
+    assert K.shape == G.shape
+    assert elem_scaled_err(K, G) < 1e-12
+    assert big_rel_err(K, G) < 1e-12
+    sim.close()
+
+
+def test_okada_assembly_ref32io(ucg, oracle_lib, cfg1_small):
+    sim = _sim(ucg, cfg1_small, 1)
+    K = sim.copy_G()
+    M = oracle_lib.Mesh(cfg1_small["mu"], cfg1_small["lam"], rect=cfg1_small["mesh"]["rect"],
+                        okada_mode=oracle_lib.OKADA_REF32IO)
+    G = M.build_g()
+    assert elem_scaled_err(K, G) < 1e-6
+    assert np.mean(K == G) > 0.9
+    sim.close()
+
+
+def test_okada_assembly_oblique(ucg, oracle_lib):
+    """Dipping, rotated rectangles (strike 30 deg, dip 50 deg), both modes."""
+    from unicycle_b200 import configs
+    c = configs.cfg1(nx=8, nz=4, size=900.0)
+    x, L, W, st, dp = c["mesh"]["rect"]
+    c["mesh"]["rect"] = (x, L, W, np.full_like(st, np.radians(30.0)), np.full_like(dp, np.radians(50.0)))
+    for mode in (0, 1):
+        sim = _sim(ucg, c, mode)
+        K = sim.copy_G()
+        G = oracle_lib.Mesh(c["mu"], c["lam"], rect=c["mesh"]["rect"], okada_mode=mode).build_g()
+        assert elem_scaled_err(K, G) < (1e-12 if mode == 0 else 1e-6)
+        sim.close()
+
+
+def test_nikkhoo_assembly_vs_reference_golden(ucg):
+    g = np.load(os.path.join(GOLD, "nw15_mesh_G.npz"))
+    sim = ucg.Simulation(float(g["mu"]), float(g["lam"]))
+    sim.set_triangles(g["i1"], g["i2"], g["i3"], g["v"])
+    sim.buildG()
+    K = sim.copy_G()
+    ref = g["G"]
+    assert elem_scaled_err(K, ref) < 1e-12
+    assert big_rel_err(K, ref) < 1e-12
+    sim.close()
+
+
+def test_nikkhoo_assembly_vs_oracle(ucg, oracle_lib):
+    from unicycle_b200 import configs
+    c = configs.cfg2(nx=14, nz=12)
+    i1, i2, i3, v = c["mesh"]["tri"]
+    sim = ucg.Simulation(c["mu"], c["lam"])
+    sim.set_triangles(i1, i2, i3, v)
+    sim.buildG()
+    K = sim.copy_G()
+    G = oracle_lib.Mesh(c["mu"], c["lam"], tri=(v, i1, i2, i3)).build_g()
+    assert elem_scaled_err(K, G) < 1e-12
+    assert big_rel_err(K, G) < 1e-12
+    sim.close()
+
+
+def test_mixed_rect_tri_layout(ucg, oracle_lib):
+    """Rectangles and triangles together: block order and column offsets."""
+    from unicycle_b200 import configs
+    r = configs.cfg1(nx=6, nz=3, size=1000.0)
+    t = configs.cfg2(nx=4, nz=3)
+    i1, i2, i3, v = t["mesh"]["tri"]
+    v = v + np.array([0.0, 20e3, 0.0])
+    sim = ucg.Simulation(r["mu"], r["lam"])
+    sim.set_rectangles(*r["mesh"]["rect"])
+    sim.set_triangles(i1, i2, i3, v)
+    sim.buildG()
+    K = sim.copy_G()
+    G = oracle_lib.Mesh(r["mu"], r["lam"], rect=r["mesh"]["rect"], tri=(v, i1, i2, i3)).build_g()
+    assert K.shape == G.shape == (3 * (18 + 24), 2 * (18 + 24))
+    assert elem_scaled_err(K, G) < 1e-12
+    sim.close()
+
+
+def _odefun_scales(ref, n):
+    r = ref.reshape(n, 7)
+    return np.maximum(np.abs(r).max(axis=0), 1e-300)
+
+
+def test_odefun_matches_oracle(ucg, oracle_lib, cfg1_small):
+    c = cfg1_small
+    sim = _sim(ucg, c)
+    K = sim.copy_G()
+    md = oracle_lib.Model(K, c["friction"])
+    rng = np.random.default_rng(0)
+    n = c["n_patch"]
+    for trial in range(3):
+        y = c["y0"].copy()
+        y[6::7] += rng.normal(0, 1.0, n)          # log10 V perturbation
+        y[5::7] += rng.normal(0, 0.5, n)
+        y[2::7] += rng.normal(0, 1.0, n)
+        y[3::7] += rng.normal(0, 1.0, n)
+        dy, vmax = sim.odefun(y)
+        ref, vref = md.odefun(y)
+        sc = _odefun_scales(ref, n)
+        err = np.abs(dy - ref).reshape(n, 7) / sc
+        assert err.max() < 1e-10, (trial, err.max(axis=0))
+        assert vmax == pytest.approx(vref, rel=1e-14)
+    sim.close()
+
+
+def test_rkqs_matches_oracle(ucg, oracle_lib, cfg1_small):
+    c = cfg1_small
+    sim = _sim(ucg, c)
+    md = oracle_lib.Model(sim.copy_G(), c["friction"])
+    y0 = c["y0"]
+    dydt, _ = md.odefun(y0)
+    for htry in (1e-3, 1e5, 1e7):
+        yscal = np.abs(y0) + np.abs(htry * dydt) + 1e-30
+        t, y1, hdid, hnext, nrej = sim.RKQSm(0.0, y0, dydt, yscal, htry)
+        rc, y1r, hdr, hnr, nrr = md.rkqs(y0, dydt, yscal, htry, c["epsilon"])
+        assert rc == 0 and nrej == nrr
+        assert hdid == pytest.approx(hdr, rel=1e-12)
+        assert hnext == pytest.approx(hnr, rel=1e-9)
+        assert np.max(np.abs(y1 - y1r) / (np.abs(y1r) + 1e-12)) < 1e-9
+    sim.close()
+
+
+def test_history_1000_steps_matches_oracle(ucg, oracle_lib):
+    """The 512-patch strike-slip fault: 1000 accepted main-loop steps through the
+    host-array ABI (ucg_step) against the oracle restatement of the reference
+    main loop.  log10 V and log10 theta within 1e-9 relative, identical
+    accept/reject sequence, times within 1e-9."""
+    from unicycle_b200 import configs
+    c = configs.cfg1()
+    sim = _sim(ucg, c)
+    md = oracle_lib.Model(sim.copy_G(), c["friction"])
+    y = c["y0"].copy()
+    yr = y.copy()
+    t = tr = 0.0
+    dt = dtr = c["dt0"]
+    worst = 0.0
+    for k in range(1000):
+        t, y, dydt, dt, dd, nrej = sim.step(t, y, dt)
+        rc, tr, yr, dydtr, dtr, ddr, nrejr = md.step(tr, yr, dtr, c["epsilon"])
+        assert rc == 0 and nrej == nrejr, k
+        assert t == pytest.approx(tr, rel=1e-9)
+        for col in (5, 6):
+            e = np.max(np.abs(y[col::7] - yr[col::7]) / np.abs(yr[col::7]))
+            worst = max(worst, e)
+    assert worst < 1e-9, worst
+    sim.close()
+
+
+def test_device_run_equals_host_steps(ucg):
+    """ucg_run (device-resident loop, queued attempts) and ucg_step (one host
+    round trip per step) execute the same kernels: identical trajectories."""
+    from unicycle_b200 import configs
+    c = configs.cfg1(nx=16, nz=8)
+    sim = _sim(ucg, c)
+    y, t, dt = c["y0"].copy(), 0.0, c["dt0"]
+    for _ in range(200):
+        t, y, _, dt, _, _ = sim.step(t, y, dt)
+    sim2 = _sim(ucg, c)
+    sim2.set_state(c["y0"], 0.0, c["dt0"])
+    steps = sim2.run(1e30, 200)
+    y2, t2, dt2, acc, rej = sim2.get_state()
+    assert steps == 200 and acc == 200
+    assert t2 == t and dt2 == dt
+    assert np.array_equal(y2, y)
+    sim.close()
+    sim2.close()
+
+
+def test_split_bf16_matvec_error_bound(ucg, cfg1_small):
+    """Split-BF16 K: traction rates within the stated bound of the FP64 path."""
+    c = cfg1_small
+    sim = _sim(ucg, c)
+    y = c["y0"].copy()
+    y[6::7] += np.random.default_rng(1).normal(0, 1.0, c["n_patch"])
+    d64, _ = sim.odefun(y)
+    sim.set_precision("split_bf16")
+    d16, _ = sim.odefun(y)
+    n = c["n_patch"]
+    for col in (2, 3, 4):
+        a, b = d16[col::7], d64[col::7]
+        assert np.max(np.abs(a - b)) <= 1e-4 * np.max(np.abs(b)) + 1e-30, col
+    sim.close()
+
+
+def test_nonfinite_state_reports_status(ucg, cfg1_small):
+    from unicycle_b200 import UcgError
+    c = cfg1_small
+    sim = _sim(ucg, c)
+    y = c["y0"].copy()
+    y[6] = np.nan
+    with pytest.raises(UcgError) as ei:
+        sim.step(0.0, y, 1e-3)
+    assert ei.value.status == 5
+    # the context stays usable
+    t, y1, *_ = sim.step(0.0, c["y0"], 1e-3)
+    assert np.all(np.isfinite(y1))
+    sim.close()
+
+
+def test_stepsize_underflow_reports_status(ucg, cfg1_small):
+    """yscal = 0 makes every error ratio infinite: the step shrinks to zero and
+    the reference's "stepsize underflow in RKQS" becomes UCG_E_STEP_UNDERFLOW."""
+    from unicycle_b200 import UcgError
+    c = cfg1_small
+    sim = _sim(ucg, c)
+    y0 = c["y0"]
+    dydt, _ = sim.odefun(y0)
+    with pytest.raises(UcgError) as ei:
+        sim.RKQSm(0.0, y0, dydt, np.zeros_like(y0), 1.0)
+    assert ei.value.status == 4
+    sim.close()

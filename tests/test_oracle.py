@@ -1,0 +1,211 @@
+"""CPU tests of the oracle: pins against the reference's own C (golden fixtures
+and, where built, the live oracle/_ref library) and physical identities that
+tie the Okada restatement to the reference Nikkhoo-Walter code."""
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+MU = LAM = 30.0e3
+
+
+def rel_err(a, b, floor):
+    return np.max(np.abs(a - b) / np.maximum(np.abs(b), floor))
+
+
+def elem_scaled_err(G, ref, dof=3):
+    """max |G - ref| / (max |ref| over the receiver element's rows).  Entries far
+    below the element's traction scale are sums with heavy cancellation whose
+    last bits are rounding noise in any FP64 evaluation (the reference's own C
+    differs from an 80-bit evaluation there), so they are compared on the
+    element's scale."""
+    d = np.abs(G - ref)
+    em = np.abs(ref).reshape(-1, dof, ref.shape[1]).max(axis=(1, 2))
+    return np.max(d / np.repeat(em, dof)[:, None])
+
+
+def test_nw15_restatement_matches_reference_pairs(oracle_lib):
+    g = np.load(os.path.join(GOLD, "nw15_pairs.npz"))
+    P, X, S = g["P"], g["X"], g["S"]
+    worst = 0.0
+    for k in range(len(X)):
+        for j, (s, d) in enumerate(((1.0, 0.0), (0.0, 1.0))):
+            a = oracle_lib.nw15_stress(X[k], P[k, 0], P[k, 1], P[k, 2], s, d, 0.0, MU, LAM)
+            scale = np.max(np.abs(S[k, j]))
+            worst = max(worst, np.max(np.abs(a - S[k, j])) / scale)
+    # random points include near-singular geometry; the reference itself differs
+    # from an 80-bit evaluation by up to ~4e-6 there
+    assert worst < 1e-6, worst
+
+
+def test_nw15_restatement_matches_reference_mesh(oracle_lib):
+    g = np.load(os.path.join(GOLD, "nw15_mesh_G.npz"))
+    M = oracle_lib.Mesh(MU, LAM, tri=(g["v"], g["i1"], g["i2"], g["i3"]))
+    G = M.build_g()
+    ref = g["G"]
+    assert elem_scaled_err(G, ref) < 1e-12
+    big = np.abs(ref) > 1e-2 * np.abs(ref).max()
+    assert rel_err(G[big], ref[big], 0.0) < 1e-12
+
+
+def test_nw15_live_reference(oracle_lib):
+    if oracle_lib.ref_lib() is None:
+        pytest.skip("reference C sources not present here")
+    rng = np.random.default_rng(5)
+    for _ in range(50):
+        P = rng.uniform([-3e3, -3e3, 1e3], [3e3, 3e3, 6e3], size=(3, 3))
+        x = rng.uniform([-8e3, -8e3, 0.5e3], [8e3, 8e3, 10e3])
+        for s, d in ((1.0, 0.0), (0.0, 1.0)):
+            a = oracle_lib.nw15_stress(x, *P, s, d, 0.0, MU, LAM)
+            b = oracle_lib.nw15_stress_ref(x, *P, s, d, 0.0, MU, LAM)
+            assert np.max(np.abs(a - b)) <= 1e-8 * np.max(np.abs(b))
+
+
+def _rect_as_triangles(q, L, W, strike, dip):
+    sv = np.array([np.cos(strike), np.sin(strike), 0.0])
+    dv = np.array([np.sin(strike) * np.cos(dip), -np.cos(strike) * np.cos(dip), -np.sin(dip)])
+    A = q
+    B = q + L * sv
+    C = q + L * sv - W * dv
+    D = q - W * dv
+    return (A, B, C), (A, C, D)
+
+
+@pytest.mark.parametrize("dip_deg", [90.0, 60.0, 30.0])
+def test_okada_equals_two_triangles(oracle_lib, dip_deg):
+    """A rectangle is two triangles: the Okada restatement against the
+    reference's own Nikkhoo-Walter code (or its restatement) away from edges.
+    Strike 0: the reference's rotation of the gradient back from the strike
+    frame (okada92.f90:172, uxzr = -cos*uxz + sin*uyz) has the opposite sign on
+    the sin*uyz term from the chain rule, so for strike != 0 the reference's
+    Okada stress differs from the two-triangle field; the restatement keeps the
+    reference's expression (see test_okada_reference_uxz_rotation)."""
+    nw = oracle_lib.nw15_stress_ref if oracle_lib.ref_lib() is not None else oracle_lib.nw15_stress
+    q = np.array([0.0, 0.0, 2000.0])
+    L, W, strike, dip = 3000.0, 2000.0, 0.0, np.radians(dip_deg)
+    t1, t2 = _rect_as_triangles(q, L, W, strike, dip)
+    rng = np.random.default_rng(7)
+    worst = 0.0
+    for _ in range(40):
+        x = rng.uniform([-6e3, -6e3, 100.0], [9e3, 9e3, 9e3])
+        for s, d in ((1.0, 0.0), (0.0, 1.0)):
+            ok = oracle_lib.okada_stress(oracle_lib.OKADA_FP64, x, q, L, W, strike, dip, s, d, 0.0, MU, LAM)
+            tr = nw(x, *t1, s, d, 0.0, MU, LAM) + nw(x, *t2, s, d, 0.0, MU, LAM)
+            worst = max(worst, np.max(np.abs(ok - tr)) / np.max(np.abs(tr)))
+    assert worst < 1e-9, worst
+
+
+def test_okada_reference_uxz_rotation(oracle_lib):
+    """For strike != 0 the restatement reproduces the reference's uxzr
+    expression: the difference from the two-triangle field is exactly the stress
+    of the doubled sin(strike)*uyz term in e13."""
+    q = np.array([0.0, 0.0, 2000.0])
+    L, W, strike, dip = 3000.0, 2000.0, np.radians(20.0), np.radians(60.0)
+    t1, t2 = _rect_as_triangles(q, L, W, strike, dip)
+    x = np.array([5000.0, -3000.0, 4000.0])
+    ok = oracle_lib.okada_stress(0, x, q, L, W, strike, dip, 1.0, 0.0, 0.0, MU, LAM)
+    tr = oracle_lib.nw15_stress(x, *t1, 1.0, 0.0, 0.0, MU, LAM) + oracle_lib.nw15_stress(x, *t2, 1.0, 0.0, 0.0, MU, LAM)
+    # DC3D gradient entry uyz for this point (DC3D frame)
+    cs, ss = np.cos(strike), np.sin(strike)
+    X = (x[0] - q[0]) * cs + (x[1] - q[1]) * ss
+    Y = (x[0] - q[0]) * ss - (x[1] - q[1]) * cs
+    _, u = oracle_lib.dc3d(0, 2.0 / 3.0, X, Y, -x[2], q[2], np.degrees(dip), 0.0, L, -W, 0.0, 1.0, 0.0, 0.0)
+    uyz = u[10]
+    # reference: e13 = (uxzr + uzxr)/2 with uxzr carrying +sin*uyz instead of -sin*uyz
+    d13 = 2.0 * MU * (ss * uyz)   # = 2 mu * (half of the 2 sin uyz difference)
+    diff = ok - tr
+    assert abs(diff[2] - d13) < 1e-9 * np.max(np.abs(tr))
+    assert np.max(np.abs(diff[[0, 1, 3, 4, 5]])) < 1e-9 * np.max(np.abs(tr))
+
+
+def test_okada_free_surface_traction_free(oracle_lib):
+    q = np.array([0.0, 0.0, 1000.0])
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        x = np.array([rng.uniform(-5e3, 5e3), rng.uniform(-5e3, 5e3), 0.0])
+        for s, d in ((1.0, 0.0), (0.0, 1.0)):
+            # strike 0: see test_okada_reference_uxz_rotation
+            sig = oracle_lib.okada_stress(oracle_lib.OKADA_FP64, x, q, 2000.0, 1500.0, 0.0, 1.1, s, d, 0.0, MU, LAM)
+            scale = np.max(np.abs(sig))
+            assert np.max(np.abs(sig[[2, 4, 5]])) < 1e-9 * scale
+
+
+def test_nw15_free_surface_traction_free(oracle_lib):
+    P = [np.array([0.0, 0.0, 1000.0]), np.array([2000.0, 500.0, 1500.0]), np.array([500.0, 1500.0, 3000.0])]
+    rng = np.random.default_rng(4)
+    for _ in range(20):
+        x = np.array([rng.uniform(-5e3, 5e3), rng.uniform(-5e3, 5e3), 0.0])
+        for s, d in ((1.0, 0.0), (0.0, 1.0)):
+            sig = oracle_lib.nw15_stress(x, *P, s, d, 0.0, MU, LAM)
+            assert np.max(np.abs(sig[[2, 4, 5]])) < 1e-9 * np.max(np.abs(sig))
+
+
+def test_okada_far_field_decay(oracle_lib):
+    q = np.array([0.0, 0.0, 5000.0])
+    sig1 = oracle_lib.okada_stress(0, np.array([0.0, 50e3, 5000.0]), q, 100.0, 100.0, 0.0, np.pi / 2, 1, 0, 0, MU, LAM)
+    sig2 = oracle_lib.okada_stress(0, np.array([0.0, 100e3, 5000.0]), q, 100.0, 100.0, 0.0, np.pi / 2, 1, 0, 0, MU, LAM)
+    ratio = np.max(np.abs(sig1)) / np.max(np.abs(sig2))
+    assert 6.0 < ratio < 10.0   # ~ r^-3 (half-space corrections perturb it)
+
+
+def test_okada_ref32io_close_to_fp64(oracle_lib):
+    rng = np.random.default_rng(8)
+    q = np.array([1000.0, -500.0, 1500.0])
+    for _ in range(30):
+        x = rng.uniform([-5e3, -5e3, 200.0], [5e3, 5e3, 6e3])
+        a = oracle_lib.okada_stress(0, x, q, 1250.0, 1250.0, 0.4, 1.2, 1, 0, 0, MU, LAM)
+        b = oracle_lib.okada_stress(1, x, q, 1250.0, 1250.0, 0.4, 1.2, 1, 0, 0, MU, LAM)
+        assert np.max(np.abs(a - b)) <= 1e-5 * np.max(np.abs(a))
+
+
+def test_okada_singular_edge_is_zero(oracle_lib):
+    # DC3D rejects points on the fault edge (dc3d.f:69-73) and returns zeros
+    ret, u = oracle_lib.dc3d(0, 2.0 / 3.0, 0.0, 0.0, -1.0, 1.0, 90.0, 0.0, 1.0, -1.0, 0.0, 1.0, 0.0, 0.0)
+    assert ret == 1 and np.all(u == 0.0)
+
+
+def test_rkck_fifth_order_local_error(oracle_lib):
+    """Cash-Karp local error of the 5th-order solution scales as h^5 (the
+    embedded 4th-order difference, yerr, as h^5 too)."""
+    from unicycle_b200 import configs
+    c = configs.cfg1(nx=4, nz=2)
+    M = oracle_lib.Mesh(c["mu"], c["lam"], rect=c["mesh"]["rect"])
+    G = M.build_g()
+    md = oracle_lib.Model(G, c["friction"])
+    y0 = c["y0"]
+    dydt, _ = md.odefun(y0)
+    errs = []
+    for h in (2e6, 1e6):
+        y1, yerr = md.rkck(y0, dydt, h)
+        # reference solution with 64 substeps
+        y = y0.copy()
+        for _ in range(64):
+            k, _ = md.odefun(y)
+            y, _ = md.rkck(y, k, h / 64)
+        errs.append(np.max(np.abs(y1 - y)))
+    assert errs[0] / errs[1] > 20.0   # 2^5 = 32, loosely
+
+
+def test_rkqs_controller_rejects_and_shrinks(oracle_lib):
+    from unicycle_b200 import configs
+    c = configs.cfg1(nx=8, nz=4)
+    M = oracle_lib.Mesh(c["mu"], c["lam"], rect=c["mesh"]["rect"])
+    md = oracle_lib.Model(M.build_g(), c["friction"])
+    y0 = c["y0"]
+    dydt, _ = md.odefun(y0)
+    yscal = np.abs(y0) + np.abs(1e7 * dydt) + 1e-30
+    rc, y1, hdid, hnext, nrej = md.rkqs(y0, dydt, yscal, 1e7, 1e-8)
+    assert rc == 0 and nrej >= 1 and hdid < 1e7 and hnext > 0.0
+
+
+def test_state_init_matches_reference_formula(oracle_lib):
+    from unicycle_b200 import configs
+    c = configs.cfg1(nx=4, nz=2)
+    md = oracle_lib.Model(np.zeros((24, 16)), c["friction"])
+    y = md.init_state()
+    fr = c["friction"]
+    tau = fr["sig"] * (fr["mu0"] + (fr["a"] - fr["b"]) * np.log(fr["Vpl"] / fr["Vo"])) - fr["damping"] * fr["Vpl"]
+    assert np.allclose(y[2::7], tau * np.cos(fr["rake"]), rtol=1e-15)
+    assert np.allclose(y[6::7], np.log10(0.99 * fr["Vpl"]), rtol=1e-15)

@@ -1,0 +1,92 @@
+"""ctypes binding of libucg.so (include/ucg.h).
+
+The shared library is the product: every numerical call goes through it.  If it
+is missing or cannot be loaded the import fails loudly; there is no fallback.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libucg.so")
+
+UCG_OK = 0
+UCG_E_BADARG = 1
+UCG_E_CUDA = 2
+UCG_E_OOM = 3
+UCG_E_STEP_UNDERFLOW = 4
+UCG_E_NONFINITE = 5
+UCG_E_TIMEOUT = 6
+UCG_E_STATE = 7
+UCG_E_UNSUPPORTED = 8
+UCG_E_NODEVICE = 9
+
+UCG_OKADA_FP64 = 0
+UCG_OKADA_REF32IO = 1
+UCG_PREC_FP64 = 0
+UCG_PREC_SPLIT_BF16 = 1
+UCG_DRIVER_RATESTATE = 0
+UCG_DRIVER_VISCOUSCYCLES = 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_lp = ctypes.POINTER(ctypes.c_long)
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_l = ctypes.c_long
+_d = ctypes.c_double
+
+# name -> (restype, argtypes); the complete exported surface of include/ucg.h
+SIGNATURES = {
+    "ucg_create": (_i, [ctypes.POINTER(_vp), _i, _d, _d, _i]),
+    "ucg_destroy": (None, [_vp]),
+    "ucg_strerror": (ctypes.c_char_p, [_i]),
+    "ucg_last_error": (ctypes.c_char_p, [_vp]),
+    "ucg_set_rectangles": (_i, [_vp, _i, _dp, _dp, _dp, _dp, _dp]),
+    "ucg_set_triangles": (_i, [_vp, _i, _ip, _ip, _ip, _i, _dp]),
+    "ucg_set_volumes": (_i, [_vp, _i, _dp, _dp, _dp, _dp, _dp]),
+    "ucg_set_friction": (_i, [_vp] + [_dp] * 9),
+    "ucg_set_rheology": (_i, [_vp, _dp, _dp, _dp, _i]),
+    "ucg_assemble": (_i, [_vp, _i]),
+    "ucg_dims": (_i, [_vp, _lp, _lp]),
+    "ucg_copy_G": (_i, [_vp, _dp, _l, _l, _l]),
+    "ucg_set_precision": (_i, [_vp, _i]),
+    "ucg_keep_fp64": (_i, [_vp, _i]),
+    "ucg_state_len": (_l, [_vp]),
+    "ucg_init_state": (_i, [_vp, _dp, _dp, _dp, _dp, _dp]),
+    "ucg_odefun": (_i, [_vp, _d, _dp, _dp, _dp]),
+    "ucg_set_tolerance": (_i, [_vp, _d, _d]),
+    "ucg_rkqs": (_i, [_vp, _dp, _dp, _dp, _dp, _d, _dp, _dp, _lp]),
+    "ucg_step": (_i, [_vp, _dp, _dp, _dp, _dp, _dp, _lp]),
+    "ucg_set_state": (_i, [_vp, _dp, _d, _d]),
+    "ucg_get_state": (_i, [_vp, _dp, _dp, _dp, _lp, _lp]),
+    "ucg_run": (_i, [_vp, _d, _l, _lp]),
+    "ucg_launch_count": (_l, [_vp]),
+    "ucg_stream": (_vp, [_vp]),
+    "ucg_profile_traction": (_i, [_vp, _i, _dp]),
+}
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    """Load libucg.so and bind every entry point; raises if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(
+            f"libucg.so not found at {path}: build it with `python -m unicycle_b200.build` "
+            "(or __graft_entry__.build()); there is no CPU fallback")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class UcgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status

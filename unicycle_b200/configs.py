@@ -1,0 +1,134 @@
+"""Seeded synthetic workloads of the 3-D quasi-dynamic benchmark configurations.
+
+Units: lengths in m, stresses in MPa, time in s, angles in radians.
+Every generator returns plain numpy dictionaries:
+  mesh:     {"rect": (x, L, W, strike, dip)} and/or {"tri": (i1, i2, i3, v)}
+  friction: per patch Vpl, rake, mu0, sig, a, b, L, Vo, damping
+  y0:       initial state vector (7 per patch)
+plus the elastic moduli and integration settings.  Values the benchmark
+descriptions leave open (mu0 = 0.6, Vo = 1e-6 m/s, 1 yr = 3.15576e7 s, the
+megathrust bottom depth) are fixed here and recorded in the returned dict.
+"""
+import numpy as np
+
+YEAR = 3.15576e7
+MU = 30.0e3          # MPa
+NU = 0.25
+LAM = 2.0 * MU * NU / (1.0 - 2.0 * NU)   # = MU for nu = 1/4
+VS = 3464.0          # m/s
+ETA = MU / (2.0 * VS)  # MPa s / m (radiation damping)
+MU0 = 0.6
+VO = 1.0e-6
+LG10 = np.log(10.0)
+
+
+def steady_state(V0, fr):
+    """Initial state at steady state theta = L/V0, traction along the rake
+    (fortran/3d/src/ratestate.f90:589-607 with V0 in place of 0.99 Vpl)."""
+    n = len(V0)
+    y = np.zeros(7 * n)
+    tau = fr["sig"] * (fr["mu0"] + (fr["a"] - fr["b"]) * np.log(V0 / fr["Vo"])) - fr["damping"] * V0
+    y[2::7] = tau * np.cos(fr["rake"])
+    y[3::7] = tau * np.sin(fr["rake"])
+    y[5::7] = np.log(fr["L"] / V0) / LG10
+    y[6::7] = np.log(V0) / LG10
+    return y
+
+
+def cfg1(nx=32, nz=16, size=1250.0, seed=1):
+    """Vertical strike-slip fault, nx x nz Okada rectangles of `size` m, a central
+    velocity-weakening zone (columns 5-28, rows 5-12 of 32 x 16), V0 = 0.9 Vpl
+    lognormal(0, 0.1), rtol 1e-8, 300 yr."""
+    ix, iz = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    ix, iz = ix.ravel(), iz.ravel()
+    n = nx * nz
+    x = np.stack([ix * size, np.zeros(n), iz * size], axis=1).astype(float)
+    L = np.full(n, size)
+    W = np.full(n, size)
+    strike = np.zeros(n)
+    dip = np.full(n, np.pi / 2)
+    # velocity-weakening window scaled from the 32 x 16 layout
+    c0, c1 = int(round(4 * nx / 32)), int(round(28 * nx / 32))
+    r0, r1 = int(round(4 * nz / 16)), int(round(12 * nz / 16))
+    vw = (ix >= c0) & (ix < c1) & (iz >= r0) & (iz < r1)
+    fr = dict(Vpl=np.full(n, 1.0e-9), rake=np.zeros(n), mu0=np.full(n, MU0), sig=np.full(n, 50.0),
+              a=np.full(n, 0.01), b=np.where(vw, 0.014, 0.006), L=np.full(n, 0.01), Vo=np.full(n, VO),
+              damping=np.full(n, ETA))
+    rng = np.random.default_rng(seed)
+    V0 = 0.9 * fr["Vpl"] * np.exp(0.1 * rng.standard_normal(n))
+    return dict(name=f"cfg1-strike-slip-{nx}x{nz}", mu=MU, lam=LAM, mesh=dict(rect=(x, L, W, strike, dip)),
+                friction=fr, y0=steady_state(V0, fr), epsilon=1.0e-8, t_end=300 * YEAR, dt0=1.0e-3,
+                n_patch=n)
+
+
+def megathrust_mesh(nx=100, nz=100, dx=2000.0, z_bottom=50.0e3):
+    """Curved thrust surface: strike north, dipping east; dip 10 deg at the trench
+    rising linearly to 25 deg at 40 km depth, constant below; bottom edge at
+    z_bottom.  nx along-strike cells of dx, nz down-dip rows of equal down-dip
+    length; every quad split into 2 triangles."""
+    # profile: integrate dz/ds = sin(dip(z)), dx/ds = cos(dip(z)) to z_bottom
+    def dip_at(z):
+        return np.radians(10.0 + 15.0 * np.clip(z / 40.0e3, 0.0, 1.0))
+    ds = 1.0
+    s_pts, e_pts, z_pts = [0.0], [0.0], [0.0]
+    while z_pts[-1] < z_bottom:
+        d = dip_at(z_pts[-1] + 0.5 * ds * np.sin(dip_at(z_pts[-1])))
+        e_pts.append(e_pts[-1] + ds * np.cos(d))
+        z_pts.append(z_pts[-1] + ds * np.sin(d))
+        s_pts.append(s_pts[-1] + ds)
+    s_pts, e_pts, z_pts = map(np.asarray, (s_pts, e_pts, z_pts))
+    s_tot = np.interp(z_bottom, z_pts, s_pts)
+    s_nodes = np.linspace(0.0, s_tot, nz + 1)
+    e_nodes = np.interp(s_nodes, s_pts, e_pts)
+    z_nodes = np.interp(s_nodes, s_pts, z_pts)
+    n_nodes = np.arange(nx + 1) * dx
+    N, K = np.meshgrid(n_nodes, np.arange(nz + 1), indexing="ij")
+    v = np.stack([N.ravel(), e_nodes[K.ravel()], z_nodes[K.ravel()]], axis=1)
+    vid = lambda i, k: i * (nz + 1) + k + 1   # 1-based
+    i1, i2, i3 = [], [], []
+    for i in range(nx):
+        for k in range(nz):
+            a, b, c, d = vid(i, k), vid(i + 1, k), vid(i + 1, k + 1), vid(i, k + 1)
+            i1 += [a, a]
+            i2 += [b, c]
+            i3 += [c, d]
+    return np.array(i1), np.array(i2), np.array(i3), v
+
+
+def tri_centroids(i1, i2, i3, v):
+    return (v[i1 - 1] + v[i2 - 1] + v[i3 - 1]) / 3.0
+
+
+def cfg2(nx=100, nz=100, seed=2):
+    """Curved megathrust, Nikkhoo-Walter triangles (2 nx nz of them), rake 90,
+    a = 0.01 with depth-dependent a-b, Dc log-uniform [5, 50] mm,
+    sigma = min(18 MPa/km * z, 50 MPa), 1000 yr."""
+    i1, i2, i3, v = megathrust_mesh(nx, nz)
+    n = len(i1)
+    zc = tri_centroids(i1, i2, i3, v)[:, 2] / 1.0e3   # km
+    amb = np.interp(zc, [0.0, 5.0, 10.0, 35.0, 40.0, 1.0e9], [0.004, 0.004, -0.004, -0.004, 0.004, 0.004])
+    a = np.full(n, 0.01)
+    rng = np.random.default_rng(seed)
+    Dc = np.exp(rng.uniform(np.log(5.0e-3), np.log(50.0e-3), n))
+    sig = np.minimum(18.0 * zc, 50.0)
+    fr = dict(Vpl=np.full(n, 1.0e-9), rake=np.full(n, np.pi / 2), mu0=np.full(n, MU0), sig=sig, a=a,
+              b=a - amb, L=Dc, Vo=np.full(n, VO), damping=np.full(n, ETA))
+    V0 = 0.9 * fr["Vpl"]
+    return dict(name=f"cfg2-megathrust-{n}tri", mu=MU, lam=LAM, mesh=dict(tri=(i1, i2, i3, v)), friction=fr,
+                y0=steady_state(np.full(n, V0[0]), fr), epsilon=1.0e-8, t_end=1000 * YEAR, dt0=1.0e-3,
+                n_patch=n, z_bottom=50.0e3)
+
+
+def build(sim, cfg, okada_mode=0):
+    """Load a config into a Simulation and assemble its Green's functions."""
+    m = cfg["mesh"]
+    if "rect" in m:
+        sim.set_rectangles(*m["rect"])
+    if "tri" in m:
+        sim.set_triangles(*m["tri"])
+    fr = cfg["friction"]
+    sim.set_friction(fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
+                     fr["damping"])
+    sim.set_tolerance(cfg["epsilon"])
+    sim.buildG(okada_mode)
+    return sim

@@ -1,0 +1,90 @@
+// Forward-mode dual numbers for device code: a value and its gradient with
+// respect to the three observation coordinates.  Evaluating a closed-form
+// displacement field on these yields its exact displacement gradient (to
+// rounding), from which strain and stress follow.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace ucg {
+
+struct Dd {
+    double v, x, y, z;
+};
+
+__device__ __forceinline__ Dd dd(double c) { return Dd{c, 0.0, 0.0, 0.0}; }
+__device__ __forceinline__ Dd operator+(Dd a, Dd b) { return Dd{a.v + b.v, a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ Dd operator-(Dd a, Dd b) { return Dd{a.v - b.v, a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ Dd operator-(Dd a) { return Dd{-a.v, -a.x, -a.y, -a.z}; }
+__device__ __forceinline__ Dd operator*(Dd a, Dd b)
+{
+    return Dd{a.v * b.v, a.x * b.v + a.v * b.x, a.y * b.v + a.v * b.y, a.z * b.v + a.v * b.z};
+}
+__device__ __forceinline__ Dd operator+(Dd a, double c) { return Dd{a.v + c, a.x, a.y, a.z}; }
+__device__ __forceinline__ Dd operator+(double c, Dd a) { return Dd{a.v + c, a.x, a.y, a.z}; }
+__device__ __forceinline__ Dd operator-(Dd a, double c) { return Dd{a.v - c, a.x, a.y, a.z}; }
+__device__ __forceinline__ Dd operator-(double c, Dd a) { return Dd{c - a.v, -a.x, -a.y, -a.z}; }
+__device__ __forceinline__ Dd operator*(Dd a, double c) { return Dd{a.v * c, a.x * c, a.y * c, a.z * c}; }
+__device__ __forceinline__ Dd operator*(double c, Dd a) { return Dd{a.v * c, a.x * c, a.y * c, a.z * c}; }
+// reciprocal carries one division; quotients multiply by it
+__device__ __forceinline__ Dd rcp(Dd a)
+{
+    double r = 1.0 / a.v, s = -r * r;
+    return Dd{r, s * a.x, s * a.y, s * a.z};
+}
+__device__ __forceinline__ Dd operator/(Dd a, Dd b)
+{
+    double r = 1.0 / b.v, q = a.v * r;
+    return Dd{q, (a.x - q * b.x) * r, (a.y - q * b.y) * r, (a.z - q * b.z) * r};
+}
+__device__ __forceinline__ Dd operator/(Dd a, double c)
+{
+    double r = 1.0 / c;
+    return Dd{a.v * r, a.x * r, a.y * r, a.z * r};
+}
+__device__ __forceinline__ Dd operator/(double c, Dd a)
+{
+    double r = 1.0 / a.v, q = c * r, s = -q * r;
+    return Dd{q, s * a.x, s * a.y, s * a.z};
+}
+__device__ __forceinline__ Dd dsqrt(Dd a)
+{
+    double s = sqrt(a.v), h = 0.5 / s;
+    return Dd{s, h * a.x, h * a.y, h * a.z};
+}
+__device__ __forceinline__ Dd dlog(Dd a)
+{
+    double r = 1.0 / a.v;
+    return Dd{log(a.v), r * a.x, r * a.y, r * a.z};
+}
+__device__ __forceinline__ Dd datan(Dd a)
+{
+    double r = 1.0 / (1.0 + a.v * a.v);
+    return Dd{atan(a.v), r * a.x, r * a.y, r * a.z};
+}
+__device__ __forceinline__ Dd datan2(Dd y, Dd x)
+{
+    double r = 1.0 / (x.v * x.v + y.v * y.v);
+    return Dd{atan2(y.v, x.v), (x.v * y.x - y.v * x.x) * r, (x.v * y.y - y.v * x.y) * r,
+              (x.v * y.z - y.v * x.z) * r};
+}
+// gradient-only variants: the value of the log / arctangent is not needed when
+// only the gradient of the field is formed (the value never feeds back into a
+// product), which saves the transcendental evaluation.
+__device__ __forceinline__ Dd dlog_g(Dd a)
+{
+    double r = 1.0 / a.v;
+    return Dd{0.0, r * a.x, r * a.y, r * a.z};
+}
+__device__ __forceinline__ Dd datan_g(Dd a)
+{
+    double r = 1.0 / (1.0 + a.v * a.v);
+    return Dd{0.0, r * a.x, r * a.y, r * a.z};
+}
+__device__ __forceinline__ Dd datan2_g(Dd y, Dd x)
+{
+    double r = 1.0 / (x.v * x.v + y.v * y.v);
+    return Dd{0.0, (x.v * y.x - y.v * x.x) * r, (x.v * y.y - y.v * x.y) * r,
+              (x.v * y.z - y.v * x.z) * r};
+}
+
+}  // namespace ucg

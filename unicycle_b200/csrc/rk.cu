@@ -1,0 +1,655 @@
+// Right-hand side and Cash-Karp RK4(5) stepping on the device.
+//
+// One attempt of RKQSm (fortran/3d/src/ode45.f90:51-108) is a fixed sequence of
+// launches, captured once into a CUDA graph:
+//
+//   stage 1   k_prologue<1>  commit an accepted candidate, v = V(cos,sin)(rake)-Vpl
+//             k_traction<1>  t = K v  fused with the rate-state / Maxwell epilogue
+//   stage s   k_prologue<s>  ytmp = y + h*sum_j b_sj k_j  (BLAS-1 order of RKCKm)
+//             k_traction<s>  k_s = f(ytmp)                              (s = 2..6)
+//   finish    k_finish       ycand, yerr, max|yerr/yscal| (ordered-bit atomicMax)
+//   control   k_control      accept/reject, step size, time, counters (1 thread)
+//
+// Every kernel reads the control block first and returns at once when the
+// integration is inactive, or (stage 1) when the state did not change since the
+// last f(y), so the same graph serves accepted and rejected attempts and many
+// attempts can be queued without host round trips.
+//
+// The stage combinations, yout and yerr follow the reference's operation order
+// with explicit round-to-nearest multiplies and adds (no FMA contraction), so
+// they round exactly as the oracle's restatement of RKCKm.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include "ucg_internal.cuh"
+
+namespace ucg {
+
+__device__ __constant__ double c_B[6][5] = {
+    {0, 0, 0, 0, 0},
+    {0.2, 0, 0, 0, 0},
+    {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
+    {0.3, -0.9, 1.2, 0, 0},
+    {-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0},
+    {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+
+#define C1 (37.0 / 378.0)
+#define C3 (250.0 / 621.0)
+#define C4 (125.0 / 594.0)
+#define C6 (512.0 / 1771.0)
+#define DC1 (C1 - 2825.0 / 27648.0)
+#define DC3 (C3 - 18575.0 / 48384.0)
+#define DC4 (C4 - 13525.0 / 55296.0)
+#define DC5 (-277.0 / 14336.0)
+#define DC6 (C6 - 0.25)
+
+static const double LG10 = 2.302585092994045684017991454684364208;
+
+struct StageArgs {
+    const double *y;       // state at the start of the step
+    double *ys;            // stage state written by the prologue (y itself for stage 1)
+    double *k[6];
+    double *v;
+    double *ycand, *yerr, *yscal;
+    Friction fr;
+    Rheology rh;
+    int np, nvol;
+    long len;
+};
+
+__device__ __forceinline__ bool ctl_live(const Ctl *c) { return c->active && c->status == 0; }
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long *p, double x)
+{
+    // non-negative doubles order like their bit patterns
+    atomicMax(p, (unsigned long long)__double_as_longlong(x));
+}
+
+// ---- stage prologue ------------------------------------------------------------
+
+// stage combination for one entry with the reference BLAS-1 order
+template <int S>
+__device__ __forceinline__ double stage_comb(const StageArgs &a, long i, double h)
+{
+    const double y = a.y[i];
+    if (S == 1) return y;
+    if (S == 2) return __dadd_rn(y, __dmul_rn(__dmul_rn(h, c_B[1][0]), a.k[0][i]));
+    double r = __dmul_rn(c_B[S - 1][0], a.k[0][i]);
+#pragma unroll
+    for (int j = 1; j < S - 1; j++) r = __dadd_rn(r, __dmul_rn(c_B[S - 1][j], a.k[j][i]));
+    return __dadd_rn(y, __dmul_rn(h, r));
+}
+
+template <int S>
+__global__ void k_prologue(StageArgs a, Ctl *ctl)
+{
+    if (!ctl_live(ctl)) return;
+    if (S == 1 && !ctl->need_stage1) return;
+    const double h = ctl->h;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ne = a.np + a.nvol;
+    if (e >= ne) return;
+    const bool patch = e < a.np;
+    const long o = patch ? 7L * e : 7L * a.np + 12L * (e - a.np);
+    const int w = patch ? 7 : 12;
+    double *ys = a.ys;
+    if (S == 1) {
+        if (ctl->pending) {
+            double *y = const_cast<double *>(a.y);
+            for (int q = 0; q < w; q++) y[o + q] = a.ycand[o + q];
+        }
+    } else {
+        for (int q = 0; q < w; q++) ys[o + q] = stage_comb<S>(a, o + q, h);
+        if (S == 2 && ctl->need_stage1) {
+            // yscal = |y| + |dt_try*dydt| + TINY (ratestate.f90:315); h == dt_try here
+            for (int q = 0; q < w; q++)
+                a.yscal[o + q] = fabs(a.y[o + q]) + fabs(h * a.k[0][o + q]) + 1.0e-30;
+        }
+    }
+    const double *yy = (S == 1) ? a.y : ys;
+    double *ks = a.k[S - 1];
+    if (patch) {
+        // ratestate.f90:667-707
+        const double rake = atan2(yy[o + 3], yy[o + 2]);
+        const double vel = exp(yy[o + 6] * LG10);
+        const double vs = vel * cos(rake), vd = vel * sin(rake);
+        ks[o + 0] = vs;
+        ks[o + 1] = vd;
+        a.v[2L * e + 0] = vs - a.fr.vpl_c[e];
+        a.v[2L * e + 1] = vd - a.fr.vpl_s[e];
+        if (S == 1) atomic_max_pos((unsigned long long *)&ctl->vmax, vel);
+        if (!isfinite(vel) || !isfinite(rake)) ctl->nonfinite = 1;
+    } else {
+        // viscouscycles.f90:938-995
+        const int iv = e - a.np;
+        double s11 = yy[o + 6], s12 = yy[o + 7], s13 = yy[o + 8];
+        double s22 = yy[o + 9], s23 = yy[o + 10], s33 = yy[o + 11];
+        const double p = (s11 + s22 + s33) / 3.0;
+        s11 = s11 - p; s22 = s22 - p; s33 = s33 - p;
+        double ev[6] = {0, 0, 0, 0, 0, 0};
+        if (a.rh.nonlinear) {
+            const double sII = sqrt((s11 * s11 + 2.0 * s12 * s12 + 2.0 * s13 * s13 + s22 * s22 +
+                                     2.0 * s23 * s23 + s33 * s33) / 2.0);
+            const double eII = a.rh.gd0[iv] * pow(sII, a.rh.npow[iv] - 1);
+            ev[0] += eII * s11; ev[1] += eII * s12; ev[2] += eII * s13;
+            ev[3] += eII * s22; ev[4] += eII * s23; ev[5] += eII * s33;
+        }
+        for (int q = 0; q < 6; q++) {
+            ks[o + q] = ev[q];
+            a.v[2L * a.np + 6L * iv + q] = ev[q] - a.rh.ebg[6L * iv + q];
+        }
+    }
+}
+
+// ---- traction product fused with the right-hand side ----------------------------
+//
+// K (m x n, row-major) times v.  A CTA owns 12 consecutive rows: 4 patches
+// (3 rows each) or 2 volumes (6 rows each).  Its 8 warps sweep interleaved
+// 64-column slices of those 12 rows, so every v element loaded feeds 12 K
+// elements; K is streamed once with 16-byte non-allocating loads.  The 12 row
+// sums are reduced across lanes and warps, and the elementwise rate-state
+// (ratestate.f90:731-776) or Maxwell (viscouscycles.f90:1072-1080) epilogue of
+// each owned element runs on the reduced values, writing k_s directly.
+
+constexpr int MV_WARPS = 8;
+constexpr int MV_ROWS = 12;
+
+__device__ __forceinline__ double2 ld_stream(const double *p)
+{
+    double2 r;
+    asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(r.x), "=d"(r.y) : "l"(p));
+    return r;
+}
+
+__device__ __forceinline__ void rhs_patch(const StageArgs &a, const double *yy, double *ks, int e,
+                                          const double t[3])
+{
+    const long o = 7L * e;
+    const double rake = atan2(yy[o + 3], yy[o + 2]);
+    const double vel = exp(yy[o + 6] * LG10);
+    const double L = a.fr.L[e], bb = a.fr.b[e], sg = a.fr.sig[e], aa = a.fr.a[e], eta = a.fr.damping[e];
+    const double cr = cos(rake), sr = sin(rake);
+    const double dth = (exp(-yy[o + 5] * LG10) - vel / L) / LG10;
+    const double dtau = t[0] * cr + t[1] * sr;
+    const double dv = (dtau - bb * sg * dth * LG10) / (aa * sg + eta * vel) / LG10;
+    const double corr = eta * vel * dv * LG10;
+    ks[o + 2] = t[0] - corr * cr;
+    ks[o + 3] = t[1] - corr * sr;
+    ks[o + 4] = t[2];
+    ks[o + 5] = dth;
+    ks[o + 6] = dv;
+}
+
+template <int S>
+__global__ void __launch_bounds__(MV_WARPS * 32) k_traction(const double *__restrict__ K, long n,
+                                                             StageArgs a, Ctl *ctl, int pblocks,
+                                                             int vblocks)
+{
+    if (!ctl_live(ctl)) return;
+    if (S == 1 && !ctl->need_stage1) return;
+    __shared__ double red[MV_WARPS][MV_ROWS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double *yy = (S == 1) ? a.y : a.ys;
+    double *ks = a.k[S - 1];
+    for (int blk = blockIdx.x; blk < pblocks + vblocks; blk += gridDim.x) {
+        long row0;
+        int nrows, e0, nel;
+        bool patch = blk < pblocks;
+        if (patch) {
+            e0 = blk * 4;
+            nel = min(4, a.np - e0);
+            row0 = 3L * e0;
+            nrows = 3 * nel;
+        } else {
+            e0 = (blk - pblocks) * 2;
+            nel = min(2, a.nvol - e0);
+            row0 = 3L * a.np + 6L * e0;
+            nrows = 6 * nel;
+        }
+        double acc[MV_ROWS];
+#pragma unroll
+        for (int r = 0; r < MV_ROWS; r++) acc[r] = 0.0;
+        const double *Kr = K + row0 * n;
+        for (long c = 64L * warp + 2 * lane; c < n; c += 64L * MV_WARPS) {
+            const double2 vv = *reinterpret_cast<const double2 *>(a.v + c);
+            if (nrows == MV_ROWS) {
+                double2 kv[MV_ROWS];
+#pragma unroll
+                for (int r = 0; r < MV_ROWS; r++) kv[r] = ld_stream(Kr + r * n + c);
+#pragma unroll
+                for (int r = 0; r < MV_ROWS; r++) acc[r] = fma(kv[r].y, vv.y, fma(kv[r].x, vv.x, acc[r]));
+            } else {
+#pragma unroll
+                for (int r = 0; r < MV_ROWS; r++) {
+                    if (r < nrows) {
+                        double2 kv = ld_stream(Kr + r * n + c);
+                        acc[r] = fma(kv.y, vv.y, fma(kv.x, vv.x, acc[r]));
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < MV_ROWS; r++) {
+            double s = acc[r];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+            acc[r] = s;
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int r = 0; r < MV_ROWS; r++) red[warp][r] = acc[r];
+        }
+        __syncthreads();
+        if (threadIdx.x < nel) {
+            const int q = threadIdx.x;
+            if (patch) {
+                double t[3];
+                for (int c3 = 0; c3 < 3; c3++) {
+                    double s = 0.0;
+                    for (int w = 0; w < MV_WARPS; w++) s += red[w][3 * q + c3];
+                    t[c3] = s;
+                }
+                rhs_patch(a, yy, ks, e0 + q, t);
+            } else {
+                const long o = 7L * a.np + 12L * (e0 + q);
+                for (int c6 = 0; c6 < 6; c6++) {
+                    double s = 0.0;
+                    for (int w = 0; w < MV_WARPS; w++) s += red[w][6 * q + c6];
+                    ks[o + 6 + c6] = s;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Split-BF16 variant: K = diag(s) (hi + lo) with hi, lo stored interleaved as
+// bf16 pairs (4 bytes per entry, half the FP64 bytes).  Products and sums are
+// FP32; the per-row scale is applied in FP64 before the same epilogue.
+template <int S>
+__global__ void __launch_bounds__(MV_WARPS * 32) k_traction_split(const __nv_bfloat162 *__restrict__ Kp,
+        const float *__restrict__ scale, long n, StageArgs a, Ctl *ctl, int pblocks, int vblocks)
+{
+    if (!ctl_live(ctl)) return;
+    if (S == 1 && !ctl->need_stage1) return;
+    __shared__ double red[MV_WARPS][MV_ROWS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double *yy = (S == 1) ? a.y : a.ys;
+    double *ks = a.k[S - 1];
+    for (int blk = blockIdx.x; blk < pblocks + vblocks; blk += gridDim.x) {
+        long row0;
+        int nrows, e0, nel;
+        const bool patch = blk < pblocks;
+        if (patch) {
+            e0 = blk * 4; nel = min(4, a.np - e0); row0 = 3L * e0; nrows = 3 * nel;
+        } else {
+            e0 = (blk - pblocks) * 2; nel = min(2, a.nvol - e0); row0 = 3L * a.np + 6L * e0; nrows = 6 * nel;
+        }
+        float acc[MV_ROWS];
+#pragma unroll
+        for (int r = 0; r < MV_ROWS; r++) acc[r] = 0.0f;
+        const __nv_bfloat162 *Kr = Kp + row0 * n;
+        // 4 columns per lane per step (one 16-byte load per row); n is a multiple of 2
+        for (long c = 128L * warp + 4 * lane; c < n; c += 128L * MV_WARPS) {
+            const bool full = c + 4 <= n;
+            float vv[4];
+            {
+                const double2 v01 = *reinterpret_cast<const double2 *>(a.v + c);
+                vv[0] = (float)v01.x; vv[1] = (float)v01.y;
+                if (full) {
+                    const double2 v23 = *reinterpret_cast<const double2 *>(a.v + c + 2);
+                    vv[2] = (float)v23.x; vv[3] = (float)v23.y;
+                } else {
+                    vv[2] = 0.0f; vv[3] = 0.0f;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < MV_ROWS; r++) {
+                if (r < nrows) {
+                    const __nv_bfloat162 *p = Kr + r * n + c;
+                    uint4 raw;
+                    if (full) {
+                        asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+                                     : "=r"(raw.x), "=r"(raw.y), "=r"(raw.z), "=r"(raw.w) : "l"(p));
+                    } else {
+                        uint2 h2 = *reinterpret_cast<const uint2 *>(p);
+                        raw = make_uint4(h2.x, h2.y, 0u, 0u);
+                    }
+                    const uint32_t w4[4] = {raw.x, raw.y, raw.z, raw.w};
+                    float s = acc[r];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float hi = __uint_as_float(w4[q] << 16);
+                        const float lo = __uint_as_float(w4[q] & 0xffff0000u);
+                        s = fmaf(hi, vv[q], s);
+                        s = fmaf(lo, vv[q], s);
+                    }
+                    acc[r] = s;
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < MV_ROWS; r++) {
+            float s = acc[r];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+            acc[r] = s;
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int r = 0; r < MV_ROWS; r++) red[warp][r] = (double)acc[r];
+        }
+        __syncthreads();
+        if (threadIdx.x < nel) {
+            const int q = threadIdx.x;
+            if (patch) {
+                double t[3];
+                for (int c3 = 0; c3 < 3; c3++) {
+                    double s = 0.0;
+                    for (int w = 0; w < MV_WARPS; w++) s += red[w][3 * q + c3];
+                    t[c3] = s * (double)scale[row0 + 3 * q + c3];
+                }
+                rhs_patch(a, yy, ks, e0 + q, t);
+            } else {
+                const long o = 7L * a.np + 12L * (e0 + q);
+                for (int c6 = 0; c6 < 6; c6++) {
+                    double s = 0.0;
+                    for (int w = 0; w < MV_WARPS; w++) s += red[w][6 * q + c6];
+                    ks[o + 6 + c6] = s * (double)scale[row0 + 6 * q + c6];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---- finish: candidate, error estimate, error norm ------------------------------
+
+__global__ void k_finish(StageArgs a, Ctl *ctl)
+{
+    if (!ctl_live(ctl)) return;
+    const double h = ctl->h;
+    double mx = 0.0;
+    bool bad = false;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < a.len; i += (long)gridDim.x * blockDim.x) {
+        const double k1 = a.k[0][i], k3 = a.k[2][i], k4 = a.k[3][i], k5 = a.k[4][i], k6 = a.k[5][i];
+        // ode45.f90:184-200
+        double r = __dmul_rn(C1, k1);
+        r = __dadd_rn(r, __dmul_rn(C3, k3));
+        r = __dadd_rn(r, __dmul_rn(C4, k4));
+        r = __dadd_rn(r, __dmul_rn(C6, k6));
+        const double yc = __dadd_rn(a.y[i], __dmul_rn(h, r));
+        double e = __dmul_rn(DC1, k1);
+        e = __dadd_rn(e, __dmul_rn(DC3, k3));
+        e = __dadd_rn(e, __dmul_rn(DC4, k4));
+        e = __dadd_rn(e, __dmul_rn(DC5, k5));
+        e = __dadd_rn(e, __dmul_rn(DC6, k6));
+        e = __dmul_rn(h, e);
+        a.ycand[i] = yc;
+        a.yerr[i] = e;
+        // MAXVAL semantics: a NaN ratio (0/0) does not raise the maximum; an
+        // infinite one does and drives the step to underflow as in the
+        // reference.  A non-finite candidate state is reported as such.
+        const double q = fabs(e / a.yscal[i]);
+        if (!isfinite(yc)) bad = true;
+        mx = fmax(mx, q);
+    }
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    bad = __any_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+        if (mx > 0.0) atomic_max_pos(&ctl->errbits, mx);
+        if (bad) ctl->nonfinite = 1;
+    }
+}
+
+// ---- control: RKQSm decision ---------------------------------------------------
+
+__global__ void k_control(Ctl *ctl)
+{
+    if (!ctl_live(ctl)) return;
+    const double SAFETY = 0.7, PGROW = -0.2, PSHRNK = -0.15, ERRCON = 1.89e-4;
+    double errmax = __longlong_as_double((long long)ctl->errbits);
+    ctl->errbits = 0ull;
+    if (ctl->nonfinite) {
+        ctl->status = UCG_E_NONFINITE;
+        ctl->active = 0;
+        return;
+    }
+    errmax = errmax / ctl->epsilon;
+    double h = ctl->h;
+    if (errmax > 1.0) {
+        h = h * SAFETY * pow(errmax, PSHRNK);
+        if (h < 0.5 * h) h = 0.5 * h;   // never taken (ode45.f90:83)
+        ctl->h = h;
+        ctl->rejected += 1;
+        ctl->need_stage1 = 0;
+        ctl->pending = 0;
+        const double tnew = 0.0 + h;     // the main loop passes t0 = 0 (ratestate.f90:317)
+        if (tnew == 0.0) {
+            ctl->status = UCG_E_STEP_UNDERFLOW;
+            ctl->active = 0;
+        }
+    } else {
+        double hnext;
+        if (errmax > ERRCON) hnext = SAFETY * h * pow(errmax, PGROW);
+        else hnext = 10.0 * h;
+        if (hnext > ctl->hmax) hnext = ctl->hmax;
+        ctl->hdid = h;
+        ctl->time = ctl->time + h;
+        ctl->dt_next = hnext;
+        ctl->h = hnext;
+        ctl->accepted += 1;
+        ctl->pending = 1;
+        ctl->vmax = 0.0;
+        ctl->need_stage1 = 1;
+        if (ctl->time >= ctl->t_end || ctl->accepted >= ctl->step_target) ctl->active = 0;
+    }
+}
+
+__global__ void k_commit(StageArgs a, const Ctl *ctl)
+{
+    if (!ctl->pending) return;
+    double *y = const_cast<double *>(a.y);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < a.len; i += (long)gridDim.x * blockDim.x)
+        y[i] = a.ycand[i];
+}
+
+__global__ void k_clear_pending(Ctl *ctl) { ctl->pending = 0; }
+
+// ---- host side -----------------------------------------------------------------
+
+static StageArgs stage_args(ucg_ctx *c, int s)
+{
+    StageArgs a;
+    a.y = c->st.y;
+    a.ys = (s == 1) ? c->st.y : c->st.ytmp;
+    for (int j = 0; j < 6; j++) a.k[j] = c->st.k[j];
+    a.v = c->st.v;
+    a.ycand = c->st.ycand;
+    a.yerr = c->st.yerr;
+    a.yscal = c->st.yscal;
+    a.fr = c->fr;
+    a.rh = c->rh;
+    a.np = c->nr + c->nt;
+    a.nvol = c->nv;
+    a.len = c->state_len;
+    return a;
+}
+
+int rk_alloc(ucg_ctx *c)
+{
+    rk_free(c);
+    const long len = c->state_len;
+    double **bufs[] = {&c->st.y, &c->st.ycand, &c->st.ytmp, &c->st.yerr, &c->st.yscal,
+                       &c->st.k[0], &c->st.k[1], &c->st.k[2], &c->st.k[3], &c->st.k[4], &c->st.k[5]};
+    for (double **b : bufs) {
+        if (cudaMalloc(b, sizeof(double) * (len + 2)) != cudaSuccess) return UCG_E_OOM;
+        cudaMemsetAsync(*b, 0, sizeof(double) * (len + 2), c->stream);
+    }
+    if (cudaMalloc(&c->st.v, sizeof(double) * (c->n + 2)) != cudaSuccess) return UCG_E_OOM;
+    if (cudaMalloc(&c->ctl, sizeof(Ctl)) != cudaSuccess) return UCG_E_OOM;
+    if (cudaMallocHost(&c->ctl_host, sizeof(Ctl)) != cudaSuccess) return UCG_E_OOM;
+    if (cudaMallocHost(&c->pin, sizeof(double) * (2 * len + 8)) != cudaSuccess) return UCG_E_OOM;
+    memset(c->ctl_host, 0, sizeof(Ctl));
+    c->ctl_host->epsilon = c->epsilon;
+    c->ctl_host->hmax = c->hmax;
+    UCG_CUDA(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+    return UCG_OK;
+}
+
+void rk_free(ucg_ctx *c)
+{
+    double **bufs[] = {&c->st.y, &c->st.ycand, &c->st.ytmp, &c->st.yerr, &c->st.yscal,
+                       &c->st.k[0], &c->st.k[1], &c->st.k[2], &c->st.k[3], &c->st.k[4], &c->st.k[5],
+                       &c->st.v};
+    for (double **b : bufs) {
+        if (*b) cudaFree(*b);
+        *b = nullptr;
+    }
+    if (c->ctl) cudaFree(c->ctl);
+    c->ctl = nullptr;
+    if (c->ctl_host) cudaFreeHost(c->ctl_host);
+    c->ctl_host = nullptr;
+    if (c->pin) cudaFreeHost(c->pin);
+    c->pin = nullptr;
+    if (c->attempt_graph) cudaGraphExecDestroy(c->attempt_graph);
+    c->attempt_graph = nullptr;
+}
+
+static int traction_grid(ucg_ctx *c, int *pb, int *vb)
+{
+    const int np = c->nr + c->nt;
+    *pb = (np + 3) / 4;
+    *vb = (c->nv + 1) / 2;
+    const int blocks = *pb + *vb;
+    const int cap = c->sms * 8;
+    return blocks < cap ? blocks : cap;
+}
+
+template <int S>
+static void enqueue_stage(ucg_ctx *c)
+{
+    const int ne = c->nr + c->nt + c->nv;
+    StageArgs a = stage_args(c, S);
+    k_prologue<S><<<(ne + 127) / 128, 128, 0, c->stream>>>(a, c->ctl);
+    int pb, vb;
+    int grid = traction_grid(c, &pb, &vb);
+    if (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi)
+        k_traction_split<S><<<grid, MV_WARPS * 32, 0, c->stream>>>(
+            reinterpret_cast<const __nv_bfloat162 *>(c->Khi), c->Kscale, c->n, a, c->ctl, pb, vb);
+    else
+        k_traction<S><<<grid, MV_WARPS * 32, 0, c->stream>>>(c->K, c->n, a, c->ctl, pb, vb);
+    c->launches.count += 2;
+}
+
+static void enqueue_attempt_raw(ucg_ctx *c)
+{
+    enqueue_stage<1>(c);
+    enqueue_stage<2>(c);
+    enqueue_stage<3>(c);
+    enqueue_stage<4>(c);
+    enqueue_stage<5>(c);
+    enqueue_stage<6>(c);
+    StageArgs a = stage_args(c, 6);
+    const int fin_grid = (int)((c->state_len + 255) / 256 < (long)c->sms * 4 ? (c->state_len + 255) / 256 : c->sms * 4);
+    k_finish<<<fin_grid > 0 ? fin_grid : 1, 256, 0, c->stream>>>(a, c->ctl);
+    k_control<<<1, 1, 0, c->stream>>>(c->ctl);
+    c->launches.count += 2;
+}
+
+void rk_enqueue_attempt(ucg_ctx *c)
+{
+    if (!c->attempt_graph || c->graph_precision != c->precision) {
+        if (c->attempt_graph) cudaGraphExecDestroy(c->attempt_graph);
+        c->attempt_graph = nullptr;
+        cudaGraph_t g;
+        long before = c->launches.count;
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            enqueue_attempt_raw(c);
+            if (cudaStreamEndCapture(c->stream, &g) == cudaSuccess) {
+                if (cudaGraphInstantiate(&c->attempt_graph, g, 0) != cudaSuccess) c->attempt_graph = nullptr;
+                cudaGraphDestroy(g);
+            }
+        }
+        c->launches.count = before;
+        c->graph_precision = c->precision;
+        cudaGetLastError();
+    }
+    if (c->attempt_graph) {
+        cudaGraphLaunch(c->attempt_graph, c->stream);
+        c->launches.count += 14;
+    } else {
+        enqueue_attempt_raw(c);
+    }
+}
+
+void rk_enqueue_commit(ucg_ctx *c)
+{
+    StageArgs a = stage_args(c, 1);
+    k_commit<<<(int)((c->state_len + 255) / 256), 256, 0, c->stream>>>(a, c->ctl);
+    k_clear_pending<<<1, 1, 0, c->stream>>>(c->ctl);
+    c->launches.count += 2;
+}
+
+// Mean device time of the stage-2 traction launch (the dominant kernel), timed
+// with events on the context stream.  The control block is made live for the
+// measurement and restored afterwards.
+int rk_profile_traction(ucg_ctx *c, int reps, double *ms)
+{
+    Ctl *h = c->ctl_host;
+    UCG_CUDA(cudaMemcpyAsync(h, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    Ctl saved = *h;
+    h->active = 1;
+    h->status = 0;
+    UCG_CUDA(cudaMemcpyAsync(c->ctl, h, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+    StageArgs a = stage_args(c, 2);
+    int pb, vb;
+    const int grid = traction_grid(c, &pb, &vb);
+    cudaEvent_t e0, e1;
+    UCG_CUDA(cudaEventCreate(&e0));
+    UCG_CUDA(cudaEventCreate(&e1));
+    UCG_CUDA(cudaEventRecord(e0, c->stream));
+    for (int r = 0; r < reps; r++) {
+        if (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi)
+            k_traction_split<2><<<grid, MV_WARPS * 32, 0, c->stream>>>(
+                reinterpret_cast<const __nv_bfloat162 *>(c->Khi), c->Kscale, c->n, a, c->ctl, pb, vb);
+        else
+            k_traction<2><<<grid, MV_WARPS * 32, 0, c->stream>>>(c->K, c->n, a, c->ctl, pb, vb);
+    }
+    c->launches.count += reps;
+    UCG_CUDA(cudaEventRecord(e1, c->stream));
+    UCG_CUDA(cudaEventSynchronize(e1));
+    float t = 0.0f;
+    UCG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = (double)t / reps;
+    *h = saved;
+    UCG_CUDA(cudaMemcpyAsync(c->ctl, h, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    return UCG_OK;
+}
+
+// f(y) for the state currently in st.y into st.k[0]
+int rk_odefun(ucg_ctx *c)
+{
+    Ctl *h = c->ctl_host;
+    UCG_CUDA(cudaMemcpyAsync(h, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    h->active = 1;
+    h->status = 0;
+    h->need_stage1 = 1;
+    h->pending = 0;
+    h->vmax = 0.0;
+    h->nonfinite = 0;
+    UCG_CUDA(cudaMemcpyAsync(c->ctl, h, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+    enqueue_stage<1>(c);
+    UCG_CUDA(cudaGetLastError());
+    UCG_CUDA(cudaMemcpyAsync(h, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    return h->nonfinite ? UCG_E_NONFINITE : UCG_OK;
+}
+
+}  // namespace ucg

@@ -1,0 +1,76 @@
+// Split-BF16 storage of the traction matrix: K = diag(s) (hi + lo).
+//
+// s_r = max_c |K_rc| (FP32), hi = bf16(K/s), lo = bf16(K/s - hi).  hi carries
+// 8 significant bits and lo the next 8, so each entry keeps about 16 bits
+// (relative error <= 2^-16 of the row maximum).  hi/lo are stored interleaved as
+// one bf16 pair per entry (4 bytes: half the FP64 stream of the traction product).
+#include <cmath>
+#include "ucg_internal.cuh"
+
+namespace ucg {
+
+__global__ void k_row_absmax(const double *__restrict__ K, long n, float *__restrict__ scale)
+{
+    const long r = blockIdx.x;
+    const double *row = K + r * n;
+    double m = 0.0;
+    for (long c = threadIdx.x; c < n; c += blockDim.x) m = fmax(m, fabs(row[c]));
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    __shared__ double wm[32];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t = fmax(t, wm[w]);
+        // round the scale up to FP32 so that |K/s| <= 1
+        float s = (float)t;
+        if ((double)s < t) s = nextafterf(s, INFINITY);
+        scale[r] = (t > 0.0) ? s : 1.0f;
+    }
+}
+
+__global__ void k_split(const double *__restrict__ K, long n, long total, const float *__restrict__ scale,
+                        __nv_bfloat162 *__restrict__ out)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long r = i / n;
+        const double x = K[i] / (double)scale[r];
+        const __nv_bfloat16 hi = __double2bfloat16(x);
+        const double rem = x - (double)__bfloat162float(hi);
+        const __nv_bfloat16 lo = __double2bfloat16(rem);
+        out[i] = __halves2bfloat162(hi, lo);
+    }
+}
+
+int split_bf16_build(ucg_ctx *c)
+{
+    if (!c->K) return UCG_E_STATE;
+    split_bf16_free(c);
+    UCG_CUDA(cudaSetDevice(c->device));
+    const long total = c->n * c->m;
+    cudaError_t e = cudaMalloc(&c->Khi, sizeof(__nv_bfloat162) * (size_t)total);
+    if (e != cudaSuccess) { c->Khi = nullptr; return cuda_fail(c, e, "cudaMalloc(split K)"); }
+    UCG_CUDA(cudaMalloc(&c->Kscale, sizeof(float) * (size_t)c->m));
+    k_row_absmax<<<(unsigned)c->m, 256, 0, c->stream>>>(c->K, c->n, c->Kscale);
+    const int grid = c->sms * 16;
+    k_split<<<grid, 256, 0, c->stream>>>(c->K, c->n, total, c->Kscale, reinterpret_cast<__nv_bfloat162 *>(c->Khi));
+    c->launches.count += 2;
+    UCG_CUDA(cudaGetLastError());
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    if (!c->keep_fp64) {
+        cudaFree(c->K);
+        c->K = nullptr;
+    }
+    return UCG_OK;
+}
+
+void split_bf16_free(ucg_ctx *c)
+{
+    if (c->Khi) cudaFree(c->Khi);
+    if (c->Kscale) cudaFree(c->Kscale);
+    c->Khi = nullptr;
+    c->Klo = nullptr;
+    c->Kscale = nullptr;
+}
+
+}  // namespace ucg

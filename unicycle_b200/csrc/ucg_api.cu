@@ -1,0 +1,592 @@
+// C ABI of libucg.so (include/ucg.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include "ucg_internal.cuh"
+#include "strainvolume.cuh"
+
+using namespace ucg;
+
+namespace ucg {
+int cuda_fail(ucg_ctx *c, cudaError_t e, const char *what)
+{
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    if (c) c->err = buf;
+    if (e == cudaErrorMemoryAllocation) return UCG_E_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return UCG_E_NODEVICE;
+    return UCG_E_CUDA;
+}
+}  // namespace ucg
+
+static int bad(ucg_ctx *c, const char *msg)
+{
+    if (c) c->err = msg;
+    return UCG_E_BADARG;
+}
+
+static int set_err(ucg_ctx *c, int status, const char *msg)
+{
+    if (c) c->err = msg;
+    return status;
+}
+
+extern "C" {
+
+const char *ucg_strerror(int s)
+{
+    switch (s) {
+    case UCG_OK: return "ok";
+    case UCG_E_BADARG: return "invalid argument";
+    case UCG_E_CUDA: return "CUDA error";
+    case UCG_E_OOM: return "out of device memory";
+    case UCG_E_STEP_UNDERFLOW: return "stepsize underflow in RKQS";
+    case UCG_E_NONFINITE: return "non-finite state or rate";
+    case UCG_E_TIMEOUT: return "device wait timed out";
+    case UCG_E_STATE: return "call out of order";
+    case UCG_E_UNSUPPORTED: return "unsupported";
+    case UCG_E_NODEVICE: return "no usable CUDA device";
+    default: return "unknown status";
+    }
+}
+
+const char *ucg_last_error(ucg_ctx *c) { return c ? c->err.c_str() : ""; }
+
+int ucg_create(ucg_ctx **out, int device, double mu, double lambda, int flags)
+{
+    if (!out) return UCG_E_BADARG;
+    *out = nullptr;
+    if (!(mu > 0.0) || !std::isfinite(lambda) || !(lambda + mu > 0.0)) return UCG_E_BADARG;
+    if (flags != UCG_DRIVER_RATESTATE && flags != UCG_DRIVER_VISCOUSCYCLES) return UCG_E_BADARG;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return UCG_E_NODEVICE;
+    if (device < 0 || device >= count) return UCG_E_BADARG;
+    ucg_ctx *c = new (std::nothrow) ucg_ctx();
+    if (!c) return UCG_E_OOM;
+    c->device = device;
+    c->mu = mu;
+    c->lambda = lambda;
+    c->driver = flags;
+    if ((e = cudaSetDevice(device)) != cudaSuccess || (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        int s = cuda_fail(c, e, "ucg_create");
+        delete c;
+        return s;
+    }
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    *out = c;
+    return UCG_OK;
+}
+
+static void free_params(ucg_ctx *c)
+{
+    double **p[] = {&c->fr.vpl_c, &c->fr.vpl_s, &c->fr.a, &c->fr.b, &c->fr.sig, &c->fr.L, &c->fr.damping,
+                    &c->rh.ebg, &c->rh.gd0, &c->rh.npow};
+    for (double **q : p) {
+        if (*q) cudaFree(*q);
+        *q = nullptr;
+    }
+}
+
+void ucg_destroy(ucg_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    rk_free(c);
+    split_bf16_free(c);
+    free_params(c);
+    if (c->K) cudaFree(c->K);
+    if (c->rcv) cudaFree(c->rcv);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+static void invalidate(ucg_ctx *c)
+{
+    c->assembled = false;
+    c->state_ready = false;
+    rk_free(c);
+    split_bf16_free(c);
+}
+
+int ucg_set_rectangles(ucg_ctx *c, int n, const double *x, const double *L, const double *W,
+                       const double *strike, const double *dip)
+{
+    if (!c || n < 0) return UCG_E_BADARG;
+    if (n > 0 && (!x || !L || !W || !strike || !dip)) return bad(c, "null array");
+    for (int i = 0; i < n; i++)
+        if (!(L[i] > 0.0) || !(W[i] > 0.0) || !std::isfinite(strike[i]) || !std::isfinite(dip[i]) ||
+            !std::isfinite(x[3 * i]) || !std::isfinite(x[3 * i + 1]) || !std::isfinite(x[3 * i + 2]))
+            return bad(c, "invalid rectangle geometry");
+    c->nr = n;
+    c->rx.assign(x, x + 3L * n);
+    c->rL.assign(L, L + n);
+    c->rW.assign(W, W + n);
+    c->rstrike.assign(strike, strike + n);
+    c->rdip.assign(dip, dip + n);
+    invalidate(c);
+    c->have_friction = false;
+    return UCG_OK;
+}
+
+int ucg_set_triangles(ucg_ctx *c, int n, const int *i1, const int *i2, const int *i3, int nve,
+                      const double *v)
+{
+    if (!c || n < 0 || nve < 0) return UCG_E_BADARG;
+    if (n > 0 && (!i1 || !i2 || !i3 || !v)) return bad(c, "null array");
+    for (int j = 0; j < n; j++) {
+        const int ids[3] = {i1[j], i2[j], i3[j]};
+        for (int k = 0; k < 3; k++)
+            if (ids[k] < 1 || ids[k] > nve) return bad(c, "triangle vertex index out of range (1-based)");
+        if (ids[0] == ids[1] || ids[1] == ids[2] || ids[0] == ids[2]) return bad(c, "degenerate triangle");
+    }
+    for (long k = 0; k < 3L * nve; k++)
+        if (!std::isfinite(v[k])) return bad(c, "non-finite vertex");
+    c->nt = n;
+    c->nve = nve;
+    c->ti1.assign(i1, i1 + n);
+    c->ti2.assign(i2, i2 + n);
+    c->ti3.assign(i3, i3 + n);
+    c->tvert.assign(v, v + 3L * nve);
+    invalidate(c);
+    c->have_friction = false;
+    return UCG_OK;
+}
+
+int ucg_set_volumes(ucg_ctx *c, int n, const double *x, const double *L, const double *T,
+                    const double *W, const double *strike)
+{
+    if (!c || n < 0) return UCG_E_BADARG;
+    if (n > 0 && (!x || !L || !T || !W || !strike)) return bad(c, "null array");
+    for (int i = 0; i < n; i++) {
+        if (!(L[i] > 0.0) || !(T[i] > 0.0) || !(W[i] > 0.0) || !std::isfinite(strike[i]))
+            return bad(c, "invalid strain-volume geometry");
+        // strainvolume.f90:1064-1072 stops on a negative source depth
+        if (!(x[3 * i + 2] >= 0.0)) return bad(c, "strain-volume depth (q3) must be positive");
+    }
+    if (n > 0 && !kVolumesBuilt) return set_err(c, UCG_E_UNSUPPORTED, "strain volumes not built");
+    c->nv = n;
+    c->vx.assign(x, x + 3L * n);
+    c->vL.assign(L, L + n);
+    c->vT.assign(T, T + n);
+    c->vW.assign(W, W + n);
+    c->vstrike.assign(strike, strike + n);
+    invalidate(c);
+    c->have_rheology = false;
+    return UCG_OK;
+}
+
+static int upload(ucg_ctx *c, double **dst, const std::vector<double> &h)
+{
+    if (*dst) cudaFree(*dst);
+    *dst = nullptr;
+    if (h.empty()) return UCG_OK;
+    UCG_CUDA(cudaMalloc(dst, sizeof(double) * h.size()));
+    UCG_CUDA(cudaMemcpyAsync(*dst, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    return UCG_OK;
+}
+
+int ucg_set_friction(ucg_ctx *c, const double *Vpl, const double *rake, const double *mu0,
+                     const double *sig, const double *a, const double *b, const double *L,
+                     const double *Vo, const double *damping)
+{
+    if (!c) return UCG_E_BADARG;
+    const int np = c->nr + c->nt;
+    if (np > 0 && (!Vpl || !rake || !mu0 || !sig || !a || !b || !L || !Vo || !damping))
+        return bad(c, "null array");
+    UCG_CUDA(cudaSetDevice(c->device));
+    std::vector<double> vc(np), vs(np), va(a, a + np), vb(b, b + np), vsg(sig, sig + np), vL(L, L + np),
+        vd(damping, damping + np);
+    for (int i = 0; i < np; i++) {
+        if (!(L[i] > 0.0) || !std::isfinite(Vpl[i]) || !std::isfinite(rake[i]))
+            return bad(c, "invalid friction parameters");
+        vc[i] = Vpl[i] * cos(rake[i]);
+        vs[i] = Vpl[i] * sin(rake[i]);
+    }
+    int rc;
+    if ((rc = upload(c, &c->fr.vpl_c, vc)) || (rc = upload(c, &c->fr.vpl_s, vs)) || (rc = upload(c, &c->fr.a, va)) ||
+        (rc = upload(c, &c->fr.b, vb)) || (rc = upload(c, &c->fr.sig, vsg)) || (rc = upload(c, &c->fr.L, vL)) ||
+        (rc = upload(c, &c->fr.damping, vd)))
+        return rc;
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    c->hVpl.assign(Vpl, Vpl + np);
+    c->hrake.assign(rake, rake + np);
+    c->hmu0.assign(mu0, mu0 + np);
+    c->hsig.assign(sig, sig + np);
+    c->ha.assign(a, a + np);
+    c->hb.assign(b, b + np);
+    c->hL.assign(L, L + np);
+    c->hVo.assign(Vo, Vo + np);
+    c->hdamp.assign(damping, damping + np);
+    c->have_friction = true;
+    return UCG_OK;
+}
+
+int ucg_set_rheology(ucg_ctx *c, const double *e_bg, const double *gammadot0m, const double *npowerm,
+                     int nonlinear_maxwell)
+{
+    if (!c) return UCG_E_BADARG;
+    const int nv = c->nv;
+    if (nv > 0 && (!e_bg || !gammadot0m || !npowerm)) return bad(c, "null array");
+    UCG_CUDA(cudaSetDevice(c->device));
+    std::vector<double> e(e_bg, e_bg + 6L * nv), g(gammadot0m, gammadot0m + nv), p(npowerm, npowerm + nv);
+    int rc;
+    if ((rc = upload(c, &c->rh.ebg, e)) || (rc = upload(c, &c->rh.gd0, g)) || (rc = upload(c, &c->rh.npow, p)))
+        return rc;
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    c->hebg = e;
+    c->hgd0 = g;
+    c->hnpow = p;
+    c->rh.nonlinear = nonlinear_maxwell != 0;
+    c->have_rheology = true;
+    return UCG_OK;
+}
+
+int ucg_assemble(ucg_ctx *c, int okada_mode)
+{
+    if (!c) return UCG_E_BADARG;
+    if (okada_mode != UCG_OKADA_FP64 && okada_mode != UCG_OKADA_REF32IO) return bad(c, "okada_mode");
+    if (c->nr + c->nt + c->nv == 0) return set_err(c, UCG_E_STATE, "no elements");
+    split_bf16_free(c);
+    int rc = assemble_matrix(c, okada_mode);
+    if (rc) return rc;
+    if (c->precision == UCG_PREC_SPLIT_BF16) return split_bf16_build(c);
+    return UCG_OK;
+}
+
+int ucg_dims(ucg_ctx *c, long *n, long *m)
+{
+    if (!c) return UCG_E_BADARG;
+    const int np = c->nr + c->nt;
+    if (n) *n = 2L * np + 6L * c->nv;
+    if (m) *m = 3L * np + 6L * c->nv;
+    return UCG_OK;
+}
+
+int ucg_copy_G(ucg_ctx *c, double *G, long ld, long k0, long k1)
+{
+    if (!c || !G) return UCG_E_BADARG;
+    if (!c->assembled || !c->K) return set_err(c, UCG_E_STATE, "matrix not assembled (or FP64 copy released)");
+    if (ld < c->n || k0 < 0 || k1 > c->m || k0 > k1) return bad(c, "copy range");
+    UCG_CUDA(cudaSetDevice(c->device));
+    UCG_CUDA(cudaMemcpy2DAsync(G, sizeof(double) * ld, c->K + k0 * c->n, sizeof(double) * c->n,
+                               sizeof(double) * c->n, k1 - k0, cudaMemcpyDeviceToHost, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    return UCG_OK;
+}
+
+int ucg_set_precision(ucg_ctx *c, int precision)
+{
+    if (!c) return UCG_E_BADARG;
+    if (precision != UCG_PREC_FP64 && precision != UCG_PREC_SPLIT_BF16) return bad(c, "precision");
+    if (precision == UCG_PREC_FP64 && c->assembled && !c->K)
+        return set_err(c, UCG_E_STATE, "FP64 matrix was released; re-assemble");
+    c->precision = precision;
+    if (precision == UCG_PREC_SPLIT_BF16 && c->assembled && !c->Khi) return split_bf16_build(c);
+    return UCG_OK;
+}
+
+int ucg_keep_fp64(ucg_ctx *c, int keep)
+{
+    if (!c) return UCG_E_BADARG;
+    c->keep_fp64 = keep != 0;
+    if (!c->keep_fp64 && c->Khi && c->K) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->K);
+        c->K = nullptr;
+    }
+    return UCG_OK;
+}
+
+long ucg_state_len(ucg_ctx *c)
+{
+    if (!c) return -1;
+    return 7L * (c->nr + c->nt) + 12L * c->nv;
+}
+
+int ucg_init_state(ucg_ctx *c, double *y, const double *nGm, const double *nQm, const double *nRm,
+                   const double *To)
+{
+    if (!c || !y) return UCG_E_BADARG;
+    if (!c->have_friction && c->nr + c->nt > 0) return set_err(c, UCG_E_STATE, "friction not set");
+    if (c->nv > 0 && (!c->have_rheology || !nGm || !nQm || !nRm || !To))
+        return set_err(c, UCG_E_STATE, "rheology / volume initial-stress parameters missing");
+    // initStateVector (ratestate.f90:548-610; viscouscycles.f90:710-820): O(N)
+    // host arithmetic on the parameters kept at ucg_set_friction / ucg_set_rheology
+    const double lg10 = log(10.0);
+    const bool visc = c->driver == UCG_DRIVER_VISCOUSCYCLES;
+    const int np = c->nr + c->nt;
+    for (int i = 0; i < np; i++) {
+        double *yy = y + 7L * i;
+        double tau = c->hsig[i] * (c->hmu0[i] + (c->ha[i] - c->hb[i]) * log(c->hVpl[i] / c->hVo[i]));
+        tau = visc ? tau + c->hdamp[i] * c->hVpl[i] : tau - c->hdamp[i] * c->hVpl[i];
+        yy[0] = 0.0;
+        yy[1] = 0.0;
+        yy[2] = tau * cos(c->hrake[i]);
+        yy[3] = tau * sin(c->hrake[i]);
+        yy[4] = 0.0;
+        yy[5] = log(c->hL[i] / c->hVpl[i]) / lg10;
+        yy[6] = log(c->hVpl[i] * (visc ? 0.98 : 0.99)) / lg10;
+    }
+    for (int i = 0; i < c->nv; i++) {
+        double *yy = y + 7L * np + 12L * i;
+        const double *e = &c->hebg[6L * i];
+        const double eps = sqrt((e[0] * e[0] + 2 * e[1] * e[1] + 2 * e[2] * e[2] + e[3] * e[3] +
+                                 2 * e[4] * e[4] + e[5] * e[5]) / 2.0);
+        for (int k = 0; k < 6; k++) yy[k] = 0.0;
+        if (0.0 < eps) {
+            const double tau = nGm[i] * pow(eps / c->hgd0[i] * exp(nQm[i] / (nRm[i] * To[i])), 1.0 / c->hnpow[i]);
+            for (int k = 0; k < 6; k++) yy[6 + k] = tau * e[k] / eps;
+        } else {
+            for (int k = 0; k < 6; k++) yy[6 + k] = 0.0;
+        }
+    }
+    return UCG_OK;
+}
+
+static int ensure_state(ucg_ctx *c)
+{
+    if (!c->assembled) return set_err(c, UCG_E_STATE, "matrix not assembled");
+    if (c->nr + c->nt > 0 && !c->have_friction) return set_err(c, UCG_E_STATE, "friction not set");
+    if (c->nv > 0 && !c->have_rheology) return set_err(c, UCG_E_STATE, "rheology not set");
+    if (c->precision == UCG_PREC_FP64 && !c->K) return set_err(c, UCG_E_STATE, "FP64 matrix released");
+    if (!c->state_ready) {
+        c->state_len = ucg_state_len(c);
+        int rc = rk_alloc(c);
+        if (rc) return set_err(c, rc, "state allocation failed");
+        c->state_ready = true;
+    }
+    return UCG_OK;
+}
+
+static int pull_ctl(ucg_ctx *c)
+{
+    UCG_CUDA(cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    return UCG_OK;
+}
+
+static int push_ctl(ucg_ctx *c)
+{
+    UCG_CUDA(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+    return UCG_OK;
+}
+
+static int put_vec(ucg_ctx *c, double *dst, const double *src)
+{
+    memcpy(c->pin, src, sizeof(double) * c->state_len);
+    UCG_CUDA(cudaMemcpyAsync(dst, c->pin, sizeof(double) * c->state_len, cudaMemcpyHostToDevice, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    return UCG_OK;
+}
+
+int ucg_odefun(ucg_ctx *c, double t, const double *y, double *dydt, double *vmax)
+{
+    (void)t;
+    if (!c || !y || !dydt) return UCG_E_BADARG;
+    int rc = ensure_state(c);
+    if (rc) return rc;
+    UCG_CUDA(cudaSetDevice(c->device));
+    if ((rc = put_vec(c, c->st.y, y))) return rc;
+    rc = rk_odefun(c);
+    UCG_CUDA(cudaMemcpyAsync(c->pin, c->st.k[0], sizeof(double) * c->state_len, cudaMemcpyDeviceToHost, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    memcpy(dydt, c->pin, sizeof(double) * c->state_len);
+    if (vmax) *vmax = c->ctl_host->vmax;
+    c->ctl_host->need_stage1 = 1;   // device y is the caller's; next step re-evaluates
+    return rc;
+}
+
+int ucg_set_tolerance(ucg_ctx *c, double epsilon, double max_step)
+{
+    if (!c || !(epsilon > 0.0) || !(max_step > 0.0)) return UCG_E_BADARG;
+    c->epsilon = epsilon;
+    c->hmax = max_step;
+    if (c->ctl_host) {
+        int rc = pull_ctl(c);
+        if (rc) return rc;
+        c->ctl_host->epsilon = epsilon;
+        c->ctl_host->hmax = max_step;
+        return push_ctl(c);
+    }
+    return UCG_OK;
+}
+
+// run queued attempts until `target` accepted steps (or inactive); polls the
+// control block every `batch` attempts
+static int drive(ucg_ctx *c, int batch)
+{
+    for (;;) {
+        for (int i = 0; i < batch; i++) rk_enqueue_attempt(c);
+        int rc = pull_ctl(c);
+        if (rc) return rc;
+        if (!c->ctl_host->active || c->ctl_host->status) break;
+    }
+    rk_enqueue_commit(c);
+    return pull_ctl(c);
+}
+
+int ucg_rkqs(ucg_ctx *c, double *t, double *y, const double *dydt, const double *yscal, double htry,
+             double *hdid, double *hnext, long *nrej)
+{
+    if (!c || !t || !y || !dydt || !yscal || !hdid || !hnext) return UCG_E_BADARG;
+    if (!(htry > 0.0)) return bad(c, "htry must be positive");
+    int rc = ensure_state(c);
+    if (rc) return rc;
+    UCG_CUDA(cudaSetDevice(c->device));
+    if ((rc = put_vec(c, c->st.y, y)) || (rc = put_vec(c, c->st.k[0], dydt)) || (rc = put_vec(c, c->st.yscal, yscal)))
+        return rc;
+    if ((rc = pull_ctl(c))) return rc;
+    Ctl *h = c->ctl_host;
+    const long acc0 = h->accepted, rej0 = h->rejected;
+    h->h = htry;
+    h->time = *t;
+    h->t_end = INFINITY;
+    h->step_target = acc0 + 1;
+    h->need_stage1 = 0;
+    h->pending = 0;
+    h->status = 0;
+    h->active = 1;
+    h->nonfinite = 0;
+    h->errbits = 0;
+    h->epsilon = c->epsilon;
+    h->hmax = c->hmax;
+    if ((rc = push_ctl(c))) return rc;
+    if ((rc = drive(c, 1))) return rc;
+    if (nrej) *nrej = h->rejected - rej0;
+    if (h->status) return set_err(c, h->status, ucg_strerror(h->status));
+    UCG_CUDA(cudaMemcpyAsync(c->pin, c->st.y, sizeof(double) * c->state_len, cudaMemcpyDeviceToHost, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    memcpy(y, c->pin, sizeof(double) * c->state_len);
+    *hdid = h->hdid;
+    *hnext = h->dt_next;
+    *t = h->time;
+    h->need_stage1 = 1;
+    return UCG_OK;
+}
+
+int ucg_step(ucg_ctx *c, double *time, double *y, double *dydt, double *dt_next, double *dt_done, long *nrej)
+{
+    if (!c || !time || !y || !dydt || !dt_next || !dt_done) return UCG_E_BADARG;
+    if (!(*dt_next > 0.0)) return bad(c, "dt_next must be positive");
+    int rc = ensure_state(c);
+    if (rc) return rc;
+    UCG_CUDA(cudaSetDevice(c->device));
+    if ((rc = put_vec(c, c->st.y, y))) return rc;
+    Ctl *h = c->ctl_host;
+    if ((rc = pull_ctl(c))) return rc;
+    const long rej0 = h->rejected;
+    h->h = *dt_next;
+    h->time = *time;
+    h->t_end = INFINITY;
+    h->step_target = h->accepted + 1;
+    h->need_stage1 = 1;
+    h->pending = 0;
+    h->status = 0;
+    h->active = 1;
+    h->nonfinite = 0;
+    h->errbits = 0;
+    h->vmax = 0.0;
+    h->epsilon = c->epsilon;
+    h->hmax = c->hmax;
+    if ((rc = push_ctl(c))) return rc;
+    if ((rc = drive(c, 1))) return rc;
+    if (nrej) *nrej = h->rejected - rej0;
+    if (h->status) return set_err(c, h->status, ucg_strerror(h->status));
+    UCG_CUDA(cudaMemcpyAsync(c->pin, c->st.y, sizeof(double) * c->state_len, cudaMemcpyDeviceToHost, c->stream));
+    UCG_CUDA(cudaMemcpyAsync(c->pin + c->state_len, c->st.k[0], sizeof(double) * c->state_len,
+                             cudaMemcpyDeviceToHost, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    memcpy(y, c->pin, sizeof(double) * c->state_len);
+    memcpy(dydt, c->pin + c->state_len, sizeof(double) * c->state_len);
+    *time = h->time;
+    *dt_done = h->hdid;
+    *dt_next = h->dt_next;
+    return UCG_OK;
+}
+
+int ucg_set_state(ucg_ctx *c, const double *y, double time, double dt_next)
+{
+    if (!c || !y || !(dt_next > 0.0)) return UCG_E_BADARG;
+    int rc = ensure_state(c);
+    if (rc) return rc;
+    UCG_CUDA(cudaSetDevice(c->device));
+    if ((rc = put_vec(c, c->st.y, y))) return rc;
+    if ((rc = pull_ctl(c))) return rc;
+    Ctl *h = c->ctl_host;
+    h->time = time;
+    h->h = dt_next;
+    h->dt_next = dt_next;
+    h->need_stage1 = 1;
+    h->pending = 0;
+    h->status = 0;
+    h->nonfinite = 0;
+    h->errbits = 0;
+    h->epsilon = c->epsilon;
+    h->hmax = c->hmax;
+    return push_ctl(c);
+}
+
+int ucg_get_state(ucg_ctx *c, double *y, double *time, double *dt_next, long *accepted, long *rejected)
+{
+    if (!c) return UCG_E_BADARG;
+    if (!c->state_ready) return set_err(c, UCG_E_STATE, "no device state");
+    UCG_CUDA(cudaSetDevice(c->device));
+    int rc = pull_ctl(c);
+    if (rc) return rc;
+    if (y) {
+        UCG_CUDA(cudaMemcpyAsync(c->pin, c->st.y, sizeof(double) * c->state_len, cudaMemcpyDeviceToHost, c->stream));
+        UCG_CUDA(cudaStreamSynchronize(c->stream));
+        memcpy(y, c->pin, sizeof(double) * c->state_len);
+    }
+    if (time) *time = c->ctl_host->time;
+    if (dt_next) *dt_next = c->ctl_host->h;
+    if (accepted) *accepted = c->ctl_host->accepted;
+    if (rejected) *rejected = c->ctl_host->rejected;
+    return UCG_OK;
+}
+
+int ucg_run(ucg_ctx *c, double t_end, long max_steps, long *steps)
+{
+    if (!c || max_steps < 0) return UCG_E_BADARG;
+    if (!c->state_ready) return set_err(c, UCG_E_STATE, "call ucg_set_state first");
+    UCG_CUDA(cudaSetDevice(c->device));
+    int rc = pull_ctl(c);
+    if (rc) return rc;
+    Ctl *h = c->ctl_host;
+    const long acc0 = h->accepted;
+    if (max_steps == 0 || h->time >= t_end) {
+        if (steps) *steps = 0;
+        return UCG_OK;
+    }
+    h->t_end = t_end;
+    h->step_target = acc0 + max_steps;
+    h->status = 0;
+    h->active = 1;
+    h->nonfinite = 0;
+    h->epsilon = c->epsilon;
+    h->hmax = c->hmax;
+    if ((rc = push_ctl(c))) return rc;
+    // queue attempts in batches sized to the remaining steps
+    rc = drive(c, max_steps < 32 ? (int)max_steps : 32);
+    if (rc) return rc;
+    if (steps) *steps = h->accepted - acc0;
+    if (h->status) return set_err(c, h->status, ucg_strerror(h->status));
+    return UCG_OK;
+}
+
+long ucg_launch_count(ucg_ctx *c) { return c ? c->launches.count : -1; }
+
+void *ucg_stream(ucg_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int ucg_profile_traction(ucg_ctx *c, int reps, double *ms)
+{
+    if (!c || reps <= 0 || !ms) return UCG_E_BADARG;
+    if (!c->state_ready) return set_err(c, UCG_E_STATE, "no device state");
+    UCG_CUDA(cudaSetDevice(c->device));
+    return rk_profile_traction(c, reps, ms);
+}
+
+}  // extern "C"
