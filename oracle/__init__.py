@@ -278,9 +278,9 @@ class Model:
     def step(self, time, y, dt_next, eps, hmax=1.7976931348623158e308):
         """One main-loop iteration.  Returns (rc, time, y, dydt_at_start, dt_next, dt_done, nrej)."""
         y = _d(y).copy()
-        tm = np.array([time])
+        tm = np.array([time], dtype=np.float64)
         dydt = np.zeros(self.len)
-        dn = np.array([dt_next])
+        dn = np.array([dt_next], dtype=np.float64)
         dd = np.zeros(1)
         nrej = np.zeros(1, dtype=np.int64)
         rc = lib().orc_step(ctypes.byref(self.md), _ptr(tm), _ptr(y), _ptr(dydt), _ptr(dn), eps,

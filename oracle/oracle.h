@@ -92,6 +92,8 @@ typedef struct {
 } orc_model;
 
 long orc_state_len(const orc_model *md);
+/* one DGEMV dot product in the fixed summation order documented in ratestate.c */
+double orc_dot_fixed_order(const double *col, const double *v, long n);
 void orc_init_state(const orc_model *md, double *y);
 /* odefun: dydt = f(y); vmax (may be NULL) receives max patch velocity.
    work must hold n + m doubles. */

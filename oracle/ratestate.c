@@ -24,6 +24,38 @@ static long nsrc(const orc_model *md) { return 2L * md->np + 6L * md->nvol; }
 static long nrcv(const orc_model *md) { return 3L * md->np + 6L * md->nvol; }
 
 long orc_state_len(const orc_model *md) { return 7L * md->np + 12L * md->nvol; }
+
+/*
+ * The reference's DGEMV leaves the summation order of each dot product to the
+ * BLAS it links.  The order matters here: the RKQS error norm is dominated by
+ * state components that are zero analytically and hold only rounding residue
+ * (e.g. the dip-slip rate of a pure strike-slip fault), so the accepted step
+ * sizes follow the last bits of those sums.  The oracle therefore fixes one
+ * order, the device kernel's: 256 partial sums (8 groups x 32 slots), slot
+ * (w, l) accumulating columns c = 64 w + 2 l + 512 k two at a time with fused
+ * multiply-adds; the 32 slots of a group combine by an xor butterfly
+ * (distance 16, 8, 4, 2, 1) and the 8 groups are added in order.
+ */
+double orc_dot_fixed_order(const double *col, const double *v, long n)
+{
+    double part[8];
+    for (int w = 0; w < 8; w++) {
+        double lane[32], tmp[32];
+        for (int l = 0; l < 32; l++) {
+            double acc = 0.0;
+            for (long c = 64L * w + 2 * l; c < n; c += 512) acc = fma(col[c + 1], v[c + 1], fma(col[c], v[c], acc));
+            lane[l] = acc;
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            for (int l = 0; l < 32; l++) tmp[l] = lane[l] + lane[l ^ off];
+            memcpy(lane, tmp, sizeof lane);
+        }
+        part[w] = lane[0];
+    }
+    double s = 0.0;
+    for (int w = 0; w < 8; w++) s += part[w];
+    return s;
+}
 long orc_work_len(const orc_model *md)
 {
     return 10 * orc_state_len(md) + nsrc(md) + nrcv(md);
@@ -102,10 +134,7 @@ void orc_odefun(const orc_model *md, const double *y, double *dydt, double *vmax
     /* step 2/3: t = G^T v (DGEMV "T"), column k is contiguous */
     for (long k = 0; k < m; k++) {
         if (!md->G) { t[k] = 0.0; continue; }
-        const double *col = md->G + k * n;
-        double s = 0.0;
-        for (long c = 0; c < n; c++) s += col[c] * v[c];
-        t[k] = s;
+        t[k] = orc_dot_fixed_order(md->G + k * n, v, n);
     }
     /* step 3/3: remaining state rates */
     for (int i = 0; i < md->np; i++) {

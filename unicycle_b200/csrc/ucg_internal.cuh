@@ -77,6 +77,7 @@ struct ucg_ctx {
     bool keep_fp64 = true;
     __nv_bfloat16 *Khi = nullptr, *Klo = nullptr;
     float *Kscale = nullptr;   // per row
+    long ldk_split = 0;        // row stride of the split matrix (n padded to a multiple of 8)
 
     // receivers: 12 doubles per element (xc, sv, dv, nv)
     double *rcv = nullptr;
