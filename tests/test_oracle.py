@@ -209,3 +209,28 @@ def test_state_init_matches_reference_formula(oracle_lib):
     tau = fr["sig"] * (fr["mu0"] + (fr["a"] - fr["b"]) * np.log(fr["Vpl"] / fr["Vo"])) - fr["damping"] * fr["Vpl"]
     assert np.allclose(y[2::7], tau * np.cos(fr["rake"]), rtol=1e-15)
     assert np.allclose(y[6::7], np.log10(0.99 * fr["Vpl"]), rtol=1e-15)
+
+
+def test_reference_step_control_is_rounding_sensitive(oracle_lib):
+    """Documents a property of the reference algorithm: on the symmetric
+    strike-slip fault the RKQS error norm is set by state components that are
+    zero analytically (dip slip, dip traction) and hold only rounding residue,
+    so perturbing G by one ulp already moves the accepted step sizes by more
+    than 1e-4 within a few steps.  History comparisons are therefore made
+    against this envelope (tests/test_gpu_parity.py)."""
+    from unicycle_b200 import configs
+    c = configs.cfg1(nx=16, nz=8)
+    G = oracle_lib.Mesh(c["mu"], c["lam"], rect=c["mesh"]["rect"]).build_g()
+
+    def times(Gm):
+        md = oracle_lib.Model(Gm, c["friction"])
+        y, t, dt, out = c["y0"].copy(), 0.0, c["dt0"], []
+        for _ in range(8):
+            rc, t, y, _, dt, _, _ = md.step(t, y, dt, c["epsilon"])
+            out.append(t)
+        return np.array(out)
+
+    rng = np.random.default_rng(0)
+    Gp = G * (1.0 + rng.choice([-1.0, 0.0, 1.0], size=G.shape) * 2.220446049250313e-16)
+    a, b = times(G), times(Gp)
+    assert np.max(np.abs(a - b) / a) > 1e-4

@@ -74,25 +74,32 @@ __device__ __forceinline__ RcvInfo rcv_info(int e, int np)
     return ri;
 }
 
-// write the 2 slip columns (one double2 per row) of a patch source
+// write (ACC = false) or add (ACC = true) the 2 slip columns, one double2 per
+// row, of a patch source
+template <bool ACC = false>
 __device__ __forceinline__ void store_patch_source(double *K, long n, long col, const double *rc,
                                                    const RcvInfo &ri, const double sS[6],
                                                    const double sD[6])
 {
+    double oS[6], oD[6];
     if (ri.nrow == 3) {
-        double tS[3], tD[3];
-        traction3(rc, sS, tS);
-        traction3(rc, sD, tD);
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-            *reinterpret_cast<double2 *>(K + (ri.row + c) * n + col) = make_double2(tS[c], tD[c]);
+        traction3(rc, sS, oS);
+        traction3(rc, sD, oD);
     } else {
-        double oS[6], oD[6];
         stress6(rc, sS, oS);
         stress6(rc, sD, oD);
+    }
 #pragma unroll
-        for (int c = 0; c < 6; c++)
-            *reinterpret_cast<double2 *>(K + (ri.row + c) * n + col) = make_double2(oS[c], oD[c]);
+    for (int c = 0; c < 6; c++) {
+        if (c < ri.nrow) {
+            double2 *p = reinterpret_cast<double2 *>(K + (ri.row + c) * n + col);
+            if (ACC) {
+                const double2 o = *p;
+                *p = make_double2(o.x + oS[c], o.y + oD[c]);
+            } else {
+                *p = make_double2(oS[c], oD[c]);
+            }
+        }
     }
 }
 
@@ -162,6 +169,7 @@ __global__ void __launch_bounds__(128) k_assemble_rect(double *__restrict__ K, l
 
 // ---- triangles (Nikkhoo & Walter 2015) -----------------------------------------
 
+template <int PART>
 __global__ void __launch_bounds__(128) k_assemble_tri(double *__restrict__ K, long n, long col0,
         const double *__restrict__ rcv, int nrcv, int np, const double *__restrict__ rec, int ns,
         NwConst cst)
@@ -175,8 +183,8 @@ __global__ void __launch_bounds__(128) k_assemble_tri(double *__restrict__ K, lo
 #pragma unroll
         for (int f = 0; f < RC_SIZE; f++) rloc[f] = __ldg(rc + f);
         double sS[6], sD[6];
-        nw_pair_stress(rloc, R, cst, sS, sD);
-        store_patch_source(K, n, col0 + 2L * j, rloc, rcv_info(e, np), sS, sD);
+        nw_part_stress<PART>(rloc, R, cst, sS, sD);
+        store_patch_source<PART != 0>(K, n, col0 + 2L * j, rloc, rcv_info(e, np), sS, sD);
     }
 }
 
@@ -391,8 +399,11 @@ int assemble_matrix(ucg_ctx *c, int okada_mode)
         if ((rc = upload(s))) return rc;
         NwConst cst{c->lambda / (c->lambda + c->mu) / 2.0, c->mu, c->lambda};
         dim3 grid((c->nt + TPB - 1) / TPB, gy);
-        k_assemble_tri<<<grid, TPB, 0, c->stream>>>(c->K, n, 2L * c->nr, c->rcv, ne, np, dsrc, c->nt, cst);
-        c->launches.count++;
+        // main TD, image TD and free-surface term in three accumulating passes
+        k_assemble_tri<0><<<grid, TPB, 0, c->stream>>>(c->K, n, 2L * c->nr, c->rcv, ne, np, dsrc, c->nt, cst);
+        k_assemble_tri<1><<<grid, TPB, 0, c->stream>>>(c->K, n, 2L * c->nr, c->rcv, ne, np, dsrc, c->nt, cst);
+        k_assemble_tri<2><<<grid, TPB, 0, c->stream>>>(c->K, n, 2L * c->nr, c->rcv, ne, np, dsrc, c->nt, cst);
+        c->launches.count += 3;
         UCG_CUDA(cudaGetLastError());
     }
     if (c->nv) {

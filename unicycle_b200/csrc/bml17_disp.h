@@ -57,11 +57,13 @@ template <class T> SV_HD T acoth(const T &X)
 }
 
 // The 27 integrals at one corner (y1, y2, y3) of the cuboid, observation point
-// (x1, x2, x3) in the cuboid frame (x1', x2', depth).  Output J[i][j][k] with
-// i in {1,2,3}, j in {1,2,3}, k in {12,13,23} -> J[i-1][j-1][0..2].
-template <class T>
+// (x1, x2, x3) in the cuboid frame (x1', x2', depth).  Each integral J_ijk
+// (i, j in {1,2,3}, k in {12,13,23}) is handed to emit(i-1, j-1, k-index, J) as
+// soon as it is formed, so callers can fold it into their sums without holding
+// all 27 at once.
+template <class T, class F>
 SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, double y3, double nu,
-                  double G, T J[3][3][3])
+                  double G, F &&emit)
 {
     const double PI = 3.141592653589793115997963468544185161;
     const double c = (1.0 / 16.0) / (1.0 - nu) / PI / G;
@@ -79,7 +81,7 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
     const T Bq = -(nm * n2) * r2 * r2 * dp + nm * n2 * r2 * y3 * (2.0 * x3 + y3) + x3 * (s12 + x3 * dp);
 
     // J1112, strainvolume.f90:344-367
-    J[0][0][0] = c * (2.0 * ir2 * x3 * d1 * d2 * y3 / s13
+    emit(0, 0, 0, T(c * (2.0 * ir2 * x3 * d1 * d2 * y3 / s13
         - 4.0 * nm * n2 * dp * atan3(d2, d1)
         - x3 * sv_atan2(x3, d1) - 3.0 * x3 * sv_atan2(3.0 * x3, d1)
         + 4.0 * nu * x3 * sv_atan2(-nu * x3, d1)
@@ -91,9 +93,9 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
         + xlogy(-(-3.0 + 4.0 * nu) * d1, r1 + d2)
         + xlogy((5.0 + 4.0 * nu * (-3.0 + 2.0 * nu)) * d1, r2 + d2)
         + xlogy(-4.0 * nm * d2, r1 + d1)
-        + xlogy(-4.0 * nm * d2, r2 + d1));
+        + xlogy(-4.0 * nm * d2, r2 + d1))));
     // J1113, strainvolume.f90:373-396
-    J[0][0][1] = c * (2.0 * ir2 * d1 / s12 * Bq
+    emit(0, 0, 1, T(c * (2.0 * ir2 * d1 / s12 * Bq
         + x2 * sv_atan2(-x2, d1) - 3.0 * x2 * sv_atan2(3.0 * x2, d1)
         + 4.0 * nu * x2 * sv_atan2(-nu * x2, d1)
         - 4.0 * nm * d2 * sv_atan2(r1 * d2, d1 * dm)
@@ -103,9 +105,9 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
         + xlogy(-(-3.0 + 4.0 * nu) * d1, r1 + dm)
         + xlogy(-(3.0 - 6.0 * nu + 4.0 * nu * nu) * d1, r2 + dp)
         + xlogy(-4.0 * nm * dm, r1 + d1)
-        + xlogy(4.0 * nm * dp, r2 + d1));
+        + xlogy(4.0 * nm * dp, r2 + d1))));
     // J1123, strainvolume.f90:402-430
-    J[0][0][2] = c * (-2.0 * ir2 / s12 * d2 / s13
+    emit(0, 0, 2, T(c * (-2.0 * ir2 / s12 * d2 / s13
             * (x3 * ((x3 * x3 + d11) * (x3 * x3 + d11 + d22) + x3 * (3.0 * x3 * x3 + 2.0 * d11 + d22) * y3
                      + 3.0 * x3 * x3 * y3 * y3 + x3 * y3 * y3 * y3)
                - nm * n2 * r2 * r2 * dp * s13 + nm * n2 * r2 * y3 * (2.0 * x3 + y3) * s13)
@@ -120,43 +122,43 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
         + xlogy(-(-3.0 + 4.0 * nu) * d2, r1 + dm)
         + xlogy(-(3.0 - 6.0 * nu + 4.0 * nu * nu) * d2, r2 + dp)
         + xlogy(-(-3.0 + 4.0 * nu) * dm, r1 + d2)
-        + xlogy(-(5.0 + 4.0 * nu * (-3.0 + 2.0 * nu)) * dp, r2 + d2));
+        + xlogy(-(5.0 + 4.0 * nu * (-3.0 + 2.0 * nu)) * dp, r2 + d2))));
     // J2112 = J1212, strainvolume.f90:436-448, 560-572
     const T j2112 = c * (-r1 + (1.0 + 8.0 * nm * nu) * r2 - 2.0 * ir2 * x3 * y3
         + xlogy(-4.0 * nm * n2 * dp, r2 + dp));
-    J[1][0][0] = j2112;
-    J[0][1][0] = j2112;
+    emit(1, 0, 0, T(j2112));
+    emit(0, 1, 0, T(j2112));
     // J2113 = J1213, strainvolume.f90:454-469, 578-593
     const T j2113 = c * (2.0 * ir2 / s12 * d2 * Bq
         + xlogy(-(-1.0 - 2.0 * nu + 4.0 * nu * nu) * d2, r2 + dp)
         + xlogy(-d2, r1 + dm));
-    J[1][0][1] = j2113;
-    J[0][1][1] = j2113;
+    emit(1, 0, 1, T(j2113));
+    emit(0, 1, 1, T(j2113));
     // J2123 = J1223, strainvolume.f90:475-490, 599-614
     const T j2123 = c * (2.0 * ir2 * d1 / s12 * Bq
         + xlogy(-(-1.0 - 2.0 * nu + 4.0 * nu * nu) * d1, r2 + dp)
         + xlogy(-d1, r1 + dm));
-    J[1][0][2] = j2123;
-    J[0][1][2] = j2123;
+    emit(1, 0, 2, T(j2123));
+    emit(0, 1, 2, T(j2123));
     // J3112, strainvolume.f90:496-513
-    J[2][0][0] = -c * (-2.0 * ir2 * x3 * d2 * y3 * dp / s13
+    emit(2, 0, 0, T(-c * (-2.0 * ir2 * x3 * d2 * y3 * dp / s13
         + 4.0 * nm * n2 * d1 * atan3(d1, d2)
         + 4.0 * nm * n2 * d1 * sv_atan2(r2 * (-d1), d2 * dp)
         + xlogy(-4.0 * nm * n2 * d2, r2 + dp)
         + xlogy(dm, r1 + d2)
-        + xlogy(-x3 - 7.0 * y3 - 8.0 * nu * nu * dp + 8.0 * nu * (x3 + 2.0 * y3), r2 + d2));
+        + xlogy(-x3 - 7.0 * y3 - 8.0 * nu * nu * dp + 8.0 * nu * (x3 + 2.0 * y3), r2 + d2))));
     // J3113, strainvolume.f90:519-532
-    J[2][0][1] = -c * (r1 + (-1.0 - 8.0 * nm * nu) * r2 - 2.0 * ir2 * x3 * y3
+    emit(2, 0, 1, T(-c * (r1 + (-1.0 - 8.0 * nm * nu) * r2 - 2.0 * ir2 * x3 * y3
         + 2.0 * (-3.0 + 4.0 * nu) * x3 * acoth(ir2 * dp)
-        + xlogy(2.0 * (3.0 * x3 + 2.0 * y3 - 6.0 * nu * dp + 4.0 * nu * nu * dp), r2 + dp));
+        + xlogy(2.0 * (3.0 * x3 + 2.0 * y3 - 6.0 * nu * dp + 4.0 * nu * nu * dp), r2 + dp))));
     // J3123, strainvolume.f90:538-554
-    J[2][0][2] = -c * (2.0 * ir2 * x3 * d1 * d2 * y3 / s13
+    emit(2, 0, 2, T(-c * (2.0 * ir2 * x3 * d1 * d2 * y3 / s13
         + 4.0 * nm * n2 * dp * atan3(d2, d1)
         + 4.0 * n2 * (nu * x3 + nm * y3) * sv_atan2(r2 * d1, d2 * dp)
         + xlogy(d1, r1 + d2)
-        + xlogy(-(1.0 + 8.0 * nm * nu) * d1, r2 + d2));
+        + xlogy(-(1.0 + 8.0 * nm * nu) * d1, r2 + d2))));
     // J2212, strainvolume.f90:620-643
-    J[1][1][0] = c * (2.0 * ir2 * x3 * d1 * d2 * y3 / s23
+    emit(1, 1, 0, T(c * (2.0 * ir2 * x3 * d1 * d2 * y3 / s23
         - 4.0 * nm * n2 * dp * atan3(d1, d2)
         - x3 * sv_atan2(x3, d1) - 3.0 * x3 * sv_atan2(3.0 * x3, d1)
         + 4.0 * nu * x3 * sv_atan2(-nu * x3, d1)
@@ -168,9 +170,9 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
         + xlogy(-4.0 * nm * d1, r1 + d2)
         + xlogy(-4.0 * nm * d1, r2 + d2)
         + xlogy(-(-3.0 + 4.0 * nu) * d2, r1 + d1)
-        + xlogy((5.0 + 4.0 * nu * (-3.0 + 2.0 * nu)) * d2, r2 + d1));
+        + xlogy((5.0 + 4.0 * nu * (-3.0 + 2.0 * nu)) * d2, r2 + d1))));
     // J2213, strainvolume.f90:649-677
-    J[1][1][1] = c * (-2.0 * ir2 * d1 / s12 / s23
+    emit(1, 1, 1, T(c * (-2.0 * ir2 * d1 / s12 / s23
             * (x3 * ((x3 * x3 + d22) * (x3 * x3 + d11 + d22) + x3 * (3.0 * x3 * x3 + d11 + 2.0 * d22) * y3
                      + 3.0 * x3 * x3 * y3 * y3 + x3 * y3 * y3 * y3)
                - nm * n2 * r2 * r2 * dp * s23 + nm * n2 * r2 * y3 * (2.0 * x3 + y3) * s23)
@@ -185,9 +187,9 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
         + xlogy(-(-3.0 + 4.0 * nu) * d1, r1 + dm)
         + xlogy(-(3.0 - 6.0 * nu + 4.0 * nu * nu) * d1, r2 + dp)
         + xlogy(-(-3.0 + 4.0 * nu) * dm, r1 + d1)
-        + xlogy(-(5.0 + 4.0 * nu * (-3.0 + 2.0 * nu)) * dp, r2 + d1));
+        + xlogy(-(5.0 + 4.0 * nu * (-3.0 + 2.0 * nu)) * dp, r2 + d1))));
     // J2223, strainvolume.f90:683-706
-    J[1][1][2] = c * (2.0 * ir2 / s12 * d2 * Bq
+    emit(1, 1, 2, T(c * (2.0 * ir2 / s12 * d2 * Bq
         + x1 * sv_atan2(-x1, d2) - 3.0 * x1 * sv_atan2(3.0 * x1, d2)
         + 4.0 * nu * x1 * sv_atan2(-nu * x1, d2)
         - 4.0 * nm * d1 * sv_atan2(r1 * d1, d2 * dm)
@@ -197,60 +199,60 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
         + xlogy(-(-3.0 + 4.0 * nu) * d2, r1 + dm)
         + xlogy(-(3.0 - 6.0 * nu + 4.0 * nu * nu) * d2, r2 + dp)
         + xlogy(-4.0 * nm * dm, r1 + d2)
-        + xlogy(4.0 * nm * dp, r2 + d2));
+        + xlogy(4.0 * nm * dp, r2 + d2))));
     // J3212, strainvolume.f90:712-729
-    J[2][1][0] = -c * (-2.0 * ir2 * x3 * d1 * y3 * dp / s23
+    emit(2, 1, 0, T(-c * (-2.0 * ir2 * x3 * d1 * y3 * dp / s23
         + 4.0 * nm * n2 * d2 * atan3(d2, d1)
         + 4.0 * nm * n2 * d2 * sv_atan2(r2 * (-d2), d1 * dp)
         + xlogy(-4.0 * nm * n2 * d1, r2 + dp)
         + xlogy(dm, r1 + d1)
-        + xlogy(-x3 - 7.0 * y3 - 8.0 * nu * nu * dp + 8.0 * nu * (x3 + 2.0 * y3), r2 + d1));
+        + xlogy(-x3 - 7.0 * y3 - 8.0 * nu * nu * dp + 8.0 * nu * (x3 + 2.0 * y3), r2 + d1))));
     // J3213, strainvolume.f90:735-751
-    J[2][1][1] = -c * (2.0 * ir2 * x3 * d1 * d2 * y3 / s23
+    emit(2, 1, 1, T(-c * (2.0 * ir2 * x3 * d1 * d2 * y3 / s23
         + 4.0 * nm * n2 * dp * atan3(d1, d2)
         + 4.0 * n2 * (nu * x3 + nm * y3) * sv_atan2(r2 * d2, d1 * dp)
         + xlogy(d2, r1 + d1)
-        + xlogy(-(1.0 + 8.0 * nm * nu) * d2, r2 + d1));
+        + xlogy(-(1.0 + 8.0 * nm * nu) * d2, r2 + d1))));
     // J3223, strainvolume.f90:757-770
-    J[2][1][2] = -c * (r1 + (-1.0 - 8.0 * nm * nu) * r2 - 2.0 * ir2 * x3 * y3
+    emit(2, 1, 2, T(-c * (r1 + (-1.0 - 8.0 * nm * nu) * r2 - 2.0 * ir2 * x3 * y3
         + 2.0 * (-3.0 + 4.0 * nu) * x3 * acoth(ir2 * dp)
-        + xlogy(2.0 * (3.0 * x3 + 2.0 * y3 - 6.0 * nu * dp + 4.0 * nu * nu * dp), r2 + dp));
+        + xlogy(2.0 * (3.0 * x3 + 2.0 * y3 - 6.0 * nu * dp + 4.0 * nu * nu * dp), r2 + dp))));
     // J1312, strainvolume.f90:776-793
-    J[0][2][0] = -c * (2.0 * ir2 * x3 * d2 * y3 * dp / s13
+    emit(0, 2, 0, T(-c * (2.0 * ir2 * x3 * d2 * y3 * dp / s13
         - 4.0 * nm * n2 * d1 * atan3(d1, d2)
         + 4.0 * nm * n2 * d1 * sv_atan2(r2 * d1, d2 * dp)
         + xlogy(4.0 * nm * n2 * d2, r2 + dp)
         + xlogy(dm, r1 + d2)
-        + xlogy((7.0 + 8.0 * (-2.0 + nu) * nu) * x3 + y3 + 8.0 * nm * nu * y3, r2 + d2));
+        + xlogy((7.0 + 8.0 * (-2.0 + nu) * nu) * x3 + y3 + 8.0 * nm * nu * y3, r2 + d2))));
     // J1313, strainvolume.f90:799-812
-    J[0][2][1] = -c * (r1 + ir2 * ((7.0 + 8.0 * (-2.0 + nu) * nu) * r2 * r2 + 2.0 * x3 * y3)
+    emit(0, 2, 1, T(-c * (r1 + ir2 * ((7.0 + 8.0 * (-2.0 + nu) * nu) * r2 * r2 + 2.0 * x3 * y3)
         + 2.0 * (-3.0 + 4.0 * nu) * x3 * acoth(ir2 * dp)
-        + xlogy(2.0 * (-3.0 * x3 - 2.0 * y3 + 6.0 * nu * dp - 4.0 * nu * nu * dp), r2 + dp));
+        + xlogy(2.0 * (-3.0 * x3 - 2.0 * y3 + 6.0 * nu * dp - 4.0 * nu * nu * dp), r2 + dp))));
     // J1323, strainvolume.f90:818-834
-    J[0][2][2] = -c * (-2.0 * ir2 * x3 * d1 * d2 * y3 / s13
+    emit(0, 2, 2, T(-c * (-2.0 * ir2 * x3 * d1 * d2 * y3 / s13
         - 4.0 * nm * n2 * dp * atan3(d2, d1)
         - 4.0 * nm * (-3.0 * x3 - y3 + 2.0 * nu * dp) * sv_atan2(r2 * d1, d2 * dp)
         + xlogy(d1, r1 + d2)
-        + xlogy((7.0 + 8.0 * (-2.0 + nu) * nu) * d1, r2 + d2));
+        + xlogy((7.0 + 8.0 * (-2.0 + nu) * nu) * d1, r2 + d2))));
     // J2312, strainvolume.f90:840-857
-    J[1][2][0] = -c * (2.0 * ir2 * x3 * d1 * y3 * dp / s23
+    emit(1, 2, 0, T(-c * (2.0 * ir2 * x3 * d1 * y3 * dp / s23
         - 4.0 * nm * n2 * d2 * atan3(d2, d1)
         + 4.0 * nm * n2 * d2 * sv_atan2(r2 * d2, d1 * dp)
         + xlogy(4.0 * nm * n2 * d1, r2 + dp)
         + xlogy(dm, r1 + d1)
-        + xlogy((7.0 + 8.0 * (-2.0 + nu) * nu) * x3 + y3 + 8.0 * nm * nu * y3, r2 + d1));
+        + xlogy((7.0 + 8.0 * (-2.0 + nu) * nu) * x3 + y3 + 8.0 * nm * nu * y3, r2 + d1))));
     // J2313, strainvolume.f90:863-879
-    J[1][2][1] = -c * (-2.0 * ir2 * x3 * d1 * d2 * y3 / s23
+    emit(1, 2, 1, T(-c * (-2.0 * ir2 * x3 * d1 * d2 * y3 / s23
         - 4.0 * nm * n2 * dp * atan3(d1, d2)
         - 4.0 * nm * (-3.0 * x3 - y3 + 2.0 * nu * dp) * sv_atan2(r2 * d2, d1 * dp)
         + xlogy(d2, r1 + d1)
-        + xlogy((7.0 + 8.0 * (-2.0 + nu) * nu) * d2, r2 + d1));
+        + xlogy((7.0 + 8.0 * (-2.0 + nu) * nu) * d2, r2 + d1))));
     // J2323, strainvolume.f90:885-898
-    J[1][2][2] = -c * (r1 + ir2 * ((7.0 + 8.0 * (-2.0 + nu) * nu) * r2 * r2 + 2.0 * x3 * y3)
+    emit(1, 2, 2, T(-c * (r1 + ir2 * ((7.0 + 8.0 * (-2.0 + nu) * nu) * r2 * r2 + 2.0 * x3 * y3)
         + 2.0 * (-3.0 + 4.0 * nu) * x3 * acoth(ir2 * dp)
-        + xlogy(2.0 * (-3.0 * x3 - 2.0 * y3 + 6.0 * nu * dp - 4.0 * nu * nu * dp), r2 + dp));
+        + xlogy(2.0 * (-3.0 * x3 - 2.0 * y3 + 6.0 * nu * dp - 4.0 * nu * nu * dp), r2 + dp))));
     // J3312, strainvolume.f90:904-929
-    J[2][2][0] = c * (2.0 * ir2 * x3 * d1 * d2 * y3 / s13 / s23 * (d11 + d22 + 2.0 * dpp)
+    emit(2, 2, 0, T(c * (2.0 * ir2 * x3 * d1 * d2 * y3 / s13 / s23 * (d11 + d22 + 2.0 * dpp)
         - 3.0 * x3 * sv_atan2(3.0 * x3, d1) - 5.0 * x3 * sv_atan2(5.0 * x3, d2)
         + 12.0 * nu * x3 * sv_atan2(-3.0 * nu * x3, d2) + 4.0 * nu * x3 * sv_atan2(-nu * x3, d1)
         - 8.0 * nu * nu * x3 * sv_atan2(nu * nu * x3, d2)
@@ -262,9 +264,9 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
         + xlogy(-(-3.0 + 4.0 * nu) * d1, r1 + d2)
         + xlogy((5.0 + 4.0 * nu * (-3.0 + 2.0 * nu)) * d1, r2 + d2)
         + xlogy(-(-3.0 + 4.0 * nu) * d2, r1 + d1)
-        + xlogy((5.0 + 4.0 * nu * (-3.0 + 2.0 * nu)) * d2, r2 + d1));
+        + xlogy((5.0 + 4.0 * nu * (-3.0 + 2.0 * nu)) * d2, r2 + d1))));
     // J3313, strainvolume.f90:935-959
-    J[2][2][1] = c * (2.0 * ir2 * x3 * d1 * y3 * dp / s23
+    emit(2, 2, 1, T(c * (2.0 * ir2 * x3 * d1 * y3 * dp / s23
         + 5.0 * x2 * sv_atan2(-5.0 * x2, d1) - 3.0 * x2 * sv_atan2(3.0 * x2, d1)
         + 4.0 * nu * x2 * sv_atan2(-nu * x2, d1) - 12.0 * nu * x2 * sv_atan2(3.0 * nu * x2, d1)
         + 8.0 * nu * nu * x2 * sv_atan2(-nu * nu * x2, d1)
@@ -277,9 +279,9 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
         + xlogy(-4.0 * nm * d1, r1 + dm)
         + xlogy(-8.0 * nm * nm * d1, r2 + dp)
         + xlogy(-(-3.0 + 4.0 * nu) * dm, r1 + d1)
-        + xlogy(-7.0 * x3 - 5.0 * y3 + 12.0 * nu * dp - 8.0 * nu * nu * dp, r2 + d1));
+        + xlogy(-7.0 * x3 - 5.0 * y3 + 12.0 * nu * dp - 8.0 * nu * nu * dp, r2 + d1))));
     // J3323, strainvolume.f90:965-989
-    J[2][2][2] = c * (2.0 * ir2 * x3 * d2 * y3 * dp / s13
+    emit(2, 2, 2, T(c * (2.0 * ir2 * x3 * d2 * y3 * dp / s13
         + 5.0 * x1 * sv_atan2(-5.0 * x1, d2) - 3.0 * x1 * sv_atan2(3.0 * x1, d2)
         + 4.0 * nu * x1 * sv_atan2(-nu * x1, d2) - 12.0 * nu * x1 * sv_atan2(3.0 * nu * x1, d2)
         + 8.0 * nu * nu * x1 * sv_atan2(-nu * nu * x1, d2)
@@ -292,7 +294,7 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
         + xlogy(-4.0 * nm * d2, r1 + dm)
         + xlogy(-8.0 * nm * nm * d2, r2 + dp)
         + xlogy(-(-3.0 + 4.0 * nu) * dm, r1 + d2)
-        + xlogy(-7.0 * x3 - 5.0 * y3 + 12.0 * nu * dp - 8.0 * nu * nu * dp, r2 + d2));
+        + xlogy(-7.0 * x3 - 5.0 * y3 + 12.0 * nu * dp - 8.0 * nu * nu * dp, r2 + d2))));
 }
 
 // Displacement (u1', u2', u3) in the cuboid frame for unit eigenstrain component
@@ -310,29 +312,39 @@ SV_HD void displacement(const T &x1, const T &x2, const T &x3, double q3, double
     const double cy2[8] = {Tk / 2, -Tk / 2, -Tk / 2, Tk / 2, Tk / 2, -Tk / 2, -Tk / 2, Tk / 2};
     const double cy3[8] = {q3 + W, q3 + W, q3, q3, q3 + W, q3 + W, q3, q3};
     const double sg[8] = {1.0, -1.0, 1.0, -1.0, -1.0, 1.0, -1.0, 1.0};
+    const double l2g = lambda + 2.0 * G, g2 = 2.0 * G;
     for (int k = 0; k < 8; k++) {
-        T J[3][3][3];
-        corner(x1, x2, x3, cy1[k], cy2[k], cy3[k], nu, G, J);
-        for (int i = 0; i < 3; i++) {
-            // IU_i = (lam ekk + 2G e11) Ji123 + 2G e12 (Ji223 + Ji113) + 2G e13 (Ji323 + Ji112)
-            //      + (lam ekk + 2G e22) Ji213 + 2G e23 (Ji212 + Ji313) + (lam ekk + 2G e33) Ji312
-            const T &a123 = J[i][0][2], &a223 = J[i][1][2], &a113 = J[i][0][1], &a323 = J[i][2][2];
-            const T &a112 = J[i][0][0], &a213 = J[i][1][1], &a212 = J[i][1][0], &a313 = J[i][2][1];
-            const T &a312 = J[i][2][0];
-            const T iso = lambda * (a123 + a213 + a312);   // lam * ekk part for unit normal strains
-            T c11 = iso + 2.0 * G * a123;
-            T c22 = iso + 2.0 * G * a213;
-            T c33 = iso + 2.0 * G * a312;
-            T c12 = 2.0 * G * (a223 + a113);
-            T c13 = 2.0 * G * (a323 + a112);
-            T c23 = 2.0 * G * (a212 + a313);
-            u[0][i] = u[0][i] + sg[k] * c11;
-            u[1][i] = u[1][i] + sg[k] * c12;
-            u[2][i] = u[2][i] + sg[k] * c13;
-            u[3][i] = u[3][i] + sg[k] * c22;
-            u[4][i] = u[4][i] + sg[k] * c23;
-            u[5][i] = u[5][i] + sg[k] * c33;
-        }
+        const double sgk = sg[k];
+        // IU_i = (lam ekk + 2G e11) Ji123 + 2G e12 (Ji223 + Ji113) + 2G e13 (Ji323 + Ji112)
+        //      + (lam ekk + 2G e22) Ji213 + 2G e23 (Ji212 + Ji313) + (lam ekk + 2G e33) Ji312
+        // for the six unit eigenstrains q = 11, 12, 13, 22, 23, 33
+        corner(x1, x2, x3, cy1[k], cy2[k], cy3[k], nu, G, [&](int i, int j, int kk, const T &J) {
+            const T sJ = sgk * J;
+            const int jk = 3 * j + kk;
+            switch (jk) {
+            case 2:  // J_i123
+                u[0][i] = u[0][i] + l2g * sJ; u[3][i] = u[3][i] + lambda * sJ; u[5][i] = u[5][i] + lambda * sJ;
+                break;
+            case 4:  // J_i213
+                u[0][i] = u[0][i] + lambda * sJ; u[3][i] = u[3][i] + l2g * sJ; u[5][i] = u[5][i] + lambda * sJ;
+                break;
+            case 6:  // J_i312
+                u[0][i] = u[0][i] + lambda * sJ; u[3][i] = u[3][i] + lambda * sJ; u[5][i] = u[5][i] + l2g * sJ;
+                break;
+            case 5:  // J_i223
+            case 1:  // J_i113
+                u[1][i] = u[1][i] + g2 * sJ;
+                break;
+            case 8:  // J_i323
+            case 0:  // J_i112
+                u[2][i] = u[2][i] + g2 * sJ;
+                break;
+            case 3:  // J_i212
+            case 7:  // J_i313
+                u[4][i] = u[4][i] + g2 * sJ;
+                break;
+            }
+        });
     }
 }
 

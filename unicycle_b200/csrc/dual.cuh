@@ -9,6 +9,9 @@ namespace ucg {
 
 struct Dd {
     double v, x, y, z;
+    Dd() = default;
+    __host__ __device__ constexpr Dd(double c) : v(c), x(0.0), y(0.0), z(0.0) {}
+    __host__ __device__ constexpr Dd(double c, double a, double b, double e) : v(c), x(a), y(b), z(e) {}
 };
 
 __device__ __forceinline__ Dd dd(double c) { return Dd{c, 0.0, 0.0, 0.0}; }
@@ -86,5 +89,52 @@ __device__ __forceinline__ Dd datan2_g(Dd y, Dd x)
     return Dd{0.0, (x.v * y.x - y.v * x.x) * r, (x.v * y.y - y.v * x.y) * r,
               (x.v * y.z - y.v * x.z) * r};
 }
+
+// Single-direction dual: a value and one directional derivative.  Evaluating a
+// field once per coordinate direction with these keeps half the live state of
+// the three-direction type, which matters for the longest expressions.
+struct Dd1 {
+    double v, d;
+    Dd1() = default;
+    __host__ __device__ constexpr Dd1(double c) : v(c), d(0.0) {}
+    __host__ __device__ constexpr Dd1(double c, double e) : v(c), d(e) {}
+};
+__device__ __forceinline__ Dd1 operator+(Dd1 a, Dd1 b) { return Dd1{a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dd1 operator-(Dd1 a, Dd1 b) { return Dd1{a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dd1 operator-(Dd1 a) { return Dd1{-a.v, -a.d}; }
+__device__ __forceinline__ Dd1 operator*(Dd1 a, Dd1 b) { return Dd1{a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dd1 operator+(Dd1 a, double c) { return Dd1{a.v + c, a.d}; }
+__device__ __forceinline__ Dd1 operator+(double c, Dd1 a) { return Dd1{a.v + c, a.d}; }
+__device__ __forceinline__ Dd1 operator-(Dd1 a, double c) { return Dd1{a.v - c, a.d}; }
+__device__ __forceinline__ Dd1 operator-(double c, Dd1 a) { return Dd1{c - a.v, -a.d}; }
+__device__ __forceinline__ Dd1 operator*(Dd1 a, double c) { return Dd1{a.v * c, a.d * c}; }
+__device__ __forceinline__ Dd1 operator*(double c, Dd1 a) { return Dd1{a.v * c, a.d * c}; }
+__device__ __forceinline__ Dd1 rcp(Dd1 a)
+{
+    double r = 1.0 / a.v;
+    return Dd1{r, -r * r * a.d};
+}
+__device__ __forceinline__ Dd1 operator/(Dd1 a, Dd1 b)
+{
+    double r = 1.0 / b.v, q = a.v * r;
+    return Dd1{q, (a.d - q * b.d) * r};
+}
+__device__ __forceinline__ Dd1 operator/(Dd1 a, double c)
+{
+    double r = 1.0 / c;
+    return Dd1{a.v * r, a.d * r};
+}
+__device__ __forceinline__ Dd1 operator/(double c, Dd1 a)
+{
+    double r = 1.0 / a.v, q = c * r;
+    return Dd1{q, -q * r * a.d};
+}
+__device__ __forceinline__ Dd1 dsqrt(Dd1 a)
+{
+    double s = sqrt(a.v);
+    return Dd1{s, 0.5 / s * a.d};
+}
+__device__ __forceinline__ Dd1 dlog_g(Dd1 a) { return Dd1{0.0, a.d / a.v}; }
+__device__ __forceinline__ Dd1 datan_g(Dd1 a) { return Dd1{0.0, a.d / (1.0 + a.v * a.v)}; }
 
 }  // namespace ucg

@@ -314,6 +314,7 @@ __device__ inline bool nw_td_fs(const Dd X[3], const NwRec &R, int o, double nu,
 
 // AngDisDispFSC (DispInHalfSpace.c:577-617) for the two slip modes.
 // sc: sinB, cosB, cotB, cot(B/2); b: (b1,b2,b3) per mode (6); gradient only.
+template <class Dd>
 __device__ inline void nw_fsc(Dd y1, Dd y2, Dd y3, double sinB, double cosB, double cotB,
                               double coth, const double b[6], double nu, double a, Dd oS[3],
                               Dd oD[3])
@@ -333,52 +334,89 @@ __device__ inline void nw_fsc(Dd y1, Dd y2, Dd y3, double sinB, double cosB, dou
     Dd rsy = rb * sinB - y1;
     Dd y2s = y2 * y2;
 
-    Dd e11 = -2.0 * n1 * n12 * Fib * cot2 + n12 * y2 * iry * ((n12 - a * irb) * cotB - y1 * iry * (nu + a * irb))
+    // fold each basis term into the two modes as soon as it is formed, so
+    // that only the outputs and the shared sub-terms stay live
+    oS[0] = Dd(0.0); oS[1] = Dd(0.0); oS[2] = Dd(0.0); oD[0] = Dd(0.0); oD[1] = Dd(0.0); oD[2] = Dd(0.0);
+    {
+        const Dd e11 = -2.0 * n1 * n12 * Fib * cot2 + n12 * y2 * iry * ((n12 - a * irb) * cotB - y1 * iry * (nu + a * irb))
            + n12 * y2 * cosB * cotB * irz * cpa + a * y2 * ya * cotB * irb3
            + y2 * ya * irb * iry * (-n12 * cotB + y1 * iry * (2.0 * nu + a * irb) + a * y1 * irb2)
            + y2 * ya * irb * irz * (cosB * irz * (w * (n12 * cosB - a * irb) * cotB + 2.0 * n1 * rsy * cosB)
                                     - a * y3b * cosB * cotB * irb2);
-    Dd e12 = n12 * ((2.0 * n1 * cot2 - nu) * lry - (2.0 * n1 * cot2 + n12) * cosB * lrz)
+        oS[0] = oS[0] + b[0] * e11;
+        oD[0] = oD[0] + b[3] * e11;
+    }
+    {
+        const Dd e12 = n12 * ((2.0 * n1 * cot2 - nu) * lry - (2.0 * n1 * cot2 + n12) * cosB * lrz)
            - n12 * iry * (y1 * cotB * (n12 - a * irb) + nu * y3b - a + y2s * iry * (nu + a * irb))
            - n12 * z1b * cotB * irz * cpa - a * y1 * ya * cotB * irb3
            + ya * iry * (-2.0 * nu + irb * (n12 * y1 * cotB - a) + y2s * irb * iry * (2.0 * nu + a * irb) + a * y2s * irb3)
            + ya * irz * (cosB * cosB - irb * (n12 * z1b * cotB + a * cosB) + a * y3b * z1b * cotB * irb3
                          - irb * irz * (y2s * cosB * cosB - a * z1b * cotB * irb * w));
-    Dd e13 = 2.0 * n1 * ((n12 * Fib * cotB) + (y2 * iry * (2.0 * nu + a * irb)) - (y2 * cosB * irz * cpa))
+        oS[1] = oS[1] + b[0] * e12;
+        oD[1] = oD[1] + b[3] * e12;
+    }
+    {
+        const Dd e13 = 2.0 * n1 * ((n12 * Fib * cotB) + (y2 * iry * (2.0 * nu + a * irb)) - (y2 * cosB * irz * cpa))
            + y2 * ya * irb * (2.0 * nu * iry + a * irb2)
            + y2 * ya * cosB * irb * irz * (n12 - w * irz * cpa - a * y3b * irb2);
-    Dd e21 = n12 * ((2.0 * n1 * cot2 + nu) * lry - (2.0 * n1 * cot2 + 1.0) * cosB * lrz)
+        oS[2] = oS[2] + b[0] * e13;
+        oD[2] = oD[2] + b[3] * e13;
+    }
+    {
+        const Dd e21 = n12 * ((2.0 * n1 * cot2 + nu) * lry - (2.0 * n1 * cot2 + 1.0) * cosB * lrz)
            + n12 * iry * (-n12 * y1 * cotB + nu * y3b - a + a * y1 * cotB * irb + y1 * y1 * iry * (nu + a * irb))
            - n12 * cotB * irz * (z1b * cosB - a * rsy * irb / cosB) - a * y1 * ya * cotB * irb3
            + ya * iry * (2.0 * nu + irb * (n12 * y1 * cotB + a) - y1 * y1 * irb * iry * (2.0 * nu + a * irb) - a * y1 * y1 * irb3)
            + ya * cotB * irz * (-cosB * sinB + a * y1 * y3b * irb3 / cosB
                                 + rsy * irb * (2.0 * n1 * cosB - w * irz * (1.0 + a * irb / cosB)));
-    Dd e22 = 2.0 * n1 * n12 * Fib * cot2 + n12 * y2 * iry * (-(n12 - a * irb) * cotB + y1 * iry * (nu + a * irb))
+        oS[0] = oS[0] + b[1] * e21;
+        oD[0] = oD[0] + b[4] * e21;
+    }
+    {
+        const Dd e22 = 2.0 * n1 * n12 * Fib * cot2 + n12 * y2 * iry * (-(n12 - a * irb) * cotB + y1 * iry * (nu + a * irb))
            - n12 * y2 * cotB * irz * (1.0 + a * irb / cosB) - a * y2 * ya * cotB * irb3
            + y2 * ya * irb * iry * (n12 * cotB - 2.0 * nu * y1 * iry - a * y1 * irb * (irb + iry))
            + y2 * ya * cotB * irb * irz * (-2.0 * n1 * cosB + w * irz * (1.0 + a * irb / cosB) + a * y3b * irb2 / cosB);
-    Dd e23 = -2.0 * n1 * n12 * cotB * (lry - cosB * lrz) - 2.0 * n1 * y1 * iry * (2.0 * nu + a * irb)
+        oS[1] = oS[1] + b[1] * e22;
+        oD[1] = oD[1] + b[4] * e22;
+    }
+    {
+        const Dd e23 = -2.0 * n1 * n12 * cotB * (lry - cosB * lrz) - 2.0 * n1 * y1 * iry * (2.0 * nu + a * irb)
            + 2.0 * n1 * z1b * irz * cpa + ya * irb * (n12 * cotB - 2.0 * nu * y1 * iry - a * y1 * irb2)
            - ya * irz * (cosB * sinB + w * cotB * irb * (2.0 * n1 * cosB - w * irz)
                          + a * irb * (sinB - y3b * z1b * irb2 - z1b * w * irb * irz));
-    Dd e31 = n12 * (y2 * iry * (1.0 + a * irb) - y2 * cosB * irz * cpa) - y2 * ya * irb * (a * irb2 + iry)
+        oS[2] = oS[2] + b[1] * e23;
+        oD[2] = oD[2] + b[4] * e23;
+    }
+    {
+        const Dd e31 = n12 * (y2 * iry * (1.0 + a * irb) - y2 * cosB * irz * cpa) - y2 * ya * irb * (a * irb2 + iry)
            + y2 * ya * cosB * irb * irz * (w * irz * cpa + a * y3b * irb2);
-    Dd e32 = n12 * (-sinB * lrz - y1 * iry * (1.0 + a * irb) + z1b * irz * cpa)
+        oS[0] = oS[0] + b[2] * e31;
+        oD[0] = oD[0] + b[5] * e31;
+    }
+    {
+        const Dd e32 = n12 * (-sinB * lrz - y1 * iry * (1.0 + a * irb) + z1b * irz * cpa)
            + y1 * ya * irb * (a * irb2 + iry)
            - ya * irz * (sinB * (cosB - a * irb) + z1b * irb * (1.0 + a * y3b * irb2)
                          - irb * irz * (y2s * cosB * sinB - a * z1b * irb * w));
-    Dd e33 = 2.0 * n1 * Fib + 2.0 * n1 * (y2 * sinB * irz * cpa)
+        oS[1] = oS[1] + b[2] * e32;
+        oD[1] = oD[1] + b[5] * e32;
+    }
+    {
+        const Dd e33 = 2.0 * n1 * Fib + 2.0 * n1 * (y2 * sinB * irz * cpa)
            + y2 * ya * sinB * irb * irz * (1.0 + w * irz * cpa + a * y3b * irb2);
-    // e_bc: displacement component c per unit b_b
-    oS[0] = k * (b[0] * e11 + b[1] * e21 + b[2] * e31);
-    oS[1] = k * (b[0] * e12 + b[1] * e22 + b[2] * e32);
-    oS[2] = k * (b[0] * e13 + b[1] * e23 + b[2] * e33);
-    oD[0] = k * (b[3] * e11 + b[4] * e21 + b[5] * e31);
-    oD[1] = k * (b[3] * e12 + b[4] * e22 + b[5] * e32);
-    oD[2] = k * (b[3] * e13 + b[4] * e23 + b[5] * e33);
+        oS[2] = oS[2] + b[2] * e33;
+        oD[2] = oD[2] + b[5] * e33;
+    }
+    for (int c = 0; c < 3; c++) {
+        oS[c] = k * oS[c];
+        oD[c] = k * oD[c];
+    }
 }
 
 // harmonic function of one side (AngSetupFSC), added into uS, uD (EFCS).
+template <class Dd>
 __device__ inline void nw_side(const Dd X[3], const NwRec &R, int o, double nu, Dd uS[3], Dd uD[3])
 {
     if (R[o + FS_DEG] != 0.0) return;
@@ -433,49 +471,51 @@ __device__ __forceinline__ void nw_stress(const Dd u[3], double mu, double lambd
     s[5] = 2.0 * mu * ezz + lambda * kk;
 }
 
-// Stress (NED, s11,s12,s13,s22,s23,s33) at receiver xr (NED) for unit strike slip
-// (sS) and unit dip slip (sD) of the triangle whose record is R.
-__device__ inline void nw_pair_stress(const double xr[3], const NwRec &R, const NwConst &c,
-                                      double sS[6], double sD[6])
+// ENU stress (C order) -> NED s11,s12,s13,s22,s23,s33 (nikkhoo15.f90:156-161)
+__device__ __forceinline__ void nw_to_ned(const double e[6], double s[6])
 {
-    // ENU observation point with identity seeds
+    s[0] = e[3]; s[1] = e[1]; s[2] = -e[4]; s[3] = e[0]; s[4] = -e[2]; s[5] = e[5];
+}
+
+// One part of the TD stress at receiver xr (NED) for unit strike slip (sS) and
+// unit dip slip (sD): PART 0 main TD, 1 image TD (with the surface sign flip),
+// 2 harmonic free-surface term.  The three parts sum to straininhalfspace_'s
+// stress; evaluating them in separate passes keeps the live state of each pass
+// small enough for the register file.
+template <int PART>
+__device__ inline void nw_part_stress(const double xr[3], const NwRec &R, const NwConst &c, double sS[6],
+                                      double sD[6])
+{
     Dd X[3] = {Dd{xr[1], 1.0, 0.0, 0.0}, Dd{xr[0], 0.0, 1.0, 0.0}, Dd{-xr[2], 0.0, 0.0, 1.0}};
-    double mS[6], mD[6], iS[6], iD[6], hS[6], hD[6];
-    {
-        Dd uS[3], uD[3];
-        if (!nw_td_fs(X, R, NW_MAIN, c.nu, uS, uD)) {
+    Dd uS[3] = {dd(0), dd(0), dd(0)}, uD[3] = {dd(0), dd(0), dd(0)};
+    if (PART == 2) {
+        // one pass per derivative direction with single-direction duals
+        double gS[3][3], gD[3][3];
+#pragma unroll 1
+        for (int dir = 0; dir < 3; dir++) {
+            Dd1 X1[3] = {Dd1{xr[1], dir == 0 ? 1.0 : 0.0}, Dd1{xr[0], dir == 1 ? 1.0 : 0.0},
+                         Dd1{-xr[2], dir == 2 ? 1.0 : 0.0}};
+            Dd1 vS[3] = {Dd1(0.0), Dd1(0.0), Dd1(0.0)}, vD[3] = {Dd1(0.0), Dd1(0.0), Dd1(0.0)};
+#pragma unroll 1
+            for (int side = 0; side < 3; side++) nw_side<Dd1>(X1, R, NW_FS + side * FS_SIZE, c.nu, vS, vD);
+            for (int k = 0; k < 3; k++) { gS[k][dir] = vS[k].d; gD[k][dir] = vD[k].d; }
+        }
+        for (int k = 0; k < 3; k++) {
+            uS[k] = Dd{0.0, gS[k][0], gS[k][1], gS[k][2]};
+            uD[k] = Dd{0.0, gD[k][0], gD[k][1], gD[k][2]};
+        }
+    } else {
+        if (!nw_td_fs(X, R, PART == 0 ? NW_MAIN : NW_IMG, c.nu, uS, uD)) {
             for (int k = 0; k < 6; k++) { sS[k] = nan(""); sD[k] = nan(""); }
             return;
         }
-        nw_stress(uS, c.mu, c.lambda, mS);
-        nw_stress(uD, c.mu, c.lambda, mD);
-    }
-    {
-        Dd uS[3] = {dd(0), dd(0), dd(0)}, uD[3] = {dd(0), dd(0), dd(0)};
-        nw_side(X, R, NW_FS + 0 * FS_SIZE, c.nu, uS, uD);
-        nw_side(X, R, NW_FS + 1 * FS_SIZE, c.nu, uS, uD);
-        nw_side(X, R, NW_FS + 2 * FS_SIZE, c.nu, uS, uD);
-        nw_stress(uS, c.mu, c.lambda, hS);
-        nw_stress(uD, c.mu, c.lambda, hD);
-    }
-    {
-        Dd uS[3], uD[3];
-        if (!nw_td_fs(X, R, NW_IMG, c.nu, uS, uD)) {
-            for (int k = 0; k < 6; k++) { sS[k] = nan(""); sD[k] = nan(""); }
-            return;
-        }
-        nw_stress(uS, c.mu, c.lambda, iS);
-        nw_stress(uD, c.mu, c.lambda, iD);
-        if (R[NW_SURF] != 0.0) { iS[4] = -iS[4]; iS[5] = -iS[5]; iD[4] = -iD[4]; iD[5] = -iD[5]; }
     }
     double eS[6], eD[6];
-    for (int k = 0; k < 6; k++) {
-        eS[k] = mS[k] + iS[k] + hS[k];
-        eD[k] = mD[k] + iD[k] + hD[k];
-    }
-    // ENU -> NED (nikkhoo15.f90:156-161)
-    sS[0] = eS[3]; sS[1] = eS[1]; sS[2] = -eS[4]; sS[3] = eS[0]; sS[4] = -eS[2]; sS[5] = eS[5];
-    sD[0] = eD[3]; sD[1] = eD[1]; sD[2] = -eD[4]; sD[3] = eD[0]; sD[4] = -eD[2]; sD[5] = eD[5];
+    nw_stress(uS, c.mu, c.lambda, eS);
+    nw_stress(uD, c.mu, c.lambda, eD);
+    if (PART == 1 && R[NW_SURF] != 0.0) { eS[4] = -eS[4]; eS[5] = -eS[5]; eD[4] = -eD[4]; eD[5] = -eD[5]; }
+    nw_to_ned(eS, sS);
+    nw_to_ned(eD, sD);
 }
 
 }  // namespace ucg
