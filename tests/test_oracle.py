@@ -219,7 +219,7 @@ def test_reference_step_control_is_rounding_sensitive(oracle_lib):
     than 1e-4 within a few steps.  History comparisons are therefore made
     against this envelope (tests/test_gpu_parity.py)."""
     from unicycle_b200 import configs
-    c = configs.cfg1(nx=16, nz=8)
+    c = configs.cfg1()
     G = oracle_lib.Mesh(c["mu"], c["lam"], rect=c["mesh"]["rect"]).build_g()
 
     def times(Gm):
