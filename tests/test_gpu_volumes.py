@@ -1,0 +1,82 @@
+"""GPU tests of the strain-volume path (Barbot, Moore & Lambert 2017 cuboids)
+and the coupled fault + volume (viscous-cycles) right-hand side.
+
+The device differentiates the published displacement integrals exactly (dual
+numbers); the oracle differentiates the same integrals numerically
+(Richardson central differences, ~1e-9 accurate), so volume columns are
+compared at 3e-8 of the receiver's scale; Okada columns stay at 1e-12."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _elem_err(K, G, dofs):
+    """max |K-G| / receiver-element scale, with per-element row counts."""
+    worst, r = 0.0, 0
+    for d in dofs:
+        sc = np.max(np.abs(G[r:r + d]))
+        worst = max(worst, np.max(np.abs(K[r:r + d] - G[r:r + d])) / sc)
+        r += d
+    return worst
+
+
+@pytest.fixture(scope="module")
+def small_cfg3():
+    from unicycle_b200 import configs
+    return configs.cfg3(nxf=8, nzf=4, nxv=4, nyv=2, nzv=2)
+
+
+def test_volume_assembly_vs_oracle(ucg, oracle_lib, small_cfg3):
+    from unicycle_b200 import configs
+    c = small_cfg3
+    sim = ucg.Simulation(c["mu"], c["lam"], driver="viscouscycles")
+    configs.build_coupled(sim, c)
+    K = sim.copy_G()
+    M = oracle_lib.Mesh(c["mu"], c["lam"], rect=c["mesh"]["rect"], vol=c["mesh"]["vol"])
+    G = M.build_g()
+    nf, nv = c["n_patch"], c["n_vol"]
+    assert K.shape == G.shape == (3 * nf + 6 * nv, 2 * nf + 6 * nv)
+    dofs = [3] * nf + [6] * nv
+    # fault-source columns (Okada) to 1e-12, volume-source columns to the oracle's accuracy
+    assert _elem_err(K[:, :2 * nf], G[:, :2 * nf], dofs) < 1e-12
+    assert _elem_err(K[:, 2 * nf:], G[:, 2 * nf:], dofs) < 3e-8
+    sim.close()
+
+
+def test_viscous_odefun_vs_oracle(ucg, oracle_lib, small_cfg3):
+    from unicycle_b200 import configs
+    c = small_cfg3
+    sim = ucg.Simulation(c["mu"], c["lam"], driver="viscouscycles")
+    configs.build_coupled(sim, c)
+    K = sim.copy_G()
+    y0 = configs.coseismic_preload(K, c)
+    md = oracle_lib.Model(K, c["friction"], vol=c["rheology"] | {"ebg": c["rheology"]["ebg"].ravel()},
+                          viscous=True, nonlinear_maxwell=True)
+    dy, vmax = sim.odefun(y0)
+    ref, vref = md.odefun(y0)
+    nf = c["n_patch"]
+    for part, (lo, hi, w) in {"fault": (0, 7 * nf, 7), "vol": (7 * nf, len(y0), 12)}.items():
+        a, b = dy[lo:hi].reshape(-1, w), ref[lo:hi].reshape(-1, w)
+        sc = np.maximum(np.abs(b).max(axis=0), 1e-300)
+        assert np.max(np.abs(a - b) / sc) < 1e-10, part
+    sim.close()
+
+
+def test_coupled_postseismic_relaxation_runs(ucg, small_cfg3):
+    """Device-resident integration of the coseismically loaded coupled model:
+    volume stresses relax (Maxwell) and the state stays finite."""
+    from unicycle_b200 import configs
+    c = small_cfg3
+    sim = ucg.Simulation(c["mu"], c["lam"], driver="viscouscycles")
+    configs.build_coupled(sim, c)
+    y0 = configs.coseismic_preload(sim.copy_G(), c)
+    sim.set_state(y0, 0.0, c["dt0"])
+    steps = sim.run(5 * configs.YEAR, 5000)
+    y, t, dt, acc, rej = sim.get_state()
+    nf = c["n_patch"]
+    s0 = np.abs(y0[7 * nf:].reshape(-1, 12)[:, 6:]).max()
+    s1 = np.abs(y[7 * nf:].reshape(-1, 12)[:, 6:]).max()
+    assert np.all(np.isfinite(y)) and steps > 10 and t > 0
+    assert s1 < s0          # relaxation of the coseismic stress change
+    sim.close()

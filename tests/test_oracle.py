@@ -234,3 +234,58 @@ def test_reference_step_control_is_rounding_sensitive(oracle_lib):
     Gp = G * (1.0 + rng.choice([-1.0, 0.0, 1.0], size=G.shape) * 2.220446049250313e-16)
     a, b = times(G), times(Gp)
     assert np.max(np.abs(a - b) / a) > 1e-4
+
+
+# ---- strain volumes (Barbot, Moore & Lambert 2017) ---------------------------
+
+NU = 0.25
+
+
+def _sv(oracle_lib, x, q, L, T, W, th, eps):
+    return oracle_lib.bml17_stress(np.asarray(x, float), np.asarray(q, float), L, T, W, th, eps, MU, NU)
+
+
+@pytest.mark.parametrize("q", range(6))
+def test_bml17_free_surface_traction_free(oracle_lib, q):
+    eps = np.eye(6)[q]
+    for x in ([5000.0, -4000.0, 0.0], [-2500.0, 3000.0, 0.0]):
+        s = _sv(oracle_lib, x, [0.0, 0.0, 2000.0], 3000.0, 2000.0, 1500.0, 0.3, eps)
+        ref = _sv(oracle_lib, [x[0], x[1], 1500.0], [0.0, 0.0, 2000.0], 3000.0, 2000.0, 1500.0, 0.3, eps)
+        assert np.max(np.abs(s[[2, 4, 5]])) < 2e-8 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("axis", ["L", "T", "W"])
+def test_bml17_cuboid_additivity(oracle_lib, axis):
+    """A cuboid split in two halves produces the sum of their fields."""
+    q = np.array([1000.0, -500.0, 2000.0])
+    L, T, W, th = 3000.0, 2000.0, 1500.0, 0.4
+    sv = np.array([np.cos(th), np.sin(th), 0.0])
+    nv = np.array([-np.sin(th), np.cos(th), 0.0])
+    if axis == "L":
+        halves = [(q, L / 2, T, W), (q + sv * L / 2, L / 2, T, W)]
+    elif axis == "T":
+        halves = [(q - nv * T / 4, L, T / 2, W), (q + nv * T / 4, L, T / 2, W)]
+    else:
+        halves = [(q, L, T, W / 2), (q + np.array([0, 0, W / 2]), L, T, W / 2)]
+    rng = np.random.default_rng(9)
+    for _ in range(4):
+        x = rng.uniform([-4e3, -4e3, 4500.0], [6e3, 5e3, 7e3])
+        for k in range(6):
+            eps = np.eye(6)[k]
+            whole = _sv(oracle_lib, x, q, L, T, W, th, eps)
+            parts = sum(_sv(oracle_lib, x, qq, LL, TT, WW, th, eps) for qq, LL, TT, WW in halves)
+            assert np.max(np.abs(whole - parts)) < 3e-8 * np.max(np.abs(whole))   # numerical derivative
+
+
+def test_bml17_thin_layer_is_a_dislocation(oracle_lib):
+    """A thin vertical layer of thickness T with shear eigenstrain e12 radiates
+    like a vertical strike-slip fault with slip 2 e12 T (Okada restatement) up
+    to O(T / distance)."""
+    q = np.array([0.0, 0.0, 1000.0])
+    L, W, T = 4000.0, 3000.0, 2.0
+    e12 = 1.0e-3
+    x = np.array([2500.0, 3500.0, 2500.0])
+    # cuboid: strike 0, centred on the plane x2 = 0 (q is the strike-line corner)
+    s_vol = _sv(oracle_lib, x, q, L, T, W, 0.0, np.array([0, e12, 0, 0, 0, 0.0]))
+    s_ok = oracle_lib.okada_stress(0, x, q, L, W, 0.0, np.pi / 2, 2 * e12 * T, 0.0, 0.0, MU, 30.0e3)
+    assert np.max(np.abs(s_vol - s_ok)) < 5e-3 * np.max(np.abs(s_ok))

@@ -132,3 +132,68 @@ def build(sim, cfg, okada_mode=0):
     sim.set_tolerance(cfg["epsilon"])
     sim.buildG(okada_mode)
     return sim
+
+
+def cfg3(nxf=64, nzf=64, nxv=32, nyv=16, nzv=16, cell=2000.0, seed=3):
+    """Coupled fault and distributed deformation: a vertical strike-slip fault of
+    nxf x nzf Okada rectangles (64 km x 30 km at full size) above a mantle wedge
+    of nxv x nyv x nzv vertical cuboids of `cell` m starting at 30 km (16 layers of
+    2 km reach 62 km), linear Maxwell rheology (npowerm = 1,
+    gammadot0m = 1/(2 eta)), viscosity log-uniform in [1e18, 1e20] Pa s, no
+    background strain rate.  The initial state is the response to a uniform 5 m
+    strike slip on the fault (one product with the fault columns of K); 50 yr."""
+    dx, dz = 64.0e3 / nxf, 30.0e3 / nzf
+    ix, iz = np.meshgrid(np.arange(nxf), np.arange(nzf), indexing="ij")
+    ix, iz = ix.ravel(), iz.ravel()
+    nf = nxf * nzf
+    x = np.stack([ix * dx, np.zeros(nf), iz * dz], axis=1).astype(float)
+    rect = (x, np.full(nf, dx), np.full(nf, dz), np.zeros(nf), np.full(nf, np.pi / 2))
+    # cuboids centred under the fault: x along strike, y across, z from 30 km
+    jx, jy, jz = np.meshgrid(np.arange(nxv), np.arange(nyv), np.arange(nzv), indexing="ij")
+    jx, jy, jz = jx.ravel(), jy.ravel(), jz.ravel()
+    nv = nxv * nyv * nzv
+    x0 = 32.0e3 - nxv * cell / 2.0
+    vx = np.stack([x0 + jx * cell, (jy - nyv / 2.0 + 0.5) * cell, 30.0e3 + jz * cell], axis=1)
+    vol = (vx, np.full(nv, cell), np.full(nv, cell), np.full(nv, cell), np.zeros(nv))
+    fr = dict(Vpl=np.full(nf, 1.0e-9), rake=np.zeros(nf), mu0=np.full(nf, MU0), sig=np.full(nf, 50.0),
+              a=np.full(nf, 0.01), b=np.full(nf, 0.006), L=np.full(nf, 0.01), Vo=np.full(nf, VO),
+              damping=np.full(nf, ETA))
+    rng = np.random.default_rng(seed)
+    eta = np.exp(rng.uniform(np.log(1.0e18), np.log(1.0e20), nv)) / 1.0e6   # MPa s
+    rheo = dict(ebg=np.zeros((nv, 6)), gammadot0m=1.0 / (2.0 * eta), npowerm=np.ones(nv),
+                nGm=np.full(nv, MU), nQm=np.zeros(nv), nRm=np.ones(nv), To=np.ones(nv))
+    y0 = np.zeros(7 * nf + 12 * nv)
+    y0[:7 * nf] = steady_state(np.full(nf, 0.99e-9), fr)
+    return dict(name=f"cfg3-coupled-{nf}rect-{nv}vol", mu=MU, lam=LAM,
+                mesh=dict(rect=rect, vol=vol), friction=fr, rheology=rheo, y0=y0, epsilon=1.0e-8,
+                t_end=50 * YEAR, dt0=1.0e-3, n_patch=nf, n_vol=nv, coseismic_slip=5.0)
+
+
+def coseismic_preload(K, cfg):
+    """Add the stress change of the config's uniform coseismic strike slip to the
+    initial state (tractions on the fault, stresses in the volumes): one product
+    of the fault-source columns of K (rows = receiver DOFs) with the slip."""
+    nf, nv = cfg["n_patch"], cfg.get("n_vol", 0)
+    s = np.zeros(K.shape[1])
+    s[0:2 * nf:2] = cfg["coseismic_slip"]
+    dt = K @ s
+    y = cfg["y0"].copy()
+    for c in range(3):
+        y[2 + c:7 * nf:7] += dt[c:3 * nf:3]
+    for c in range(6):
+        y[7 * nf + 6 + c::12] += dt[3 * nf + c::6]
+    return y
+
+
+def build_coupled(sim, cfg):
+    """Load a fault + volume config (viscous-cycles driver) and assemble."""
+    sim.set_rectangles(*cfg["mesh"]["rect"])
+    sim.set_volumes(*cfg["mesh"]["vol"])
+    fr = cfg["friction"]
+    sim.set_friction(fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
+                     fr["damping"])
+    rh = cfg["rheology"]
+    sim.set_rheology(rh["ebg"], rh["gammadot0m"], rh["npowerm"], nonlinear_maxwell=True)
+    sim.set_tolerance(cfg["epsilon"])
+    sim.buildG()
+    return sim

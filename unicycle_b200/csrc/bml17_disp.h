@@ -300,7 +300,9 @@ SV_HD void corner(const T &x1, const T &x2, const T &x3, double y1, double y2, d
 // Displacement (u1', u2', u3) in the cuboid frame for unit eigenstrain component
 // q (0..5: 11, 12, 13, 22, 23, 33), all six at once: u[q][i].
 // IU1..IU3 of strainvolume.f90:296-338 and the 8-corner sum of 254-261.
-template <class T>
+// COMP = 0, 1, 2 forms displacement component COMP+1 only (the other
+// integrals are not evaluated); COMP = -1 forms all three.
+template <int COMP = -1, class T>
 SV_HD void displacement(const T &x1, const T &x2, const T &x3, double q3, double L, double Tk,
                         double W, double nu, double G, T u[6][3])
 {
@@ -319,6 +321,7 @@ SV_HD void displacement(const T &x1, const T &x2, const T &x3, double q3, double
         //      + (lam ekk + 2G e22) Ji213 + 2G e23 (Ji212 + Ji313) + (lam ekk + 2G e33) Ji312
         // for the six unit eigenstrains q = 11, 12, 13, 22, 23, 33
         corner(x1, x2, x3, cy1[k], cy2[k], cy3[k], nu, G, [&](int i, int j, int kk, const T &J) {
+            if (COMP >= 0 && i != COMP) return;
             const T sJ = sgk * J;
             const int jk = 3 * j + kk;
             switch (jk) {
