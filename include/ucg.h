@@ -182,6 +182,28 @@ void *ucg_stream(ucg_ctx *ctx);
    stepped at least once).  No reference counterpart. */
 int ucg_profile_traction(ucg_ctx *ctx, int reps, double *ms);
 
+/* ---- allocation-free right-hand side ------------------------------------- */
+
+/* dydt = f(y) for a fault model held entirely in caller-owned DEVICE memory,
+   without any device allocation: for callers that cannot call cudaMalloc at
+   this point (an external memory manager owns the device, or an
+   allocation-free real-time loop).  No counterpart in the reference (it is the
+   odefun of fortran/3d/src/ratestate.f90:624-778 without a context).
+   K: m x n row-major traction matrix (m = 3 np, n = 2 np; patches only);
+   y, dydt: 7 np state and rate; per patch Vpl*cos(rake), Vpl*sin(rake), a, b,
+   sig, L, damping.  Work is queued on `stream` (a cudaStream_t, NULL for the
+   default stream) on the current device.  The only working storage is a fixed
+   8 MB array in the library's device image, which bounds n at 2^20 source DOFs
+   (UCG_E_BADARG beyond); every GPU that loads the library holds it until the
+   process exits.  The first call on a device resolves that array's device
+   address and should come before any stream capture.  Calls share the array:
+   calls that overlap on the GPU race and must be ordered by the caller. */
+int ucg_odefun_noalloc(const double *K, long n, long m, int np, const double *y,
+                       const double *Vpl_cos_rake, const double *Vpl_sin_rake,
+                       const double *a, const double *b, const double *sig,
+                       const double *L, const double *damping, double *dydt,
+                       void *stream);
+
 #ifdef __cplusplus
 }
 #endif

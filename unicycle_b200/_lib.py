@@ -63,6 +63,7 @@ SIGNATURES = {
     "ucg_launch_count": (_l, [_vp]),
     "ucg_stream": (_vp, [_vp]),
     "ucg_profile_traction": (_i, [_vp, _i, _dp]),
+    "ucg_odefun_noalloc": (_i, [_vp, _l, _l, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None

@@ -718,4 +718,94 @@ int rk_odefun(ucg_ctx *c)
     return h->nonfinite ? UCG_E_NONFINITE : UCG_OK;
 }
 
+// ---- allocation-free right-hand side --------------------------------------------
+//
+// ucg_odefun_noalloc evaluates dydt = f(y) for a fault model whose matrix, state,
+// friction parameters and output all live in caller-owned device memory, for
+// callers that cannot allocate device memory at the point of the call (code
+// running under an external memory manager or an allocation-free real-time
+// loop, which must not call cudaMalloc or pull in an allocating library).  The
+// only working storage it needs -- the source velocity vector v and the control
+// block the kernels read -- lives in the fixed array below.  The array is part
+// of the loaded library: every GPU that loads libucg.so holds its 8 MB until
+// the process exits.  Calls share it, so calls that overlap on the GPU (on
+// different streams without ordering) race on v; the array keeps the last
+// call's contents, and the control block is reset at the start of every call.
+
+namespace {
+
+constexpr long NOALLOC_MAX_N = 1L << 20;                // source DOFs (2 per patch)
+constexpr long NOALLOC_CTL_DOUBLES = (sizeof(Ctl) + sizeof(double) - 1) / sizeof(double);
+
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_MAX_N + NOALLOC_CTL_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static double *g_noalloc_addr[NOALLOC_MAX_DEVICES];      // device address per device, set once
+
+__global__ void k_noalloc_ctl_reset(Ctl *ctl)
+{
+    Ctl z;
+    memset(&z, 0, sizeof z);
+    z.active = 1;
+    z.need_stage1 = 1;
+    z.step_target = 1;
+    z.t_end = 1.0e300;
+    *ctl = z;
+}
+
+}  // namespace
+
 }  // namespace ucg
+
+extern "C" int ucg_odefun_noalloc(const double *K, long n, long m, int np, const double *y,
+                                  const double *Vpl_cos_rake, const double *Vpl_sin_rake,
+                                  const double *a, const double *b, const double *sig, const double *L,
+                                  const double *damping, double *dydt, void *stream)
+{
+    using namespace ucg;
+    if (!K || !y || !dydt || !Vpl_cos_rake || !Vpl_sin_rake || !a || !b || !sig || !L || !damping)
+        return UCG_E_BADARG;
+    if (np <= 0 || n != 2L * np || m != 3L * np) return UCG_E_BADARG;
+    if (n > NOALLOC_MAX_N) return UCG_E_BADARG;   // beyond the fixed scratch: 2^20 source DOFs
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return UCG_E_NODEVICE;
+    // set-up, once per device, with that device current: the host-side name of
+    // the array is not a device address, so resolve it here
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return UCG_E_CUDA;
+        g_noalloc_addr[dev] = static_cast<double *>(p);
+    }
+    double *v = g_noalloc_addr[dev];
+    Ctl *ctl = reinterpret_cast<Ctl *>(v + NOALLOC_MAX_N);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+    StageArgs sa{};
+    sa.y = y;
+    sa.ys = const_cast<double *>(y);
+    for (int j = 0; j < 6; j++) sa.k[j] = dydt;
+    sa.v = v;
+    sa.fr.vpl_c = const_cast<double *>(Vpl_cos_rake);
+    sa.fr.vpl_s = const_cast<double *>(Vpl_sin_rake);
+    sa.fr.a = const_cast<double *>(a);
+    sa.fr.b = const_cast<double *>(b);
+    sa.fr.sig = const_cast<double *>(sig);
+    sa.fr.L = const_cast<double *>(L);
+    sa.fr.damping = const_cast<double *>(damping);
+    sa.np = np;
+    sa.nvol = 0;
+    sa.len = 7L * np;
+
+    k_noalloc_ctl_reset<<<1, 1, 0, st>>>(ctl);
+    k_prologue<1><<<(np + 127) / 128, 128, 0, st>>>(sa, ctl);
+    int dcount = 0;
+    cudaDeviceGetAttribute(&dcount, cudaDevAttrMultiProcessorCount, dev);
+    const int pb = (np + 3) / 4;
+    const int grid = pb < dcount ? pb : dcount;
+    const size_t smem = (size_t)TM_STAGES * TM_STAGE_BYTES;
+    auto kfn = k_traction<1, double>;
+    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return UCG_E_CUDA;
+    kfn<<<grid, (MV_WARPS + 1) * 32, smem, st>>>(K, n, n, nullptr, sa, ctl, pb, 0);
+    return cudaGetLastError() == cudaSuccess ? UCG_OK : UCG_E_CUDA;
+}
