@@ -204,6 +204,84 @@ int ucg_odefun_noalloc(const double *K, long n, long m, int np, const double *y,
                        const double *L, const double *damping, double *dydt,
                        void *stream);
 
+/* ---- batched ensembles (tensor-core traction product) --------------------- */
+
+/* An ensemble marches many instances (frictional-parameter sets) of one or
+   more fault geometries together.  Each Runge-Kutta stage evaluates T = K V for
+   all instances of a geometry as one contraction on the tcgen05 tensor cores,
+   with K and V held as bf16 hi/lo pairs (K with a power-of-two scale per row)
+   and FP32 accumulation; state, stage combinations, error norm and step
+   control stay FP64, and every instance keeps its own step size, time and
+   RKQSm decision (fortran/3d/src/ode45.f90:51-108, per instance).  A run is
+   one CUDA-graph launch whose while loop repeats the attempt of all instances
+   until every instance reaches t_end or the attempt budget is spent.  No
+   reference counterpart: the reference runs one parameter set per job. */
+typedef struct ucg_ensemble ucg_ensemble;
+
+#define UCG_ENS_STREAM_K   0   /* (tile, k-block) sequence cut into equal ranges per SM */
+#define UCG_ENS_SPLIT_LPT  1   /* k-split tiles, longest-first onto the least loaded SM */
+
+int ucg_ens_create(ucg_ensemble **ens, int device);
+void ucg_ens_destroy(ucg_ensemble *ens);
+const char *ucg_ens_last_error(ucg_ensemble *ens);
+
+/* Add a geometry from a context that holds an assembled FP64 matrix (patches
+   only), with n_instances instances (1..4096).  The matrix is converted to the
+   tensor-core image at the call; the context may be destroyed afterwards.
+   *geometry receives the geometry index. */
+int ucg_ens_add_geometry(ucg_ensemble *ens, ucg_ctx *ctx, int n_instances, int *geometry);
+
+/* Friction of one instance, the arrays of ucg_set_friction (per patch). */
+int ucg_ens_set_friction(ucg_ensemble *ens, int geometry, int instance, const double *Vpl,
+                         const double *rake, const double *mu0, const double *sig,
+                         const double *a, const double *b, const double *L,
+                         const double *Vo, const double *damping);
+
+/* epsilon and maximumTimeStep of fortran/3d/src/ode45.f90:40-43, all instances. */
+int ucg_ens_set_tolerance(ucg_ensemble *ens, double epsilon, double max_step);
+
+/* State of one instance (7 per patch, the layout of ucg_set_state).  An
+   instance takes part in runs once its state has been set. */
+int ucg_ens_set_state(ucg_ensemble *ens, int geometry, int instance, double time,
+                      const double *y, double dt_next);
+int ucg_ens_get_state(ucg_ensemble *ens, int geometry, int instance, double *y, double *time,
+                      double *dt_next, long *accepted, long *rejected, int *status);
+
+/* Contraction plan: instance tile width ni (32, 64 or 128 instances per MMA)
+   and schedule (UCG_ENS_*; chunk = k-blocks per split for UCG_ENS_SPLIT_LPT,
+   0 = whole tiles).  Without a call the first run picks ni from the largest
+   instance count and stream-K. */
+int ucg_ens_plan(ucg_ensemble *ens, int ni, int schedule, int chunk);
+
+/* Autotuner: times every candidate plan (`reps` launches each) on the device,
+   installs the fastest and writes a one-line-per-candidate report. */
+int ucg_ens_tune(ucg_ensemble *ens, int reps, char *report, long report_len);
+
+/* March every instance to t_end (attempts of all instances in lockstep, at
+   most max_attempts in this call).  *attempts receives the attempts made. */
+int ucg_ens_run(ucg_ensemble *ens, double t_end, long max_attempts, long *attempts);
+
+/* T = K V through the tensor-core contraction for one geometry: V is
+   instance-major (n_instances x n source DOFs), T instance-major
+   (n_instances x m receiver DOFs), host arrays. */
+int ucg_ens_matvec(ucg_ensemble *ens, int geometry, const double *V, double *T);
+
+/* Event catalogue per instance: an event starts at the first accepted step
+   whose starting max slip rate is >= vmax_on and ends once it is < vmax_off
+   (defaults 1e-3 and 1e-4 m/s).  *n_events receives the number of events,
+   *t_first the start time of the first one (-1 when there was none). */
+int ucg_ens_set_event_threshold(ucg_ensemble *ens, double vmax_on, double vmax_off);
+int ucg_ens_get_events(ucg_ensemble *ens, int geometry, int instance, long *n_events,
+                       double *t_first);
+
+/* Attempts so far, instances still active after the last attempt, kernel
+   launches issued and the installed plan's name. */
+int ucg_ens_info(ucg_ensemble *ens, long *total_attempts, int *active, long *launches,
+                 char *plan, long plan_len);
+
+/* Mean device time of one contraction launch over `reps` launches. */
+int ucg_ens_profile_contract(ucg_ensemble *ens, int reps, double *ms);
+
 #ifdef __cplusplus
 }
 #endif

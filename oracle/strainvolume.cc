@@ -10,7 +10,10 @@
  * strainvolume.f90:215-991, as coded in unicycle_b200/csrc/bml17_disp.h) and
  * differentiates them NUMERICALLY -- Richardson-extrapolated central
  * differences -- independently of the device path, which differentiates them
- * exactly with dual numbers.  Strain rotation, eigenstrain removal and Hooke's
+ * exactly with dual numbers.  The integrals cancel heavily (sums of terms up to
+ * ~1e6 times the result), so the displacements are evaluated in x87 extended
+ * precision (long double, 64-bit significand): a binary64 difference quotient
+ * would carry errors near 1e-6 of the stress, the extended one about 1e-9.  Strain rotation, eigenstrain removal and Hooke's
  * law follow strainvolume.f90:1108-1140.  Pins: physical identities (the
  * free surface is traction free, a cuboid split in two sums to the whole, a
  * thin cuboid in shear matches an Okada dislocation), tests/test_oracle.py.
@@ -19,24 +22,25 @@
 #include <cstdlib>
 #include "oracle.h"
 
-static inline double sv_sqrt(double a) { return std::sqrt(a); }
-static inline double sv_log(double a) { return std::log(a); }
-static inline double sv_atan(double a) { return std::atan(a); }
-static inline double sv_atan2(double y, double x) { return std::atan2(y, x); }
-static inline double sv_val(double a) { return a; }
+typedef long double xreal;
+static inline xreal sv_sqrt(xreal a) { return sqrtl(a); }
+static inline xreal sv_log(xreal a) { return logl(a); }
+static inline xreal sv_atan(xreal a) { return atanl(a); }
+static inline xreal sv_atan2(xreal y, xreal x) { return atan2l(y, x); }
+static inline double sv_val(xreal a) { return (double)a; }
 
 #include "../unicycle_b200/csrc/bml17_disp.h"
 
 namespace {
 
 /* u_i for eigenstrain eps (cuboid frame), observation in the cuboid frame */
-void disp(double x1p, double x2p, double x3, double q3, double L, double T, double W, const double eps[6],
-          double G, double nu, double u[3])
+void disp(xreal x1p, xreal x2p, xreal x3, double q3, double L, double T, double W, const double eps[6],
+          double G, double nu, xreal u[3])
 {
-    double uq[6][3];
-    bml17::displacement<-1, double>(x1p, x2p, x3, q3, L, T, W, nu, G, uq);
+    xreal uq[6][3];
+    bml17::displacement<-1, xreal>(x1p, x2p, x3, q3, L, T, W, nu, G, uq);
     for (int i = 0; i < 3; i++) {
-        double s = 0.0;
+        xreal s = 0.0L;
         for (int q = 0; q < 6; q++) s += eps[q] * uq[q][i];
         u[i] = s;
     }
@@ -55,18 +59,18 @@ extern "C" void orc_bml17_stress(double x1, double x2, double x3, double q1, dou
     const double ct = std::cos(theta), st = std::sin(theta);
     const double x1p = (x1 - q1) * ct + (x2 - q2) * st;
     const double x2p = -(x1 - q1) * st + (x2 - q2) * ct;
-    const double h = 1.0e-3 * std::fmin(L, std::fmin(T, W));
+    const xreal h = 1.0e-3L * std::fmin(L, std::fmin(T, W));
     double grad[3][3];  /* grad[i][d] = d u_i / d x_d (cuboid frame) */
     for (int d = 0; d < 3; d++) {
-        double up1[3], um1[3], up2[3], um2[3];
-        double p[3] = {x1p, x2p, x3};
+        xreal up1[3], um1[3], up2[3], um2[3];
+        xreal p[3] = {x1p, x2p, x3};
         if (d == 2 && x3 < 4 * h) {
             /* next to the free surface: one-sided fourth-order stencil below it */
-            double f[5][3];
+            xreal f[5][3];
             for (int k = 0; k < 5; k++) disp(x1p, x2p, x3 + k * h, q3, L, T, W, eps, G, nu, f[k]);
             for (int i = 0; i < 3; i++)
-                grad[i][2] = (-25.0 * f[0][i] + 48.0 * f[1][i] - 36.0 * f[2][i] + 16.0 * f[3][i] - 3.0 * f[4][i]) /
-                             (12.0 * h);
+                grad[i][2] = (double)((-25.0L * f[0][i] + 48.0L * f[1][i] - 36.0L * f[2][i] + 16.0L * f[3][i] -
+                                       3.0L * f[4][i]) / (12.0L * h));
             continue;
         }
         p[d] += h;       disp(p[0], p[1], p[2], q3, L, T, W, eps, G, nu, up1);
@@ -74,9 +78,9 @@ extern "C" void orc_bml17_stress(double x1, double x2, double x3, double q1, dou
         p[d] += 3 * h;   disp(p[0], p[1], p[2], q3, L, T, W, eps, G, nu, up2);
         p[d] -= 4 * h;   disp(p[0], p[1], p[2], q3, L, T, W, eps, G, nu, um2);
         for (int i = 0; i < 3; i++) {
-            const double d1 = (up1[i] - um1[i]) / (2 * h);
-            const double d2 = (up2[i] - um2[i]) / (4 * h);
-            grad[i][d] = (4.0 * d1 - d2) / 3.0;
+            const xreal d1 = (up1[i] - um1[i]) / (2 * h);
+            const xreal d2 = (up2[i] - um2[i]) / (4 * h);
+            grad[i][d] = (double)((4.0L * d1 - d2) / 3.0L);
         }
     }
     const double lambda = G * 2.0 * nu / (1 - 2 * nu);
@@ -135,5 +139,7 @@ extern "C" void orc_vol_frames(int ns, const double *x, const double *L, const d
 extern "C" void orc_bml17_disp(double x1p, double x2p, double x3, double q3, double L, double T, double W,
                                const double eps[6], double G, double nu, double u[3])
 {
-    disp(x1p, x2p, x3, q3, L, T, W, eps, G, nu, u);
+    xreal ux[3];
+    disp(x1p, x2p, x3, q3, L, T, W, eps, G, nu, ux);
+    for (int i = 0; i < 3; i++) u[i] = (double)ux[i];
 }

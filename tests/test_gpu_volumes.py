@@ -3,8 +3,10 @@ and the coupled fault + volume (viscous-cycles) right-hand side.
 
 The device differentiates the published displacement integrals exactly (dual
 numbers); the oracle differentiates the same integrals numerically
-(Richardson central differences, ~1e-9 accurate), so volume columns are
-compared at 3e-8 of the receiver's scale; Okada columns stay at 1e-12."""
+(Richardson central differences in extended precision, ~1e-9 accurate), so
+volume columns are compared at 3e-8 of the receiver's scale; Okada columns stay
+at 1e-12.  No receiver of the configs lies on the plane of a cuboid face, where
+the closed forms are undefined, so every entry must be finite."""
 import numpy as np
 import pytest
 
@@ -37,6 +39,7 @@ def test_volume_assembly_vs_oracle(ucg, oracle_lib, small_cfg3):
     G = M.build_g()
     nf, nv = c["n_patch"], c["n_vol"]
     assert K.shape == G.shape == (3 * nf + 6 * nv, 2 * nf + 6 * nv)
+    assert np.all(np.isfinite(G)) and np.all(np.isfinite(K))
     dofs = [3] * nf + [6] * nv
     # fault-source columns (Okada) to 1e-12, volume-source columns to the oracle's accuracy
     assert _elem_err(K[:, :2 * nf], G[:, :2 * nf], dofs) < 1e-12

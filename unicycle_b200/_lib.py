@@ -26,6 +26,8 @@ UCG_PREC_FP64 = 0
 UCG_PREC_SPLIT_BF16 = 1
 UCG_DRIVER_RATESTATE = 0
 UCG_DRIVER_VISCOUSCYCLES = 1
+UCG_ENS_STREAM_K = 0
+UCG_ENS_SPLIT_LPT = 1
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -64,6 +66,22 @@ SIGNATURES = {
     "ucg_stream": (_vp, [_vp]),
     "ucg_profile_traction": (_i, [_vp, _i, _dp]),
     "ucg_odefun_noalloc": (_i, [_vp, _l, _l, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ucg_ens_create": (_i, [ctypes.POINTER(_vp), _i]),
+    "ucg_ens_destroy": (None, [_vp]),
+    "ucg_ens_last_error": (ctypes.c_char_p, [_vp]),
+    "ucg_ens_add_geometry": (_i, [_vp, _vp, _i, _ip]),
+    "ucg_ens_set_friction": (_i, [_vp, _i, _i] + [_dp] * 9),
+    "ucg_ens_set_tolerance": (_i, [_vp, _d, _d]),
+    "ucg_ens_set_state": (_i, [_vp, _i, _i, _d, _dp, _d]),
+    "ucg_ens_get_state": (_i, [_vp, _i, _i, _dp, _dp, _dp, _lp, _lp, _ip]),
+    "ucg_ens_plan": (_i, [_vp, _i, _i, _i]),
+    "ucg_ens_tune": (_i, [_vp, _i, ctypes.c_char_p, _l]),
+    "ucg_ens_run": (_i, [_vp, _d, _l, _lp]),
+    "ucg_ens_matvec": (_i, [_vp, _i, _dp, _dp]),
+    "ucg_ens_set_event_threshold": (_i, [_vp, _d, _d]),
+    "ucg_ens_get_events": (_i, [_vp, _i, _i, _lp, _dp]),
+    "ucg_ens_info": (_i, [_vp, _lp, _ip, _lp, ctypes.c_char_p, _l]),
+    "ucg_ens_profile_contract": (_i, [_vp, _i, _dp]),
 }
 
 _lib = None

@@ -148,12 +148,16 @@ def cfg3(nxf=64, nzf=64, nxv=32, nyv=16, nzv=16, cell=2000.0, seed=3):
     nf = nxf * nzf
     x = np.stack([ix * dx, np.zeros(nf), iz * dz], axis=1).astype(float)
     rect = (x, np.full(nf, dx), np.full(nf, dz), np.zeros(nf), np.full(nf, np.pi / 2))
-    # cuboids centred under the fault: x along strike, y across, z from 30 km
+    # cuboids under the fault: x along strike, y across, z from 30 km.  One
+    # column of cuboids is centred on the fault plane (y = 0), so that no fault
+    # receiver lies on the plane of a cuboid face: there the closed-form
+    # integrals (the reference's derivative forms too, e.g. the 0/0 of
+    # y1**2/(y1**2+(x2p-y2)**2) at strainvolume.f90:1860) are undefined.
     jx, jy, jz = np.meshgrid(np.arange(nxv), np.arange(nyv), np.arange(nzv), indexing="ij")
     jx, jy, jz = jx.ravel(), jy.ravel(), jz.ravel()
     nv = nxv * nyv * nzv
     x0 = 32.0e3 - nxv * cell / 2.0
-    vx = np.stack([x0 + jx * cell, (jy - nyv / 2.0 + 0.5) * cell, 30.0e3 + jz * cell], axis=1)
+    vx = np.stack([x0 + jx * cell, (jy - nyv // 2) * cell, 30.0e3 + jz * cell], axis=1)
     vol = (vx, np.full(nv, cell), np.full(nv, cell), np.full(nv, cell), np.zeros(nv))
     fr = dict(Vpl=np.full(nf, 1.0e-9), rake=np.zeros(nf), mu0=np.full(nf, MU0), sig=np.full(nf, 50.0),
               a=np.full(nf, 0.01), b=np.full(nf, 0.006), L=np.full(nf, 0.01), Vo=np.full(nf, VO),
@@ -197,3 +201,63 @@ def build_coupled(sim, cfg):
     sim.set_tolerance(cfg["epsilon"])
     sim.buildG()
     return sim
+
+
+def cfg4(shapes=((64, 16), (64, 32), (96, 32), (128, 32)), n_sets=64, size=625.0, seed=4):
+    """Batched ensemble: planar faults of nx x nz Okada rectangles of `size` m with
+    seeded strike (uniform) and dip (uniform 60-90 deg), top edge at the surface;
+    each with n_sets frictional parameter sets.  a = 0.01 everywhere; outside the
+    velocity-weakening window (the cfg1 window scaled to nx x nz) b = 0.006 and
+    Dc = 10 mm; inside it a-b ~ U[-0.006, -0.002] and Dc log-uniform [1, 20] mm,
+    one draw per set.  sigma = 50 MPa, Vpl = 1e-9 m/s, rake 0; V0 = 0.9 Vpl
+    lognormal(0, 0.1) per set, steady state; rtol 1e-8; 500 yr."""
+    rng = np.random.default_rng(seed)
+    geoms = []
+    for nx, nz in shapes:
+        phi = rng.uniform(0.0, 2.0 * np.pi)
+        delta = np.radians(rng.uniform(60.0, 90.0))
+        sv = np.array([np.cos(phi), np.sin(phi), 0.0])
+        dv = np.array([np.sin(phi) * np.cos(delta), -np.cos(phi) * np.cos(delta), -np.sin(delta)])  # up-dip
+        ix, iz = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+        ix, iz = ix.ravel(), iz.ravel()
+        n = nx * nz
+        x = ix[:, None] * size * sv[None, :] - iz[:, None] * size * dv[None, :]
+        x[:, 2] = np.abs(x[:, 2])   # down is positive; exact zero at the top row
+        mesh = dict(rect=(x, np.full(n, size), np.full(n, size), np.full(n, phi), np.full(n, delta)))
+        c0, c1 = int(round(4 * nx / 32)), int(round(28 * nx / 32))
+        r0, r1 = int(round(4 * nz / 16)), int(round(12 * nz / 16))
+        vw = (ix >= c0) & (ix < c1) & (iz >= r0) & (iz < r1)
+        sets, y0s = [], []
+        for _ in range(n_sets):
+            amb = rng.uniform(-0.006, -0.002)
+            dc = np.exp(rng.uniform(np.log(1.0e-3), np.log(20.0e-3)))
+            fr = dict(Vpl=np.full(n, 1.0e-9), rake=np.zeros(n), mu0=np.full(n, MU0), sig=np.full(n, 50.0),
+                      a=np.full(n, 0.01), b=np.where(vw, 0.01 - amb, 0.006), L=np.where(vw, dc, 0.01),
+                      Vo=np.full(n, VO), damping=np.full(n, ETA))
+            V0 = 0.9 * fr["Vpl"] * np.exp(0.1 * rng.standard_normal(n))
+            sets.append(fr)
+            y0s.append(steady_state(V0, fr))
+        geoms.append(dict(name=f"cfg4-{nx}x{nz}", mesh=mesh, friction=sets[0], sets=sets, y0s=y0s, n_patch=n,
+                          mu=MU, lam=LAM, epsilon=1.0e-8))
+    return dict(name="cfg4-ensemble", geoms=geoms, epsilon=1.0e-8, t_end=500 * YEAR, dt0=1.0e-3)
+
+
+def build_ensemble(ens, cfg, sim_factory):
+    """Assemble every geometry of an ensemble config (cfg4) with a Simulation made
+    by sim_factory(mu, lam), add it to `ens` with all its parameter sets and
+    initial states.  Returns the geometry indices."""
+    ids = []
+    for g in cfg["geoms"]:
+        sim = sim_factory(g["mu"], g["lam"])
+        try:
+            build(sim, g)
+            gi = ens.add_geometry(sim, len(g["sets"]))
+        finally:
+            sim.close()
+        for i, (fr, y0) in enumerate(zip(g["sets"], g["y0s"])):
+            ens.set_friction(gi, i, fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"],
+                             fr["Vo"], fr["damping"])
+            ens.set_state(gi, i, y0, 0.0, cfg["dt0"])
+        ids.append(gi)
+    ens.set_tolerance(cfg["epsilon"])
+    return ids

@@ -1,0 +1,1608 @@
+// Batched ensembles: many frictional-parameter instances that share a fault
+// geometry march together, so that the traction product of every Runge-Kutta
+// stage becomes one dense contraction T = K V per geometry (K: 3N x 2N receiver
+// x source DOFs, V: 2N x instances) on the tcgen05 tensor cores.
+//
+// Precision.  K and V are both held as bf16 hi/lo pairs, K with a power-of-two
+// scale per row: K = s (Khi + Klo), V = Vhi + Vlo.  Each k-block issues three
+// MMAs, Khi Vhi + Khi Vlo + Klo Vhi, accumulating in FP32 in tensor memory; the
+// dropped Klo Vlo term and the residuals are of relative size 2^-16.  State,
+// stage combinations, error norm and step control stay FP64 and follow the
+// single-instance integrator (rk.cu) per instance: every instance has its own
+// step size, time, accept/reject decision and counters, and the reference
+// RKQSm controller (fortran/3d/src/ode45.f90:51-108) judges each of them.
+//
+// Anchored stages.  The contraction's rounding (about 1e-5 of |K| |v|) would
+// otherwise enter the embedded error estimate h sum_i dc_i k_i directly: for
+// components whose state and rate are near zero (dip and normal traction and
+// dip slip of a strike-slip fault) the ratio |yerr/yscal| is then set by the
+// rounding and not by h, and at rtol 1e-8 nearly every attempt is rejected.
+// Stage 1 of a step therefore contracts v1 = v(y) once (the anchor t1 = K v1,
+// kept with v1), and stages 2-6 contract only the increment: t_s = t1 +
+// K (v_s - v1).  Since sum_i dc_i = 0 the anchor's rounding cancels from the
+// error estimate, and the increments' rounding scales with |v_s - v1|, which
+// vanishes with h like the truncation error it competes with.
+//
+// Memory layout.  K is stored once per geometry, already in the byte image of
+// the shared-memory tiles that the MMA reads: for every 128-row tile and
+// 64-source k-block, a 16 KB hi image then a 16 KB lo image, rows of 128 bytes
+// in the 128-byte swizzle (16-byte chunk c of row r at chunk c ^ (r mod 8)).
+// One 32 KB cp.async.bulk moves a whole k-block of a tile.  V is written by the
+// stage prologue directly in the same image form (instances are the rows of the
+// B operand).  No tensor map is needed and nothing is re-laid out per stage.
+//
+// Contraction kernel.  Persistent, one CTA per SM, 192 threads: warp 0 issues
+// the bulk copies (4 stages in flight), one lane of warp 1 issues tcgen05.mma
+// and tcgen05.commit, warps 2-5 drain the FP32 accumulators (two in tensor
+// memory, so that the drain of one segment overlaps the MMAs of the next) to a
+// workspace.  Work is a list of segments (tile, k-range) per CTA, produced on
+// the host by a scheduler that the autotuner picks (stream-K, or split-K with
+// longest-first packing), so geometries of uneven sizes balance across the SMs.
+// The partial sums of a tile are added in k order, in FP64, by the stage
+// epilogue kernel: results are deterministic for a given schedule and an
+// instance's column never depends on the other instances.
+//
+// Every mbarrier wait is bounded (about 4 s of %globaltimer); one that runs out
+// records UCG_E_TIMEOUT, the CTA stops issuing, waits (bounded) for its copies
+// and MMAs in flight, frees its tensor memory and returns.
+//
+// One attempt of all instances is 6 x (prologue, contraction, epilogue) plus a
+// finish and a control kernel; the attempt is the body of a CUDA-graph while
+// loop whose condition the control kernel sets, so a whole run of many
+// attempts is ONE graph launch.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <queue>
+#include <string>
+#include <vector>
+#include <cuda_bf16.h>
+#include "ucg_internal.cuh"
+
+namespace ucg {
+namespace ens {
+
+constexpr int BM = 128;                 // K rows per tile (MMA M)
+constexpr int BK = 64;                  // sources per k-block (one 128-byte bf16 row)
+constexpr int A_HALF = BM * BK * 2;     // one bf16 image of a tile k-block: 16 KB
+constexpr int A_IMG = 2 * A_HALF;       // hi + lo
+constexpr int MAX_GEOM = 16;
+constexpr int EW_THREADS = 128;         // element-wise kernels: elements per block
+constexpr int ST_THREADS = 256;         // finish kernel: state entries per block
+constexpr unsigned long long TIMEOUT_NS = 4000000000ull;
+
+template <int NI>
+struct Tile {
+    static constexpr int B_HALF = NI * BK * 2;
+    static constexpr int B_IMG = 2 * B_HALF;
+    static constexpr int STAGE = A_IMG + B_IMG;
+    static constexpr int STAGES = NI <= 64 ? 4 : 3;
+    static constexpr int SMEM = STAGES * STAGE + 1024;   // + slack for 1024-byte alignment
+    static constexpr uint32_t TMEM_COLS = 2 * NI;         // two FP32 accumulators of NI columns
+    // instruction descriptor: F32 accumulator, bf16 A and B, both K-major,
+    // N = NI (bits 17-22, N/8), M = 128 (bits 24-28, M/16)
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NI >> 3) << 17) |
+                                      ((uint32_t)(BM >> 4) << 24);
+};
+
+// byte offset of element (r, k) in a 128-byte-swizzled tile image with 128-byte rows
+__host__ __device__ __forceinline__ uint32_t sw128(int r, int k)
+{
+    return (uint32_t)r * 128u + ((((uint32_t)(k >> 3) ^ (uint32_t)(r & 7)) << 4) | ((uint32_t)(k & 7) << 1));
+}
+
+// per-instance integrator control (the single-instance Ctl, one per instance)
+struct InstCtl {
+    double h, time, dt_next, hdid, vmax;
+    unsigned long long errbits;
+    long long accepted, rejected;
+    int need_stage1, pending, status, active, nonfinite, in_event;
+    double t_event;             // start time of the first step with max V >= the event threshold
+    long long n_events;         // threshold up-crossings
+};
+
+struct EnsGlobal {
+    double t_end, epsilon, hmax;
+    long long attempts;         // attempts of the current launch
+    long long budget;           // attempt limit of the current launch
+    long long total_attempts;
+    double ev_on, ev_off;       // event thresholds on max V (m/s)
+    int active_count;
+    int err;                    // UCG_E_TIMEOUT from the contraction
+};
+
+struct GeomDev {
+    int np, ninst, mtiles, kblocks;
+    int tile0;                  // global id of tile (nt = 0, mt = 0)
+    int blk_e0, epb_e;          // element-wise grid: first block, blocks per instance
+    int blk_s0, epb_s;          // state-wise grid
+    uint8_t *B;                 // V images [ntile][kblock][hi | lo]
+    const float *rscale;        // per K row (mtiles * 128)
+    double *y, *ys, *k[6], *ycand, *yerr, *yscal;           // [ninst][7 np]
+    double *v1, *t1;            // stage-1 anchor: [ninst][2 np] velocities, [ninst][3 np] tractions
+    const double *vpl_c, *vpl_s, *a, *b, *sig, *L, *damping; // [ninst][np]
+    InstCtl *ctl;               // [ninst]
+};
+
+struct EnsArgs {
+    int ngeom, ni, blocks_e, blocks_s;
+    GeomDev g[MAX_GEOM];
+    const float *ws;            // partial sums [slot][ni][128]
+    const int *piece0, *npieces;
+    EnsGlobal *glob;
+};
+
+struct GemmTile {
+    const uint8_t *a;           // K images of k-block 0 of this tile
+    const uint8_t *b;           // V images of k-block 0 of this instance tile
+};
+struct GemmSeg {
+    int tile, kb0, kb1, slot;
+};
+
+// ---- PTX helpers ------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t s_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bar_init(uint64_t *b, uint32_t n)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_addr(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void bar_expect_tx(uint64_t *b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s_addr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bar_arrive(uint64_t *b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(s_addr(b)) : "memory");
+}
+__device__ __forceinline__ bool bar_try(uint64_t *b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(s_addr(b)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+// bounded wait; abort == nullptr waits out the deadline regardless of other threads
+__device__ __forceinline__ bool bar_wait(uint64_t *b, uint32_t parity, volatile int *abort)
+{
+    if (bar_try(b, parity)) return true;
+    const unsigned long long t0 = now_ns();
+    for (unsigned it = 1;; it++) {
+        if (bar_try(b, parity)) return true;
+        if ((it & 127u) == 0u) {
+            if (abort && *abort) return false;
+            if (now_ns() - t0 > TIMEOUT_NS) return false;
+        }
+    }
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *b)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(s_addr(dst)), "l"(src), "r"(bytes), "r"(s_addr(b)) : "memory");
+}
+// shared-memory matrix descriptor: K-major operand, 128-byte swizzle, 8-row
+// groups 1024 bytes apart (SBO), descriptor version 1
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) |
+           ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
+}
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                 " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                 ::"r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc) : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t *b)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s_addr(b))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ---- the contraction ---------------------------------------------------------------
+
+template <int NI>
+__global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__restrict__ tiles,
+        const GemmSeg *__restrict__ segs, const int *__restrict__ cta_seg, float *__restrict__ ws, int *err)
+{
+    using T = Tile<NI>;
+    extern __shared__ unsigned char dyn_smem[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dyn_smem) + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) uint64_t full[T::STAGES], empty[T::STAGES], acc_full[2], acc_empty[2], drain;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q0 = cta_seg[blockIdx.x], q1 = cta_seg[blockIdx.x + 1];
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < T::STAGES; s++) {
+            bar_init(&full[s], 1);
+            bar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            bar_init(&acc_full[b], 1);
+            bar_init(&acc_empty[b], 4);
+        }
+        bar_init(&drain, 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_addr(&tmem_slot)),
+                     "r"(T::TMEM_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    auto fail = [&]() {
+        abort_flag = 1;
+        atomicExch(err, (int)UCG_E_TIMEOUT);
+    };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer: one 32 KB copy of K and one copy of V per k-block
+            long issued = 0;
+            for (int q = q0; q < q1 && !abort_flag; q++) {
+                const GemmSeg sg = segs[q];
+                const GemmTile tl = tiles[sg.tile];
+                for (int kb = sg.kb0; kb < sg.kb1; kb++) {
+                    const int s = (int)(issued % T::STAGES);
+                    const uint32_t ph = (uint32_t)((issued / T::STAGES) & 1);
+                    if (!bar_wait(&empty[s], ph ^ 1u, &abort_flag)) {
+                        if (!abort_flag) fail();
+                        break;
+                    }
+                    uint8_t *st = smem + (size_t)s * T::STAGE;
+                    bar_expect_tx(&full[s], (uint32_t)(A_IMG + T::B_IMG));
+                    bulk_load(st, tl.a + (size_t)kb * A_IMG, A_IMG, &full[s]);
+                    bulk_load(st + A_IMG, tl.b + (size_t)kb * T::B_IMG, T::B_IMG, &full[s]);
+                    issued++;
+                }
+            }
+            // the last copy into each stage has landed before the CTA may exit
+            for (long i = issued - T::STAGES > 0 ? issued - T::STAGES : 0; i < issued; i++)
+                bar_wait(&full[i % T::STAGES], (uint32_t)((i / T::STAGES) & 1), nullptr);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            long it = 0;
+            int tc = 0;
+            bool issued_any = false;
+            for (int q = q0; q < q1 && !abort_flag; q++, tc++) {
+                const GemmSeg sg = segs[q];
+                const int buf = tc & 1;
+                const uint32_t use = (uint32_t)(tc >> 1);
+                if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag)) {
+                    if (!abort_flag) fail();
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(buf * NI);
+                bool ok = true;
+                for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
+                    const int s = (int)(it % T::STAGES);
+                    const uint32_t ph = (uint32_t)((it / T::STAGES) & 1);
+                    if (!bar_wait(&full[s], ph, &abort_flag)) {
+                        if (!abort_flag) fail();
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a = s_addr(smem + (size_t)s * T::STAGE);
+                    const uint32_t b = a + A_IMG;
+#pragma unroll
+                    for (int j = 0; j < BK / 16; j++) {
+                        const uint64_t ahi = sw128_desc(a + 32u * j), alo = sw128_desc(a + A_HALF + 32u * j);
+                        const uint64_t bhi = sw128_desc(b + 32u * j), blo = sw128_desc(b + T::B_HALF + 32u * j);
+                        mma_bf16(d, ahi, bhi, T::IDESC, (kb > sg.kb0 || j > 0) ? 1u : 0u);
+                        mma_bf16(d, ahi, blo, T::IDESC, 1u);
+                        mma_bf16(d, alo, bhi, T::IDESC, 1u);
+                    }
+                    issued_any = true;
+                    mma_commit(&empty[s]);   // frees the stage once these MMAs have read it
+                }
+                if (!ok) break;
+                mma_commit(&acc_full[buf]);
+            }
+            // no MMA may be in flight when the tensor memory is released
+            if (issued_any) {
+                mma_commit(&drain);
+                bar_wait(&drain, 0u, nullptr);
+            }
+        }
+        __syncwarp();
+    } else {
+        // drain: warp w reads tensor-memory lanes 32 (w mod 4) .. +31 = tile rows
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;
+        int tc = 0;
+        for (int q = q0; q < q1; q++, tc++) {
+            const GemmSeg sg = segs[q];
+            const int buf = tc & 1;
+            const uint32_t use = (uint32_t)(tc >> 1);
+            int ok = 0;
+            if (lane == 0) ok = bar_wait(&acc_full[buf], use & 1u, &abort_flag) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) {
+                if (lane == 0 && !abort_flag) fail();
+                break;
+            }
+            tc_fence_after();
+            float *dst = ws + (size_t)sg.slot * NI * BM + row;
+            const uint32_t tbase = tmem + (uint32_t)(buf * NI) + ((uint32_t)(quarter * 32) << 16);
+#pragma unroll
+            for (int c0 = 0; c0 < NI; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(tbase + (uint32_t)c0, r);
+#pragma unroll
+                for (int i = 0; i < 16; i++) dst[(size_t)(c0 + i) * BM] = __uint_as_float(r[i]);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) bar_arrive(&acc_empty[buf]);
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(T::TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// ---- K images ----------------------------------------------------------------------
+
+// power-of-two row scale >= max |K(r,:)| (1 for an all-zero row)
+__global__ void k_row_scale(const double *__restrict__ K, long m, long n, long rows_pad, float *__restrict__ scale)
+{
+    const long r = blockIdx.x * (long)(blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= rows_pad) return;
+    double mx = 0.0;
+    if (r < m)
+        for (long c = lane; c < n; c += 32) mx = fmax(mx, fabs(K[r * n + c]));
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if (lane == 0) {
+        float s = 1.0f;
+        if (mx > 0.0) {
+            int e;
+            frexp(mx, &e);               // mx = f 2^e, 0.5 <= f < 1
+            s = ldexpf(1.0f, e);         // s >= mx, |K/s| <= 1
+        }
+        scale[r] = s;
+    }
+}
+
+// one thread per (row, 8 sources): 8 doubles in, 16 bytes of hi and of lo out
+__global__ void k_pack_k(const double *__restrict__ K, long m, long n, int kblocks, long rows_pad,
+                         const float *__restrict__ scale, uint8_t *__restrict__ img)
+{
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long per_row = (long)kblocks * (BK / 8);
+    if (t >= rows_pad * per_row) return;
+    const long r = t / per_row;
+    const int c8 = (int)(t % per_row);
+    const int kb = c8 / (BK / 8), kk = (c8 % (BK / 8)) * 8;
+    const long c0 = (long)kb * BK + kk;
+    const double inv = 1.0 / (double)scale[r];
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) {
+        const double x0 = (r < m && c0 + j < n) ? K[r * n + c0 + j] * inv : 0.0;
+        const double x1 = (r < m && c0 + j + 1 < n) ? K[r * n + c0 + j + 1] * inv : 0.0;
+        const __nv_bfloat16 h0 = __double2bfloat16(x0), h1 = __double2bfloat16(x1);
+        const __nv_bfloat16 l0 = __double2bfloat16(x0 - (double)__bfloat162float(h0));
+        const __nv_bfloat16 l1 = __double2bfloat16(x1 - (double)__bfloat162float(h1));
+        hi[j / 2] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+        lo[j / 2] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    }
+    const long mt = r / BM;
+    const int rr = (int)(r % BM);
+    uint8_t *base = img + ((size_t)mt * kblocks + kb) * A_IMG + sw128(rr, kk);
+    *reinterpret_cast<uint4 *>(base) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4 *>(base + A_HALF) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+}
+
+// write the source pair (c, c+1), c even, of instance i into the V images
+__device__ __forceinline__ void put_v(uint8_t *B, int ni, int kblocks, int i, long c, double v0, double v1)
+{
+    const int nt = i / ni, rr = i % ni;
+    const int kb = (int)(c / BK), kk = (int)(c % BK);
+    const size_t bimg = (size_t)2 * ni * BK * 2;
+    uint8_t *base = B + ((size_t)nt * kblocks + kb) * bimg + sw128(rr, kk);
+    const __nv_bfloat16 h0 = __double2bfloat16(v0), h1 = __double2bfloat16(v1);
+    const __nv_bfloat16 l0 = __double2bfloat16(v0 - (double)__bfloat162float(h0));
+    const __nv_bfloat16 l1 = __double2bfloat16(v1 - (double)__bfloat162float(h1));
+    *reinterpret_cast<__nv_bfloat162 *>(base) = __halves2bfloat162(h0, h1);
+    *reinterpret_cast<__nv_bfloat162 *>(base + (size_t)ni * BK * 2) = __halves2bfloat162(l0, l1);
+}
+
+// dense V (instance-major, ninst x n) into the images of one geometry
+__global__ void k_pack_v_dense(uint8_t *B, int ni, int kblocks, int ninst, long n, const double *__restrict__ V)
+{
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long pairs = (n + 1) / 2;
+    if (t >= (long)ninst * pairs) return;
+    const int i = (int)(t / pairs);
+    const long c = 2 * (t % pairs);
+    const double v0 = V[(long)i * n + c];
+    const double v1 = (c + 1 < n) ? V[(long)i * n + c + 1] : 0.0;
+    put_v(B, ni, kblocks, i, c, v0, v1);
+}
+
+__device__ __forceinline__ double traction_row(const EnsArgs *A, const GeomDev &G, int i, long r)
+{
+    const int ni = A->ni;
+    const int mt = (int)(r / BM), rr = (int)(r % BM);
+    const int tile = G.tile0 + (i / ni) * G.mtiles + mt;
+    const int p0 = A->piece0[tile], np_ = A->npieces[tile];
+    const float *w = A->ws + ((size_t)p0 * ni + (i % ni)) * BM + rr;
+    double s = 0.0;
+    for (int p = 0; p < np_; p++) s += (double)w[(size_t)p * ni * BM];
+    return s * (double)G.rscale[r];
+}
+
+// T (instance-major, ninst x m) of geometry gi from the workspace
+__global__ void k_reduce_dense(const EnsArgs *A, int gi, double *T)
+{
+    const GeomDev &G = A->g[gi];
+    const long m = 3L * G.np;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= (long)G.ninst * m) return;
+    const int i = (int)(t / m);
+    const long r = t % m;
+    T[t] = traction_row(A, G, i, r);
+}
+
+// ---- Runge-Kutta stages for all instances --------------------------------------------
+
+__device__ __constant__ double e_B[6][5] = {
+    {0, 0, 0, 0, 0},
+    {0.2, 0, 0, 0, 0},
+    {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
+    {0.3, -0.9, 1.2, 0, 0},
+    {-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0},
+    {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+
+static const double E_LG10 = 2.302585092994045684017991454684364208;
+
+__device__ __forceinline__ bool inst_live(const InstCtl *c, const EnsGlobal *g)
+{
+    return c->active && c->status == 0 && g->err == 0;
+}
+
+__device__ __forceinline__ int geom_of(const EnsArgs *A, int blk, bool state_grid)
+{
+    int gi = 0;
+    while (gi + 1 < A->ngeom && blk >= (state_grid ? A->g[gi + 1].blk_s0 : A->g[gi + 1].blk_e0)) gi++;
+    return gi;
+}
+
+template <int S>
+__device__ __forceinline__ double ens_comb(const GeomDev &G, long i, double h)
+{
+    const double y = G.y[i];
+    if (S == 1) return y;
+    if (S == 2) return __dadd_rn(y, __dmul_rn(__dmul_rn(h, e_B[1][0]), G.k[0][i]));
+    double r = __dmul_rn(e_B[S - 1][0], G.k[0][i]);
+#pragma unroll
+    for (int j = 1; j < S - 1; j++) r = __dadd_rn(r, __dmul_rn(e_B[S - 1][j], G.k[j][i]));
+    return __dadd_rn(y, __dmul_rn(h, r));
+}
+
+// stage state, velocities and the V images (ratestate.f90:667-707 per instance)
+template <int S>
+__global__ void k_ens_prologue(const EnsArgs *__restrict__ A)
+{
+    const int gi = geom_of(A, blockIdx.x, false);
+    const GeomDev &G = A->g[gi];
+    const int local = blockIdx.x - G.blk_e0;
+    const int i = local / G.epb_e;
+    const int e = (local % G.epb_e) * EW_THREADS + threadIdx.x;
+    if (i >= G.ninst || e >= G.np) return;
+    InstCtl *c = G.ctl + i;
+    const long o = (long)i * 7 * G.np + 7L * e;
+    if (S == 1 && c->pending)
+        for (int q = 0; q < 7; q++) G.y[o + q] = G.ycand[o + q];
+    double v0 = 0.0, v1 = 0.0;
+    if (inst_live(c, A->glob) && !(S == 1 && !c->need_stage1)) {
+        const double h = c->h;
+        if (S > 1) {
+            for (int q = 0; q < 7; q++) G.ys[o + q] = ens_comb<S>(G, o + q, h);
+            if (S == 2 && c->need_stage1)
+                for (int q = 0; q < 7; q++)
+                    G.yscal[o + q] = fabs(G.y[o + q]) + fabs(h * G.k[0][o + q]) + 1.0e-30;
+        }
+        const double *yy = (S == 1) ? G.y : G.ys;
+        const double rake = atan2(yy[o + 3], yy[o + 2]);
+        const double vel = exp(yy[o + 6] * E_LG10);
+        const double vs = vel * cos(rake), vd = vel * sin(rake);
+        double *ks = G.k[S - 1];
+        ks[o + 0] = vs;
+        ks[o + 1] = vd;
+        const long pe = (long)i * G.np + e;
+        v0 = vs - G.vpl_c[pe];
+        v1 = vd - G.vpl_s[pe];
+        if (!isfinite(vel) || !isfinite(rake)) {
+            c->nonfinite = 1;
+            v0 = v1 = 0.0;
+        }
+        if (S == 1) {
+            atomicMax((unsigned long long *)&c->vmax, (unsigned long long)__double_as_longlong(vel));
+            G.v1[2 * pe] = v0;
+            G.v1[2 * pe + 1] = v1;
+        } else {
+            // increment over the stage-1 anchor
+            v0 = v0 - G.v1[2 * pe];
+            v1 = v1 - G.v1[2 * pe + 1];
+        }
+    }
+    put_v(G.B, A->ni, G.kblocks, i, 2L * e, v0, v1);
+}
+
+// traction rates from the contraction and the rate-state right-hand side
+// (ratestate.f90:731-776 per instance)
+template <int S>
+__global__ void k_ens_rhs(const EnsArgs *__restrict__ A)
+{
+    const int gi = geom_of(A, blockIdx.x, false);
+    const GeomDev &G = A->g[gi];
+    const int local = blockIdx.x - G.blk_e0;
+    const int i = local / G.epb_e;
+    const int e = (local % G.epb_e) * EW_THREADS + threadIdx.x;
+    if (i >= G.ninst || e >= G.np) return;
+    const InstCtl *c = G.ctl + i;
+    if (!inst_live(c, A->glob) || (S == 1 && !c->need_stage1)) return;
+    double t[3];
+    double *t1 = G.t1 + (long)i * 3 * G.np + 3L * e;
+    for (int q = 0; q < 3; q++) {
+        const double inc = traction_row(A, G, i, 3L * e + q);
+        if (S == 1) {
+            t1[q] = inc;
+            t[q] = inc;
+        } else {
+            t[q] = t1[q] + inc;
+        }
+    }
+    const double *yy = (S == 1) ? G.y : G.ys;
+    const long o = (long)i * 7 * G.np + 7L * e;
+    const long pe = (long)i * G.np + e;
+    const double rake = atan2(yy[o + 3], yy[o + 2]);
+    const double vel = exp(yy[o + 6] * E_LG10);
+    const double L = G.L[pe], bb = G.b[pe], sg = G.sig[pe], aa = G.a[pe], eta = G.damping[pe];
+    const double cr = cos(rake), sr = sin(rake);
+    const double dth = (exp(-yy[o + 5] * E_LG10) - vel / L) / E_LG10;
+    const double dtau = t[0] * cr + t[1] * sr;
+    const double dv = (dtau - bb * sg * dth * E_LG10) / (aa * sg + eta * vel) / E_LG10;
+    const double corr = eta * vel * dv * E_LG10;
+    double *ks = G.k[S - 1];
+    ks[o + 2] = t[0] - corr * cr;
+    ks[o + 3] = t[1] - corr * sr;
+    ks[o + 4] = t[2];
+    ks[o + 5] = dth;
+    ks[o + 6] = dv;
+}
+
+#define E_C1 (37.0 / 378.0)
+#define E_C3 (250.0 / 621.0)
+#define E_C4 (125.0 / 594.0)
+#define E_C6 (512.0 / 1771.0)
+#define E_DC1 (E_C1 - 2825.0 / 27648.0)
+#define E_DC3 (E_C3 - 18575.0 / 48384.0)
+#define E_DC4 (E_C4 - 13525.0 / 55296.0)
+#define E_DC5 (-277.0 / 14336.0)
+#define E_DC6 (E_C6 - 0.25)
+
+// candidate, error estimate and max |yerr/yscal| per instance (ode45.f90:184-200, 68-76)
+__global__ void k_ens_finish(const EnsArgs *__restrict__ A)
+{
+    const int gi = geom_of(A, blockIdx.x, true);
+    const GeomDev &G = A->g[gi];
+    const int local = blockIdx.x - G.blk_s0;
+    const int i = local / G.epb_s;
+    if (i >= G.ninst) return;
+    InstCtl *c = G.ctl + i;
+    if (!inst_live(c, A->glob)) return;        // uniform over the block
+    const long len = 7L * G.np;
+    const long j = (long)(local % G.epb_s) * ST_THREADS + threadIdx.x;
+    const double h = c->h;
+    double mx = 0.0;
+    bool bad = false;
+    if (j < len) {
+        const long x = (long)i * len + j;
+        const double k1 = G.k[0][x], k3 = G.k[2][x], k4 = G.k[3][x], k5 = G.k[4][x], k6 = G.k[5][x];
+        double r = __dmul_rn(E_C1, k1);
+        r = __dadd_rn(r, __dmul_rn(E_C3, k3));
+        r = __dadd_rn(r, __dmul_rn(E_C4, k4));
+        r = __dadd_rn(r, __dmul_rn(E_C6, k6));
+        const double yc = __dadd_rn(G.y[x], __dmul_rn(h, r));
+        double er = __dmul_rn(E_DC1, k1);
+        er = __dadd_rn(er, __dmul_rn(E_DC3, k3));
+        er = __dadd_rn(er, __dmul_rn(E_DC4, k4));
+        er = __dadd_rn(er, __dmul_rn(E_DC5, k5));
+        er = __dadd_rn(er, __dmul_rn(E_DC6, k6));
+        er = __dmul_rn(h, er);
+        G.ycand[x] = yc;
+        G.yerr[x] = er;
+        mx = fmax(0.0, fabs(er / G.yscal[x]));
+        bad = !isfinite(yc);
+    }
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    bad = __any_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+        if (mx > 0.0) atomicMax(&c->errbits, (unsigned long long)__double_as_longlong(mx));
+        if (bad) c->nonfinite = 1;
+    }
+}
+
+// RKQSm decision per instance (ode45.f90:77-106) and the loop condition
+__global__ void k_ens_control(const EnsArgs *__restrict__ A, cudaGraphConditionalHandle cond)
+{
+    EnsGlobal *gl = A->glob;
+    const double SAFETY = 0.7, PGROW = -0.2, PSHRNK = -0.15, ERRCON = 1.89e-4;
+    int live = 0;
+    for (int gi = 0; gi < A->ngeom; gi++) {
+        const GeomDev &G = A->g[gi];
+        for (int i = threadIdx.x; i < G.ninst; i += blockDim.x) {
+            InstCtl *c = G.ctl + i;
+            if (!inst_live(c, gl)) continue;
+            double errmax = __longlong_as_double((long long)c->errbits);
+            c->errbits = 0ull;
+            if (c->nonfinite) {
+                c->status = UCG_E_NONFINITE;
+                c->active = 0;
+                continue;
+            }
+            errmax = errmax / gl->epsilon;
+            double h = c->h;
+            if (errmax > 1.0) {
+                h = h * SAFETY * pow(errmax, PSHRNK);
+                if (h < 0.5 * h) h = 0.5 * h;
+                c->h = h;
+                c->rejected += 1;
+                c->need_stage1 = 0;
+                c->pending = 0;
+                if (0.0 + h == 0.0) {
+                    c->status = UCG_E_STEP_UNDERFLOW;
+                    c->active = 0;
+                    continue;
+                }
+            } else {
+                double hnext;
+                if (errmax > ERRCON) hnext = SAFETY * h * pow(errmax, PGROW);
+                else hnext = 10.0 * h;
+                if (hnext > gl->hmax) hnext = gl->hmax;
+                // event catalogue: max V at the start of this step against the thresholds
+                if (!c->in_event && c->vmax >= gl->ev_on) {
+                    c->in_event = 1;
+                    if (c->n_events == 0) c->t_event = c->time;
+                    c->n_events += 1;
+                } else if (c->in_event && c->vmax < gl->ev_off) {
+                    c->in_event = 0;
+                }
+                c->hdid = h;
+                c->time = c->time + h;
+                c->dt_next = hnext;
+                c->h = hnext;
+                c->accepted += 1;
+                c->pending = 1;
+                c->vmax = 0.0;
+                c->need_stage1 = 1;
+                if (c->time >= gl->t_end) {
+                    c->active = 0;
+                    continue;
+                }
+            }
+            live++;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) live += __shfl_xor_sync(0xffffffffu, live, off);
+    __shared__ int wsum[32];
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = live;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += wsum[w];
+        gl->active_count = tot;
+        gl->attempts += 1;
+        gl->total_attempts += 1;
+        const bool more = tot > 0 && gl->attempts < gl->budget && gl->err == 0;
+        cudaGraphSetConditional(cond, more ? 1u : 0u);
+    }
+}
+
+// start of a launch: activate every healthy instance short of t_end
+__global__ void k_ens_begin(const EnsArgs *__restrict__ A)
+{
+    EnsGlobal *gl = A->glob;
+    for (int gi = 0; gi < A->ngeom; gi++) {
+        const GeomDev &G = A->g[gi];
+        for (int i = threadIdx.x; i < G.ninst; i += blockDim.x) {
+            InstCtl *c = G.ctl + i;
+            c->active = (c->status == 0 && c->time < gl->t_end) ? 1 : 0;
+        }
+    }
+    if (threadIdx.x == 0) gl->attempts = 0;
+}
+
+// end of a launch: copy accepted candidates that no later attempt committed
+__global__ void k_ens_commit(const EnsArgs *__restrict__ A)
+{
+    const int gi = geom_of(A, blockIdx.x, true);
+    const GeomDev &G = A->g[gi];
+    const int local = blockIdx.x - G.blk_s0;
+    const int i = local / G.epb_s;
+    if (i >= G.ninst || !G.ctl[i].pending) return;
+    const long len = 7L * G.np;
+    const long j = (long)(local % G.epb_s) * ST_THREADS + threadIdx.x;
+    if (j < len) G.y[(long)i * len + j] = G.ycand[(long)i * len + j];
+}
+
+__global__ void k_ens_clear_pending(const EnsArgs *__restrict__ A)
+{
+    for (int gi = 0; gi < A->ngeom; gi++) {
+        const GeomDev &G = A->g[gi];
+        for (int i = threadIdx.x; i < G.ninst; i += blockDim.x) G.ctl[i].pending = 0;
+    }
+}
+
+}  // namespace ens
+}  // namespace ucg
+
+// ======================================================================================
+// host side
+// ======================================================================================
+
+using namespace ucg;
+using namespace ucg::ens;
+
+struct EnsGeomHost {
+    int np = 0, ninst = 0, mtiles = 0, kblocks = 0;
+    long m = 0, n = 0;
+    uint8_t *A = nullptr;      // K images
+    float *rscale = nullptr;
+    double *state = nullptr;   // 12 vectors of ninst * 7 np
+    double *anchor = nullptr;  // v1 (ninst * 2 np) then t1 (ninst * 3 np)
+    double *par = nullptr;     // 7 vectors of ninst * np
+    InstCtl *ctl = nullptr;
+    uint8_t *B = nullptr;      // V images for the current ni
+    int b_ni = 0;
+};
+
+struct ucg_ensemble {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sms = 148;
+    std::string err;
+    std::vector<EnsGeomHost> geoms;
+    double epsilon = 1.0e-6, hmax = 1.7976931348623158e308;
+
+    // plan: instance tile width, schedule, workspace
+    int ni = 0;
+    bool planned = false;
+    std::string plan_name;
+    GemmTile *d_tiles = nullptr;
+    GemmSeg *d_segs = nullptr;
+    int *d_cta = nullptr;
+    int *d_piece0 = nullptr, *d_npieces = nullptr;
+    float *ws = nullptr;
+    size_t ws_bytes = 0;
+    int nsegs = 0, ntiles = 0, nslots = 0;
+    std::string tune_report;
+
+    EnsArgs *d_args = nullptr;
+    EnsGlobal *d_glob = nullptr;
+    EnsGlobal *h_glob = nullptr;   // pinned
+    cudaGraphExec_t graph = nullptr;
+    long launches = 0;
+};
+
+namespace {
+
+int efail(ucg_ensemble *E, cudaError_t e, const char *what)
+{
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    E->err = buf;
+    return e == cudaErrorMemoryAllocation ? UCG_E_OOM : UCG_E_CUDA;
+}
+#define ECUDA(call)                                             \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return efail(E, e_, #call);      \
+    } while (0)
+
+int ebad(ucg_ensemble *E, int st, const char *msg)
+{
+    E->err = msg;
+    return st;
+}
+
+// ---- schedules ------------------------------------------------------------------------
+
+struct Sched {
+    std::vector<GemmSeg> segs;
+    std::vector<int> cta;        // P + 1 offsets into segs
+    std::vector<int> piece0, npieces;
+    int nslots = 0;
+    std::string name;
+};
+
+// number the partial sums of each tile in k order
+void number_pieces(Sched &s, int ntiles)
+{
+    std::vector<std::vector<int>> per(ntiles);
+    for (int q = 0; q < (int)s.segs.size(); q++) per[s.segs[q].tile].push_back(q);
+    s.piece0.assign(ntiles, 0);
+    s.npieces.assign(ntiles, 0);
+    int slot = 0;
+    for (int t = 0; t < ntiles; t++) {
+        std::sort(per[t].begin(), per[t].end(), [&](int x, int y) { return s.segs[x].kb0 < s.segs[y].kb0; });
+        s.piece0[t] = slot;
+        s.npieces[t] = (int)per[t].size();
+        for (int q : per[t]) s.segs[q].slot = slot++;
+    }
+    s.nslots = slot;
+}
+
+// stream-K: the (tile, k-block) sequence cut into P equal contiguous ranges
+Sched sched_stream_k(const std::vector<int> &tkb, int P)
+{
+    Sched s;
+    s.name = "stream-k";
+    const int nt = (int)tkb.size();
+    std::vector<long> pre(nt + 1, 0);
+    for (int t = 0; t < nt; t++) pre[t + 1] = pre[t] + tkb[t];
+    const long W = pre[nt];
+    s.cta.assign(P + 1, 0);
+    int t = 0;
+    for (int c = 0; c < P; c++) {
+        const long lo = W * c / P, hi = W * (c + 1) / P;
+        s.cta[c] = (int)s.segs.size();
+        while (t < nt && pre[t + 1] <= lo) t++;
+        for (int u = t; u < nt && pre[u] < hi; u++) {
+            const long a = std::max(lo, pre[u]) - pre[u], b = std::min(hi, pre[u + 1]) - pre[u];
+            if (b > a) s.segs.push_back(GemmSeg{u, (int)a, (int)b, 0});
+        }
+    }
+    s.cta[P] = (int)s.segs.size();
+    number_pieces(s, nt);
+    return s;
+}
+
+// split-K with chunks of about `chunk` k-blocks, longest-first onto the least
+// loaded CTA (each segment also costs `ovh` k-blocks of drain and pipeline fill)
+Sched sched_split_lpt(const std::vector<int> &tkb, int P, int chunk, int ovh)
+{
+    Sched s;
+    s.name = chunk > 0 ? "split-k" + std::to_string(chunk) + "+lpt" : "tiles+lpt";
+    struct Unit { int tile, kb0, kb1; };
+    std::vector<Unit> units;
+    for (int t = 0; t < (int)tkb.size(); t++) {
+        const int parts = chunk > 0 ? std::max(1, (tkb[t] + chunk - 1) / chunk) : 1;
+        for (int j = 0; j < parts; j++) {
+            const int a = (int)((long)tkb[t] * j / parts), b = (int)((long)tkb[t] * (j + 1) / parts);
+            if (b > a) units.push_back(Unit{t, a, b});
+        }
+    }
+    std::stable_sort(units.begin(), units.end(),
+                     [](const Unit &x, const Unit &y) { return (x.kb1 - x.kb0) > (y.kb1 - y.kb0); });
+    using Load = std::pair<long, int>;
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (int c = 0; c < P; c++) heap.push(Load(0, c));
+    std::vector<std::vector<Unit>> per(P);
+    for (const Unit &u : units) {
+        Load l = heap.top();
+        heap.pop();
+        per[l.second].push_back(u);
+        l.first += (u.kb1 - u.kb0) + ovh;
+        heap.push(l);
+    }
+    s.cta.assign(P + 1, 0);
+    for (int c = 0; c < P; c++) {
+        std::sort(per[c].begin(), per[c].end(),
+                  [](const Unit &x, const Unit &y) { return x.tile != y.tile ? x.tile < y.tile : x.kb0 < y.kb0; });
+        s.cta[c] = (int)s.segs.size();
+        for (const Unit &u : per[c]) s.segs.push_back(GemmSeg{u.tile, u.kb0, u.kb1, 0});
+    }
+    s.cta[P] = (int)s.segs.size();
+    number_pieces(s, (int)tkb.size());
+    return s;
+}
+
+// predicted makespan in k-blocks (the largest per-CTA load)
+long sched_cost(const Sched &s, int ovh)
+{
+    long worst = 0;
+    for (size_t c = 0; c + 1 < s.cta.size(); c++) {
+        long l = 0;
+        for (int q = s.cta[c]; q < s.cta[c + 1]; q++) l += s.segs[q].kb1 - s.segs[q].kb0 + ovh;
+        worst = std::max(worst, l);
+    }
+    return worst;
+}
+
+size_t b_bytes(const EnsGeomHost &g, int ni)
+{
+    const int ntl = (g.ninst + ni - 1) / ni;
+    return (size_t)ntl * g.kblocks * (size_t)(2 * ni * BK * 2);
+}
+
+// the dynamic shared-memory limit is raised once per plan, outside any capture
+template <int NI>
+cudaError_t prepare_contract_t()
+{
+    return cudaFuncSetAttribute(k_bf16x3_contract<NI>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tile<NI>::SMEM);
+}
+
+cudaError_t prepare_contract(int ni)
+{
+    switch (ni) {
+    case 32: return prepare_contract_t<32>();
+    case 64: return prepare_contract_t<64>();
+    case 128: return prepare_contract_t<128>();
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int NI>
+cudaError_t launch_contract_t(ucg_ensemble *E)
+{
+    k_bf16x3_contract<NI><<<E->sms, 192, Tile<NI>::SMEM, E->stream>>>(E->d_tiles, E->d_segs, E->d_cta, E->ws,
+                                                                      &E->d_glob->err);
+    E->launches++;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_contract(ucg_ensemble *E)
+{
+    switch (E->ni) {
+    case 32: return launch_contract_t<32>(E);
+    case 64: return launch_contract_t<64>(E);
+    case 128: return launch_contract_t<128>(E);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+void free_plan(ucg_ensemble *E)
+{
+    void *ptrs[] = {E->d_tiles, E->d_segs, E->d_cta, E->d_piece0, E->d_npieces, E->ws};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    E->d_tiles = nullptr;
+    E->d_segs = nullptr;
+    E->d_cta = nullptr;
+    E->d_piece0 = E->d_npieces = nullptr;
+    E->ws = nullptr;
+    E->ws_bytes = 0;
+    if (E->graph) cudaGraphExecDestroy(E->graph);
+    E->graph = nullptr;
+    E->planned = false;
+}
+
+std::vector<int> tile_kblocks(ucg_ensemble *E, int ni)
+{
+    std::vector<int> tkb;
+    for (const EnsGeomHost &g : E->geoms) {
+        const int ntl = (g.ninst + ni - 1) / ni;
+        for (int nt = 0; nt < ntl; nt++)
+            for (int mt = 0; mt < g.mtiles; mt++) tkb.push_back(g.kblocks);
+    }
+    return tkb;
+}
+
+// (re)allocate the V images for instance tiles of width ni
+int ensure_b(ucg_ensemble *E, int ni)
+{
+    for (EnsGeomHost &g : E->geoms) {
+        if (g.B && g.b_ni == ni) continue;
+        if (g.B) cudaFree(g.B);
+        g.B = nullptr;
+        const size_t bytes = b_bytes(g, ni);
+        ECUDA(cudaMalloc(&g.B, bytes));
+        ECUDA(cudaMemsetAsync(g.B, 0, bytes, E->stream));
+        g.b_ni = ni;
+    }
+    return UCG_OK;
+}
+
+// upload tiles, schedule and the kernel argument block for (ni, schedule)
+int install_plan(ucg_ensemble *E, int ni, const Sched &s)
+{
+    free_plan(E);
+    int st = ensure_b(E, ni);
+    if (st) return st;
+    ECUDA(prepare_contract(ni));
+    E->ni = ni;
+    std::vector<GemmTile> tiles;
+    for (const EnsGeomHost &g : E->geoms) {
+        const int ntl = (g.ninst + ni - 1) / ni;
+        for (int nt = 0; nt < ntl; nt++)
+            for (int mt = 0; mt < g.mtiles; mt++)
+                tiles.push_back(GemmTile{g.A + (size_t)mt * g.kblocks * A_IMG,
+                                         g.B + (size_t)nt * g.kblocks * (size_t)(2 * ni * BK * 2)});
+    }
+    E->ntiles = (int)tiles.size();
+    E->nsegs = (int)s.segs.size();
+    E->nslots = s.nslots;
+    ECUDA(cudaMalloc(&E->d_tiles, sizeof(GemmTile) * tiles.size()));
+    ECUDA(cudaMalloc(&E->d_segs, sizeof(GemmSeg) * std::max<size_t>(1, s.segs.size())));
+    ECUDA(cudaMalloc(&E->d_cta, sizeof(int) * s.cta.size()));
+    ECUDA(cudaMalloc(&E->d_piece0, sizeof(int) * tiles.size()));
+    ECUDA(cudaMalloc(&E->d_npieces, sizeof(int) * tiles.size()));
+    E->ws_bytes = (size_t)std::max(1, s.nslots) * ni * BM * sizeof(float);
+    ECUDA(cudaMalloc(&E->ws, E->ws_bytes));
+    ECUDA(cudaMemsetAsync(E->ws, 0, E->ws_bytes, E->stream));
+    ECUDA(cudaMemcpyAsync(E->d_tiles, tiles.data(), sizeof(GemmTile) * tiles.size(), cudaMemcpyHostToDevice, E->stream));
+    if (!s.segs.empty())
+        ECUDA(cudaMemcpyAsync(E->d_segs, s.segs.data(), sizeof(GemmSeg) * s.segs.size(), cudaMemcpyHostToDevice,
+                              E->stream));
+    ECUDA(cudaMemcpyAsync(E->d_cta, s.cta.data(), sizeof(int) * s.cta.size(), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(E->d_piece0, s.piece0.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(E->d_npieces, s.npieces.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice,
+                          E->stream));
+
+    // kernel argument block
+    EnsArgs a;
+    memset(&a, 0, sizeof a);
+    a.ngeom = (int)E->geoms.size();
+    a.ni = ni;
+    int tile0 = 0, be = 0, bs = 0;
+    for (int gi = 0; gi < a.ngeom; gi++) {
+        const EnsGeomHost &g = E->geoms[gi];
+        GeomDev &d = a.g[gi];
+        d.np = g.np;
+        d.ninst = g.ninst;
+        d.mtiles = g.mtiles;
+        d.kblocks = g.kblocks;
+        d.tile0 = tile0;
+        tile0 += ((g.ninst + ni - 1) / ni) * g.mtiles;
+        d.epb_e = (g.np + EW_THREADS - 1) / EW_THREADS;
+        d.blk_e0 = be;
+        be += d.epb_e * g.ninst;
+        d.epb_s = (int)((7L * g.np + ST_THREADS - 1) / ST_THREADS);
+        d.blk_s0 = bs;
+        bs += d.epb_s * g.ninst;
+        d.B = g.B;
+        d.rscale = g.rscale;
+        const long len = (long)g.ninst * 7 * g.np;
+        double *v = g.state;
+        d.y = v; v += len;
+        d.ys = v; v += len;
+        for (int j = 0; j < 6; j++) { d.k[j] = v; v += len; }
+        d.ycand = v; v += len;
+        d.yerr = v; v += len;
+        d.yscal = v; v += len;
+        d.v1 = g.anchor;
+        d.t1 = g.anchor + 2L * g.ninst * g.np;
+        const long pl = (long)g.ninst * g.np;
+        d.vpl_c = g.par; d.vpl_s = g.par + pl; d.a = g.par + 2 * pl; d.b = g.par + 3 * pl;
+        d.sig = g.par + 4 * pl; d.L = g.par + 5 * pl; d.damping = g.par + 6 * pl;
+        d.ctl = g.ctl;
+    }
+    a.blocks_e = be;
+    a.blocks_s = bs;
+    a.ws = E->ws;
+    a.piece0 = E->d_piece0;
+    a.npieces = E->d_npieces;
+    a.glob = E->d_glob;
+    ECUDA(cudaMemcpyAsync(E->d_args, &a, sizeof a, cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    E->plan_name = "ni=" + std::to_string(ni) + " " + s.name;
+    E->planned = true;
+    return UCG_OK;
+}
+
+int default_ni(ucg_ensemble *E)
+{
+    int mx = 1;
+    for (const EnsGeomHost &g : E->geoms) mx = std::max(mx, g.ninst);
+    return mx <= 32 ? 32 : (mx <= 64 ? 64 : 128);
+}
+
+int ensure_plan(ucg_ensemble *E)
+{
+    if (E->planned) return UCG_OK;
+    if (E->geoms.empty()) return ebad(E, UCG_E_STATE, "ensemble has no geometry");
+    const int ni = default_ni(E);
+    return install_plan(E, ni, sched_stream_k(tile_kblocks(E, ni), E->sms));
+}
+
+int time_contract(ucg_ensemble *E, int reps, double *ms)
+{
+    cudaEvent_t a, b;
+    ECUDA(cudaEventCreate(&a));
+    ECUDA(cudaEventCreate(&b));
+    for (int w = 0; w < 2; w++) ECUDA(launch_contract(E));
+    ECUDA(cudaEventRecord(a, E->stream));
+    for (int r = 0; r < reps; r++) ECUDA(launch_contract(E));
+    ECUDA(cudaEventRecord(b, E->stream));
+    ECUDA(cudaEventSynchronize(b));
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = (double)t / reps;
+    int e = 0;
+    ECUDA(cudaMemcpy(&e, &E->d_glob->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return ebad(E, e, "contraction: a bounded device wait gave up");
+    return UCG_OK;
+}
+
+// one Runge-Kutta stage for every instance
+template <int S>
+cudaError_t enqueue_stage(ucg_ensemble *E, int be)
+{
+    k_ens_prologue<S><<<be, EW_THREADS, 0, E->stream>>>(E->d_args);
+    cudaError_t e = launch_contract(E);
+    if (e != cudaSuccess) return e;
+    k_ens_rhs<S><<<be, EW_THREADS, 0, E->stream>>>(E->d_args);
+    E->launches += 2;
+    return cudaGetLastError();
+}
+
+int build_graph(ucg_ensemble *E)
+{
+    if (E->graph) return UCG_OK;
+    int be = 0, bs = 0;
+    for (const EnsGeomHost &g : E->geoms) {
+        be += g.ninst * ((g.np + EW_THREADS - 1) / EW_THREADS);
+        bs += g.ninst * (int)((7L * g.np + ST_THREADS - 1) / ST_THREADS);
+    }
+    cudaGraph_t g;
+    ECUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1u, cudaGraphCondAssignDefault);
+    // head: activate
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(E->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        k_ens_begin<<<1, 256, 0, E->stream>>>(E->d_args);
+        cudaGraph_t tmp;
+        e = cudaStreamEndCapture(E->stream, &tmp);
+    }
+    cudaGraphNode_t head = nullptr, loop = nullptr;
+    if (e == cudaSuccess) {
+        size_t nn = 1;
+        e = cudaGraphGetNodes(g, &head, &nn);
+        if (e == cudaSuccess && nn != 1) e = cudaErrorInvalidValue;
+    }
+    // while (cond) { one attempt }
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&loop, g, &head, 1, &cp);
+    if (e == cudaSuccess) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(E->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t le = enqueue_stage<1>(E, be);
+            if (le == cudaSuccess) le = enqueue_stage<2>(E, be);
+            if (le == cudaSuccess) le = enqueue_stage<3>(E, be);
+            if (le == cudaSuccess) le = enqueue_stage<4>(E, be);
+            if (le == cudaSuccess) le = enqueue_stage<5>(E, be);
+            if (le == cudaSuccess) le = enqueue_stage<6>(E, be);
+            k_ens_finish<<<bs, ST_THREADS, 0, E->stream>>>(E->d_args);
+            k_ens_control<<<1, 256, 0, E->stream>>>(E->d_args, cond);
+            E->launches += 2;
+            cudaGraph_t tmp;
+            e = cudaStreamEndCapture(E->stream, &tmp);
+            if (e == cudaSuccess && le != cudaSuccess) e = le;
+        }
+    }
+    // tail: commit what the last attempts accepted
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(E->stream, g, &loop, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        k_ens_commit<<<bs, ST_THREADS, 0, E->stream>>>(E->d_args);
+        k_ens_clear_pending<<<1, 256, 0, E->stream>>>(E->d_args);
+        cudaGraph_t tmp;
+        e = cudaStreamEndCapture(E->stream, &tmp);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&E->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        E->graph = nullptr;
+        return efail(E, e, "ensemble graph");
+    }
+    return UCG_OK;
+}
+
+bool geom_ok(ucg_ensemble *E, int gi, int i)
+{
+    return E && gi >= 0 && gi < (int)E->geoms.size() && i >= 0 && i < E->geoms[gi].ninst;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ucg_ens_create(ucg_ensemble **out, int device)
+{
+    if (!out) return UCG_E_BADARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return UCG_E_NODEVICE;
+    if (device < 0 || device >= count) return UCG_E_BADARG;
+    ucg_ensemble *E = new (std::nothrow) ucg_ensemble();
+    if (!E) return UCG_E_OOM;
+    E->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&E->d_args, sizeof(EnsArgs));
+    if (e == cudaSuccess) e = cudaMalloc(&E->d_glob, sizeof(EnsGlobal));
+    if (e == cudaSuccess) e = cudaMallocHost(&E->h_glob, sizeof(EnsGlobal));
+    if (e != cudaSuccess) {
+        delete E;
+        return e == cudaErrorMemoryAllocation ? UCG_E_OOM : UCG_E_CUDA;
+    }
+    cudaDeviceGetAttribute(&E->sms, cudaDevAttrMultiProcessorCount, device);
+    memset(E->h_glob, 0, sizeof(EnsGlobal));
+    E->h_glob->epsilon = E->epsilon;
+    E->h_glob->hmax = E->hmax;
+    E->h_glob->ev_on = 1.0e-3;
+    E->h_glob->ev_off = 1.0e-4;
+    cudaMemcpy(E->d_glob, E->h_glob, sizeof(EnsGlobal), cudaMemcpyHostToDevice);
+    *out = E;
+    return UCG_OK;
+}
+
+void ucg_ens_destroy(ucg_ensemble *E)
+{
+    if (!E) return;
+    cudaSetDevice(E->device);
+    if (E->stream) cudaStreamSynchronize(E->stream);
+    free_plan(E);
+    for (EnsGeomHost &g : E->geoms) {
+        void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl, g.B};
+        for (void *p : ptrs)
+            if (p) cudaFree(p);
+    }
+    if (E->d_args) cudaFree(E->d_args);
+    if (E->d_glob) cudaFree(E->d_glob);
+    if (E->h_glob) cudaFreeHost(E->h_glob);
+    if (E->stream) cudaStreamDestroy(E->stream);
+    delete E;
+}
+
+const char *ucg_ens_last_error(ucg_ensemble *E) { return E ? E->err.c_str() : ""; }
+
+int ucg_ens_add_geometry(ucg_ensemble *E, ucg_ctx *c, int n_instances, int *geometry)
+{
+    if (!E || !c) return UCG_E_BADARG;
+    if (n_instances < 1 || n_instances > 4096) return ebad(E, UCG_E_BADARG, "n_instances must be 1..4096");
+    if ((int)E->geoms.size() >= MAX_GEOM) return ebad(E, UCG_E_BADARG, "too many geometries");
+    if (!c->assembled || !c->K) return ebad(E, UCG_E_STATE, "context has no assembled FP64 matrix");
+    if (c->nv != 0) return ebad(E, UCG_E_UNSUPPORTED, "ensembles take fault patches only");
+    if (c->device != E->device) return ebad(E, UCG_E_BADARG, "context on another device");
+    ECUDA(cudaSetDevice(E->device));
+    // the context's work (assembly) must be complete
+    ECUDA(cudaStreamSynchronize(c->stream));
+    EnsGeomHost g;
+    g.np = c->nr + c->nt;
+    g.m = c->m;
+    g.n = c->n;
+    g.ninst = n_instances;
+    g.mtiles = (int)((g.m + BM - 1) / BM);
+    g.kblocks = (int)((g.n + BK - 1) / BK);
+    const long rows_pad = (long)g.mtiles * BM;
+    const size_t aimg = (size_t)g.mtiles * g.kblocks * A_IMG;
+    const long len = (long)g.ninst * 7 * g.np;
+    cudaError_t e = cudaMalloc(&g.A, aimg);
+    if (e == cudaSuccess) e = cudaMalloc(&g.rscale, sizeof(float) * rows_pad);
+    if (e == cudaSuccess) e = cudaMalloc(&g.state, sizeof(double) * 12 * len);
+    if (e == cudaSuccess) e = cudaMalloc(&g.anchor, sizeof(double) * 5L * g.ninst * g.np);
+    if (e == cudaSuccess) e = cudaMalloc(&g.par, sizeof(double) * 7L * g.ninst * g.np);
+    if (e == cudaSuccess) e = cudaMalloc(&g.ctl, sizeof(InstCtl) * g.ninst);
+    if (e == cudaSuccess) e = cudaMemsetAsync(g.state, 0, sizeof(double) * 12 * len, E->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(g.anchor, 0, sizeof(double) * 5L * g.ninst * g.np, E->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(g.par, 0, sizeof(double) * 7L * g.ninst * g.np, E->stream);
+    if (e == cudaSuccess) {
+        std::vector<InstCtl> ctl(g.ninst);
+        memset(ctl.data(), 0, sizeof(InstCtl) * g.ninst);
+        for (InstCtl &x : ctl) {
+            x.need_stage1 = 1;
+            x.status = UCG_E_STATE;    // no state yet: inactive until ucg_ens_set_state
+        }
+        e = cudaMemcpy(g.ctl, ctl.data(), sizeof(InstCtl) * g.ninst, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) {
+        k_row_scale<<<(unsigned)((rows_pad + 7) / 8), 256, 0, E->stream>>>(c->K, g.m, g.n, rows_pad, g.rscale);
+        const long work = rows_pad * (long)g.kblocks * (BK / 8);
+        k_pack_k<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(c->K, g.m, g.n, g.kblocks, rows_pad,
+                                                                       g.rscale, g.A);
+        E->launches += 2;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
+    if (e != cudaSuccess) {
+        void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl};
+        for (void *p : ptrs)
+            if (p) cudaFree(p);
+        return efail(E, e, "ucg_ens_add_geometry");
+    }
+    free_plan(E);
+    E->geoms.push_back(g);
+    if (geometry) *geometry = (int)E->geoms.size() - 1;
+    return UCG_OK;
+}
+
+int ucg_ens_set_friction(ucg_ensemble *E, int gi, int inst, const double *Vpl, const double *rake,
+                         const double *mu0, const double *sig, const double *a, const double *b, const double *L,
+                         const double *Vo, const double *damping)
+{
+    (void)mu0;
+    (void)Vo;
+    if (!geom_ok(E, gi, inst)) return E ? ebad(E, UCG_E_BADARG, "geometry/instance out of range") : UCG_E_BADARG;
+    if (!Vpl || !rake || !sig || !a || !b || !L || !damping) return ebad(E, UCG_E_BADARG, "null array");
+    EnsGeomHost &g = E->geoms[gi];
+    const int np = g.np;
+    std::vector<double> h(7L * np);
+    for (int e = 0; e < np; e++) {
+        h[e] = Vpl[e] * cos(rake[e]);
+        h[np + e] = Vpl[e] * sin(rake[e]);
+        h[2 * np + e] = a[e];
+        h[3 * np + e] = b[e];
+        h[4 * np + e] = sig[e];
+        h[5 * np + e] = L[e];
+        h[6 * np + e] = damping[e];
+    }
+    const long pl = (long)g.ninst * np;
+    for (int q = 0; q < 7; q++)
+        ECUDA(cudaMemcpy(g.par + q * pl + (long)inst * np, h.data() + (long)q * np, sizeof(double) * np,
+                         cudaMemcpyHostToDevice));
+    return UCG_OK;
+}
+
+int ucg_ens_set_tolerance(ucg_ensemble *E, double epsilon, double max_step)
+{
+    if (!E) return UCG_E_BADARG;
+    if (!(epsilon > 0.0) || !(max_step > 0.0)) return ebad(E, UCG_E_BADARG, "tolerance and max step must be > 0");
+    E->epsilon = epsilon;
+    E->hmax = max_step;
+    return UCG_OK;
+}
+
+int ucg_ens_set_state(ucg_ensemble *E, int gi, int inst, double time, const double *y, double dt_next)
+{
+    if (!geom_ok(E, gi, inst)) return E ? ebad(E, UCG_E_BADARG, "geometry/instance out of range") : UCG_E_BADARG;
+    if (!y || !(dt_next > 0.0)) return ebad(E, UCG_E_BADARG, "null state or dt_next <= 0");
+    EnsGeomHost &g = E->geoms[gi];
+    const long len = 7L * g.np;
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    ECUDA(cudaMemcpy(g.state + (long)inst * len, y, sizeof(double) * len, cudaMemcpyHostToDevice));
+    InstCtl x;
+    memset(&x, 0, sizeof x);
+    x.h = dt_next;
+    x.dt_next = dt_next;
+    x.time = time;
+    x.need_stage1 = 1;
+    x.status = UCG_OK;
+    ECUDA(cudaMemcpy(g.ctl + inst, &x, sizeof x, cudaMemcpyHostToDevice));
+    return UCG_OK;
+}
+
+int ucg_ens_get_state(ucg_ensemble *E, int gi, int inst, double *y, double *time, double *dt_next, long *accepted,
+                      long *rejected, int *status)
+{
+    if (!geom_ok(E, gi, inst)) return E ? ebad(E, UCG_E_BADARG, "geometry/instance out of range") : UCG_E_BADARG;
+    EnsGeomHost &g = E->geoms[gi];
+    const long len = 7L * g.np;
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    if (y) ECUDA(cudaMemcpy(y, g.state + (long)inst * len, sizeof(double) * len, cudaMemcpyDeviceToHost));
+    InstCtl x;
+    ECUDA(cudaMemcpy(&x, g.ctl + inst, sizeof x, cudaMemcpyDeviceToHost));
+    if (time) *time = x.time;
+    if (dt_next) *dt_next = x.h;
+    if (accepted) *accepted = (long)x.accepted;
+    if (rejected) *rejected = (long)x.rejected;
+    if (status) *status = x.status;
+    return UCG_OK;
+}
+
+int ucg_ens_plan(ucg_ensemble *E, int ni, int schedule, int chunk)
+{
+    if (!E) return UCG_E_BADARG;
+    if (E->geoms.empty()) return ebad(E, UCG_E_STATE, "ensemble has no geometry");
+    if (ni != 32 && ni != 64 && ni != 128) return ebad(E, UCG_E_BADARG, "ni must be 32, 64 or 128");
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    const std::vector<int> tkb = tile_kblocks(E, ni);
+    if (schedule == UCG_ENS_STREAM_K) return install_plan(E, ni, sched_stream_k(tkb, E->sms));
+    if (schedule == UCG_ENS_SPLIT_LPT) return install_plan(E, ni, sched_split_lpt(tkb, E->sms, chunk, 2));
+    return ebad(E, UCG_E_BADARG, "unknown schedule");
+}
+
+int ucg_ens_tune(ucg_ensemble *E, int reps, char *report, long report_len)
+{
+    if (!E) return UCG_E_BADARG;
+    if (E->geoms.empty()) return ebad(E, UCG_E_STATE, "ensemble has no geometry");
+    if (reps < 1) reps = 5;
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    int maxinst = 1;
+    for (const EnsGeomHost &g : E->geoms) maxinst = std::max(maxinst, g.ninst);
+    std::vector<int> nis = {default_ni(E)};
+    if (maxinst > 64 && nis[0] != 64) nis.push_back(64);
+    std::string rep;
+    double best = 1e300;
+    int best_ni = 0, best_kind = 0, best_chunk = 0;
+    for (int ni : nis) {
+        const std::vector<int> tkb = tile_kblocks(E, ni);
+        struct Cand { int kind, chunk; };
+        std::vector<Cand> cands = {{UCG_ENS_STREAM_K, 0}, {UCG_ENS_SPLIT_LPT, 0}};
+        for (int ch : {8, 16, 32, 64}) cands.push_back({UCG_ENS_SPLIT_LPT, ch});
+        for (const Cand &cd : cands) {
+            const Sched s = cd.kind == UCG_ENS_STREAM_K ? sched_stream_k(tkb, E->sms)
+                                                        : sched_split_lpt(tkb, E->sms, cd.chunk, 2);
+            int st = install_plan(E, ni, s);
+            if (st) return st;
+            double ms = 0.0;
+            st = time_contract(E, reps, &ms);
+            if (st) return st;
+            char line[160];
+            snprintf(line, sizeof line, "ni=%d %-16s segments=%-5d predicted=%-6ld k-blocks  %.4f ms\n", ni,
+                     s.name.c_str(), (int)s.segs.size(), sched_cost(s, 2), ms);
+            rep += line;
+            if (ms < best) {
+                best = ms;
+                best_ni = ni;
+                best_kind = cd.kind;
+                best_chunk = cd.chunk;
+            }
+        }
+    }
+    const int st = ucg_ens_plan(E, best_ni, best_kind, best_chunk);
+    if (st) return st;
+    rep += "chosen: " + E->plan_name + "\n";
+    E->tune_report = rep;
+    if (report && report_len > 0) {
+        strncpy(report, rep.c_str(), (size_t)report_len - 1);
+        report[report_len - 1] = '\0';
+    }
+    return UCG_OK;
+}
+
+int ucg_ens_matvec(ucg_ensemble *E, int gi, const double *V, double *T)
+{
+    if (!E || gi < 0 || gi >= (int)(E ? E->geoms.size() : 0)) return UCG_E_BADARG;
+    if (!V || !T) return ebad(E, UCG_E_BADARG, "null array");
+    ECUDA(cudaSetDevice(E->device));
+    int st = ensure_plan(E);
+    if (st) return st;
+    const EnsGeomHost &g = E->geoms[gi];
+    double *dV = nullptr, *dT = nullptr;
+    ECUDA(cudaMalloc(&dV, sizeof(double) * g.ninst * g.n));
+    cudaError_t e = cudaMalloc(&dT, sizeof(double) * g.ninst * g.m);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dV, V, sizeof(double) * g.ninst * g.n, cudaMemcpyHostToDevice, E->stream);
+    if (e == cudaSuccess) {
+        const long work = (long)g.ninst * ((g.n + 1) / 2);
+        k_pack_v_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(g.B, E->ni, g.kblocks, g.ninst, g.n, dV);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = launch_contract(E);
+    if (e == cudaSuccess) {
+        const long work = (long)g.ninst * g.m;
+        k_reduce_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(E->d_args, gi, dT);
+        E->launches += 2;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(T, dT, sizeof(double) * g.ninst * g.m, cudaMemcpyDeviceToHost, E->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
+    cudaFree(dV);
+    if (dT) cudaFree(dT);
+    if (e != cudaSuccess) return efail(E, e, "ucg_ens_matvec");
+    int derr = 0;
+    ECUDA(cudaMemcpy(&derr, &E->d_glob->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (derr) return ebad(E, derr, "contraction: a bounded device wait gave up");
+    return UCG_OK;
+}
+
+int ucg_ens_run(ucg_ensemble *E, double t_end, long max_attempts, long *attempts)
+{
+    if (!E) return UCG_E_BADARG;
+    if (attempts) *attempts = 0;
+    if (max_attempts < 1) return ebad(E, UCG_E_BADARG, "max_attempts must be >= 1");
+    ECUDA(cudaSetDevice(E->device));
+    int st = ensure_plan(E);
+    if (st) return st;
+    st = build_graph(E);
+    if (st) return st;
+    ECUDA(cudaStreamSynchronize(E->stream));
+    E->h_glob->t_end = t_end;
+    E->h_glob->epsilon = E->epsilon;
+    E->h_glob->hmax = E->hmax;
+    E->h_glob->budget = max_attempts;
+    E->h_glob->attempts = 0;
+    E->h_glob->err = 0;
+    ECUDA(cudaMemcpyAsync(&E->d_glob->t_end, &E->h_glob->t_end, sizeof(double) * 3, cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(&E->d_glob->budget, &E->h_glob->budget, sizeof(long long), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(&E->d_glob->err, &E->h_glob->err, sizeof(int), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaGraphLaunch(E->graph, E->stream));
+    ECUDA(cudaMemcpyAsync(E->h_glob, E->d_glob, sizeof(EnsGlobal), cudaMemcpyDeviceToHost, E->stream));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    if (attempts) *attempts = (long)E->h_glob->attempts;
+    if (E->h_glob->err) return ebad(E, E->h_glob->err, "contraction: a bounded device wait gave up");
+    return UCG_OK;
+}
+
+int ucg_ens_set_event_threshold(ucg_ensemble *E, double vmax_on, double vmax_off)
+{
+    if (!E) return UCG_E_BADARG;
+    if (!(vmax_on > 0.0) || !(vmax_off > 0.0) || vmax_off > vmax_on)
+        return ebad(E, UCG_E_BADARG, "need 0 < vmax_off <= vmax_on");
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    E->h_glob->ev_on = vmax_on;
+    E->h_glob->ev_off = vmax_off;
+    ECUDA(cudaMemcpy(&E->d_glob->ev_on, &E->h_glob->ev_on, 2 * sizeof(double), cudaMemcpyHostToDevice));
+    return UCG_OK;
+}
+
+int ucg_ens_get_events(ucg_ensemble *E, int gi, int inst, long *n_events, double *t_first)
+{
+    if (!geom_ok(E, gi, inst)) return E ? ebad(E, UCG_E_BADARG, "geometry/instance out of range") : UCG_E_BADARG;
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    InstCtl x;
+    ECUDA(cudaMemcpy(&x, E->geoms[gi].ctl + inst, sizeof x, cudaMemcpyDeviceToHost));
+    if (n_events) *n_events = (long)x.n_events;
+    if (t_first) *t_first = x.n_events ? x.t_event : -1.0;
+    return UCG_OK;
+}
+
+int ucg_ens_info(ucg_ensemble *E, long *total_attempts, int *active, long *launches, char *plan, long plan_len)
+{
+    if (!E) return UCG_E_BADARG;
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    EnsGlobal g;
+    ECUDA(cudaMemcpy(&g, E->d_glob, sizeof g, cudaMemcpyDeviceToHost));
+    if (total_attempts) *total_attempts = (long)g.total_attempts;
+    if (active) *active = g.active_count;
+    if (launches) *launches = E->launches;
+    if (plan && plan_len > 0) {
+        strncpy(plan, E->plan_name.c_str(), (size_t)plan_len - 1);
+        plan[plan_len - 1] = '\0';
+    }
+    return UCG_OK;
+}
+
+int ucg_ens_profile_contract(ucg_ensemble *E, int reps, double *ms)
+{
+    if (!E || !ms || reps < 1) return UCG_E_BADARG;
+    ECUDA(cudaSetDevice(E->device));
+    int st = ensure_plan(E);
+    if (st) return st;
+    return time_contract(E, reps, ms);
+}
+
+}  // extern "C"

@@ -1,0 +1,129 @@
+"""Batched ensembles over the libucg C ABI (ucg_ens_* in include/ucg.h).
+
+Many frictional-parameter instances of one or more fault geometries march
+together; the traction product of every Runge-Kutta stage is one tensor-core
+contraction per geometry.  Each instance follows the reference main loop
+(fortran/3d/src/ratestate.f90:307-326) with its own step size and RKQSm
+decision (fortran/3d/src/ode45.f90:51-108).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import UcgError
+from .simulation import _d, _p
+
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class Ensemble:
+    """Instances of fault geometries marched together on one device."""
+
+    def __init__(self, device=0):
+        self.lib = _lib.load()
+        self.ens = ctypes.c_void_p()
+        st = self.lib.ucg_ens_create(ctypes.byref(self.ens), device)
+        if st:
+            raise UcgError(st, f"ucg_ens_create: {self.lib.ucg_strerror(st).decode()}")
+        self.geoms = []   # (n_patches, n_instances)
+
+    def close(self):
+        if self.ens:
+            self.lib.ucg_ens_destroy(self.ens)
+            self.ens = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st, what):
+        if st:
+            msg = self.lib.ucg_ens_last_error(self.ens).decode() or self.lib.ucg_strerror(st).decode()
+            raise UcgError(st, f"{what}: {msg}")
+
+    def add_geometry(self, sim, n_instances):
+        """Add the assembled geometry of `sim` (a Simulation) with n_instances instances."""
+        g = ctypes.c_int()
+        self._check(self.lib.ucg_ens_add_geometry(self.ens, sim.ctx, int(n_instances), ctypes.byref(g)),
+                    "add_geometry")
+        n, m = sim.dims
+        self.geoms.append((n // 2, int(n_instances), n, m))
+        return g.value
+
+    def set_friction(self, geometry, instance, Vpl, rake, mu0, sig, a, b, L, Vo, damping):
+        arrs = [_d(x) for x in (Vpl, rake, mu0, sig, a, b, L, Vo, damping)]
+        self._check(self.lib.ucg_ens_set_friction(self.ens, geometry, instance, *[_p(x) for x in arrs]),
+                    "set_friction")
+
+    def set_tolerance(self, epsilon, maximum_step=1.7976931348623158e308):
+        self._check(self.lib.ucg_ens_set_tolerance(self.ens, epsilon, maximum_step), "set_tolerance")
+
+    def set_state(self, geometry, instance, y, time=0.0, dt_next=1.0e-3):
+        self._check(self.lib.ucg_ens_set_state(self.ens, geometry, instance, time, _p(_d(y)), dt_next),
+                    "set_state")
+
+    def get_state(self, geometry, instance):
+        """Returns (y, time, dt_next, accepted, rejected, status)."""
+        y = np.empty(7 * self.geoms[geometry][0])
+        t, dn = ctypes.c_double(), ctypes.c_double()
+        acc, rej = ctypes.c_long(), ctypes.c_long()
+        st = ctypes.c_int()
+        self._check(self.lib.ucg_ens_get_state(self.ens, geometry, instance, _p(y), ctypes.byref(t),
+                                               ctypes.byref(dn), ctypes.byref(acc), ctypes.byref(rej),
+                                               ctypes.byref(st)), "get_state")
+        return y, t.value, dn.value, acc.value, rej.value, st.value
+
+    def plan(self, ni=64, schedule=_lib.UCG_ENS_STREAM_K, chunk=0):
+        self._check(self.lib.ucg_ens_plan(self.ens, ni, schedule, chunk), "plan")
+
+    def tune(self, reps=5):
+        """Time every candidate contraction plan, install the fastest, return the report."""
+        buf = ctypes.create_string_buffer(8192)
+        self._check(self.lib.ucg_ens_tune(self.ens, reps, buf, len(buf)), "tune")
+        return buf.value.decode()
+
+    def run(self, t_end, max_attempts):
+        """March every instance to t_end; returns the attempts made."""
+        n = ctypes.c_long()
+        self._check(self.lib.ucg_ens_run(self.ens, t_end, max_attempts, ctypes.byref(n)), "run")
+        return n.value
+
+    def matvec(self, geometry, V):
+        """T = K V through the tensor-core contraction; V: (n_instances, n) -> (n_instances, m)."""
+        _, ninst, n, m = self.geoms[geometry]
+        V = _d(V).reshape(ninst, n)
+        T = np.empty((ninst, m))
+        self._check(self.lib.ucg_ens_matvec(self.ens, geometry, _p(V), _p(T)), "matvec")
+        return T
+
+    def set_event_threshold(self, vmax_on=1.0e-3, vmax_off=1.0e-4):
+        self._check(self.lib.ucg_ens_set_event_threshold(self.ens, vmax_on, vmax_off), "set_event_threshold")
+
+    def events(self, geometry, instance):
+        """(number of events, start time of the first event or -1)."""
+        ne, tf = ctypes.c_long(), ctypes.c_double()
+        self._check(self.lib.ucg_ens_get_events(self.ens, geometry, instance, ctypes.byref(ne), ctypes.byref(tf)),
+                    "events")
+        return ne.value, tf.value
+
+    def info(self):
+        """(total attempts, active instances, kernel launches, plan name)."""
+        ta, act, la = ctypes.c_long(), ctypes.c_int(), ctypes.c_long()
+        buf = ctypes.create_string_buffer(256)
+        self._check(self.lib.ucg_ens_info(self.ens, ctypes.byref(ta), ctypes.byref(act), ctypes.byref(la),
+                                          buf, len(buf)), "info")
+        return ta.value, act.value, la.value, buf.value.decode()
+
+    def profile_contract(self, reps=10):
+        ms = ctypes.c_double()
+        self._check(self.lib.ucg_ens_profile_contract(self.ens, reps, ctypes.byref(ms)), "profile_contract")
+        return ms.value
