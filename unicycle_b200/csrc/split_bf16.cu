@@ -73,6 +73,7 @@ int split_bf16_build(ucg_ctx *c)
 
 void split_bf16_free(ucg_ctx *c)
 {
+    if (c->Khi || c->Kscale) rk_drop_graph(c);
     if (c->Khi) cudaFree(c->Khi);
     if (c->Kscale) cudaFree(c->Kscale);
     c->Khi = nullptr;

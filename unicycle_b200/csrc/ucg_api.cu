@@ -83,10 +83,13 @@ static void free_params(ucg_ctx *c)
 {
     double **p[] = {&c->fr.vpl_c, &c->fr.vpl_s, &c->fr.a, &c->fr.b, &c->fr.sig, &c->fr.L, &c->fr.damping,
                     &c->rh.ebg, &c->rh.gd0, &c->rh.npow};
+    rk_drop_graph(c);
     for (double **q : p) {
         if (*q) cudaFree(*q);
         *q = nullptr;
     }
+    for (size_t &n : c->cap_fr) n = 0;
+    for (size_t &n : c->cap_rh) n = 0;
 }
 
 void ucg_destroy(ucg_ctx *c)
@@ -178,12 +181,23 @@ int ucg_set_volumes(ucg_ctx *c, int n, const double *x, const double *L, const d
     return UCG_OK;
 }
 
-static int upload(ucg_ctx *c, double **dst, const std::vector<double> &h)
+// Parameter arrays are rewritten in place when their length is unchanged: the
+// captured attempt graph holds their device addresses, so they must stay valid.
+// A new length (new geometry) reallocates and drops the graph.
+static int upload(ucg_ctx *c, double **dst, size_t *cap, const std::vector<double> &h)
 {
+    if (*dst && *cap == h.size()) {
+        if (!h.empty())
+            UCG_CUDA(cudaMemcpyAsync(*dst, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->stream));
+        return UCG_OK;
+    }
+    rk_drop_graph(c);
     if (*dst) cudaFree(*dst);
     *dst = nullptr;
+    *cap = 0;
     if (h.empty()) return UCG_OK;
     UCG_CUDA(cudaMalloc(dst, sizeof(double) * h.size()));
+    *cap = h.size();
     UCG_CUDA(cudaMemcpyAsync(*dst, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->stream));
     return UCG_OK;
 }
@@ -206,9 +220,11 @@ int ucg_set_friction(ucg_ctx *c, const double *Vpl, const double *rake, const do
         vs[i] = Vpl[i] * sin(rake[i]);
     }
     int rc;
-    if ((rc = upload(c, &c->fr.vpl_c, vc)) || (rc = upload(c, &c->fr.vpl_s, vs)) || (rc = upload(c, &c->fr.a, va)) ||
-        (rc = upload(c, &c->fr.b, vb)) || (rc = upload(c, &c->fr.sig, vsg)) || (rc = upload(c, &c->fr.L, vL)) ||
-        (rc = upload(c, &c->fr.damping, vd)))
+    size_t *cap = c->cap_fr;
+    if ((rc = upload(c, &c->fr.vpl_c, &cap[0], vc)) || (rc = upload(c, &c->fr.vpl_s, &cap[1], vs)) ||
+        (rc = upload(c, &c->fr.a, &cap[2], va)) || (rc = upload(c, &c->fr.b, &cap[3], vb)) ||
+        (rc = upload(c, &c->fr.sig, &cap[4], vsg)) || (rc = upload(c, &c->fr.L, &cap[5], vL)) ||
+        (rc = upload(c, &c->fr.damping, &cap[6], vd)))
         return rc;
     UCG_CUDA(cudaStreamSynchronize(c->stream));
     c->hVpl.assign(Vpl, Vpl + np);
@@ -233,12 +249,14 @@ int ucg_set_rheology(ucg_ctx *c, const double *e_bg, const double *gammadot0m, c
     UCG_CUDA(cudaSetDevice(c->device));
     std::vector<double> e(e_bg, e_bg + 6L * nv), g(gammadot0m, gammadot0m + nv), p(npowerm, npowerm + nv);
     int rc;
-    if ((rc = upload(c, &c->rh.ebg, e)) || (rc = upload(c, &c->rh.gd0, g)) || (rc = upload(c, &c->rh.npow, p)))
+    if ((rc = upload(c, &c->rh.ebg, &c->cap_rh[0], e)) || (rc = upload(c, &c->rh.gd0, &c->cap_rh[1], g)) ||
+        (rc = upload(c, &c->rh.npow, &c->cap_rh[2], p)))
         return rc;
     UCG_CUDA(cudaStreamSynchronize(c->stream));
     c->hebg = e;
     c->hgd0 = g;
     c->hnpow = p;
+    if (c->rh.nonlinear != (nonlinear_maxwell != 0)) rk_drop_graph(c);   // captured by value
     c->rh.nonlinear = nonlinear_maxwell != 0;
     c->have_rheology = true;
     return UCG_OK;
@@ -249,6 +267,7 @@ int ucg_assemble(ucg_ctx *c, int okada_mode)
     if (!c) return UCG_E_BADARG;
     if (okada_mode != UCG_OKADA_FP64 && okada_mode != UCG_OKADA_REF32IO) return bad(c, "okada_mode");
     if (c->nr + c->nt + c->nv == 0) return set_err(c, UCG_E_STATE, "no elements");
+    rk_drop_graph(c);
     split_bf16_free(c);
     int rc = assemble_matrix(c, okada_mode);
     if (rc) return rc;
@@ -293,6 +312,7 @@ int ucg_keep_fp64(ucg_ctx *c, int keep)
     if (!c) return UCG_E_BADARG;
     c->keep_fp64 = keep != 0;
     if (!c->keep_fp64 && c->Khi && c->K) {
+        rk_drop_graph(c);
         cudaStreamSynchronize(c->stream);
         cudaFree(c->K);
         c->K = nullptr;
@@ -436,8 +456,11 @@ int ucg_rkqs(ucg_ctx *c, double *t, double *y, const double *dydt, const double 
     int rc = ensure_state(c);
     if (rc) return rc;
     UCG_CUDA(cudaSetDevice(c->device));
-    if ((rc = put_vec(c, c->st.y, y)) || (rc = put_vec(c, c->st.k[0], dydt)) || (rc = put_vec(c, c->st.yscal, yscal)))
-        return rc;
+    if ((rc = put_vec(c, c->st.y, y))) return rc;
+    // anchored stages need the stage-1 product of this y even though the
+    // caller supplies dydt
+    if (rk_anchored(c) && (rc = rk_odefun(c))) return set_err(c, rc, ucg_strerror(rc));
+    if ((rc = put_vec(c, c->st.k[0], dydt)) || (rc = put_vec(c, c->st.yscal, yscal))) return rc;
     if ((rc = pull_ctl(c))) return rc;
     Ctl *h = c->ctl_host;
     const long acc0 = h->accepted, rej0 = h->rejected;

@@ -46,6 +46,7 @@ struct Stages {
     double *k[6];            // k[0] = dydt (stage 1), k[1..5] = AK2..AK6
     double *v;               // source-DOF velocity / strain-rate vector (n)
     double *t;               // receiver traction / stress (m) for odefun reads
+    double *v1, *t1;         // stage-1 anchor of the split-BF16 product (n, m)
 };
 
 struct Launches {
@@ -88,6 +89,8 @@ struct ucg_ctx {
     bool have_friction = false, have_rheology = false;
     ucg::Friction fr{};
     ucg::Rheology rh{};
+    size_t cap_fr[7] = {0, 0, 0, 0, 0, 0, 0};   // allocated lengths of the arrays above
+    size_t cap_rh[3] = {0, 0, 0};
 
     // integrator
     double epsilon = 1.0e-6;
@@ -117,6 +120,8 @@ int rk_odefun(ucg_ctx *c);                  // k[0] = f(y) on device, sets vmax
 int rk_profile_traction(ucg_ctx *c, int reps, double *ms);
 void rk_enqueue_attempt(ucg_ctx *c);        // one Cash-Karp attempt + control
 void rk_enqueue_commit(ucg_ctx *c);         // copy a pending candidate into y
+bool rk_anchored(const ucg_ctx *c);         // stages contract increments over the stage-1 anchor
+void rk_drop_graph(ucg_ctx *c);             // before freeing anything the attempt graph reads
 int split_bf16_build(ucg_ctx *c);
 void split_bf16_free(ucg_ctx *c);
 

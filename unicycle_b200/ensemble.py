@@ -82,6 +82,26 @@ class Ensemble:
                                                ctypes.byref(st)), "get_state")
         return y, t.value, dn.value, acc.value, rej.value, st.value
 
+    def set_states(self, geometry, y, time, dt_next):
+        """All instances of a geometry: y (n_instances, 7 n), time and dt_next (n_instances,)."""
+        ninst = self.geoms[geometry][1]
+        y = _d(y).reshape(ninst, -1)
+        t = _d(np.broadcast_to(np.asarray(time, dtype=float), (ninst,)))
+        dn = _d(np.broadcast_to(np.asarray(dt_next, dtype=float), (ninst,)))
+        self._check(self.lib.ucg_ens_set_states(self.ens, geometry, _p(y), _p(t), _p(dn)), "set_states")
+
+    def get_states(self, geometry, out=None):
+        """(y (n_instances, 7 n), time, dt_next, accepted, rejected, status) of all instances."""
+        npatch, ninst = self.geoms[geometry][0], self.geoms[geometry][1]
+        y = out if out is not None else np.empty((ninst, 7 * npatch))
+        t, dn = np.empty(ninst), np.empty(ninst)
+        acc, rej = np.empty(ninst, dtype=np.int64), np.empty(ninst, dtype=np.int64)
+        st = np.empty(ninst, dtype=np.int32)
+        lp = ctypes.POINTER(ctypes.c_long)
+        self._check(self.lib.ucg_ens_get_states(self.ens, geometry, _p(y), _p(t), _p(dn), acc.ctypes.data_as(lp),
+                                                rej.ctypes.data_as(lp), st.ctypes.data_as(_ip)), "get_states")
+        return y, t, dn, acc, rej, st
+
     def plan(self, ni=64, schedule=_lib.UCG_ENS_STREAM_K, chunk=0):
         self._check(self.lib.ucg_ens_plan(self.ens, ni, schedule, chunk), "plan")
 
@@ -116,12 +136,20 @@ class Ensemble:
         return ne.value, tf.value
 
     def info(self):
-        """(total attempts, active instances, kernel launches, plan name)."""
+        """dict: attempts, active, launches, accepted, rejected, time_sum, plan."""
         ta, act, la = ctypes.c_long(), ctypes.c_int(), ctypes.c_long()
+        acc, rej, ts = ctypes.c_long(), ctypes.c_long(), ctypes.c_double()
         buf = ctypes.create_string_buffer(256)
         self._check(self.lib.ucg_ens_info(self.ens, ctypes.byref(ta), ctypes.byref(act), ctypes.byref(la),
-                                          buf, len(buf)), "info")
-        return ta.value, act.value, la.value, buf.value.decode()
+                                          ctypes.byref(acc), ctypes.byref(rej), ctypes.byref(ts), buf, len(buf)),
+                    "info")
+        return dict(attempts=ta.value, active=act.value, launches=la.value, accepted=acc.value,
+                    rejected=rej.value, time_sum=ts.value, plan=buf.value.decode())
+
+    @property
+    def stream(self):
+        """The ensemble's cudaStream_t as an integer handle."""
+        return self.lib.ucg_ens_stream(self.ens)
 
     def profile_contract(self, reps=10):
         ms = ctypes.c_double()
