@@ -24,7 +24,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -51,6 +50,9 @@ def parse():
     p.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16"])
     p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split"])
     p.add_argument("--sets", type=int, default=N_SETS, help="instances in the ensemble workload")
+    p.add_argument("--ens-eager", action="store_true",
+                   help="launch the ensemble's attempt kernels from the host instead of one graph launch "
+                        "(for ncu, which does not follow conditional graph nodes)")
     p.add_argument("--spinup", type=int, default=20,
                    help="untimed accepted steps (plain) / attempts (ensemble) before warm-up, past the start-up "
                         "transient of the step size")
@@ -79,53 +81,50 @@ def load_traffic(name):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and throttle reasons sampled through NVML every 20 ms during the
+    timed region (nvidia-smi's own loop is too coarse for sub-second regions)."""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
-        self.proc = None
+        self.sm, self.mx, self.reasons = [], None, set()
+        self.stop = threading.Event()
+        self.t = None
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+            def loop():
+                while not self.stop.is_set():
+                    try:
+                        self.sm.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        for nm, bit in self.REASONS.items():
+                            if r & bit:
+                                self.reasons.add(nm)
+                    except Exception:
+                        pass
+                    self.stop.wait(0.02)
+            self.t = threading.Thread(target=loop, daemon=True)
             self.t.start()
         except Exception:
-            self.proc = None
+            self.t = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([s.strip() for s in line.split(",")])
-
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self.stop.set()
+        if self.t:
+            self.t.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            try:
-                sm.append(float(r[1]))
-                mx = float(r[2])
-                for k, nm in enumerate(names):
-                    if r[5 + k].lower().startswith("active"):
-                        reasons.add(nm)
-            except Exception:
-                pass
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.mx,
+                "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvml, 20 ms"}
 
 
 def dist_init(args):
@@ -373,6 +372,8 @@ def run_ensemble(args, world, rank, local):
                          fr["damping"])
         ens.set_state(0, i, y0, 0.0, cfg["dt0"])
     ens.set_tolerance(cfg["epsilon"])
+    if args.ens_eager:
+        ens.use_graph(False)
     tune_report = ens.tune(reps=3)
     stream = torch.cuda.ExternalStream(ens.stream, device=local)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

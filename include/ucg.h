@@ -265,6 +265,11 @@ int ucg_ens_plan(ucg_ensemble *ens, int ni, int schedule, int chunk);
    installs the fastest and writes a one-line-per-candidate report. */
 int ucg_ens_tune(ucg_ensemble *ens, int reps, char *report, long report_len);
 
+/* Run attempts as one CUDA-graph launch (use_graph != 0, the default) or
+   launch the same kernels one by one from the host (for profilers that do not
+   follow conditional graph nodes). */
+int ucg_ens_use_graph(ucg_ensemble *ens, int use_graph);
+
 /* March every instance to t_end (attempts of all instances in lockstep, at
    most max_attempts in this call).  *attempts receives the attempts made. */
 int ucg_ens_run(ucg_ensemble *ens, double t_end, long max_attempts, long *attempts);

@@ -240,3 +240,24 @@ def test_ensemble_run_stops_at_t_end(ucg):
     ens.close()
     for s in sims:
         s.close()
+
+
+def test_host_launched_attempts_match_graph(ucg):
+    """The attempt loop launched kernel by kernel from the host (for profilers)
+    gives bit-identical trajectories to the single graph launch."""
+    cfg = _small_cfg(shapes=((16, 8),), n_sets=8)
+    sims = _geometry_sims(ucg, cfg)
+    a = _ensemble(ucg, cfg, sims)
+    b = _ensemble(ucg, cfg, sims)
+    b.use_graph(False)
+    a.run(1.0e30, 40)
+    b.run(1.0e30, 40)
+    ya, *ra = a.get_states(0)
+    yb, *rb = b.get_states(0)
+    assert np.array_equal(ya, yb)
+    for x, y in zip(ra, rb):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
+    for s in sims:
+        s.close()

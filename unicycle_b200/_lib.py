@@ -78,6 +78,7 @@ SIGNATURES = {
     "ucg_ens_get_states": (_i, [_vp, _i, _dp, _dp, _dp, _lp, _lp, _ip]),
     "ucg_ens_plan": (_i, [_vp, _i, _i, _i]),
     "ucg_ens_tune": (_i, [_vp, _i, ctypes.c_char_p, _l]),
+    "ucg_ens_use_graph": (_i, [_vp, _i]),
     "ucg_ens_run": (_i, [_vp, _d, _l, _lp]),
     "ucg_ens_matvec": (_i, [_vp, _i, _dp, _dp]),
     "ucg_ens_set_event_threshold": (_i, [_vp, _d, _d]),

@@ -662,7 +662,7 @@ __global__ void k_ens_finish(const EnsArgs *__restrict__ A)
 }
 
 // RKQSm decision per instance (ode45.f90:77-106) and the loop condition
-__global__ void k_ens_control(const EnsArgs *__restrict__ A, cudaGraphConditionalHandle cond)
+__global__ void k_ens_control(const EnsArgs *__restrict__ A, cudaGraphConditionalHandle cond, int in_graph)
 {
     EnsGlobal *gl = A->glob;
     const double SAFETY = 0.7, PGROW = -0.2, PSHRNK = -0.15, ERRCON = 1.89e-4;
@@ -733,7 +733,7 @@ __global__ void k_ens_control(const EnsArgs *__restrict__ A, cudaGraphConditiona
         gl->attempts += 1;
         gl->total_attempts += 1;
         const bool more = tot > 0 && gl->attempts < gl->budget && gl->err == 0;
-        cudaGraphSetConditional(cond, more ? 1u : 0u);
+        if (in_graph) cudaGraphSetConditional(cond, more ? 1u : 0u);
     }
 }
 
@@ -820,6 +820,7 @@ struct ucg_ensemble {
     EnsGlobal *d_glob = nullptr;
     EnsGlobal *h_glob = nullptr;   // pinned
     cudaGraphExec_t graph = nullptr;
+    bool use_graph = true;     // false: attempts launched one by one from the host
     long launches = 0;
 };
 
@@ -1215,7 +1216,7 @@ int build_graph(ucg_ensemble *E)
             if (le == cudaSuccess) le = enqueue_stage<5>(E, be);
             if (le == cudaSuccess) le = enqueue_stage<6>(E, be);
             k_ens_finish<<<bs, ST_THREADS, 0, E->stream>>>(E->d_args);
-            k_ens_control<<<1, 256, 0, E->stream>>>(E->d_args, cond);
+            k_ens_control<<<1, 256, 0, E->stream>>>(E->d_args, cond, 1);
             E->launches += 2;
             cudaGraph_t tmp;
             e = cudaStreamEndCapture(E->stream, &tmp);
@@ -1577,6 +1578,51 @@ int ucg_ens_matvec(ucg_ensemble *E, int gi, const double *V, double *T)
     return UCG_OK;
 }
 
+namespace {
+// the attempt loop without the graph: the same kernels launched from the host,
+// for tools that do not follow conditional graph nodes
+int run_eager(ucg_ensemble *E)
+{
+    int be = 0, bs = 0;
+    for (const EnsGeomHost &g : E->geoms) {
+        be += g.ninst * ((g.np + EW_THREADS - 1) / EW_THREADS);
+        bs += g.ninst * (int)((7L * g.np + ST_THREADS - 1) / ST_THREADS);
+    }
+    k_ens_begin<<<1, 256, 0, E->stream>>>(E->d_args);
+    E->launches++;
+    for (long a = 0; a < E->h_glob->budget; a++) {
+        cudaError_t le = enqueue_stage<1>(E, be);
+        if (le == cudaSuccess) le = enqueue_stage<2>(E, be);
+        if (le == cudaSuccess) le = enqueue_stage<3>(E, be);
+        if (le == cudaSuccess) le = enqueue_stage<4>(E, be);
+        if (le == cudaSuccess) le = enqueue_stage<5>(E, be);
+        if (le == cudaSuccess) le = enqueue_stage<6>(E, be);
+        if (le != cudaSuccess) return efail(E, le, "ensemble attempt");
+        k_ens_finish<<<bs, ST_THREADS, 0, E->stream>>>(E->d_args);
+        k_ens_control<<<1, 256, 0, E->stream>>>(E->d_args, 0, 0);
+        E->launches += 2;
+        if ((a & 15) == 15 || a + 1 == E->h_glob->budget) {
+            EnsGlobal g;
+            ECUDA(cudaMemcpyAsync(&g, E->d_glob, sizeof g, cudaMemcpyDeviceToHost, E->stream));
+            ECUDA(cudaStreamSynchronize(E->stream));
+            if (g.active_count == 0 || g.err) break;
+        }
+    }
+    k_ens_commit<<<bs, ST_THREADS, 0, E->stream>>>(E->d_args);
+    k_ens_clear_pending<<<1, 256, 0, E->stream>>>(E->d_args);
+    E->launches += 2;
+    ECUDA(cudaGetLastError());
+    return UCG_OK;
+}
+}  // namespace
+
+int ucg_ens_use_graph(ucg_ensemble *E, int use_graph)
+{
+    if (!E) return UCG_E_BADARG;
+    E->use_graph = use_graph != 0;
+    return UCG_OK;
+}
+
 int ucg_ens_run(ucg_ensemble *E, double t_end, long max_attempts, long *attempts)
 {
     if (!E) return UCG_E_BADARG;
@@ -1585,8 +1631,10 @@ int ucg_ens_run(ucg_ensemble *E, double t_end, long max_attempts, long *attempts
     ECUDA(cudaSetDevice(E->device));
     int st = ensure_plan(E);
     if (st) return st;
-    st = build_graph(E);
-    if (st) return st;
+    if (E->use_graph) {
+        st = build_graph(E);
+        if (st) return st;
+    }
     ECUDA(cudaStreamSynchronize(E->stream));
     E->h_glob->t_end = t_end;
     E->h_glob->epsilon = E->epsilon;
@@ -1597,7 +1645,12 @@ int ucg_ens_run(ucg_ensemble *E, double t_end, long max_attempts, long *attempts
     ECUDA(cudaMemcpyAsync(&E->d_glob->t_end, &E->h_glob->t_end, sizeof(double) * 3, cudaMemcpyHostToDevice, E->stream));
     ECUDA(cudaMemcpyAsync(&E->d_glob->budget, &E->h_glob->budget, sizeof(long long), cudaMemcpyHostToDevice, E->stream));
     ECUDA(cudaMemcpyAsync(&E->d_glob->err, &E->h_glob->err, sizeof(int), cudaMemcpyHostToDevice, E->stream));
-    ECUDA(cudaGraphLaunch(E->graph, E->stream));
+    if (E->use_graph) {
+        ECUDA(cudaGraphLaunch(E->graph, E->stream));
+    } else {
+        st = run_eager(E);
+        if (st) return st;
+    }
     ECUDA(cudaMemcpyAsync(E->h_glob, E->d_glob, sizeof(EnsGlobal), cudaMemcpyDeviceToHost, E->stream));
     ECUDA(cudaStreamSynchronize(E->stream));
     if (attempts) *attempts = (long)E->h_glob->attempts;

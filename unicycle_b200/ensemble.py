@@ -111,6 +111,10 @@ class Ensemble:
         self._check(self.lib.ucg_ens_tune(self.ens, reps, buf, len(buf)), "tune")
         return buf.value.decode()
 
+    def use_graph(self, flag=True):
+        """Attempts as one CUDA-graph launch (default) or host-launched kernels."""
+        self._check(self.lib.ucg_ens_use_graph(self.ens, 1 if flag else 0), "use_graph")
+
     def run(self, t_end, max_attempts):
         """March every instance to t_end; returns the attempts made."""
         n = ctypes.c_long()
