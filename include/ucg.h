@@ -300,6 +300,53 @@ void *ucg_ens_stream(ucg_ensemble *ens);
 /* Mean device time of one contraction launch over `reps` launches. */
 int ucg_ens_profile_contract(ucg_ensemble *ens, int reps, double *ms);
 
+/* ---- learned step-size proposal ------------------------------------------- */
+
+/* A perceptron 11 -> 64 -> 64 -> 64 (GELU) -> 1 with FP16 weights and
+   activations (FP32 sums, FP32 master weights for training) that proposes
+   log10 of the next step size from: log10 max V and min log10 theta at the
+   start of the step, log10 of the last 8 accepted steps (most recent first)
+   and log10 max(errmax, 1e-12) of the step just accepted.  Trained on the
+   device by the library's own forward/backward kernels on traces that the
+   ensemble integrator records.  In use, the proposal (limited to 0.2..10 times
+   the accepted step) replaces RKQSm's hnext; the embedded error estimate still
+   judges the attempt, and a rejected proposal is shrunk by the plain RKQSm
+   rule (fortran/3d/src/ode45.f90:79-84).  No reference counterpart. */
+typedef struct ucg_mlp ucg_mlp;
+
+#define UCG_MLP_NIN     11
+#define UCG_MLP_NPARAM  9153   /* W1[64][11] b1 W2[64][64] b2 W3[64][64] b3 W4[64] b4 */
+#define UCG_MLP_NNORM   24     /* input means[11], deviations[11], output mean, deviation */
+#define UCG_TRACE_LEN   14     /* 11 inputs, log10 h of the next first attempt, log10 errmax, accepted */
+
+int ucg_mlp_create(ucg_mlp **mlp, int device, unsigned long long seed);
+void ucg_mlp_destroy(ucg_mlp *mlp);
+const char *ucg_mlp_last_error(ucg_mlp *mlp);
+/* FP32 master weights (UCG_MLP_NPARAM) and standardisation (UCG_MLP_NNORM);
+   either may be NULL. */
+int ucg_mlp_set_params(ucg_mlp *mlp, const float *params, const float *norm);
+int ucg_mlp_get_params(ucg_mlp *mlp, float *params, float *norm);
+/* Training set: x (n x 11 raw inputs), y (n labels, log10 dt); standardise != 0
+   sets the standardisation from this set. */
+int ucg_mlp_set_data(ucg_mlp *mlp, const float *x, const float *y, long n, int standardise);
+/* Gradient of the mean loss over samples [offset, offset+count) at the current
+   FP16 weights (UCG_MLP_NPARAM floats) and the mean loss. */
+int ucg_mlp_gradient(ucg_mlp *mlp, long offset, long count, float *grad, double *loss);
+/* Adam over shuffled mini-batches; epoch_loss (may be NULL) gets the mean
+   loss of each epoch. */
+int ucg_mlp_train(ucg_mlp *mlp, int epochs, int batch, float lr, unsigned long long seed,
+                  float *epoch_loss);
+/* log10 dt for raw inputs x (n x 11), with the controllers' own evaluation. */
+int ucg_mlp_predict(ucg_mlp *mlp, const float *x, long n, float *y);
+
+/* Use a model (NULL: the plain RKQSm controller) for every instance of an
+   ensemble.  The model must outlive its use. */
+int ucg_ens_set_step_model(ucg_ensemble *ens, const ucg_mlp *model);
+/* Record traces (capacity records of UCG_TRACE_LEN floats; 0 stops and frees)
+   and read them back. */
+int ucg_ens_record_traces(ucg_ensemble *ens, long capacity);
+int ucg_ens_get_traces(ucg_ensemble *ens, float *buf, long max_records, long *n_records);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,10 @@ def lib():
         L.orc_step.restype = ctypes.c_int
         L.orc_step.argtypes = [ctypes.POINTER(_Model), _dp, _dp, _dp, _dp, ctypes.c_double,
                                ctypes.c_double, _dp, _lp, _dp]
+        _fp = ctypes.POINTER(ctypes.c_float)
+        L.orc_mlp_nparam.restype = ctypes.c_int
+        L.orc_mlp_loss_grad.argtypes = [_fp, _fp, _fp, _fp, ctypes.c_long, ctypes.c_int, _dp, _dp]
+        L.orc_mlp_predict.argtypes = [_fp, _fp, _fp, ctypes.c_long, ctypes.c_int, _dp]
         _lib = L
     return _lib
 
@@ -316,3 +320,30 @@ def rk_overhead_seconds(cfg, reps=3):
     for _ in range(reps):
         rc, t, y, _, dt, _, _ = md.step(t, y, dt, cfg["epsilon"])
     return (time.perf_counter() - t0) / reps
+
+
+def _f(x):
+    return np.ascontiguousarray(x, dtype=np.float32)
+
+
+def mlp_loss_grad(params, norm, X, Y, fp16=True, grad=True):
+    """Mean loss and its gradient for the step-size perceptron (oracle/mlp.c)."""
+    L = lib()
+    params, norm, X, Y = _f(params), _f(norm), _f(X), _f(Y)
+    fp = ctypes.POINTER(ctypes.c_float)
+    g = np.zeros(L.orc_mlp_nparam()) if grad else None
+    loss = np.zeros(1)
+    L.orc_mlp_loss_grad(params.ctypes.data_as(fp), norm.ctypes.data_as(fp), X.ctypes.data_as(fp),
+                        Y.ctypes.data_as(fp), len(Y), 1 if fp16 else 0,
+                        g.ctypes.data_as(_dp) if grad else None, _ptr(loss))
+    return loss[0], g
+
+
+def mlp_predict(params, norm, X, fp16=True):
+    L = lib()
+    params, norm, X = _f(params), _f(norm), _f(X)
+    fp = ctypes.POINTER(ctypes.c_float)
+    out = np.zeros(X.shape[0])
+    L.orc_mlp_predict(params.ctypes.data_as(fp), norm.ctypes.data_as(fp), X.ctypes.data_as(fp), X.shape[0],
+                      1 if fp16 else 0, _ptr(out))
+    return out

@@ -118,6 +118,12 @@ long orc_work_len(const orc_model *md);
    build only; 0 otherwise). */
 double orc_flop_count(void);
 
+/* step-size perceptron (mlp.c): loss and gradient, predictions */
+int  orc_mlp_nparam(void);
+void orc_mlp_loss_grad(const float *params, const float *norm, const float *X, const float *Y, long n,
+                       int fp16, double *grad, double *loss);
+void orc_mlp_predict(const float *params, const float *norm, const float *X, long n, int fp16, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,5 +9,6 @@ from ._lib import (UCG_OKADA_FP64, UCG_OKADA_REF32IO, UCG_PREC_FP64,  # noqa: F4
                    UCG_PREC_SPLIT_BF16)
 from .simulation import Simulation  # noqa: F401
 from .ensemble import Ensemble  # noqa: F401
+from .stepmodel import StepModel  # noqa: F401
 
-__all__ = ["Simulation", "Ensemble", "configs", "UcgError", "load"]
+__all__ = ["Simulation", "Ensemble", "StepModel", "configs", "UcgError", "load"]

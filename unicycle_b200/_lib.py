@@ -28,11 +28,16 @@ UCG_DRIVER_RATESTATE = 0
 UCG_DRIVER_VISCOUSCYCLES = 1
 UCG_ENS_STREAM_K = 0
 UCG_ENS_SPLIT_LPT = 1
+UCG_MLP_NIN = 11
+UCG_MLP_NPARAM = 9153
+UCG_MLP_NNORM = 24
+UCG_TRACE_LEN = 14
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 _lp = ctypes.POINTER(ctypes.c_long)
 _vp = ctypes.c_void_p
+_fp = ctypes.POINTER(ctypes.c_float)
 _i = ctypes.c_int
 _l = ctypes.c_long
 _d = ctypes.c_double
@@ -86,6 +91,18 @@ SIGNATURES = {
     "ucg_ens_info": (_i, [_vp, _lp, _ip, _lp, _lp, _lp, _dp, ctypes.c_char_p, _l]),
     "ucg_ens_stream": (_vp, [_vp]),
     "ucg_ens_profile_contract": (_i, [_vp, _i, _dp]),
+    "ucg_mlp_create": (_i, [ctypes.POINTER(_vp), _i, ctypes.c_ulonglong]),
+    "ucg_mlp_destroy": (None, [_vp]),
+    "ucg_mlp_last_error": (ctypes.c_char_p, [_vp]),
+    "ucg_mlp_set_params": (_i, [_vp, _fp, _fp]),
+    "ucg_mlp_get_params": (_i, [_vp, _fp, _fp]),
+    "ucg_mlp_set_data": (_i, [_vp, _fp, _fp, _l, _i]),
+    "ucg_mlp_gradient": (_i, [_vp, _l, _l, _fp, _dp]),
+    "ucg_mlp_train": (_i, [_vp, _i, _i, ctypes.c_float, ctypes.c_ulonglong, _fp]),
+    "ucg_mlp_predict": (_i, [_vp, _fp, _l, _fp]),
+    "ucg_ens_set_step_model": (_i, [_vp, _vp]),
+    "ucg_ens_record_traces": (_i, [_vp, _l]),
+    "ucg_ens_get_traces": (_i, [_vp, _fp, _l, _lp]),
 }
 
 _lib = None

@@ -281,3 +281,11 @@ def parameter_sets(cfg, n_sets, seed=1000):
         sets.append(fr)
         y0s.append(steady_state(V0, fr))
     return sets, y0s
+
+
+def cfg1_instances(seeds, nx=32, nz=16, size=1250.0):
+    """cfg1 once per seed (the seed draws the lognormal initial slip-rate
+    perturbation; geometry and friction are shared): the config of seed[0] and
+    the initial states of all seeds, for an ensemble."""
+    cfgs = [cfg1(nx=nx, nz=nz, size=size, seed=s) for s in seeds]
+    return cfgs[0], [c["y0"] for c in cfgs]

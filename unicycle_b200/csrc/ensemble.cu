@@ -61,6 +61,7 @@
 #include <vector>
 #include <cuda_bf16.h>
 #include "ucg_internal.cuh"
+#include "mlp.cuh"
 
 namespace ucg {
 namespace ens {
@@ -102,6 +103,11 @@ struct InstCtl {
     int need_stage1, pending, status, active, nonfinite, in_event;
     double t_event;             // start time of the first step with max V >= the event threshold
     long long n_events;         // threshold up-crossings
+    // step-size model inputs (mlp.cuh)
+    double hist[8];             // last accepted steps, most recent first
+    unsigned long long thmin_key;   // min log10 theta at the start of the step (ordered key)
+    int nhist, first_attempt, has_feat, pad2;
+    float feat[mlp::NIN];       // inputs at the last acceptance (for the trace of the next first attempt)
 };
 
 struct EnsGlobal {
@@ -112,7 +118,17 @@ struct EnsGlobal {
     double ev_on, ev_off;       // event thresholds on max V (m/s)
     int active_count;
     int err;                    // UCG_E_TIMEOUT from the contraction
+    // step-size model and trace recording
+    const __half *mlp_P;
+    const mlp::Norm *mlp_N;
+    float *trace;               // records of TRACE_LEN floats
+    unsigned long long trace_cap, trace_n;
 };
+
+// one trace record: the 11 model inputs at an acceptance, then log10 of the
+// next step's first attempt and log10 max(errmax, 1e-12) of that attempt, and
+// 1 if it was accepted
+constexpr int TRACE_LEN = mlp::NIN + 3;
 
 struct GeomDev {
     int np, ninst, mtiles, kblocks;
@@ -555,6 +571,7 @@ __global__ void k_ens_prologue(const EnsArgs *__restrict__ A)
         }
         if (S == 1) {
             atomicMax((unsigned long long *)&c->vmax, (unsigned long long)__double_as_longlong(vel));
+            atomicMin(&c->thmin_key, mlp::ord_key(yy[o + 5]));
             G.v1[2 * pe] = v0;
             G.v1[2 * pe + 1] = v1;
         } else {
@@ -681,6 +698,17 @@ __global__ void k_ens_control(const EnsArgs *__restrict__ A, cudaGraphConditiona
             }
             errmax = errmax / gl->epsilon;
             double h = c->h;
+            if (gl->trace && c->first_attempt && c->has_feat) {
+                const unsigned long long k = atomicAdd(&gl->trace_n, 1ull);
+                if (k < gl->trace_cap) {
+                    float *rec = gl->trace + k * TRACE_LEN;
+                    for (int q = 0; q < mlp::NIN; q++) rec[q] = c->feat[q];
+                    rec[mlp::NIN] = (float)log10(h);
+                    rec[mlp::NIN + 1] = (float)log10(fmax(errmax, 1e-12));
+                    rec[mlp::NIN + 2] = errmax > 1.0 ? 0.0f : 1.0f;
+                }
+            }
+            c->first_attempt = 0;
             if (errmax > 1.0) {
                 h = h * SAFETY * pow(errmax, PSHRNK);
                 if (h < 0.5 * h) h = 0.5 * h;
@@ -698,6 +726,21 @@ __global__ void k_ens_control(const EnsArgs *__restrict__ A, cudaGraphConditiona
                 if (errmax > ERRCON) hnext = SAFETY * h * pow(errmax, PGROW);
                 else hnext = 10.0 * h;
                 if (hnext > gl->hmax) hnext = gl->hmax;
+                // inputs of the step-size model at this acceptance, and its proposal
+                for (int q = 7; q > 0; q--) c->hist[q] = c->hist[q - 1];
+                c->hist[0] = h;
+                c->nhist = c->nhist < 8 ? c->nhist + 1 : 8;
+                c->has_feat = c->nhist >= 8;
+                if (c->has_feat) {
+                    mlp::features(c->vmax, mlp::ord_val(c->thmin_key), c->hist, errmax, c->feat);
+                    if (gl->mlp_P) {
+                        const double hp = pow(10.0, (double)mlp::eval(gl->mlp_P, *gl->mlp_N, c->feat));
+                        hnext = fmin(fmax(hp, 0.2 * h), 10.0 * h);
+                        if (hnext > gl->hmax) hnext = gl->hmax;
+                    }
+                }
+                c->first_attempt = 1;
+                c->thmin_key = ~0ull;
                 // event catalogue: max V at the start of this step against the thresholds
                 if (!c->in_event && c->vmax >= gl->ev_on) {
                     c->in_event = 1;
@@ -1291,6 +1334,7 @@ void ucg_ens_destroy(ucg_ensemble *E)
         for (void *p : ptrs)
             if (p) cudaFree(p);
     }
+    if (E->h_glob && E->h_glob->trace) cudaFree(E->h_glob->trace);
     if (E->d_args) cudaFree(E->d_args);
     if (E->d_glob) cudaFree(E->d_glob);
     if (E->h_glob) cudaFreeHost(E->h_glob);
@@ -1412,6 +1456,7 @@ int ucg_ens_set_state(ucg_ensemble *E, int gi, int inst, double time, const doub
     x.time = time;
     x.need_stage1 = 1;
     x.status = UCG_OK;
+    x.thmin_key = ~0ull;
     ECUDA(cudaMemcpy(g.ctl + inst, &x, sizeof x, cudaMemcpyHostToDevice));
     return UCG_OK;
 }
@@ -1453,6 +1498,7 @@ int ucg_ens_set_states(ucg_ensemble *E, int gi, const double *y, const double *t
         x[i].time = time[i];
         x[i].need_stage1 = 1;
         x[i].status = UCG_OK;
+        x[i].thmin_key = ~0ull;
     }
     ECUDA(cudaMemcpyAsync(g.ctl, x.data(), sizeof(InstCtl) * g.ninst, cudaMemcpyHostToDevice, E->stream));
     ECUDA(cudaStreamSynchronize(E->stream));
@@ -1655,6 +1701,50 @@ int ucg_ens_run(ucg_ensemble *E, double t_end, long max_attempts, long *attempts
     ECUDA(cudaStreamSynchronize(E->stream));
     if (attempts) *attempts = (long)E->h_glob->attempts;
     if (E->h_glob->err) return ebad(E, E->h_glob->err, "contraction: a bounded device wait gave up");
+    return UCG_OK;
+}
+
+int ucg_ens_set_step_model(ucg_ensemble *E, const ucg_mlp *model)
+{
+    if (!E) return UCG_E_BADARG;
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    mlp_device_params(model, &E->h_glob->mlp_P, &E->h_glob->mlp_N);
+    ECUDA(cudaMemcpy(&E->d_glob->mlp_P, &E->h_glob->mlp_P, sizeof(void *) * 2, cudaMemcpyHostToDevice));
+    return UCG_OK;
+}
+
+int ucg_ens_record_traces(ucg_ensemble *E, long capacity)
+{
+    if (!E || capacity < 0) return UCG_E_BADARG;
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    if (E->h_glob->trace) cudaFree(E->h_glob->trace);
+    E->h_glob->trace = nullptr;
+    E->h_glob->trace_cap = 0;
+    E->h_glob->trace_n = 0;
+    if (capacity > 0) {
+        ECUDA(cudaMalloc(&E->h_glob->trace, sizeof(float) * TRACE_LEN * (size_t)capacity));
+        E->h_glob->trace_cap = (unsigned long long)capacity;
+    }
+    ECUDA(cudaMemcpy(&E->d_glob->trace, &E->h_glob->trace, sizeof(float *) + 2 * sizeof(unsigned long long),
+                     cudaMemcpyHostToDevice));
+    return UCG_OK;
+}
+
+int ucg_ens_get_traces(ucg_ensemble *E, float *buf, long max_records, long *n_records)
+{
+    if (!E) return UCG_E_BADARG;
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    unsigned long long n = 0;
+    ECUDA(cudaMemcpy(&n, &E->d_glob->trace_n, sizeof n, cudaMemcpyDeviceToHost));
+    n = std::min(n, E->h_glob->trace_cap);
+    if (n_records) *n_records = (long)n;
+    if (buf && max_records > 0 && E->h_glob->trace) {
+        const unsigned long long k = std::min(n, (unsigned long long)max_records);
+        ECUDA(cudaMemcpy(buf, E->h_glob->trace, sizeof(float) * TRACE_LEN * k, cudaMemcpyDeviceToHost));
+    }
     return UCG_OK;
 }
 

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <string>
 #include <vector>
 #include "../../include/ucg.h"
@@ -124,6 +125,12 @@ bool rk_anchored(const ucg_ctx *c);         // stages contract increments over t
 void rk_drop_graph(ucg_ctx *c);             // before freeing anything the attempt graph reads
 int split_bf16_build(ucg_ctx *c);
 void split_bf16_free(ucg_ctx *c);
+
+// mlp.cu: device addresses of a step-size model's FP16 weights and standardisation
+}  // namespace ucg
+namespace ucg { namespace mlp { struct Norm; } }
+namespace ucg {
+void mlp_device_params(const ucg_mlp *m, const __half **P, const mlp::Norm **N);
 
 // error helper: records the CUDA error text and maps to a status
 int cuda_fail(ucg_ctx *c, cudaError_t e, const char *what);

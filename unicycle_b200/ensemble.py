@@ -139,6 +139,27 @@ class Ensemble:
                     "events")
         return ne.value, tf.value
 
+    def set_step_model(self, model):
+        """Use a StepModel's proposals for every instance (None: the plain controller)."""
+        self._check(self.lib.ucg_ens_set_step_model(self.ens, model.mlp if model is not None else None),
+                    "set_step_model")
+        self._model = model   # keep it alive while in use
+
+    def record_traces(self, capacity):
+        """Start recording step traces (capacity records); 0 stops."""
+        self._check(self.lib.ucg_ens_record_traces(self.ens, int(capacity)), "record_traces")
+
+    def traces(self):
+        """The recorded traces, (n, 14) float32."""
+        from .stepmodel import TRACE_LEN
+        n = ctypes.c_long()
+        self._check(self.lib.ucg_ens_get_traces(self.ens, None, 0, ctypes.byref(n)), "traces")
+        buf = np.empty((n.value, TRACE_LEN), np.float32)
+        if n.value:
+            self._check(self.lib.ucg_ens_get_traces(self.ens, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                    n.value, ctypes.byref(n)), "traces")
+        return buf
+
     def info(self):
         """dict: attempts, active, launches, accepted, rejected, time_sum, plan."""
         ta, act, la = ctypes.c_long(), ctypes.c_int(), ctypes.c_long()
