@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--ens-eager", action="store_true",
                    help="launch the ensemble's attempt kernels from the host instead of one graph launch "
                         "(for ncu, which does not follow conditional graph nodes)")
+    p.add_argument("--no-learned", action="store_true", help="skip the learned step-size leg")
+    p.add_argument("--trace-runs", type=int, default=64, help="seeded cfg1 runs that record training traces")
+    p.add_argument("--trace-attempts", type=int, default=16000, help="attempts of the trace-recording runs")
     p.add_argument("--spinup", type=int, default=20,
                    help="untimed accepted steps (plain) / attempts (ensemble) before warm-up, past the start-up "
                         "transient of the step size")
@@ -352,6 +355,98 @@ def load_tensor_peak():
     return 1590.0, "fallback"
 
 
+def learned_leg(args, local, sim20, sets, y0s, plain_window):
+    """The learned step-size proposal: traces from seeded cfg1 runs train the
+    perceptron on the device; it is then compared with the plain controller on
+    held-out cfg1 seeds (to 15 simulated years) and on the N = 20k ensemble
+    over the same attempt window as the headline run."""
+    import torch
+    import unicycle_b200
+    from unicycle_b200 import configs
+    from unicycle_b200.stepmodel import training_set
+
+    def cuda_time(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+
+    c1, y_train = configs.cfg1_instances(range(100, 100 + args.trace_runs))
+    _, y_test = configs.cfg1_instances(range(200, 216))
+    sim1 = unicycle_b200.Simulation(c1["mu"], c1["lam"], device=local)
+    configs.build(sim1, c1)
+    f1 = c1["friction"]
+
+    def ens1(y0s_, model):
+        e = unicycle_b200.Ensemble(device=local)
+        e.add_geometry(sim1, len(y0s_))
+        for i, y0 in enumerate(y0s_):
+            e.set_friction(0, i, f1["Vpl"], f1["rake"], f1["mu0"], f1["sig"], f1["a"], f1["b"], f1["L"], f1["Vo"],
+                           f1["damping"])
+        e.set_states(0, np.stack(y0s_), 0.0, c1["dt0"])
+        e.set_tolerance(c1["epsilon"])
+        e.set_step_model(model)
+        return e
+
+    tr = ens1(y_train, None)
+    tr.record_traces(int(1.1 * args.trace_runs * args.trace_attempts))
+    _, t_traces = cuda_time(lambda: tr.run(300 * YEAR, args.trace_attempts))
+    traces = tr.traces()
+    tr.close()
+    x, y = training_set(traces)
+    model = unicycle_b200.StepModel(device=local, seed=1)
+    model.set_data(x, y)
+    losses, t_train = cuda_time(lambda: model.train(epochs=20, batch=4096, lr=1e-3))
+    out = {"traces": int(len(traces)), "trace_runs": args.trace_runs, "trace_seconds": t_traces,
+           "train_epochs": 20, "train_seconds": t_train, "loss_first_last": [float(losses[0]), float(losses[-1])]}
+    # held-out cfg1 runs to 15 simulated years
+    t_end = 15 * YEAR
+    held = {}
+    for name, mdl in (("plain", None), ("learned", model)):
+        e = ens1(y_test, mdl)
+        _, secs = cuda_time(lambda: e.run(t_end, 400000))
+        _, t, _, acc, rej, st = e.get_states(0)
+        onsets = np.array([e.events(0, i)[1] for i in range(len(y_test))])
+        held[name] = dict(attempts=int(np.sum(acc + rej)), rejected_fraction=float(np.sum(rej) / np.sum(acc + rej)),
+                          seconds=secs, seconds_per_sim_year=secs / (15.0 * len(y_test)), onsets=onsets)
+        e.close()
+    ok = (held["plain"]["onsets"] > 0) & (held["learned"]["onsets"] > 0)
+    rel = np.abs(held["learned"]["onsets"] - held["plain"]["onsets"])[ok] / held["plain"]["onsets"][ok]
+    for h in held.values():
+        h.pop("onsets")
+    out["held_out_cfg1"] = {"runs": len(y_test), "t_end_years": 15, **{k: v for k, v in held.items()},
+                            "attempt_ratio_plain_over_learned": held["plain"]["attempts"] / held["learned"]["attempts"],
+                            "wallclock_gain_per_sim_year": held["plain"]["seconds"] / held["learned"]["seconds"],
+                            "max_onset_rel_diff": float(rel.max()) if len(rel) else None}
+    sim1.close()
+    # the N = 20k ensemble over the headline's attempt window, same start
+    e = unicycle_b200.Ensemble(device=local)
+    e.add_geometry(sim20, len(sets))
+    for i, fr in enumerate(sets):
+        e.set_friction(0, i, fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
+                       fr["damping"])
+    e.set_states(0, np.stack(y0s), 0.0, configs.cfg2(nx=args.nx, nz=args.nz)["dt0"])
+    e.set_tolerance(1.0e-8)
+    e.set_step_model(model)
+    e.run(1e300, plain_window["before"])
+    i0 = e.info()
+    _, secs = cuda_time(lambda: e.run(1e300, plain_window["attempts"]))
+    i1 = e.info()
+    acc, rej = i1["accepted"] - i0["accepted"], i1["rejected"] - i0["rejected"]
+    syh = (i1["time_sum"] - i0["time_sum"]) / YEAR / (secs / 3600.0)
+    out["megathrust_20k_ensemble"] = {
+        "attempts": plain_window["attempts"], "learned": {"accepted": acc, "rejected_fraction": rej / max(1, acc + rej),
+                                                          "sim_years_per_hour": syh},
+        "plain": {"accepted": plain_window["accepted"],
+                  "rejected_fraction": plain_window["rejected"] / max(1, plain_window["accepted"] +
+                                                                     plain_window["rejected"]),
+                  "sim_years_per_hour": plain_window["sim_years_per_hour"]}}
+    e.close()
+    model.close()
+    return out
+
+
 def run_ensemble(args, world, rank, local):
     """Headline: args.sets frictional parameter sets of the N = 20k model in one
     ensemble, beside the same model as one plain FP64 instance."""
@@ -420,6 +515,12 @@ def run_ensemble(args, world, rank, local):
         acc_e2e += int(acc_h.sum())
     torch.cuda.synchronize()
     e2e_elapsed = reduce_max(time.perf_counter() - t0, world, args)
+    ens.close()
+    learned = None
+    if not args.no_learned and rank == 0:
+        learned = learned_leg(args, local, sim, sets, y0s,
+                              {"before": args.spinup + args.warmup, "attempts": args.steps, "accepted": accepted,
+                               "rejected": rejected, "sim_years_per_hour": sim_years / (elapsed / 3600.0)})
     out = None
     if rank == 0:
         value = world * accepted / elapsed_max
@@ -463,8 +564,8 @@ def run_ensemble(args, world, rank, local):
             "gpu_launches": int(attempts * 20 + 3),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "learned_step": learned,
         }
-    ens.close()
     sim.close()
     return out
 

@@ -678,95 +678,130 @@ __global__ void k_ens_finish(const EnsArgs *__restrict__ A)
     }
 }
 
-// RKQSm decision per instance (ode45.f90:77-106) and the loop condition
-__global__ void k_ens_control(const EnsArgs *__restrict__ A, cudaGraphConditionalHandle cond, int in_graph)
+// RKQSm decision per instance (ode45.f90:77-106) and the loop condition.  With a
+// step-size model, the instances that accepted in this attempt are collected per
+// chunk of blockDim.x instances and each warp evaluates the model for one of
+// them from a shared-memory copy of its weights.
+constexpr int CTL_THREADS = 256;
+
+__global__ void __launch_bounds__(CTL_THREADS) k_ens_control(const EnsArgs *__restrict__ A,
+                                                               cudaGraphConditionalHandle cond, int in_graph)
 {
     EnsGlobal *gl = A->glob;
     const double SAFETY = 0.7, PGROW = -0.2, PSHRNK = -0.15, ERRCON = 1.89e-4;
+    __shared__ __half wt[mlp::NPARAM + 1];
+    __shared__ mlp::Norm norm;
+    __shared__ float feat[CTL_THREADS][mlp::NIN];
+    __shared__ InstCtl *who[CTL_THREADS];
+    __shared__ int nwho;
+    __shared__ int wsum[CTL_THREADS / 32];
+    const bool model = gl->mlp_P != nullptr;
+    if (model) {
+        for (int p = threadIdx.x; p < mlp::NPARAM; p += blockDim.x) wt[p] = gl->mlp_P[p];
+        if (threadIdx.x == 0) norm = *gl->mlp_N;
+    }
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     int live = 0;
     for (int gi = 0; gi < A->ngeom; gi++) {
         const GeomDev &G = A->g[gi];
-        for (int i = threadIdx.x; i < G.ninst; i += blockDim.x) {
-            InstCtl *c = G.ctl + i;
-            if (!inst_live(c, gl)) continue;
-            double errmax = __longlong_as_double((long long)c->errbits);
-            c->errbits = 0ull;
-            if (c->nonfinite) {
-                c->status = UCG_E_NONFINITE;
-                c->active = 0;
-                continue;
-            }
-            errmax = errmax / gl->epsilon;
-            double h = c->h;
-            if (gl->trace && c->first_attempt && c->has_feat) {
-                const unsigned long long k = atomicAdd(&gl->trace_n, 1ull);
-                if (k < gl->trace_cap) {
-                    float *rec = gl->trace + k * TRACE_LEN;
-                    for (int q = 0; q < mlp::NIN; q++) rec[q] = c->feat[q];
-                    rec[mlp::NIN] = (float)log10(h);
-                    rec[mlp::NIN + 1] = (float)log10(fmax(errmax, 1e-12));
-                    rec[mlp::NIN + 2] = errmax > 1.0 ? 0.0f : 1.0f;
-                }
-            }
-            c->first_attempt = 0;
-            if (errmax > 1.0) {
-                h = h * SAFETY * pow(errmax, PSHRNK);
-                if (h < 0.5 * h) h = 0.5 * h;
-                c->h = h;
-                c->rejected += 1;
-                c->need_stage1 = 0;
-                c->pending = 0;
-                if (0.0 + h == 0.0) {
-                    c->status = UCG_E_STEP_UNDERFLOW;
+        for (int base = 0; base < G.ninst; base += blockDim.x) {
+            if (threadIdx.x == 0) nwho = 0;
+            __syncthreads();
+            const int i = base + threadIdx.x;
+            InstCtl *c = i < G.ninst ? G.ctl + i : nullptr;
+            if (c && inst_live(c, gl)) {
+                double errmax = __longlong_as_double((long long)c->errbits);
+                c->errbits = 0ull;
+                if (c->nonfinite) {
+                    c->status = UCG_E_NONFINITE;
                     c->active = 0;
-                    continue;
-                }
-            } else {
-                double hnext;
-                if (errmax > ERRCON) hnext = SAFETY * h * pow(errmax, PGROW);
-                else hnext = 10.0 * h;
-                if (hnext > gl->hmax) hnext = gl->hmax;
-                // inputs of the step-size model at this acceptance, and its proposal
-                for (int q = 7; q > 0; q--) c->hist[q] = c->hist[q - 1];
-                c->hist[0] = h;
-                c->nhist = c->nhist < 8 ? c->nhist + 1 : 8;
-                c->has_feat = c->nhist >= 8;
-                if (c->has_feat) {
-                    mlp::features(c->vmax, mlp::ord_val(c->thmin_key), c->hist, errmax, c->feat);
-                    if (gl->mlp_P) {
-                        const double hp = pow(10.0, (double)mlp::eval(gl->mlp_P, *gl->mlp_N, c->feat));
-                        hnext = fmin(fmax(hp, 0.2 * h), 10.0 * h);
+                } else {
+                    errmax = errmax / gl->epsilon;
+                    double h = c->h;
+                    if (gl->trace && c->first_attempt && c->has_feat) {
+                        const unsigned long long k = atomicAdd(&gl->trace_n, 1ull);
+                        if (k < gl->trace_cap) {
+                            float *rec = gl->trace + k * TRACE_LEN;
+                            for (int q = 0; q < mlp::NIN; q++) rec[q] = c->feat[q];
+                            rec[mlp::NIN] = (float)log10(h);
+                            rec[mlp::NIN + 1] = (float)log10(fmax(errmax, 1e-12));
+                            rec[mlp::NIN + 2] = errmax > 1.0 ? 0.0f : 1.0f;
+                        }
+                    }
+                    c->first_attempt = 0;
+                    if (errmax > 1.0) {
+                        h = h * SAFETY * pow(errmax, PSHRNK);
+                        if (h < 0.5 * h) h = 0.5 * h;
+                        c->h = h;
+                        c->rejected += 1;
+                        c->need_stage1 = 0;
+                        c->pending = 0;
+                        if (0.0 + h == 0.0) {
+                            c->status = UCG_E_STEP_UNDERFLOW;
+                            c->active = 0;
+                        } else {
+                            live++;
+                        }
+                    } else {
+                        double hnext;
+                        if (errmax > ERRCON) hnext = SAFETY * h * pow(errmax, PGROW);
+                        else hnext = 10.0 * h;
                         if (hnext > gl->hmax) hnext = gl->hmax;
+                        // inputs of the step-size model at this acceptance
+                        for (int q = 7; q > 0; q--) c->hist[q] = c->hist[q - 1];
+                        c->hist[0] = h;
+                        c->nhist = c->nhist < 8 ? c->nhist + 1 : 8;
+                        c->has_feat = c->nhist >= 8;
+                        if (c->has_feat) {
+                            mlp::features(c->vmax, mlp::ord_val(c->thmin_key), c->hist, errmax, c->feat);
+                            if (model) {
+                                const int k = atomicAdd(&nwho, 1);
+                                who[k] = c;
+                                for (int q = 0; q < mlp::NIN; q++) feat[k][q] = c->feat[q];
+                            }
+                        }
+                        c->first_attempt = 1;
+                        c->thmin_key = ~0ull;
+                        // event catalogue: max V at the start of this step against the thresholds
+                        if (!c->in_event && c->vmax >= gl->ev_on) {
+                            c->in_event = 1;
+                            if (c->n_events == 0) c->t_event = c->time;
+                            c->n_events += 1;
+                        } else if (c->in_event && c->vmax < gl->ev_off) {
+                            c->in_event = 0;
+                        }
+                        c->hdid = h;
+                        c->time = c->time + h;
+                        c->dt_next = hnext;
+                        c->h = hnext;
+                        c->accepted += 1;
+                        c->pending = 1;
+                        c->vmax = 0.0;
+                        c->need_stage1 = 1;
+                        if (c->time >= gl->t_end) c->active = 0;
+                        else live++;
                     }
                 }
-                c->first_attempt = 1;
-                c->thmin_key = ~0ull;
-                // event catalogue: max V at the start of this step against the thresholds
-                if (!c->in_event && c->vmax >= gl->ev_on) {
-                    c->in_event = 1;
-                    if (c->n_events == 0) c->t_event = c->time;
-                    c->n_events += 1;
-                } else if (c->in_event && c->vmax < gl->ev_off) {
-                    c->in_event = 0;
-                }
-                c->hdid = h;
-                c->time = c->time + h;
-                c->dt_next = hnext;
-                c->h = hnext;
-                c->accepted += 1;
-                c->pending = 1;
-                c->vmax = 0.0;
-                c->need_stage1 = 1;
-                if (c->time >= gl->t_end) {
-                    c->active = 0;
-                    continue;
+            }
+            __syncthreads();
+            // the model's proposals for this chunk's acceptances: one warp each
+            for (int k = warp; k < nwho; k += nwarps) {
+                float x[mlp::NIN];
+                for (int q = 0; q < mlp::NIN; q++) x[q] = feat[k][q];
+                const float lp = mlp::eval_warp(wt, norm, x);
+                if ((threadIdx.x & 31) == 0) {
+                    InstCtl *c = who[k];
+                    const double h = c->hdid;
+                    double hn = fmin(fmax(pow(10.0, (double)lp), 0.2 * h), 10.0 * h);
+                    if (hn > gl->hmax) hn = gl->hmax;
+                    c->h = hn;
+                    c->dt_next = hn;
                 }
             }
-            live++;
+            __syncthreads();
         }
     }
     for (int off = 16; off > 0; off >>= 1) live += __shfl_xor_sync(0xffffffffu, live, off);
-    __shared__ int wsum[32];
     if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = live;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1259,7 +1294,7 @@ int build_graph(ucg_ensemble *E)
             if (le == cudaSuccess) le = enqueue_stage<5>(E, be);
             if (le == cudaSuccess) le = enqueue_stage<6>(E, be);
             k_ens_finish<<<bs, ST_THREADS, 0, E->stream>>>(E->d_args);
-            k_ens_control<<<1, 256, 0, E->stream>>>(E->d_args, cond, 1);
+            k_ens_control<<<1, CTL_THREADS, 0, E->stream>>>(E->d_args, cond, 1);
             E->launches += 2;
             cudaGraph_t tmp;
             e = cudaStreamEndCapture(E->stream, &tmp);
@@ -1645,7 +1680,7 @@ int run_eager(ucg_ensemble *E)
         if (le == cudaSuccess) le = enqueue_stage<6>(E, be);
         if (le != cudaSuccess) return efail(E, le, "ensemble attempt");
         k_ens_finish<<<bs, ST_THREADS, 0, E->stream>>>(E->d_args);
-        k_ens_control<<<1, 256, 0, E->stream>>>(E->d_args, 0, 0);
+        k_ens_control<<<1, CTL_THREADS, 0, E->stream>>>(E->d_args, 0, 0);
         E->launches += 2;
         if ((a & 15) == 15 || a + 1 == E->h_glob->budget) {
             EnsGlobal g;

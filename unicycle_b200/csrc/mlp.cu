@@ -11,8 +11,8 @@
 //                 FP32 gradient with one atomic per weight and CTA.
 //   k_mlp_adam    Adam on the FP32 master weights, refreshes the FP16 copy and
 //                 clears the gradient.
-//   k_mlp_predict the controllers' own single-sample evaluation (mlp::eval),
-//                 one thread per sample.
+//   k_mlp_predict the controllers' own single-sample evaluation
+//                 (mlp::eval_warp), one warp per sample.
 //
 // Loss: 0.5 (y_hat - label_hat)^2 averaged over the batch, in standardised
 // units.  Training data are the integrator's own traces (ensemble.cu records
@@ -166,14 +166,23 @@ __global__ void k_mlp_to_half(const float *__restrict__ W, __half *__restrict__ 
     if (p < NPARAM) P[p] = __float2half(W[p]);
 }
 
+// FP16 weights in the inference layout (transposed hidden blocks)
+__global__ void k_mlp_inference_copy(const __half *__restrict__ P, __half *__restrict__ T)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < NPARAM) T[to_inference_index(p)] = P[p];
+}
+
+// one warp per sample, the controllers' evaluation
 __global__ void k_mlp_predict(const __half *__restrict__ P, const Norm *__restrict__ Nn, const float *__restrict__ X,
                               long n, float *__restrict__ Y)
 {
-    const long j = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long j = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
     if (j >= n) return;
     float x[NIN];
     for (int i = 0; i < NIN; i++) x[i] = X[j * NIN + i];
-    Y[j] = eval(P, *Nn, x);
+    const float y = eval_warp(P, *Nn, x);
+    if ((threadIdx.x & 31) == 0) Y[j] = y;
 }
 
 }  // namespace mlp
@@ -188,6 +197,7 @@ struct ucg_mlp {
     std::string err;
     float *W = nullptr, *M = nullptr, *V = nullptr, *G = nullptr;   // FP32 master, Adam moments, gradient
     __half *P = nullptr;                                            // FP16 weights the kernels use
+    __half *T = nullptr;                                            // the same, inference layout
     Norm *norm = nullptr;                                           // device
     Norm hnorm{};
     double *loss = nullptr;
@@ -242,6 +252,7 @@ int ucg_mlp_create(ucg_mlp **out, int device, unsigned long long seed)
     for (float **p : f32)
         if (e == cudaSuccess) e = cudaMalloc(p, sizeof(float) * NPARAM);
     if (e == cudaSuccess) e = cudaMalloc(&m->P, sizeof(__half) * NPARAM);
+    if (e == cudaSuccess) e = cudaMalloc(&m->T, sizeof(__half) * NPARAM);
     if (e == cudaSuccess) e = cudaMalloc(&m->norm, sizeof(Norm));
     if (e == cudaSuccess) e = cudaMalloc(&m->loss, sizeof(double));
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -270,6 +281,7 @@ int ucg_mlp_create(ucg_mlp **out, int device, unsigned long long seed)
     cudaMemset(m->G, 0, sizeof(float) * NPARAM);
     cudaMemcpy(m->norm, &m->hnorm, sizeof(Norm), cudaMemcpyHostToDevice);
     k_mlp_to_half<<<(NPARAM + 255) / 256, 256, 0, m->stream>>>(m->W, m->P);
+    k_mlp_inference_copy<<<(NPARAM + 255) / 256, 256, 0, m->stream>>>(m->P, m->T);
     cudaStreamSynchronize(m->stream);
     *out = m;
     return UCG_OK;
@@ -280,7 +292,7 @@ void ucg_mlp_destroy(ucg_mlp *m)
     if (!m) return;
     cudaSetDevice(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
-    void *ptrs[] = {m->W, m->M, m->V, m->G, m->P, m->norm, m->loss, m->X, m->Y, m->idx};
+    void *ptrs[] = {m->W, m->M, m->V, m->G, m->P, m->T, m->norm, m->loss, m->X, m->Y, m->idx};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -297,6 +309,7 @@ int ucg_mlp_set_params(ucg_mlp *m, const float *params, const float *norm)
     if (params) {
         MCUDA(cudaMemcpy(m->W, params, sizeof(float) * NPARAM, cudaMemcpyHostToDevice));
         k_mlp_to_half<<<(NPARAM + 255) / 256, 256, 0, m->stream>>>(m->W, m->P);
+        k_mlp_inference_copy<<<(NPARAM + 255) / 256, 256, 0, m->stream>>>(m->P, m->T);
         MCUDA(cudaGetLastError());
         MCUDA(cudaMemset(m->M, 0, sizeof(float) * NPARAM));
         MCUDA(cudaMemset(m->V, 0, sizeof(float) * NPARAM));
@@ -427,6 +440,9 @@ int ucg_mlp_train(ucg_mlp *m, int epochs, int batch, float lr, unsigned long lon
         MCUDA(cudaStreamSynchronize(m->stream));
         if (epoch_loss) epoch_loss[ep] = (float)(l / m->n);
     }
+    k_mlp_inference_copy<<<(NPARAM + 255) / 256, 256, 0, m->stream>>>(m->P, m->T);
+    MCUDA(cudaGetLastError());
+    MCUDA(cudaStreamSynchronize(m->stream));
     return UCG_OK;
 }
 
@@ -439,7 +455,7 @@ int ucg_mlp_predict(ucg_mlp *m, const float *x, long n, float *y)
     cudaError_t e = cudaMalloc(&dy, sizeof(float) * n);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dx, x, sizeof(float) * NIN * n, cudaMemcpyHostToDevice, m->stream);
     if (e == cudaSuccess) {
-        k_mlp_predict<<<(unsigned)((n + 127) / 128), 128, 0, m->stream>>>(m->P, m->norm, dx, n, dy);
+        k_mlp_predict<<<(unsigned)((n + 3) / 4), 128, 0, m->stream>>>(m->T, m->norm, dx, n, dy);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(y, dy, sizeof(float) * n, cudaMemcpyDeviceToHost, m->stream);
@@ -455,7 +471,7 @@ namespace ucg {
 // device addresses of a model's FP16 weights and standardisation, for the controllers
 void mlp_device_params(const ucg_mlp *m, const __half **P, const mlp::Norm **N)
 {
-    *P = m ? m->P : nullptr;
+    *P = m ? m->T : nullptr;
     *N = m ? m->norm : nullptr;
 }
 }  // namespace ucg

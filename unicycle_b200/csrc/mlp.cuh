@@ -39,31 +39,52 @@ __host__ __device__ inline float gelu_df(float z)
     return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
-// one sample, one thread: log10 of the proposed step from raw inputs
-__device__ inline float eval(const __half *__restrict__ P, const Norm &N, const float x[NIN])
+// Inference layout: the same blocks with W1, W2, W3 transposed ([in][out]),
+// so that the 32 lanes of a warp read 32 consecutive outputs' weights.
+__host__ __device__ inline int to_inference_index(int p)
 {
+    if (p < OFF_B1) return OFF_W1 + (p % NIN) * NH + p / NIN;
+    if (p >= OFF_W2 && p < OFF_B2) return OFF_W2 + ((p - OFF_W2) % NH) * NH + (p - OFF_W2) / NH;
+    if (p >= OFF_W3 && p < OFF_B3) return OFF_W3 + ((p - OFF_W3) % NH) * NH + (p - OFF_W3) / NH;
+    return p;
+}
+
+// One sample, one warp, weights T in the inference layout (global or shared
+// memory): lane l owns outputs l and l + 32 of every hidden layer, activations
+// travel by shuffles; each output's sum runs over its inputs in order, the last
+// layer's dot product is reduced across the warp.
+__device__ inline float eval_warp(const __half *T, const Norm &N, const float x[NIN])
+{
+    const int l = threadIdx.x & 31;
     float a0[NIN];
 #pragma unroll
     for (int i = 0; i < NIN; i++) a0[i] = __half2float(__float2half((x[i] - N.xm[i]) / N.xs[i]));
-    float a1[NH], a2[NH];
-    for (int o = 0; o < NH; o++) {
-        float z = __half2float(P[OFF_B1 + o]);
+    float lo, hi;
+    {
+        float z0 = __half2float(T[OFF_B1 + l]), z1 = __half2float(T[OFF_B1 + l + 32]);
 #pragma unroll
-        for (int i = 0; i < NIN; i++) z += __half2float(P[OFF_W1 + o * NIN + i]) * a0[i];
-        a1[o] = __half2float(__float2half(gelu_f(z)));
+        for (int i = 0; i < NIN; i++) {
+            z0 += __half2float(T[OFF_W1 + i * NH + l]) * a0[i];
+            z1 += __half2float(T[OFF_W1 + i * NH + l + 32]) * a0[i];
+        }
+        lo = __half2float(__float2half(gelu_f(z0)));
+        hi = __half2float(__float2half(gelu_f(z1)));
     }
-    for (int o = 0; o < NH; o++) {
-        float z = __half2float(P[OFF_B2 + o]);
-        for (int i = 0; i < NH; i++) z += __half2float(P[OFF_W2 + o * NH + i]) * a1[i];
-        a2[o] = __half2float(__float2half(gelu_f(z)));
+#pragma unroll
+    for (int layer = 0; layer < 2; layer++) {
+        const int ow = layer == 0 ? OFF_W2 : OFF_W3, ob = layer == 0 ? OFF_B2 : OFF_B3;
+        float z0 = __half2float(T[ob + l]), z1 = __half2float(T[ob + l + 32]);
+        for (int i = 0; i < NH; i++) {
+            const float a = __shfl_sync(0xffffffffu, i < 32 ? lo : hi, i & 31);
+            z0 += __half2float(T[ow + i * NH + l]) * a;
+            z1 += __half2float(T[ow + i * NH + l + 32]) * a;
+        }
+        lo = __half2float(__float2half(gelu_f(z0)));
+        hi = __half2float(__float2half(gelu_f(z1)));
     }
-    float out = __half2float(P[OFF_B4]);
-    for (int o = 0; o < NH; o++) {
-        float z = __half2float(P[OFF_B3 + o]);
-        for (int i = 0; i < NH; i++) z += __half2float(P[OFF_W3 + o * NH + i]) * a2[i];
-        out += __half2float(P[OFF_W4 + o]) * __half2float(__float2half(gelu_f(z)));
-    }
-    return out * N.ys + N.ym;
+    float out = __half2float(T[OFF_W4 + l]) * lo + __half2float(T[OFF_W4 + l + 32]) * hi;
+    for (int off = 16; off > 0; off >>= 1) out += __shfl_xor_sync(0xffffffffu, out, off);
+    return (out + __half2float(T[OFF_B4])) * N.ys + N.ym;
 }
 
 // feature vector from the controller's state at an accepted step
