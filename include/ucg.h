@@ -276,8 +276,10 @@ int ucg_ens_run(ucg_ensemble *ens, double t_end, long max_attempts, long *attemp
 
 /* T = K V through the tensor-core contraction for one geometry: V is
    instance-major (n_instances x n source DOFs), T instance-major
-   (n_instances x m receiver DOFs), host arrays. */
-int ucg_ens_matvec(ucg_ensemble *ens, int geometry, const double *V, double *T);
+   (n_instances x m receiver DOFs), host arrays.  terms = 3: Khi Vhi + Khi Vlo +
+   Klo Vhi (the stage-1 anchor's product); terms = 2: Khi Vhi + Khi Vlo (the
+   stage increments' product, half the matrix bytes). */
+int ucg_ens_matvec(ucg_ensemble *ens, int geometry, const double *V, double *T, int terms);
 
 /* Event catalogue per instance: an event starts at the first accepted step
    whose starting max slip rate is >= vmax_on and ends once it is < vmax_off
@@ -297,8 +299,10 @@ int ucg_ens_info(ucg_ensemble *ens, long *total_attempts, int *active, long *lau
 /* The ensemble's CUDA stream (a cudaStream_t), for callers' events. */
 void *ucg_ens_stream(ucg_ensemble *ens);
 
-/* Mean device time of one contraction launch over `reps` launches. */
-int ucg_ens_profile_contract(ucg_ensemble *ens, int reps, double *ms);
+/* Mean device time of one contraction launch over `reps` launches, for the
+   anchor's (three-term) and the increments' (two-term) form; either pointer
+   may be NULL. */
+int ucg_ens_profile_contract(ucg_ensemble *ens, int reps, double *ms_anchor, double *ms_increment);
 
 /* ---- learned step-size proposal ------------------------------------------- */
 

@@ -67,6 +67,11 @@ def test_contraction_matches_fp64(ucg):
         T = ens.matvec(gi, V)
         worst.append(_check_contraction(K, V, T))
     print("max |T - KV| / (|K||V|):", worst)
+    # the increments' form reads K hi only: error up to the bf16 unit roundoff 2^-8
+    K = sims[0].copy_G()
+    V = rng.standard_normal((len(cfg["geoms"][0]["sets"]), K.shape[1]))
+    r2 = _check_contraction(K, V, ens.matvec(0, V, terms=2), bound=5e-3)
+    print("two-term form: max |T - KV| / (|K||V|):", r2)
     for s in sims:
         s.close()
     ens.close()

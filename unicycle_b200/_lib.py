@@ -85,12 +85,12 @@ SIGNATURES = {
     "ucg_ens_tune": (_i, [_vp, _i, ctypes.c_char_p, _l]),
     "ucg_ens_use_graph": (_i, [_vp, _i]),
     "ucg_ens_run": (_i, [_vp, _d, _l, _lp]),
-    "ucg_ens_matvec": (_i, [_vp, _i, _dp, _dp]),
+    "ucg_ens_matvec": (_i, [_vp, _i, _dp, _dp, _i]),
     "ucg_ens_set_event_threshold": (_i, [_vp, _d, _d]),
     "ucg_ens_get_events": (_i, [_vp, _i, _i, _lp, _dp]),
     "ucg_ens_info": (_i, [_vp, _lp, _ip, _lp, _lp, _lp, _dp, ctypes.c_char_p, _l]),
     "ucg_ens_stream": (_vp, [_vp]),
-    "ucg_ens_profile_contract": (_i, [_vp, _i, _dp]),
+    "ucg_ens_profile_contract": (_i, [_vp, _i, _dp, _dp]),
     "ucg_mlp_create": (_i, [ctypes.POINTER(_vp), _i, ctypes.c_ulonglong]),
     "ucg_mlp_destroy": (None, [_vp]),
     "ucg_mlp_last_error": (ctypes.c_char_p, [_vp]),

@@ -75,12 +75,15 @@ constexpr int EW_THREADS = 128;         // element-wise kernels: elements per bl
 constexpr int ST_THREADS = 256;         // finish kernel: state entries per block
 constexpr unsigned long long TIMEOUT_NS = 4000000000ull;
 
-template <int NI>
+// KLO: the stage also reads the K lo image (three MMAs per k-step); without it
+// (stage increments) only the hi image is read and two MMAs run, Khi Vhi + Khi Vlo
+template <int NI, bool KLO>
 struct Tile {
     static constexpr int B_HALF = NI * BK * 2;
     static constexpr int B_IMG = 2 * B_HALF;
-    static constexpr int STAGE = A_IMG + B_IMG;
-    static constexpr int STAGES = NI <= 64 ? 4 : 3;
+    static constexpr int A_BYTES = KLO ? A_IMG : A_HALF;
+    static constexpr int STAGE = A_BYTES + B_IMG;
+    static constexpr int STAGES = (6 * 32768) / STAGE < 8 ? (6 * 32768) / STAGE : 8;   // ~192 KB in flight
     static constexpr int SMEM = STAGES * STAGE + 1024;   // + slack for 1024-byte alignment
     static constexpr uint32_t TMEM_COLS = 2 * NI;         // two FP32 accumulators of NI columns
     // instruction descriptor: F32 accumulator, bf16 A and B, both K-major,
@@ -237,11 +240,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16])
 
 // ---- the contraction ---------------------------------------------------------------
 
-template <int NI>
+template <int NI, bool KLO>
 __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__restrict__ tiles,
         const GemmSeg *__restrict__ segs, const int *__restrict__ cta_seg, float *__restrict__ ws, int *err)
 {
-    using T = Tile<NI>;
+    using T = Tile<NI, KLO>;
     extern __shared__ unsigned char dyn_smem[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dyn_smem) + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full[T::STAGES], empty[T::STAGES], acc_full[2], acc_empty[2], drain;
@@ -293,9 +296,9 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                         break;
                     }
                     uint8_t *st = smem + (size_t)s * T::STAGE;
-                    bar_expect_tx(&full[s], (uint32_t)(A_IMG + T::B_IMG));
-                    bulk_load(st, tl.a + (size_t)kb * A_IMG, A_IMG, &full[s]);
-                    bulk_load(st + A_IMG, tl.b + (size_t)kb * T::B_IMG, T::B_IMG, &full[s]);
+                    bar_expect_tx(&full[s], (uint32_t)(T::A_BYTES + T::B_IMG));
+                    bulk_load(st, tl.a + (size_t)kb * A_IMG, T::A_BYTES, &full[s]);
+                    bulk_load(st + T::A_BYTES, tl.b + (size_t)kb * T::B_IMG, T::B_IMG, &full[s]);
                     issued++;
                 }
             }
@@ -329,14 +332,14 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                     }
                     tc_fence_after();
                     const uint32_t a = s_addr(smem + (size_t)s * T::STAGE);
-                    const uint32_t b = a + A_IMG;
+                    const uint32_t b = a + T::A_BYTES;
 #pragma unroll
                     for (int j = 0; j < BK / 16; j++) {
-                        const uint64_t ahi = sw128_desc(a + 32u * j), alo = sw128_desc(a + A_HALF + 32u * j);
+                        const uint64_t ahi = sw128_desc(a + 32u * j);
                         const uint64_t bhi = sw128_desc(b + 32u * j), blo = sw128_desc(b + T::B_HALF + 32u * j);
                         mma_bf16(d, ahi, bhi, T::IDESC, (kb > sg.kb0 || j > 0) ? 1u : 0u);
                         mma_bf16(d, ahi, blo, T::IDESC, 1u);
-                        mma_bf16(d, alo, bhi, T::IDESC, 1u);
+                        if (KLO) mma_bf16(d, sw128_desc(a + A_HALF + 32u * j), bhi, T::IDESC, 1u);
                     }
                     issued_any = true;
                     mma_commit(&empty[s]);   // frees the stage once these MMAs have read it
@@ -541,46 +544,62 @@ __global__ void k_ens_prologue(const EnsArgs *__restrict__ A)
     const int local = blockIdx.x - G.blk_e0;
     const int i = local / G.epb_e;
     const int e = (local % G.epb_e) * EW_THREADS + threadIdx.x;
-    if (i >= G.ninst || e >= G.np) return;
+    if (i >= G.ninst) return;                        // uniform over the block
+    const bool valid = e < G.np;
     InstCtl *c = G.ctl + i;
-    const long o = (long)i * 7 * G.np + 7L * e;
-    if (S == 1 && c->pending)
-        for (int q = 0; q < 7; q++) G.y[o + q] = G.ycand[o + q];
-    double v0 = 0.0, v1 = 0.0;
-    if (inst_live(c, A->glob) && !(S == 1 && !c->need_stage1)) {
-        const double h = c->h;
-        if (S > 1) {
-            for (int q = 0; q < 7; q++) G.ys[o + q] = ens_comb<S>(G, o + q, h);
-            if (S == 2 && c->need_stage1)
-                for (int q = 0; q < 7; q++)
-                    G.yscal[o + q] = fabs(G.y[o + q]) + fabs(h * G.k[0][o + q]) + 1.0e-30;
+    unsigned long long vkey = 0ull, tkey = ~0ull;   // max V and min log10 theta of this element (stage 1)
+    if (valid) {
+        const long o = (long)i * 7 * G.np + 7L * e;
+        if (S == 1 && c->pending)
+            for (int q = 0; q < 7; q++) G.y[o + q] = G.ycand[o + q];
+        double v0 = 0.0, v1 = 0.0;
+        if (inst_live(c, A->glob) && !(S == 1 && !c->need_stage1)) {
+            const double h = c->h;
+            if (S > 1) {
+                for (int q = 0; q < 7; q++) G.ys[o + q] = ens_comb<S>(G, o + q, h);
+                if (S == 2 && c->need_stage1)
+                    for (int q = 0; q < 7; q++)
+                        G.yscal[o + q] = fabs(G.y[o + q]) + fabs(h * G.k[0][o + q]) + 1.0e-30;
+            }
+            const double *yy = (S == 1) ? G.y : G.ys;
+            const double rake = atan2(yy[o + 3], yy[o + 2]);
+            const double vel = exp(yy[o + 6] * E_LG10);
+            const double vs = vel * cos(rake), vd = vel * sin(rake);
+            double *ks = G.k[S - 1];
+            ks[o + 0] = vs;
+            ks[o + 1] = vd;
+            const long pe = (long)i * G.np + e;
+            v0 = vs - G.vpl_c[pe];
+            v1 = vd - G.vpl_s[pe];
+            if (!isfinite(vel) || !isfinite(rake)) {
+                c->nonfinite = 1;
+                v0 = v1 = 0.0;
+            }
+            if (S == 1) {
+                vkey = (unsigned long long)__double_as_longlong(vel);
+                tkey = mlp::ord_key(yy[o + 5]);
+                G.v1[2 * pe] = v0;
+                G.v1[2 * pe + 1] = v1;
+            } else {
+                // increment over the stage-1 anchor
+                v0 = v0 - G.v1[2 * pe];
+                v1 = v1 - G.v1[2 * pe + 1];
+            }
         }
-        const double *yy = (S == 1) ? G.y : G.ys;
-        const double rake = atan2(yy[o + 3], yy[o + 2]);
-        const double vel = exp(yy[o + 6] * E_LG10);
-        const double vs = vel * cos(rake), vd = vel * sin(rake);
-        double *ks = G.k[S - 1];
-        ks[o + 0] = vs;
-        ks[o + 1] = vd;
-        const long pe = (long)i * G.np + e;
-        v0 = vs - G.vpl_c[pe];
-        v1 = vd - G.vpl_s[pe];
-        if (!isfinite(vel) || !isfinite(rake)) {
-            c->nonfinite = 1;
-            v0 = v1 = 0.0;
+        put_v(G.B, A->ni, G.kblocks, i, 2L * e, v0, v1);
+    }
+    if (S == 1) {
+        // the block's elements belong to one instance: reduce over the warp,
+        // one atomic per warp (identity values on lanes past the last element)
+        for (int off = 16; off > 0; off >>= 1) {
+            vkey = max(vkey, __shfl_xor_sync(0xffffffffu, vkey, off));
+            tkey = min(tkey, __shfl_xor_sync(0xffffffffu, tkey, off));
         }
-        if (S == 1) {
-            atomicMax((unsigned long long *)&c->vmax, (unsigned long long)__double_as_longlong(vel));
-            atomicMin(&c->thmin_key, mlp::ord_key(yy[o + 5]));
-            G.v1[2 * pe] = v0;
-            G.v1[2 * pe + 1] = v1;
-        } else {
-            // increment over the stage-1 anchor
-            v0 = v0 - G.v1[2 * pe];
-            v1 = v1 - G.v1[2 * pe + 1];
+        if ((threadIdx.x & 31) == 0) {
+            if (vkey) atomicMax((unsigned long long *)&c->vmax, vkey);
+            if (tkey != ~0ull) atomicMin(&c->thmin_key, tkey);
         }
     }
-    put_v(G.B, A->ni, G.kblocks, i, 2L * e, v0, v1);
 }
 
 // traction rates from the contraction and the rate-state right-hand side
@@ -1037,7 +1056,11 @@ size_t b_bytes(const EnsGeomHost &g, int ni)
 template <int NI>
 cudaError_t prepare_contract_t()
 {
-    return cudaFuncSetAttribute(k_bf16x3_contract<NI>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tile<NI>::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(k_bf16x3_contract<NI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Tile<NI, true>::SMEM);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_bf16x3_contract<NI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Tile<NI, false>::SMEM);
 }
 
 cudaError_t prepare_contract(int ni)
@@ -1050,21 +1073,23 @@ cudaError_t prepare_contract(int ni)
     }
 }
 
-template <int NI>
+template <int NI, bool KLO>
 cudaError_t launch_contract_t(ucg_ensemble *E)
 {
-    k_bf16x3_contract<NI><<<E->sms, 192, Tile<NI>::SMEM, E->stream>>>(E->d_tiles, E->d_segs, E->d_cta, E->ws,
-                                                                      &E->d_glob->err);
+    k_bf16x3_contract<NI, KLO><<<E->sms, 192, Tile<NI, KLO>::SMEM, E->stream>>>(E->d_tiles, E->d_segs, E->d_cta,
+                                                                                E->ws, &E->d_glob->err);
     E->launches++;
     return cudaGetLastError();
 }
 
-cudaError_t launch_contract(ucg_ensemble *E)
+// klo: also read the K lo image (the stage-1 anchor); without it the stage
+// increments' product Khi (Vhi + Vlo)
+cudaError_t launch_contract(ucg_ensemble *E, bool klo = true)
 {
     switch (E->ni) {
-    case 32: return launch_contract_t<32>(E);
-    case 64: return launch_contract_t<64>(E);
-    case 128: return launch_contract_t<128>(E);
+    case 32: return klo ? launch_contract_t<32, true>(E) : launch_contract_t<32, false>(E);
+    case 64: return klo ? launch_contract_t<64, true>(E) : launch_contract_t<64, false>(E);
+    case 128: return klo ? launch_contract_t<128, true>(E) : launch_contract_t<128, false>(E);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1215,16 +1240,16 @@ int ensure_plan(ucg_ensemble *E)
 
 // mean device time per launch: the best of three trials of `reps` launches, so
 // that a host-side stall between launches does not decide a plan
-int time_contract(ucg_ensemble *E, int reps, double *ms)
+int time_contract(ucg_ensemble *E, int reps, double *ms, bool klo = true)
 {
     cudaEvent_t a, b;
     ECUDA(cudaEventCreate(&a));
     ECUDA(cudaEventCreate(&b));
-    for (int w = 0; w < 2; w++) ECUDA(launch_contract(E));
+    for (int w = 0; w < 2; w++) ECUDA(launch_contract(E, klo));
     double best = 1e300;
     for (int trial = 0; trial < 3; trial++) {
         ECUDA(cudaEventRecord(a, E->stream));
-        for (int r = 0; r < reps; r++) ECUDA(launch_contract(E));
+        for (int r = 0; r < reps; r++) ECUDA(launch_contract(E, klo));
         ECUDA(cudaEventRecord(b, E->stream));
         ECUDA(cudaEventSynchronize(b));
         float t = 0.0f;
@@ -1245,7 +1270,7 @@ template <int S>
 cudaError_t enqueue_stage(ucg_ensemble *E, int be)
 {
     k_ens_prologue<S><<<be, EW_THREADS, 0, E->stream>>>(E->d_args);
-    cudaError_t e = launch_contract(E);
+    cudaError_t e = launch_contract(E, S == 1);
     if (e != cudaSuccess) return e;
     k_ens_rhs<S><<<be, EW_THREADS, 0, E->stream>>>(E->d_args);
     E->launches += 2;
@@ -1598,12 +1623,16 @@ int ucg_ens_tune(ucg_ensemble *E, int reps, char *report, long report_len)
                                                         : sched_split_lpt(tkb, E->sms, cd.chunk, 2);
             int st = install_plan(E, ni, s);
             if (st) return st;
-            double ms = 0.0;
-            st = time_contract(E, reps, &ms);
+            // one attempt contracts the anchor once (hi + lo) and five increments (hi)
+            double ms_full = 0.0, ms_hi = 0.0;
+            st = time_contract(E, reps, &ms_full, true);
+            if (!st) st = time_contract(E, reps, &ms_hi, false);
             if (st) return st;
-            char line[160];
-            snprintf(line, sizeof line, "ni=%d %-16s segments=%-5d predicted=%-6ld k-blocks  %.4f ms\n", ni,
-                     s.name.c_str(), (int)s.segs.size(), sched_cost(s, 2), ms);
+            const double ms = ms_full + 5.0 * ms_hi;
+            char line[200];
+            snprintf(line, sizeof line,
+                     "ni=%d %-16s segments=%-5d predicted=%-6ld k-blocks  anchor %.4f ms  increment %.4f ms  "
+                     "attempt %.4f ms\n", ni, s.name.c_str(), (int)s.segs.size(), sched_cost(s, 2), ms_full, ms_hi, ms);
             rep += line;
             if (ms < best) {
                 best = ms;
@@ -1624,10 +1653,11 @@ int ucg_ens_tune(ucg_ensemble *E, int reps, char *report, long report_len)
     return UCG_OK;
 }
 
-int ucg_ens_matvec(ucg_ensemble *E, int gi, const double *V, double *T)
+int ucg_ens_matvec(ucg_ensemble *E, int gi, const double *V, double *T, int terms)
 {
     if (!E || gi < 0 || gi >= (int)(E ? E->geoms.size() : 0)) return UCG_E_BADARG;
     if (!V || !T) return ebad(E, UCG_E_BADARG, "null array");
+    if (terms != 2 && terms != 3) return ebad(E, UCG_E_BADARG, "terms must be 2 or 3");
     ECUDA(cudaSetDevice(E->device));
     int st = ensure_plan(E);
     if (st) return st;
@@ -1641,7 +1671,7 @@ int ucg_ens_matvec(ucg_ensemble *E, int gi, const double *V, double *T)
         k_pack_v_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(g.B, E->ni, g.kblocks, g.ninst, g.n, dV);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = launch_contract(E);
+    if (e == cudaSuccess) e = launch_contract(E, terms == 3);
     if (e == cudaSuccess) {
         const long work = (long)g.ninst * g.m;
         k_reduce_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(E->d_args, gi, dT);
@@ -1842,13 +1872,15 @@ int ucg_ens_info(ucg_ensemble *E, long *total_attempts, int *active, long *launc
 
 void *ucg_ens_stream(ucg_ensemble *E) { return E ? (void *)E->stream : nullptr; }
 
-int ucg_ens_profile_contract(ucg_ensemble *E, int reps, double *ms)
+int ucg_ens_profile_contract(ucg_ensemble *E, int reps, double *ms_anchor, double *ms_increment)
 {
-    if (!E || !ms || reps < 1) return UCG_E_BADARG;
+    if (!E || reps < 1) return UCG_E_BADARG;
     ECUDA(cudaSetDevice(E->device));
     int st = ensure_plan(E);
     if (st) return st;
-    return time_contract(E, reps, ms);
+    if (ms_anchor && (st = time_contract(E, reps, ms_anchor, true))) return st;
+    if (ms_increment && (st = time_contract(E, reps, ms_increment, false))) return st;
+    return UCG_OK;
 }
 
 }  // extern "C"

@@ -121,12 +121,13 @@ class Ensemble:
         self._check(self.lib.ucg_ens_run(self.ens, t_end, max_attempts, ctypes.byref(n)), "run")
         return n.value
 
-    def matvec(self, geometry, V):
-        """T = K V through the tensor-core contraction; V: (n_instances, n) -> (n_instances, m)."""
+    def matvec(self, geometry, V, terms=3):
+        """T = K V through the tensor-core contraction; V: (n_instances, n) -> (n_instances, m).
+        terms=3: the anchor's product (K hi and lo), terms=2: the increments' (K hi only)."""
         _, ninst, n, m = self.geoms[geometry]
         V = _d(V).reshape(ninst, n)
         T = np.empty((ninst, m))
-        self._check(self.lib.ucg_ens_matvec(self.ens, geometry, _p(V), _p(T)), "matvec")
+        self._check(self.lib.ucg_ens_matvec(self.ens, geometry, _p(V), _p(T), int(terms)), "matvec")
         return T
 
     def set_event_threshold(self, vmax_on=1.0e-3, vmax_off=1.0e-4):
@@ -177,6 +178,8 @@ class Ensemble:
         return self.lib.ucg_ens_stream(self.ens)
 
     def profile_contract(self, reps=10):
-        ms = ctypes.c_double()
-        self._check(self.lib.ucg_ens_profile_contract(self.ens, reps, ctypes.byref(ms)), "profile_contract")
-        return ms.value
+        """Mean device ms per launch: (anchor form, increment form)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.ucg_ens_profile_contract(self.ens, reps, ctypes.byref(a), ctypes.byref(b)),
+                    "profile_contract")
+        return a.value, b.value
