@@ -48,7 +48,9 @@ def parse():
     p.add_argument("--nx", type=int, default=100, help="along-strike cells (2 triangles each per row)")
     p.add_argument("--nz", type=int, default=100, help="down-dip rows")
     p.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16"])
-    p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split"])
+    p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split", "coupled"])
+    p.add_argument("--coupled-size", default="64,64,16,8,8",
+                   help="coupled assembly leg: fault nx,nz and volume nx,ny,nz")
     p.add_argument("--sets", type=int, default=N_SETS, help="instances in the ensemble workload")
     p.add_argument("--ens-eager", action="store_true",
                    help="launch the ensemble's attempt kernels from the host instead of one graph launch "
@@ -56,6 +58,8 @@ def parse():
     p.add_argument("--no-learned", action="store_true", help="skip the learned step-size leg")
     p.add_argument("--trace-runs", type=int, default=64, help="seeded cfg1 runs that record training traces")
     p.add_argument("--trace-attempts", type=int, default=16000, help="attempts of the trace-recording runs")
+    p.add_argument("--learned-eval-years", type=float, default=15.0,
+                   help="simulated years of the held-out comparison (0: train only, no comparison)")
     p.add_argument("--spinup", type=int, default=20,
                    help="untimed accepted steps (plain) / attempts (ensemble) before warm-up, past the start-up "
                         "transient of the step size")
@@ -292,7 +296,8 @@ def run_ours(args, world, rank, local, keep_sim=False, plain_steps=None):
     elapsed_max = reduce_max(elapsed, world, args)
     # roofline of the dominant kernel (traction product), timed live
     ms_mv = sim.profile_traction(reps=10)
-    K_bytes = 8.0 * (3 * n) * (2 * n) if args.precision == "fp64" else 4.0 * (3 * n) * (2 * n) + 4.0 * 3 * n
+    # the profiled launch is stage 2: FP64 K, or (split) the hi plane of the anchored increments
+    K_bytes = 8.0 * (3 * n) * (2 * n) if args.precision == "fp64" else 2.0 * (3 * n) * (2 * n) + 4.0 * 3 * n
     alg_bytes = K_bytes + 8.0 * (2 * n + 3 * n)
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (ms_mv / 1e3) / 1e9
@@ -331,7 +336,8 @@ def run_ours(args, world, rank, local, keep_sim=False, plain_steps=None):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": load_traffic("k_traction"),
                          "kernel": "k_traction (FP64 K.v + rate-state epilogue)" if args.precision == "fp64"
-                         else "k_traction_split", "ms_per_launch": ms_mv, "peak_source": peak_kind,
+                         else "k_traction<S,bf16> (hi plane x velocity increments + rate-state epilogue)",
+                         "ms_per_launch": ms_mv, "peak_source": peak_kind,
                          "bytes_per_launch": alg_bytes},
             "e2e": {"value": world * e2e_steps / e2e_elapsed, "unit": "steps/s",
                     "h2d_bytes_per_step": 8 * 7 * n, "d2h_bytes_per_step": 2 * 8 * 7 * n},
@@ -353,6 +359,25 @@ def load_tensor_peak():
         with open(path) as f:
             return float(json.load(f)["bf16_tflops"]), "measured"
     return 1590.0, "fallback"
+
+
+def assembly_leg(args, local):
+    """Green's-function assembly per source family on a coupled fault + volume
+    model (cfg3 geometry, reduced wedge): device time of the rectangle and the
+    cuboid columns, in Mentries/s."""
+    import unicycle_b200
+    from unicycle_b200 import configs
+    nxf, nzf, nxv, nyv, nzv = (int(v) for v in args.coupled_size.split(","))
+    c = configs.cfg3(nxf=nxf, nzf=nzf, nxv=nxv, nyv=nyv, nzv=nzv)
+    sim = unicycle_b200.Simulation(c["mu"], c["lam"], driver="viscouscycles", device=local)
+    configs.build_coupled(sim, c)
+    rect_ms, _, vol_ms = sim.assembly_times()
+    n, m = sim.dims
+    nf, nv = c["n_patch"], c["n_vol"]
+    sim.close()
+    return {"model": f"{nf} rectangles + {nv} cuboids (K {m} x {n})",
+            "okada_rect": {"entries": m * 2 * nf, "ms": rect_ms, "mentries_per_s": m * 2 * nf / rect_ms / 1e3},
+            "bml17_vol": {"entries": m * 6 * nv, "ms": vol_ms, "mentries_per_s": m * 6 * nv / vol_ms / 1e3}}
 
 
 def learned_leg(args, local, sim20, sets, y0s, plain_window):
@@ -400,8 +425,12 @@ def learned_leg(args, local, sim20, sets, y0s, plain_window):
     losses, t_train = cuda_time(lambda: model.train(epochs=20, batch=4096, lr=1e-3))
     out = {"traces": int(len(traces)), "trace_runs": args.trace_runs, "trace_seconds": t_traces,
            "train_epochs": 20, "train_seconds": t_train, "loss_first_last": [float(losses[0]), float(losses[-1])]}
-    # held-out cfg1 runs to 15 simulated years
-    t_end = 15 * YEAR
+    if args.learned_eval_years <= 0:
+        sim1.close()
+        model.close()
+        return out
+    # held-out cfg1 runs
+    t_end = args.learned_eval_years * YEAR
     held = {}
     for name, mdl in (("plain", None), ("learned", model)):
         e = ens1(y_test, mdl)
@@ -409,13 +438,14 @@ def learned_leg(args, local, sim20, sets, y0s, plain_window):
         _, t, _, acc, rej, st = e.get_states(0)
         onsets = np.array([e.events(0, i)[1] for i in range(len(y_test))])
         held[name] = dict(attempts=int(np.sum(acc + rej)), rejected_fraction=float(np.sum(rej) / np.sum(acc + rej)),
-                          seconds=secs, seconds_per_sim_year=secs / (15.0 * len(y_test)), onsets=onsets)
+                          seconds=secs, seconds_per_sim_year=secs / (args.learned_eval_years * len(y_test)),
+                          onsets=onsets)
         e.close()
     ok = (held["plain"]["onsets"] > 0) & (held["learned"]["onsets"] > 0)
     rel = np.abs(held["learned"]["onsets"] - held["plain"]["onsets"])[ok] / held["plain"]["onsets"][ok]
     for h in held.values():
         h.pop("onsets")
-    out["held_out_cfg1"] = {"runs": len(y_test), "t_end_years": 15, **{k: v for k, v in held.items()},
+    out["held_out_cfg1"] = {"runs": len(y_test), "t_end_years": args.learned_eval_years, **held,
                             "attempt_ratio_plain_over_learned": held["plain"]["attempts"] / held["learned"]["attempts"],
                             "wallclock_gain_per_sim_year": held["plain"]["seconds"] / held["learned"]["seconds"],
                             "max_onset_rel_diff": float(rel.max()) if len(rel) else None}
@@ -521,6 +551,10 @@ def run_ensemble(args, world, rank, local):
     torch.cuda.synchronize()
     e2e_elapsed = reduce_max(time.perf_counter() - t0, world, args)
     ens.close()
+    tri_ms = sim.assembly_times()[1]
+    families = assembly_leg(args, local) if rank == 0 else None
+    if families:
+        families["nikkhoo_tri"] = {"entries": 6 * n * n, "ms": tri_ms, "mentries_per_s": 6 * n * n / tri_ms / 1e3}
     learned = None
     if not args.no_learned and rank == 0:
         learned = learned_leg(args, local, sim, sets, y0s,
@@ -577,6 +611,7 @@ def run_ensemble(args, world, rank, local):
             "gpu_launches": int(attempts * 20 + 3),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "assembly_families": families,
             "learned_step": learned,
         }
     sim.close()
@@ -590,6 +625,19 @@ def main():
         out = run_reference(args, world, rank)
     elif args.workload == "ensemble":
         out = run_ensemble(args, world, rank, local)
+    elif args.workload == "coupled":
+        import torch
+        torch.cuda.set_device(local)
+        fam = assembly_leg(args, local) if rank == 0 else None
+        out = None
+        if rank == 0:
+            tot_e = fam["okada_rect"]["entries"] + fam["bml17_vol"]["entries"]
+            tot_ms = fam["okada_rect"]["ms"] + fam["bml17_vol"]["ms"]
+            out = {"metric": "GF assembly Mentries/s (coupled fault + volume)", "value": tot_e / tot_ms / 1e3,
+                   "unit": "Mentries/s", "n_gpus": world, "steps": 1, "warmup": 0, "ms_per_step": tot_ms,
+                   "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                   "data": "synthetic (seeded cfg3 geometry)", "config": {"workload": fam["model"]},
+                   "assembly_families": fam}
     else:
         if args.workload == "split":
             args.precision = "split_bf16"

@@ -102,6 +102,11 @@ int ucg_set_rheology(ucg_ctx *ctx, const double *e_bg, const double *gammadot0m,
    okada_mode: UCG_OKADA_*. */
 int ucg_assemble(ucg_ctx *ctx, int okada_mode);
 
+/* Device time (ms) of the last ucg_assemble per source family: the columns of
+   rectangles, triangles and volumes (all receivers each).  No reference
+   counterpart (a measurement aid). */
+int ucg_assembly_times(ucg_ctx *ctx, double *rect_ms, double *tri_ms, double *vol_ms);
+
 /* Sizes of the reference layout G(n,m): n source DOFs, m receiver DOFs. */
 int ucg_dims(ucg_ctx *ctx, long *n, long *m);
 

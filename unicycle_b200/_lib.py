@@ -54,6 +54,7 @@ SIGNATURES = {
     "ucg_set_friction": (_i, [_vp] + [_dp] * 9),
     "ucg_set_rheology": (_i, [_vp, _dp, _dp, _dp, _i]),
     "ucg_assemble": (_i, [_vp, _i]),
+    "ucg_assembly_times": (_i, [_vp, _dp, _dp, _dp]),
     "ucg_dims": (_i, [_vp, _lp, _lp]),
     "ucg_copy_G": (_i, [_vp, _dp, _l, _l, _l]),
     "ucg_set_precision": (_i, [_vp, _i]),

@@ -377,10 +377,15 @@ int assemble_matrix(ucg_ctx *c, int okada_mode)
         return UCG_OK;
     };
     int rc;
+    // device time of each family's launches (ucg_assembly_times)
+    cudaEvent_t ev[6];
+    for (cudaEvent_t &e : ev) UCG_CUDA(cudaEventCreate(&e));
+    for (double &t : c->asm_ms) t = 0.0;
     if (c->nr) {
         std::vector<double> s;
         build_rect_sources(c, okada_mode, s);
         if ((rc = upload(s))) return rc;
+        UCG_CUDA(cudaEventRecord(ev[0], c->stream));
         const double alpha_d = (c->lambda + c->mu) / (c->lambda + 2.0 * c->mu);
         const double alpha = okada_mode == UCG_OKADA_REF32IO ? (double)f32(alpha_d) : alpha_d;
         dim3 grid((c->nr + TPB - 1) / TPB, gy);
@@ -392,11 +397,13 @@ int assemble_matrix(ucg_ctx *c, int okada_mode)
                                                                ok_med(alpha), c->mu, c->lambda);
         c->launches.count++;
         UCG_CUDA(cudaGetLastError());
+        UCG_CUDA(cudaEventRecord(ev[1], c->stream));
     }
     if (c->nt) {
         std::vector<double> s;
         build_tri_sources(c, s);
         if ((rc = upload(s))) return rc;
+        UCG_CUDA(cudaEventRecord(ev[2], c->stream));
         NwConst cst{c->lambda / (c->lambda + c->mu) / 2.0, c->mu, c->lambda};
         dim3 grid((c->nt + TPB - 1) / TPB, gy);
         // main TD, image TD and free-surface term in three accumulating passes
@@ -405,18 +412,27 @@ int assemble_matrix(ucg_ctx *c, int okada_mode)
         k_assemble_tri<2><<<grid, TPB, 0, c->stream>>>(c->K, n, 2L * c->nr, c->rcv, ne, np, dsrc, c->nt, cst);
         c->launches.count += 3;
         UCG_CUDA(cudaGetLastError());
+        UCG_CUDA(cudaEventRecord(ev[3], c->stream));
     }
     if (c->nv) {
         std::vector<double> s;
         build_vol_sources(c, s);
         if ((rc = upload(s))) return rc;
+        UCG_CUDA(cudaEventRecord(ev[4], c->stream));
         const double nu = c->lambda / (c->lambda + c->mu) / 2.0;
         dim3 grid((c->nv + TPB - 1) / TPB, gy);
         k_assemble_vol<<<grid, TPB, 0, c->stream>>>(c->K, n, 2L * np, c->rcv, ne, np, dsrc, c->nv, c->mu, nu);
         c->launches.count++;
         UCG_CUDA(cudaGetLastError());
+        UCG_CUDA(cudaEventRecord(ev[5], c->stream));
     }
     UCG_CUDA(cudaStreamSynchronize(c->stream));
+    const int have[3] = {c->nr > 0, c->nt > 0, c->nv > 0};
+    for (int f = 0; f < 3; f++) {
+        float ms = 0.0f;
+        if (have[f] && cudaEventElapsedTime(&ms, ev[2 * f], ev[2 * f + 1]) == cudaSuccess) c->asm_ms[f] = ms;
+    }
+    for (cudaEvent_t &e : ev) cudaEventDestroy(e);
     if (dsrc) cudaFree(dsrc);
     c->okada_mode = okada_mode;
     c->assembled = true;

@@ -286,6 +286,10 @@ template <> struct TmTraits<__nv_bfloat162> {
     static constexpr int PER = 4, CH = 1024;
     using Acc = float;
 };
+template <> struct TmTraits<__nv_bfloat16> {   // the hi plane alone (anchored stages 2-6)
+    static constexpr int PER = 8, CH = 2048;
+    using Acc = float;
+};
 
 template <class KT>
 __device__ __forceinline__ void tm_accumulate(const KT *srow, int cl, const double *v, long c, long n,
@@ -312,6 +316,21 @@ __device__ __forceinline__ void tm_accumulate<__nv_bfloat162>(const __nv_bfloat1
         const float lo = __uint_as_float(w4[q] & 0xffff0000u);
         acc = fmaf(hi, vq, acc);
         acc = fmaf(lo, vq, acc);
+    }
+}
+
+template <>
+__device__ __forceinline__ void tm_accumulate<__nv_bfloat16>(const __nv_bfloat16 *srow, int cl, const double *v,
+                                                             long c, long n, float &acc)
+{
+    const uint4 raw = *reinterpret_cast<const uint4 *>(srow + cl);
+    const uint32_t w4[4] = {raw.x, raw.y, raw.z, raw.w};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float v0 = (c + 2 * q < n) ? (float)v[c + 2 * q] : 0.0f;
+        const float v1 = (c + 2 * q + 1 < n) ? (float)v[c + 2 * q + 1] : 0.0f;
+        acc = fmaf(__uint_as_float(w4[q] << 16), v0, acc);
+        acc = fmaf(__uint_as_float(w4[q] & 0xffff0000u), v1, acc);
     }
 }
 
@@ -643,7 +662,12 @@ static void launch_traction(ucg_ctx *c, const StageArgs &a, int grid, int pb, in
 {
     const int threads = (MV_WARPS + 1) * 32;
     const size_t smem = (size_t)TM_STAGES * TM_STAGE_BYTES;
-    if (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi) {
+    if (S > 1 && rk_anchored(c) && c->Khi_plane) {
+        // anchored stages multiply the increments by the hi plane alone
+        auto kfn = k_traction<S, __nv_bfloat16>;
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kfn<<<grid, threads, smem, c->stream>>>(c->Khi_plane, c->n, c->ldk_split, c->Kscale, a, c->ctl, pb, vb);
+    } else if (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi) {
         auto kfn = k_traction<S, __nv_bfloat162>;
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kfn<<<grid, threads, smem, c->stream>>>(reinterpret_cast<const __nv_bfloat162 *>(c->Khi), c->n,

@@ -275,6 +275,16 @@ int ucg_assemble(ucg_ctx *c, int okada_mode)
     return UCG_OK;
 }
 
+int ucg_assembly_times(ucg_ctx *c, double *rect_ms, double *tri_ms, double *vol_ms)
+{
+    if (!c) return UCG_E_BADARG;
+    if (!c->assembled) return set_err(c, UCG_E_STATE, "matrix not assembled");
+    if (rect_ms) *rect_ms = c->asm_ms[0];
+    if (tri_ms) *tri_ms = c->asm_ms[1];
+    if (vol_ms) *vol_ms = c->asm_ms[2];
+    return UCG_OK;
+}
+
 int ucg_dims(ucg_ctx *c, long *n, long *m)
 {
     if (!c) return UCG_E_BADARG;

@@ -100,6 +100,13 @@ class Simulation:
     def buildG(self, okada_mode=_lib.UCG_OKADA_FP64):
         self._check(self.lib.ucg_assemble(self.ctx, okada_mode), "buildG")
 
+    def assembly_times(self):
+        """Device ms of the last buildG per source family: (rectangles, triangles, volumes)."""
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.ucg_assembly_times(self.ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+                    "assembly_times")
+        return a.value, b.value, c.value
+
     @property
     def dims(self):
         n = ctypes.c_long()
