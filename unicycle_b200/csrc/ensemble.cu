@@ -76,16 +76,17 @@ constexpr int ST_THREADS = 256;         // finish kernel: state entries per bloc
 constexpr unsigned long long TIMEOUT_NS = 4000000000ull;
 
 // KLO: the stage also reads the K lo image (three MMAs per k-step); without it
-// (stage increments) only the hi image is read and two MMAs run, Khi Vhi + Khi Vlo
-template <int NI, bool KLO>
+// (stage increments) only the hi image is read and two MMAs run, Khi Vhi + Khi Vlo.
+// MT: M-tiles per work unit sharing each V stage (2 halves the V bytes per K byte).
+template <int NI, bool KLO, int MT>
 struct Tile {
     static constexpr int B_HALF = NI * BK * 2;
     static constexpr int B_IMG = 2 * B_HALF;
-    static constexpr int A_BYTES = KLO ? A_IMG : A_HALF;
-    static constexpr int STAGE = A_BYTES + B_IMG;
+    static constexpr int A_BYTES = KLO ? A_IMG : A_HALF;   // per M-tile
+    static constexpr int STAGE = MT * A_BYTES + B_IMG;
     static constexpr int STAGES = (6 * 32768) / STAGE < 8 ? (6 * 32768) / STAGE : 8;   // ~192 KB in flight
     static constexpr int SMEM = STAGES * STAGE + 1024;   // + slack for 1024-byte alignment
-    static constexpr uint32_t TMEM_COLS = 2 * NI;         // two FP32 accumulators of NI columns
+    static constexpr uint32_t TMEM_COLS = 2 * MT * NI;    // two sets of MT FP32 accumulators of NI columns
     // instruction descriptor: F32 accumulator, bf16 A and B, both K-major,
     // N = NI (bits 17-22, N/8), M = 128 (bits 24-28, M/16)
     static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NI >> 3) << 17) |
@@ -135,7 +136,8 @@ constexpr int TRACE_LEN = mlp::NIN + 3;
 
 struct GeomDev {
     int np, ninst, mtiles, kblocks;
-    int tile0;                  // global id of tile (nt = 0, mt = 0)
+    int tile0;                  // unit id of tile (nt = 0, mt = 0) in the single-tile plan
+    int pair0, mpairs;          // unit id of pair (nt = 0, 0) in the paired plan; pairs per instance tile
     int blk_e0, epb_e;          // element-wise grid: first block, blocks per instance
     int blk_s0, epb_s;          // state-wise grid
     uint8_t *B;                 // V images [ntile][kblock][hi | lo]
@@ -149,13 +151,16 @@ struct GeomDev {
 struct EnsArgs {
     int ngeom, ni, blocks_e, blocks_s;
     GeomDev g[MAX_GEOM];
-    const float *ws;            // partial sums [slot][ni][128]
-    const int *piece0, *npieces;
+    const float *ws1, *ws2;     // partial sums: [slot][ni][128] (single tiles), [slot][2][ni][128] (pairs)
+    const int *piece0_1, *npieces_1, *piece0_2, *npieces_2;
     EnsGlobal *glob;
 };
 
+// a work unit: one M-tile, or two consecutive M-tiles of a geometry (a1 null when
+// the geometry's last tile has no partner)
 struct GemmTile {
-    const uint8_t *a;           // K images of k-block 0 of this tile
+    const uint8_t *a;           // K images of k-block 0 of the (first) M-tile
+    const uint8_t *a1;          // the second M-tile's, or null
     const uint8_t *b;           // V images of k-block 0 of this instance tile
 };
 struct GemmSeg {
@@ -240,11 +245,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16])
 
 // ---- the contraction ---------------------------------------------------------------
 
-template <int NI, bool KLO>
+template <int NI, bool KLO, int MT>
 __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__restrict__ tiles,
         const GemmSeg *__restrict__ segs, const int *__restrict__ cta_seg, float *__restrict__ ws, int *err)
 {
-    using T = Tile<NI, KLO>;
+    using T = Tile<NI, KLO, MT>;
     extern __shared__ unsigned char dyn_smem[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dyn_smem) + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full[T::STAGES], empty[T::STAGES], acc_full[2], acc_empty[2], drain;
@@ -283,11 +288,13 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
 
     if (warp == 0) {
         if (lane == 0) {
-            // producer: one 32 KB copy of K and one copy of V per k-block
+            // producer: per k-block one copy of K per M-tile of the unit and one copy of V
             long issued = 0;
             for (int q = q0; q < q1 && !abort_flag; q++) {
                 const GemmSeg sg = segs[q];
                 const GemmTile tl = tiles[sg.tile];
+                const bool two = MT == 2 && tl.a1 != nullptr;
+                const uint32_t bytes = (uint32_t)((two ? 2 : 1) * T::A_BYTES + T::B_IMG);
                 for (int kb = sg.kb0; kb < sg.kb1; kb++) {
                     const int s = (int)(issued % T::STAGES);
                     const uint32_t ph = (uint32_t)((issued / T::STAGES) & 1);
@@ -296,9 +303,10 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                         break;
                     }
                     uint8_t *st = smem + (size_t)s * T::STAGE;
-                    bar_expect_tx(&full[s], (uint32_t)(T::A_BYTES + T::B_IMG));
+                    bar_expect_tx(&full[s], bytes);
                     bulk_load(st, tl.a + (size_t)kb * A_IMG, T::A_BYTES, &full[s]);
-                    bulk_load(st + T::A_BYTES, tl.b + (size_t)kb * T::B_IMG, T::B_IMG, &full[s]);
+                    if (two) bulk_load(st + T::A_BYTES, tl.a1 + (size_t)kb * A_IMG, T::A_BYTES, &full[s]);
+                    bulk_load(st + MT * T::A_BYTES, tl.b + (size_t)kb * T::B_IMG, T::B_IMG, &full[s]);
                     issued++;
                 }
             }
@@ -313,6 +321,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
             bool issued_any = false;
             for (int q = q0; q < q1 && !abort_flag; q++, tc++) {
                 const GemmSeg sg = segs[q];
+                const int nt = (MT == 2 && tiles[sg.tile].a1 != nullptr) ? 2 : 1;
                 const int buf = tc & 1;
                 const uint32_t use = (uint32_t)(tc >> 1);
                 if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag)) {
@@ -320,7 +329,6 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d = tmem + (uint32_t)(buf * NI);
                 bool ok = true;
                 for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
                     const int s = (int)(it % T::STAGES);
@@ -332,14 +340,22 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                     }
                     tc_fence_after();
                     const uint32_t a = s_addr(smem + (size_t)s * T::STAGE);
-                    const uint32_t b = a + T::A_BYTES;
+                    const uint32_t b = a + MT * T::A_BYTES;
 #pragma unroll
                     for (int j = 0; j < BK / 16; j++) {
-                        const uint64_t ahi = sw128_desc(a + 32u * j);
                         const uint64_t bhi = sw128_desc(b + 32u * j), blo = sw128_desc(b + T::B_HALF + 32u * j);
-                        mma_bf16(d, ahi, bhi, T::IDESC, (kb > sg.kb0 || j > 0) ? 1u : 0u);
-                        mma_bf16(d, ahi, blo, T::IDESC, 1u);
-                        if (KLO) mma_bf16(d, sw128_desc(a + A_HALF + 32u * j), bhi, T::IDESC, 1u);
+                        const uint32_t acc = (kb > sg.kb0 || j > 0) ? 1u : 0u;
+#pragma unroll
+                        for (int u = 0; u < MT; u++) {
+                            if (u < nt) {
+                                const uint32_t d = tmem + (uint32_t)((buf * MT + u) * NI);
+                                const uint32_t au = a + (uint32_t)(u * T::A_BYTES);
+                                const uint64_t ahi = sw128_desc(au + 32u * j);
+                                mma_bf16(d, ahi, bhi, T::IDESC, acc);
+                                mma_bf16(d, ahi, blo, T::IDESC, 1u);
+                                if (KLO) mma_bf16(d, sw128_desc(au + A_HALF + 32u * j), bhi, T::IDESC, 1u);
+                            }
+                        }
                     }
                     issued_any = true;
                     mma_commit(&empty[s]);   // frees the stage once these MMAs have read it
@@ -361,6 +377,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
         int tc = 0;
         for (int q = q0; q < q1; q++, tc++) {
             const GemmSeg sg = segs[q];
+            const int nt = (MT == 2 && tiles[sg.tile].a1 != nullptr) ? 2 : 1;
             const int buf = tc & 1;
             const uint32_t use = (uint32_t)(tc >> 1);
             int ok = 0;
@@ -371,14 +388,17 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                 break;
             }
             tc_fence_after();
-            float *dst = ws + (size_t)sg.slot * NI * BM + row;
-            const uint32_t tbase = tmem + (uint32_t)(buf * NI) + ((uint32_t)(quarter * 32) << 16);
+            for (int u = 0; u < nt; u++) {
+                float *dst = ws + ((size_t)sg.slot * MT + u) * NI * BM + row;
+                const uint32_t tbase =
+                    tmem + (uint32_t)((buf * MT + u) * NI) + ((uint32_t)(quarter * 32) << 16);
 #pragma unroll
-            for (int c0 = 0; c0 < NI; c0 += 16) {
-                uint32_t r[16];
-                tmem_ld16(tbase + (uint32_t)c0, r);
+                for (int c0 = 0; c0 < NI; c0 += 16) {
+                    uint32_t r[16];
+                    tmem_ld16(tbase + (uint32_t)c0, r);
 #pragma unroll
-                for (int i = 0; i < 16; i++) dst[(size_t)(c0 + i) * BM] = __uint_as_float(r[i]);
+                    for (int i = 0; i < 16; i++) dst[(size_t)(c0 + i) * BM] = __uint_as_float(r[i]);
+                }
             }
             tc_fence_before();
             __syncwarp();
@@ -475,20 +495,36 @@ __global__ void k_pack_v_dense(uint8_t *B, int ni, int kblocks, int ninst, long 
     put_v(B, ni, kblocks, i, c, v0, v1);
 }
 
-__device__ __forceinline__ double traction_row(const EnsArgs *A, const GeomDev &G, int i, long r)
+// row r of instance i from the partial sums, added in k order: `paired`
+// selects the paired plan's workspace (stage increments) over the single-tile
+// plan's (anchor)
+__device__ __forceinline__ double traction_row(const EnsArgs *A, const GeomDev &G, int i, long r, bool paired)
 {
     const int ni = A->ni;
     const int mt = (int)(r / BM), rr = (int)(r % BM);
-    const int tile = G.tile0 + (i / ni) * G.mtiles + mt;
-    const int p0 = A->piece0[tile], np_ = A->npieces[tile];
-    const float *w = A->ws + ((size_t)p0 * ni + (i % ni)) * BM + rr;
+    const float *w;
+    int np_;
+    size_t stride;
+    if (paired) {
+        const int unit = G.pair0 + (i / ni) * G.mpairs + mt / 2;
+        const int p0 = A->piece0_2[unit];
+        np_ = A->npieces_2[unit];
+        w = A->ws2 + (((size_t)p0 * 2 + (mt & 1)) * ni + (i % ni)) * BM + rr;
+        stride = (size_t)2 * ni * BM;
+    } else {
+        const int unit = G.tile0 + (i / ni) * G.mtiles + mt;
+        const int p0 = A->piece0_1[unit];
+        np_ = A->npieces_1[unit];
+        w = A->ws1 + ((size_t)p0 * ni + (i % ni)) * BM + rr;
+        stride = (size_t)ni * BM;
+    }
     double s = 0.0;
-    for (int p = 0; p < np_; p++) s += (double)w[(size_t)p * ni * BM];
+    for (int p = 0; p < np_; p++) s += (double)w[(size_t)p * stride];
     return s * (double)G.rscale[r];
 }
 
 // T (instance-major, ninst x m) of geometry gi from the workspace
-__global__ void k_reduce_dense(const EnsArgs *A, int gi, double *T)
+__global__ void k_reduce_dense(const EnsArgs *A, int gi, double *T, int paired)
 {
     const GeomDev &G = A->g[gi];
     const long m = 3L * G.np;
@@ -496,7 +532,7 @@ __global__ void k_reduce_dense(const EnsArgs *A, int gi, double *T)
     if (t >= (long)G.ninst * m) return;
     const int i = (int)(t / m);
     const long r = t % m;
-    T[t] = traction_row(A, G, i, r);
+    T[t] = traction_row(A, G, i, r, paired != 0);
 }
 
 // ---- Runge-Kutta stages for all instances --------------------------------------------
@@ -618,7 +654,7 @@ __global__ void k_ens_rhs(const EnsArgs *__restrict__ A)
     double t[3];
     double *t1 = G.t1 + (long)i * 3 * G.np + 3L * e;
     for (int q = 0; q < 3; q++) {
-        const double inc = traction_row(A, G, i, 3L * e + q);
+        const double inc = traction_row(A, G, i, 3L * e + q, S > 1);
         if (S == 1) {
             t1[q] = inc;
             t[q] = inc;
@@ -892,6 +928,16 @@ struct EnsGeomHost {
     int b_ni = 0;
 };
 
+struct PlanBufs {
+    GemmTile *tiles = nullptr;
+    GemmSeg *segs = nullptr;
+    int *cta = nullptr;
+    int *piece0 = nullptr, *npieces = nullptr;
+    float *ws = nullptr;
+    int nunits = 0, nsegs = 0, nslots = 0;
+    std::string name;
+};
+
 struct ucg_ensemble {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -900,17 +946,12 @@ struct ucg_ensemble {
     std::vector<EnsGeomHost> geoms;
     double epsilon = 1.0e-6, hmax = 1.7976931348623158e308;
 
-    // plan: instance tile width, schedule, workspace
+    // plan: instance tile width and two schedules with their workspaces: single
+    // M-tiles for the anchor's contraction, pairs of M-tiles for the increments'
     int ni = 0;
     bool planned = false;
     std::string plan_name;
-    GemmTile *d_tiles = nullptr;
-    GemmSeg *d_segs = nullptr;
-    int *d_cta = nullptr;
-    int *d_piece0 = nullptr, *d_npieces = nullptr;
-    float *ws = nullptr;
-    size_t ws_bytes = 0;
-    int nsegs = 0, ntiles = 0, nslots = 0;
+    PlanBufs p1, p2;
     std::string tune_report;
 
     EnsArgs *d_args = nullptr;
@@ -1056,11 +1097,11 @@ size_t b_bytes(const EnsGeomHost &g, int ni)
 template <int NI>
 cudaError_t prepare_contract_t()
 {
-    cudaError_t e = cudaFuncSetAttribute(k_bf16x3_contract<NI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Tile<NI, true>::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(k_bf16x3_contract<NI, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Tile<NI, true, 1>::SMEM);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_bf16x3_contract<NI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                Tile<NI, false>::SMEM);
+    return cudaFuncSetAttribute(k_bf16x3_contract<NI, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Tile<NI, false, 2>::SMEM);
 }
 
 cudaError_t prepare_contract(int ni)
@@ -1073,50 +1114,54 @@ cudaError_t prepare_contract(int ni)
     }
 }
 
-template <int NI, bool KLO>
-cudaError_t launch_contract_t(ucg_ensemble *E)
+template <int NI, bool KLO, int MT>
+cudaError_t launch_contract_t(ucg_ensemble *E, const PlanBufs &P)
 {
-    k_bf16x3_contract<NI, KLO><<<E->sms, 192, Tile<NI, KLO>::SMEM, E->stream>>>(E->d_tiles, E->d_segs, E->d_cta,
-                                                                                E->ws, &E->d_glob->err);
+    k_bf16x3_contract<NI, KLO, MT><<<E->sms, 192, Tile<NI, KLO, MT>::SMEM, E->stream>>>(P.tiles, P.segs, P.cta,
+                                                                                        P.ws, &E->d_glob->err);
     E->launches++;
     return cudaGetLastError();
 }
 
-// klo: also read the K lo image (the stage-1 anchor); without it the stage
-// increments' product Khi (Vhi + Vlo)
+// klo: the anchor's contraction (K hi and lo, single M-tiles); otherwise the
+// stage increments' Khi (Vhi + Vlo) over pairs of M-tiles
 cudaError_t launch_contract(ucg_ensemble *E, bool klo = true)
 {
     switch (E->ni) {
-    case 32: return klo ? launch_contract_t<32, true>(E) : launch_contract_t<32, false>(E);
-    case 64: return klo ? launch_contract_t<64, true>(E) : launch_contract_t<64, false>(E);
-    case 128: return klo ? launch_contract_t<128, true>(E) : launch_contract_t<128, false>(E);
+    case 32: return klo ? launch_contract_t<32, true, 1>(E, E->p1) : launch_contract_t<32, false, 2>(E, E->p2);
+    case 64: return klo ? launch_contract_t<64, true, 1>(E, E->p1) : launch_contract_t<64, false, 2>(E, E->p2);
+    case 128: return klo ? launch_contract_t<128, true, 1>(E, E->p1) : launch_contract_t<128, false, 2>(E, E->p2);
     default: return cudaErrorInvalidValue;
     }
 }
 
-void free_plan(ucg_ensemble *E)
+void free_bufs(PlanBufs &P)
 {
-    void *ptrs[] = {E->d_tiles, E->d_segs, E->d_cta, E->d_piece0, E->d_npieces, E->ws};
+    void *ptrs[] = {P.tiles, P.segs, P.cta, P.piece0, P.npieces, P.ws};
     for (void *p : ptrs)
         if (p) cudaFree(p);
-    E->d_tiles = nullptr;
-    E->d_segs = nullptr;
-    E->d_cta = nullptr;
-    E->d_piece0 = E->d_npieces = nullptr;
-    E->ws = nullptr;
-    E->ws_bytes = 0;
+    P = PlanBufs();
+}
+
+void free_plan(ucg_ensemble *E)
+{
+    free_bufs(E->p1);
+    free_bufs(E->p2);
     if (E->graph) cudaGraphExecDestroy(E->graph);
     E->graph = nullptr;
     E->planned = false;
 }
 
-std::vector<int> tile_kblocks(ucg_ensemble *E, int ni)
+// work units (single M-tiles, mt = 1, or pairs, mt = 2) and their k-blocks, in
+// unit-id order: geometry, instance tile, M-tile (pair)
+std::vector<int> unit_kblocks(ucg_ensemble *E, int ni, int mt)
 {
     std::vector<int> tkb;
     for (const EnsGeomHost &g : E->geoms) {
         const int ntl = (g.ninst + ni - 1) / ni;
+        const int nu = (g.mtiles + mt - 1) / mt;
         for (int nt = 0; nt < ntl; nt++)
-            for (int mt = 0; mt < g.mtiles; mt++) tkb.push_back(g.kblocks);
+            for (int u = 0; u < nu; u++) tkb.push_back(g.kblocks);
     }
     return tkb;
 }
@@ -1136,48 +1181,57 @@ int ensure_b(ucg_ensemble *E, int ni)
     return UCG_OK;
 }
 
-// upload tiles, schedule and the kernel argument block for (ni, schedule)
-int install_plan(ucg_ensemble *E, int ni, const Sched &s)
+int upload_plan(ucg_ensemble *E, PlanBufs &P, int ni, int mt, const Sched &s)
+{
+    std::vector<GemmTile> units;
+    for (const EnsGeomHost &g : E->geoms) {
+        const int ntl = (g.ninst + ni - 1) / ni;
+        for (int nt = 0; nt < ntl; nt++)
+            for (int t = 0; t < g.mtiles; t += mt)
+                units.push_back(GemmTile{g.A + (size_t)t * g.kblocks * A_IMG,
+                                         (mt == 2 && t + 1 < g.mtiles) ? g.A + (size_t)(t + 1) * g.kblocks * A_IMG
+                                                                       : nullptr,
+                                         g.B + (size_t)nt * g.kblocks * (size_t)(2 * ni * BK * 2)});
+    }
+    P.nunits = (int)units.size();
+    P.nsegs = (int)s.segs.size();
+    P.nslots = s.nslots;
+    P.name = s.name;
+    ECUDA(cudaMalloc(&P.tiles, sizeof(GemmTile) * units.size()));
+    ECUDA(cudaMalloc(&P.segs, sizeof(GemmSeg) * std::max<size_t>(1, s.segs.size())));
+    ECUDA(cudaMalloc(&P.cta, sizeof(int) * s.cta.size()));
+    ECUDA(cudaMalloc(&P.piece0, sizeof(int) * units.size()));
+    ECUDA(cudaMalloc(&P.npieces, sizeof(int) * units.size()));
+    const size_t ws_bytes = (size_t)std::max(1, s.nslots) * mt * ni * BM * sizeof(float);
+    ECUDA(cudaMalloc(&P.ws, ws_bytes));
+    ECUDA(cudaMemsetAsync(P.ws, 0, ws_bytes, E->stream));
+    ECUDA(cudaMemcpyAsync(P.tiles, units.data(), sizeof(GemmTile) * units.size(), cudaMemcpyHostToDevice, E->stream));
+    if (!s.segs.empty())
+        ECUDA(cudaMemcpyAsync(P.segs, s.segs.data(), sizeof(GemmSeg) * s.segs.size(), cudaMemcpyHostToDevice,
+                              E->stream));
+    ECUDA(cudaMemcpyAsync(P.cta, s.cta.data(), sizeof(int) * s.cta.size(), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(P.piece0, s.piece0.data(), sizeof(int) * units.size(), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(P.npieces, s.npieces.data(), sizeof(int) * units.size(), cudaMemcpyHostToDevice,
+                          E->stream));
+    return UCG_OK;
+}
+
+// upload both schedules and the kernel argument block for instance tiles of width ni
+int install_plan(ucg_ensemble *E, int ni, const Sched &s1, const Sched &s2)
 {
     free_plan(E);
     int st = ensure_b(E, ni);
     if (st) return st;
     ECUDA(prepare_contract(ni));
     E->ni = ni;
-    std::vector<GemmTile> tiles;
-    for (const EnsGeomHost &g : E->geoms) {
-        const int ntl = (g.ninst + ni - 1) / ni;
-        for (int nt = 0; nt < ntl; nt++)
-            for (int mt = 0; mt < g.mtiles; mt++)
-                tiles.push_back(GemmTile{g.A + (size_t)mt * g.kblocks * A_IMG,
-                                         g.B + (size_t)nt * g.kblocks * (size_t)(2 * ni * BK * 2)});
-    }
-    E->ntiles = (int)tiles.size();
-    E->nsegs = (int)s.segs.size();
-    E->nslots = s.nslots;
-    ECUDA(cudaMalloc(&E->d_tiles, sizeof(GemmTile) * tiles.size()));
-    ECUDA(cudaMalloc(&E->d_segs, sizeof(GemmSeg) * std::max<size_t>(1, s.segs.size())));
-    ECUDA(cudaMalloc(&E->d_cta, sizeof(int) * s.cta.size()));
-    ECUDA(cudaMalloc(&E->d_piece0, sizeof(int) * tiles.size()));
-    ECUDA(cudaMalloc(&E->d_npieces, sizeof(int) * tiles.size()));
-    E->ws_bytes = (size_t)std::max(1, s.nslots) * ni * BM * sizeof(float);
-    ECUDA(cudaMalloc(&E->ws, E->ws_bytes));
-    ECUDA(cudaMemsetAsync(E->ws, 0, E->ws_bytes, E->stream));
-    ECUDA(cudaMemcpyAsync(E->d_tiles, tiles.data(), sizeof(GemmTile) * tiles.size(), cudaMemcpyHostToDevice, E->stream));
-    if (!s.segs.empty())
-        ECUDA(cudaMemcpyAsync(E->d_segs, s.segs.data(), sizeof(GemmSeg) * s.segs.size(), cudaMemcpyHostToDevice,
-                              E->stream));
-    ECUDA(cudaMemcpyAsync(E->d_cta, s.cta.data(), sizeof(int) * s.cta.size(), cudaMemcpyHostToDevice, E->stream));
-    ECUDA(cudaMemcpyAsync(E->d_piece0, s.piece0.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, E->stream));
-    ECUDA(cudaMemcpyAsync(E->d_npieces, s.npieces.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice,
-                          E->stream));
+    if ((st = upload_plan(E, E->p1, ni, 1, s1)) || (st = upload_plan(E, E->p2, ni, 2, s2))) return st;
 
     // kernel argument block
     EnsArgs a;
     memset(&a, 0, sizeof a);
     a.ngeom = (int)E->geoms.size();
     a.ni = ni;
-    int tile0 = 0, be = 0, bs = 0;
+    int tile0 = 0, pair0 = 0, be = 0, bs = 0;
     for (int gi = 0; gi < a.ngeom; gi++) {
         const EnsGeomHost &g = E->geoms[gi];
         GeomDev &d = a.g[gi];
@@ -1185,8 +1239,12 @@ int install_plan(ucg_ensemble *E, int ni, const Sched &s)
         d.ninst = g.ninst;
         d.mtiles = g.mtiles;
         d.kblocks = g.kblocks;
+        const int ntl = (g.ninst + ni - 1) / ni;
         d.tile0 = tile0;
-        tile0 += ((g.ninst + ni - 1) / ni) * g.mtiles;
+        tile0 += ntl * g.mtiles;
+        d.mpairs = (g.mtiles + 1) / 2;
+        d.pair0 = pair0;
+        pair0 += ntl * d.mpairs;
         d.epb_e = (g.np + EW_THREADS - 1) / EW_THREADS;
         d.blk_e0 = be;
         be += d.epb_e * g.ninst;
@@ -1212,13 +1270,16 @@ int install_plan(ucg_ensemble *E, int ni, const Sched &s)
     }
     a.blocks_e = be;
     a.blocks_s = bs;
-    a.ws = E->ws;
-    a.piece0 = E->d_piece0;
-    a.npieces = E->d_npieces;
+    a.ws1 = E->p1.ws;
+    a.piece0_1 = E->p1.piece0;
+    a.npieces_1 = E->p1.npieces;
+    a.ws2 = E->p2.ws;
+    a.piece0_2 = E->p2.piece0;
+    a.npieces_2 = E->p2.npieces;
     a.glob = E->d_glob;
     ECUDA(cudaMemcpyAsync(E->d_args, &a, sizeof a, cudaMemcpyHostToDevice, E->stream));
     ECUDA(cudaStreamSynchronize(E->stream));
-    E->plan_name = "ni=" + std::to_string(ni) + " " + s.name;
+    E->plan_name = "ni=" + std::to_string(ni) + " anchor " + s1.name + ", increments " + s2.name + " (pairs)";
     E->planned = true;
     return UCG_OK;
 }
@@ -1230,12 +1291,19 @@ int default_ni(ucg_ensemble *E)
     return mx <= 32 ? 32 : (mx <= 64 ? 64 : 128);
 }
 
+// the schedule of a kind for the single-tile (mt 1) or paired (mt 2) units
+Sched make_sched(ucg_ensemble *E, int ni, int mt, int kind, int chunk)
+{
+    const std::vector<int> tkb = unit_kblocks(E, ni, mt);
+    return kind == UCG_ENS_STREAM_K ? sched_stream_k(tkb, E->sms) : sched_split_lpt(tkb, E->sms, chunk, 2);
+}
+
 int ensure_plan(ucg_ensemble *E)
 {
     if (E->planned) return UCG_OK;
     if (E->geoms.empty()) return ebad(E, UCG_E_STATE, "ensemble has no geometry");
     const int ni = default_ni(E);
-    return install_plan(E, ni, sched_stream_k(tile_kblocks(E, ni), E->sms));
+    return install_plan(E, ni, make_sched(E, ni, 1, UCG_ENS_STREAM_K, 0), make_sched(E, ni, 2, UCG_ENS_STREAM_K, 0));
 }
 
 // mean device time per launch: the best of three trials of `reps` launches, so
@@ -1591,12 +1659,10 @@ int ucg_ens_plan(ucg_ensemble *E, int ni, int schedule, int chunk)
     if (!E) return UCG_E_BADARG;
     if (E->geoms.empty()) return ebad(E, UCG_E_STATE, "ensemble has no geometry");
     if (ni != 32 && ni != 64 && ni != 128) return ebad(E, UCG_E_BADARG, "ni must be 32, 64 or 128");
+    if (schedule != UCG_ENS_STREAM_K && schedule != UCG_ENS_SPLIT_LPT) return ebad(E, UCG_E_BADARG, "unknown schedule");
     ECUDA(cudaSetDevice(E->device));
     ECUDA(cudaStreamSynchronize(E->stream));
-    const std::vector<int> tkb = tile_kblocks(E, ni);
-    if (schedule == UCG_ENS_STREAM_K) return install_plan(E, ni, sched_stream_k(tkb, E->sms));
-    if (schedule == UCG_ENS_SPLIT_LPT) return install_plan(E, ni, sched_split_lpt(tkb, E->sms, chunk, 2));
-    return ebad(E, UCG_E_BADARG, "unknown schedule");
+    return install_plan(E, ni, make_sched(E, ni, 1, schedule, chunk), make_sched(E, ni, 2, schedule, chunk));
 }
 
 int ucg_ens_tune(ucg_ensemble *E, int reps, char *report, long report_len)
@@ -1611,38 +1677,43 @@ int ucg_ens_tune(ucg_ensemble *E, int reps, char *report, long report_len)
     std::vector<int> nis = {default_ni(E)};
     if (maxinst > 64 && nis[0] != 64) nis.push_back(64);
     std::string rep;
+    // the anchor's schedule (single tiles) and the increments' (pairs) are chosen
+    // independently; an attempt costs one anchor and five increment contractions
     double best = 1e300;
-    int best_ni = 0, best_kind = 0, best_chunk = 0;
+    int best_ni = 0;
+    struct Cand { int kind, chunk; };
+    Cand b1{UCG_ENS_STREAM_K, 0}, b2{UCG_ENS_STREAM_K, 0};
     for (int ni : nis) {
-        const std::vector<int> tkb = tile_kblocks(E, ni);
-        struct Cand { int kind, chunk; };
         std::vector<Cand> cands = {{UCG_ENS_STREAM_K, 0}, {UCG_ENS_SPLIT_LPT, 0}};
         for (int ch : {8, 16, 32, 64}) cands.push_back({UCG_ENS_SPLIT_LPT, ch});
+        double bf = 1e300, bh = 1e300;
+        Cand c1 = cands[0], c2 = cands[0];
         for (const Cand &cd : cands) {
-            const Sched s = cd.kind == UCG_ENS_STREAM_K ? sched_stream_k(tkb, E->sms)
-                                                        : sched_split_lpt(tkb, E->sms, cd.chunk, 2);
-            int st = install_plan(E, ni, s);
-            if (st) return st;
-            // one attempt contracts the anchor once (hi + lo) and five increments (hi)
+            const Sched s1 = make_sched(E, ni, 1, cd.kind, cd.chunk), s2 = make_sched(E, ni, 2, cd.kind, cd.chunk);
+            int st = install_plan(E, ni, s1, s2);
             double ms_full = 0.0, ms_hi = 0.0;
-            st = time_contract(E, reps, &ms_full, true);
+            if (!st) st = time_contract(E, reps, &ms_full, true);
             if (!st) st = time_contract(E, reps, &ms_hi, false);
             if (st) return st;
-            const double ms = ms_full + 5.0 * ms_hi;
             char line[200];
             snprintf(line, sizeof line,
-                     "ni=%d %-16s segments=%-5d predicted=%-6ld k-blocks  anchor %.4f ms  increment %.4f ms  "
-                     "attempt %.4f ms\n", ni, s.name.c_str(), (int)s.segs.size(), sched_cost(s, 2), ms_full, ms_hi, ms);
+                     "ni=%d %-16s anchor: %5d segments, predicted %6ld k-blocks, %.4f ms   increments (pairs): "
+                     "%5d segments, predicted %6ld k-blocks, %.4f ms\n", ni, s1.name.c_str(), (int)s1.segs.size(),
+                     sched_cost(s1, 2), ms_full, (int)s2.segs.size(), sched_cost(s2, 2), ms_hi);
             rep += line;
-            if (ms < best) {
-                best = ms;
-                best_ni = ni;
-                best_kind = cd.kind;
-                best_chunk = cd.chunk;
-            }
+            if (ms_full < bf) { bf = ms_full; c1 = cd; }
+            if (ms_hi < bh) { bh = ms_hi; c2 = cd; }
+        }
+        if (bf + 5.0 * bh < best) {
+            best = bf + 5.0 * bh;
+            best_ni = ni;
+            b1 = c1;
+            b2 = c2;
         }
     }
-    const int st = ucg_ens_plan(E, best_ni, best_kind, best_chunk);
+    ECUDA(cudaStreamSynchronize(E->stream));
+    const int st = install_plan(E, best_ni, make_sched(E, best_ni, 1, b1.kind, b1.chunk),
+                                make_sched(E, best_ni, 2, b2.kind, b2.chunk));
     if (st) return st;
     rep += "chosen: " + E->plan_name + "\n";
     E->tune_report = rep;
@@ -1674,7 +1745,7 @@ int ucg_ens_matvec(ucg_ensemble *E, int gi, const double *V, double *T, int term
     if (e == cudaSuccess) e = launch_contract(E, terms == 3);
     if (e == cudaSuccess) {
         const long work = (long)g.ninst * g.m;
-        k_reduce_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(E->d_args, gi, dT);
+        k_reduce_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(E->d_args, gi, dT, terms == 2 ? 1 : 0);
         E->launches += 2;
         e = cudaGetLastError();
     }

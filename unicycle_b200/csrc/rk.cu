@@ -291,46 +291,65 @@ template <> struct TmTraits<__nv_bfloat16> {   // the hi plane alone (anchored s
     using Acc = float;
 };
 
+// the thread's PER values of v for one chunk, loaded once and used for all the
+// rows of the stage; then one row's contribution
+template <class KT> struct TmV;
+template <> struct TmV<double> { double2 x; };
+template <> struct TmV<__nv_bfloat162> { float x[4]; };
+template <> struct TmV<__nv_bfloat16> { float x[8]; };
+
 template <class KT>
-__device__ __forceinline__ void tm_accumulate(const KT *srow, int cl, const double *v, long c, long n,
-                                              typename TmTraits<KT>::Acc &acc);
+__device__ __forceinline__ void tm_load_v(const double *v, long c, long n, TmV<KT> &vr);
 template <>
-__device__ __forceinline__ void tm_accumulate<double>(const double *srow, int cl, const double *v, long c, long n,
-                                                      double &acc)
+__device__ __forceinline__ void tm_load_v<double>(const double *v, long c, long n, TmV<double> &vr)
 {
     (void)n;
-    const double2 kv = *reinterpret_cast<const double2 *>(srow + cl);
-    const double2 vv = *reinterpret_cast<const double2 *>(v + c);
-    acc = fma(kv.y, vv.y, fma(kv.x, vv.x, acc));
+    vr.x = *reinterpret_cast<const double2 *>(v + c);
 }
 template <>
-__device__ __forceinline__ void tm_accumulate<__nv_bfloat162>(const __nv_bfloat162 *srow, int cl, const double *v,
-                                                              long c, long n, float &acc)
+__device__ __forceinline__ void tm_load_v<__nv_bfloat162>(const double *v, long c, long n, TmV<__nv_bfloat162> &vr)
 {
-    const uint4 raw = *reinterpret_cast<const uint4 *>(srow + cl);
-    const uint32_t w4[4] = {raw.x, raw.y, raw.z, raw.w};
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const float vq = (c + q < n) ? (float)v[c + q] : 0.0f;
-        const float hi = __uint_as_float(w4[q] << 16);
-        const float lo = __uint_as_float(w4[q] & 0xffff0000u);
-        acc = fmaf(hi, vq, acc);
-        acc = fmaf(lo, vq, acc);
-    }
+    for (int q = 0; q < 4; q++) vr.x[q] = (c + q < n) ? (float)v[c + q] : 0.0f;
+}
+template <>
+__device__ __forceinline__ void tm_load_v<__nv_bfloat16>(const double *v, long c, long n, TmV<__nv_bfloat16> &vr)
+{
+#pragma unroll
+    for (int q = 0; q < 8; q++) vr.x[q] = (c + q < n) ? (float)v[c + q] : 0.0f;
 }
 
+template <class KT>
+__device__ __forceinline__ void tm_accumulate(const KT *srow, int cl, const TmV<KT> &vr,
+                                              typename TmTraits<KT>::Acc &acc);
 template <>
-__device__ __forceinline__ void tm_accumulate<__nv_bfloat16>(const __nv_bfloat16 *srow, int cl, const double *v,
-                                                             long c, long n, float &acc)
+__device__ __forceinline__ void tm_accumulate<double>(const double *srow, int cl, const TmV<double> &vr, double &acc)
+{
+    const double2 kv = *reinterpret_cast<const double2 *>(srow + cl);
+    acc = fma(kv.y, vr.x.y, fma(kv.x, vr.x.x, acc));
+}
+template <>
+__device__ __forceinline__ void tm_accumulate<__nv_bfloat162>(const __nv_bfloat162 *srow, int cl,
+                                                              const TmV<__nv_bfloat162> &vr, float &acc)
 {
     const uint4 raw = *reinterpret_cast<const uint4 *>(srow + cl);
     const uint32_t w4[4] = {raw.x, raw.y, raw.z, raw.w};
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        const float v0 = (c + 2 * q < n) ? (float)v[c + 2 * q] : 0.0f;
-        const float v1 = (c + 2 * q + 1 < n) ? (float)v[c + 2 * q + 1] : 0.0f;
-        acc = fmaf(__uint_as_float(w4[q] << 16), v0, acc);
-        acc = fmaf(__uint_as_float(w4[q] & 0xffff0000u), v1, acc);
+        acc = fmaf(__uint_as_float(w4[q] << 16), vr.x[q], acc);
+        acc = fmaf(__uint_as_float(w4[q] & 0xffff0000u), vr.x[q], acc);
+    }
+}
+template <>
+__device__ __forceinline__ void tm_accumulate<__nv_bfloat16>(const __nv_bfloat16 *srow, int cl,
+                                                             const TmV<__nv_bfloat16> &vr, float &acc)
+{
+    const uint4 raw = *reinterpret_cast<const uint4 *>(srow + cl);
+    const uint32_t w4[4] = {raw.x, raw.y, raw.z, raw.w};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        acc = fmaf(__uint_as_float(w4[q] << 16), vr.x[2 * q], acc);
+        acc = fmaf(__uint_as_float(w4[q] & 0xffff0000u), vr.x[2 * q + 1], acc);
     }
 }
 
@@ -423,9 +442,11 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
             const int cl = PER * t;
             const long c = ch * CH + cl;
             if (ready && c < n) {
+                TmV<KT> vr;
+                tm_load_v<KT>(a.v, c, n, vr);
 #pragma unroll
                 for (int r = 0; r < MV_ROWS; r++)
-                    if (r < nrows) tm_accumulate<KT>(src + (size_t)r * CH, cl, a.v, c, n, acc[r]);
+                    if (r < nrows) tm_accumulate<KT>(src + (size_t)r * CH, cl, vr, acc[r]);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
