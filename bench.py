@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--nx", type=int, default=100, help="along-strike cells (2 triangles each per row)")
     p.add_argument("--nz", type=int, default=100, help="down-dip rows")
     p.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16"])
-    p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split", "coupled"])
+    p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split", "coupled", "cfg4"])
     p.add_argument("--coupled-size", default="64,64,16,8,8",
                    help="coupled assembly leg: fault nx,nz and volume nx,ny,nz")
     p.add_argument("--sets", type=int, default=N_SETS, help="instances in the ensemble workload")
@@ -380,6 +380,75 @@ def assembly_leg(args, local):
             "bml17_vol": {"entries": m * 6 * nv, "ms": vol_ms, "mentries_per_s": m * 6 * nv / vol_ms / 1e3}}
 
 
+def run_cfg4(args, world, rank, local):
+    """The batched-ensemble configuration: 4 fault geometries of 1,024 to 4,096
+    rectangles x 64 frictional parameter sets in one ensemble (256 instances),
+    against the plain FP64 single-instance path run over the same instances one
+    after another (estimated from one instance per geometry)."""
+    import torch
+    import unicycle_b200
+    from unicycle_b200 import configs
+    torch.cuda.set_device(local)
+    cfg = configs.cfg4()
+    ens = unicycle_b200.Ensemble(device=local)
+    configs.build_ensemble(ens, cfg, lambda mu, lam: unicycle_b200.Simulation(mu, lam, device=local))
+    report = ens.tune(reps=3)
+    stream = torch.cuda.ExternalStream(ens.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    spin = max(args.spinup, 300)   # past the start-up transient of the step size (dt0 = 1 ms)
+    ens.run(cfg["t_end"], spin + args.warmup)
+    i0 = ens.info()
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0.record(stream)
+        attempts = ens.run(cfg["t_end"], args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    elapsed = reduce_max(e0.elapsed_time(e1) / 1e3, world, args)
+    i1 = ens.info()
+    ens.close()
+    acc, rej = i1["accepted"] - i0["accepted"], i1["rejected"] - i0["rejected"]
+    syh = (i1["time_sum"] - i0["time_sum"]) / YEAR / (elapsed / 3600.0)
+    # plain FP64: one instance per geometry, same spin-up, same number of steps
+    plain = []
+    for g in cfg["geoms"]:
+        sim = unicycle_b200.Simulation(g["mu"], g["lam"], device=local)
+        configs.build(sim, g)
+        sim.set_state(g["y0s"][0], 0.0, cfg["dt0"])
+        sim.run(cfg["t_end"], spin + args.warmup)
+        _, t0, _, a0, _ = sim.get_state()
+        st = torch.cuda.ExternalStream(sim.stream, device=local)
+        torch.cuda.synchronize()
+        e0.record(st)
+        n = sim.run(cfg["t_end"], max(5, args.steps // 2))
+        e1.record(st)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        _, t1, _, a1, _ = sim.get_state()
+        plain.append({"patches": g["n_patch"], "steps_per_s": n / sec, "sim_years_per_hour": (t1 - t0) / YEAR / (sec / 3600)})
+        sim.close()
+    # the 256 instances one after another on the plain path
+    per_step = sum(64.0 / p["steps_per_s"] for p in plain) / 256.0
+    plain_agg = 1.0 / per_step
+    plain_syh = sum(p["sim_years_per_hour"] for p in plain) / 4.0
+    if rank != 0:
+        return None
+    return {"metric": "RK45 steps/s, cfg4 batched ensemble (aggregate over 256 instances)", "value": world * acc / elapsed,
+            "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * elapsed / attempts, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3/f32 product, f64 state", "data": "synthetic (seeded cfg4: 4 faults x 64 parameter sets)",
+            "config": {"workload": "4 rectangle faults (1,024 / 2,048 / 3,072 / 4,096 patches) x 64 frictional "
+                                   "parameter sets, one ensemble", "plan": i1["plan"], "rtol": cfg["epsilon"],
+                       "step": "one attempt of every instance"},
+            "sim_years_per_hour": world * syh, "accepted_steps": acc, "rejected_fraction": rej / max(1, acc + rej),
+            "plain_fp64": {"per_geometry": plain, "aggregate_steps_per_s": plain_agg,
+                           "sim_years_per_hour_per_instance": plain_syh},
+            "speedup_vs_plain_fp64": {"steps_per_s": acc / elapsed / plain_agg,
+                                      "sim_years_per_hour": syh / plain_syh if plain_syh > 0 else None},
+            "autotune": report.strip().splitlines(), "clocks": clk.summary(), "gpu_launches": int(attempts * 20 + 3)}
+
+
 def learned_leg(args, local, sim20, sets, y0s, plain_window):
     """The learned step-size proposal: traces from seeded cfg1 runs train the
     perceptron on the device; it is then compared with the plain controller on
@@ -625,6 +694,8 @@ def main():
         out = run_reference(args, world, rank)
     elif args.workload == "ensemble":
         out = run_ensemble(args, world, rank, local)
+    elif args.workload == "cfg4":
+        out = run_cfg4(args, world, rank, local)
     elif args.workload == "coupled":
         import torch
         torch.cuda.set_device(local)
