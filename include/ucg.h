@@ -174,6 +174,51 @@ int ucg_get_state(ucg_ctx *ctx, double *y, double *time, double *dt_next,
    UCG_E_STEP_UNDERFLOW / UCG_E_NONFINITE as the device detects them. */
 int ucg_run(ucg_ctx *ctx, double t_end, long max_steps, long *steps);
 
+/* ---- observation points (buildO / exportPoints) ---------------------------- */
+
+/* Observation points (north, east, down), 3 per point: the
+   reference's observationPoint list (input.f90, "observation points").
+   Replaces any previous set and its O; stops a recording in progress. */
+int ucg_set_observation_points(ucg_ctx *ctx, int nobs, const double *x);
+/* Assemble O on the device: the displacement (north, east, down) at every
+   point for unit slip (strike, dip) of every patch and unit eigenstrain
+   (11, 12, 13, 22, 23, 33) of every volume, laid out 3 nobs rows x n columns
+   (row-major; the columns of K).  Replaces buildO (fortran/3d/src/greens.f90:
+   302-462) with computeDisplacementOkada92 / Nikkhoo15 / VerticalStrainVolume;
+   okada_mode as for ucg_assemble.  Stops a recording in progress. */
+int ucg_build_O(ucg_ctx *ctx, int okada_mode);
+/* number of points, values recorded per point (3, or 9 with volumes: total,
+   faulting, flow as viscouscycles' exportPoints writes them) and the device
+   time of the last ucg_build_O */
+int ucg_observation_info(ucg_ctx *ctx, int *nobs, int *per_point, double *build_ms);
+/* copy O (3 nobs x n doubles, row-major) to the host */
+int ucg_copy_O(ucg_ctx *ctx, double *O);
+/* Displacement at every point for the state y (3 nobs values each): the total
+   O u, and optionally (NULL to skip) the faulting and flow sets of
+   viscouscycles.f90:521-633.  As buildO does, a volume's down column counts
+   toward the faulting set, so the flow set's down component is zero. */
+int ucg_displacements(ucg_ctx *ctx, const double *y, double *d, double *d_fault, double *d_flow);
+
+/* ---- output recording (export / exportPoints) ------------------------------ */
+
+/* Record on the device, without host round trips, at the start of every
+   `every`-th accepted step of ucg_run / ucg_step: time, dt_done (the step just
+   taken; 0 at the first), max slip rate, the accepted-step count, then for each
+   listed element (0-based, patches then volumes) its state (7 or 12 values)
+   and its rate dydt in a slot of 24 (state at 0.., rate at 12..), then the
+   displacements at every observation point built with ucg_build_O (3 per
+   point, or 9 with volumes: total, faulting, flow; see ucg_displacements).
+   The observation set is the one built when recording starts.  Replaces the per-step formatted writes of export() and
+   exportPoints() (fortran/3d/src/ratestate.f90:405-537: time.txt, the
+   observation states, opts-*.dat).  Records go to a ring of `capacity`
+   records (0 stops recording); ucg_records drains them in order. */
+int ucg_record(ucg_ctx *ctx, int every, const int *elements, int nelem, long capacity);
+/* doubles per record with the current settings */
+long ucg_record_len(ucg_ctx *ctx);
+/* Copy up to max_records of the records not yet drained, oldest first;
+   *lost receives the records overwritten before they were drained. */
+int ucg_records(ucg_ctx *ctx, double *out, long max_records, long *n_records, long *lost);
+
 /* Number of kernel launches this context has issued (for launch accounting). */
 long ucg_launch_count(ucg_ctx *ctx);
 

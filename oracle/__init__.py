@@ -95,6 +95,10 @@ def lib():
         L.orc_step.restype = ctypes.c_int
         L.orc_step.argtypes = [ctypes.POINTER(_Model), _dp, _dp, _dp, _dp, ctypes.c_double,
                                ctypes.c_double, _dp, _lp, _dp]
+        L.orc_okada_disp.argtypes = [ctypes.c_int] + [ctypes.c_double] * 15 + [_dp]
+        L.orc_nw15_disp.argtypes = [ctypes.c_double] * 3 + [_dp] * 3 + [ctypes.c_double] * 5 + [_dp]
+        L.orc_bml17_disp_ned.argtypes = [ctypes.c_double] * 10 + [_dp, ctypes.c_double, ctypes.c_double, _dp]
+        L.orc_build_o.argtypes = [ctypes.POINTER(_Mesh), ctypes.c_int, _dp, _dp]
         _fp = ctypes.POINTER(ctypes.c_float)
         L.orc_mlp_nparam.restype = ctypes.c_int
         L.orc_mlp_loss_grad.argtypes = [_fp, _fp, _fp, _fp, ctypes.c_long, ctypes.c_int, _dp, _dp]
@@ -211,6 +215,14 @@ class Mesh:
     @property
     def mcols(self):
         return lib().orc_g_cols(ctypes.byref(self.m))
+
+    def build_o(self, xobs):
+        """O (3 nobs x n, row-major): displacement (north, east, down) at the points
+        for unit slip / eigenstrain on every source (greens.f90:302-462)."""
+        xobs = _d(xobs).reshape(-1, 3)
+        O = np.zeros((3 * len(xobs), self.n))
+        lib().orc_build_o(ctypes.byref(self.m), len(xobs), _ptr(xobs), _ptr(O))
+        return O
 
     def build_g(self, k0=0, k1=None):
         """Columns [k0,k1) of the reference G(n,m); returned as (k1-k0, n), i.e.
@@ -347,3 +359,40 @@ def mlp_predict(params, norm, X, fp16=True):
     L.orc_mlp_predict(params.ctypes.data_as(fp), norm.ctypes.data_as(fp), X.ctypes.data_as(fp), X.shape[0],
                       1 if fp16 else 0, _ptr(out))
     return out
+
+
+def nw15_disp_ref(x, P1, P2, P3, s, d, t, G, lam):
+    """The reference's own dispinhalfspace_ (compiled from its sources) with the
+    NED conventions of computeDisplacementNikkhoo15 (nikkhoo15.f90:324-367)."""
+    R = ref_lib()
+    if R is None:
+        return None
+    if not hasattr(R, "_disp_bound"):
+        R.dispinhalfspace_.argtypes = [_dp] + [ctypes.c_double] * 3 + [_dp] * 3 + [ctypes.c_double] * 4
+        R.dispinhalfspace_.restype = None
+        R._disp_bound = True
+    nu = lam / (lam + G) / 2.0
+    q = [_d([p[1], p[0], -p[2]]) for p in (P1, P2, P3)]
+    u = np.zeros(3)
+    R.dispinhalfspace_(_ptr(u), x[1], x[0], -x[2], _ptr(q[0]), _ptr(q[1]), _ptr(q[2]), s, -d, t, nu)
+    return np.array([u[1], u[0], -u[2]])
+
+
+def nw15_disp(x, P1, P2, P3, s, d, t, G, lam):
+    u = np.zeros(3)
+    lib().orc_nw15_disp(x[0], x[1], x[2], _ptr(_d(P1)), _ptr(_d(P2)), _ptr(_d(P3)), s, d, t, G, lam, _ptr(u))
+    return u
+
+
+def okada_disp(mode, x, q, L, W, strike, dip, s, d, t, G, lam):
+    u = np.zeros(3)
+    lib().orc_okada_disp(mode, x[0], x[1], x[2], q[0], q[1], q[2], L, W, strike, dip, s, d, t, G, lam, _ptr(u))
+    return u
+
+
+def bml17_disp(x, q, L, T, W, theta, eps, G, nu):
+    """Displacement (north, east, down) of a cuboid with eigenstrain eps
+    (strainvolume.f90:215-991, computeDisplacementVerticalStrainVolume)."""
+    u = np.zeros(3)
+    lib().orc_bml17_disp_ned(x[0], x[1], x[2], q[0], q[1], q[2], L, T, W, theta, _ptr(_d(eps)), G, nu, _ptr(u))
+    return u

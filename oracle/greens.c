@@ -166,3 +166,46 @@ void orc_dgemv_t(long n, long m, const double *G, const double *v, double *t, in
     }
     (void)threads;
 }
+
+/* buildO, greens.f90:302-462: O (3 nobs rows x n source DOFs, row-major; row
+   3k + c is the reference's column of observation point k, component c) holds
+   the displacement (north, east, down) at each point for unit slip (strike,
+   dip) on each patch and unit eigenstrain on each volume. */
+void orc_build_o(const orc_mesh *m, int nobs, const double *xobs, double *O)
+{
+    const long n = orc_g_rows(m);
+    const double nu = m->lambda / (m->lambda + m->mu) / 2.0;
+    for (int k = 0; k < nobs; k++) {
+        const double *x = xobs + 3L * k;
+        long col = 0;
+        for (long i = 0; i < m->nr; i++) {
+            for (int j = 0; j < 2; j++, col++) {
+                double u[3];
+                orc_okada_disp(m->okada_mode, x[0], x[1], x[2], m->rx[3 * i], m->rx[3 * i + 1], m->rx[3 * i + 2],
+                               m->rL[i], m->rW[i], m->rstrike[i], m->rdip[i], (double)(j == 0), (double)(j == 1),
+                               0.0, m->mu, m->lambda, u);
+                for (int c = 0; c < 3; c++) O[(3L * k + c) * n + col] = u[c];
+            }
+        }
+        for (long i = 0; i < m->nt; i++) {
+            const double *A = m->tv + 3L * (m->ti1[i] - 1);
+            const double *B = m->tv + 3L * (m->ti2[i] - 1);
+            const double *C = m->tv + 3L * (m->ti3[i] - 1);
+            for (int j = 0; j < 2; j++, col++) {
+                double u[3];
+                orc_nw15_disp(x[0], x[1], x[2], A, B, C, (double)(j == 0), (double)(j == 1), 0.0, m->mu,
+                              m->lambda, u);
+                for (int c = 0; c < 3; c++) O[(3L * k + c) * n + col] = u[c];
+            }
+        }
+        for (long i = 0; i < m->nv; i++) {
+            for (int j = 0; j < 6; j++, col++) {
+                double eps[6] = {0, 0, 0, 0, 0, 0}, u[3];
+                eps[j] = 1.0;
+                orc_bml17_disp_ned(x[0], x[1], x[2], m->vx[3 * i], m->vx[3 * i + 1], m->vx[3 * i + 2], m->vL[i],
+                                   m->vT[i], m->vW[i], m->vstrike[i], eps, m->mu, nu, u);
+                for (int c = 0; c < 3; c++) O[(3L * k + c) * n + col] = u[c];
+            }
+        }
+    }
+}

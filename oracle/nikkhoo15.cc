@@ -371,6 +371,33 @@ extern "C" void orc_nw15_stress(double x1, double x2, double x3, const double P1
     sig[5] = e[5];
 }
 
+/* computeDisplacementNikkhoo15 (nikkhoo15.f90:324-367) over TDdispHS
+   (DispInHalfSpace.c:27-147): the values of the same displacement fields whose
+   gradients give the stress; NED in and out, dip slip negated. */
+extern "C" void orc_nw15_disp(double x1, double x2, double x3, const double P1[3], const double P2[3],
+                              const double P3[3], double s, double d, double t, double G, double lambda,
+                              double u[3])
+{
+    const double nu = lambda / (lambda + G) / 2.0;
+    const double Q1[3] = {P1[1], P1[0], -P1[2]}, Q2[3] = {P2[1], P2[0], -P2[2]}, Q3[3] = {P3[1], P3[0], -P3[2]};
+    const double M1[3] = {Q1[0], Q1[1], -Q1[2]}, M2[3] = {Q2[0], Q2[1], -Q2[2]}, M3[3] = {Q3[0], Q3[1], -Q3[2]};
+    D3 Xd[3] = {D3::var(x2, 0), D3::var(x1, 1), D3::var(-x3, 2)};
+    V3 ms = td_disp_fs(Xd, Q1, Q2, Q3, s, -d, t, nu);
+    V3 hs = td_disp_harm(Xd, Q1, Q2, Q3, s, -d, t, nu);
+    V3 is = td_disp_fs(Xd, M1, M2, M3, s, -d, t, nu);
+    const bool surf = M1[2] == 0.0 && M2[2] == 0.0 && M3[2] == 0.0;
+    double e[3];
+    for (int k = 0; k < 3; k++) {
+        double iv = is.c[k].v;
+        if (surf && k == 2) iv = -iv;
+        e[k] = ms.c[k].v + hs.c[k].v + iv;
+        if (surf) e[k] = -e[k];
+    }
+    u[0] = e[1];
+    u[1] = e[0];
+    u[2] = -e[2];
+}
+
 /* computeReferenceSystemNikkhoo15 / Stuart97, nikkhoo15.f90:50-101 */
 extern "C" void orc_tri_frames(int ns, int nve, const double *v, const int *i1, const int *i2,
                                const int *i3, double *sv, double *dv, double *nv, double *xc)

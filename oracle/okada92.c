@@ -526,3 +526,33 @@ void orc_okada_stress(int mode, double x1, double x2, double x3,
     sig[4] = 2.0 * G * e23;
     sig[5] = lambda * ekk + 2.0 * G * e33;
 }
+
+/* computeDisplacementOkada92, okada92.f90:230-298: displacement (north, east,
+   down) at x from slip (s, d, t) on a rectangle; zero where DC3D reports a
+   singular edge */
+void orc_okada_disp(int mode, double x1, double x2, double x3, double q1, double q2, double q3,
+                    double L, double W, double strike, double dipd, double s, double d, double t,
+                    double G, double lambda, double u[3])
+{
+    const double RAD2DEG = 57.29577951308232;
+    const int r32 = (mode == ORC_OKADA_REF32IO);
+#define CV(v) (r32 ? f32(v) : (v))
+    double alpha = CV((lambda + G) / (lambda + 2.0 * G));
+    double z = CV(-x3);
+    double csst = cos(strike), ssst = sin(strike);
+    double x = CV((x1 - q1) * csst + (x2 - q2) * ssst);
+    double y = CV((x1 - q1) * ssst - (x2 - q2) * csst);
+    double depth = CV(q3);
+    double dip = CV(dipd * RAD2DEG);
+    double al2 = CV(L), aw1 = -CV(W);
+    double disl1 = CV(s), disl2 = CV(d), disl3 = CV(t);
+#undef CV
+    double o[12];
+    if (orc_dc3d(mode, alpha, x, y, z, depth, dip, 0.0, al2, aw1, 0.0, disl1, disl2, disl3, o) != 0) {
+        u[0] = u[1] = u[2] = 0.0;
+        return;
+    }
+    u[0] = o[0] * csst + o[1] * ssst;
+    u[1] = o[0] * ssst - o[1] * csst;
+    u[2] = -o[2];
+}

@@ -118,6 +118,17 @@ long orc_work_len(const orc_model *md);
    build only; 0 otherwise). */
 double orc_flop_count(void);
 
+/* displacements (north, east, down) for the observation points (buildO) */
+void orc_okada_disp(int mode, double x1, double x2, double x3, double q1, double q2, double q3,
+                    double L, double W, double strike, double dipd, double s, double d, double t,
+                    double G, double lambda, double u[3]);
+void orc_nw15_disp(double x1, double x2, double x3, const double P1[3], const double P2[3],
+                   const double P3[3], double s, double d, double t, double G, double lambda, double u[3]);
+void orc_bml17_disp_ned(double x1, double x2, double x3, double q1, double q2, double q3, double L,
+                        double T, double W, double theta, const double eps[6], double G, double nu,
+                        double u[3]);
+void orc_build_o(const orc_mesh *m, int nobs, const double *xobs, double *O);
+
 /* step-size perceptron (mlp.c): loss and gradient, predictions */
 int  orc_mlp_nparam(void);
 void orc_mlp_loss_grad(const float *params, const float *norm, const float *X, const float *Y, long n,

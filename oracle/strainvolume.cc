@@ -143,3 +143,19 @@ extern "C" void orc_bml17_disp(double x1p, double x2p, double x3, double q3, dou
     disp(x1p, x2p, x3, q3, L, T, W, eps, G, nu, ux);
     for (int i = 0; i < 3; i++) u[i] = (double)ux[i];
 }
+
+/* computeDisplacementVerticalStrainVolume, strainvolume.f90:215-991:
+   displacement (north, east, down) at x from eigenstrain eps (cuboid frame) */
+extern "C" void orc_bml17_disp_ned(double x1, double x2, double x3, double q1, double q2, double q3, double L,
+                                   double T, double W, double theta, const double eps[6], double G, double nu,
+                                   double u[3])
+{
+    const double ct = std::cos(theta), st = std::sin(theta);
+    const double x1p = (x1 - q1) * ct + (x2 - q2) * st;
+    const double x2p = -(x1 - q1) * st + (x2 - q2) * ct;
+    xreal up[3];
+    disp(x1p, x2p, x3, q3, L, T, W, eps, G, nu, up);
+    u[0] = (double)up[0] * ct - (double)up[1] * st;
+    u[1] = (double)up[0] * st + (double)up[1] * ct;
+    u[2] = (double)up[2];
+}

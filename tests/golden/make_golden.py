@@ -10,6 +10,11 @@ does (fortran/3d/src/nikkhoo15.f90:120-163) and writes:
   nw15_mesh_G.npz  the full interaction matrix in the reference layout
                    (greens.f90:176-218 traction rows) for a 6 x 5 (60-triangle)
                    curved-megathrust mesh from unicycle_b200.configs.cfg2
+  nw15_disp_pairs.npz  displacement (north, east, down) from dispinhalfspace_
+                   called as computeDisplacementNikkhoo15 does
+                   (nikkhoo15.f90:324-367), seeded triangle/point pairs with
+                   surface-reaching triangles and surface points, unit strike
+                   and unit dip slip
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -51,6 +56,19 @@ def pairs(n=300, seed=11):
     return P, X, S
 
 
+def disp_pairs(n=200, seed=13):
+    rng = np.random.default_rng(seed)
+    P = rng.uniform([-5e3, -5e3, 0.0], [5e3, 5e3, 8e3], size=(n, 3, 3))
+    P[: n // 10, :, 2] = np.maximum(P[: n // 10, :, 2] - 8e3, 0.0)
+    X = rng.uniform([-10e3, -10e3, 0.0], [10e3, 10e3, 12e3], size=(n, 3))
+    X[n // 2:, 2] = 0.0   # half of the points on the free surface (GPS-like)
+    U = np.zeros((n, 2, 3))
+    for k in range(n):
+        for j, (s, d) in enumerate(((1.0, 0.0), (0.0, 1.0))):
+            U[k, j] = oracle.nw15_disp_ref(X[k], P[k, 0], P[k, 1], P[k, 2], s, d, 0.0, MU, LAM)
+    return P, X, U
+
+
 def mesh_G(nx=6, nz=5):
     c = configs.cfg2(nx=nx, nz=nz)
     i1, i2, i3, v = c["mesh"]["tri"]
@@ -75,6 +93,8 @@ def main():
     np.savez_compressed(os.path.join(HERE, "nw15_pairs.npz"), P=P, X=X, S=S, mu=MU, lam=LAM)
     (i1, i2, i3, v), G = mesh_G()
     np.savez_compressed(os.path.join(HERE, "nw15_mesh_G.npz"), i1=i1, i2=i2, i3=i3, v=v, G=G, mu=MU, lam=LAM)
+    P, X, U = disp_pairs()
+    np.savez_compressed(os.path.join(HERE, "nw15_disp_pairs.npz"), P=P, X=X, U=U, mu=MU, lam=LAM)
     print("wrote", os.listdir(HERE))
 
 

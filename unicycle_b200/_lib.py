@@ -68,6 +68,14 @@ SIGNATURES = {
     "ucg_set_state": (_i, [_vp, _dp, _d, _d]),
     "ucg_get_state": (_i, [_vp, _dp, _dp, _dp, _lp, _lp]),
     "ucg_run": (_i, [_vp, _d, _l, _lp]),
+    "ucg_set_observation_points": (_i, [_vp, _i, _dp]),
+    "ucg_build_O": (_i, [_vp, _i]),
+    "ucg_observation_info": (_i, [_vp, _ip, _ip, _dp]),
+    "ucg_copy_O": (_i, [_vp, _dp]),
+    "ucg_displacements": (_i, [_vp, _dp, _dp, _dp, _dp]),
+    "ucg_record": (_i, [_vp, _i, _ip, _i, _l]),
+    "ucg_record_len": (_l, [_vp]),
+    "ucg_records": (_i, [_vp, _dp, _l, _lp, _lp]),
     "ucg_launch_count": (_l, [_vp]),
     "ucg_stream": (_vp, [_vp]),
     "ucg_profile_traction": (_i, [_vp, _i, _dp]),

@@ -232,6 +232,84 @@ __global__ void __launch_bounds__(128) k_assemble_vol(double *__restrict__ K, lo
     }
 }
 
+// ---- observation points: the displacement kernels O (buildO) ---------------------
+//
+// O is row-major with 3 nobs rows (north, east, down per point) and n columns
+// (the source DOFs of K); row 3k + c is column (k, c) of the reference's
+// O(n, 3 nobs) (fortran/3d/src/greens.f90:302-462).  Same launch shape as K:
+// one thread per source, the grid's y dimension strides over points, and each
+// row store of a warp is one coalesced segment.
+
+template <bool R32>
+__global__ void __launch_bounds__(128) k_observe_rect(double *__restrict__ O, long n, long col0,
+        const double *__restrict__ obs, int nobs, const double *__restrict__ src, int ns, OkMed med)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    double sr[RS_SIZE];
+#pragma unroll
+    for (int f = 0; f < RS_SIZE; f++) sr[f] = __ldg(src + (long)f * ns + j);
+    OkDip dp;
+    dp.sd = sr[RS_SD]; dp.cd = sr[RS_CD]; dp.sdsd = sr[RS_SDSD]; dp.cdcd = sr[RS_CDCD];
+    dp.sdcd = sr[RS_SDCD];
+    const double csst = sr[RS_CS], ssst = sr[RS_SS];
+    for (int k = blockIdx.y; k < nobs; k += gridDim.y) {
+        const double x1 = __ldg(obs + 3L * k), x2 = __ldg(obs + 3L * k + 1), x3 = __ldg(obs + 3L * k + 2);
+        // okada92.f90:251-290
+        double x = (x1 - sr[RS_Q1]) * csst + (x2 - sr[RS_Q2]) * ssst;
+        double y = (x1 - sr[RS_Q1]) * ssst - (x2 - sr[RS_Q2]) * csst;
+        double z = -x3;
+        if (R32) {
+            x = (double)__double2float_rn(x);
+            y = (double)__double2float_rn(y);
+            z = (double)__double2float_rn(z);
+        }
+        double us[3], ud[3];
+        ok_dc3d_disp<R32>(med, dp, x, y, z, sr[RS_DEPTH], sr[RS_AL2], sr[RS_AW1], us, ud);
+        const double oS[3] = {us[0] * csst + us[1] * ssst, us[0] * ssst - us[1] * csst, -us[2]};
+        const double oD[3] = {ud[0] * csst + ud[1] * ssst, ud[0] * ssst - ud[1] * csst, -ud[2]};
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            *reinterpret_cast<double2 *>(O + (3L * k + c) * n + col0 + 2L * j) = make_double2(oS[c], oD[c]);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_observe_tri(double *__restrict__ O, long n, long col0,
+        const double *__restrict__ obs, int nobs, const double *__restrict__ rec, int ns, double nu)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    NwRec R{rec + j, (long)ns};
+    for (int k = blockIdx.y; k < nobs; k += gridDim.y) {
+        const double xr[3] = {__ldg(obs + 3L * k), __ldg(obs + 3L * k + 1), __ldg(obs + 3L * k + 2)};
+        double uS[3], uD[3];
+        nw_pair_disp(xr, R, nu, uS, uD);
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            *reinterpret_cast<double2 *>(O + (3L * k + c) * n + col0 + 2L * j) = make_double2(uS[c], uD[c]);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_observe_vol(double *__restrict__ O, long n, long col0,
+        const double *__restrict__ obs, int nobs, const double *__restrict__ rec, int ns, double mu, double nu)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    SvRec R{rec + j, (long)ns};
+    for (int k = blockIdx.y; k < nobs; k += gridDim.y) {
+        const double xr[3] = {__ldg(obs + 3L * k), __ldg(obs + 3L * k + 1), __ldg(obs + 3L * k + 2)};
+        double u[6][3];
+        sv_pair_disp(xr, R, mu, nu, u);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double2 *p = reinterpret_cast<double2 *>(O + (3L * k + c) * n + col0 + 6L * j);
+            p[0] = make_double2(u[0][c], u[1][c]);
+            p[1] = make_double2(u[2][c], u[3][c]);
+            p[2] = make_double2(u[4][c], u[5][c]);
+        }
+    }
+}
+
 // ---- host side -----------------------------------------------------------------
 
 static float f32(double v) { return (float)v; }
@@ -436,6 +514,88 @@ int assemble_matrix(ucg_ctx *c, int okada_mode)
     if (dsrc) cudaFree(dsrc);
     c->okada_mode = okada_mode;
     c->assembled = true;
+    return UCG_OK;
+}
+
+int assemble_observation(ucg_ctx *c, int okada_mode)
+{
+    const int np = c->nr + c->nt;
+    const long n = 2L * np + 6L * c->nv;
+    const int nobs = (int)(c->obs_x.size() / 3);
+    if (np + c->nv == 0 || nobs == 0) return UCG_E_BADARG;
+    UCG_CUDA(cudaSetDevice(c->device));
+    const size_t bytes = sizeof(double) * (size_t)n * 3 * (size_t)nobs;
+    if (c->O && c->O_bytes != bytes) {
+        cudaFree(c->O);
+        c->O = nullptr;
+    }
+    if (!c->O) {
+        cudaError_t e = cudaMalloc(&c->O, bytes);
+        if (e != cudaSuccess) {
+            c->O = nullptr;
+            return cuda_fail(c, e, "cudaMalloc(O)");
+        }
+        c->O_bytes = bytes;
+    }
+    if (c->obs_dev) cudaFree(c->obs_dev);
+    c->obs_dev = nullptr;
+    UCG_CUDA(cudaMalloc(&c->obs_dev, sizeof(double) * c->obs_x.size()));
+    UCG_CUDA(cudaMemcpyAsync(c->obs_dev, c->obs_x.data(), sizeof(double) * c->obs_x.size(),
+                             cudaMemcpyHostToDevice, c->stream));
+    const int TPB = 128;
+    const int gy = nobs < 65535 ? nobs : 65535;
+    double *dsrc = nullptr;
+    auto upload = [&](const std::vector<double> &h) -> int {
+        if (dsrc) { cudaStreamSynchronize(c->stream); cudaFree(dsrc); dsrc = nullptr; }
+        UCG_CUDA(cudaMalloc(&dsrc, sizeof(double) * h.size()));
+        UCG_CUDA(cudaMemcpyAsync(dsrc, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->stream));
+        return UCG_OK;
+    };
+    int rc;
+    cudaEvent_t ev[2];
+    for (cudaEvent_t &e : ev) UCG_CUDA(cudaEventCreate(&e));
+    UCG_CUDA(cudaEventRecord(ev[0], c->stream));
+    if (c->nr) {
+        std::vector<double> s;
+        build_rect_sources(c, okada_mode, s);
+        if ((rc = upload(s))) return rc;
+        const double alpha_d = (c->lambda + c->mu) / (c->lambda + 2.0 * c->mu);
+        const double alpha = okada_mode == UCG_OKADA_REF32IO ? (double)f32(alpha_d) : alpha_d;
+        dim3 grid((c->nr + TPB - 1) / TPB, gy);
+        if (okada_mode == UCG_OKADA_REF32IO)
+            k_observe_rect<true><<<grid, TPB, 0, c->stream>>>(c->O, n, 0, c->obs_dev, nobs, dsrc, c->nr, ok_med(alpha));
+        else
+            k_observe_rect<false><<<grid, TPB, 0, c->stream>>>(c->O, n, 0, c->obs_dev, nobs, dsrc, c->nr, ok_med(alpha));
+        c->launches.count++;
+        UCG_CUDA(cudaGetLastError());
+    }
+    if (c->nt) {
+        std::vector<double> s;
+        build_tri_sources(c, s);
+        if ((rc = upload(s))) return rc;
+        dim3 grid((c->nt + TPB - 1) / TPB, gy);
+        k_observe_tri<<<grid, TPB, 0, c->stream>>>(c->O, n, 2L * c->nr, c->obs_dev, nobs, dsrc, c->nt,
+                                                   c->lambda / (c->lambda + c->mu) / 2.0);
+        c->launches.count++;
+        UCG_CUDA(cudaGetLastError());
+    }
+    if (c->nv) {
+        std::vector<double> s;
+        build_vol_sources(c, s);
+        if ((rc = upload(s))) return rc;
+        dim3 grid((c->nv + TPB - 1) / TPB, gy);
+        k_observe_vol<<<grid, TPB, 0, c->stream>>>(c->O, n, 2L * np, c->obs_dev, nobs, dsrc, c->nv, c->mu,
+                                                   c->lambda / (c->lambda + c->mu) / 2.0);
+        c->launches.count++;
+        UCG_CUDA(cudaGetLastError());
+    }
+    UCG_CUDA(cudaEventRecord(ev[1], c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) c->obs_ms = ms;
+    for (cudaEvent_t &e : ev) cudaEventDestroy(e);
+    if (dsrc) cudaFree(dsrc);
+    c->O_ready = true;
     return UCG_OK;
 }
 

@@ -137,4 +137,32 @@ __device__ __forceinline__ Dd1 dsqrt(Dd1 a)
 __device__ __forceinline__ Dd1 dlog_g(Dd1 a) { return Dd1{0.0, a.d / a.v}; }
 __device__ __forceinline__ Dd1 datan_g(Dd1 a) { return Dd1{0.0, a.d / (1.0 + a.v * a.v)}; }
 
+// Plain value: the same closed forms evaluated for the displacement itself
+// (observation-point displacements).  The "gradient-only" forms of the dual
+// types above skip the value of a logarithm or arctangent; for this type the
+// value is all there is, so they evaluate it.
+struct Dv {
+    double v;
+    Dv() = default;
+    __host__ __device__ constexpr Dv(double c) : v(c) {}
+};
+__device__ __forceinline__ Dv operator+(Dv a, Dv b) { return Dv{a.v + b.v}; }
+__device__ __forceinline__ Dv operator-(Dv a, Dv b) { return Dv{a.v - b.v}; }
+__device__ __forceinline__ Dv operator-(Dv a) { return Dv{-a.v}; }
+__device__ __forceinline__ Dv operator*(Dv a, Dv b) { return Dv{a.v * b.v}; }
+__device__ __forceinline__ Dv operator+(Dv a, double c) { return Dv{a.v + c}; }
+__device__ __forceinline__ Dv operator+(double c, Dv a) { return Dv{c + a.v}; }
+__device__ __forceinline__ Dv operator-(Dv a, double c) { return Dv{a.v - c}; }
+__device__ __forceinline__ Dv operator-(double c, Dv a) { return Dv{c - a.v}; }
+__device__ __forceinline__ Dv operator*(Dv a, double c) { return Dv{a.v * c}; }
+__device__ __forceinline__ Dv operator*(double c, Dv a) { return Dv{c * a.v}; }
+__device__ __forceinline__ Dv rcp(Dv a) { return Dv{1.0 / a.v}; }
+__device__ __forceinline__ Dv operator/(Dv a, Dv b) { return Dv{a.v / b.v}; }
+__device__ __forceinline__ Dv operator/(Dv a, double c) { return Dv{a.v / c}; }
+__device__ __forceinline__ Dv operator/(double c, Dv a) { return Dv{c / a.v}; }
+__device__ __forceinline__ Dv dsqrt(Dv a) { return Dv{sqrt(a.v)}; }
+__device__ __forceinline__ Dv dlog_g(Dv a) { return Dv{log(a.v)}; }
+__device__ __forceinline__ Dv datan_g(Dv a) { return Dv{atan(a.v)}; }
+__device__ __forceinline__ Dv datan2_g(Dv y, Dv x) { return Dv{atan2(y.v, x.v)}; }
+
 }  // namespace ucg

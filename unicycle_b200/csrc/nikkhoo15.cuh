@@ -231,35 +231,36 @@ __device__ inline int nw_trimode(double x, double y, double z, double p1a, doubl
 // Angular dislocation (AngDisDisp without tensile term, DispInHalfSpace.c:541-575)
 // plus the TDSetupD rotation (DispInHalfSpace.c:419-460).  Adds the TD-frame
 // displacement of both modes into dS, dD.
-__device__ inline void nw_angdis(Dd x, Dd y, Dd z, double cosA, double sinA, double nu,
+template <class T>
+__device__ inline void nw_angdis(T x, T y, T z, double cosA, double sinA, double nu,
                                  double tvy, double tvz, double svy, double svz, double bS_y,
-                                 double bS_z, double bD_y, double bD_z, Dd dS[3], Dd dD[3])
+                                 double bS_z, double bD_y, double bD_z, T dS[3], T dD[3])
 {
     const double a00 = svz, a01 = -svy, a10 = svy, a11 = svz;
-    Dd ty = y - tvy, tz = z - tvz;
-    Dd y1 = a00 * ty + a01 * tz;
-    Dd z1 = a10 * ty + a11 * tz;
-    Dd eta = y1 * cosA - z1 * sinA;
-    Dd zeta = y1 * sinA + z1 * cosA;
-    Dd r = dsqrt(x * x + y1 * y1 + z1 * z1);
-    Dd rmz = r - z1, rmzeta = r - zeta;
-    Dd irz = rcp(rmz), irze = rcp(rmzeta), ir = rcp(r);
-    Dd lz = dlog_g(rmz), lzeta = dlog_g(rmzeta);
+    T ty = y - tvy, tz = z - tvz;
+    T y1 = a00 * ty + a01 * tz;
+    T z1 = a10 * ty + a11 * tz;
+    T eta = y1 * cosA - z1 * sinA;
+    T zeta = y1 * sinA + z1 * cosA;
+    T r = dsqrt(x * x + y1 * y1 + z1 * z1);
+    T rmz = r - z1, rmzeta = r - zeta;
+    T irz = rcp(rmz), irze = rcp(rmzeta), ir = rcp(r);
+    T lz = dlog_g(rmz), lzeta = dlog_g(rmzeta);
     const double k = 1.0 / 8.0 / 3.141592653589793 / (1.0 - nu);
     const double n12 = 1.0 - 2.0 * nu;
-    Dd x2 = x * x;
+    T x2 = x * x;
     // basis for by (F_y) and bz (F_z), ADCS components (u, v, w)
-    Dd uy = k * (x2 * cosA * ir * irze - x2 * ir * irz - n12 * (cosA * lzeta - lz));
-    Dd vy = k * x * (y1 * cosA * ir * irze - sinA * cosA * irze - y1 * ir * irz);
-    Dd wy = k * x * (z1 * cosA * ir * irze - cosA * cosA * irze + ir);
-    Dd uz = sinA * k * (n12 * lzeta - x2 * ir * irze);
-    Dd vz = sinA * k * x * (sinA * irze - y1 * ir * irze);
-    Dd wz = sinA * k * x * (cosA * irze - z1 * ir * irze);
+    T uy = k * (x2 * cosA * ir * irze - x2 * ir * irz - n12 * (cosA * lzeta - lz));
+    T vy = k * x * (y1 * cosA * ir * irze - sinA * cosA * irze - y1 * ir * irz);
+    T wy = k * x * (z1 * cosA * ir * irze - cosA * cosA * irze + ir);
+    T uz = sinA * k * (n12 * lzeta - x2 * ir * irze);
+    T vz = sinA * k * x * (sinA * irze - y1 * ir * irze);
+    T wz = sinA * k * x * (cosA * irze - z1 * ir * irze);
     // modes: (by1, bz1) = A2 (by, bz)
     const double byS = a00 * bS_y + a01 * bS_z, bzS = a10 * bS_y + a11 * bS_z;
     const double byD = a00 * bD_y + a01 * bD_z, bzD = a10 * bD_y + a11 * bD_z;
-    Dd u0S = byS * uy + bzS * uz, u1S = byS * vy + bzS * vz, u2S = byS * wy + bzS * wz;
-    Dd u0D = byD * uy + bzD * uz, u1D = byD * vy + bzD * vz, u2D = byD * wy + bzD * wz;
+    T u0S = byS * uy + bzS * uz, u1S = byS * vy + bzS * vz, u2S = byS * wy + bzS * wz;
+    T u0D = byD * uy + bzD * uz, u1D = byD * vy + bzD * vz, u2D = byD * wy + bzD * wz;
     // back to the TD frame with the transpose of A2
     dS[0] = dS[0] + u0S;
     dS[1] = dS[1] + (a00 * u1S + a10 * u2S);
@@ -269,21 +270,23 @@ __device__ inline void nw_angdis(Dd x, Dd y, Dd z, double cosA, double sinA, dou
     dD[2] = dD[2] + (a01 * u1D + a11 * u2D);
 }
 
-// TDdispFS (DispInHalfSpace.c:153-302), EFCS displacement gradients of both modes.
+// TDdispFS (DispInHalfSpace.c:153-302), EFCS displacements of both modes: their
+// gradients for the dual types, their values for Dv.
 // Returns false when the point lies on a TD side (reference result: NaN).
-__device__ inline bool nw_td_fs(const Dd X[3], const NwRec &R, int o, double nu, Dd uS[3], Dd uD[3])
+template <class T>
+__device__ inline bool nw_td_fs(const T X[3], const NwRec &R, int o, double nu, T uS[3], T uD[3])
 {
-    Dd dX0 = X[0] - R[o + TD_P2], dX1 = X[1] - R[o + TD_P2 + 1], dX2 = X[2] - R[o + TD_P2 + 2];
-    Dd x = R[o + TD_N] * dX0 + R[o + TD_N + 1] * dX1 + R[o + TD_N + 2] * dX2;
-    Dd y = R[o + TD_S] * dX0 + R[o + TD_S + 1] * dX1 + R[o + TD_S + 2] * dX2;
-    Dd z = R[o + TD_D] * dX0 + R[o + TD_D + 1] * dX1 + R[o + TD_D + 2] * dX2;
+    T dX0 = X[0] - R[o + TD_P2], dX1 = X[1] - R[o + TD_P2 + 1], dX2 = X[2] - R[o + TD_P2 + 2];
+    T x = R[o + TD_N] * dX0 + R[o + TD_N + 1] * dX1 + R[o + TD_N + 2] * dX2;
+    T y = R[o + TD_S] * dX0 + R[o + TD_S + 1] * dX1 + R[o + TD_S + 2] * dX2;
+    T z = R[o + TD_D] * dX0 + R[o + TD_D + 1] * dX1 + R[o + TD_D + 2] * dX2;
     const double p1y = R[o + TD_P1], p1z = R[o + TD_P1 + 1];
     const double p3y = R[o + TD_P3], p3z = R[o + TD_P3 + 1];
     const int mode = nw_trimode(y.v, z.v, x.v, p1y, p1z, p3y, p3z);
     if (mode == 0) return false;
     const double sg1 = (mode == 1) ? -1.0 : 1.0;   // sign on e13 (corner 1)
     const double sg2 = (mode == 1) ? 1.0 : -1.0;   // sign on e12, e23 (corners 2, 3)
-    Dd dS[3] = {dd(0), dd(0), dd(0)}, dD[3] = {dd(0), dd(0), dd(0)};
+    T dS[3] = {T(0.0), T(0.0), T(0.0)}, dD[3] = {T(0.0), T(0.0), T(0.0)};
     // modes in the TD frame: strike (by=1, bz=0), dip (by=0, bz=-1)
     nw_angdis(x, y, z, R[o + TD_CS + 0], R[o + TD_CS + 1], nu, p1y, p1z, sg1 * R[o + TD_E13],
               sg1 * R[o + TD_E13 + 1], 1.0, 0.0, 0.0, -1.0, dS, dD);
@@ -291,17 +294,17 @@ __device__ inline bool nw_td_fs(const Dd X[3], const NwRec &R, int o, double nu,
               sg2 * R[o + TD_E12 + 1], 1.0, 0.0, 0.0, -1.0, dS, dD);
     nw_angdis(x, y, z, R[o + TD_CS + 4], R[o + TD_CS + 5], nu, p3y, p3z, sg2 * R[o + TD_E23],
               sg2 * R[o + TD_E23 + 1], 1.0, 0.0, 0.0, -1.0, dS, dD);
-    // Burgers function of the TD (solid angle), gradient only
-    Dd ax = -x, ay = p1y - y, az = p1z - z;
-    Dd bx = -x, by = -y, bz = -z;
-    Dd cx = -x, cy = p3y - y, cz = p3z - z;
-    Dd na = dsqrt(ax * ax + ay * ay + az * az);
-    Dd nb = dsqrt(bx * bx + by * by + bz * bz);
-    Dd nc = dsqrt(cx * cx + cy * cy + cz * cz);
-    Dd num = ax * (by * cz - bz * cy) - ay * (bx * cz - bz * cx) + az * (bx * cy - by * cx);
-    Dd den = na * nb * nc + (ax * bx + ay * by + az * bz) * nc + (ax * cx + ay * cy + az * cz) * nb
+    // Burgers function of the TD (solid angle)
+    T ax = -x, ay = p1y - y, az = p1z - z;
+    T bx = -x, by = -y, bz = -z;
+    T cx = -x, cy = p3y - y, cz = p3z - z;
+    T na = dsqrt(ax * ax + ay * ay + az * az);
+    T nb = dsqrt(bx * bx + by * by + bz * bz);
+    T nc = dsqrt(cx * cx + cy * cy + cz * cz);
+    T num = ax * (by * cz - bz * cy) - ay * (bx * cz - bz * cx) + az * (bx * cy - by * cx);
+    T den = na * nb * nc + (ax * bx + ay * by + az * bz) * nc + (ax * cx + ay * cy + az * cz) * nb
            + (bx * cx + by * cy + bz * cz) * na;
-    Dd Fi = datan2_g(num, den) * (-2.0 / 4.0 / 3.141592653589793);
+    T Fi = datan2_g(num, den) * (-2.0 / 4.0 / 3.141592653589793);
     dS[1] = dS[1] + Fi;          // by = 1
     dD[2] = dD[2] - Fi;          // bz = -1
     for (int k = 0; k < 3; k++) {
@@ -313,7 +316,7 @@ __device__ inline bool nw_td_fs(const Dd X[3], const NwRec &R, int o, double nu,
 }
 
 // AngDisDispFSC (DispInHalfSpace.c:577-617) for the two slip modes.
-// sc: sinB, cosB, cotB, cot(B/2); b: (b1,b2,b3) per mode (6); gradient only.
+// sc: sinB, cosB, cotB, cot(B/2); b: (b1,b2,b3) per mode (6).
 template <class Dd>
 __device__ inline void nw_fsc(Dd y1, Dd y2, Dd y3, double sinB, double cosB, double cotB,
                               double coth, const double b[6], double nu, double a, Dd oS[3],
@@ -516,6 +519,37 @@ __device__ inline void nw_part_stress(const double xr[3], const NwRec &R, const 
     if (PART == 1 && R[NW_SURF] != 0.0) { eS[4] = -eS[4]; eS[5] = -eS[5]; eD[4] = -eD[4]; eD[5] = -eD[5]; }
     nw_to_ned(eS, sS);
     nw_to_ned(eD, sD);
+}
+
+// Displacement (north, east, down) at xr (NED) for unit strike slip (uS) and
+// unit dip slip (uD) of one TD, as dispinhalfspace_ called by
+// computeDisplacementNikkhoo15 (nikkhoo15.f90:324-367; DispInHalfSpace.c:
+// 64-151): main TD + image TD (vertical component negated when all vertices
+// lie at z = 0) + the three free-surface sides, the whole sum negated for such
+// surface TDs, then ENU -> NED.  A point on a TD side gives NaN, as in the
+// reference.
+__device__ inline void nw_pair_disp(const double xr[3], const NwRec &R, double nu, double uS[3], double uD[3])
+{
+    const Dv X[3] = {Dv(xr[1]), Dv(xr[0]), Dv(-xr[2])};
+    Dv mS[3] = {Dv(0.0), Dv(0.0), Dv(0.0)}, mD[3] = {Dv(0.0), Dv(0.0), Dv(0.0)};
+    Dv iS[3] = {Dv(0.0), Dv(0.0), Dv(0.0)}, iD[3] = {Dv(0.0), Dv(0.0), Dv(0.0)};
+    Dv hS[3] = {Dv(0.0), Dv(0.0), Dv(0.0)}, hD[3] = {Dv(0.0), Dv(0.0), Dv(0.0)};
+    if (!nw_td_fs(X, R, NW_MAIN, nu, mS, mD) || !nw_td_fs(X, R, NW_IMG, nu, iS, iD)) {
+        for (int k = 0; k < 3; k++) { uS[k] = nan(""); uD[k] = nan(""); }
+        return;
+    }
+    const bool surf = R[NW_SURF] != 0.0;
+    if (surf) { iS[2] = -iS[2]; iD[2] = -iD[2]; }
+#pragma unroll 1
+    for (int side = 0; side < 3; side++) nw_side<Dv>(X, R, NW_FS + side * FS_SIZE, nu, hS, hD);
+    double eS[3], eD[3];
+    for (int k = 0; k < 3; k++) {
+        eS[k] = (mS[k] + iS[k] + hS[k]).v;
+        eD[k] = (mD[k] + iD[k] + hD[k]).v;
+        if (surf) { eS[k] = -eS[k]; eD[k] = -eD[k]; }
+    }
+    uS[0] = eS[1]; uS[1] = eS[0]; uS[2] = -eS[2];
+    uD[0] = eD[1]; uD[1] = eD[0]; uD[2] = -eD[2];
 }
 
 }  // namespace ucg

@@ -393,6 +393,153 @@ singular:
     return false;
 }
 
+// ---- displacement (observation points) ------------------------------------------
+
+// The displacement entries DU(1..3) of parts A/B/C need three more corner
+// quantities of DCCON2 (dc3d.f:596-665): TT, ALX, ALE.
+struct OkLogs {
+    double tt, alx, ale;
+};
+
+__device__ inline OkLogs ok_logs(const OkCorner &c, int kxi, int ket)
+{
+    OkLogs l;
+    l.tt = (c.q == 0.0) ? 0.0 : atan(c.xi * c.et / (c.q * c.r));
+    l.alx = (kxi == 1) ? -log(c.r - c.xi) : log(c.r + c.xi);
+    l.ale = (ket == 1) ? -log(c.r - c.et) : log(c.r + c.et);
+    return l;
+}
+
+// Part A (dc3d.f:200-282) DU(1..3), strike (s) and dip (d) slip.
+__device__ inline void ok_part_a_disp(const OkCorner &c, const OkLogs &l, const OkMed &m, double s[3],
+                                      double d[3])
+{
+    const double qx = c.q * c.x11, qy = c.q * c.y11;
+    s[0] = OK_K * (l.tt / 2.0 + m.alp2 * c.xi * qy);
+    s[1] = OK_K * (m.alp2 * c.q / c.r);
+    s[2] = OK_K * (m.alp1 * l.ale - m.alp2 * c.q * qy);
+    d[0] = OK_K * (m.alp2 * c.q / c.r);
+    d[1] = OK_K * (l.tt / 2.0 + m.alp2 * c.et * qx);
+    d[2] = OK_K * (m.alp1 * l.alx - m.alp2 * c.q * qx);
+}
+
+// Part B (dc3d.f:284-400) DU(1..3), with the I1..I4 terms the gradient does not use.
+__device__ inline void ok_part_b_disp(const OkCorner &c, const OkLogs &l, const OkDip &dp, const OkMed &m,
+                                      double s[3], double d[3])
+{
+    const double xi = c.xi, et = c.et, q = c.q, R = c.r, Y = c.y;
+    const double rd = R + c.d;
+    double ai3, ai4;
+    if (dp.cd != 0.0) {
+        if (xi == 0.0) {
+            ai4 = 0.0;
+        } else {
+            const double x = sqrt(c.xi2 + c.q2);
+            ai4 = 1.0 / dp.cdcd * (xi / rd * dp.sdcd +
+                  2.0 * atan((et * (x + q * dp.cd) + x * (R + x) * dp.sd) / (xi * (R + x) * dp.cd)));
+        }
+        ai3 = (Y * dp.cd / rd - l.ale + dp.sd * log(rd)) / dp.cdcd;
+    } else {
+        const double rd2 = rd * rd;
+        ai3 = (et / rd + Y * q / rd2 - l.ale) / 2.0;
+        ai4 = xi * Y / rd2 / 2.0;
+    }
+    const double ai1 = -xi / rd * dp.cd - ai4 * dp.sd;
+    const double ai2 = log(rd) + ai3 * dp.sd;
+    const double qx = q * c.x11, qy = q * c.y11, a3 = m.alp3;
+    s[0] = OK_K * (-xi * qy - l.tt - a3 * ai1 * dp.sd);
+    s[1] = OK_K * (-q / R + a3 * Y / rd * dp.sd);
+    s[2] = OK_K * (q * qy - a3 * ai2 * dp.sd);
+    d[0] = OK_K * (-q / R + a3 * ai3 * dp.sdcd);
+    d[1] = OK_K * (-et * qx - l.tt - a3 * xi / rd * dp.sdcd);
+    d[2] = OK_K * (q * qx + a3 * ai4 * dp.sdcd);
+}
+
+// Displacement (ux, uy, uz in the DC3D frame) for unit strike slip (us) and
+// unit dip slip (ud): DC3D's U(1..3) (dc3d.f:1-198) with the same corner
+// loop, snapping, edge rejection and REAL*4 handling as ok_dc3d_grad.
+template <bool R32>
+__device__ inline bool ok_dc3d_disp(const OkMed &m, const OkDip &dp, double x, double y, double z,
+                                    double depth, double al2, double aw1, double us[3], double ud[3])
+{
+    const double eps = R32 ? (double)1.0e-6f : 1.0e-6;
+    for (int i = 0; i < 3; i++) { us[i] = 0.0; ud[i] = 0.0; }
+    double xi[2], et[2];
+    if (R32) {
+        xi[0] = (double)((float)x - 0.0f);
+        xi[1] = (double)((float)x - (float)al2);
+    } else {
+        xi[0] = x;
+        xi[1] = x - al2;
+    }
+    if (fabs(xi[0]) < eps) xi[0] = 0.0;
+    if (fabs(xi[1]) < eps) xi[1] = 0.0;
+    int kxi[2], ket[2];
+    OkCorner c;
+#pragma unroll 1
+    for (int img = 0; img < 2; img++) {
+        const double D = R32 ? (double)(img ? (float)depth - (float)z : (float)depth + (float)z)
+                             : (img ? depth - z : depth + z);
+        const double p = y * dp.cd + D * dp.sd;
+        double q = y * dp.sd - D * dp.cd;
+        et[0] = p - aw1;
+        et[1] = p;
+        if (fabs(q) < eps) q = 0.0;
+        if (fabs(et[0]) < eps) et[0] = 0.0;
+        if (fabs(et[1]) < eps) et[1] = 0.0;
+        if (ok_edges(xi, et, q, eps, kxi, ket)) {
+            for (int i = 0; i < 3; i++) { us[i] = 0.0; ud[i] = 0.0; }
+            return false;
+        }
+#pragma unroll 1
+        for (int kk = 0; kk < 4; kk++) {
+            const int k = kk >> 1, j = kk & 1;
+            ok_corner(xi[j], et[k], q, dp, kxi[k], ket[j], c);
+            const OkLogs l = ok_logs(c, kxi[k], ket[j]);
+            double as[3], ad[3];
+            ok_part_a_disp(c, l, m, as, ad);
+            const double sg = (j + k != 1) ? 1.0 : -1.0;
+            if (!img) {
+#pragma unroll
+                for (int t = 0; t < 2; t++) {
+                    const double *a = t ? ad : as;
+                    double *u = t ? ud : us;
+                    const double du0 = -a[0];
+                    const double du1 = -a[1] * dp.cd + a[2] * dp.sd;
+                    const double du2 = -a[1] * dp.sd - a[2] * dp.cd;
+                    u[0] = (sg > 0.0) ? u[0] + du0 : u[0] - du0;
+                    u[1] = (sg > 0.0) ? u[1] + du1 : u[1] - du1;
+                    u[2] = (sg > 0.0) ? u[2] + du2 : u[2] - du2;
+                }
+            } else {
+                double bs[3], bd[3], cs9[9], cd9[9], c0s[3], c0d[3];
+                ok_part_b_disp(c, l, dp, m, bs, bd);
+                ok_part_c(c, dp, m, z, cs9, cd9, c0s, c0d);
+#pragma unroll
+                for (int t = 0; t < 2; t++) {
+                    const double *a = t ? ad : as;
+                    const double *b = t ? bd : bs;
+                    const double *cc = t ? c0d : c0s;
+                    double *u = t ? ud : us;
+                    const double du0 = a[0] + b[0] + z * cc[0];
+                    const double du1 = (a[1] + b[1] + z * cc[1]) * dp.cd - (a[2] + b[2] + z * cc[2]) * dp.sd;
+                    const double du2 = (a[1] + b[1] - z * cc[1]) * dp.sd + (a[2] + b[2] - z * cc[2]) * dp.cd;
+                    u[0] = (sg > 0.0) ? u[0] + du0 : u[0] - du0;
+                    u[1] = (sg > 0.0) ? u[1] + du1 : u[1] - du1;
+                    u[2] = (sg > 0.0) ? u[2] + du2 : u[2] - du2;
+                }
+            }
+        }
+    }
+    if (R32) {
+        for (int i = 0; i < 3; i++) {
+            us[i] = (double)__double2float_rn(us[i]);
+            ud[i] = (double)__double2float_rn(ud[i]);
+        }
+    }
+    return true;
+}
+
 #undef OK_K
 
 }  // namespace ucg

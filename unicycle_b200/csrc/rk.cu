@@ -581,6 +581,55 @@ __global__ void k_control(Ctl *ctl)
     }
 }
 
+// one output record at the start of a step (after stage 1: y and its rate k1)
+__global__ void k_record(StageArgs a, const Ctl *ctl, Rec *rec)
+{
+    if (!rec->enabled || !ctl_live(ctl) || !ctl->need_stage1) return;
+    const long long step = ctl->accepted - rec->base;
+    if (step < 0 || step % rec->every) return;
+    const long long idx = step / rec->every;
+    double *r = rec->buf + (idx % rec->cap) * rec->len;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    if (t == 0) {
+        r[0] = ctl->time;
+        r[1] = ctl->hdid;
+        r[2] = ctl->vmax;
+        r[3] = (double)ctl->accepted;
+    }
+    // listed elements: state then rate, 7 per patch / 12 per volume, in a slot of 24
+    for (int j = t; j < rec->nelem * 24; j += nt) {
+        const int e = rec->elem[j / 24], q = j % 24;
+        const bool patch = e < a.np;
+        const int w = patch ? 7 : 12;
+        const long o = patch ? 7L * e : 7L * a.np + 12L * (e - a.np);
+        double v = 0.0;
+        if (q < w) v = a.y[o + q];
+        else if (q >= 12 && q - 12 < w) v = a.k[0][o + q - 12];
+        r[4 + j] = v;
+    }
+    // observation-point displacements: row k of O against the slip (patches)
+    // and the strain (volumes) of the state, one warp per row
+    const int warp = t >> 5, nw = nt >> 5;
+    double *ro = r + 4 + 24 * rec->nelem;
+    for (int k = warp; k < 3 * rec->nobs; k += nw) {
+        double sf, sl;
+        observe_row(rec->O + (long)k * (2L * a.np + 6L * a.nvol), a.np, a.nvol, a.y, sf, sl);
+        if ((t & 31) == 0) {
+            const int p = k / 3, c = k % 3;
+            if (rec->per_point == 3) {
+                ro[3 * p + c] = sf + sl;
+            } else {
+                double d, df, dl;
+                observe_split(c, sf, sl, d, df, dl);
+                ro[9 * p + c] = d;
+                ro[9 * p + 3 + c] = df;
+                ro[9 * p + 6 + c] = dl;
+            }
+        }
+    }
+    if (t == 0) rec->written = idx + 1;
+}
+
 __global__ void k_commit(StageArgs a, const Ctl *ctl)
 {
     if (!ctl->pending) return;
@@ -640,6 +689,12 @@ int rk_alloc(ucg_ctx *c)
     if (cudaMalloc(&c->st.v1, sizeof(double) * (c->n + 2)) != cudaSuccess) return UCG_E_OOM;
     if (cudaMalloc(&c->st.t1, sizeof(double) * (c->m + 2)) != cudaSuccess) return UCG_E_OOM;
     if (cudaMalloc(&c->ctl, sizeof(Ctl)) != cudaSuccess) return UCG_E_OOM;
+    if (cudaMalloc(&c->rec, sizeof(Rec)) != cudaSuccess) return UCG_E_OOM;
+    {
+        Rec off{};
+        UCG_CUDA(cudaMemcpyAsync(c->rec, &off, sizeof(Rec), cudaMemcpyHostToDevice, c->stream));
+        c->rec_host = off;
+    }
     if (cudaMallocHost(&c->ctl_host, sizeof(Ctl)) != cudaSuccess) return UCG_E_OOM;
     if (cudaMallocHost(&c->pin, sizeof(double) * (2 * len + 8)) != cudaSuccess) return UCG_E_OOM;
     memset(c->ctl_host, 0, sizeof(Ctl));
@@ -660,6 +715,14 @@ void rk_free(ucg_ctx *c)
     }
     if (c->ctl) cudaFree(c->ctl);
     c->ctl = nullptr;
+    if (c->rec) cudaFree(c->rec);
+    c->rec = nullptr;
+    if (c->rec_buf) cudaFree(c->rec_buf);
+    c->rec_buf = nullptr;
+    if (c->rec_elem) cudaFree(c->rec_elem);
+    c->rec_elem = nullptr;
+    c->rec_host = Rec{};
+    c->rec_drained = 0;
     if (c->ctl_host) cudaFreeHost(c->ctl_host);
     c->ctl_host = nullptr;
     if (c->pin) cudaFreeHost(c->pin);
@@ -715,6 +778,11 @@ static void enqueue_stage(ucg_ctx *c)
 static void enqueue_attempt_raw(ucg_ctx *c)
 {
     enqueue_stage<1>(c);
+    // the recorder joins the attempt (and its graph) only while recording is on
+    if (c->rec_host.enabled) {
+        k_record<<<c->sms, 256, 0, c->stream>>>(stage_args(c, 1), c->ctl, c->rec);
+        c->launches.count += 1;
+    }
     enqueue_stage<2>(c);
     enqueue_stage<3>(c);
     enqueue_stage<4>(c);

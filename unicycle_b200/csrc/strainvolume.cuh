@@ -24,6 +24,16 @@ __device__ __forceinline__ double sv_val(Dd a) { return a.v; }
 
 }  // namespace ucg
 
+// and for plain doubles (observation-point displacements); declared in the
+// integrals' namespace so that the unqualified calls there find them
+namespace bml17 {
+__host__ __device__ __forceinline__ double sv_sqrt(double a) { return sqrt(a); }
+__host__ __device__ __forceinline__ double sv_log(double a) { return log(a); }
+__host__ __device__ __forceinline__ double sv_atan(double a) { return atan(a); }
+__host__ __device__ __forceinline__ double sv_atan2(double y, double x) { return atan2(y, x); }
+__host__ __device__ __forceinline__ double sv_val(double a) { return a; }
+}  // namespace bml17
+
 #include "bml17_disp.h"
 
 namespace ucg {
@@ -113,6 +123,25 @@ __device__ inline void sv_pair_stress(const double *rc, const SvRec &R, double m
         sig[q][3] = lambda * kk + 2 * mu * e22;
         sig[q][4] = 2 * mu * e23;
         sig[q][5] = lambda * kk + 2 * mu * e33r;
+    }
+}
+
+// Displacement (north, east, down) at xr (NED) for the six unit eigenstrains
+// of one cuboid (computeDisplacementVerticalStrainVolume, strainvolume.f90:
+// 215-991): the receiver rotated into the cuboid frame, the 8-corner sum of
+// the displacement integrals, the horizontal components rotated back.
+__device__ inline void sv_pair_disp(const double xr[3], const SvRec &R, double mu, double nu, double u[6][3])
+{
+    const double ct = R[SV_C], st = R[SV_S];
+    const double x1p = (xr[0] - R[SV_Q1]) * ct + (xr[1] - R[SV_Q2]) * st;
+    const double x2p = -(xr[0] - R[SV_Q1]) * st + (xr[1] - R[SV_Q2]) * ct;
+    double up[6][3];
+    bml17::displacement<-1, double>(x1p, x2p, xr[2], R[SV_Q3], R[SV_L], R[SV_T], R[SV_W], nu, mu, up);
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        u[q][0] = up[q][0] * ct - up[q][1] * st;
+        u[q][1] = up[q][0] * st + up[q][1] * ct;
+        u[q][2] = up[q][2];
     }
 }
 

@@ -1,4 +1,5 @@
 // C ABI of libucg.so (include/ucg.h).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -79,6 +80,16 @@ int ucg_create(ucg_ctx **out, int device, double mu, double lambda, int flags)
     return UCG_OK;
 }
 
+static void free_observation(ucg_ctx *c)
+{
+    if (c->O) cudaFree(c->O);
+    if (c->obs_dev) cudaFree(c->obs_dev);
+    c->O = nullptr;
+    c->obs_dev = nullptr;
+    c->O_bytes = 0;
+    c->O_ready = false;
+}
+
 static void free_params(ucg_ctx *c)
 {
     double **p[] = {&c->fr.vpl_c, &c->fr.vpl_s, &c->fr.a, &c->fr.b, &c->fr.sig, &c->fr.L, &c->fr.damping,
@@ -100,6 +111,7 @@ void ucg_destroy(ucg_ctx *c)
     rk_free(c);
     split_bf16_free(c);
     free_params(c);
+    free_observation(c);
     if (c->K) cudaFree(c->K);
     if (c->rcv) cudaFree(c->rcv);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -112,6 +124,7 @@ static void invalidate(ucg_ctx *c)
     c->state_ready = false;
     rk_free(c);
     split_bf16_free(c);
+    free_observation(c);
 }
 
 int ucg_set_rectangles(ucg_ctx *c, int n, const double *x, const double *L, const double *W,
@@ -409,6 +422,191 @@ static int put_vec(ucg_ctx *c, double *dst, const double *src)
     memcpy(c->pin, src, sizeof(double) * c->state_len);
     UCG_CUDA(cudaMemcpyAsync(dst, c->pin, sizeof(double) * c->state_len, cudaMemcpyHostToDevice, c->stream));
     UCG_CUDA(cudaStreamSynchronize(c->stream));
+    return UCG_OK;
+}
+
+static int obs_per_point(const ucg_ctx *c) { return c->nv > 0 ? 9 : 3; }
+
+long ucg_record_len(ucg_ctx *c)
+{
+    if (!c) return 0;
+    if (c->rec_host.enabled) return c->rec_host.len;
+    const int nobs = c->O_ready ? (int)(c->obs_x.size() / 3) : 0;
+    return 4L + 24L * c->rec_host.nelem + (long)obs_per_point(c) * nobs;
+}
+
+int ucg_record(ucg_ctx *c, int every, const int *elements, int nelem, long capacity)
+{
+    if (!c) return UCG_E_BADARG;
+    if (capacity < 0 || every < 1 || nelem < 0 || (nelem > 0 && !elements)) return bad(c, "recording arguments");
+    const int ne = c->nr + c->nt + c->nv;
+    for (int j = 0; j < nelem; j++)
+        if (elements[j] < 0 || elements[j] >= ne) return bad(c, "recorded element out of range");
+    int rc = ensure_state(c);
+    if (rc) return rc;
+    UCG_CUDA(cudaSetDevice(c->device));
+    if ((rc = pull_ctl(c))) return rc;
+    if (c->rec_buf) cudaFree(c->rec_buf);
+    if (c->rec_elem) cudaFree(c->rec_elem);
+    c->rec_buf = nullptr;
+    c->rec_elem = nullptr;
+    Rec r{};
+    if (capacity > 0) {
+        const int nobs = c->O_ready ? (int)(c->obs_x.size() / 3) : 0;
+        r.per_point = obs_per_point(c);
+        r.len = 4 + 24 * nelem + r.per_point * nobs;
+        UCG_CUDA(cudaMalloc(&c->rec_buf, sizeof(double) * (size_t)r.len * (size_t)capacity));
+        if (nelem > 0) {
+            UCG_CUDA(cudaMalloc(&c->rec_elem, sizeof(int) * nelem));
+            UCG_CUDA(cudaMemcpy(c->rec_elem, elements, sizeof(int) * nelem, cudaMemcpyHostToDevice));
+        }
+        r.buf = c->rec_buf;
+        r.cap = capacity;
+        r.base = c->ctl_host->accepted;
+        r.elem = c->rec_elem;
+        r.O = nobs ? c->O : nullptr;
+        r.every = every;
+        r.nelem = nelem;
+        r.nobs = nobs;
+        r.enabled = 1;
+    }
+    if (c->rec_host.enabled != r.enabled) rk_drop_graph(c);   // the attempt gains / loses k_record
+    c->rec_host = r;
+    c->rec_drained = 0;
+    UCG_CUDA(cudaMemcpyAsync(c->rec, &c->rec_host, sizeof(Rec), cudaMemcpyHostToDevice, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    return UCG_OK;
+}
+
+int ucg_records(ucg_ctx *c, double *out, long max_records, long *n_records, long *lost)
+{
+    if (!c || (!out && max_records > 0)) return UCG_E_BADARG;
+    if (n_records) *n_records = 0;
+    if (lost) *lost = 0;
+    if (!c->rec || !c->rec_host.enabled) return UCG_OK;
+    UCG_CUDA(cudaSetDevice(c->device));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    long long written = 0;
+    UCG_CUDA(cudaMemcpy(&written, &c->rec->written, sizeof written, cudaMemcpyDeviceToHost));
+    const long long cap = c->rec_host.cap, len = c->rec_host.len;
+    long long start = c->rec_drained;
+    if (written - start > cap) {
+        if (lost) *lost = (long)(written - start - cap);
+        start = written - cap;
+    }
+    const long long k = std::min<long long>(written - start, max_records);
+    for (long long j = 0; j < k;) {
+        const long long slot = (start + j) % cap, run = std::min(k - j, cap - slot);
+        UCG_CUDA(cudaMemcpy(out + j * len, c->rec_buf + slot * len, sizeof(double) * run * len,
+                            cudaMemcpyDeviceToHost));
+        j += run;
+    }
+    c->rec_drained = start + k;
+    if (n_records) *n_records = (long)k;
+    return UCG_OK;
+}
+
+// stop a recording whose layout depends on the observation points
+static int stop_recording(ucg_ctx *c)
+{
+    if (!c->rec || !c->rec_host.enabled) return UCG_OK;
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    rk_drop_graph(c);
+    c->rec_host = Rec{};
+    UCG_CUDA(cudaMemcpy(c->rec, &c->rec_host, sizeof(Rec), cudaMemcpyHostToDevice));
+    if (c->rec_buf) cudaFree(c->rec_buf);
+    if (c->rec_elem) cudaFree(c->rec_elem);
+    c->rec_buf = nullptr;
+    c->rec_elem = nullptr;
+    c->rec_drained = 0;
+    return UCG_OK;
+}
+
+int ucg_set_observation_points(ucg_ctx *c, int nobs, const double *x)
+{
+    if (!c || nobs < 0 || (nobs > 0 && !x)) return UCG_E_BADARG;
+    for (long i = 0; i < 3L * nobs; i++)
+        if (!std::isfinite(x[i])) return bad(c, "non-finite observation point");
+    UCG_CUDA(cudaSetDevice(c->device));
+    int rc = stop_recording(c);
+    if (rc) return rc;
+    free_observation(c);
+    c->obs_x.assign(x, x + 3L * nobs);
+    return UCG_OK;
+}
+
+int ucg_build_O(ucg_ctx *c, int okada_mode)
+{
+    if (!c) return UCG_E_BADARG;
+    if (okada_mode != UCG_OKADA_FP64 && okada_mode != UCG_OKADA_REF32IO) return bad(c, "okada_mode");
+    if (c->nr + c->nt + c->nv == 0) return set_err(c, UCG_E_STATE, "no elements");
+    if (c->obs_x.empty()) return set_err(c, UCG_E_STATE, "no observation points");
+    UCG_CUDA(cudaSetDevice(c->device));
+    int rc = stop_recording(c);
+    if (rc) return rc;
+    c->O_ready = false;
+    return assemble_observation(c, okada_mode);
+}
+
+int ucg_observation_info(ucg_ctx *c, int *nobs, int *per_point, double *build_ms)
+{
+    if (!c) return UCG_E_BADARG;
+    if (nobs) *nobs = (int)(c->obs_x.size() / 3);
+    if (per_point) *per_point = obs_per_point(c);
+    if (build_ms) *build_ms = c->O_ready ? c->obs_ms : 0.0;
+    return UCG_OK;
+}
+
+int ucg_copy_O(ucg_ctx *c, double *O)
+{
+    if (!c || !O) return UCG_E_BADARG;
+    if (!c->O_ready) return set_err(c, UCG_E_STATE, "O not built");
+    UCG_CUDA(cudaSetDevice(c->device));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    UCG_CUDA(cudaMemcpy(O, c->O, c->O_bytes, cudaMemcpyDeviceToHost));
+    return UCG_OK;
+}
+
+// d (and the faulting / flow sets) at every point, one warp per row of O
+__global__ void k_observe_state(const double *__restrict__ O, int np, int nvol, int nobs,
+                                const double *__restrict__ y, double *d, double *df, double *dl)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const long n = 2L * np + 6L * nvol;
+    for (int k = warp; k < 3 * nobs; k += nw) {
+        double sf, sl;
+        observe_row(O + (long)k * n, np, nvol, y, sf, sl);
+        if ((threadIdx.x & 31) == 0) observe_split(k % 3, sf, sl, d[k], df[k], dl[k]);
+    }
+}
+
+int ucg_displacements(ucg_ctx *c, const double *y, double *d, double *d_fault, double *d_flow)
+{
+    if (!c || !y || !d) return UCG_E_BADARG;
+    if (!c->O_ready) return set_err(c, UCG_E_STATE, "O not built");
+    UCG_CUDA(cudaSetDevice(c->device));
+    const long len = 7L * (c->nr + c->nt) + 12L * c->nv;
+    const int nobs = (int)(c->obs_x.size() / 3);
+    const long rows = 3L * nobs;
+    double *buf = nullptr;
+    UCG_CUDA(cudaMalloc(&buf, sizeof(double) * (len + 3 * rows)));
+    cudaError_t e = cudaMemcpyAsync(buf, y, sizeof(double) * len, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        const int blocks = (int)std::min<long>((rows + 7) / 8, (long)c->sms * 8);
+        k_observe_state<<<blocks, 256, 0, c->stream>>>(c->O, c->nr + c->nt, c->nv, nobs, buf, buf + len,
+                                                       buf + len + rows, buf + len + 2 * rows);
+        c->launches.count++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d, buf + len, sizeof(double) * rows, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && d_fault)
+        e = cudaMemcpyAsync(d_fault, buf + len + rows, sizeof(double) * rows, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && d_flow)
+        e = cudaMemcpyAsync(d_flow, buf + len + 2 * rows, sizeof(double) * rows, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(buf);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ucg_displacements");
     return UCG_OK;
 }
 

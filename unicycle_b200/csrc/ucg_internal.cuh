@@ -29,6 +29,56 @@ struct Ctl {
     double vmax;       // max patch velocity at the last f(y)
 };
 
+// Device-side output recorder (the reference's export/exportPoints,
+// ratestate.f90:405-537): at the start of every `every`-th accepted step, one
+// record of time, dt_done, max V, the state and rate of the listed elements and
+// the observation-point displacements O u, written into a ring buffer.
+struct Rec {
+    double *buf;            // cap records of len doubles
+    long long cap, base;    // ring capacity; accepted steps when recording started
+    long long written;      // records written since recording started
+    const int *elem;        // listed elements (0-based, patches then volumes)
+    const double *O;        // 3 nobs x n observation-point displacement kernels (row-major)
+    int every, nelem, nobs, len;
+    int per_point;          // 3 (total) or, with volumes, 9 (total, faulting, flow)
+    int enabled;
+};
+
+// Displacement of observation-point row Ok (one row of O) for the state y
+// (exportPoints: slip of every patch, strain of every volume): the sums over
+// the fault columns (sf) and over the volume columns (sl), reduced over the
+// warp; every lane of the calling warp receives both.
+__device__ inline void observe_row(const double *__restrict__ Ok, int np, int nvol, const double *__restrict__ y,
+                                   double &sf, double &sl)
+{
+    const int lane = threadIdx.x & 31;
+    const long nf = 2L * np, n = nf + 6L * nvol;
+    double a = 0.0, b = 0.0;
+    for (long c = lane; c < nf; c += 32) a = fma(Ok[c], y[7L * (c >> 1) + (c & 1)], a);
+    for (long c = nf + lane; c < n; c += 32) {
+        const long v = c - nf;
+        b = fma(Ok[c], y[7L * np + 12L * (v / 6) + v % 6], b);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, off);
+        b += __shfl_xor_sync(0xffffffffu, b, off);
+    }
+    sf = a;
+    sl = b;
+}
+
+// The three displacement sets of viscouscycles' exportPoints from the two
+// partial sums of component c: total (O), "faulting" (Of) and "flow" (Ol).
+// buildO (greens.f90:423-430) stores a volume's vertical column in Of rather
+// than Ol, so the down component of the faulting set includes the volumes'
+// and the flow set's down component is zero; kept for identical output.
+__device__ __forceinline__ void observe_split(int c, double sf, double sl, double &d, double &df, double &dl)
+{
+    d = sf + sl;
+    df = (c == 2) ? sf + sl : sf;
+    dl = (c == 2) ? 0.0 : sl;
+}
+
 // Per-element constitutive data, structure of arrays.
 struct Friction {
     double *vpl_c, *vpl_s;   // Vpl*cos(rake), Vpl*sin(rake)
@@ -101,6 +151,18 @@ struct ucg_ctx {
     ucg::Stages st{};
     ucg::Ctl *ctl = nullptr;     // device
     ucg::Ctl *ctl_host = nullptr; // pinned mirror
+    ucg::Rec *rec = nullptr;      // device recorder block (allocated with the integrator)
+    ucg::Rec rec_host{};          // host copy of its settings
+    long long rec_drained = 0;    // records handed to the caller
+    int *rec_elem = nullptr;      // device copy of the listed elements
+    double *rec_buf = nullptr;
+    // observation points (north, east, down) and their displacement kernels
+    std::vector<double> obs_x;
+    double *obs_dev = nullptr;
+    double *O = nullptr;         // 3 nobs x n, row-major
+    size_t O_bytes = 0;
+    bool O_ready = false;
+    double obs_ms = 0.0;         // device time of the last O assembly
     double *pin = nullptr;       // pinned staging (state length * 2)
     long state_len = 0;
     bool state_ready = false;
@@ -116,6 +178,7 @@ namespace ucg {
 
 // assemble.cu
 int assemble_matrix(ucg_ctx *c, int okada_mode);
+int assemble_observation(ucg_ctx *c, int okada_mode);   // O for c->obs_x (sets O_ready)
 // rk.cu
 int rk_alloc(ucg_ctx *c);
 void rk_free(ucg_ctx *c);

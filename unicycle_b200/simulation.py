@@ -195,6 +195,68 @@ class Simulation:
         self._check(self.lib.ucg_run(self.ctx, t_end, max_steps, ctypes.byref(steps)), "run")
         return steps.value
 
+    def set_observation_points(self, x):
+        """Observation points (nobs, 3): north, east, down."""
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        self._check(self.lib.ucg_set_observation_points(self.ctx, len(x), _p(x)), "set_observation_points")
+
+    def buildO(self, okada_mode=_lib.UCG_OKADA_FP64):
+        """Assemble the observation-point displacement kernels on the device (buildO)."""
+        self._check(self.lib.ucg_build_O(self.ctx, okada_mode), "build_O")
+
+    def observation_info(self):
+        nobs, per, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._check(self.lib.ucg_observation_info(self.ctx, ctypes.byref(nobs), ctypes.byref(per), ctypes.byref(ms)),
+                    "observation_info")
+        return dict(nobs=nobs.value, per_point=per.value, build_ms=ms.value)
+
+    def copy_O(self):
+        """O as a (3 nobs, n) array: row 3k + c is component c (north, east,
+        down) at point k, column j the unit source DOF j of K."""
+        n, _ = self.dims
+        out = np.empty((3 * self.observation_info()["nobs"], n))
+        self._check(self.lib.ucg_copy_O(self.ctx, _p(out)), "copy_O")
+        return out
+
+    def displacements(self, y):
+        """(total, faulting, flow) displacements, each (nobs, 3), for state y."""
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        k = self.observation_info()["nobs"]
+        d, f, l = (np.empty((k, 3)) for _ in range(3))
+        self._check(self.lib.ucg_displacements(self.ctx, _p(y), _p(d), _p(f), _p(l)), "displacements")
+        return d, f, l
+
+    def record(self, every=1, elements=(), capacity=100000):
+        """Record every `every`-th accepted step on the device (export / exportPoints);
+        capacity 0 stops."""
+        el = np.ascontiguousarray(elements, dtype=np.int32)
+        self._check(self.lib.ucg_record(self.ctx, every, el.ctypes.data_as(_ip) if len(el) else None, len(el),
+                                        capacity), "record")
+        self._rec_elem = el
+
+    def records(self, max_records=1 << 20):
+        """Drained records as a dict of arrays: time, dt_done, vmax, step,
+        state (n, nelem, 12), rate (n, nelem, 12), displacement (n, nobs, 3)
+        (with volumes also displacement_fault and displacement_flow); and the
+        number of records lost to the ring's overrun."""
+        L = self.lib.ucg_record_len(self.ctx)
+        buf = np.empty((max_records, L))
+        n, lost = ctypes.c_long(), ctypes.c_long()
+        self._check(self.lib.ucg_records(self.ctx, _p(buf), max_records, ctypes.byref(n), ctypes.byref(lost)),
+                    "records")
+        b = buf[:n.value]
+        ne = len(getattr(self, "_rec_elem", ()))
+        per = self.observation_info()["per_point"]
+        nobs = (L - 4 - 24 * ne) // per
+        ev = b[:, 4:4 + 24 * ne].reshape(-1, ne, 24)
+        dsp = b[:, 4 + 24 * ne:].reshape(-1, nobs, per)
+        out = dict(time=b[:, 0], dt_done=b[:, 1], vmax=b[:, 2], step=b[:, 3].astype(np.int64),
+                   state=ev[:, :, :12], rate=ev[:, :, 12:], displacement=dsp[:, :, :3], lost=lost.value)
+        if per == 9:
+            out["displacement_fault"] = dsp[:, :, 3:6]
+            out["displacement_flow"] = dsp[:, :, 6:9]
+        return out
+
     @property
     def launch_count(self):
         return self.lib.ucg_launch_count(self.ctx)
