@@ -219,6 +219,80 @@ long ucg_record_len(ucg_ctx *ctx);
    *lost receives the records overwritten before they were drained. */
 int ucg_records(ucg_ctx *ctx, double *out, long max_records, long *n_records, long *lost);
 
+/* ---- input decks (init) ---------------------------------------------------- */
+
+/* A parsed input deck of the reference's 3-D drivers: the text read by init()
+   of fortran/3d/src/ratestate.f90:958-1739 (driver UCG_DRIVER_RATESTATE) or
+   fortran/3d/src/viscouscycles.f90:1291-2069 (UCG_DRIVER_VISCOUSCYCLES),
+   with the same sections, order and validation; angles are returned in
+   radians.  Host-only: needs no device. */
+typedef struct ucg_deck ucg_deck;
+
+typedef struct {
+    int driver;
+    double lambda, mu, interval;
+    int n_rect, n_tri, n_vertex, n_vol;
+    int nonlinear_maxwell;  /* nonlinear Maxwell properties given for every volume */
+    int thermal;            /* thermal properties given for every volume */
+    int n_obs_state;        /* observation patches, then observation volumes */
+    int n_obs_point;
+    int n_events;           /* perturbations; the first is at t = 0 */
+} ucg_deck_info;
+
+/* Parse the whole deck text; on UCG_E_BADARG err receives the line number and
+   the reason (the reference's STOP message). */
+int ucg_deck_parse(const char *text, int driver, ucg_deck **deck, char *err, long err_len);
+/* the same for a file */
+int ucg_deck_read(const char *path, int driver, ucg_deck **deck, char *err, long err_len);
+void ucg_deck_free(ucg_deck *deck);
+int ucg_deck_summary(const ucg_deck *deck, ucg_deck_info *info);
+/* output directory (the deck's first line) */
+const char *ucg_deck_wdir(const ucg_deck *deck);
+/* name of observation point k (0-based; at most 10 characters) */
+const char *ucg_deck_point_name(const ucg_deck *deck, int k);
+/* Copy up to max values of a field into out (out may be NULL); returns the
+   field's length, or a negative status for an unknown field.  Doubles:
+   rect.x (3 per patch), rect.length, rect.width, rect.strike, rect.dip,
+   tri.vertices (3 per vertex), patch.Vpl, patch.rake, patch.mu0, patch.sig,
+   patch.a, patch.b, patch.L, patch.Vo, patch.damping (rectangles then
+   triangles), vol.x, vol.length, vol.width, vol.thickness, vol.strike,
+   vol.e_bg (6 per volume), vol.Gm, vol.gammadot0m, vol.npowerm, vol.Q, vol.R,
+   vol.rhoc, vol.To, obs.x (3 per point), events.time.  Integers: tri.i1,
+   tri.i2, tri.i3 (1-based vertices), obs.state (1-based elements, volumes
+   numbered after all patches). */
+long ucg_deck_get(const ucg_deck *deck, const char *field, double *out, long max);
+long ucg_deck_get_int(const ucg_deck *deck, const char *field, int *out, long max);
+/* Load the deck's elements, friction, rheology and observation points into a
+   context (ucg_set_*); ucg_deck_create also creates the context with the
+   deck's moduli and driver. */
+int ucg_deck_apply(const ucg_deck *deck, ucg_ctx *ctx);
+int ucg_deck_create(const ucg_deck *deck, int device, ucg_ctx **ctx);
+/* initStateVector with the deck's volume properties (ucg_init_state) */
+int ucg_deck_init_state(const ucg_deck *deck, ucg_ctx *ctx, double *y);
+
+/* Options of the reference's command line (ratestate.f90:975-1030) and of
+   the device loop. */
+typedef struct {
+    double epsilon;           /* --epsilon (reference default 1e-6) */
+    double maximum_step;      /* --maximum-step (default: no limit) */
+    long maximum_iterations;  /* --maximum-iterations (default 1000000) */
+    int okada_mode;           /* UCG_OKADA_* for buildG and buildO */
+    int precision;            /* UCG_PREC_* of the traction product */
+    int device;
+    long chunk;               /* iterations per device run between recorder drains */
+    const char *wdir;         /* output directory; NULL: the deck's */
+    int verbose;              /* progress lines on standard output */
+} ucg_run_options;
+
+/* The whole run of a deck, as the reference's main program does it
+   (ratestate.f90:170-372): buildG, buildO, initStateVector, dt = 1e-3, then
+   iterations until the deck's time interval or maximum_iterations, writing
+   time.txt, patch-%08d.dat / volume-%08d.dat for the observation states and
+   opts-<name>.dat for the observation points into the output directory, in
+   the reference's formats.  *iterations and *time receive the iterations run
+   and the final time; the return is the integrator's status. */
+int ucg_deck_run(const ucg_deck *deck, const ucg_run_options *opt, long *iterations, double *time);
+
 /* Number of kernel launches this context has issued (for launch accounting). */
 long ucg_launch_count(ucg_ctx *ctx);
 

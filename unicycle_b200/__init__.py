@@ -10,5 +10,6 @@ from ._lib import (UCG_OKADA_FP64, UCG_OKADA_REF32IO, UCG_PREC_FP64,  # noqa: F4
 from .simulation import Simulation  # noqa: F401
 from .ensemble import Ensemble  # noqa: F401
 from .stepmodel import StepModel  # noqa: F401
+from .deck import Deck, write_deck  # noqa: F401
 
-__all__ = ["Simulation", "Ensemble", "StepModel", "configs", "UcgError", "load"]
+__all__ = ["Simulation", "Ensemble", "StepModel", "Deck", "write_deck", "configs", "UcgError", "load"]

@@ -42,6 +42,21 @@ _i = ctypes.c_int
 _l = ctypes.c_long
 _d = ctypes.c_double
 
+
+
+class DeckInfo(ctypes.Structure):
+    """ucg_deck_info"""
+    _fields_ = [("driver", _i), ("lambda_", _d), ("mu", _d), ("interval", _d), ("n_rect", _i), ("n_tri", _i),
+                ("n_vertex", _i), ("n_vol", _i), ("nonlinear_maxwell", _i), ("thermal", _i),
+                ("n_obs_state", _i), ("n_obs_point", _i), ("n_events", _i)]
+
+
+class RunOptions(ctypes.Structure):
+    """ucg_run_options"""
+    _fields_ = [("epsilon", _d), ("maximum_step", _d), ("maximum_iterations", _l), ("okada_mode", _i),
+                ("precision", _i), ("device", _i), ("chunk", _l), ("wdir", ctypes.c_char_p), ("verbose", _i)]
+
+
 # name -> (restype, argtypes); the complete exported surface of include/ucg.h
 SIGNATURES = {
     "ucg_create": (_i, [ctypes.POINTER(_vp), _i, _d, _d, _i]),
@@ -112,6 +127,18 @@ SIGNATURES = {
     "ucg_ens_set_step_model": (_i, [_vp, _vp]),
     "ucg_ens_record_traces": (_i, [_vp, _l]),
     "ucg_ens_get_traces": (_i, [_vp, _fp, _l, _lp]),
+    "ucg_deck_parse": (_i, [ctypes.c_char_p, _i, ctypes.POINTER(_vp), ctypes.c_char_p, _l]),
+    "ucg_deck_read": (_i, [ctypes.c_char_p, _i, ctypes.POINTER(_vp), ctypes.c_char_p, _l]),
+    "ucg_deck_free": (None, [_vp]),
+    "ucg_deck_summary": (_i, [_vp, ctypes.POINTER(DeckInfo)]),
+    "ucg_deck_wdir": (ctypes.c_char_p, [_vp]),
+    "ucg_deck_point_name": (ctypes.c_char_p, [_vp, _i]),
+    "ucg_deck_get": (_l, [_vp, ctypes.c_char_p, _dp, _l]),
+    "ucg_deck_get_int": (_l, [_vp, ctypes.c_char_p, _ip, _l]),
+    "ucg_deck_apply": (_i, [_vp, _vp]),
+    "ucg_deck_create": (_i, [_vp, _i, ctypes.POINTER(_vp)]),
+    "ucg_deck_init_state": (_i, [_vp, _vp, _dp]),
+    "ucg_deck_run": (_i, [_vp, ctypes.POINTER(RunOptions), _lp, _dp]),
 }
 
 _lib = None

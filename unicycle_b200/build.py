@@ -22,7 +22,7 @@ PER_FILE = {"rk.cu": ["-fmad=false"]}
 
 
 def sources():
-    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
 
 
 def stale():

@@ -42,6 +42,16 @@ class Simulation:
         self.mu, self.lam, self.driver = mu, lam, driver
         self.nr = self.nt = self.nv = 0
 
+    @classmethod
+    def adopt(cls, ctx, mu, lam, driver, nr=0, nt=0, nv=0):
+        """Wrap a context created elsewhere through the C ABI (ucg_deck_create)."""
+        self = cls.__new__(cls)
+        self.lib = _lib.load()
+        self.ctx = ctx
+        self.mu, self.lam, self.driver = mu, lam, driver
+        self.nr, self.nt, self.nv = nr, nt, nv
+        return self
+
     def close(self):
         if self.ctx:
             self.lib.ucg_destroy(self.ctx)
