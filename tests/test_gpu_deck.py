@@ -11,10 +11,17 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _rows(path, skip=0):
+def _rows(path, skip=0, w=19):
+    """Fixed-width fields as Fortran writes them: the first 19 columns, then
+    fields of w columns (a negative ES20.12E3 value fills its field, so
+    columns, not blanks, separate the values)."""
     with open(path) as f:
         lines = f.read().splitlines()[skip:]
-    return lines, np.array([[float(v) for v in ln.split()] for ln in lines])
+    rows = []
+    for ln in lines:
+        vals = [float(ln[:19])] + [float(ln[p:p + w]) for p in range(19, len(ln), w)]
+        rows.append(vals)
+    return lines, np.array(rows)
 
 
 def test_deck_context_equals_api_context(ucg):
@@ -66,7 +73,7 @@ def test_deck_run_writes_reference_files(ucg, tmp_path):
     np.testing.assert_allclose(T[1:, 0], want_t, rtol=1e-12)
     np.testing.assert_allclose(T[1:, 1], want_dt, rtol=1e-12)
     for e in (1, 50):
-        lines, P = _rows(tmp_path / f"patch-{e:08d}.dat")
+        lines, P = _rows(tmp_path / f"patch-{e:08d}.dat", w=20)
         assert P.shape == (n, 15) and all(len(ln) == 19 + 20 * 14 for ln in lines)
         ys = np.array([s[1][7 * (e - 1): 7 * e] for s in seen])
         rs = np.array([s[2][7 * (e - 1): 7 * e] for s in seen])
@@ -94,7 +101,7 @@ def test_viscous_deck_run(ucg, tmp_path):
     sim.buildG(0)
     sim.buildO(0)
     seen = _step_loop(sim, d.init_state(sim), n, 1e-6)
-    lines, V = _rows(tmp_path / "volume-00000002.dat")
+    lines, V = _rows(tmp_path / "volume-00000002.dat", w=20)
     assert V.shape == (n, 25) and all(len(ln) == 19 + 20 * 24 for ln in lines)
     o = 7 * nf + 12
     np.testing.assert_allclose(V[:, 1:13], np.array([s[1][o:o + 12] for s in seen]), rtol=1e-12, atol=1e-300)
