@@ -199,6 +199,22 @@ int ucg_copy_O(ucg_ctx *ctx, double *O);
    toward the faulting set, so the flow set's down component is zero. */
 int ucg_displacements(ucg_ctx *ctx, const double *y, double *d, double *d_fault, double *d_flow);
 
+/* ---- coseismic perturbations (in%event) --------------------------------------- */
+
+/* A perturbation at `time`: u holds a slip increment (strike, dip) per patch and
+   an eigenstrain increment (11, 12, 13, 22, 23, 33) per volume, the source-DOF
+   layout of K's columns.  ucg_run ends the step that reaches `time` exactly on
+   it, adds u to the slip / strain components of the state and K u to the
+   tractions / stresses (the stress change the increment causes), and restarts
+   from the reference's initial tentative step (1e-3 s).  The reference reads
+   perturbation times into in%event (viscouscycles.f90:2022-2049) without using
+   them; this gives them content.  Perturbations at or after a time passed to
+   ucg_set_state are pending again.  Needs the FP64 K (ucg_keep_fp64). */
+int ucg_add_event(ucg_ctx *ctx, double time, const double *u);
+int ucg_clear_events(ucg_ctx *ctx);
+/* the same increment applied to the device state now */
+int ucg_apply_perturbation(ucg_ctx *ctx, const double *u);
+
 /* ---- output recording (export / exportPoints) ------------------------------ */
 
 /* Record on the device, without host round trips, at the start of every

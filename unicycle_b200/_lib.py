@@ -88,6 +88,9 @@ SIGNATURES = {
     "ucg_observation_info": (_i, [_vp, _ip, _ip, _dp]),
     "ucg_copy_O": (_i, [_vp, _dp]),
     "ucg_displacements": (_i, [_vp, _dp, _dp, _dp, _dp]),
+    "ucg_add_event": (_i, [_vp, _d, _dp]),
+    "ucg_clear_events": (_i, [_vp]),
+    "ucg_apply_perturbation": (_i, [_vp, _dp]),
     "ucg_record": (_i, [_vp, _i, _ip, _i, _l]),
     "ucg_record_len": (_l, [_vp]),
     "ucg_records": (_i, [_vp, _dp, _l, _lp, _lp]),

@@ -26,6 +26,7 @@
 // instead of dominating it on components whose state and rate are near zero,
 // which at rtol 1e-8 would reject nearly every attempt.  The FP64 path keeps
 // the reference's plain form.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -556,6 +557,7 @@ __global__ void k_control(Ctl *ctl)
         h = h * SAFETY * pow(errmax, PSHRNK);
         if (h < 0.5 * h) h = 0.5 * h;   // never taken (ode45.f90:83)
         ctl->h = h;
+        ctl->clamped = 0;   // a shrunk step stays short of t_stop
         ctl->rejected += 1;
         ctl->need_stage1 = 0;
         ctl->pending = 0;
@@ -570,9 +572,14 @@ __global__ void k_control(Ctl *ctl)
         else hnext = 10.0 * h;
         if (hnext > ctl->hmax) hnext = ctl->hmax;
         ctl->hdid = h;
-        ctl->time = ctl->time + h;
+        ctl->time = ctl->clamped ? ctl->t_stop : ctl->time + h;
         ctl->dt_next = hnext;
         ctl->h = hnext;
+        ctl->clamped = 0;
+        if (ctl->stop_on && ctl->time < ctl->t_stop && ctl->time + hnext > ctl->t_stop) {
+            ctl->h = ctl->t_stop - ctl->time;
+            ctl->clamped = 1;
+        }
         ctl->accepted += 1;
         ctl->pending = 1;
         ctl->vmax = 0.0;
@@ -723,6 +730,8 @@ void rk_free(ucg_ctx *c)
     c->rec_elem = nullptr;
     c->rec_host = Rec{};
     c->rec_drained = 0;
+    if (c->pert) cudaFree(c->pert);
+    c->pert = nullptr;
     if (c->ctl_host) cudaFreeHost(c->ctl_host);
     c->ctl_host = nullptr;
     if (c->pin) cudaFreeHost(c->pin);
@@ -861,6 +870,44 @@ int rk_profile_traction(ucg_ctx *c, int reps, double *ms)
     *ms = (double)t / reps;
     *h = saved;
     UCG_CUDA(cudaMemcpyAsync(c->ctl, h, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    return UCG_OK;
+}
+
+// A coseismic perturbation of the state: slip (2 per patch) and eigenstrain
+// (6 per volume) increments u, and the stress they cause, K u, added to the
+// tractions (3 per patch) and stresses (6 per volume).  One warp per row of K.
+__global__ void k_perturb(const double *__restrict__ K, long m, long n, int np, const double *__restrict__ u,
+                          double *__restrict__ y)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x, nt = (long)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    for (long r = t >> 5; r < m; r += nt >> 5) {
+        const double *Kr = K + r * n;
+        double s = 0.0;
+        for (long c = lane; c < n; c += 32) s = fma(Kr[c], u[c], s);
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (lane == 0) {
+            const long i = r < 3L * np ? 7L * (r / 3) + 2 + r % 3
+                                       : 7L * np + 12L * ((r - 3L * np) / 6) + 6 + (r - 3L * np) % 6;
+            y[i] += s;
+        }
+    }
+    for (long c = t; c < n; c += nt) {
+        const long i = c < 2L * np ? 7L * (c >> 1) + (c & 1) : 7L * np + 12L * ((c - 2L * np) / 6) + (c - 2L * np) % 6;
+        y[i] += u[c];
+    }
+}
+
+int rk_perturb(ucg_ctx *c, const double *u)
+{
+    if (!c->K) return UCG_E_STATE;
+    if (!c->pert) UCG_CUDA(cudaMalloc(&c->pert, sizeof(double) * c->n));
+    UCG_CUDA(cudaMemcpyAsync(c->pert, u, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->stream));
+    const int blocks = (int)std::min<long>((c->m + 7) / 8, 8L * c->sms);
+    k_perturb<<<blocks, 256, 0, c->stream>>>(c->K, c->m, c->n, c->nr + c->nt, c->pert, c->st.y);
+    c->launches.count++;
+    UCG_CUDA(cudaGetLastError());
     UCG_CUDA(cudaStreamSynchronize(c->stream));
     return UCG_OK;
 }

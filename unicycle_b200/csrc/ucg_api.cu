@@ -750,6 +750,9 @@ int ucg_set_state(ucg_ctx *c, const double *y, double time, double dt_next)
     h->time = time;
     h->h = dt_next;
     h->dt_next = dt_next;
+    h->clamped = 0;
+    // perturbations at or after the new time are pending again
+    for (auto &ev : c->events) ev.applied = ev.time < time;
     h->need_stage1 = 1;
     h->pending = 0;
     h->status = 0;
@@ -779,6 +782,25 @@ int ucg_get_state(ucg_ctx *c, double *y, double *time, double *dt_next, long *ac
     return UCG_OK;
 }
 
+// apply every pending perturbation whose time has been reached; the next step
+// restarts from the reference's initial tentative step
+static int apply_due_events(ucg_ctx *c)
+{
+    Ctl *h = c->ctl_host;
+    for (auto &ev : c->events) {
+        if (ev.applied || ev.time > h->time) continue;
+        int rc = rk_perturb(c, ev.u.data());
+        if (rc) return set_err(c, rc, "perturbations need the FP64 matrix (keep_fp64)");
+        ev.applied = true;
+        h->need_stage1 = 1;
+        h->pending = 0;
+        h->h = std::min(1.0e-3, c->hmax);
+        h->dt_next = h->h;
+        h->clamped = 0;
+    }
+    return UCG_OK;
+}
+
 int ucg_run(ucg_ctx *c, double t_end, long max_steps, long *steps)
 {
     if (!c || max_steps < 0) return UCG_E_BADARG;
@@ -792,20 +814,75 @@ int ucg_run(ucg_ctx *c, double t_end, long max_steps, long *steps)
         if (steps) *steps = 0;
         return UCG_OK;
     }
-    h->t_end = t_end;
-    h->step_target = acc0 + max_steps;
-    h->status = 0;
-    h->active = 1;
-    h->nonfinite = 0;
-    h->epsilon = c->epsilon;
-    h->hmax = c->hmax;
+    // segments between perturbation times: each ends exactly on the next
+    // pending perturbation, which is applied before the following segment
+    for (;;) {
+        if ((rc = apply_due_events(c))) return rc;
+        double t_next = INFINITY;
+        for (const auto &ev : c->events)
+            if (!ev.applied && ev.time > h->time) t_next = std::min(t_next, ev.time);
+        const bool stop = t_next < t_end;
+        h->t_end = stop ? t_next : t_end;
+        h->stop_on = stop ? 1 : 0;
+        h->t_stop = stop ? t_next : 0.0;
+        h->clamped = 0;
+        if (stop && h->time + h->h > t_next) {
+            h->h = t_next - h->time;
+            h->clamped = 1;
+        }
+        h->step_target = acc0 + max_steps;
+        h->status = 0;
+        h->active = 1;
+        h->nonfinite = 0;
+        h->epsilon = c->epsilon;
+        h->hmax = c->hmax;
+        if ((rc = push_ctl(c))) return rc;
+        // queue attempts in batches sized to the remaining steps
+        const long left = acc0 + max_steps - h->accepted;
+        rc = drive(c, left < 32 ? (int)left : 32);
+        if (rc) return rc;
+        if (h->status || !stop || h->accepted >= acc0 + max_steps || h->time < t_next) break;
+    }
+    h->stop_on = 0;
+    h->clamped = 0;
     if ((rc = push_ctl(c))) return rc;
-    // queue attempts in batches sized to the remaining steps
-    rc = drive(c, max_steps < 32 ? (int)max_steps : 32);
-    if (rc) return rc;
     if (steps) *steps = h->accepted - acc0;
     if (h->status) return set_err(c, h->status, ucg_strerror(h->status));
     return UCG_OK;
+}
+
+int ucg_add_event(ucg_ctx *c, double time, const double *u)
+{
+    if (!c || !u || !std::isfinite(time)) return UCG_E_BADARG;
+    const long n = 2L * (c->nr + c->nt) + 6L * c->nv;
+    if (n == 0) return set_err(c, UCG_E_STATE, "no elements");
+    for (long i = 0; i < n; i++)
+        if (!std::isfinite(u[i])) return bad(c, "non-finite perturbation");
+    ucg_ctx::Event ev{time, std::vector<double>(u, u + n), false};
+    auto it = c->events.begin();
+    while (it != c->events.end() && it->time <= time) ++it;
+    c->events.insert(it, ev);
+    return UCG_OK;
+}
+
+int ucg_clear_events(ucg_ctx *c)
+{
+    if (!c) return UCG_E_BADARG;
+    c->events.clear();
+    return UCG_OK;
+}
+
+int ucg_apply_perturbation(ucg_ctx *c, const double *u)
+{
+    if (!c || !u) return UCG_E_BADARG;
+    if (!c->state_ready) return set_err(c, UCG_E_STATE, "call ucg_set_state first");
+    UCG_CUDA(cudaSetDevice(c->device));
+    int rc = pull_ctl(c);
+    if (rc) return rc;
+    if ((rc = rk_perturb(c, u))) return set_err(c, rc, "perturbations need the FP64 matrix (keep_fp64)");
+    c->ctl_host->need_stage1 = 1;
+    c->ctl_host->pending = 0;
+    return push_ctl(c);
 }
 
 long ucg_launch_count(ucg_ctx *c) { return c ? c->launches.count : -1; }

@@ -27,6 +27,10 @@ struct Ctl {
     int active;        // 0 once t_end or step_target is reached
     int nonfinite;     // set by kernels that meet a NaN/Inf
     double vmax;       // max patch velocity at the last f(y)
+    // landing on a perturbation time: with stop_on set, no step crosses t_stop;
+    // the step that reaches it ends exactly on it (clamped marks that attempt)
+    double t_stop;
+    int stop_on, clamped;
 };
 
 // Device-side output recorder (the reference's export/exportPoints,
@@ -167,6 +171,16 @@ struct ucg_ctx {
     long state_len = 0;
     bool state_ready = false;
 
+    // coseismic perturbations (ucg_add_event): applied by ucg_run when the
+    // integration reaches their time; u has the source-DOF layout of K's columns
+    struct Event {
+        double time;
+        std::vector<double> u;
+        bool applied;
+    };
+    std::vector<Event> events;
+    double *pert = nullptr;      // device copy of the perturbation being applied (n)
+
     cudaGraphExec_t attempt_graph = nullptr;
     int graph_precision = -1;
     int sms = 148;
@@ -187,6 +201,7 @@ int rk_profile_traction(ucg_ctx *c, int reps, double *ms);
 void rk_enqueue_attempt(ucg_ctx *c);        // one Cash-Karp attempt + control
 void rk_enqueue_commit(ucg_ctx *c);         // copy a pending candidate into y
 bool rk_anchored(const ucg_ctx *c);         // stages contract increments over the stage-1 anchor
+int rk_perturb(ucg_ctx *c, const double *u); // y += slip/strain u and the stress change K u (host u)
 void rk_drop_graph(ucg_ctx *c);             // before freeing anything the attempt graph reads
 int split_bf16_build(ucg_ctx *c);
 void split_bf16_free(ucg_ctx *c);

@@ -236,6 +236,29 @@ class Simulation:
         self._check(self.lib.ucg_displacements(self.ctx, _p(y), _p(d), _p(f), _p(l)), "displacements")
         return d, f, l
 
+    def _pert(self, slip=None, strain=None):
+        n, _ = self.dims
+        u = np.zeros(n)
+        np_ = self.nr + self.nt
+        if slip is not None:
+            u[: 2 * np_] = np.asarray(slip, dtype=np.float64).ravel()
+        if strain is not None:
+            u[2 * np_:] = np.asarray(strain, dtype=np.float64).ravel()
+        return u
+
+    def add_event(self, time, slip=None, strain=None):
+        """Coseismic perturbation at `time`: slip (npatch, 2) strike/dip increments
+        and strain (nvol, 6) eigenstrain increments; applied by run()."""
+        u = self._pert(slip, strain)
+        self._check(self.lib.ucg_add_event(self.ctx, float(time), _p(u)), "add_event")
+
+    def clear_events(self):
+        self._check(self.lib.ucg_clear_events(self.ctx), "clear_events")
+
+    def apply_perturbation(self, slip=None, strain=None):
+        u = self._pert(slip, strain)
+        self._check(self.lib.ucg_apply_perturbation(self.ctx, _p(u)), "apply_perturbation")
+
     def record(self, every=1, elements=(), capacity=100000):
         """Record every `every`-th accepted step on the device (export / exportPoints);
         capacity 0 stops."""
@@ -258,8 +281,8 @@ class Simulation:
         ne = len(getattr(self, "_rec_elem", ()))
         per = self.observation_info()["per_point"]
         nobs = (L - 4 - 24 * ne) // per
-        ev = b[:, 4:4 + 24 * ne].reshape(-1, ne, 24)
-        dsp = b[:, 4 + 24 * ne:].reshape(-1, nobs, per)
+        ev = b[:, 4:4 + 24 * ne].reshape(len(b), ne, 24)
+        dsp = b[:, 4 + 24 * ne:].reshape(len(b), nobs, per)
         out = dict(time=b[:, 0], dt_done=b[:, 1], vmax=b[:, 2], step=b[:, 3].astype(np.int64),
                    state=ev[:, :, :12], rate=ev[:, :, 12:], displacement=dsp[:, :, :3], lost=lost.value)
         if per == 9:
