@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--nx", type=int, default=100, help="along-strike cells (2 triangles each per row)")
     p.add_argument("--nz", type=int, default=100, help="down-dip rows")
     p.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16"])
-    p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split", "coupled", "cfg4"])
+    p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split", "coupled", "cfg4", "hmatrix"])
     p.add_argument("--coupled-size", default="64,64,16,8,8",
                    help="coupled assembly leg: fault nx,nz and volume nx,ny,nz")
     p.add_argument("--sets", type=int, default=N_SETS, help="instances in the ensemble workload")
@@ -56,6 +56,10 @@ def parse():
                    help="launch the ensemble's attempt kernels from the host instead of one graph launch "
                         "(for ncu, which does not follow conditional graph nodes)")
     p.add_argument("--no-learned", action="store_true", help="skip the learned step-size leg")
+    p.add_argument("--no-hmatrix", action="store_true", help="skip the hierarchical-matrix leg")
+    p.add_argument("--hm-eta", type=float, default=2.0, help="hierarchical matrix: admissibility parameter")
+    p.add_argument("--hm-eps", type=float, default=1e-6, help="hierarchical matrix: ACA relative accuracy")
+    p.add_argument("--hm-leaf", type=int, default=32, help="hierarchical matrix: patches per cluster leaf")
     p.add_argument("--trace-runs", type=int, default=64, help="seeded cfg1 runs that record training traces")
     p.add_argument("--trace-attempts", type=int, default=16000, help="attempts of the trace-recording runs")
     p.add_argument("--learned-eval-years", type=float, default=15.0,
@@ -546,6 +550,130 @@ def learned_leg(args, local, sim20, sets, y0s, plain_window):
     return out
 
 
+def hmatrix_leg(args, local, sim, cfg, plain):
+    """The same N = 20k model with its K replaced by the hierarchical
+    approximation (ucg_build_hmatrix): build, storage, accuracy on a row block
+    of the dense K, the product's bandwidth and the plain integrator's steps/s
+    against the dense FP64 path."""
+    import torch
+    import unicycle_b200
+    n = cfg["n_patch"]
+    m, nn = 3 * n, 2 * n
+    t0 = time.perf_counter()
+    sim.build_hmatrix(eta=args.hm_eta, eps=args.hm_eps, leaf=args.hm_leaf)
+    build_s = time.perf_counter() - t0
+    info = sim.hmatrix_info()
+    x = np.random.default_rng(3).standard_normal(nn)
+    Kr = sim.copy_G(0, 3 * 256)
+    y = sim.hmatrix_matvec(x)[:3 * 256]
+    ref = Kr @ x
+    err = float(np.linalg.norm(y - ref) / np.linalg.norm(ref))
+    ms = sim.hmatrix_profile(20)
+    alg = info["bytes"] + 8.0 * (nn + m)
+    peak, peak_kind = load_peaks()
+    sim.set_precision(unicycle_b200.UCG_PREC_HMATRIX)
+    stream = torch.cuda.ExternalStream(sim.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sim.set_state(cfg["y0"], 0.0, cfg["dt0"])
+    sim.run(1e300, args.spinup + args.warmup)
+    _, t_w, *_ = sim.get_state()
+    steps_req = max(10, args.steps // 2)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    steps = sim.run(1e300, steps_req)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    _, t_t, *_ = sim.get_state()
+    sim.set_precision(unicycle_b200.UCG_PREC_FP64)
+    return {"eta": args.hm_eta, "eps": args.hm_eps, "leaf": args.hm_leaf, "build_seconds": build_s,
+            "blocks_dense": info["n_dense"], "blocks_lowrank": info["n_lowrank"], "max_rank": info["max_rank"],
+            "bytes": info["bytes"], "compression_vs_dense_fp64": info["compression"],
+            "product_rel_error_rows_0_767": err,
+            "steps_per_s": steps / el, "ms_per_step": 1e3 * el / steps,
+            "speedup_vs_plain_fp64_steps": steps / el / plain["value"],
+            "sim_years_per_hour": (t_t - t_w) / YEAR / (el / 3600.0),
+            "roofline": {"bound": "hbm", "kernel": "hierarchical product (k_hm_gather, k_hm_z, k_hm_rows, "
+                                                   "k_hm_reduce)", "ms_per_launch": ms, "bytes_per_launch": alg,
+                         "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind}}
+
+
+def run_hmatrix(args, world, rank, local):
+    """--workload hmatrix: the cfg2 megathrust at --nx x --nz cells held only as
+    its hierarchical approximation (no dense K; at 200 x 200 = 80,000 triangles
+    the dense FP64 K would be 307 GB, beyond the B200's HBM)."""
+    import torch
+    import unicycle_b200
+    from unicycle_b200 import configs
+    torch.cuda.set_device(local)
+    cfg = configs.cfg2(nx=args.nx, nz=args.nz)
+    n = cfg["n_patch"]
+    m, nn = 3 * n, 2 * n
+    sim = unicycle_b200.Simulation(cfg["mu"], cfg["lam"], device=local)
+    i1, i2, i3, v = cfg["mesh"]["tri"]
+    sim.set_triangles(i1, i2, i3, v)
+    fr = cfg["friction"]
+    sim.set_friction(fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
+                     fr["damping"])
+    sim.set_tolerance(cfg["epsilon"])
+    t0 = time.perf_counter()
+    sim.build_hmatrix(eta=args.hm_eta, eps=args.hm_eps, leaf=args.hm_leaf)
+    build_s = time.perf_counter() - t0
+    info = sim.hmatrix_info()
+    sim.set_precision(unicycle_b200.UCG_PREC_HMATRIX)
+    stream = torch.cuda.ExternalStream(sim.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sim.set_state(cfg["y0"], 0.0, cfg["dt0"])
+    sim.run(1e300, args.spinup + args.warmup)
+    _, t_w, *_ = sim.get_state()
+    launches0 = sim.launch_count
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0.record(stream)
+        steps = sim.run(1e300, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    launches = sim.launch_count - launches0
+    el_max = reduce_max(el, world, args)
+    y_t, t_t, dt_t, *_ = sim.get_state()
+    ms = sim.hmatrix_profile(10)
+    alg = info["bytes"] + 8.0 * (nn + m)
+    peak, peak_kind = load_peaks()
+    e2e_steps = max(3, args.steps // 6)
+    y_h, t_h, dt_h = y_t.copy(), t_t, dt_t
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        t_h, y_h, _, dt_h, _, _ = sim.step(t_h, y_h, dt_h)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_el = reduce_max(e0.elapsed_time(e1) / 1e3, world, args)
+    sim.close()
+    if rank != 0:
+        return None
+    return {"metric": METRIC, "value": world * steps / el_max, "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el_max / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded cfg2 curved megathrust; random Dc)",
+            "config": {"workload": f"megathrust {n} Nikkhoo-Walter triangles, hierarchical K only",
+                       "n_triangles": n, "K_shape": [m, nn], "dense_fp64_bytes": 8.0 * m * nn,
+                       "parallelism": f"replicas x{world}", "rtol": cfg["epsilon"],
+                       "l2": "inputs larger than L2 (H %.1f GB)" % (info["bytes"] / 1e9)},
+            "sim_years_per_hour": (t_t - t_w) / YEAR / (el / 3600.0),
+            "hmatrix": {"build_seconds": build_s, "eta": args.hm_eta, "eps": args.hm_eps, "leaf": args.hm_leaf,
+                        **{k: info[k] for k in ("n_dense", "n_lowrank", "max_rank", "bytes", "compression")}},
+            "roofline": {"bound": "hbm", "kernel": "hierarchical product (k_hm_gather, k_hm_z, k_hm_rows, "
+                                                   "k_hm_reduce)", "ms_per_launch": ms, "bytes_per_launch": alg,
+                         "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None},
+            "e2e": {"value": world * e2e_steps / e2e_el, "unit": "steps/s", "h2d_bytes_per_step": 8 * 7 * n,
+                    "d2h_bytes_per_step": 2 * 8 * 7 * n},
+            "gpu_launches": int(launches), "clocks": clk.summary(), "cpu_baseline": None}
+
+
 def run_ensemble(args, world, rank, local):
     """Headline: args.sets frictional parameter sets of the N = 20k model in one
     ensemble, beside the same model as one plain FP64 instance."""
@@ -624,6 +752,7 @@ def run_ensemble(args, world, rank, local):
     families = assembly_leg(args, local) if rank == 0 else None
     if families:
         families["nikkhoo_tri"] = {"entries": 6 * n * n, "ms": tri_ms, "mentries_per_s": 6 * n * n / tri_ms / 1e3}
+    hmat = hmatrix_leg(args, local, sim, cfg, plain) if rank == 0 and not args.no_hmatrix else None
     learned = None
     if not args.no_learned and rank == 0:
         learned = learned_leg(args, local, sim, sets, y0s,
@@ -682,6 +811,7 @@ def run_ensemble(args, world, rank, local):
             "cpu_baseline": cpu,
             "assembly_families": families,
             "learned_step": learned,
+            "hmatrix": hmat,
         }
     sim.close()
     return out
@@ -696,6 +826,8 @@ def main():
         out = run_ensemble(args, world, rank, local)
     elif args.workload == "cfg4":
         out = run_cfg4(args, world, rank, local)
+    elif args.workload == "hmatrix":
+        out = run_hmatrix(args, world, rank, local)
     elif args.workload == "coupled":
         import torch
         torch.cuda.set_device(local)

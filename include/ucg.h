@@ -42,6 +42,7 @@ typedef struct ucg_ctx ucg_ctx;
 /* matrix storage for the traction product (ucg_set_precision) */
 #define UCG_PREC_FP64        0  /* K in binary64, FP64 matvec (the plain method) */
 #define UCG_PREC_SPLIT_BF16  1  /* K = diag(s)(hi + lo), bf16 hi/lo, FP32 accumulation */
+#define UCG_PREC_HMATRIX     2  /* hierarchical approximation of K (ucg_build_hmatrix), FP64 */
 
 /* driver conventions (ucg_create flags) */
 #define UCG_DRIVER_RATESTATE      0  /* fortran/3d/src/ratestate.f90     */
@@ -121,6 +122,26 @@ int ucg_set_precision(ucg_ctx *ctx, int precision);
 /* Keep (keep != 0, default) or release the FP64 K after a split-BF16 copy
    exists, freeing its HBM. */
 int ucg_keep_fp64(ucg_ctx *ctx, int keep);
+
+/* Hierarchical approximation of K for a fault model of one patch family
+   (rectangles or triangles; no volumes): patches ordered by a cluster tree
+   of `leaf` patches, pairs of clusters with max(diam) <= eta dist stored as
+   low-rank factors found by adaptive cross approximation to relative accuracy
+   eps (each checked against its dense block), the rest dense.  Every block is
+   assembled on the device and compressed at once, so the dense K is never
+   held (models beyond what a dense K fits in HBM).  The reference's MATLAB
+   toolbox does this with the hmmvp library
+   (matlab/+unicycle/+ode/+hmmvp/rateandstate.m:71-143).  Selected for the
+   traction product with ucg_set_precision(ctx, UCG_PREC_HMATRIX). */
+int ucg_build_hmatrix(ucg_ctx *ctx, int okada_mode, double eta, double eps, int leaf);
+/* blocks stored dense (including low-rank candidates that failed their check)
+   and low-rank, bytes stored, the largest rank, device time of the build */
+int ucg_hmatrix_info(ucg_ctx *ctx, long *n_dense, long *n_lowrank, long *bytes, int *max_rank,
+                     double *build_ms);
+/* y (m) = H x (n), host arrays */
+int ucg_hmatrix_matvec(ucg_ctx *ctx, const double *x, double *y);
+/* mean device time (ms) of one product H v over reps launches */
+int ucg_hmatrix_profile(ucg_ctx *ctx, int reps, double *ms);
 
 /* ---- state and right-hand side ------------------------------------------- */
 

@@ -24,6 +24,7 @@ UCG_OKADA_FP64 = 0
 UCG_OKADA_REF32IO = 1
 UCG_PREC_FP64 = 0
 UCG_PREC_SPLIT_BF16 = 1
+UCG_PREC_HMATRIX = 2
 UCG_DRIVER_RATESTATE = 0
 UCG_DRIVER_VISCOUSCYCLES = 1
 UCG_ENS_STREAM_K = 0
@@ -74,6 +75,10 @@ SIGNATURES = {
     "ucg_copy_G": (_i, [_vp, _dp, _l, _l, _l]),
     "ucg_set_precision": (_i, [_vp, _i]),
     "ucg_keep_fp64": (_i, [_vp, _i]),
+    "ucg_build_hmatrix": (_i, [_vp, _i, _d, _d, _i]),
+    "ucg_hmatrix_info": (_i, [_vp, _lp, _lp, _lp, _ip, _dp]),
+    "ucg_hmatrix_matvec": (_i, [_vp, _dp, _dp]),
+    "ucg_hmatrix_profile": (_i, [_vp, _i, _dp]),
     "ucg_state_len": (_l, [_vp]),
     "ucg_init_state": (_i, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "ucg_odefun": (_i, [_vp, _d, _dp, _dp, _dp]),

@@ -20,6 +20,7 @@
 #include "okada92.cuh"
 #include "nikkhoo15.cuh"
 #include "strainvolume.cuh"
+#include "blocks.cuh"
 
 namespace ucg {
 
@@ -108,6 +109,59 @@ __device__ __forceinline__ void store_patch_source(double *K, long n, long col, 
 enum { RS_Q1 = 0, RS_Q2, RS_CS, RS_SS, RS_DEPTH, RS_AL2, RS_AW1, RS_SD, RS_CD, RS_SDSD, RS_CDCD,
        RS_SDCD, RS_SIZE };
 
+// Stress (s11, s12, s13, s22, s23, s33 for strike and dip slip) at receiver
+// point (x1, x2, x3) of one rectangle record sr (okada92.f90:121-205).
+template <bool R32>
+__device__ __forceinline__ void rect_pair_sig(const double sr[RS_SIZE], const OkDip &dp, double x1, double x2,
+                                              double x3, const OkMed &med, double mu, double lambda,
+                                              double sig[2][6])
+{
+    const double csst = sr[RS_CS], ssst = sr[RS_SS];
+    double x = (x1 - sr[RS_Q1]) * csst + (x2 - sr[RS_Q2]) * ssst;
+    double y = (x1 - sr[RS_Q1]) * ssst - (x2 - sr[RS_Q2]) * csst;
+    double z = -x3;
+    if (R32) {
+        x = (double)__double2float_rn(x);
+        y = (double)__double2float_rn(y);
+        z = (double)__double2float_rn(z);
+    }
+    double gs[9], gd[9];
+    ok_dc3d_grad<R32>(med, dp, x, y, z, sr[RS_DEPTH], sr[RS_AL2], sr[RS_AW1], gs, gd);
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const double *g = t ? gd : gs;
+        // okada92.f90:165-205: rotate the gradient back from the strike frame
+        const double uxx = g[0], uyx = g[1], uzx = g[2], uxy = g[3], uyy = g[4], uzy = g[5];
+        const double uxz = g[6], uyz = g[7], uzz = g[8];
+        const double uxxr = (csst * uxx + ssst * uyx) * csst - (-csst * uxy - ssst * uyy) * ssst;
+        const double uxyr = (csst * uxx + ssst * uyx) * ssst + (-csst * uxy - ssst * uyy) * csst;
+        const double uxzr = -csst * uxz + ssst * uyz;
+        const double uyxr = (ssst * uxx - csst * uyx) * csst - (-ssst * uxy + csst * uyy) * ssst;
+        const double uyyr = (ssst * uxx - csst * uyx) * ssst + (-ssst * uxy + csst * uyy) * csst;
+        const double uyzr = -ssst * uxz + csst * uyz;
+        const double uzxr = -csst * uzx - ssst * uzy;
+        const double uzyr = -ssst * uzx + csst * uzy;
+        const double e11 = uxxr, e12 = (uxyr + uyxr) / 2.0, e13 = (uxzr + uzxr) / 2.0;
+        const double e22 = uyyr, e23 = (uyzr + uzyr) / 2.0, e33 = uzz;
+        const double ekk = e11 + e22 + e33;
+        sig[t][0] = lambda * ekk + 2.0 * mu * e11;
+        sig[t][1] = 2.0 * mu * e12;
+        sig[t][2] = 2.0 * mu * e13;
+        sig[t][3] = lambda * ekk + 2.0 * mu * e22;
+        sig[t][4] = 2.0 * mu * e23;
+        sig[t][5] = lambda * ekk + 2.0 * mu * e33;
+    }
+}
+
+__device__ __forceinline__ void rect_record(const double *__restrict__ src, int ns, int j, double sr[RS_SIZE],
+                                            OkDip &dp)
+{
+#pragma unroll
+    for (int f = 0; f < RS_SIZE; f++) sr[f] = __ldg(src + (long)f * ns + j);
+    dp.sd = sr[RS_SD]; dp.cd = sr[RS_CD]; dp.sdsd = sr[RS_SDSD]; dp.cdcd = sr[RS_CDCD];
+    dp.sdcd = sr[RS_SDCD];
+}
+
 template <bool R32>
 __global__ void __launch_bounds__(128) k_assemble_rect(double *__restrict__ K, long n, long col0,
         const double *__restrict__ rcv, int nrcv, int np, const double *__restrict__ src, int ns,
@@ -116,50 +170,12 @@ __global__ void __launch_bounds__(128) k_assemble_rect(double *__restrict__ K, l
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ns) return;
     double sr[RS_SIZE];
-#pragma unroll
-    for (int f = 0; f < RS_SIZE; f++) sr[f] = __ldg(src + (long)f * ns + j);
     OkDip dp;
-    dp.sd = sr[RS_SD]; dp.cd = sr[RS_CD]; dp.sdsd = sr[RS_SDSD]; dp.cdcd = sr[RS_CDCD];
-    dp.sdcd = sr[RS_SDCD];
+    rect_record(src, ns, j, sr, dp);
     for (int e = blockIdx.y; e < nrcv; e += gridDim.y) {
         const double *rc = rcv + (long)e * RC_SIZE;
-        const double x1 = __ldg(rc + 0), x2 = __ldg(rc + 1), x3 = __ldg(rc + 2);
-        const double csst = sr[RS_CS], ssst = sr[RS_SS];
-        double x = (x1 - sr[RS_Q1]) * csst + (x2 - sr[RS_Q2]) * ssst;
-        double y = (x1 - sr[RS_Q1]) * ssst - (x2 - sr[RS_Q2]) * csst;
-        double z = -x3;
-        if (R32) {
-            x = (double)__double2float_rn(x);
-            y = (double)__double2float_rn(y);
-            z = (double)__double2float_rn(z);
-        }
-        double gs[9], gd[9];
-        ok_dc3d_grad<R32>(med, dp, x, y, z, sr[RS_DEPTH], sr[RS_AL2], sr[RS_AW1], gs, gd);
         double sig[2][6];
-#pragma unroll
-        for (int t = 0; t < 2; t++) {
-            const double *g = t ? gd : gs;
-            // okada92.f90:165-205: rotate the gradient back from the strike frame
-            const double uxx = g[0], uyx = g[1], uzx = g[2], uxy = g[3], uyy = g[4], uzy = g[5];
-            const double uxz = g[6], uyz = g[7], uzz = g[8];
-            const double uxxr = (csst * uxx + ssst * uyx) * csst - (-csst * uxy - ssst * uyy) * ssst;
-            const double uxyr = (csst * uxx + ssst * uyx) * ssst + (-csst * uxy - ssst * uyy) * csst;
-            const double uxzr = -csst * uxz + ssst * uyz;
-            const double uyxr = (ssst * uxx - csst * uyx) * csst - (-ssst * uxy + csst * uyy) * ssst;
-            const double uyyr = (ssst * uxx - csst * uyx) * ssst + (-ssst * uxy + csst * uyy) * csst;
-            const double uyzr = -ssst * uxz + csst * uyz;
-            const double uzxr = -csst * uzx - ssst * uzy;
-            const double uzyr = -ssst * uzx + csst * uzy;
-            const double e11 = uxxr, e12 = (uxyr + uyxr) / 2.0, e13 = (uxzr + uzxr) / 2.0;
-            const double e22 = uyyr, e23 = (uyzr + uzyr) / 2.0, e33 = uzz;
-            const double ekk = e11 + e22 + e33;
-            sig[t][0] = lambda * ekk + 2.0 * mu * e11;
-            sig[t][1] = 2.0 * mu * e12;
-            sig[t][2] = 2.0 * mu * e13;
-            sig[t][3] = lambda * ekk + 2.0 * mu * e22;
-            sig[t][4] = 2.0 * mu * e23;
-            sig[t][5] = lambda * ekk + 2.0 * mu * e33;
-        }
+        rect_pair_sig<R32>(sr, dp, __ldg(rc + 0), __ldg(rc + 1), __ldg(rc + 2), med, mu, lambda, sig);
         double rloc[RC_SIZE];
 #pragma unroll
         for (int f = 0; f < RC_SIZE; f++) rloc[f] = __ldg(rc + f);
@@ -227,6 +243,70 @@ __global__ void __launch_bounds__(128) k_assemble_vol(double *__restrict__ K, lo
                 reinterpret_cast<double2 *>(p)[0] = make_double2(o[0][c], o[1][c]);
                 reinterpret_cast<double2 *>(p)[1] = make_double2(o[2][c], o[3][c]);
                 reinterpret_cast<double2 *>(p)[2] = make_double2(o[4][c], o[5][c]);
+            }
+        }
+    }
+}
+
+// ---- dense blocks of K for the hierarchical approximation -------------------------
+//
+// Rows of receivers ridx[0..nrb) (element ids, patches only: 3 traction rows
+// each) against the columns of sources sidx[0..nsb) of one family (2 slip
+// columns each); out is row-major (3 nrb) x (2 nsb).  The same pair kernels as
+// K; the grid's y dimension strides over the receivers.
+
+template <bool R32>
+__global__ void __launch_bounds__(128) k_block_rect(double *__restrict__ out, const int *__restrict__ ridx, int nrb,
+        const int *__restrict__ sidx, int nsb, const double *__restrict__ rcv, const double *__restrict__ src,
+        int ns, OkMed med, double mu, double lambda)
+{
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jj >= nsb) return;
+    double sr[RS_SIZE];
+    OkDip dp;
+    rect_record(src, ns, __ldg(sidx + jj), sr, dp);
+    const long ld = 2L * nsb;
+    for (int ii = blockIdx.y; ii < nrb; ii += gridDim.y) {
+        const double *rc = rcv + (long)__ldg(ridx + ii) * RC_SIZE;
+        double rloc[RC_SIZE];
+#pragma unroll
+        for (int f = 0; f < RC_SIZE; f++) rloc[f] = __ldg(rc + f);
+        double sig[2][6], tS[3], tD[3];
+        rect_pair_sig<R32>(sr, dp, rloc[0], rloc[1], rloc[2], med, mu, lambda, sig);
+        traction3(rloc, sig[0], tS);
+        traction3(rloc, sig[1], tD);
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            *reinterpret_cast<double2 *>(out + (3L * ii + c) * ld + 2L * jj) = make_double2(tS[c], tD[c]);
+    }
+}
+
+template <int PART>
+__global__ void __launch_bounds__(128) k_block_tri(double *__restrict__ out, const int *__restrict__ ridx, int nrb,
+        const int *__restrict__ sidx, int nsb, const double *__restrict__ rcv, const double *__restrict__ rec,
+        int ns, NwConst cst)
+{
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jj >= nsb) return;
+    NwRec R{rec + __ldg(sidx + jj), (long)ns};
+    const long ld = 2L * nsb;
+    for (int ii = blockIdx.y; ii < nrb; ii += gridDim.y) {
+        const double *rc = rcv + (long)__ldg(ridx + ii) * RC_SIZE;
+        double rloc[RC_SIZE];
+#pragma unroll
+        for (int f = 0; f < RC_SIZE; f++) rloc[f] = __ldg(rc + f);
+        double sS[6], sD[6], tS[3], tD[3];
+        nw_part_stress<PART>(rloc, R, cst, sS, sD);
+        traction3(rloc, sS, tS);
+        traction3(rloc, sD, tD);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double2 *p = reinterpret_cast<double2 *>(out + (3L * ii + c) * ld + 2L * jj);
+            if (PART == 0) {
+                *p = make_double2(tS[c], tD[c]);
+            } else {
+                const double2 o = *p;
+                *p = make_double2(o.x + tS[c], o.y + tD[c]);
             }
         }
     }
@@ -597,6 +677,105 @@ int assemble_observation(ucg_ctx *c, int okada_mode)
     if (dsrc) cudaFree(dsrc);
     c->O_ready = true;
     return UCG_OK;
+}
+
+// ---- block sources (hierarchical approximation) -----------------------------------
+
+int block_sources_build(ucg_ctx *c, int okada_mode, BlockSources *bs)
+{
+    if ((c->nr > 0) == (c->nt > 0) || c->nv > 0) return UCG_E_UNSUPPORTED;   // one patch family
+    UCG_CUDA(cudaSetDevice(c->device));
+    std::vector<double> rh;
+    build_receivers(c, rh);
+    if (c->rcv) cudaFree(c->rcv);
+    c->rcv = nullptr;
+    UCG_CUDA(cudaMalloc(&c->rcv, sizeof(double) * rh.size()));
+    UCG_CUDA(cudaMemcpy(c->rcv, rh.data(), sizeof(double) * rh.size(), cudaMemcpyHostToDevice));
+    std::vector<double> s;
+    bs->family = c->nr > 0 ? 0 : 1;
+    bs->okada_mode = okada_mode;
+    if (bs->family == 0) {
+        build_rect_sources(c, okada_mode, s);
+        bs->ns = c->nr;
+        const double alpha_d = (c->lambda + c->mu) / (c->lambda + 2.0 * c->mu);
+        bs->med = ok_med(okada_mode == UCG_OKADA_REF32IO ? (double)f32(alpha_d) : alpha_d);
+    } else {
+        build_tri_sources(c, s);
+        bs->ns = c->nt;
+        bs->cst = NwConst{c->lambda / (c->lambda + c->mu) / 2.0, c->mu, c->lambda};
+    }
+    UCG_CUDA(cudaMalloc(&bs->src, sizeof(double) * s.size()));
+    UCG_CUDA(cudaMemcpy(bs->src, s.data(), sizeof(double) * s.size(), cudaMemcpyHostToDevice));
+    return UCG_OK;
+}
+
+void block_sources_free(BlockSources *bs)
+{
+    if (bs->src) cudaFree(bs->src);
+    bs->src = nullptr;
+}
+
+void assemble_block(ucg_ctx *c, const BlockSources &bs, const int *ridx, int nrb, const int *sidx, int nsb,
+                    double *out)
+{
+    const int TPB = 128;
+    dim3 grid((nsb + TPB - 1) / TPB, nrb < 65535 ? nrb : 65535);
+    if (bs.family == 0) {
+        if (bs.okada_mode == UCG_OKADA_REF32IO)
+            k_block_rect<true><<<grid, TPB, 0, c->stream>>>(out, ridx, nrb, sidx, nsb, c->rcv, bs.src, bs.ns,
+                                                           bs.med, c->mu, c->lambda);
+        else
+            k_block_rect<false><<<grid, TPB, 0, c->stream>>>(out, ridx, nrb, sidx, nsb, c->rcv, bs.src, bs.ns,
+                                                            bs.med, c->mu, c->lambda);
+        c->launches.count++;
+    } else {
+        k_block_tri<0><<<grid, TPB, 0, c->stream>>>(out, ridx, nrb, sidx, nsb, c->rcv, bs.src, bs.ns, bs.cst);
+        k_block_tri<1><<<grid, TPB, 0, c->stream>>>(out, ridx, nrb, sidx, nsb, c->rcv, bs.src, bs.ns, bs.cst);
+        k_block_tri<2><<<grid, TPB, 0, c->stream>>>(out, ridx, nrb, sidx, nsb, c->rcv, bs.src, bs.ns, bs.cst);
+        c->launches.count += 3;
+    }
+}
+
+// element bounding boxes (lo[3], hi[3] per element, patches in K's order) and centres
+void element_boxes(const ucg_ctx *c, std::vector<double> &box, std::vector<double> &ctr)
+{
+    const int np = c->nr + c->nt;
+    box.assign(6L * np, 0.0);
+    ctr.assign(3L * np, 0.0);
+    for (int i = 0; i < np; i++) {
+        double p[4][3];
+        int nv;
+        if (i < c->nr) {
+            const double st = c->rstrike[i], dp = c->rdip[i];
+            const double sv[3] = {cos(st), sin(st), 0.0};
+            const double dv[3] = {+sin(st) * cos(dp), -cos(st) * cos(dp), -sin(dp)};
+            for (int k = 0; k < 3; k++) {
+                const double x = c->rx[3 * i + k];
+                p[0][k] = x;
+                p[1][k] = x + c->rL[i] * sv[k];
+                p[2][k] = x + c->rL[i] * sv[k] - c->rW[i] * dv[k];
+                p[3][k] = x - c->rW[i] * dv[k];
+            }
+            nv = 4;
+        } else {
+            const int j = i - c->nr;
+            const int id[3] = {c->ti1[j] - 1, c->ti2[j] - 1, c->ti3[j] - 1};
+            for (int q = 0; q < 3; q++)
+                for (int k = 0; k < 3; k++) p[q][k] = c->tvert[3L * id[q] + k];
+            nv = 3;
+        }
+        for (int k = 0; k < 3; k++) {
+            double lo = p[0][k], hi = p[0][k], s = 0.0;
+            for (int q = 0; q < nv; q++) {
+                lo = std::fmin(lo, p[q][k]);
+                hi = std::fmax(hi, p[q][k]);
+                s += p[q][k];
+            }
+            box[6L * i + k] = lo;
+            box[6L * i + 3 + k] = hi;
+            ctr[3L * i + k] = s / nv;
+        }
+    }
 }
 
 }  // namespace ucg

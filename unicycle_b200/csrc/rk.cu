@@ -208,6 +208,20 @@ __device__ __forceinline__ void rhs_patch(const StageArgs &a, const double *yy, 
     ks[o + 6] = dv;
 }
 
+// Right-hand side of every patch from a traction vector already formed (the
+// hierarchical product): the epilogue of k_traction without the matvec.
+template <int S>
+__global__ void k_rhs_t(StageArgs a, const Ctl *ctl, const double *__restrict__ t)
+{
+    if (!ctl_live(ctl)) return;
+    if (S == 1 && !ctl->need_stage1) return;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.np) return;
+    const double *yy = (S == 1) ? a.y : a.ys;
+    const double tr[3] = {t[3L * e], t[3L * e + 1], t[3L * e + 2]};
+    rhs_patch(a, yy, a.k[S - 1], e, tr);
+}
+
 // ---- TMA bulk-copy pipeline ------------------------------------------------------
 //
 // The traction product streams K once per stage evaluation and is bound by HBM
@@ -778,10 +792,18 @@ static void enqueue_stage(ucg_ctx *c)
     const int ne = c->nr + c->nt + c->nv;
     StageArgs a = stage_args(c, S);
     k_prologue<S><<<(ne + 127) / 128, 128, 0, c->stream>>>(a, c->ctl);
+    c->launches.count += 1;
+    if (c->precision == UCG_PREC_HMATRIX) {
+        double *t = hmatrix_t(c);
+        hmatrix_apply(c, c->st.v, t);
+        k_rhs_t<S><<<(c->nr + c->nt + 127) / 128, 128, 0, c->stream>>>(a, c->ctl, t);
+        c->launches.count += 1;
+        return;
+    }
     int pb, vb;
     int grid = traction_grid(c, &pb, &vb);
     launch_traction<S>(c, a, grid, pb, vb);
-    c->launches.count += 2;
+    c->launches.count += 1;
 }
 
 static void enqueue_attempt_raw(ucg_ctx *c)
@@ -813,6 +835,7 @@ void rk_enqueue_attempt(ucg_ctx *c)
         long before = c->launches.count;
         if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
             enqueue_attempt_raw(c);
+            c->graph_launches = c->launches.count - before;
             if (cudaStreamEndCapture(c->stream, &g) == cudaSuccess) {
                 if (cudaGraphInstantiate(&c->attempt_graph, g, 0) != cudaSuccess) c->attempt_graph = nullptr;
                 cudaGraphDestroy(g);
@@ -824,7 +847,7 @@ void rk_enqueue_attempt(ucg_ctx *c)
     }
     if (c->attempt_graph) {
         cudaGraphLaunch(c->attempt_graph, c->stream);
-        c->launches.count += 14;
+        c->launches.count += c->graph_launches;
     } else {
         enqueue_attempt_raw(c);
     }
@@ -899,13 +922,28 @@ __global__ void k_perturb(const double *__restrict__ K, long m, long n, int np, 
     }
 }
 
+// the same with the stress change t = H u already formed (hierarchical matrix)
+__global__ void k_perturb_t(long m, long n, int np, const double *__restrict__ t, const double *__restrict__ u,
+                            double *__restrict__ y)
+{
+    const long i0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nt = (long)gridDim.x * blockDim.x;
+    for (long r = i0; r < m; r += nt) y[7L * (r / 3) + 2 + r % 3] += t[r];
+    for (long c = i0; c < n; c += nt) y[7L * (c >> 1) + (c & 1)] += u[c];
+}
+
 int rk_perturb(ucg_ctx *c, const double *u)
 {
-    if (!c->K) return UCG_E_STATE;
+    if (!c->K && !(c->hm && c->nv == 0)) return UCG_E_STATE;
     if (!c->pert) UCG_CUDA(cudaMalloc(&c->pert, sizeof(double) * c->n));
     UCG_CUDA(cudaMemcpyAsync(c->pert, u, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->stream));
     const int blocks = (int)std::min<long>((c->m + 7) / 8, 8L * c->sms);
-    k_perturb<<<blocks, 256, 0, c->stream>>>(c->K, c->m, c->n, c->nr + c->nt, c->pert, c->st.y);
+    if (c->K) {
+        k_perturb<<<blocks, 256, 0, c->stream>>>(c->K, c->m, c->n, c->nr + c->nt, c->pert, c->st.y);
+    } else {
+        double *t = hmatrix_t(c);
+        hmatrix_apply(c, c->pert, t);
+        k_perturb_t<<<blocks, 256, 0, c->stream>>>(c->m, c->n, c->nr + c->nt, t, c->pert, c->st.y);
+    }
     c->launches.count++;
     UCG_CUDA(cudaGetLastError());
     UCG_CUDA(cudaStreamSynchronize(c->stream));

@@ -112,6 +112,7 @@ void ucg_destroy(ucg_ctx *c)
     split_bf16_free(c);
     free_params(c);
     free_observation(c);
+    hmatrix_free(c);
     if (c->K) cudaFree(c->K);
     if (c->rcv) cudaFree(c->rcv);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -125,6 +126,8 @@ static void invalidate(ucg_ctx *c)
     rk_free(c);
     split_bf16_free(c);
     free_observation(c);
+    hmatrix_free(c);
+    if (c->precision == UCG_PREC_HMATRIX) c->precision = UCG_PREC_FP64;
 }
 
 int ucg_set_rectangles(ucg_ctx *c, int n, const double *x, const double *L, const double *W,
@@ -322,7 +325,13 @@ int ucg_copy_G(ucg_ctx *c, double *G, long ld, long k0, long k1)
 int ucg_set_precision(ucg_ctx *c, int precision)
 {
     if (!c) return UCG_E_BADARG;
-    if (precision != UCG_PREC_FP64 && precision != UCG_PREC_SPLIT_BF16) return bad(c, "precision");
+    if (precision != UCG_PREC_FP64 && precision != UCG_PREC_SPLIT_BF16 && precision != UCG_PREC_HMATRIX)
+        return bad(c, "precision");
+    if (precision == UCG_PREC_HMATRIX) {
+        if (!c->hm) return set_err(c, UCG_E_STATE, "build the hierarchical matrix first (ucg_build_hmatrix)");
+        c->precision = precision;
+        return UCG_OK;
+    }
     if (precision == UCG_PREC_FP64 && c->assembled && !c->K)
         return set_err(c, UCG_E_STATE, "FP64 matrix was released; re-assemble");
     c->precision = precision;
@@ -391,10 +400,11 @@ int ucg_init_state(ucg_ctx *c, double *y, const double *nGm, const double *nQm, 
 
 static int ensure_state(ucg_ctx *c)
 {
-    if (!c->assembled) return set_err(c, UCG_E_STATE, "matrix not assembled");
+    if (!c->assembled && !c->hm) return set_err(c, UCG_E_STATE, "matrix not assembled");
     if (c->nr + c->nt > 0 && !c->have_friction) return set_err(c, UCG_E_STATE, "friction not set");
     if (c->nv > 0 && !c->have_rheology) return set_err(c, UCG_E_STATE, "rheology not set");
-    if (c->precision == UCG_PREC_FP64 && !c->K) return set_err(c, UCG_E_STATE, "FP64 matrix released");
+    if (c->precision == UCG_PREC_FP64 && !c->K) return set_err(c, UCG_E_STATE, "FP64 matrix released or not assembled");
+    if (c->precision == UCG_PREC_HMATRIX && !c->hm) return set_err(c, UCG_E_STATE, "hierarchical matrix not built");
     if (!c->state_ready) {
         c->state_len = ucg_state_len(c);
         int rc = rk_alloc(c);
@@ -607,6 +617,80 @@ int ucg_displacements(ucg_ctx *c, const double *y, double *d, double *d_fault, d
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(buf);
     if (e != cudaSuccess) return cuda_fail(c, e, "ucg_displacements");
+    return UCG_OK;
+}
+
+int ucg_build_hmatrix(ucg_ctx *c, int okada_mode, double eta, double eps, int leaf)
+{
+    if (!c) return UCG_E_BADARG;
+    if (okada_mode != UCG_OKADA_FP64 && okada_mode != UCG_OKADA_REF32IO) return bad(c, "okada_mode");
+    if (!(eta > 0.0) || !(eps > 0.0 && eps < 1.0) || leaf < 4) return bad(c, "hierarchical matrix parameters");
+    if (c->nr + c->nt == 0) return set_err(c, UCG_E_STATE, "no elements");
+    UCG_CUDA(cudaSetDevice(c->device));
+    rk_drop_graph(c);
+    const long n = 2L * (c->nr + c->nt) + 6L * c->nv, m = 3L * (c->nr + c->nt) + 6L * c->nv;
+    if (c->state_ready && (c->n != n || c->m != m)) {
+        rk_free(c);
+        c->state_ready = false;
+    }
+    c->n = n;
+    c->m = m;
+    return hmatrix_build(c, okada_mode, eta, eps, leaf);
+}
+
+int ucg_hmatrix_info(ucg_ctx *c, long *n_dense, long *n_lowrank, long *bytes, int *max_rank, double *build_ms)
+{
+    if (!c) return UCG_E_BADARG;
+    if (!c->hm) return set_err(c, UCG_E_STATE, "hierarchical matrix not built");
+    size_t b = 0;
+    hmatrix_info(c, n_dense, n_lowrank, nullptr, &b, max_rank, build_ms);
+    if (bytes) *bytes = (long)b;
+    return UCG_OK;
+}
+
+int ucg_hmatrix_matvec(ucg_ctx *c, const double *x, double *y)
+{
+    if (!c || !x || !y) return UCG_E_BADARG;
+    if (!c->hm) return set_err(c, UCG_E_STATE, "hierarchical matrix not built");
+    UCG_CUDA(cudaSetDevice(c->device));
+    double *xd = nullptr;
+    UCG_CUDA(cudaMalloc(&xd, sizeof(double) * (c->n + 2)));
+    cudaError_t e = cudaMemcpyAsync(xd, x, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        double *t = hmatrix_t(c);
+        hmatrix_apply(c, xd, t);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(y, t, sizeof(double) * c->m, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(xd);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ucg_hmatrix_matvec");
+    return UCG_OK;
+}
+
+int ucg_hmatrix_profile(ucg_ctx *c, int reps, double *ms)
+{
+    if (!c || reps <= 0 || !ms) return UCG_E_BADARG;
+    if (!c->hm) return set_err(c, UCG_E_STATE, "hierarchical matrix not built");
+    UCG_CUDA(cudaSetDevice(c->device));
+    double *xd = nullptr;
+    UCG_CUDA(cudaMalloc(&xd, sizeof(double) * (c->n + 2)));
+    UCG_CUDA(cudaMemsetAsync(xd, 0, sizeof(double) * (c->n + 2), c->stream));
+    cudaEvent_t e0, e1;
+    UCG_CUDA(cudaEventCreate(&e0));
+    UCG_CUDA(cudaEventCreate(&e1));
+    double *t = hmatrix_t(c);
+    hmatrix_apply(c, xd, t);   // warm-up
+    UCG_CUDA(cudaEventRecord(e0, c->stream));
+    for (int r = 0; r < reps; r++) hmatrix_apply(c, xd, t);
+    UCG_CUDA(cudaEventRecord(e1, c->stream));
+    UCG_CUDA(cudaEventSynchronize(e1));
+    float f = 0.0f;
+    cudaEventElapsedTime(&f, e0, e1);
+    *ms = (double)f / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(xd);
     return UCG_OK;
 }
 

@@ -9,6 +9,7 @@
 #include "../../include/ucg.h"
 
 namespace ucg {
+struct HMat;
 
 // Device-resident integrator control block (one per context).
 struct Ctl {
@@ -181,8 +182,11 @@ struct ucg_ctx {
     std::vector<Event> events;
     double *pert = nullptr;      // device copy of the perturbation being applied (n)
 
+    ucg::HMat *hm = nullptr;     // hierarchical approximation of K (hmatrix.cu)
+
     cudaGraphExec_t attempt_graph = nullptr;
     int graph_precision = -1;
+    long graph_launches = 0;     // kernels in one launch of the attempt graph
     int sms = 148;
 
     ucg::Launches launches;
@@ -205,6 +209,13 @@ int rk_perturb(ucg_ctx *c, const double *u); // y += slip/strain u and the stres
 void rk_drop_graph(ucg_ctx *c);             // before freeing anything the attempt graph reads
 int split_bf16_build(ucg_ctx *c);
 void split_bf16_free(ucg_ctx *c);
+// hmatrix.cu
+int hmatrix_build(ucg_ctx *c, int okada_mode, double eta, double eps, int leaf);
+void hmatrix_free(ucg_ctx *c);
+void hmatrix_apply(ucg_ctx *c, const double *v, double *t);   // t = H v, K's row order
+double *hmatrix_t(ucg_ctx *c);                                 // the product's output buffer
+void hmatrix_info(const ucg_ctx *c, long *n_dense, long *n_lowrank, long *n_fallback, size_t *bytes,
+                  int *max_rank, double *build_ms);
 
 // mlp.cu: device addresses of a step-size model's FP16 weights and standardisation
 }  // namespace ucg

@@ -110,6 +110,32 @@ class Simulation:
     def buildG(self, okada_mode=_lib.UCG_OKADA_FP64):
         self._check(self.lib.ucg_assemble(self.ctx, okada_mode), "buildG")
 
+    def build_hmatrix(self, okada_mode=_lib.UCG_OKADA_FP64, eta=2.0, eps=1.0e-6, leaf=32):
+        """Hierarchical approximation of K (one patch family): clusters of `leaf`
+        patches, admissibility max(diam) <= eta dist, ACA to relative accuracy eps."""
+        self._check(self.lib.ucg_build_hmatrix(self.ctx, okada_mode, float(eta), float(eps), int(leaf)),
+                    "build_hmatrix")
+
+    def hmatrix_info(self):
+        nd, nl, b, r, ms = ctypes.c_long(), ctypes.c_long(), ctypes.c_long(), ctypes.c_int(), ctypes.c_double()
+        self._check(self.lib.ucg_hmatrix_info(self.ctx, ctypes.byref(nd), ctypes.byref(nl), ctypes.byref(b),
+                                              ctypes.byref(r), ctypes.byref(ms)), "hmatrix_info")
+        n, m = self.dims
+        return dict(n_dense=nd.value, n_lowrank=nl.value, bytes=b.value, max_rank=r.value, build_ms=ms.value,
+                    dense_bytes=8 * n * m, compression=8.0 * n * m / max(b.value, 1))
+
+    def hmatrix_matvec(self, x):
+        n, m = self.dims
+        x = _d(x)
+        y = np.empty(m)
+        self._check(self.lib.ucg_hmatrix_matvec(self.ctx, _p(x), _p(y)), "hmatrix_matvec")
+        return y
+
+    def hmatrix_profile(self, reps=20):
+        ms = ctypes.c_double()
+        self._check(self.lib.ucg_hmatrix_profile(self.ctx, reps, ctypes.byref(ms)), "hmatrix_profile")
+        return ms.value
+
     def assembly_times(self):
         """Device ms of the last buildG per source family: (rectangles, triangles, volumes)."""
         a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
