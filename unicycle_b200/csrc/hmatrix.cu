@@ -23,16 +23,17 @@
 //              checked against the dense block on a pseudo-random probe
 //              vector; a block that fails the check, or whose factors would not
 //              be smaller, is kept dense.
-//   storage    FP64.  U is stored rank-major (k x m), V rank-major (k x n),
-//              dense blocks column-major.
+//   storage    FP64.  V is stored rank-major (k x n); the rows of U and of the
+//              dense blocks are repacked into panels, one per row leaf and chunk
+//              of at most 16 KB, each a column-major (rows x columns) slab.
 //   product    t = H v: v is gathered into the permuted order (every block's
-//              columns become a contiguous slice), z_b = V_b^T v_sigma for every
-//              low-rank block (one warp per rank vector); then, per chunk of
-//              about 96 KB of a row leaf's blocks, one thread per row sweeps the
-//              dense columns times v and the U columns times z (consecutive rows
-//              are consecutive addresses in both layouts); a last kernel adds a
-//              leaf's chunks in order and writes K's row order.  Every stored byte is read once per product and
-//              the summation order is fixed (deterministic).
+//              columns become a contiguous slice); z_b = V_b^T v_sigma for every
+//              low-rank block (one warp per rank vector); one CTA per chunk
+//              copies its panel into shared memory with one bulk copy and one
+//              thread per row multiplies it by the matching slices of v or z;
+//              a last kernel adds a leaf's chunks in order and writes K's row
+//              order.  Every stored byte is read once per product and the
+//              summation order is fixed (deterministic).
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -418,7 +419,7 @@ __global__ void k_hm_z(const HLowRank *__restrict__ lr, const int2 *__restrict__
 // order.  Many small CTAs per SM keep many copies in flight.  The wait for the
 // copy is bounded (about 4 s); when it runs out the chunk writes NaN, which the
 // integrator reports as a non-finite rate, and the kernel flags status.
-constexpr long HM_CHUNK_BYTES = 32 * 1024;
+constexpr long HM_CHUNK_BYTES = 16 * 1024;
 constexpr unsigned long long HM_TIMEOUT_NS = 4000000000ull;
 
 __device__ __forceinline__ uint32_t hm_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -522,9 +523,16 @@ __global__ void k_hm_reduce(const int *__restrict__ leaf_e0, const int *__restri
     const int e0 = leaf_e0[L], rows = 3 * (leaf_e0[L + 1] - e0);
     const int c0 = leaf_chunk[L], c1 = leaf_chunk[L + 1];
     for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-        double s = 0.0;
-        for (int c = c0; c < c1; c++) s += part[(long)c * rows_max + i];
-        t[3L * perm[e0 + i / 3] + i % 3] = s;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int c = c0;
+        for (; c + 3 < c1; c += 4) {
+            s0 += part[(long)c * rows_max + i];
+            s1 += part[(long)(c + 1) * rows_max + i];
+            s2 += part[(long)(c + 2) * rows_max + i];
+            s3 += part[(long)(c + 3) * rows_max + i];
+        }
+        for (; c < c1; c++) s0 += part[(long)c * rows_max + i];
+        t[3L * perm[e0 + i / 3] + i % 3] = (s0 + s1) + (s2 + s3);
     }
 }
 
@@ -838,6 +846,7 @@ int hmatrix_build(ucg_ctx *c, int okada_mode, double eta, double eps, int leaf)
     UCG_CUDA(cudaMalloc(&h->z_d, sizeof(double) * h->nz));
     UCG_CUDA(cudaMalloc(&h->t_d, sizeof(double) * (3L * np + 2)));
     UCG_CUDA(cudaMalloc(&h->xp_d, sizeof(double) * (2L * np + 2)));
+    UCG_CUDA(cudaFuncSetAttribute(k_hm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HM_CHUNK_BYTES));
     UCG_CUDA(cudaMalloc(&h->status_d, sizeof(int)));
     UCG_CUDA(cudaMemset(h->status_d, 0, sizeof(int)));
     UCG_CUDA(cudaMalloc(&h->part_d, sizeof(double) * (size_t)h->n_chunks * 3 * h->max_leaf));
