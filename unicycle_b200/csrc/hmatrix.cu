@@ -515,24 +515,34 @@ __global__ void k_pack(const PackJob *__restrict__ jobs, double *__restrict__ pa
     }
 }
 
+// t for one row leaf: blockDim / gs groups of gs threads (gs >= rows) each add
+// every ng-th chunk of the leaf, then group 0 adds the groups' sums in order.
 __global__ void k_hm_reduce(const int *__restrict__ leaf_e0, const int *__restrict__ leaf_chunk,
                             const int *__restrict__ perm, const double *__restrict__ part, int rows_max,
-                            double *__restrict__ t)
+                            double *__restrict__ t, int gs)
 {
+    extern __shared__ double sh[];
     const int L = blockIdx.x;
     const int e0 = leaf_e0[L], rows = 3 * (leaf_e0[L + 1] - e0);
     const int c0 = leaf_chunk[L], c1 = leaf_chunk[L + 1];
-    for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int c = c0;
-        for (; c + 3 < c1; c += 4) {
+    const int ng = blockDim.x / gs, g = threadIdx.x / gs, i = threadIdx.x % gs;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    if (i < rows) {
+        int c = c0 + g;
+        for (; c + 3 * ng < c1; c += 4 * ng) {
             s0 += part[(long)c * rows_max + i];
-            s1 += part[(long)(c + 1) * rows_max + i];
-            s2 += part[(long)(c + 2) * rows_max + i];
-            s3 += part[(long)(c + 3) * rows_max + i];
+            s1 += part[(long)(c + ng) * rows_max + i];
+            s2 += part[(long)(c + 2 * ng) * rows_max + i];
+            s3 += part[(long)(c + 3 * ng) * rows_max + i];
         }
-        for (; c < c1; c++) s0 += part[(long)c * rows_max + i];
-        t[3L * perm[e0 + i / 3] + i % 3] = (s0 + s1) + (s2 + s3);
+        for (; c < c1; c += ng) s0 += part[(long)c * rows_max + i];
+    }
+    sh[threadIdx.x] = (s0 + s1) + (s2 + s3);
+    __syncthreads();
+    if (g == 0 && i < rows) {
+        double s = 0.0;
+        for (int k = 0; k < ng; k++) s += sh[k * gs + i];
+        t[3L * perm[e0 + i / 3] + i % 3] = s;
     }
 }
 
@@ -882,7 +892,9 @@ void hmatrix_apply(ucg_ctx *c, const double *v, double *t)
     const int rows = 3 * h->max_leaf;
     k_hm_rows<<<h->n_chunks, ((rows + 31) / 32) * 32, HM_CHUNK_BYTES, c->stream>>>(
         h->terms_d, h->chunks_d, h->leaf_e0_d, h->panel, h->xp_d, h->z_d, h->part_d, rows, h->status_d);
-    k_hm_reduce<<<h->n_leaves, 128, 0, c->stream>>>(h->leaf_e0_d, h->leaf_chunk_d, h->perm_d, h->part_d, rows, t);
+    const int gs = ((rows + 31) / 32) * 32, nthr = std::max(gs, (1024 / gs) * gs);
+    k_hm_reduce<<<h->n_leaves, nthr, sizeof(double) * nthr, c->stream>>>(h->leaf_e0_d, h->leaf_chunk_d, h->perm_d,
+                                                                         h->part_d, rows, t, gs);
     c->launches.count += 3;
 }
 
