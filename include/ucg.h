@@ -319,6 +319,8 @@ typedef struct {
     long chunk;               /* iterations per device run between recorder drains */
     const char *wdir;         /* output directory; NULL: the deck's */
     int verbose;              /* progress lines on standard output */
+    double hm_eta, hm_eps;    /* UCG_PREC_HMATRIX: ucg_build_hmatrix parameters (0: 2, 1e-6) */
+    int hm_leaf;              /*   and leaf size (0: 32); the dense K is then never assembled */
 } ucg_run_options;
 
 /* The whole run of a deck, as the reference's main program does it

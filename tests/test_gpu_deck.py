@@ -114,3 +114,41 @@ def test_viscous_deck_run(ucg, tmp_path):
         np.testing.assert_allclose(D[i, 1:], want, rtol=1e-12, atol=1e-15 * np.abs(want).max())
     assert os.path.exists(tmp_path / "patch-00000003.dat")
     sim.close()
+
+
+def test_deck_run_on_hierarchical_matrix(ucg, tmp_path):
+    """A deck run on the hierarchical K (no dense K assembled) writes the files
+    of the host-driven step loop on the same hierarchical K, line for line (the
+    product is deterministic).  Against the dense run only the first steps are
+    compared: the reference's step control follows the rounding residue of
+    near-zero components at start-up, so any change of the product, even one
+    ulp of K, moves the later step sequence."""
+    from unicycle_b200 import Deck, configs, write_deck
+    c = configs.cfg1(nx=32, nz=16)
+    pts = [("GPS1", (5000.0, 3000.0, 0.0))]
+    n = 40
+    d = Deck(write_deck(c, wdir=str(tmp_path), obs_patches=[7], obs_points=pts))
+    it, _ = d.run(maximum_iterations=n, epsilon=1e-6, chunk=16, okada_mode=0, precision=ucg.UCG_PREC_HMATRIX,
+                  hm_leaf=16)
+    assert it == n
+    sim = d.simulation()
+    sim.build_hmatrix(okada_mode=0, eta=2.0, eps=1e-6, leaf=16)
+    sim.set_precision(ucg.UCG_PREC_HMATRIX)
+    sim.set_observation_points([p for _, p in pts])
+    sim.buildO(0)
+    seen = _step_loop(sim, d.init_state(sim), n, 1e-6)
+    _, T = _rows(tmp_path / "time.txt", skip=1)
+    np.testing.assert_allclose(T[1:, 0], [s_[0] for s_ in seen], rtol=1e-12)
+    _, P = _rows(tmp_path / "patch-00000007.dat", w=20)
+    np.testing.assert_allclose(P[:, 1:8], np.array([s_[1][42:49] for s_ in seen]), rtol=1e-12, atol=1e-300)
+    _, D = _rows(tmp_path / "opts-GPS1.dat")
+    want = np.array([sim.displacements(s_[1])[0][0] for s_ in seen])
+    np.testing.assert_allclose(D[:, 1:], want, rtol=1e-12, atol=1e-15 * np.abs(want).max())
+    sim.close()
+    # the dense run agrees over the first steps
+    wd = tmp_path / "dense"
+    wd.mkdir()
+    Deck(write_deck(c, wdir=str(wd), obs_patches=[7], obs_points=pts)).run(
+        maximum_iterations=n, epsilon=1e-6, chunk=16, okada_mode=0)
+    _, Td = _rows(wd / "time.txt", skip=1)
+    np.testing.assert_allclose(T[:4, 0], Td[:4, 0], rtol=1e-9)

@@ -55,7 +55,8 @@ class DeckInfo(ctypes.Structure):
 class RunOptions(ctypes.Structure):
     """ucg_run_options"""
     _fields_ = [("epsilon", _d), ("maximum_step", _d), ("maximum_iterations", _l), ("okada_mode", _i),
-                ("precision", _i), ("device", _i), ("chunk", _l), ("wdir", ctypes.c_char_p), ("verbose", _i)]
+                ("precision", _i), ("device", _i), ("chunk", _l), ("wdir", ctypes.c_char_p), ("verbose", _i),
+                ("hm_eta", _d), ("hm_eps", _d), ("hm_leaf", _i)]
 
 
 # name -> (restype, argtypes); the complete exported surface of include/ucg.h

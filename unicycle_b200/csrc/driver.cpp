@@ -86,7 +86,15 @@ extern "C" int ucg_deck_run(const ucg_deck *deck, const ucg_run_options *opt, lo
         ~Guard() { ucg_destroy(c); }
     } guard{c};
     if ((rc = ucg_set_tolerance(c, opt->epsilon, opt->maximum_step))) return rc;
-    if ((rc = ucg_assemble(c, opt->okada_mode))) return rc;
+    if (opt->precision == UCG_PREC_HMATRIX) {
+        // hierarchical K only: the dense K is never assembled
+        const double eta = opt->hm_eta > 0.0 ? opt->hm_eta : 2.0;
+        const double eps = opt->hm_eps > 0.0 ? opt->hm_eps : 1.0e-6;
+        const int leaf = opt->hm_leaf > 0 ? opt->hm_leaf : 32;
+        if ((rc = ucg_build_hmatrix(c, opt->okada_mode, eta, eps, leaf))) return rc;
+    } else if ((rc = ucg_assemble(c, opt->okada_mode))) {
+        return rc;
+    }
     if (opt->precision != UCG_PREC_FP64 && (rc = ucg_set_precision(c, opt->precision))) return rc;
     const int nobs = info.n_obs_point;
     if (nobs > 0 && (rc = ucg_build_O(c, opt->okada_mode))) return rc;

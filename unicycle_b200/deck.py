@@ -98,13 +98,17 @@ class Deck:
         return y
 
     def run(self, wdir=None, epsilon=1.0e-6, maximum_step=None, maximum_iterations=1000000,
-            okada_mode=_lib.UCG_OKADA_REF32IO, precision=_lib.UCG_PREC_FP64, device=0, chunk=4096, verbose=False):
+            okada_mode=_lib.UCG_OKADA_REF32IO, precision=_lib.UCG_PREC_FP64, device=0, chunk=4096, verbose=False,
+            hm_eta=0.0, hm_eps=0.0, hm_leaf=0):
         """The reference's main program on the device; writes time.txt, the
         observation-state and observation-point files into wdir (default: the
-        deck's output directory).  Returns (iterations, final time)."""
+        deck's output directory).  precision UCG_PREC_HMATRIX builds the
+        hierarchical K (hm_eta, hm_eps, hm_leaf; 0 for the defaults) instead
+        of the dense one.  Returns (iterations, final time)."""
         o = _lib.RunOptions(epsilon, 1.7976931348623157e308 if maximum_step is None else maximum_step,
                             maximum_iterations, okada_mode, precision, device, chunk,
-                            None if wdir is None else os.fspath(wdir).encode(), int(verbose))
+                            None if wdir is None else os.fspath(wdir).encode(), int(verbose), float(hm_eta),
+                            float(hm_eps), int(hm_leaf))
         it, t = ctypes.c_long(), ctypes.c_double()
         st = self.lib.ucg_deck_run(self.h, ctypes.byref(o), ctypes.byref(it), ctypes.byref(t))
         if st:
