@@ -43,6 +43,8 @@ typedef struct ucg_ctx ucg_ctx;
 #define UCG_PREC_FP64        0  /* K in binary64, FP64 matvec (the plain method) */
 #define UCG_PREC_SPLIT_BF16  1  /* K = diag(s)(hi + lo), bf16 hi/lo, FP32 accumulation */
 #define UCG_PREC_HMATRIX     2  /* hierarchical approximation of K (ucg_build_hmatrix), FP64 */
+#define UCG_PREC_HMATRIX_SPLIT 3  /* the same stored as bf16 hi + lo, anchored stages (hi alone for
+                                     the stage increments), FP64 sums */
 
 /* driver conventions (ucg_create flags) */
 #define UCG_DRIVER_RATESTATE      0  /* fortran/3d/src/ratestate.f90     */

@@ -126,3 +126,35 @@ def test_hmatrix_without_dense_matrix(ucg):
     assert sim.run(1e30, 50) == 50
     sim.close()
     dense.close()
+
+
+def test_hmatrix_split_matches_fp64(ucg):
+    """The hierarchical K stored as bf16 hi + lo with anchored stages: the
+    right-hand side within the split product's bound of the FP64 hierarchical
+    one, and the first event's onset within 1e-4 of the FP64 integrator's."""
+    from unicycle_b200 import configs
+    cfg = configs.cfg4(shapes=((32, 16),), n_sets=2, size=1250.0, seed=11)
+    g = cfg["geoms"][0]
+    sim = ucg.Simulation(g["mu"], g["lam"])
+    configs.build(sim, g)
+    sim.build_hmatrix(eta=2.0, eps=1e-6, leaf=32)
+    fr = g["sets"][0]
+    sim.set_friction(fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"], fr["damping"])
+    y0 = g["y0s"][0]
+    sim.set_precision(ucg.UCG_PREC_HMATRIX)
+    d64, _ = sim.odefun(y0)
+    sim.set_precision(ucg.UCG_PREC_HMATRIX_SPLIT)
+    dsp, _ = sim.odefun(y0)
+    idx = np.concatenate([np.arange(q, len(y0), 7) for q in (2, 3, 4)])
+    rel = np.max(np.abs(dsp[idx] - d64[idx])) / np.max(np.abs(d64[idx]))
+    print(f"split vs FP64 hierarchical right-hand side: {rel:.2e}")
+    assert rel < 1e-4
+    sim.set_precision(ucg.UCG_PREC_FP64)
+    t64, k64 = _first_event(sim, y0, cfg["dt0"])
+    sim.set_precision(ucg.UCG_PREC_HMATRIX_SPLIT)
+    ts, ks = _first_event(sim, y0, cfg["dt0"])
+    print(f"fp64 onset {t64:.9e} ({k64} steps); hmatrix split {ts:.9e} ({ks} steps); rel {abs(ts - t64) / t64:.2e}")
+    assert t64 is not None and ts is not None
+    assert abs(ts - t64) <= 1e-4 * t64
+    assert ks <= 1.5 * k64 + 20
+    sim.close()

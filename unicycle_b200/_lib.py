@@ -25,6 +25,7 @@ UCG_OKADA_REF32IO = 1
 UCG_PREC_FP64 = 0
 UCG_PREC_SPLIT_BF16 = 1
 UCG_PREC_HMATRIX = 2
+UCG_PREC_HMATRIX_SPLIT = 3
 UCG_DRIVER_RATESTATE = 0
 UCG_DRIVER_VISCOUSCYCLES = 1
 UCG_ENS_STREAM_K = 0

@@ -86,7 +86,7 @@ extern "C" int ucg_deck_run(const ucg_deck *deck, const ucg_run_options *opt, lo
         ~Guard() { ucg_destroy(c); }
     } guard{c};
     if ((rc = ucg_set_tolerance(c, opt->epsilon, opt->maximum_step))) return rc;
-    if (opt->precision == UCG_PREC_HMATRIX) {
+    if (opt->precision == UCG_PREC_HMATRIX || opt->precision == UCG_PREC_HMATRIX_SPLIT) {
         // hierarchical K only: the dense K is never assembled
         const double eta = opt->hm_eta > 0.0 ? opt->hm_eta : 2.0;
         const double eps = opt->hm_eps > 0.0 ? opt->hm_eps : 1.0e-6;

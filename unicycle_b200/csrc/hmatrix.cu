@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cuda_bf16.h>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -55,6 +56,7 @@ struct HLowRank {            // device descriptor of a stored low-rank block
     int k, m, n, s0;         // rank, rows, columns, first source element (permuted)
     int r0;                  // first receiver element (permuted)
     int zoff;                // offset of its z in the product's workspace
+    long vsoff;              // offset of its V in the split (bf16 hi / lo) copy
 };
 
 struct HLeafTerm {           // the rows of one row leaf in one block (or a range of its columns)
@@ -97,6 +99,10 @@ struct HMat {
     double *part_d = nullptr;            // partial row sums (chunk, row)
     double *xp_d = nullptr;              // the product's input in the permuted order
     double *panel = nullptr;             // the row data of every chunk, chunk after chunk
+    long panel_len = 0;                  // doubles
+    std::vector<HLowRank> lr_h;          // host copy of the low-rank descriptors
+    // split copies (hi and lo bf16 of every value) for UCG_PREC_HMATRIX_SPLIT
+    __nv_bfloat16 *ph = nullptr, *pl = nullptr, *vh = nullptr, *vl = nullptr;
     int *status_d = nullptr;             // nonzero: a bulk copy of the row kernel timed out
     double *t_d = nullptr;               // product output (K's row order)
 };
@@ -494,7 +500,139 @@ __global__ void __launch_bounds__(128) k_hm_rows(const HLeafTerm *__restrict__ t
             a3 = fma(col[(j + 3) * rows], x[j + 3], a3);
         }
         for (; j < T.cols; j++) a0 = fma(col[j * rows], x[j], a0);
-        off += ((long)rows * T.cols + 1) & ~1L;
+        off += ((long)rows * T.cols + 7) & ~7L;
+    }
+    part[(long)blockIdx.x * rows_max + i] = (a0 + a1) + (a2 + a3);
+}
+
+// ---- split (bf16 hi + lo) form ---------------------------------------------------------
+//
+// Every stored value x is kept as hi = bf16(x) and lo = bf16(x - hi) (relative
+// error ~2^-16).  The anchored Runge-Kutta stages read hi and lo for the stage-1
+// product and hi alone for the stage increments (2 bytes per value), as the
+// dense split-BF16 path does.
+
+__global__ void k_split_flat(const double *__restrict__ x, long n, __nv_bfloat16 *__restrict__ hi,
+                             __nv_bfloat16 *__restrict__ lo)
+{
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const double v = x[t];
+        const __nv_bfloat16 h = __double2bfloat16(v);
+        hi[t] = h;
+        lo[t] = __double2bfloat16(v - (double)__bfloat162float(h));
+    }
+}
+
+struct SplitJob {
+    const double *src;
+    long n, dst;
+};
+
+__global__ void k_split_jobs(const SplitJob *__restrict__ jobs, __nv_bfloat16 *__restrict__ hi,
+                             __nv_bfloat16 *__restrict__ lo)
+{
+    const SplitJob J = jobs[blockIdx.x];
+    for (long t = threadIdx.x; t < J.n; t += blockDim.x) {
+        const double v = J.src[t];
+        const __nv_bfloat16 h = __double2bfloat16(v);
+        hi[J.dst + t] = h;
+        lo[J.dst + t] = __double2bfloat16(v - (double)__bfloat162float(h));
+    }
+}
+
+template <bool LO>
+__global__ void k_hm_z_split(const HLowRank *__restrict__ lr, const int2 *__restrict__ items, long n_items,
+                             const double *__restrict__ xp, const __nv_bfloat16 *__restrict__ vh,
+                             const __nv_bfloat16 *__restrict__ vl, double *__restrict__ z)
+{
+    const long w = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n_items) return;
+    const int2 it = items[w];
+    const HLowRank b = lr[it.x];
+    const long o = b.vsoff + (long)it.y * b.n;
+    const __nv_bfloat162 *h2 = reinterpret_cast<const __nv_bfloat162 *>(vh + o);
+    const __nv_bfloat162 *l2 = reinterpret_cast<const __nv_bfloat162 *>(vl + o);
+    const double2 *x = reinterpret_cast<const double2 *>(xp + 2L * b.s0);
+    double s0 = 0.0, s1 = 0.0;
+    for (int j = lane; j < (b.n >> 1); j += 32) {
+        const float2 a = __bfloat1622float2(h2[j]);
+        const double2 xx = x[j];
+        double a0 = a.x, a1 = a.y;
+        if (LO) {
+            const float2 c = __bfloat1622float2(l2[j]);
+            a0 += c.x;
+            a1 += c.y;
+        }
+        s0 = fma(a0, xx.x, s0);
+        s1 = fma(a1, xx.y, s1);
+    }
+    double s = s0 + s1;
+    for (int o2 = 16; o2 > 0; o2 >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o2);
+    if (lane == 0) z[b.zoff + it.y] = s;
+}
+
+// k_hm_rows on the split panels: the chunk's hi (and lo) bf16 values arrive by
+// bulk copy (a chunk of e values is 2 e bytes per half)
+template <bool LO>
+__global__ void __launch_bounds__(128) k_hm_rows_split(const HLeafTerm *__restrict__ terms,
+        const HChunk *__restrict__ chunks, const int *__restrict__ leaf_e0, const __nv_bfloat16 *__restrict__ ph,
+        const __nv_bfloat16 *__restrict__ pl, const double *__restrict__ xp, const double *__restrict__ z,
+        double *__restrict__ part, int rows_max, int *status)
+{
+    extern __shared__ __align__(128) __nv_bfloat16 sb[];
+    __shared__ __align__(8) uint64_t bar;
+    const HChunk ch = chunks[blockIdx.x];
+    const int rows = 3 * (leaf_e0[ch.leaf + 1] - leaf_e0[ch.leaf]);
+    const int i = threadIdx.x;
+    const long nel = ch.bytes / 8;            // values in the chunk
+    const uint32_t half = (uint32_t)(2 * nel);
+    if (nel == 0) {
+        if (i < rows) part[(long)blockIdx.x * rows_max + i] = 0.0;
+        return;
+    }
+    if (i == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(hm_smem(&bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (i == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(hm_smem(&bar)),
+                     "r"(LO ? 2 * half : half) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(hm_smem(sb)), "l"(ph + ch.off), "r"(half), "r"(hm_smem(&bar)) : "memory");
+        if (LO)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         ::"r"(hm_smem(sb + nel)), "l"(pl + ch.off), "r"(half), "r"(hm_smem(&bar)) : "memory");
+    }
+    const bool ok = hm_wait(&bar);
+    if (!__syncthreads_and(ok ? 1 : 0)) {
+        if (i == 0) atomicExch(status, 1);
+        if (i < rows) part[(long)blockIdx.x * rows_max + i] = nan("");
+        hm_wait(&bar);
+        return;
+    }
+    if (i >= rows) return;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    long off = 0;
+    for (int q = ch.q0; q < ch.q1; q++) {
+        const HLeafTerm T = terms[q];
+        const double *x = (T.xsel ? z : xp) + T.xoff;
+        const __nv_bfloat16 *col = sb + off + i;
+        auto val = [&](int j) -> double {
+            double v = (double)__bfloat162float(col[(long)j * rows]);
+            if (LO) v += (double)__bfloat162float(col[nel + (long)j * rows]);
+            return v;
+        };
+        int j = 0;
+        for (; j + 3 < T.cols; j += 4) {
+            a0 = fma(val(j), x[j], a0);
+            a1 = fma(val(j + 1), x[j + 1], a1);
+            a2 = fma(val(j + 2), x[j + 2], a2);
+            a3 = fma(val(j + 3), x[j + 3], a3);
+        }
+        for (; j < T.cols; j++) a0 = fma(val(j), x[j], a0);
+        off += ((long)rows * T.cols + 7) & ~7L;
     }
     part[(long)blockIdx.x * rows_max + i] = (a0 + a1) + (a2 + a3);
 }
@@ -558,7 +696,7 @@ void hmatrix_free(ucg_ctx *c)
     cudaStreamSynchronize(c->stream);
     for (void *p : h->allocs) cudaFree(p);
     void *ps[] = {h->perm_d, h->lr_d, h->items_d, h->terms_d, h->chunks_d, h->leaf_chunk_d, h->leaf_e0_d, h->z_d,
-                  h->t_d, h->part_d, h->xp_d, h->status_d};
+                  h->t_d, h->part_d, h->xp_d, h->status_d, h->ph, h->pl, h->vh, h->vl};
     for (void *p : ps)
         if (p) cudaFree(p);
     delete h;
@@ -808,7 +946,7 @@ int hmatrix_build(ucg_ctx *c, int okada_mode, double eta, double eps, int leaf)
         for (const HLeafTerm &T : per_leaf[L]) {
             for (int c0 = 0; c0 < T.cols; c0 += maxc) {
                 const int nc = std::min(maxc, T.cols - c0);
-                const long sz = ((long)rows * nc + 1) & ~1L;   // doubles, padded to 16 bytes
+                const long sz = ((long)rows * nc + 7) & ~7L;   // padded to 8 elements (64 / 16 bytes)
                 if (ch.bytes + 8L * sz > HM_CHUNK_BYTES) {
                     chunks.push_back(ch);
                     ch = HChunk{L, (int)terms.size(), (int)terms.size(), 0, poff};
@@ -832,6 +970,7 @@ int hmatrix_build(ucg_ctx *c, int okada_mode, double eta, double eps, int leaf)
         UCG_CUDA(cudaMalloc(&panel, sizeof(double) * std::max<long>(poff, 2)));
         h->allocs.push_back(panel);
         h->panel = panel;
+        h->panel_len = poff;
         if (!pk.empty()) {
             PackJob *pk_d = nullptr;
             UCG_CUDA(cudaMalloc(&pk_d, sizeof(PackJob) * pk.size()));
@@ -860,6 +999,14 @@ int hmatrix_build(ucg_ctx *c, int okada_mode, double eta, double eps, int leaf)
     UCG_CUDA(cudaMalloc(&h->status_d, sizeof(int)));
     UCG_CUDA(cudaMemset(h->status_d, 0, sizeof(int)));
     UCG_CUDA(cudaMalloc(&h->part_d, sizeof(double) * (size_t)h->n_chunks * 3 * h->max_leaf));
+    {
+        long vs = 0;
+        for (HLowRank &b : lr) {
+            b.vsoff = vs;
+            vs += (long)b.k * b.n;
+        }
+    }
+    h->lr_h = lr;
     if (!lr.empty()) UCG_CUDA(cudaMemcpy(h->lr_d, lr.data(), sizeof(HLowRank) * lr.size(), cudaMemcpyHostToDevice));
     if (!items.empty())
         UCG_CUDA(cudaMemcpy(h->items_d, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice));
@@ -893,6 +1040,71 @@ void hmatrix_apply(ucg_ctx *c, const double *v, double *t)
     k_hm_rows<<<h->n_chunks, ((rows + 31) / 32) * 32, HM_CHUNK_BYTES, c->stream>>>(
         h->terms_d, h->chunks_d, h->leaf_e0_d, h->panel, h->xp_d, h->z_d, h->part_d, rows, h->status_d);
     const int gs = ((rows + 31) / 32) * 32, nthr = std::max(gs, (1024 / gs) * gs);
+    k_hm_reduce<<<h->n_leaves, nthr, sizeof(double) * nthr, c->stream>>>(h->leaf_e0_d, h->leaf_chunk_d, h->perm_d,
+                                                                         h->part_d, rows, t, gs);
+    c->launches.count += 3;
+}
+
+// hi / lo bf16 copies of the panels and of V (once; kept with the matrix)
+int hmatrix_split_build(ucg_ctx *c)
+{
+    HMat *h = c->hm;
+    if (!h) return UCG_E_STATE;
+    if (h->ph) return UCG_OK;
+    long vn = 0;
+    for (const HLowRank &b : h->lr_h) vn += (long)b.k * b.n;
+    const long pn = std::max<long>(h->panel_len, 8);
+    UCG_CUDA(cudaMalloc(&h->ph, sizeof(__nv_bfloat16) * pn));
+    UCG_CUDA(cudaMalloc(&h->pl, sizeof(__nv_bfloat16) * pn));
+    UCG_CUDA(cudaMalloc(&h->vh, sizeof(__nv_bfloat16) * std::max<long>(vn, 8)));
+    UCG_CUDA(cudaMalloc(&h->vl, sizeof(__nv_bfloat16) * std::max<long>(vn, 8)));
+    if (h->panel_len > 0) {
+        k_split_flat<<<8 * c->sms, 256, 0, c->stream>>>(h->panel, h->panel_len, h->ph, h->pl);
+        c->launches.count++;
+    }
+    std::vector<SplitJob> jobs;
+    for (const HLowRank &b : h->lr_h)
+        if (b.k > 0) jobs.push_back({b.V, (long)b.k * b.n, b.vsoff});
+    if (!jobs.empty()) {
+        SplitJob *jd = nullptr;
+        UCG_CUDA(cudaMalloc(&jd, sizeof(SplitJob) * jobs.size()));
+        UCG_CUDA(cudaMemcpy(jd, jobs.data(), sizeof(SplitJob) * jobs.size(), cudaMemcpyHostToDevice));
+        k_split_jobs<<<(int)jobs.size(), 256, 0, c->stream>>>(jd, h->vh, h->vl);
+        c->launches.count++;
+        UCG_CUDA(cudaStreamSynchronize(c->stream));
+        cudaFree(jd);
+    }
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    return UCG_OK;
+}
+
+// t = H v on the split copies: hi + lo (lo = true) or hi alone
+void hmatrix_apply_split(ucg_ctx *c, const double *v, double *t, bool lo)
+{
+    HMat *h = c->hm;
+    k_hm_gather<<<(h->np + 255) / 256, 256, 0, c->stream>>>(h->perm_d, h->np, v, h->xp_d);
+    if (h->n_items > 0) {
+        const long threads = h->n_items * 32;
+        if (lo)
+            k_hm_z_split<true><<<(int)((threads + 255) / 256), 256, 0, c->stream>>>(h->lr_d, h->items_d, h->n_items,
+                                                                                 h->xp_d, h->vh, h->vl, h->z_d);
+        else
+            k_hm_z_split<false><<<(int)((threads + 255) / 256), 256, 0, c->stream>>>(h->lr_d, h->items_d, h->n_items,
+                                                                                  h->xp_d, h->vh, h->vl, h->z_d);
+        c->launches.count++;
+    }
+    const int rows = 3 * h->max_leaf;
+    const int thr = ((rows + 31) / 32) * 32;
+    const size_t smem = (size_t)(lo ? 2 : 1) * 2 * (HM_CHUNK_BYTES / 8);
+    if (lo)
+        k_hm_rows_split<true><<<h->n_chunks, thr, smem, c->stream>>>(h->terms_d, h->chunks_d, h->leaf_e0_d, h->ph,
+                                                                     h->pl, h->xp_d, h->z_d, h->part_d, rows,
+                                                                     h->status_d);
+    else
+        k_hm_rows_split<false><<<h->n_chunks, thr, smem, c->stream>>>(h->terms_d, h->chunks_d, h->leaf_e0_d, h->ph,
+                                                                      h->pl, h->xp_d, h->z_d, h->part_d, rows,
+                                                                      h->status_d);
+    const int gs = thr, nthr = std::max(gs, (1024 / gs) * gs);
     k_hm_reduce<<<h->n_leaves, nthr, sizeof(double) * nthr, c->stream>>>(h->leaf_e0_d, h->leaf_chunk_d, h->perm_d,
                                                                          h->part_d, rows, t, gs);
     c->launches.count += 3;

@@ -218,7 +218,14 @@ __global__ void k_rhs_t(StageArgs a, const Ctl *ctl, const double *__restrict__ 
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.np) return;
     const double *yy = (S == 1) ? a.y : a.ys;
-    const double tr[3] = {t[3L * e], t[3L * e + 1], t[3L * e + 2]};
+    double tr[3] = {t[3L * e], t[3L * e + 1], t[3L * e + 2]};
+    if (a.anchored) {
+        // anchored stages: stage 1 keeps t1 = K v1, the others add K (v - v1) to it
+        for (int q = 0; q < 3; q++) {
+            if (S == 1) a.t1[3L * e + q] = tr[q];
+            else tr[q] += a.t1[3L * e + q];
+        }
+    }
     rhs_patch(a, yy, a.k[S - 1], e, tr);
 }
 
@@ -663,7 +670,10 @@ __global__ void k_clear_pending(Ctl *ctl) { ctl->pending = 0; }
 
 // ---- host side -----------------------------------------------------------------
 
-bool rk_anchored(const ucg_ctx *c) { return c->precision == UCG_PREC_SPLIT_BF16 && c->Khi != nullptr; }
+bool rk_anchored(const ucg_ctx *c)
+{
+    return (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi != nullptr) || c->precision == UCG_PREC_HMATRIX_SPLIT;
+}
 
 // the attempt graph holds device addresses of the matrix and parameter arrays;
 // whoever frees or replaces one of them drops the graph first
@@ -793,9 +803,10 @@ static void enqueue_stage(ucg_ctx *c)
     StageArgs a = stage_args(c, S);
     k_prologue<S><<<(ne + 127) / 128, 128, 0, c->stream>>>(a, c->ctl);
     c->launches.count += 1;
-    if (c->precision == UCG_PREC_HMATRIX) {
+    if (c->precision == UCG_PREC_HMATRIX || c->precision == UCG_PREC_HMATRIX_SPLIT) {
         double *t = hmatrix_t(c);
-        hmatrix_apply(c, c->st.v, t);
+        if (c->precision == UCG_PREC_HMATRIX) hmatrix_apply(c, c->st.v, t);
+        else hmatrix_apply_split(c, c->st.v, t, S == 1);   // anchor: hi + lo; increments: hi
         k_rhs_t<S><<<(c->nr + c->nt + 127) / 128, 128, 0, c->stream>>>(a, c->ctl, t);
         c->launches.count += 1;
         return;

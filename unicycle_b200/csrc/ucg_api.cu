@@ -127,7 +127,7 @@ static void invalidate(ucg_ctx *c)
     split_bf16_free(c);
     free_observation(c);
     hmatrix_free(c);
-    if (c->precision == UCG_PREC_HMATRIX) c->precision = UCG_PREC_FP64;
+    if (c->precision == UCG_PREC_HMATRIX || c->precision == UCG_PREC_HMATRIX_SPLIT) c->precision = UCG_PREC_FP64;
 }
 
 int ucg_set_rectangles(ucg_ctx *c, int n, const double *x, const double *L, const double *W,
@@ -325,10 +325,16 @@ int ucg_copy_G(ucg_ctx *c, double *G, long ld, long k0, long k1)
 int ucg_set_precision(ucg_ctx *c, int precision)
 {
     if (!c) return UCG_E_BADARG;
-    if (precision != UCG_PREC_FP64 && precision != UCG_PREC_SPLIT_BF16 && precision != UCG_PREC_HMATRIX)
+    if (precision != UCG_PREC_FP64 && precision != UCG_PREC_SPLIT_BF16 && precision != UCG_PREC_HMATRIX &&
+        precision != UCG_PREC_HMATRIX_SPLIT)
         return bad(c, "precision");
-    if (precision == UCG_PREC_HMATRIX) {
+    if (precision == UCG_PREC_HMATRIX || precision == UCG_PREC_HMATRIX_SPLIT) {
         if (!c->hm) return set_err(c, UCG_E_STATE, "build the hierarchical matrix first (ucg_build_hmatrix)");
+        if (precision == UCG_PREC_HMATRIX_SPLIT) {
+            UCG_CUDA(cudaSetDevice(c->device));
+            int rc = hmatrix_split_build(c);
+            if (rc) return rc;
+        }
         c->precision = precision;
         return UCG_OK;
     }
@@ -404,7 +410,8 @@ static int ensure_state(ucg_ctx *c)
     if (c->nr + c->nt > 0 && !c->have_friction) return set_err(c, UCG_E_STATE, "friction not set");
     if (c->nv > 0 && !c->have_rheology) return set_err(c, UCG_E_STATE, "rheology not set");
     if (c->precision == UCG_PREC_FP64 && !c->K) return set_err(c, UCG_E_STATE, "FP64 matrix released or not assembled");
-    if (c->precision == UCG_PREC_HMATRIX && !c->hm) return set_err(c, UCG_E_STATE, "hierarchical matrix not built");
+    if ((c->precision == UCG_PREC_HMATRIX || c->precision == UCG_PREC_HMATRIX_SPLIT) && !c->hm)
+        return set_err(c, UCG_E_STATE, "hierarchical matrix not built");
     if (!c->state_ready) {
         c->state_len = ucg_state_len(c);
         int rc = rk_alloc(c);

@@ -213,6 +213,8 @@ void split_bf16_free(ucg_ctx *c);
 int hmatrix_build(ucg_ctx *c, int okada_mode, double eta, double eps, int leaf);
 void hmatrix_free(ucg_ctx *c);
 void hmatrix_apply(ucg_ctx *c, const double *v, double *t);   // t = H v, K's row order
+int hmatrix_split_build(ucg_ctx *c);                          // bf16 hi / lo copies (UCG_PREC_HMATRIX_SPLIT)
+void hmatrix_apply_split(ucg_ctx *c, const double *v, double *t, bool lo);
 double *hmatrix_t(ucg_ctx *c);                                 // the product's output buffer
 void hmatrix_info(const ucg_ctx *c, long *n_dense, long *n_lowrank, long *n_fallback, size_t *bytes,
                   int *max_rank, double *build_ms);
