@@ -585,7 +585,24 @@ def hmatrix_leg(args, local, sim, cfg, plain):
     torch.cuda.synchronize()
     el = e0.elapsed_time(e1) / 1e3
     _, t_t, *_ = sim.get_state()
+    # the same on the split (bf16 hi + lo) copy with anchored stages
+    sim.set_precision(unicycle_b200.UCG_PREC_HMATRIX_SPLIT)
+    sim.set_state(cfg["y0"], 0.0, cfg["dt0"])
+    sim.run(1e300, args.spinup + args.warmup)
+    _, ts_w, *_ = sim.get_state()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    steps_s = sim.run(1e300, steps_req)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    el_s = e0.elapsed_time(e1) / 1e3
+    _, ts_t, *_ = sim.get_state()
     sim.set_precision(unicycle_b200.UCG_PREC_FP64)
+    split = {"steps_per_s": steps_s / el_s, "ms_per_step": 1e3 * el_s / steps_s,
+             "speedup_vs_plain_fp64_steps": steps_s / el_s / plain["value"],
+             "sim_years_per_hour": (ts_t - ts_w) / YEAR / (el_s / 3600.0),
+             "bytes_stage1": info["bytes"] / 2, "bytes_increments": info["bytes"] / 4,
+             "note": "bf16 hi + lo of every stored value; stage 1 reads both, stages 2-6 the hi copy alone"}
     return {"eta": args.hm_eta, "eps": args.hm_eps, "leaf": args.hm_leaf, "build_seconds": build_s,
             "blocks_dense": info["n_dense"], "blocks_lowrank": info["n_lowrank"], "max_rank": info["max_rank"],
             "bytes": info["bytes"], "compression_vs_dense_fp64": info["compression"],
@@ -593,6 +610,7 @@ def hmatrix_leg(args, local, sim, cfg, plain):
             "steps_per_s": steps / el, "ms_per_step": 1e3 * el / steps,
             "speedup_vs_plain_fp64_steps": steps / el / plain["value"],
             "sim_years_per_hour": (t_t - t_w) / YEAR / (el / 3600.0),
+            "split": split,
             "roofline": {"bound": "hbm", "kernel": "hierarchical product (k_hm_gather, k_hm_z, k_hm_rows, "
                                                    "k_hm_reduce)", "ms_per_launch": ms, "bytes_per_launch": alg,
                          "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
@@ -621,7 +639,8 @@ def run_hmatrix(args, world, rank, local):
     sim.build_hmatrix(eta=args.hm_eta, eps=args.hm_eps, leaf=args.hm_leaf)
     build_s = time.perf_counter() - t0
     info = sim.hmatrix_info()
-    sim.set_precision(unicycle_b200.UCG_PREC_HMATRIX)
+    split = args.precision == "split_bf16"
+    sim.set_precision(unicycle_b200.UCG_PREC_HMATRIX_SPLIT if split else unicycle_b200.UCG_PREC_HMATRIX)
     stream = torch.cuda.ExternalStream(sim.stream, device=local)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sim.set_state(cfg["y0"], 0.0, cfg["dt0"])
@@ -656,9 +675,11 @@ def run_hmatrix(args, world, rank, local):
         return None
     return {"metric": METRIC, "value": world * steps / el_max, "unit": "steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el_max / steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x2/f64 sums" if split else "f64",
             "data": "synthetic (seeded cfg2 curved megathrust; random Dc)",
-            "config": {"workload": f"megathrust {n} Nikkhoo-Walter triangles, hierarchical K only",
+            "config": {"workload": f"megathrust {n} Nikkhoo-Walter triangles, hierarchical K only"
+                                   + (" (bf16 hi + lo, anchored stages)" if split else ""),
                        "n_triangles": n, "K_shape": [m, nn], "dense_fp64_bytes": 8.0 * m * nn,
                        "parallelism": f"replicas x{world}", "rtol": cfg["epsilon"],
                        "l2": "inputs larger than L2 (H %.1f GB)" % (info["bytes"] / 1e9)},
