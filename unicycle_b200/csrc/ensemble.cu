@@ -58,6 +58,8 @@
 #include <new>
 #include <queue>
 #include <string>
+#include <map>
+#include <array>
 #include <vector>
 #include <cuda_bf16.h>
 #include "ucg_internal.cuh"
@@ -146,6 +148,13 @@ struct GeomDev {
     double *v1, *t1;            // stage-1 anchor: [ninst][2 np] velocities, [ninst][3 np] tractions
     const double *vpl_c, *vpl_s, *a, *b, *sig, *L, *damping; // [ninst][np]
     InstCtl *ctl;               // [ninst]
+    // hierarchical K (hier != 0): B is the B space of the hierarchical contraction
+    int hier, hleaves, hunit0, hpad;
+    size_t hbtile;              // bytes of one instance tile's B space
+    const int *hperm;           // permuted position -> element
+    const int *hinv;            // element -> permuted position
+    const int2 *hrow;           // permuted position -> (row leaf, local row of its first component)
+    const int *hxpos;           // element -> B-space slot of its first source column
 };
 
 struct EnsArgs {
@@ -154,6 +163,11 @@ struct EnsArgs {
     const float *ws1, *ws2;     // partial sums: [slot][ni][128] (single tiles), [slot][2][ni][128] (pairs)
     const int *piece0_1, *npieces_1, *piece0_2, *npieces_2;
     EnsGlobal *glob;
+    // hierarchical pass 2: per unit its first piece, pieces and partial-sum rows;
+    // per piece the float offset of its partial sums
+    const float *hws2;
+    const int *hp0, *hnp, *hrows;
+    const long *hpws;
 };
 
 // a work unit: one M-tile, or two consecutive M-tiles of a geometry (a1 null when
@@ -415,6 +429,319 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
     }
 }
 
+// ---- the hierarchical contraction -------------------------------------------------------
+//
+// T = H V for a hierarchical K (hmatrix.cu) in two passes of one kernel:
+//   pass 1: Z = Vs X for every stack Vs of the low-rank blocks that share a source
+//           cluster (their V factors stacked, each block's rank rounded up to 8
+//           with zero rows), over the cluster's source columns;
+//   pass 2: T_leaf = [dense | U] [X ; Z] for every row leaf, over the leaf's
+//           dense blocks' source columns and its low-rank blocks' rank entries.
+// Operands are stored in the K-major core-matrix layout without swizzle: a
+// K-group is 8 consecutive K entries (16 bytes of bf16), an 8-row group of one
+// K-group is one 128-byte core matrix, and an image is [K-group][row group] per
+// plane (hi, then lo).  Granularity 8 along K lets a row leaf's K range
+// concatenate pieces of any length multiple of 8 (leaf columns, ranks) and the
+// B operand of every K-group be fetched from wherever its instances' values
+// live (X: the permuted sources; Z: pass 1's output), merged into one bulk copy
+// per run of consecutive K-groups.  Rows of a unit beyond its 8-row groups are
+// read by the 128-row MMA from the stage's own buffer and land in accumulator
+// lanes that are never drained.
+constexpr int HKG_STAGE = 8;                  // K-groups per pipeline stage (four K-steps of 16)
+constexpr int HA_PLANE = HKG_STAGE * 16 * 128; // one plane of a stage for 16 row groups: 16 KB
+
+template <int NI, bool KLO>
+struct HTile {
+    static constexpr int B_KG = 2 * NI * 16;              // hi + lo of one K-group for NI instances
+    static constexpr int A_BYTES = KLO ? 2 * HA_PLANE : HA_PLANE;
+    static constexpr int STAGE = A_BYTES + HKG_STAGE * B_KG;
+    static constexpr int STAGES = (6 * 32768) / STAGE < 8 ? (6 * 32768) / STAGE : 8;
+    // + 1024 for the alignment and 32 KB past the last stage: every descriptor's
+    // reach, read with its two strides either way round, stays inside the allocation
+    static constexpr int SMEM = STAGES * STAGE + 1024 + 32768;
+    static constexpr uint32_t TMEM_COLS = 2 * NI;
+    static constexpr uint32_t IDESC = Tile<NI, false, 1>::IDESC;
+};
+
+struct HUnit {                  // one M-tile of one pass for one instance tile
+    const uint8_t *a;           // hi planes [K-group][g][128 B]; the lo planes follow at a + lo_off
+    long lo_off;
+    const int *bidx;            // per K-group: its K-group in the instance tile's B space
+    const uint8_t *b;           // the instance tile's B space: [K-group][hi | lo][NI / 8][128 B]
+    int g, nkg;                 // 8-row groups (1..16), K-groups (even)
+    int rows;                   // rows of its partial sums (8 g)
+    int pad;
+};
+struct HSeg {
+    int unit, kg0, kg1, pad;    // K-groups [kg0, kg1), both even
+    long ws;                    // float offset of its partial sums [NI][rows]
+};
+
+// shared-memory descriptor of a K-major operand without swizzle: K-groups `lbo`
+// bytes apart, 8-row groups `sbo` bytes apart, descriptor version 1
+__device__ __forceinline__ uint64_t cm_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1u << 46);
+}
+
+template <int NI, bool KLO>
+__global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict__ units,
+        const HSeg *__restrict__ segs, const int *__restrict__ cta_seg, float *__restrict__ ws, int *err)
+{
+    using T = HTile<NI, KLO>;
+    extern __shared__ unsigned char dyn_smem[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dyn_smem) + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) uint64_t full[T::STAGES], empty[T::STAGES], acc_full[2], acc_empty[2], drain;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q0 = cta_seg[blockIdx.x], q1 = cta_seg[blockIdx.x + 1];
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < T::STAGES; s++) {
+            bar_init(&full[s], 1);
+            bar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            bar_init(&acc_full[b], 1);
+            bar_init(&acc_empty[b], 4);
+        }
+        bar_init(&drain, 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_addr(&tmem_slot)),
+                     "r"(T::TMEM_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    auto fail = [&]() {
+        abort_flag = 1;
+        atomicExch(err, (int)UCG_E_TIMEOUT);
+    };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer: per stage one copy of the unit's hi (and lo) planes and
+            // one copy per run of consecutive B K-groups
+            long issued = 0;
+            for (int q = q0; q < q1 && !abort_flag; q++) {
+                const HSeg sg = segs[q];
+                const HUnit U = units[sg.unit];
+                const uint32_t plane = (uint32_t)U.g * 128u;
+                for (int kg = sg.kg0; kg < sg.kg1; kg += HKG_STAGE) {
+                    const int nk = min(HKG_STAGE, sg.kg1 - kg);
+                    const int s = (int)(issued % T::STAGES);
+                    const uint32_t ph = (uint32_t)((issued / T::STAGES) & 1);
+                    if (!bar_wait(&empty[s], ph ^ 1u, &abort_flag)) {
+                        if (!abort_flag) fail();
+                        break;
+                    }
+                    uint8_t *st = smem + (size_t)s * T::STAGE;
+                    const uint32_t abytes = (uint32_t)nk * plane;
+                    bar_expect_tx(&full[s], (KLO ? 2u : 1u) * abytes + (uint32_t)nk * T::B_KG);
+                    bulk_load(st, U.a + (size_t)kg * plane, abytes, &full[s]);
+                    if (KLO) bulk_load(st + HA_PLANE, U.a + U.lo_off + (size_t)kg * plane, abytes, &full[s]);
+                    uint8_t *bst = st + T::A_BYTES;
+                    for (int j = 0; j < nk;) {
+                        const int b0 = U.bidx[kg + j];
+                        int r = 1;
+                        while (j + r < nk && U.bidx[kg + j + r] == b0 + r) r++;
+                        bulk_load(bst + (size_t)j * T::B_KG, U.b + (size_t)b0 * T::B_KG, (uint32_t)r * T::B_KG,
+                                  &full[s]);
+                        j += r;
+                    }
+                    issued++;
+                }
+            }
+            for (long i = issued - T::STAGES > 0 ? issued - T::STAGES : 0; i < issued; i++)
+                bar_wait(&full[i % T::STAGES], (uint32_t)((i / T::STAGES) & 1), nullptr);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            long it = 0;
+            int tc = 0;
+            bool issued_any = false;
+            for (int q = q0; q < q1 && !abort_flag; q++, tc++) {
+                const HSeg sg = segs[q];
+                const uint32_t plane = (uint32_t)units[sg.unit].g * 128u;
+                const int buf = tc & 1;
+                const uint32_t use = (uint32_t)(tc >> 1);
+                if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag)) {
+                    if (!abort_flag) fail();
+                    break;
+                }
+                tc_fence_after();
+                bool ok = true;
+                const uint32_t d = tmem + (uint32_t)(buf * NI);
+                for (int kg = sg.kg0; kg < sg.kg1; kg += HKG_STAGE, it++) {
+                    const int nk = min(HKG_STAGE, sg.kg1 - kg);
+                    const int s = (int)(it % T::STAGES);
+                    const uint32_t ph = (uint32_t)((it / T::STAGES) & 1);
+                    if (!bar_wait(&full[s], ph, &abort_flag)) {
+                        if (!abort_flag) fail();
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a = s_addr(smem + (size_t)s * T::STAGE);
+                    const uint32_t b = a + T::A_BYTES;
+                    for (int j = 0; j < nk / 2; j++) {
+                        const uint32_t ao = (uint32_t)(2 * j) * plane, bo = (uint32_t)(2 * j) * T::B_KG;
+                        const uint64_t ahi = cm_desc(a + ao, plane, 128u);
+                        const uint64_t bhi = cm_desc(b + bo, T::B_KG, 128u);
+                        const uint64_t blo = cm_desc(b + bo + NI * 16, T::B_KG, 128u);
+                        const uint32_t acc = (kg > sg.kg0 || j > 0) ? 1u : 0u;
+                        mma_bf16(d, ahi, bhi, T::IDESC, acc);
+                        mma_bf16(d, ahi, blo, T::IDESC, 1u);
+                        if (KLO) mma_bf16(d, cm_desc(a + HA_PLANE + ao, plane, 128u), bhi, T::IDESC, 1u);
+                    }
+                    issued_any = true;
+                    mma_commit(&empty[s]);
+                }
+                if (!ok) break;
+                mma_commit(&acc_full[buf]);
+            }
+            if (issued_any) {
+                mma_commit(&drain);
+                bar_wait(&drain, 0u, nullptr);
+            }
+        }
+        __syncwarp();
+    } else {
+        // drain: warp w reads tensor-memory lanes 32 (w mod 4) .. +31 = unit rows;
+        // rows past the unit's 8-row groups are not written
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;
+        int tc = 0;
+        for (int q = q0; q < q1; q++, tc++) {
+            const HSeg sg = segs[q];
+            const int rows = units[sg.unit].rows;
+            const int buf = tc & 1;
+            const uint32_t use = (uint32_t)(tc >> 1);
+            int ok = 0;
+            if (lane == 0) ok = bar_wait(&acc_full[buf], use & 1u, &abort_flag) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) {
+                if (lane == 0 && !abort_flag) fail();
+                break;
+            }
+            tc_fence_after();
+            float *dst = ws + sg.ws + row;
+            const uint32_t tbase = tmem + (uint32_t)(buf * NI) + ((uint32_t)(quarter * 32) << 16);
+#pragma unroll
+            for (int c0 = 0; c0 < NI; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(tbase + (uint32_t)c0, r);
+                if (row < rows) {
+#pragma unroll
+                    for (int i = 0; i < 16; i++) dst[(size_t)(c0 + i) * rows] = __uint_as_float(r[i]);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) bar_arrive(&acc_empty[buf]);
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(T::TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// one K-group of an operand image from FP64 values: value(row r, slot k) =
+// src[k][(r - row0) stride] for rows row0 .. row0 + nrows - 1, zero where src[k]
+// is null; one thread per row writes its 16 bytes of hi and of lo
+struct HPackJob {
+    uint8_t *dst;               // the K-group's hi plane; lo at dst + lo_off
+    long lo_off;
+    long stride;
+    int row0, nrows;
+    const double *src[8];
+};
+
+__global__ void k_hm_pack(const HPackJob *__restrict__ jobs)
+{
+    const HPackJob J = jobs[blockIdx.x];
+    const int t = threadIdx.x;
+    if (t >= J.nrows) return;
+    const int r = J.row0 + t;
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int k = 0; k < 8; k += 2) {
+        const double x0 = J.src[k] ? J.src[k][(long)t * J.stride] : 0.0;
+        const double x1 = J.src[k + 1] ? J.src[k + 1][(long)t * J.stride] : 0.0;
+        const __nv_bfloat16 h0 = __double2bfloat16(x0), h1 = __double2bfloat16(x1);
+        const __nv_bfloat16 l0 = __double2bfloat16(x0 - (double)__bfloat162float(h0));
+        const __nv_bfloat16 l1 = __double2bfloat16(x1 - (double)__bfloat162float(h1));
+        hi[k / 2] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+        lo[k / 2] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    }
+    uint8_t *p = J.dst + (size_t)(r >> 3) * 128 + (size_t)(r & 7) * 16;
+    *reinterpret_cast<uint4 *>(p) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4 *>(p + J.lo_off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+}
+
+// a B-space entry (instance rr of a tile, slot `pos` = 8 K-group + k, k even) and
+// the next slot from two FP64 values, split into hi and lo
+__device__ __forceinline__ void put_x(uint8_t *Bt, int ni, int rr, int pos, double v0, double v1)
+{
+    uint8_t *base = Bt + (size_t)(pos >> 3) * (2 * ni * 16) + (size_t)(rr >> 3) * 128 + (size_t)(rr & 7) * 16 +
+                    (size_t)(pos & 7) * 2;
+    const __nv_bfloat16 h0 = __double2bfloat16(v0), h1 = __double2bfloat16(v1);
+    const __nv_bfloat16 l0 = __double2bfloat16(v0 - (double)__bfloat162float(h0));
+    const __nv_bfloat16 l1 = __double2bfloat16(v1 - (double)__bfloat162float(h1));
+    *reinterpret_cast<__nv_bfloat162 *>(base) = __halves2bfloat162(h0, h1);
+    *reinterpret_cast<__nv_bfloat162 *>(base + (size_t)ni * 16) = __halves2bfloat162(l0, l1);
+}
+
+// pass 1's output into the B space: one thread per (unit, 8-row group, instance)
+// adds the unit's partial sums in k order (FP64) and writes 8 rank entries of Z
+// as hi and lo
+struct HZUnit {
+    uint8_t *b;                 // the instance tile's B space
+    int zkg0;                   // K-group of the unit's first row
+    int g, rows, p0, np, pad;
+};
+
+__global__ void k_hm_zconv(const HZUnit *__restrict__ zu, const long *__restrict__ pws,
+                           const float *__restrict__ ws, int ni)
+{
+    const HZUnit U = zu[blockIdx.x];
+    for (int w = threadIdx.x; w < U.g * ni; w += blockDim.x) {
+        const int grp = w / ni, i = w % ni;
+        double z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int p = 0; p < U.np; p++) {
+            const float4 *src = reinterpret_cast<const float4 *>(ws + pws[U.p0 + p] + (long)i * U.rows + grp * 8);
+            const float4 a = src[0], b = src[1];
+            z[0] += a.x; z[1] += a.y; z[2] += a.z; z[3] += a.w;
+            z[4] += b.x; z[5] += b.y; z[6] += b.z; z[7] += b.w;
+        }
+        uint32_t hi[4], lo[4];
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+            const __nv_bfloat16 h0 = __double2bfloat16(z[k]), h1 = __double2bfloat16(z[k + 1]);
+            const __nv_bfloat16 l0 = __double2bfloat16(z[k] - (double)__bfloat162float(h0));
+            const __nv_bfloat16 l1 = __double2bfloat16(z[k + 1] - (double)__bfloat162float(h1));
+            hi[k / 2] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+            lo[k / 2] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+        }
+        uint8_t *p = U.b + (size_t)(U.zkg0 + grp) * (2 * ni * 16) + (size_t)(i >> 3) * 128 + (size_t)(i & 7) * 16;
+        *reinterpret_cast<uint4 *>(p) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4 *>(p + (size_t)ni * 16) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    }
+}
+
 // ---- K images ----------------------------------------------------------------------
 
 // power-of-two row scale >= max |K(r,:)| (1 for an all-zero row)
@@ -523,6 +850,42 @@ __device__ __forceinline__ double traction_row(const EnsArgs *A, const GeomDev &
     return s * (double)G.rscale[r];
 }
 
+// row 3 p + q (permuted position p) of instance i for a hierarchical geometry:
+// the pass-2 partial sums of its row leaf, added in k order
+__device__ __forceinline__ double traction_row_h(const EnsArgs *A, const GeomDev &G, int i, int p, int q)
+{
+    const int2 rl = G.hrow[p];
+    const int unit = G.hunit0 + (i / A->ni) * G.hleaves + rl.x;
+    const int p0 = A->hp0[unit], np_ = A->hnp[unit];
+    const long off = (long)(i % A->ni) * A->hrows[unit] + rl.y + q;
+    double s = 0.0;
+    for (int j = 0; j < np_; j++) s += (double)A->hws2[A->hpws[p0 + j] + off];
+    return s;
+}
+
+// T (instance-major, ninst x m, K's row order) of a hierarchical geometry
+__global__ void k_reduce_h(const EnsArgs *A, int gi, double *T)
+{
+    const GeomDev &G = A->g[gi];
+    const long m = 3L * G.np;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= (long)G.ninst * m) return;
+    const int i = (int)(t / m);
+    const long r = t % m;
+    T[t] = traction_row_h(A, G, i, G.hinv[r / 3], (int)(r % 3));
+}
+
+// dense V (instance-major, ninst x n) into a hierarchical geometry's X slots
+__global__ void k_pack_x_dense(const EnsArgs *A, int gi, const double *__restrict__ V)
+{
+    const GeomDev &G = A->g[gi];
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= (long)G.ninst * G.np) return;
+    const int i = (int)(t / G.np), e = (int)(t % G.np);
+    const double *v = V + (long)i * 2 * G.np + 2L * e;
+    put_x(G.B + (size_t)(i / A->ni) * G.hbtile, A->ni, i % A->ni, G.hxpos[e], v[0], v[1]);
+}
+
 // T (instance-major, ninst x m) of geometry gi from the workspace
 __global__ void k_reduce_dense(const EnsArgs *A, int gi, double *T, int paired)
 {
@@ -622,7 +985,10 @@ __global__ void k_ens_prologue(const EnsArgs *__restrict__ A)
                 v1 = v1 - G.v1[2 * pe + 1];
             }
         }
-        put_v(G.B, A->ni, G.kblocks, i, 2L * e, v0, v1);
+        if (G.hier)
+            put_x(G.B + (size_t)(i / A->ni) * G.hbtile, A->ni, i % A->ni, G.hxpos[e], v0, v1);
+        else
+            put_v(G.B, A->ni, G.kblocks, i, 2L * e, v0, v1);
     }
     if (S == 1) {
         // the block's elements belong to one instance: reduce over the warp,
@@ -647,14 +1013,17 @@ __global__ void k_ens_rhs(const EnsArgs *__restrict__ A)
     const GeomDev &G = A->g[gi];
     const int local = blockIdx.x - G.blk_e0;
     const int i = local / G.epb_e;
-    const int e = (local % G.epb_e) * EW_THREADS + threadIdx.x;
-    if (i >= G.ninst || e >= G.np) return;
+    const int el = (local % G.epb_e) * EW_THREADS + threadIdx.x;
+    if (i >= G.ninst || el >= G.np) return;
     const InstCtl *c = G.ctl + i;
     if (!inst_live(c, A->glob) || (S == 1 && !c->need_stage1)) return;
+    // a hierarchical geometry walks its elements in the permuted order, so that
+    // consecutive threads read consecutive rows of a leaf's partial sums
+    const int e = G.hier ? G.hperm[el] : el;
     double t[3];
     double *t1 = G.t1 + (long)i * 3 * G.np + 3L * e;
     for (int q = 0; q < 3; q++) {
-        const double inc = traction_row(A, G, i, 3L * e + q, S > 1);
+        const double inc = G.hier ? traction_row_h(A, G, i, el, q) : traction_row(A, G, i, 3L * e + q, S > 1);
         if (S == 1) {
             t1[q] = inc;
             t[q] = inc;
@@ -924,8 +1293,33 @@ struct EnsGeomHost {
     double *anchor = nullptr;  // v1 (ninst * 2 np) then t1 (ninst * 3 np)
     double *par = nullptr;     // 7 vectors of ninst * np
     InstCtl *ctl = nullptr;
-    uint8_t *B = nullptr;      // V images for the current ni
+    uint8_t *B = nullptr;      // V images (B space of a hierarchical geometry) for the current ni
     int b_ni = 0;
+    // hierarchical K: operand images of both passes and the maps of the B space
+    bool hier = false;
+    struct HU {                // a unit of one pass, without its instance tile
+        long a_off, lo_off, bidx_off;
+        int g, nkg, zkg0;
+    };
+    std::vector<HU> hu1, hu2;  // pass 1 (tiles of the rank stacks), pass 2 (row leaves)
+    uint8_t *hA = nullptr;
+    int *hbidx = nullptr, *hperm = nullptr, *hinv = nullptr, *hxpos = nullptr;
+    int2 *hrow = nullptr;
+    int nbkg = 0, hleaves = 0;
+    size_t h_img_bytes = 0, h_fp64_bytes = 0;
+    long h_kg1 = 0, h_kg2 = 0;  // K-groups of the two passes (one instance tile)
+};
+
+struct HPlanBufs {
+    HUnit *units = nullptr;
+    HSeg *segs = nullptr;
+    int *cta = nullptr;
+    float *ws = nullptr;
+    long *pws = nullptr;       // per piece: float offset of its partial sums
+    int *p0 = nullptr, *np = nullptr, *rows = nullptr;   // per unit
+    HZUnit *zu = nullptr;      // pass 1: per unit its Z destination
+    int nunits = 0, nsegs = 0;
+    size_t ws_floats = 0;
 };
 
 struct PlanBufs {
@@ -952,6 +1346,7 @@ struct ucg_ensemble {
     bool planned = false;
     std::string plan_name;
     PlanBufs p1, p2;
+    HPlanBufs h1, h2;          // hierarchical geometries: pass 1 and pass 2
     std::string tune_report;
 
     EnsArgs *d_args = nullptr;
@@ -981,6 +1376,221 @@ int ebad(ucg_ensemble *E, int st, const char *msg)
 {
     E->err = msg;
     return st;
+}
+
+// ---- hierarchical geometries --------------------------------------------------------------
+//
+// The B space of one instance tile holds, K-group after K-group: X (every row
+// leaf's source columns in the permuted order, each leaf's columns rounded up
+// to 8), Z (every rank stack's rows, each block's rank rounded up to 8) and one
+// K-group of zeros that pads a unit's K range to an even number of K-groups.
+
+// operand images, B-space maps and unit templates of a hierarchical geometry
+int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
+{
+    const int np = L.np, NL = L.n_leaves;
+    std::vector<int> xkg0(NL + 1, 0), leaf_of_pos(np), kg_leaf;
+    for (int l = 0; l < NL; l++) {
+        const int sz = L.leaf_e0[l + 1] - L.leaf_e0[l];
+        if (3 * sz > BM)
+            return ebad(E, UCG_E_UNSUPPORTED,
+                        "hierarchical ensemble: row leaves of at most 42 patches (build the matrix with leaf <= 42)");
+        xkg0[l + 1] = xkg0[l] + (2 * sz + 7) / 8;
+        for (int p = L.leaf_e0[l]; p < L.leaf_e0[l + 1]; p++) leaf_of_pos[p] = l;
+        for (int q = xkg0[l]; q < xkg0[l + 1]; q++) kg_leaf.push_back(l);
+    }
+    const int nx = xkg0[NL];
+    // rank stacks: the low-rank blocks of one source cluster, in block order
+    std::map<std::pair<int, int>, std::vector<int>> stacks;
+    for (int b = 0; b < (int)L.lr.size(); b++)
+        if (L.lr[b].k > 0) stacks[{L.lr[b].s0, L.lr[b].n}].push_back(b);
+    std::vector<int> zkg_b(L.lr.size(), -1);
+    std::vector<HPackJob> jobs;
+    std::vector<long> dst_off;   // per job: byte offset of its K-group in the images
+    std::vector<int> bidx;
+    long a_off = 0;
+    auto pad8 = [](int k) { return (k + 7) & ~7; };
+    int zk = nx;
+    // pass 1
+    for (const auto &st : stacks) {
+        const int s0 = st.first.first, n = st.first.second;
+        const int ne = n / 2;
+        const int l0 = leaf_of_pos[s0], l1 = leaf_of_pos[s0 + ne - 1];
+        if (L.leaf_e0[l0] != s0 || L.leaf_e0[l1 + 1] != s0 + ne)
+            return ebad(E, UCG_E_STATE, "hierarchical matrix: a source cluster is not a union of leaves");
+        const int kx0 = xkg0[l0], nk = xkg0[l1 + 1] - kx0, nke = nk + (nk & 1);
+        std::vector<int> rowoff;
+        int R = 0;
+        for (int b : st.second) {
+            rowoff.push_back(R);
+            zkg_b[b] = zk + R / 8;
+            R += pad8(L.lr[b].k);
+        }
+        for (int t0 = 0; t0 < R; t0 += 128) {
+            const int rows_t = std::min(128, R - t0), gg = rows_t / 8;
+            EnsGeomHost::HU u;
+            u.a_off = a_off;
+            u.lo_off = (long)nke * gg * 128;
+            u.bidx_off = (long)bidx.size();
+            u.g = gg;
+            u.nkg = nke;
+            u.zkg0 = zk + t0 / 8;
+            for (int j = 0; j < nk; j++) bidx.push_back(kx0 + j);
+            if (nk & 1) bidx.push_back(-1);   // the zero K-group, resolved below
+            for (size_t bi = 0; bi < st.second.size(); bi++) {
+                const int b = st.second[bi];
+                const ucg::HLayout::LowRank &B = L.lr[b];
+                const int rb = std::max(rowoff[bi], t0), re = std::min(rowoff[bi] + B.k, t0 + rows_t);
+                if (re <= rb) continue;
+                const int lbeg = rb - rowoff[bi];
+                for (int j = 0; j < nk; j++) {
+                    HPackJob J;
+                    J.dst = nullptr;
+                    dst_off.push_back(a_off + (long)j * gg * 128);
+                    J.lo_off = u.lo_off;
+                    J.stride = B.n;
+                    J.row0 = rb - t0;
+                    J.nrows = re - rb;
+                    const int lf = kg_leaf[kx0 + j];
+                    for (int k = 0; k < 8; k++) {
+                        const int lc = 8 * (kx0 + j - xkg0[lf]) + k;
+                        const int sz = L.leaf_e0[lf + 1] - L.leaf_e0[lf];
+                        J.src[k] = nullptr;
+                        if (lc < 2 * sz) {
+                            const int c = 2 * L.leaf_e0[lf] + lc - 2 * s0;
+                            J.src[k] = B.V + (long)lbeg * B.n + c;
+                        }
+                    }
+                    jobs.push_back(J);
+                }
+            }
+            a_off += 2 * u.lo_off;
+            g.hu1.push_back(u);
+            g.h_kg1 += nke;
+        }
+        zk += R / 8;
+    }
+    const int zero_kg = zk;
+    g.nbkg = zk + 1;
+    // pass 2
+    std::vector<int> seen(g.nbkg, -1);
+    for (int l = 0; l < NL; l++) {
+        const int rows = 3 * (L.leaf_e0[l + 1] - L.leaf_e0[l]), gg = (rows + 7) / 8;
+        std::vector<int> kgs;                       // B K-groups in order of first use
+        std::vector<std::array<const double *, 8>> src;
+        for (int q = L.leaf_term0[l]; q < L.leaf_term0[l + 1]; q++) {
+            const ucg::HLayout::Term &T = L.terms[q];
+            for (int j = 0; j < T.cols; j++) {
+                int bkg, slot;
+                if (T.xsel == 0) {
+                    const long col = T.xoff + j;
+                    const int p = (int)(col / 2), lf = leaf_of_pos[p];
+                    const int lc = (int)(col - 2L * L.leaf_e0[lf]);
+                    bkg = xkg0[lf] + lc / 8;
+                    slot = lc % 8;
+                } else {
+                    const long zi = T.xoff + j;
+                    int lo = 0, hi = (int)L.lr.size() - 1;   // the block with zoff <= zi < zoff + k
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) / 2;
+                        if (L.lr[mid].zoff <= zi) lo = mid; else hi = mid - 1;
+                    }
+                    const int r = (int)(zi - L.lr[lo].zoff);
+                    if (zkg_b[lo] < 0 || r >= L.lr[lo].k)
+                        return ebad(E, UCG_E_STATE, "hierarchical matrix: a rank entry has no block");
+                    bkg = zkg_b[lo] + r / 8;
+                    slot = r % 8;
+                }
+                if (seen[bkg] != l) {
+                    seen[bkg] = l;
+                    kgs.push_back(bkg);
+                    src.emplace_back();
+                    src.back().fill(nullptr);
+                }
+                // the K-group was appended when first met; later columns of a
+                // term continue the same or the next K-group
+                int a = (int)kgs.size() - 1;
+                if (kgs[a] != bkg) {
+                    a = -1;
+                    for (int x = (int)kgs.size() - 1; x >= 0; x--)
+                        if (kgs[x] == bkg) { a = x; break; }
+                }
+                src[a][slot] = L.panel + T.poff + (long)j * rows;
+            }
+        }
+        const int nk = (int)kgs.size(), nke = nk + (nk & 1);
+        EnsGeomHost::HU u;
+        u.a_off = a_off;
+        u.lo_off = (long)nke * gg * 128;
+        u.bidx_off = (long)bidx.size();
+        u.g = gg;
+        u.nkg = nke;
+        u.zkg0 = -1;
+        for (int j = 0; j < nk; j++) {
+            bidx.push_back(kgs[j]);
+            HPackJob J;
+            J.dst = nullptr;
+            dst_off.push_back(a_off + (long)j * gg * 128);
+            J.lo_off = u.lo_off;
+            J.stride = 1;
+            J.row0 = 0;
+            J.nrows = rows;
+            for (int k = 0; k < 8; k++) J.src[k] = src[j][k];
+            jobs.push_back(J);
+        }
+        if (nk & 1) bidx.push_back(zero_kg);
+        a_off += 2 * u.lo_off;
+        g.hu2.push_back(u);
+        g.h_kg2 += nke;
+    }
+    for (int &b : bidx)
+        if (b < 0) b = zero_kg;
+    g.hleaves = NL;
+    g.h_img_bytes = (size_t)a_off;
+    // device images and maps
+    std::vector<int> inv(np), xpos(np);
+    std::vector<int2> hrow(np);
+    for (int p = 0; p < np; p++) {
+        const int e = L.perm[p], lf = leaf_of_pos[p];
+        inv[e] = p;
+        hrow[p] = make_int2(lf, 3 * (p - L.leaf_e0[lf]));
+        xpos[e] = 8 * xkg0[lf] + 2 * (p - L.leaf_e0[lf]);
+    }
+    ECUDA(cudaMalloc(&g.hA, std::max<size_t>(g.h_img_bytes, 256)));
+    ECUDA(cudaMemsetAsync(g.hA, 0, std::max<size_t>(g.h_img_bytes, 256), E->stream));
+    ECUDA(cudaMalloc(&g.hbidx, sizeof(int) * std::max<size_t>(bidx.size(), 1)));
+    ECUDA(cudaMalloc(&g.hperm, sizeof(int) * np));
+    ECUDA(cudaMalloc(&g.hinv, sizeof(int) * np));
+    ECUDA(cudaMalloc(&g.hxpos, sizeof(int) * np));
+    ECUDA(cudaMalloc(&g.hrow, sizeof(int2) * np));
+    if (!bidx.empty())
+        ECUDA(cudaMemcpyAsync(g.hbidx, bidx.data(), sizeof(int) * bidx.size(), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(g.hperm, L.perm.data(), sizeof(int) * np, cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(g.hinv, inv.data(), sizeof(int) * np, cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(g.hxpos, xpos.data(), sizeof(int) * np, cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(g.hrow, hrow.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, E->stream));
+    // the pack jobs, in batches
+    const size_t BATCH = 1 << 18;
+    HPackJob *jd = nullptr;
+    ECUDA(cudaMalloc(&jd, sizeof(HPackJob) * std::min(BATCH, std::max<size_t>(jobs.size(), 1))));
+    for (size_t j0 = 0; j0 < jobs.size(); j0 += BATCH) {
+        const size_t nb = std::min(BATCH, jobs.size() - j0);
+        for (size_t j = j0; j < j0 + nb; j++) jobs[j].dst = g.hA + dst_off[j];
+        cudaError_t e = cudaMemcpyAsync(jd, jobs.data() + j0, sizeof(HPackJob) * nb, cudaMemcpyHostToDevice, E->stream);
+        if (e == cudaSuccess) {
+            k_hm_pack<<<(unsigned)nb, 128, 0, E->stream>>>(jd);
+            E->launches++;
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);   // the job buffer is reused
+        if (e != cudaSuccess) {
+            cudaFree(jd);
+            return efail(E, e, "hierarchical operand images");
+        }
+    }
+    cudaFree(jd);
+    g.hier = true;
+    return UCG_OK;
 }
 
 // ---- schedules ------------------------------------------------------------------------
@@ -1087,10 +1697,172 @@ long sched_cost(const Sched &s, int ovh)
     return worst;
 }
 
+// stream-K over units of unequal cost per step: the summed cost cut into P equal
+// ranges; a step belongs to the CTA whose range holds the cost at its start
+Sched sched_weighted(const std::vector<int> &steps, const std::vector<int> &w, int P)
+{
+    Sched s;
+    s.name = "weighted stream-k";
+    const int nu = (int)steps.size();
+    std::vector<long> pre(nu + 1, 0);
+    for (int u = 0; u < nu; u++) pre[u + 1] = pre[u] + (long)steps[u] * w[u];
+    const long W = pre[nu];
+    auto first_step = [&](int u, long x) -> int {   // first step of u starting at cost >= x
+        if (x <= pre[u]) return 0;
+        const long k = (x - pre[u] + w[u] - 1) / w[u];
+        return (int)std::min<long>(k, steps[u]);
+    };
+    s.cta.assign(P + 1, 0);
+    int u0 = 0;
+    for (int c = 0; c < P; c++) {
+        const long lo = W * c / P, hi = W * (c + 1) / P;
+        s.cta[c] = (int)s.segs.size();
+        while (u0 < nu && pre[u0 + 1] <= lo) u0++;
+        for (int u = u0; u < nu && pre[u] < hi; u++) {
+            const int a = first_step(u, lo), b = first_step(u, hi);
+            if (b > a) s.segs.push_back(GemmSeg{u, a, b, 0});
+        }
+    }
+    s.cta[P] = (int)s.segs.size();
+    number_pieces(s, nu);
+    return s;
+}
+
 size_t b_bytes(const EnsGeomHost &g, int ni)
 {
     const int ntl = (g.ninst + ni - 1) / ni;
+    if (g.hier) return (size_t)ntl * g.nbkg * (size_t)(2 * ni * 16);
     return (size_t)ntl * g.kblocks * (size_t)(2 * ni * BK * 2);
+}
+
+void free_hbufs(HPlanBufs &P)
+{
+    void *ptrs[] = {P.units, P.segs, P.cta, P.ws, P.pws, P.p0, P.np, P.rows, P.zu};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    P = HPlanBufs();
+}
+
+// one pass of the hierarchical geometries for instance tiles of width ni: units
+// (pass 1 or 2 of every geometry and instance tile), weighted stream-K segments,
+// partial-sum offsets, and for pass 1 the Z destination of every unit
+int upload_hplan(ucg_ensemble *E, HPlanBufs &P, int ni, int pass)
+{
+    std::vector<HUnit> units;
+    std::vector<HZUnit> zu;
+    for (const EnsGeomHost &g : E->geoms) {
+        if (!g.hier) continue;
+        const int ntl = (g.ninst + ni - 1) / ni;
+        const size_t bt = (size_t)g.nbkg * 2 * ni * 16;
+        for (int nt = 0; nt < ntl; nt++)
+            for (const EnsGeomHost::HU &h : (pass == 1 ? g.hu1 : g.hu2)) {
+                HUnit u;
+                u.a = g.hA + h.a_off;
+                u.lo_off = h.lo_off;
+                u.bidx = g.hbidx + h.bidx_off;
+                u.b = g.B + nt * bt;
+                u.g = h.g;
+                u.nkg = h.nkg;
+                u.rows = 8 * h.g;
+                u.pad = 0;
+                units.push_back(u);
+                if (pass == 1) zu.push_back(HZUnit{g.B + nt * bt, h.zkg0, h.g, 8 * h.g, 0, 0, 0});
+            }
+    }
+    P.nunits = (int)units.size();
+    if (units.empty()) return UCG_OK;
+    std::vector<int> steps, w;
+    for (const HUnit &u : units) {
+        steps.push_back(u.nkg / 2);
+        w.push_back(u.g + 4);      // a K-step's bytes grow with the row groups; its MMAs do not
+    }
+    Sched s = sched_weighted(steps, w, E->sms);
+    std::vector<long> pws(std::max(1, s.nslots));
+    long off = 0;
+    for (int u = 0; u < P.nunits; u++)
+        for (int j = 0; j < s.npieces[u]; j++) {
+            pws[s.piece0[u] + j] = off;
+            off += (long)units[u].rows * ni;
+        }
+    std::vector<HSeg> segs;
+    for (const GemmSeg &q : s.segs) segs.push_back(HSeg{q.tile, 2 * q.kb0, 2 * q.kb1, 0, pws[q.slot]});
+    std::vector<int> rows;
+    for (const HUnit &u : units) rows.push_back(u.rows);
+    for (size_t u = 0; u < zu.size(); u++) {
+        zu[u].p0 = s.piece0[u];
+        zu[u].np = s.npieces[u];
+    }
+    P.nsegs = (int)segs.size();
+    P.ws_floats = (size_t)std::max<long>(off, 4);
+    ECUDA(cudaMalloc(&P.units, sizeof(HUnit) * units.size()));
+    ECUDA(cudaMalloc(&P.segs, sizeof(HSeg) * std::max<size_t>(segs.size(), 1)));
+    ECUDA(cudaMalloc(&P.cta, sizeof(int) * s.cta.size()));
+    ECUDA(cudaMalloc(&P.ws, sizeof(float) * P.ws_floats));
+    ECUDA(cudaMalloc(&P.pws, sizeof(long) * pws.size()));
+    ECUDA(cudaMalloc(&P.p0, sizeof(int) * units.size()));
+    ECUDA(cudaMalloc(&P.np, sizeof(int) * units.size()));
+    ECUDA(cudaMalloc(&P.rows, sizeof(int) * units.size()));
+    ECUDA(cudaMemsetAsync(P.ws, 0, sizeof(float) * P.ws_floats, E->stream));
+    ECUDA(cudaMemcpyAsync(P.units, units.data(), sizeof(HUnit) * units.size(), cudaMemcpyHostToDevice, E->stream));
+    if (!segs.empty())
+        ECUDA(cudaMemcpyAsync(P.segs, segs.data(), sizeof(HSeg) * segs.size(), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(P.cta, s.cta.data(), sizeof(int) * s.cta.size(), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(P.pws, pws.data(), sizeof(long) * pws.size(), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(P.p0, s.piece0.data(), sizeof(int) * units.size(), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(P.np, s.npieces.data(), sizeof(int) * units.size(), cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaMemcpyAsync(P.rows, rows.data(), sizeof(int) * units.size(), cudaMemcpyHostToDevice, E->stream));
+    if (pass == 1) {
+        ECUDA(cudaMalloc(&P.zu, sizeof(HZUnit) * zu.size()));
+        ECUDA(cudaMemcpyAsync(P.zu, zu.data(), sizeof(HZUnit) * zu.size(), cudaMemcpyHostToDevice, E->stream));
+    }
+    // the host vectors are released on return: the copies must have been made
+    ECUDA(cudaStreamSynchronize(E->stream));
+    return UCG_OK;
+}
+
+template <int NI>
+cudaError_t prepare_hcontract_t()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_hm_contract<NI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         HTile<NI, true>::SMEM);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_hm_contract<NI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                HTile<NI, false>::SMEM);
+}
+
+template <int NI, bool KLO>
+cudaError_t launch_hpass_t(ucg_ensemble *E, const HPlanBufs &P)
+{
+    k_hm_contract<NI, KLO><<<E->sms, 192, HTile<NI, KLO>::SMEM, E->stream>>>(P.units, P.segs, P.cta, P.ws,
+                                                                            &E->d_glob->err);
+    E->launches++;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hpass(ucg_ensemble *E, const HPlanBufs &P, bool klo)
+{
+    switch (E->ni) {
+    case 32: return klo ? launch_hpass_t<32, true>(E, P) : launch_hpass_t<32, false>(E, P);
+    case 64: return klo ? launch_hpass_t<64, true>(E, P) : launch_hpass_t<64, false>(E, P);
+    case 128: return klo ? launch_hpass_t<128, true>(E, P) : launch_hpass_t<128, false>(E, P);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// T = H V of every hierarchical geometry: pass 1, Z into the B space, pass 2
+cudaError_t launch_hier(ucg_ensemble *E, bool klo)
+{
+    cudaError_t e = cudaSuccess;
+    if (E->h1.nunits > 0) {
+        e = launch_hpass(E, E->h1, klo);
+        if (e != cudaSuccess) return e;
+        k_hm_zconv<<<E->h1.nunits, 256, 0, E->stream>>>(E->h1.zu, E->h1.pws, E->h1.ws, E->ni);
+        E->launches++;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (E->h2.nunits > 0) e = launch_hpass(E, E->h2, klo);
+    return e;
 }
 
 // the dynamic shared-memory limit is raised once per plan, outside any capture
@@ -1106,11 +1878,18 @@ cudaError_t prepare_contract_t()
 
 cudaError_t prepare_contract(int ni)
 {
+    cudaError_t e;
     switch (ni) {
-    case 32: return prepare_contract_t<32>();
-    case 64: return prepare_contract_t<64>();
-    case 128: return prepare_contract_t<128>();
+    case 32: e = prepare_contract_t<32>(); break;
+    case 64: e = prepare_contract_t<64>(); break;
+    case 128: e = prepare_contract_t<128>(); break;
     default: return cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess) return e;
+    switch (ni) {
+    case 32: return prepare_hcontract_t<32>();
+    case 64: return prepare_hcontract_t<64>();
+    default: return prepare_hcontract_t<128>();
     }
 }
 
@@ -1127,12 +1906,21 @@ cudaError_t launch_contract_t(ucg_ensemble *E, const PlanBufs &P)
 // stage increments' Khi (Vhi + Vlo) over pairs of M-tiles
 cudaError_t launch_contract(ucg_ensemble *E, bool klo = true)
 {
+    if (E->p1.nunits == 0) return cudaSuccess;   // no dense geometry
     switch (E->ni) {
     case 32: return klo ? launch_contract_t<32, true, 1>(E, E->p1) : launch_contract_t<32, false, 2>(E, E->p2);
     case 64: return klo ? launch_contract_t<64, true, 1>(E, E->p1) : launch_contract_t<64, false, 2>(E, E->p2);
     case 128: return klo ? launch_contract_t<128, true, 1>(E, E->p1) : launch_contract_t<128, false, 2>(E, E->p2);
     default: return cudaErrorInvalidValue;
     }
+}
+
+// the contraction of every geometry, dense and hierarchical
+cudaError_t launch_all(ucg_ensemble *E, bool klo)
+{
+    cudaError_t e = launch_contract(E, klo);
+    if (e == cudaSuccess) e = launch_hier(E, klo);
+    return e;
 }
 
 void free_bufs(PlanBufs &P)
@@ -1147,6 +1935,8 @@ void free_plan(ucg_ensemble *E)
 {
     free_bufs(E->p1);
     free_bufs(E->p2);
+    free_hbufs(E->h1);
+    free_hbufs(E->h2);
     if (E->graph) cudaGraphExecDestroy(E->graph);
     E->graph = nullptr;
     E->planned = false;
@@ -1158,6 +1948,7 @@ std::vector<int> unit_kblocks(ucg_ensemble *E, int ni, int mt)
 {
     std::vector<int> tkb;
     for (const EnsGeomHost &g : E->geoms) {
+        if (g.hier) continue;
         const int ntl = (g.ninst + ni - 1) / ni;
         const int nu = (g.mtiles + mt - 1) / mt;
         for (int nt = 0; nt < ntl; nt++)
@@ -1185,6 +1976,7 @@ int upload_plan(ucg_ensemble *E, PlanBufs &P, int ni, int mt, const Sched &s)
 {
     std::vector<GemmTile> units;
     for (const EnsGeomHost &g : E->geoms) {
+        if (g.hier) continue;
         const int ntl = (g.ninst + ni - 1) / ni;
         for (int nt = 0; nt < ntl; nt++)
             for (int t = 0; t < g.mtiles; t += mt)
@@ -1197,6 +1989,7 @@ int upload_plan(ucg_ensemble *E, PlanBufs &P, int ni, int mt, const Sched &s)
     P.nsegs = (int)s.segs.size();
     P.nslots = s.nslots;
     P.name = s.name;
+    if (units.empty()) return UCG_OK;   // no dense geometry
     ECUDA(cudaMalloc(&P.tiles, sizeof(GemmTile) * units.size()));
     ECUDA(cudaMalloc(&P.segs, sizeof(GemmSeg) * std::max<size_t>(1, s.segs.size())));
     ECUDA(cudaMalloc(&P.cta, sizeof(int) * s.cta.size()));
@@ -1225,13 +2018,14 @@ int install_plan(ucg_ensemble *E, int ni, const Sched &s1, const Sched &s2)
     ECUDA(prepare_contract(ni));
     E->ni = ni;
     if ((st = upload_plan(E, E->p1, ni, 1, s1)) || (st = upload_plan(E, E->p2, ni, 2, s2))) return st;
+    if ((st = upload_hplan(E, E->h1, ni, 1)) || (st = upload_hplan(E, E->h2, ni, 2))) return st;
 
     // kernel argument block
     EnsArgs a;
     memset(&a, 0, sizeof a);
     a.ngeom = (int)E->geoms.size();
     a.ni = ni;
-    int tile0 = 0, pair0 = 0, be = 0, bs = 0;
+    int tile0 = 0, pair0 = 0, be = 0, bs = 0, hunit0 = 0;
     for (int gi = 0; gi < a.ngeom; gi++) {
         const EnsGeomHost &g = E->geoms[gi];
         GeomDev &d = a.g[gi];
@@ -1240,11 +2034,23 @@ int install_plan(ucg_ensemble *E, int ni, const Sched &s1, const Sched &s2)
         d.mtiles = g.mtiles;
         d.kblocks = g.kblocks;
         const int ntl = (g.ninst + ni - 1) / ni;
-        d.tile0 = tile0;
-        tile0 += ntl * g.mtiles;
-        d.mpairs = (g.mtiles + 1) / 2;
-        d.pair0 = pair0;
-        pair0 += ntl * d.mpairs;
+        if (g.hier) {
+            d.hier = 1;
+            d.hleaves = g.hleaves;
+            d.hunit0 = hunit0;
+            hunit0 += ntl * g.hleaves;
+            d.hbtile = (size_t)g.nbkg * 2 * ni * 16;
+            d.hperm = g.hperm;
+            d.hinv = g.hinv;
+            d.hrow = g.hrow;
+            d.hxpos = g.hxpos;
+        } else {
+            d.tile0 = tile0;
+            tile0 += ntl * g.mtiles;
+            d.mpairs = (g.mtiles + 1) / 2;
+            d.pair0 = pair0;
+            pair0 += ntl * d.mpairs;
+        }
         d.epb_e = (g.np + EW_THREADS - 1) / EW_THREADS;
         d.blk_e0 = be;
         be += d.epb_e * g.ninst;
@@ -1276,10 +2082,25 @@ int install_plan(ucg_ensemble *E, int ni, const Sched &s1, const Sched &s2)
     a.ws2 = E->p2.ws;
     a.piece0_2 = E->p2.piece0;
     a.npieces_2 = E->p2.npieces;
+    a.hws2 = E->h2.ws;
+    a.hp0 = E->h2.p0;
+    a.hnp = E->h2.np;
+    a.hrows = E->h2.rows;
+    a.hpws = E->h2.pws;
     a.glob = E->d_glob;
     ECUDA(cudaMemcpyAsync(E->d_args, &a, sizeof a, cudaMemcpyHostToDevice, E->stream));
     ECUDA(cudaStreamSynchronize(E->stream));
     E->plan_name = "ni=" + std::to_string(ni) + " anchor " + s1.name + ", increments " + s2.name + " (pairs)";
+    if (E->h1.nunits + E->h2.nunits > 0) {
+        size_t img = 0;
+        for (const EnsGeomHost &g : E->geoms)
+            if (g.hier) img += g.h_img_bytes;
+        char buf[256];
+        snprintf(buf, sizeof buf,
+                 "; hierarchical: pass 1 %d units / %d segments, pass 2 %d units / %d segments, images %.4f GB",
+                 E->h1.nunits, E->h1.nsegs, E->h2.nunits, E->h2.nsegs, img * 1e-9);
+        E->plan_name += buf;
+    }
     E->planned = true;
     return UCG_OK;
 }
@@ -1313,11 +2134,11 @@ int time_contract(ucg_ensemble *E, int reps, double *ms, bool klo = true)
     cudaEvent_t a, b;
     ECUDA(cudaEventCreate(&a));
     ECUDA(cudaEventCreate(&b));
-    for (int w = 0; w < 2; w++) ECUDA(launch_contract(E, klo));
+    for (int w = 0; w < 2; w++) ECUDA(launch_all(E, klo));
     double best = 1e300;
     for (int trial = 0; trial < 3; trial++) {
         ECUDA(cudaEventRecord(a, E->stream));
-        for (int r = 0; r < reps; r++) ECUDA(launch_contract(E, klo));
+        for (int r = 0; r < reps; r++) ECUDA(launch_all(E, klo));
         ECUDA(cudaEventRecord(b, E->stream));
         ECUDA(cudaEventSynchronize(b));
         float t = 0.0f;
@@ -1338,7 +2159,7 @@ template <int S>
 cudaError_t enqueue_stage(ucg_ensemble *E, int be)
 {
     k_ens_prologue<S><<<be, EW_THREADS, 0, E->stream>>>(E->d_args);
-    cudaError_t e = launch_contract(E, S == 1);
+    cudaError_t e = launch_all(E, S == 1);
     if (e != cudaSuccess) return e;
     k_ens_rhs<S><<<be, EW_THREADS, 0, E->stream>>>(E->d_args);
     E->launches += 2;
@@ -1458,7 +2279,8 @@ void ucg_ens_destroy(ucg_ensemble *E)
     if (E->stream) cudaStreamSynchronize(E->stream);
     free_plan(E);
     for (EnsGeomHost &g : E->geoms) {
-        void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl, g.B};
+        void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl, g.B, g.hA, g.hbidx, g.hperm, g.hinv,
+                        g.hxpos, g.hrow};
         for (void *p : ptrs)
             if (p) cudaFree(p);
     }
@@ -1477,7 +2299,11 @@ int ucg_ens_add_geometry(ucg_ensemble *E, ucg_ctx *c, int n_instances, int *geom
     if (!E || !c) return UCG_E_BADARG;
     if (n_instances < 1 || n_instances > 4096) return ebad(E, UCG_E_BADARG, "n_instances must be 1..4096");
     if ((int)E->geoms.size() >= MAX_GEOM) return ebad(E, UCG_E_BADARG, "too many geometries");
-    if (!c->assembled || !c->K) return ebad(E, UCG_E_STATE, "context has no assembled FP64 matrix");
+    // the hierarchical K when the context steps on it or holds no dense K
+    const bool hier = c->hm && (c->precision == UCG_PREC_HMATRIX || c->precision == UCG_PREC_HMATRIX_SPLIT ||
+                                !c->assembled || !c->K);
+    if (!hier && (!c->assembled || !c->K))
+        return ebad(E, UCG_E_STATE, "context has no assembled FP64 matrix and no hierarchical matrix");
     if (c->nv != 0) return ebad(E, UCG_E_UNSUPPORTED, "ensembles take fault patches only");
     if (c->device != E->device) return ebad(E, UCG_E_BADARG, "context on another device");
     ECUDA(cudaSetDevice(E->device));
@@ -1493,8 +2319,24 @@ int ucg_ens_add_geometry(ucg_ensemble *E, ucg_ctx *c, int n_instances, int *geom
     const long rows_pad = (long)g.mtiles * BM;
     const size_t aimg = (size_t)g.mtiles * g.kblocks * A_IMG;
     const long len = (long)g.ninst * 7 * g.np;
-    cudaError_t e = cudaMalloc(&g.A, aimg);
-    if (e == cudaSuccess) e = cudaMalloc(&g.rscale, sizeof(float) * rows_pad);
+    cudaError_t e = cudaSuccess;
+    if (hier) {
+        ucg::HLayout L;
+        ucg::hmatrix_layout(c, &L);
+        int st = build_hgeom(E, L, g);
+        if (st) {
+            void *ptrs[] = {g.hA, g.hbidx, g.hperm, g.hinv, g.hxpos, g.hrow};
+            for (void *p : ptrs)
+                if (p) cudaFree(p);
+            return st;
+        }
+        size_t fb = 0;
+        ucg::hmatrix_info(c, nullptr, nullptr, nullptr, &fb, nullptr, nullptr);
+        g.h_fp64_bytes = fb;
+    } else {
+        e = cudaMalloc(&g.A, aimg);
+        if (e == cudaSuccess) e = cudaMalloc(&g.rscale, sizeof(float) * rows_pad);
+    }
     if (e == cudaSuccess) e = cudaMalloc(&g.state, sizeof(double) * 12 * len);
     if (e == cudaSuccess) e = cudaMalloc(&g.anchor, sizeof(double) * 5L * g.ninst * g.np);
     if (e == cudaSuccess) e = cudaMalloc(&g.par, sizeof(double) * 7L * g.ninst * g.np);
@@ -1511,7 +2353,7 @@ int ucg_ens_add_geometry(ucg_ensemble *E, ucg_ctx *c, int n_instances, int *geom
         }
         e = cudaMemcpy(g.ctl, ctl.data(), sizeof(InstCtl) * g.ninst, cudaMemcpyHostToDevice);
     }
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess && !hier) {
         k_row_scale<<<(unsigned)((rows_pad + 7) / 8), 256, 0, E->stream>>>(c->K, g.m, g.n, rows_pad, g.rscale);
         const long work = rows_pad * (long)g.kblocks * (BK / 8);
         k_pack_k<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(c->K, g.m, g.n, g.kblocks, rows_pad,
@@ -1521,7 +2363,7 @@ int ucg_ens_add_geometry(ucg_ensemble *E, ucg_ctx *c, int n_instances, int *geom
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
     if (e != cudaSuccess) {
-        void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl};
+        void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl, g.hA, g.hbidx, g.hperm, g.hinv, g.hxpos, g.hrow};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         return efail(E, e, "ucg_ens_add_geometry");
@@ -1738,14 +2580,24 @@ int ucg_ens_matvec(ucg_ensemble *E, int gi, const double *V, double *T, int term
     cudaError_t e = cudaMalloc(&dT, sizeof(double) * g.ninst * g.m);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dV, V, sizeof(double) * g.ninst * g.n, cudaMemcpyHostToDevice, E->stream);
     if (e == cudaSuccess) {
-        const long work = (long)g.ninst * ((g.n + 1) / 2);
-        k_pack_v_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(g.B, E->ni, g.kblocks, g.ninst, g.n, dV);
+        if (g.hier) {
+            const long work = (long)g.ninst * g.np;
+            k_pack_x_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(E->d_args, gi, dV);
+        } else {
+            const long work = (long)g.ninst * ((g.n + 1) / 2);
+            k_pack_v_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(g.B, E->ni, g.kblocks, g.ninst,
+                                                                                 g.n, dV);
+        }
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = launch_contract(E, terms == 3);
+    if (e == cudaSuccess) e = launch_all(E, terms == 3);
     if (e == cudaSuccess) {
         const long work = (long)g.ninst * g.m;
-        k_reduce_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(E->d_args, gi, dT, terms == 2 ? 1 : 0);
+        if (g.hier)
+            k_reduce_h<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(E->d_args, gi, dT);
+        else
+            k_reduce_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(E->d_args, gi, dT,
+                                                                                 terms == 2 ? 1 : 0);
         E->launches += 2;
         e = cudaGetLastError();
     }

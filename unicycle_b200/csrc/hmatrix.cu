@@ -101,6 +101,9 @@ struct HMat {
     double *panel = nullptr;             // the row data of every chunk, chunk after chunk
     long panel_len = 0;                  // doubles
     std::vector<HLowRank> lr_h;          // host copy of the low-rank descriptors
+    std::vector<int> leaf_e0_h, leaf_term0_h;   // host copies of the leaves and their term ranges
+    std::vector<HLeafTerm> terms_h;
+    std::vector<long> term_poff_h;       // panel offset (doubles) of every term
     // split copies (hi and lo bf16 of every value) for UCG_PREC_HMATRIX_SPLIT
     __nv_bfloat16 *ph = nullptr, *pl = nullptr, *vh = nullptr, *vl = nullptr;
     int *status_d = nullptr;             // nonzero: a bulk copy of the row kernel timed out
@@ -965,6 +968,11 @@ int hmatrix_build(ucg_ctx *c, int okada_mode, double eta, double eps, int leaf)
         leaf_chunk.push_back((int)chunks.size());
     }
     h->n_chunks = (int)chunks.size();
+    h->leaf_e0_h = leaf_e0;
+    h->leaf_term0_h.assign(1, 0);
+    for (int L = 0; L < h->n_leaves; L++) h->leaf_term0_h.push_back(chunks[leaf_chunk[L + 1] - 1].q1);
+    h->term_poff_h.resize(pk.size());
+    for (size_t q = 0; q < pk.size(); q++) h->term_poff_h[q] = pk[q].dst;
     {
         double *panel = nullptr;
         UCG_CUDA(cudaMalloc(&panel, sizeof(double) * std::max<long>(poff, 2)));
@@ -983,6 +991,7 @@ int hmatrix_build(ucg_ctx *c, int okada_mode, double eta, double eps, int leaf)
         for (void *p : temp_allocs) cudaFree(p);
         for (HLowRank &b : lr) b.U = nullptr;   // the product reads U from the panels
         for (HLeafTerm &T : terms) T.A = nullptr;
+        h->terms_h = terms;
     }
     h->n_items = (long)items.size();
     h->nz = std::max<long>(zoff, 1);
@@ -1111,6 +1120,26 @@ void hmatrix_apply_split(ucg_ctx *c, const double *v, double *t, bool lo)
 }
 
 double *hmatrix_t(ucg_ctx *c) { return c->hm ? c->hm->t_d : nullptr; }
+
+bool hmatrix_layout(const ucg_ctx *c, HLayout *out)
+{
+    const HMat *h = c->hm;
+    if (!h) return false;
+    out->np = h->np;
+    out->n_leaves = h->n_leaves;
+    out->perm = h->perm;
+    out->leaf_e0 = h->leaf_e0_h;
+    out->leaf_term0 = h->leaf_term0_h;
+    out->terms.clear();
+    for (size_t q = 0; q < h->terms_h.size(); q++) {
+        const HLeafTerm &T = h->terms_h[q];
+        out->terms.push_back({h->term_poff_h[q], T.cols, T.xsel, T.xoff});
+    }
+    out->lr.clear();
+    for (const HLowRank &b : h->lr_h) out->lr.push_back({b.V, b.k, b.n, b.s0, b.zoff});
+    out->panel = h->panel;
+    return true;
+}
 
 void hmatrix_info(const ucg_ctx *c, long *n_dense, long *n_lowrank, long *n_fallback, size_t *bytes, int *max_rank,
                   double *build_ms)

@@ -219,6 +219,30 @@ double *hmatrix_t(ucg_ctx *c);                                 // the product's 
 void hmatrix_info(const ucg_ctx *c, long *n_dense, long *n_lowrank, long *n_fallback, size_t *bytes,
                   int *max_rank, double *build_ms);
 
+// The structure of a built hierarchical matrix, for consumers that lay its
+// stored values out again (the ensemble's tensor-core images).  Host vectors;
+// the value pointers are device addresses owned by the matrix.
+struct HLayout {
+    struct Term {                // one column piece of a row leaf's row panel
+        long poff;               // offset (doubles) of its rows x cols column-major slab in `panel`
+        int cols;
+        int xsel;                // 0: columns of the permuted input xp; 1: rank entries of z
+        long xoff;               // first xp column or z entry
+    };
+    struct LowRank {             // a stored low-rank block
+        const double *V;         // k x n, rank-major
+        int k, n, s0, zoff;      // rank, columns, first source element (permuted), z offset
+    };
+    int np = 0, n_leaves = 0;
+    std::vector<int> perm;       // permuted position -> element
+    std::vector<int> leaf_e0;    // n_leaves + 1 element offsets of the row (and column) leaves
+    std::vector<int> leaf_term0; // n_leaves + 1 offsets into terms
+    std::vector<Term> terms;
+    std::vector<LowRank> lr;
+    const double *panel = nullptr;
+};
+bool hmatrix_layout(const ucg_ctx *c, HLayout *out);
+
 // mlp.cu: device addresses of a step-size model's FP16 weights and standardisation
 }  // namespace ucg
 namespace ucg { namespace mlp { struct Norm; } }

@@ -165,7 +165,7 @@ class Ensemble:
         """dict: attempts, active, launches, accepted, rejected, time_sum, plan."""
         ta, act, la = ctypes.c_long(), ctypes.c_int(), ctypes.c_long()
         acc, rej, ts = ctypes.c_long(), ctypes.c_long(), ctypes.c_double()
-        buf = ctypes.create_string_buffer(256)
+        buf = ctypes.create_string_buffer(1024)
         self._check(self.lib.ucg_ens_info(self.ens, ctypes.byref(ta), ctypes.byref(act), ctypes.byref(la),
                                           ctypes.byref(acc), ctypes.byref(rej), ctypes.byref(ts), buf, len(buf)),
                     "info")
