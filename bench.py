@@ -60,6 +60,9 @@ def parse():
     p.add_argument("--hm-eta", type=float, default=2.0, help="hierarchical matrix: admissibility parameter")
     p.add_argument("--hm-eps", type=float, default=1e-6, help="hierarchical matrix: ACA relative accuracy")
     p.add_argument("--hm-leaf", type=int, default=32, help="hierarchical matrix: patches per cluster leaf")
+    p.add_argument("--hm-ens-leaf", type=int, default=40,
+                   help="hierarchical ensemble: patches per cluster leaf (at most 42: a row leaf is one 128-row tile)")
+    p.add_argument("--no-hier-ensemble", action="store_true", help="skip the hierarchical-ensemble leg")
     p.add_argument("--trace-runs", type=int, default=64, help="seeded cfg1 runs that record training traces")
     p.add_argument("--trace-attempts", type=int, default=16000, help="attempts of the trace-recording runs")
     p.add_argument("--learned-eval-years", type=float, default=15.0,
@@ -617,6 +620,83 @@ def hmatrix_leg(args, local, sim, cfg, plain):
                          "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind}}
 
 
+def hier_ensemble_leg(args, local, cfg, sets, y0s, dense, Kr):
+    """The headline ensemble with K replaced by its hierarchical approximation
+    (a context that never assembles the dense K): the two-pass tcgen05
+    contraction over the hierarchical operand images, timed the same way as
+    the dense ensemble, its contraction's bandwidth, and its accuracy against
+    the FP64 hierarchical product and the dense K's first rows."""
+    import torch
+    import unicycle_b200
+    n = cfg["n_patch"]
+    nn = 2 * n
+    sim = unicycle_b200.Simulation(cfg["mu"], cfg["lam"], device=local)
+    i1, i2, i3, v = cfg["mesh"]["tri"]
+    sim.set_triangles(i1, i2, i3, v)
+    t0 = time.perf_counter()
+    sim.build_hmatrix(eta=args.hm_eta, eps=args.hm_eps, leaf=args.hm_ens_leaf)
+    build_s = time.perf_counter() - t0
+    info = sim.hmatrix_info()
+    sim.set_precision(unicycle_b200.UCG_PREC_HMATRIX)
+    ens = unicycle_b200.Ensemble(device=local)
+    t0 = time.perf_counter()
+    ens.add_geometry(sim, args.sets)
+    images_s = time.perf_counter() - t0
+    for i, (fr, y0) in enumerate(zip(sets, y0s)):
+        ens.set_friction(0, i, fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
+                         fr["damping"])
+        ens.set_state(0, i, y0, 0.0, cfg["dt0"])
+    ens.set_tolerance(cfg["epsilon"])
+    stream = torch.cuda.ExternalStream(ens.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ens.run(1e300, args.spinup + args.warmup)
+    i0 = ens.info()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    attempts = ens.run(1e300, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    i1 = ens.info()
+    acc = i1["accepted"] - i0["accepted"]
+    rej = i1["rejected"] - i0["rejected"]
+    ms_a, ms_c = ens.profile_contract(10)
+    plan = i1["plan"]
+    img = float(plan.split("images ")[1].split(" GB")[0]) * 1e9 if "images " in plan else None
+    peak, peak_kind = load_peaks()
+    # accuracy: instances 0-2 against the FP64 hierarchical product, and the
+    # first 768 rows against the dense K (the approximation's error included)
+    V = np.random.default_rng(7).standard_normal((args.sets, nn)) * 1e-9
+    T = ens.matvec(0, V)
+    T2 = ens.matvec(0, V, terms=2)
+    ref = np.stack([sim.hmatrix_matvec(V[i]) for i in range(3)])
+    e_h = float(max(np.linalg.norm(T[i] - ref[i]) / np.linalg.norm(ref[i]) for i in range(3)))
+    e_h2 = float(max(np.linalg.norm(T2[i] - ref[i]) / np.linalg.norm(ref[i]) for i in range(3)))
+    mag = np.abs(V) @ np.abs(Kr).T
+    e_k = float(np.max(np.abs(T[:, :Kr.shape[0]] - V @ Kr.T) / mag))
+    ens.close()
+    sim.close()
+    out = {"leaf": args.hm_ens_leaf, "eta": args.hm_eta, "eps": args.hm_eps, "hmatrix_build_seconds": build_s,
+           "images_seconds": images_s, "hmatrix_fp64_bytes": info["bytes"], "image_bytes": img,
+           "steps_per_s": acc / el, "ms_per_attempt": 1e3 * el / attempts, "accepted_steps": acc,
+           "rejected_attempts": rej,
+           "speedup_vs_dense_ensemble_ms_per_attempt": dense["ms_per_step"] / (1e3 * el / attempts),
+           "speedup_vs_plain_fp64_steps": acc / el / dense["plain_value"],
+           "plan": plan,
+           "contraction_ms": {"anchor": ms_a, "increment": ms_c},
+           "rel_l2_error_vs_fp64_hmatrix": {"anchor": e_h, "increment_form": e_h2},
+           "max_rel_to_abs_product_vs_dense_K_rows_0_767": e_k}
+    if img:
+        inc = img / 2
+        out["roofline"] = {"bound": "hbm", "kernel": "k_hm_contract<64,false> x2 + k_hm_zconv (increment form; "
+                                                    "operand hi planes)", "bytes_per_launch": inc,
+                           "achieved": inc / (ms_c / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                           "frac": inc / (ms_c / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+                           "anchor": {"bytes_per_launch": img, "achieved": img / (ms_a / 1e3) / 1e9,
+                                      "frac": img / (ms_a / 1e3) / 1e9 / peak}}
+    return out
+
+
 def run_hmatrix(args, world, rank, local):
     """--workload hmatrix: the cfg2 megathrust at --nx x --nz cells held only as
     its hierarchical approximation (no dense K; at 200 x 200 = 80,000 triangles
@@ -773,6 +853,10 @@ def run_ensemble(args, world, rank, local):
     families = assembly_leg(args, local) if rank == 0 else None
     if families:
         families["nikkhoo_tri"] = {"entries": 6 * n * n, "ms": tri_ms, "mentries_per_s": 6 * n * n / tri_ms / 1e3}
+    hens = None
+    if rank == 0 and not args.no_hier_ensemble:
+        hens = hier_ensemble_leg(args, local, cfg, sets, y0s,
+                                 {"ms_per_step": 1e3 * elapsed / attempts, "plain_value": plain["value"]}, Kr)
     hmat = hmatrix_leg(args, local, sim, cfg, plain) if rank == 0 and not args.no_hmatrix else None
     learned = None
     if not args.no_learned and rank == 0:
@@ -833,6 +917,7 @@ def run_ensemble(args, world, rank, local):
             "assembly_families": families,
             "learned_step": learned,
             "hmatrix": hmat,
+            "hierarchical_ensemble": hens,
         }
     sim.close()
     return out

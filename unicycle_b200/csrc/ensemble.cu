@@ -88,11 +88,22 @@ struct Tile {
     static constexpr int STAGE = MT * A_BYTES + B_IMG;
     static constexpr int STAGES = (6 * 32768) / STAGE < 8 ? (6 * 32768) / STAGE : 8;   // ~192 KB in flight
     static constexpr int SMEM = STAGES * STAGE + 1024;   // + slack for 1024-byte alignment
-    static constexpr uint32_t TMEM_COLS = 2 * MT * NI;    // two sets of MT FP32 accumulators of NI columns
+    // MERGE: the V hi and lo images lie back to back in the stage, so one MMA
+    // of N = 2 NI computes Khi Vhi and Khi Vlo into the two halves of a
+    // 2 NI-column accumulator (the drain adds them); when two sets of MT such
+    // accumulators do not fit the 512 tensor-memory columns, two MMAs of N = NI
+    // accumulate into one NI-column accumulator instead
+    static constexpr bool MERGE = 2 * MT * 2 * NI <= 512;
+    static constexpr int ACC_N = MERGE ? 2 * NI : NI;
+    static constexpr uint32_t TMEM_COLS = 2 * MT * ACC_N; // two sets of MT FP32 accumulators
     // instruction descriptor: F32 accumulator, bf16 A and B, both K-major,
-    // N = NI (bits 17-22, N/8), M = 128 (bits 24-28, M/16)
-    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NI >> 3) << 17) |
-                                      ((uint32_t)(BM >> 4) << 24);
+    // N (bits 17-22, N/8), M = 128 (bits 24-28, M/16)
+    static constexpr uint32_t idesc(int n)
+    {
+        return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+    }
+    static constexpr uint32_t IDESC = idesc(NI);
+    static constexpr uint32_t IDESC2 = idesc(2 * NI);
 };
 
 // byte offset of element (r, k) in a 128-byte-swizzled tile image with 128-byte rows
@@ -227,6 +238,22 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(s_addr(dst)), "l"(src), "r"(bytes), "r"(s_addr(b)) : "memory");
 }
+// the same with an L2 eviction priority: operand images stream through once
+// (evict first); the instances' values are read by many tiles (evict last)
+__device__ __forceinline__ uint64_t l2_policy(bool keep)
+{
+    uint64_t p;
+    if (keep)
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ void bulk_load_hint(void *dst, const void *src, uint32_t bytes, uint64_t *b, uint64_t pol)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+                 ::"r"(s_addr(dst)), "l"(src), "r"(bytes), "r"(s_addr(b)), "l"(pol) : "memory");
+}
 // shared-memory matrix descriptor: K-major operand, 128-byte swizzle, 8-row
 // groups 1024 bytes apart (SBO), descriptor version 1
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
@@ -303,6 +330,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
     if (warp == 0) {
         if (lane == 0) {
             // producer: per k-block one copy of K per M-tile of the unit and one copy of V
+            const uint64_t pol_a = l2_policy(false), pol_b = l2_policy(true);
             long issued = 0;
             for (int q = q0; q < q1 && !abort_flag; q++) {
                 const GemmSeg sg = segs[q];
@@ -318,9 +346,9 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                     }
                     uint8_t *st = smem + (size_t)s * T::STAGE;
                     bar_expect_tx(&full[s], bytes);
-                    bulk_load(st, tl.a + (size_t)kb * A_IMG, T::A_BYTES, &full[s]);
-                    if (two) bulk_load(st + T::A_BYTES, tl.a1 + (size_t)kb * A_IMG, T::A_BYTES, &full[s]);
-                    bulk_load(st + MT * T::A_BYTES, tl.b + (size_t)kb * T::B_IMG, T::B_IMG, &full[s]);
+                    bulk_load_hint(st, tl.a + (size_t)kb * A_IMG, T::A_BYTES, &full[s], pol_a);
+                    if (two) bulk_load_hint(st + T::A_BYTES, tl.a1 + (size_t)kb * A_IMG, T::A_BYTES, &full[s], pol_a);
+                    bulk_load_hint(st + MT * T::A_BYTES, tl.b + (size_t)kb * T::B_IMG, T::B_IMG, &full[s], pol_b);
                     issued++;
                 }
             }
@@ -362,12 +390,18 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
 #pragma unroll
                         for (int u = 0; u < MT; u++) {
                             if (u < nt) {
-                                const uint32_t d = tmem + (uint32_t)((buf * MT + u) * NI);
+                                const uint32_t d = tmem + (uint32_t)((buf * MT + u) * T::ACC_N);
                                 const uint32_t au = a + (uint32_t)(u * T::A_BYTES);
                                 const uint64_t ahi = sw128_desc(au + 32u * j);
-                                mma_bf16(d, ahi, bhi, T::IDESC, acc);
-                                mma_bf16(d, ahi, blo, T::IDESC, 1u);
-                                if (KLO) mma_bf16(d, sw128_desc(au + A_HALF + 32u * j), bhi, T::IDESC, 1u);
+                                if (T::MERGE) {
+                                    // rows 0..NI-1 of the B operand are Vhi, NI..2NI-1 Vlo
+                                    mma_bf16(d, ahi, bhi, T::IDESC2, acc);
+                                    if (KLO) mma_bf16(d, sw128_desc(au + A_HALF + 32u * j), bhi, T::IDESC, 1u);
+                                } else {
+                                    mma_bf16(d, ahi, bhi, T::IDESC, acc);
+                                    mma_bf16(d, ahi, blo, T::IDESC, 1u);
+                                    if (KLO) mma_bf16(d, sw128_desc(au + A_HALF + 32u * j), bhi, T::IDESC, 1u);
+                                }
                             }
                         }
                     }
@@ -405,13 +439,21 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
             for (int u = 0; u < nt; u++) {
                 float *dst = ws + ((size_t)sg.slot * MT + u) * NI * BM + row;
                 const uint32_t tbase =
-                    tmem + (uint32_t)((buf * MT + u) * NI) + ((uint32_t)(quarter * 32) << 16);
+                    tmem + (uint32_t)((buf * MT + u) * T::ACC_N) + ((uint32_t)(quarter * 32) << 16);
 #pragma unroll
                 for (int c0 = 0; c0 < NI; c0 += 16) {
                     uint32_t r[16];
                     tmem_ld16(tbase + (uint32_t)c0, r);
+                    if (T::MERGE) {
+                        uint32_t r2[16];
+                        tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
 #pragma unroll
-                    for (int i = 0; i < 16; i++) dst[(size_t)(c0 + i) * BM] = __uint_as_float(r[i]);
+                        for (int i = 0; i < 16; i++)
+                            dst[(size_t)(c0 + i) * BM] = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 16; i++) dst[(size_t)(c0 + i) * BM] = __uint_as_float(r[i]);
+                    }
                 }
             }
             tc_fence_before();
@@ -459,8 +501,12 @@ struct HTile {
     // + 1024 for the alignment and 32 KB past the last stage: every descriptor's
     // reach, read with its two strides either way round, stays inside the allocation
     static constexpr int SMEM = STAGES * STAGE + 1024 + 32768;
-    static constexpr uint32_t TMEM_COLS = 2 * NI;
+    // one MMA of N = 2 NI per K-step reads the hi and lo planes of the B
+    // K-groups together (they are consecutive 8-row groups); the drain adds
+    // the accumulator's two halves
+    static constexpr uint32_t TMEM_COLS = 4 * NI;
     static constexpr uint32_t IDESC = Tile<NI, false, 1>::IDESC;
+    static constexpr uint32_t IDESC2 = Tile<NI, false, 1>::IDESC2;
 };
 
 struct HUnit {                  // one M-tile of one pass for one instance tile
@@ -530,6 +576,7 @@ __global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict_
         if (lane == 0) {
             // producer: per stage one copy of the unit's hi (and lo) planes and
             // one copy per run of consecutive B K-groups
+            const uint64_t pol_a = l2_policy(false), pol_b = l2_policy(true);
             long issued = 0;
             for (int q = q0; q < q1 && !abort_flag; q++) {
                 const HSeg sg = segs[q];
@@ -539,6 +586,11 @@ __global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict_
                     const int nk = min(HKG_STAGE, sg.kg1 - kg);
                     const int s = (int)(issued % T::STAGES);
                     const uint32_t ph = (uint32_t)((issued / T::STAGES) & 1);
+                    // the stage's B K-groups: independent loads, in flight while
+                    // the slot is awaited
+                    int bi[HKG_STAGE];
+#pragma unroll
+                    for (int j = 0; j < HKG_STAGE; j++) bi[j] = j < nk ? __ldg(U.bidx + kg + j) : 0;
                     if (!bar_wait(&empty[s], ph ^ 1u, &abort_flag)) {
                         if (!abort_flag) fail();
                         break;
@@ -546,16 +598,23 @@ __global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict_
                     uint8_t *st = smem + (size_t)s * T::STAGE;
                     const uint32_t abytes = (uint32_t)nk * plane;
                     bar_expect_tx(&full[s], (KLO ? 2u : 1u) * abytes + (uint32_t)nk * T::B_KG);
-                    bulk_load(st, U.a + (size_t)kg * plane, abytes, &full[s]);
-                    if (KLO) bulk_load(st + HA_PLANE, U.a + U.lo_off + (size_t)kg * plane, abytes, &full[s]);
+                    bulk_load_hint(st, U.a + (size_t)kg * plane, abytes, &full[s], pol_a);
+                    if (KLO) bulk_load_hint(st + HA_PLANE, U.a + U.lo_off + (size_t)kg * plane, abytes, &full[s], pol_a);
                     uint8_t *bst = st + T::A_BYTES;
-                    for (int j = 0; j < nk;) {
-                        const int b0 = U.bidx[kg + j];
-                        int r = 1;
-                        while (j + r < nk && U.bidx[kg + j + r] == b0 + r) r++;
-                        bulk_load(bst + (size_t)j * T::B_KG, U.b + (size_t)b0 * T::B_KG, (uint32_t)r * T::B_KG,
-                                  &full[s]);
-                        j += r;
+                    // one copy per run of consecutive B K-groups
+                    int rs = 0, bs = bi[0];
+#pragma unroll
+                    for (int j = 1; j <= HKG_STAGE; j++) {
+                        if (j > nk) break;
+                        const bool cont = j < HKG_STAGE && j < nk && bi[j] == bi[j - 1] + 1;
+                        if (!cont) {
+                            bulk_load_hint(bst + (size_t)rs * T::B_KG, U.b + (size_t)bs * T::B_KG,
+                                           (uint32_t)(j - rs) * T::B_KG, &full[s], pol_b);
+                            if (j < HKG_STAGE && j < nk) {
+                                rs = j;
+                                bs = bi[j];
+                            }
+                        }
                     }
                     issued++;
                 }
@@ -579,7 +638,7 @@ __global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict_
                 }
                 tc_fence_after();
                 bool ok = true;
-                const uint32_t d = tmem + (uint32_t)(buf * NI);
+                const uint32_t d = tmem + (uint32_t)(buf * 2 * NI);
                 for (int kg = sg.kg0; kg < sg.kg1; kg += HKG_STAGE, it++) {
                     const int nk = min(HKG_STAGE, sg.kg1 - kg);
                     const int s = (int)(it % T::STAGES);
@@ -595,12 +654,10 @@ __global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict_
                     for (int j = 0; j < nk / 2; j++) {
                         const uint32_t ao = (uint32_t)(2 * j) * plane, bo = (uint32_t)(2 * j) * T::B_KG;
                         const uint64_t ahi = cm_desc(a + ao, plane, 128u);
-                        const uint64_t bhi = cm_desc(b + bo, T::B_KG, 128u);
-                        const uint64_t blo = cm_desc(b + bo + NI * 16, T::B_KG, 128u);
+                        const uint64_t bhl = cm_desc(b + bo, T::B_KG, 128u);   // hi rows, then lo rows
                         const uint32_t acc = (kg > sg.kg0 || j > 0) ? 1u : 0u;
-                        mma_bf16(d, ahi, bhi, T::IDESC, acc);
-                        mma_bf16(d, ahi, blo, T::IDESC, 1u);
-                        if (KLO) mma_bf16(d, cm_desc(a + HA_PLANE + ao, plane, 128u), bhi, T::IDESC, 1u);
+                        mma_bf16(d, ahi, bhl, T::IDESC2, acc);
+                        if (KLO) mma_bf16(d, cm_desc(a + HA_PLANE + ao, plane, 128u), bhl, T::IDESC, 1u);
                     }
                     issued_any = true;
                     mma_commit(&empty[s]);
@@ -634,14 +691,16 @@ __global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict_
             }
             tc_fence_after();
             float *dst = ws + sg.ws + row;
-            const uint32_t tbase = tmem + (uint32_t)(buf * NI) + ((uint32_t)(quarter * 32) << 16);
+            const uint32_t tbase = tmem + (uint32_t)(buf * 2 * NI) + ((uint32_t)(quarter * 32) << 16);
 #pragma unroll
             for (int c0 = 0; c0 < NI; c0 += 16) {
-                uint32_t r[16];
+                uint32_t r[16], r2[16];
                 tmem_ld16(tbase + (uint32_t)c0, r);
+                tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
                 if (row < rows) {
 #pragma unroll
-                    for (int i = 0; i < 16; i++) dst[(size_t)(c0 + i) * rows] = __uint_as_float(r[i]);
+                    for (int i = 0; i < 16; i++)
+                        dst[(size_t)(c0 + i) * rows] = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
                 }
             }
             tc_fence_before();
