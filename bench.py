@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--nx", type=int, default=100, help="along-strike cells (2 triangles each per row)")
     p.add_argument("--nz", type=int, default=100, help="down-dip rows")
     p.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16"])
-    p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split", "coupled", "cfg4", "hmatrix"])
+    p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split", "coupled", "cfg4", "hmatrix", "hens"])
     p.add_argument("--coupled-size", default="64,64,16,8,8",
                    help="coupled assembly leg: fault nx,nz and volume nx,ny,nz")
     p.add_argument("--sets", type=int, default=N_SETS, help="instances in the ensemble workload")
@@ -697,6 +697,112 @@ def hier_ensemble_leg(args, local, cfg, sets, y0s, dense, Kr):
     return out
 
 
+def run_hier_ensemble(args, world, rank, local):
+    """--workload hens: args.sets frictional parameter sets of the cfg2
+    megathrust at --nx x --nz cells in one ensemble on the hierarchical K alone
+    (no dense K is assembled; at 200 x 200 = 80,000 triangles the dense FP64 K
+    would be 307 GB).  value = accepted steps/s summed over the instances."""
+    import torch
+    import unicycle_b200
+    from unicycle_b200 import configs
+    torch.cuda.set_device(local)
+    cfg = configs.cfg2(nx=args.nx, nz=args.nz)
+    n = cfg["n_patch"]
+    m, nn = 3 * n, 2 * n
+    sets, y0s = configs.parameter_sets(cfg, args.sets)
+    sim = unicycle_b200.Simulation(cfg["mu"], cfg["lam"], device=local)
+    i1, i2, i3, v = cfg["mesh"]["tri"]
+    sim.set_triangles(i1, i2, i3, v)
+    t0 = time.perf_counter()
+    sim.build_hmatrix(eta=args.hm_eta, eps=args.hm_eps, leaf=args.hm_ens_leaf)
+    build_s = time.perf_counter() - t0
+    info = sim.hmatrix_info()
+    sim.set_precision(unicycle_b200.UCG_PREC_HMATRIX)
+    ens = unicycle_b200.Ensemble(device=local)
+    t0 = time.perf_counter()
+    ens.add_geometry(sim, args.sets)
+    images_s = time.perf_counter() - t0
+    for i, (fr, y0) in enumerate(zip(sets, y0s)):
+        ens.set_friction(0, i, fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
+                         fr["damping"])
+        ens.set_state(0, i, y0, 0.0, cfg["dt0"])
+    ens.set_tolerance(cfg["epsilon"])
+    if args.ens_eager:
+        ens.use_graph(False)
+    stream = torch.cuda.ExternalStream(ens.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ens.run(1e300, args.spinup + args.warmup)
+    i0 = ens.info()
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0.record(stream)
+        attempts = ens.run(1e300, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    el_max = reduce_max(el, world, args)
+    i1 = ens.info()
+    acc = i1["accepted"] - i0["accepted"]
+    rej = i1["rejected"] - i0["rejected"]
+    sim_years = (i1["time_sum"] - i0["time_sum"]) / YEAR
+    ms_a, ms_c = ens.profile_contract(10)
+    plan = i1["plan"]
+    img = float(plan.split("images ")[1].split(" GB")[0]) * 1e9
+    peak, peak_kind = load_peaks()
+    # accuracy against the FP64 hierarchical product (instances 0-2)
+    V = np.random.default_rng(7).standard_normal((args.sets, nn)) * 1e-9
+    T = ens.matvec(0, V)
+    ref = np.stack([sim.hmatrix_matvec(V[i]) for i in range(3)])
+    err = float(max(np.linalg.norm(T[i] - ref[i]) / np.linalg.norm(ref[i]) for i in range(3)))
+    # end to end: every attempt, all instances' states host->device (pinned) and back
+    e2e_att = max(3, min(10, args.steps // 6))
+    pin = torch.empty((args.sets, 7 * n), dtype=torch.float64, pin_memory=True).numpy()
+    y_h, t_h, dt_h, *_r = ens.get_states(0, out=pin)
+    acc_e2e = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_att):
+        ens.set_states(0, y_h, t_h, dt_h)
+        ens.run(1e300, 1)
+        y_h, t_h, dt_h, acc_h, rej_h, st_h = ens.get_states(0, out=pin)
+        acc_e2e += int(acc_h.sum())
+    torch.cuda.synchronize()
+    e2e_el = reduce_max(time.perf_counter() - t0, world, args)
+    ens.close()
+    sim.close()
+    if rank != 0:
+        return None
+    inc = img / 2
+    return {"metric": f"RK45 steps/s at N={n}, {args.sets}-instance ensemble on the hierarchical K (aggregate)",
+            "value": world * acc / el_max, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el_max / attempts, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3/f32 product, f64 state",
+            "data": "synthetic (seeded cfg2 curved megathrust; Dc redrawn per parameter set)",
+            "config": {"workload": f"megathrust {n} Nikkhoo-Walter triangles x {args.sets} frictional parameter "
+                                   "sets, one ensemble, hierarchical K only", "n_triangles": n,
+                       "instances": args.sets, "K_shape": [m, nn], "dense_fp64_bytes": 8.0 * m * nn,
+                       "step": "one attempt of every instance (timed steps = attempts)",
+                       "parallelism": f"replicas x{world}", "rtol": cfg["epsilon"],
+                       "l2": "inputs larger than L2 (operand images %.2f GB)" % (img / 1e9), "plan": plan},
+            "sim_years_per_hour": world * sim_years / (el_max / 3600.0),
+            "accepted_steps": acc, "rejected_attempts": rej,
+            "hmatrix": {"build_seconds": build_s, "images_seconds": images_s, "eta": args.hm_eta,
+                        "eps": args.hm_eps, "leaf": args.hm_ens_leaf,
+                        **{k: info[k] for k in ("n_dense", "n_lowrank", "max_rank", "bytes", "compression")}},
+            "rel_l2_error_vs_fp64_hmatrix": err,
+            "roofline": {"bound": "hbm", "kernel": "k_hm_contract<64,false> x2 + k_hm_zconv (increment form; "
+                                                   "operand hi planes)", "ms_per_launch": ms_c,
+                         "bytes_per_launch": inc, "achieved": inc / (ms_c / 1e3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": inc / (ms_c / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+                         "traffic": None,
+                         "anchor": {"ms_per_launch": ms_a, "bytes_per_launch": img,
+                                    "achieved": img / (ms_a / 1e3) / 1e9, "frac": img / (ms_a / 1e3) / 1e9 / peak}},
+            "e2e": {"value": world * acc_e2e / e2e_el, "unit": "steps/s",
+                    "h2d_bytes_per_step": 8 * 7 * n * args.sets, "d2h_bytes_per_step": 8 * 7 * n * args.sets},
+            "gpu_launches": int(attempts * 32 + 3), "clocks": clk.summary(), "cpu_baseline": None}
+
+
 def run_hmatrix(args, world, rank, local):
     """--workload hmatrix: the cfg2 megathrust at --nx x --nz cells held only as
     its hierarchical approximation (no dense K; at 200 x 200 = 80,000 triangles
@@ -934,6 +1040,8 @@ def main():
         out = run_cfg4(args, world, rank, local)
     elif args.workload == "hmatrix":
         out = run_hmatrix(args, world, rank, local)
+    elif args.workload == "hens":
+        out = run_hier_ensemble(args, world, rank, local)
     elif args.workload == "coupled":
         import torch
         torch.cuda.set_device(local)
