@@ -59,6 +59,7 @@
 #include <queue>
 #include <string>
 #include <map>
+#include <numeric>
 #include <array>
 #include <vector>
 #include <cuda_bf16.h>
@@ -495,12 +496,14 @@ constexpr int HA_PLANE = HKG_STAGE * 16 * 128; // one plane of a stage for 16 ro
 template <int NI, bool KLO>
 struct HTile {
     static constexpr int B_KG = 2 * NI * 16;              // hi + lo of one K-group for NI instances
-    static constexpr int A_BYTES = KLO ? 2 * HA_PLANE : HA_PLANE;
-    static constexpr int STAGE = A_BYTES + HKG_STAGE * B_KG;
-    static constexpr int STAGES = (6 * 32768) / STAGE < 8 ? (6 * 32768) / STAGE : 8;
-    // + 1024 for the alignment and 32 KB past the last stage: every descriptor's
-    // reach, read with its two strides either way round, stays inside the allocation
-    static constexpr int SMEM = STAGES * STAGE + 1024 + 32768;
+    // two rings: the operand images stream from HBM and need many bytes in
+    // flight; the B K-groups come from L2 and need few
+    static constexpr int A_STAGE = KLO ? 2 * HA_PLANE : HA_PLANE;
+    static constexpr int B_STAGE = HKG_STAGE * B_KG;
+    static constexpr int SB = 3;
+    static constexpr int SA_FIT = (208 * 1024 - SB * B_STAGE) / A_STAGE;
+    static constexpr int SA = SA_FIT < 12 ? SA_FIT : 12;
+    static constexpr int SMEM = SA * A_STAGE + SB * B_STAGE + 1024;   // + 1024 for the alignment
     // one MMA of N = 2 NI per K-step reads the hi and lo planes of the B
     // K-groups together (they are consecutive 8-row groups); the drain adds
     // the accumulator's two halves
@@ -532,22 +535,32 @@ __device__ __forceinline__ uint64_t cm_desc(uint32_t saddr, uint32_t lbo, uint32
 }
 
 template <int NI, bool KLO>
-__global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict__ units,
+__global__ void __launch_bounds__(224, 1) k_hm_contract(const HUnit *__restrict__ units,
         const HSeg *__restrict__ segs, const int *__restrict__ cta_seg, float *__restrict__ ws, int *err)
 {
+    // warp 0: operand-image producer; warp 1: MMA issue; warps 2-5: drain
+    // (tensor-memory lane quarter = warp mod 4); warp 6: B producer.  Both
+    // producers walk the same sequence of stages (segments in order, eight
+    // K-groups at a time), each into its own ring.
     using T = HTile<NI, KLO>;
     extern __shared__ unsigned char dyn_smem[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dyn_smem) + 1023) & ~(uintptr_t)1023);
-    __shared__ __align__(8) uint64_t full[T::STAGES], empty[T::STAGES], acc_full[2], acc_empty[2], drain;
+    uint8_t *bring = smem + (size_t)T::SA * T::A_STAGE;
+    __shared__ __align__(8) uint64_t fullA[T::SA], emptyA[T::SA], fullB[T::SB], emptyB[T::SB], acc_full[2],
+        acc_empty[2], drain;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q0 = cta_seg[blockIdx.x], q1 = cta_seg[blockIdx.x + 1];
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < T::STAGES; s++) {
-            bar_init(&full[s], 1);
-            bar_init(&empty[s], 1);
+        for (int s = 0; s < T::SA; s++) {
+            bar_init(&fullA[s], 1);
+            bar_init(&emptyA[s], 1);
+        }
+        for (int s = 0; s < T::SB; s++) {
+            bar_init(&fullB[s], 1);
+            bar_init(&emptyB[s], 1);
         }
         for (int b = 0; b < 2; b++) {
             bar_init(&acc_full[b], 1);
@@ -574,54 +587,93 @@ __global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict_
 
     if (warp == 0) {
         if (lane == 0) {
-            // producer: per stage one copy of the unit's hi (and lo) planes and
-            // one copy per run of consecutive B K-groups
-            const uint64_t pol_a = l2_policy(false), pol_b = l2_policy(true);
+            // operand images: the unit's hi (and lo) planes of the stage's K-groups
+            const uint64_t pol_a = l2_policy(false);
             long issued = 0;
             for (int q = q0; q < q1 && !abort_flag; q++) {
                 const HSeg sg = segs[q];
                 const HUnit U = units[sg.unit];
                 const uint32_t plane = (uint32_t)U.g * 128u;
+                bool ok = true;
                 for (int kg = sg.kg0; kg < sg.kg1; kg += HKG_STAGE) {
                     const int nk = min(HKG_STAGE, sg.kg1 - kg);
-                    const int s = (int)(issued % T::STAGES);
-                    const uint32_t ph = (uint32_t)((issued / T::STAGES) & 1);
-                    // the stage's B K-groups: independent loads, in flight while
-                    // the slot is awaited
-                    int bi[HKG_STAGE];
-#pragma unroll
-                    for (int j = 0; j < HKG_STAGE; j++) bi[j] = j < nk ? __ldg(U.bidx + kg + j) : 0;
-                    if (!bar_wait(&empty[s], ph ^ 1u, &abort_flag)) {
+                    const int s = (int)(issued % T::SA);
+                    const uint32_t ph = (uint32_t)((issued / T::SA) & 1);
+                    if (!bar_wait(&emptyA[s], ph ^ 1u, &abort_flag)) {
                         if (!abort_flag) fail();
+                        ok = false;
                         break;
                     }
-                    uint8_t *st = smem + (size_t)s * T::STAGE;
+                    uint8_t *st = smem + (size_t)s * T::A_STAGE;
                     const uint32_t abytes = (uint32_t)nk * plane;
-                    bar_expect_tx(&full[s], (KLO ? 2u : 1u) * abytes + (uint32_t)nk * T::B_KG);
-                    bulk_load_hint(st, U.a + (size_t)kg * plane, abytes, &full[s], pol_a);
-                    if (KLO) bulk_load_hint(st + HA_PLANE, U.a + U.lo_off + (size_t)kg * plane, abytes, &full[s], pol_a);
-                    uint8_t *bst = st + T::A_BYTES;
-                    // one copy per run of consecutive B K-groups
-                    int rs = 0, bs = bi[0];
+                    bar_expect_tx(&fullA[s], (KLO ? 2u : 1u) * abytes);
+                    bulk_load_hint(st, U.a + (size_t)kg * plane, abytes, &fullA[s], pol_a);
+                    if (KLO) bulk_load_hint(st + HA_PLANE, U.a + U.lo_off + (size_t)kg * plane, abytes, &fullA[s], pol_a);
+                    issued++;
+                }
+                if (!ok) break;
+            }
+            for (long i = issued - T::SA > 0 ? issued - T::SA : 0; i < issued; i++)
+                bar_wait(&fullA[i % T::SA], (uint32_t)((i / T::SA) & 1), nullptr);
+        }
+    } else if (warp == 6) {
+        // B: the whole warp loads the B K-groups of 32 stages at once (lane l:
+        // stage l); lane 0 takes each stage's from its lane by shuffle and
+        // issues one copy per run of consecutive B K-groups
+        const uint64_t pol_b = l2_policy(true);
+        long issued = 0;
+        bool stop = false;
+        for (int q = q0; q < q1 && !stop; q++) {
+            const HSeg sg = segs[q];
+            const HUnit U = units[sg.unit];
+            for (int kgb = sg.kg0; kgb < sg.kg1 && !stop; kgb += 32 * HKG_STAGE) {
+                int my[HKG_STAGE];
+                const int kgl = kgb + lane * HKG_STAGE;
 #pragma unroll
-                    for (int j = 1; j <= HKG_STAGE; j++) {
-                        if (j > nk) break;
-                        const bool cont = j < HKG_STAGE && j < nk && bi[j] == bi[j - 1] + 1;
-                        if (!cont) {
-                            bulk_load_hint(bst + (size_t)rs * T::B_KG, U.b + (size_t)bs * T::B_KG,
-                                           (uint32_t)(j - rs) * T::B_KG, &full[s], pol_b);
-                            if (j < HKG_STAGE && j < nk) {
-                                rs = j;
-                                bs = bi[j];
+                for (int j = 0; j < HKG_STAGE; j++) my[j] = kgl + j < sg.kg1 ? __ldg(U.bidx + kgl + j) : 0;
+                const int nst = min(32, (sg.kg1 - kgb + HKG_STAGE - 1) / HKG_STAGE);
+                for (int t = 0; t < nst; t++) {
+                    const int kg = kgb + t * HKG_STAGE;
+                    const int nk = min(HKG_STAGE, sg.kg1 - kg);
+                    int bi[HKG_STAGE];
+#pragma unroll
+                    for (int j = 0; j < HKG_STAGE; j++) bi[j] = __shfl_sync(0xffffffffu, my[j], t);
+                    const int s = (int)(issued % T::SB);
+                    const uint32_t ph = (uint32_t)((issued / T::SB) & 1);
+                    int ok = 1;
+                    if (lane == 0) ok = bar_wait(&emptyB[s], ph ^ 1u, &abort_flag) ? 1 : 0;
+                    ok = __shfl_sync(0xffffffffu, ok, 0);
+                    if (!ok) {
+                        if (lane == 0 && !abort_flag) fail();
+                        stop = true;
+                        break;
+                    }
+                    if (lane == 0) {
+                        uint8_t *bst = bring + (size_t)s * T::B_STAGE;
+                        bar_expect_tx(&fullB[s], (uint32_t)nk * T::B_KG);
+                        int rs = 0, bs = bi[0];
+#pragma unroll
+                        for (int j = 1; j <= HKG_STAGE; j++) {
+                            if (j > nk) break;
+                            const bool cont = j < HKG_STAGE && j < nk && bi[j] == bi[j - 1] + 1;
+                            if (!cont) {
+                                bulk_load_hint(bst + (size_t)rs * T::B_KG, U.b + (size_t)bs * T::B_KG,
+                                               (uint32_t)(j - rs) * T::B_KG, &fullB[s], pol_b);
+                                if (j < HKG_STAGE && j < nk) {
+                                    rs = j;
+                                    bs = bi[j];
+                                }
                             }
                         }
                     }
+                    __syncwarp();
                     issued++;
                 }
             }
-            for (long i = issued - T::STAGES > 0 ? issued - T::STAGES : 0; i < issued; i++)
-                bar_wait(&full[i % T::STAGES], (uint32_t)((i / T::STAGES) & 1), nullptr);
         }
+        if (lane == 0)
+            for (long i = issued - T::SB > 0 ? issued - T::SB : 0; i < issued; i++)
+                bar_wait(&fullB[i % T::SB], (uint32_t)((i / T::SB) & 1), nullptr);
     } else if (warp == 1) {
         if (lane == 0) {
             long it = 0;
@@ -641,16 +693,16 @@ __global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict_
                 const uint32_t d = tmem + (uint32_t)(buf * 2 * NI);
                 for (int kg = sg.kg0; kg < sg.kg1; kg += HKG_STAGE, it++) {
                     const int nk = min(HKG_STAGE, sg.kg1 - kg);
-                    const int s = (int)(it % T::STAGES);
-                    const uint32_t ph = (uint32_t)((it / T::STAGES) & 1);
-                    if (!bar_wait(&full[s], ph, &abort_flag)) {
+                    const int sa = (int)(it % T::SA), sb = (int)(it % T::SB);
+                    if (!bar_wait(&fullA[sa], (uint32_t)((it / T::SA) & 1), &abort_flag) ||
+                        !bar_wait(&fullB[sb], (uint32_t)((it / T::SB) & 1), &abort_flag)) {
                         if (!abort_flag) fail();
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t a = s_addr(smem + (size_t)s * T::STAGE);
-                    const uint32_t b = a + T::A_BYTES;
+                    const uint32_t a = s_addr(smem + (size_t)sa * T::A_STAGE);
+                    const uint32_t b = s_addr(bring + (size_t)sb * T::B_STAGE);
                     for (int j = 0; j < nk / 2; j++) {
                         const uint32_t ao = (uint32_t)(2 * j) * plane, bo = (uint32_t)(2 * j) * T::B_KG;
                         const uint64_t ahi = cm_desc(a + ao, plane, 128u);
@@ -660,7 +712,8 @@ __global__ void __launch_bounds__(192, 1) k_hm_contract(const HUnit *__restrict_
                         if (KLO) mma_bf16(d, cm_desc(a + HA_PLANE + ao, plane, 128u), bhl, T::IDESC, 1u);
                     }
                     issued_any = true;
-                    mma_commit(&empty[s]);
+                    mma_commit(&emptyA[sa]);   // each frees its slot once these MMAs have read it
+                    mma_commit(&emptyB[sb]);
                 }
                 if (!ok) break;
                 mma_commit(&acc_full[buf]);
@@ -769,7 +822,7 @@ __device__ __forceinline__ void put_x(uint8_t *Bt, int ni, int rr, int pos, doub
 // as hi and lo
 struct HZUnit {
     uint8_t *b;                 // the instance tile's B space
-    int zkg0;                   // K-group of the unit's first row
+    const int *zdst;            // per 8-row group of the unit: its K-group in the B space
     int g, rows, p0, np, pad;
 };
 
@@ -795,7 +848,7 @@ __global__ void k_hm_zconv(const HZUnit *__restrict__ zu, const long *__restrict
             hi[k / 2] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
             lo[k / 2] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
         }
-        uint8_t *p = U.b + (size_t)(U.zkg0 + grp) * (2 * ni * 16) + (size_t)(i >> 3) * 128 + (size_t)(i & 7) * 16;
+        uint8_t *p = U.b + (size_t)U.zdst[grp] * (2 * ni * 16) + (size_t)(i >> 3) * 128 + (size_t)(i & 7) * 16;
         *reinterpret_cast<uint4 *>(p) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
         *reinterpret_cast<uint4 *>(p + (size_t)ni * 16) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
     }
@@ -1358,11 +1411,12 @@ struct EnsGeomHost {
     bool hier = false;
     struct HU {                // a unit of one pass, without its instance tile
         long a_off, lo_off, bidx_off;
-        int g, nkg, zkg0;
+        long zdst_off;         // pass 1: offset of its 8-row groups' Z destinations
+        int g, nkg;
     };
     std::vector<HU> hu1, hu2;  // pass 1 (tiles of the rank stacks), pass 2 (row leaves)
     uint8_t *hA = nullptr;
-    int *hbidx = nullptr, *hperm = nullptr, *hinv = nullptr, *hxpos = nullptr;
+    int *hbidx = nullptr, *hperm = nullptr, *hinv = nullptr, *hxpos = nullptr, *hzdst = nullptr;
     int2 *hrow = nullptr;
     int nbkg = 0, hleaves = 0;
     size_t h_img_bytes = 0, h_fp64_bytes = 0;
@@ -1441,8 +1495,12 @@ int ebad(ucg_ensemble *E, int st, const char *msg)
 //
 // The B space of one instance tile holds, K-group after K-group: X (every row
 // leaf's source columns in the permuted order, each leaf's columns rounded up
-// to 8), Z (every rank stack's rows, each block's rank rounded up to 8) and one
-// K-group of zeros that pads a unit's K range to an even number of K-groups.
+// to 8), Z (every low-rank block's rank entries rounded up to 8, the blocks
+// ordered by their receiver cluster, so that the blocks over one row leaf form
+// one run per level of the cluster tree) and one K-group of zeros that pads a
+// unit's K range to an even number of K-groups.  A row leaf's K-groups are
+// ordered by their place in the B space, which merges its B copies into few
+// long runs.
 
 // operand images, B-space maps and unit templates of a hierarchical geometry
 int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
@@ -1464,12 +1522,25 @@ int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
     for (int b = 0; b < (int)L.lr.size(); b++)
         if (L.lr[b].k > 0) stacks[{L.lr[b].s0, L.lr[b].n}].push_back(b);
     std::vector<int> zkg_b(L.lr.size(), -1);
+    auto pad8 = [](int k) { return (k + 7) & ~7; };
+    int zk = nx;
+    {
+        std::vector<int> order;
+        for (int b = 0; b < (int)L.lr.size(); b++)
+            if (L.lr[b].k > 0) order.push_back(b);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            return L.lr[x].r0 != L.lr[y].r0 ? L.lr[x].r0 < L.lr[y].r0 : L.lr[x].m > L.lr[y].m;
+        });
+        for (int b : order) {
+            zkg_b[b] = zk;
+            zk += pad8(L.lr[b].k) / 8;
+        }
+    }
+    std::vector<int> zdst;
     std::vector<HPackJob> jobs;
     std::vector<long> dst_off;   // per job: byte offset of its K-group in the images
     std::vector<int> bidx;
     long a_off = 0;
-    auto pad8 = [](int k) { return (k + 7) & ~7; };
-    int zk = nx;
     // pass 1
     for (const auto &st : stacks) {
         const int s0 = st.first.first, n = st.first.second;
@@ -1480,9 +1551,10 @@ int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
         const int kx0 = xkg0[l0], nk = xkg0[l1 + 1] - kx0, nke = nk + (nk & 1);
         std::vector<int> rowoff;
         int R = 0;
+        std::vector<int> grp_dst;   // per 8-row group of the stack: its Z K-group
         for (int b : st.second) {
             rowoff.push_back(R);
-            zkg_b[b] = zk + R / 8;
+            for (int r = 0; r < pad8(L.lr[b].k); r += 8) grp_dst.push_back(zkg_b[b] + r / 8);
             R += pad8(L.lr[b].k);
         }
         for (int t0 = 0; t0 < R; t0 += 128) {
@@ -1493,7 +1565,8 @@ int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
             u.bidx_off = (long)bidx.size();
             u.g = gg;
             u.nkg = nke;
-            u.zkg0 = zk + t0 / 8;
+            u.zdst_off = (long)zdst.size();
+            for (int q = 0; q < gg; q++) zdst.push_back(grp_dst[t0 / 8 + q]);
             for (int j = 0; j < nk; j++) bidx.push_back(kx0 + j);
             if (nk & 1) bidx.push_back(-1);   // the zero K-group, resolved below
             for (size_t bi = 0; bi < st.second.size(); bi++) {
@@ -1527,7 +1600,6 @@ int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
             g.hu1.push_back(u);
             g.h_kg1 += nke;
         }
-        zk += R / 8;
     }
     const int zero_kg = zk;
     g.nbkg = zk + 1;
@@ -1578,15 +1650,20 @@ int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
             }
         }
         const int nk = (int)kgs.size(), nke = nk + (nk & 1);
+        // the leaf's K-groups in B-space order: consecutive B K-groups become
+        // one copy (the sum's order is fixed by this, so results stay deterministic)
+        std::vector<int> ord(nk);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::sort(ord.begin(), ord.end(), [&](int x, int y) { return kgs[x] < kgs[y]; });
         EnsGeomHost::HU u;
         u.a_off = a_off;
         u.lo_off = (long)nke * gg * 128;
         u.bidx_off = (long)bidx.size();
         u.g = gg;
         u.nkg = nke;
-        u.zkg0 = -1;
+        u.zdst_off = -1;
         for (int j = 0; j < nk; j++) {
-            bidx.push_back(kgs[j]);
+            bidx.push_back(kgs[ord[j]]);
             HPackJob J;
             J.dst = nullptr;
             dst_off.push_back(a_off + (long)j * gg * 128);
@@ -1594,7 +1671,7 @@ int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
             J.stride = 1;
             J.row0 = 0;
             J.nrows = rows;
-            for (int k = 0; k < 8; k++) J.src[k] = src[j][k];
+            for (int k = 0; k < 8; k++) J.src[k] = src[ord[j]][k];
             jobs.push_back(J);
         }
         if (nk & 1) bidx.push_back(zero_kg);
@@ -1618,6 +1695,9 @@ int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
     ECUDA(cudaMalloc(&g.hA, std::max<size_t>(g.h_img_bytes, 256)));
     ECUDA(cudaMemsetAsync(g.hA, 0, std::max<size_t>(g.h_img_bytes, 256), E->stream));
     ECUDA(cudaMalloc(&g.hbidx, sizeof(int) * std::max<size_t>(bidx.size(), 1)));
+    ECUDA(cudaMalloc(&g.hzdst, sizeof(int) * std::max<size_t>(zdst.size(), 1)));
+    if (!zdst.empty())
+        ECUDA(cudaMemcpyAsync(g.hzdst, zdst.data(), sizeof(int) * zdst.size(), cudaMemcpyHostToDevice, E->stream));
     ECUDA(cudaMalloc(&g.hperm, sizeof(int) * np));
     ECUDA(cudaMalloc(&g.hinv, sizeof(int) * np));
     ECUDA(cudaMalloc(&g.hxpos, sizeof(int) * np));
@@ -1825,7 +1905,7 @@ int upload_hplan(ucg_ensemble *E, HPlanBufs &P, int ni, int pass)
                 u.rows = 8 * h.g;
                 u.pad = 0;
                 units.push_back(u);
-                if (pass == 1) zu.push_back(HZUnit{g.B + nt * bt, h.zkg0, h.g, 8 * h.g, 0, 0, 0});
+                if (pass == 1) zu.push_back(HZUnit{g.B + nt * bt, g.hzdst + h.zdst_off, h.g, 8 * h.g, 0, 0, 0});
             }
     }
     P.nunits = (int)units.size();
@@ -1892,7 +1972,7 @@ cudaError_t prepare_hcontract_t()
 template <int NI, bool KLO>
 cudaError_t launch_hpass_t(ucg_ensemble *E, const HPlanBufs &P)
 {
-    k_hm_contract<NI, KLO><<<E->sms, 192, HTile<NI, KLO>::SMEM, E->stream>>>(P.units, P.segs, P.cta, P.ws,
+    k_hm_contract<NI, KLO><<<E->sms, 224, HTile<NI, KLO>::SMEM, E->stream>>>(P.units, P.segs, P.cta, P.ws,
                                                                             &E->d_glob->err);
     E->launches++;
     return cudaGetLastError();
@@ -2339,7 +2419,7 @@ void ucg_ens_destroy(ucg_ensemble *E)
     free_plan(E);
     for (EnsGeomHost &g : E->geoms) {
         void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl, g.B, g.hA, g.hbidx, g.hperm, g.hinv,
-                        g.hxpos, g.hrow};
+                        g.hxpos, g.hrow, g.hzdst};
         for (void *p : ptrs)
             if (p) cudaFree(p);
     }
@@ -2384,7 +2464,7 @@ int ucg_ens_add_geometry(ucg_ensemble *E, ucg_ctx *c, int n_instances, int *geom
         ucg::hmatrix_layout(c, &L);
         int st = build_hgeom(E, L, g);
         if (st) {
-            void *ptrs[] = {g.hA, g.hbidx, g.hperm, g.hinv, g.hxpos, g.hrow};
+            void *ptrs[] = {g.hA, g.hbidx, g.hperm, g.hinv, g.hxpos, g.hrow, g.hzdst};
             for (void *p : ptrs)
                 if (p) cudaFree(p);
             return st;
@@ -2422,7 +2502,8 @@ int ucg_ens_add_geometry(ucg_ensemble *E, ucg_ctx *c, int n_instances, int *geom
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
     if (e != cudaSuccess) {
-        void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl, g.hA, g.hbidx, g.hperm, g.hinv, g.hxpos, g.hrow};
+        void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl, g.hA, g.hbidx, g.hperm, g.hinv, g.hxpos, g.hrow,
+                        g.hzdst};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         return efail(E, e, "ucg_ens_add_geometry");

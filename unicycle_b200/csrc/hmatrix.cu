@@ -1136,7 +1136,7 @@ bool hmatrix_layout(const ucg_ctx *c, HLayout *out)
         out->terms.push_back({h->term_poff_h[q], T.cols, T.xsel, T.xoff});
     }
     out->lr.clear();
-    for (const HLowRank &b : h->lr_h) out->lr.push_back({b.V, b.k, b.n, b.s0, b.zoff});
+    for (const HLowRank &b : h->lr_h) out->lr.push_back({b.V, b.k, b.n, b.s0, b.zoff, b.r0, b.m});
     out->panel = h->panel;
     return true;
 }

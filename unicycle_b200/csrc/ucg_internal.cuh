@@ -232,6 +232,7 @@ struct HLayout {
     struct LowRank {             // a stored low-rank block
         const double *V;         // k x n, rank-major
         int k, n, s0, zoff;      // rank, columns, first source element (permuted), z offset
+        int r0, m;               // first receiver element (permuted), rows
     };
     int np = 0, n_leaves = 0;
     std::vector<int> perm;       // permuted position -> element
