@@ -490,17 +490,21 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
 // per run of consecutive K-groups.  Rows of a unit beyond its 8-row groups are
 // read by the 128-row MMA from the stage's own buffer and land in accumulator
 // lanes that are never drained.
-constexpr int HKG_STAGE = 8;                  // K-groups per pipeline stage (four K-steps of 16)
-constexpr int HA_PLANE = HKG_STAGE * 16 * 128; // one plane of a stage for 16 row groups: 16 KB
+constexpr int HKG_STAGE = 8;                  // K-groups per anchor stage (four K-steps of 16)
 
 template <int NI, bool KLO>
 struct HTile {
     static constexpr int B_KG = 2 * NI * 16;              // hi + lo of one K-group for NI instances
     // two rings: the operand images stream from HBM and need many bytes in
     // flight; the B K-groups come from L2 and need few
-    static constexpr int A_STAGE = KLO ? 2 * HA_PLANE : HA_PLANE;
-    static constexpr int B_STAGE = HKG_STAGE * B_KG;
-    static constexpr int SB = 3;
+    // K-groups per stage: 8 for the anchor (hi and lo planes), 16 for the
+    // increments (hi planes): fewer, larger stages where the stage is cheap
+    static constexpr int KG = KLO ? HKG_STAGE : 2 * HKG_STAGE;
+    static constexpr int A_PLANE = KG * 16 * 128;          // one plane of a stage for 16 row groups
+    static constexpr int A_STAGE = KLO ? 2 * A_PLANE : A_PLANE;
+    static constexpr int B_STAGE = KG * B_KG;
+    static constexpr int SB_FIT = (208 * 1024 - A_STAGE) / B_STAGE;
+    static constexpr int SB = SB_FIT < 3 ? SB_FIT : 3;
     static constexpr int SA_FIT = (208 * 1024 - SB * B_STAGE) / A_STAGE;
     static constexpr int SA = SA_FIT < 12 ? SA_FIT : 12;
     static constexpr int SMEM = SA * A_STAGE + SB * B_STAGE + 1024;   // + 1024 for the alignment
@@ -595,8 +599,8 @@ __global__ void __launch_bounds__(224, 1) k_hm_contract(const HUnit *__restrict_
                 const HUnit U = units[sg.unit];
                 const uint32_t plane = (uint32_t)U.g * 128u;
                 bool ok = true;
-                for (int kg = sg.kg0; kg < sg.kg1; kg += HKG_STAGE) {
-                    const int nk = min(HKG_STAGE, sg.kg1 - kg);
+                for (int kg = sg.kg0; kg < sg.kg1; kg += T::KG) {
+                    const int nk = min(T::KG, sg.kg1 - kg);
                     const int s = (int)(issued % T::SA);
                     const uint32_t ph = (uint32_t)((issued / T::SA) & 1);
                     if (!bar_wait(&emptyA[s], ph ^ 1u, &abort_flag)) {
@@ -608,7 +612,7 @@ __global__ void __launch_bounds__(224, 1) k_hm_contract(const HUnit *__restrict_
                     const uint32_t abytes = (uint32_t)nk * plane;
                     bar_expect_tx(&fullA[s], (KLO ? 2u : 1u) * abytes);
                     bulk_load_hint(st, U.a + (size_t)kg * plane, abytes, &fullA[s], pol_a);
-                    if (KLO) bulk_load_hint(st + HA_PLANE, U.a + U.lo_off + (size_t)kg * plane, abytes, &fullA[s], pol_a);
+                    if (KLO) bulk_load_hint(st + T::A_PLANE, U.a + U.lo_off + (size_t)kg * plane, abytes, &fullA[s], pol_a);
                     issued++;
                 }
                 if (!ok) break;
@@ -626,18 +630,18 @@ __global__ void __launch_bounds__(224, 1) k_hm_contract(const HUnit *__restrict_
         for (int q = q0; q < q1 && !stop; q++) {
             const HSeg sg = segs[q];
             const HUnit U = units[sg.unit];
-            for (int kgb = sg.kg0; kgb < sg.kg1 && !stop; kgb += 32 * HKG_STAGE) {
-                int my[HKG_STAGE];
-                const int kgl = kgb + lane * HKG_STAGE;
+            for (int kgb = sg.kg0; kgb < sg.kg1 && !stop; kgb += 32 * T::KG) {
+                int my[T::KG];
+                const int kgl = kgb + lane * T::KG;
 #pragma unroll
-                for (int j = 0; j < HKG_STAGE; j++) my[j] = kgl + j < sg.kg1 ? __ldg(U.bidx + kgl + j) : 0;
-                const int nst = min(32, (sg.kg1 - kgb + HKG_STAGE - 1) / HKG_STAGE);
+                for (int j = 0; j < T::KG; j++) my[j] = kgl + j < sg.kg1 ? __ldg(U.bidx + kgl + j) : 0;
+                const int nst = min(32, (sg.kg1 - kgb + T::KG - 1) / T::KG);
                 for (int t = 0; t < nst; t++) {
-                    const int kg = kgb + t * HKG_STAGE;
-                    const int nk = min(HKG_STAGE, sg.kg1 - kg);
-                    int bi[HKG_STAGE];
+                    const int kg = kgb + t * T::KG;
+                    const int nk = min(T::KG, sg.kg1 - kg);
+                    int bi[T::KG];
 #pragma unroll
-                    for (int j = 0; j < HKG_STAGE; j++) bi[j] = __shfl_sync(0xffffffffu, my[j], t);
+                    for (int j = 0; j < T::KG; j++) bi[j] = __shfl_sync(0xffffffffu, my[j], t);
                     const int s = (int)(issued % T::SB);
                     const uint32_t ph = (uint32_t)((issued / T::SB) & 1);
                     int ok = 1;
@@ -653,13 +657,13 @@ __global__ void __launch_bounds__(224, 1) k_hm_contract(const HUnit *__restrict_
                         bar_expect_tx(&fullB[s], (uint32_t)nk * T::B_KG);
                         int rs = 0, bs = bi[0];
 #pragma unroll
-                        for (int j = 1; j <= HKG_STAGE; j++) {
+                        for (int j = 1; j <= T::KG; j++) {
                             if (j > nk) break;
-                            const bool cont = j < HKG_STAGE && j < nk && bi[j] == bi[j - 1] + 1;
+                            const bool cont = j < T::KG && j < nk && bi[j] == bi[j - 1] + 1;
                             if (!cont) {
                                 bulk_load_hint(bst + (size_t)rs * T::B_KG, U.b + (size_t)bs * T::B_KG,
                                                (uint32_t)(j - rs) * T::B_KG, &fullB[s], pol_b);
-                                if (j < HKG_STAGE && j < nk) {
+                                if (j < T::KG && j < nk) {
                                     rs = j;
                                     bs = bi[j];
                                 }
@@ -691,8 +695,8 @@ __global__ void __launch_bounds__(224, 1) k_hm_contract(const HUnit *__restrict_
                 tc_fence_after();
                 bool ok = true;
                 const uint32_t d = tmem + (uint32_t)(buf * 2 * NI);
-                for (int kg = sg.kg0; kg < sg.kg1; kg += HKG_STAGE, it++) {
-                    const int nk = min(HKG_STAGE, sg.kg1 - kg);
+                for (int kg = sg.kg0; kg < sg.kg1; kg += T::KG, it++) {
+                    const int nk = min(T::KG, sg.kg1 - kg);
                     const int sa = (int)(it % T::SA), sb = (int)(it % T::SB);
                     if (!bar_wait(&fullA[sa], (uint32_t)((it / T::SA) & 1), &abort_flag) ||
                         !bar_wait(&fullB[sb], (uint32_t)((it / T::SB) & 1), &abort_flag)) {
@@ -709,7 +713,7 @@ __global__ void __launch_bounds__(224, 1) k_hm_contract(const HUnit *__restrict_
                         const uint64_t bhl = cm_desc(b + bo, T::B_KG, 128u);   // hi rows, then lo rows
                         const uint32_t acc = (kg > sg.kg0 || j > 0) ? 1u : 0u;
                         mma_bf16(d, ahi, bhl, T::IDESC2, acc);
-                        if (KLO) mma_bf16(d, cm_desc(a + HA_PLANE + ao, plane, 128u), bhl, T::IDESC, 1u);
+                        if (KLO) mma_bf16(d, cm_desc(a + T::A_PLANE + ao, plane, 128u), bhl, T::IDESC, 1u);
                     }
                     issued_any = true;
                     mma_commit(&emptyA[sa]);   // each frees its slot once these MMAs have read it
