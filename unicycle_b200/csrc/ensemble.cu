@@ -1050,39 +1050,52 @@ __device__ __forceinline__ double ens_comb(const GeomDev &G, long i, double h)
     return __dadd_rn(y, __dmul_rn(h, r));
 }
 
-// stage state, velocities and the V images (ratestate.f90:667-707 per instance)
+// stage state, velocities and the V images (ratestate.f90:667-707 per instance).
+// A block holds EW_THREADS consecutive elements of one instance, whose 7-double
+// state tuples are one contiguous range: the stage state is formed over that
+// range flat (coalesced), kept in shared memory, and each thread then takes its
+// element's velocity from there.  The velocity components of the stage rate
+// are written by k_ens_rhs with the rest of the tuple.
 template <int S>
-__global__ void k_ens_prologue(const EnsArgs *__restrict__ A)
+__global__ void __launch_bounds__(EW_THREADS) k_ens_prologue(const EnsArgs *__restrict__ A)
 {
+    __shared__ double sh[7 * EW_THREADS];
     const int gi = geom_of(A, blockIdx.x, false);
     const GeomDev &G = A->g[gi];
     const int local = blockIdx.x - G.blk_e0;
     const int i = local / G.epb_e;
-    const int e = (local % G.epb_e) * EW_THREADS + threadIdx.x;
+    const int e0 = (local % G.epb_e) * EW_THREADS;
     if (i >= G.ninst) return;                        // uniform over the block
-    const bool valid = e < G.np;
+    const int ne = min(EW_THREADS, G.np - e0);
+    const int e = e0 + threadIdx.x;
+    const bool valid = threadIdx.x < ne;
     InstCtl *c = G.ctl + i;
+    const bool pend = S == 1 && c->pending;
+    const bool work = inst_live(c, A->glob) && !(S == 1 && !c->need_stage1);
+    const double h = c->h;
+    const long base = (long)i * 7 * G.np + 7L * e0;
+    for (int f = threadIdx.x; f < 7 * ne; f += EW_THREADS) {
+        const long x = base + f;
+        double v = 0.0;
+        if (S == 1) {
+            v = pend ? G.ycand[x] : G.y[x];
+            if (pend) G.y[x] = v;
+        } else if (work) {
+            v = ens_comb<S>(G, x, h);
+            G.ys[x] = v;
+            if (S == 2 && c->need_stage1) G.yscal[x] = fabs(G.y[x]) + fabs(h * G.k[0][x]) + 1.0e-30;
+        }
+        sh[f] = v;
+    }
+    __syncthreads();
     unsigned long long vkey = 0ull, tkey = ~0ull;   // max V and min log10 theta of this element (stage 1)
     if (valid) {
-        const long o = (long)i * 7 * G.np + 7L * e;
-        if (S == 1 && c->pending)
-            for (int q = 0; q < 7; q++) G.y[o + q] = G.ycand[o + q];
+        const double *yy = sh + 7 * threadIdx.x;
         double v0 = 0.0, v1 = 0.0;
-        if (inst_live(c, A->glob) && !(S == 1 && !c->need_stage1)) {
-            const double h = c->h;
-            if (S > 1) {
-                for (int q = 0; q < 7; q++) G.ys[o + q] = ens_comb<S>(G, o + q, h);
-                if (S == 2 && c->need_stage1)
-                    for (int q = 0; q < 7; q++)
-                        G.yscal[o + q] = fabs(G.y[o + q]) + fabs(h * G.k[0][o + q]) + 1.0e-30;
-            }
-            const double *yy = (S == 1) ? G.y : G.ys;
-            const double rake = atan2(yy[o + 3], yy[o + 2]);
-            const double vel = exp(yy[o + 6] * E_LG10);
+        if (work) {
+            const double rake = atan2(yy[3], yy[2]);
+            const double vel = exp(yy[6] * E_LG10);
             const double vs = vel * cos(rake), vd = vel * sin(rake);
-            double *ks = G.k[S - 1];
-            ks[o + 0] = vs;
-            ks[o + 1] = vd;
             const long pe = (long)i * G.np + e;
             v0 = vs - G.vpl_c[pe];
             v1 = vd - G.vpl_s[pe];
@@ -1092,7 +1105,7 @@ __global__ void k_ens_prologue(const EnsArgs *__restrict__ A)
             }
             if (S == 1) {
                 vkey = (unsigned long long)__double_as_longlong(vel);
-                tkey = mlp::ord_key(yy[o + 5]);
+                tkey = mlp::ord_key(yy[5]);
                 G.v1[2 * pe] = v0;
                 G.v1[2 * pe + 1] = v1;
             } else {
@@ -1120,50 +1133,93 @@ __global__ void k_ens_prologue(const EnsArgs *__restrict__ A)
     }
 }
 
-// traction rates from the contraction and the rate-state right-hand side
-// (ratestate.f90:731-776 per instance)
-template <int S>
-__global__ void k_ens_rhs(const EnsArgs *__restrict__ A)
+// the stage rate of one element (ratestate.f90:731-776) from its stage state
+// yy (7 doubles) and traction t: all 7 components into k
+__device__ __forceinline__ void ens_rate(const double *yy, const double t[3], double L, double bb, double sg,
+                                         double aa, double eta, double *k)
 {
+    const double rake = atan2(yy[3], yy[2]);
+    const double vel = exp(yy[6] * E_LG10);
+    const double cr = cos(rake), sr = sin(rake);
+    const double dth = (exp(-yy[5] * E_LG10) - vel / L) / E_LG10;
+    const double dtau = t[0] * cr + t[1] * sr;
+    const double dv = (dtau - bb * sg * dth * E_LG10) / (aa * sg + eta * vel) / E_LG10;
+    const double corr = eta * vel * dv * E_LG10;
+    k[0] = vel * cr;
+    k[1] = vel * sr;
+    k[2] = t[0] - corr * cr;
+    k[3] = t[1] - corr * sr;
+    k[4] = t[2];
+    k[5] = dth;
+    k[6] = dv;
+}
+
+// traction rates from the contraction and the rate-state right-hand side
+// (ratestate.f90:731-776 per instance).  Dense geometries stage the block's
+// contiguous state range and rate range through shared memory (coalesced);
+// a hierarchical geometry walks its elements in the permuted order, so that
+// consecutive threads read consecutive rows of a leaf's partial sums.
+template <int S>
+__global__ void __launch_bounds__(EW_THREADS) k_ens_rhs(const EnsArgs *__restrict__ A)
+{
+    __shared__ double sh[7 * EW_THREADS];
     const int gi = geom_of(A, blockIdx.x, false);
     const GeomDev &G = A->g[gi];
     const int local = blockIdx.x - G.blk_e0;
     const int i = local / G.epb_e;
-    const int el = (local % G.epb_e) * EW_THREADS + threadIdx.x;
-    if (i >= G.ninst || el >= G.np) return;
+    const int e0 = (local % G.epb_e) * EW_THREADS;
+    if (i >= G.ninst) return;                        // uniform over the block
     const InstCtl *c = G.ctl + i;
     if (!inst_live(c, A->glob) || (S == 1 && !c->need_stage1)) return;
-    // a hierarchical geometry walks its elements in the permuted order, so that
-    // consecutive threads read consecutive rows of a leaf's partial sums
-    const int e = G.hier ? G.hperm[el] : el;
-    double t[3];
-    double *t1 = G.t1 + (long)i * 3 * G.np + 3L * e;
-    for (int q = 0; q < 3; q++) {
-        const double inc = G.hier ? traction_row_h(A, G, i, el, q) : traction_row(A, G, i, 3L * e + q, S > 1);
-        if (S == 1) {
-            t1[q] = inc;
-            t[q] = inc;
-        } else {
-            t[q] = t1[q] + inc;
-        }
-    }
-    const double *yy = (S == 1) ? G.y : G.ys;
-    const long o = (long)i * 7 * G.np + 7L * e;
-    const long pe = (long)i * G.np + e;
-    const double rake = atan2(yy[o + 3], yy[o + 2]);
-    const double vel = exp(yy[o + 6] * E_LG10);
-    const double L = G.L[pe], bb = G.b[pe], sg = G.sig[pe], aa = G.a[pe], eta = G.damping[pe];
-    const double cr = cos(rake), sr = sin(rake);
-    const double dth = (exp(-yy[o + 5] * E_LG10) - vel / L) / E_LG10;
-    const double dtau = t[0] * cr + t[1] * sr;
-    const double dv = (dtau - bb * sg * dth * E_LG10) / (aa * sg + eta * vel) / E_LG10;
-    const double corr = eta * vel * dv * E_LG10;
+    const int ne = min(EW_THREADS, G.np - e0);
+    const int el = e0 + threadIdx.x;
+    const bool valid = threadIdx.x < ne;
+    const double *ysrc = (S == 1) ? G.y : G.ys;
     double *ks = G.k[S - 1];
-    ks[o + 2] = t[0] - corr * cr;
-    ks[o + 3] = t[1] - corr * sr;
-    ks[o + 4] = t[2];
-    ks[o + 5] = dth;
-    ks[o + 6] = dv;
+    if (G.hier) {
+        if (!valid) return;
+        const int e = G.hperm[el];
+        double t[3];
+        double *t1 = G.t1 + (long)i * 3 * G.np + 3L * e;
+        for (int q = 0; q < 3; q++) {
+            const double inc = traction_row_h(A, G, i, el, q);
+            if (S == 1) {
+                t1[q] = inc;
+                t[q] = inc;
+            } else {
+                t[q] = t1[q] + inc;
+            }
+        }
+        const long o = (long)i * 7 * G.np + 7L * e;
+        const long pe = (long)i * G.np + e;
+        double k[7];
+        ens_rate(ysrc + o, t, G.L[pe], G.b[pe], G.sig[pe], G.a[pe], G.damping[pe], k);
+        for (int q = 0; q < 7; q++) ks[o + q] = k[q];
+        return;
+    }
+    const long base = (long)i * 7 * G.np + 7L * e0;
+    for (int f = threadIdx.x; f < 7 * ne; f += EW_THREADS) sh[f] = ysrc[base + f];
+    __syncthreads();
+    if (valid) {
+        const int e = el;
+        double t[3];
+        double *t1 = G.t1 + (long)i * 3 * G.np + 3L * e;
+        for (int q = 0; q < 3; q++) {
+            const double inc = traction_row(A, G, i, 3L * e + q, S > 1);
+            if (S == 1) {
+                t1[q] = inc;
+                t[q] = inc;
+            } else {
+                t[q] = t1[q] + inc;
+            }
+        }
+        const long pe = (long)i * G.np + e;
+        double k[7];
+        ens_rate(sh + 7 * threadIdx.x, t, G.L[pe], G.b[pe], G.sig[pe], G.a[pe], G.damping[pe], k);
+        for (int q = 0; q < 7; q++) sh[7 * threadIdx.x + q] = k[q];   // each thread its own slots
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < 7 * ne; f += EW_THREADS) ks[base + f] = sh[f];
 }
 
 #define E_C1 (37.0 / 378.0)
