@@ -14,7 +14,9 @@ FP64 state and step control).  `value` is accepted steps/s summed over the
 instances and GPUs with the state resident in HBM (one CUDA-graph launch);
 `plain_fp64` is the same model as a single FP64 instance (ucg_run), the
 baseline of the speed-up.  --workload plain / split time the single-instance
-FP64 or split-BF16 path as the headline instead.  `e2e` is the headline metric
+FP64 or split-BF16 path as the headline instead; --workload hens the ensemble on
+the hierarchical K alone (no dense K; --nx 200 --nz 200 is N = 80k), and
+--workload hmatrix the single instance on it.  `e2e` is the headline metric
 through host arrays, state host->device and device->host every step.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload ...]
