@@ -528,13 +528,15 @@ struct HUnit {                  // one M-tile of one pass for one instance tile
     long lo_off;
     const int *bidx;            // per K-group: its K-group in the instance tile's B space
     const uint8_t *b;           // the instance tile's B space: [K-group][hi | lo][NI / 8][128 B]
+    const int *zdst;            // pass 1: per 8-row group, its Z K-group in the B space
     int g, nkg;                 // 8-row groups (1..16), K-groups (even)
     int rows;                   // rows of its partial sums (8 g)
     int pad;
 };
 struct HSeg {
-    int unit, kg0, kg1, pad;    // K-groups [kg0, kg1), both even
-    long ws;                    // float offset of its partial sums [NI][rows]
+    int unit, kg0, kg1;         // K-groups [kg0, kg1), both even
+    int direct;                 // pass 1, the unit's only segment: Z straight into the B space
+    long ws;                    // float offset of its partial sums [NI][rows] (not direct)
 };
 
 // shared-memory descriptor of a K-major operand without swizzle: K-groups `lbo`
@@ -754,17 +756,45 @@ __global__ void __launch_bounds__(224, 2) k_hm_contract(const HUnit *__restrict_
                 break;
             }
             tc_fence_after();
-            float *dst = ws + sg.ws + row;
             const uint32_t tbase = tmem + (uint32_t)(buf * 2 * NI) + ((uint32_t)(quarter * 32) << 16);
-#pragma unroll
-            for (int c0 = 0; c0 < NI; c0 += 16) {
-                uint32_t r[16], r2[16];
-                tmem_ld16(tbase + (uint32_t)c0, r);
-                tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
+            if (sg.direct) {
+                // the whole K range of a pass-1 unit: Z = the sum, split into
+                // bf16 hi and lo at its B-space slot (rank entry row, instance)
+                uint8_t *zb = nullptr;
                 if (row < rows) {
+                    const HUnit &U = units[sg.unit];
+                    zb = const_cast<uint8_t *>(U.b) + (size_t)U.zdst[row >> 3] * (2 * NI * 16) + (size_t)(row & 7) * 2;
+                }
 #pragma unroll
-                    for (int i = 0; i < 16; i++)
-                        dst[(size_t)(c0 + i) * rows] = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
+                for (int c0 = 0; c0 < NI; c0 += 16) {
+                    uint32_t r[16], r2[16];
+                    tmem_ld16(tbase + (uint32_t)c0, r);
+                    tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
+                    if (row < rows) {
+#pragma unroll
+                        for (int i = 0; i < 16; i++) {
+                            const float z = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
+                            const __nv_bfloat16 h = __float2bfloat16_rn(z);
+                            const __nv_bfloat16 l = __float2bfloat16_rn(z - __bfloat162float(h));
+                            const int inst = c0 + i;
+                            uint8_t *pz = zb + (size_t)(inst >> 3) * 128 + (size_t)(inst & 7) * 16;
+                            *reinterpret_cast<__nv_bfloat16 *>(pz) = h;
+                            *reinterpret_cast<__nv_bfloat16 *>(pz + NI * 16) = l;
+                        }
+                    }
+                }
+            } else {
+                float *dst = ws + sg.ws + row;
+#pragma unroll
+                for (int c0 = 0; c0 < NI; c0 += 16) {
+                    uint32_t r[16], r2[16];
+                    tmem_ld16(tbase + (uint32_t)c0, r);
+                    tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
+                    if (row < rows) {
+#pragma unroll
+                        for (int i = 0; i < 16; i++)
+                            dst[(size_t)(c0 + i) * rows] = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
+                    }
                 }
             }
             tc_fence_before();
@@ -828,9 +858,10 @@ __device__ __forceinline__ void put_x(uint8_t *Bt, int ni, int rr, int pos, doub
     *reinterpret_cast<__nv_bfloat162 *>(base + (size_t)ni * 16) = __halves2bfloat162(l0, l1);
 }
 
-// pass 1's output into the B space: one thread per (unit, 8-row group, instance)
-// adds the unit's partial sums in k order (FP64) and writes 8 rank entries of Z
-// as hi and lo
+// pass 1's output into the B space for the units cut into several pieces (the
+// drain writes the others directly): one thread per (unit, 8-row group,
+// instance) adds the unit's partial sums in k order (FP64) and writes 8 rank
+// entries of Z as hi and lo
 struct HZUnit {
     uint8_t *b;                 // the instance tile's B space
     const int *zdst;            // per 8-row group of the unit: its K-group in the B space
@@ -1497,8 +1528,8 @@ struct HPlanBufs {
     float *ws = nullptr;
     long *pws = nullptr;       // per piece: float offset of its partial sums
     int *p0 = nullptr, *np = nullptr, *rows = nullptr;   // per unit
-    HZUnit *zu = nullptr;      // pass 1: per unit its Z destination
-    int nunits = 0, nsegs = 0;
+    HZUnit *zu = nullptr;      // pass 1: the units cut into several pieces, their Z destinations
+    int nunits = 0, nsegs = 0, nzu = 0;
     size_t ws_floats = 0;
 };
 
@@ -1967,6 +1998,7 @@ int upload_hplan(ucg_ensemble *E, HPlanBufs &P, int ni, int pass)
                 u.lo_off = h.lo_off;
                 u.bidx = g.hbidx + h.bidx_off;
                 u.b = g.B + nt * bt;
+                u.zdst = pass == 1 ? g.hzdst + h.zdst_off : nullptr;
                 u.g = h.g;
                 u.nkg = h.nkg;
                 u.rows = 8 * h.g;
@@ -1983,20 +2015,32 @@ int upload_hplan(ucg_ensemble *E, HPlanBufs &P, int ni, int pass)
         w.push_back(u.g + 4);      // a K-step's bytes grow with the row groups; its MMAs do not
     }
     Sched s = sched_weighted(steps, w, (8 * ni <= 512 ? 2 : 1) * E->sms);   // HTile<ni, *>::CTAS per SM
-    std::vector<long> pws(std::max(1, s.nslots));
+    // partial sums for every piece, except a pass-1 unit's only one, whose
+    // drain writes Z directly
+    std::vector<long> pws(std::max(1, s.nslots), 0);
     long off = 0;
-    for (int u = 0; u < P.nunits; u++)
+    for (int u = 0; u < P.nunits; u++) {
+        if (pass == 1 && s.npieces[u] == 1) continue;
         for (int j = 0; j < s.npieces[u]; j++) {
             pws[s.piece0[u] + j] = off;
             off += (long)units[u].rows * ni;
         }
+    }
     std::vector<HSeg> segs;
-    for (const GemmSeg &q : s.segs) segs.push_back(HSeg{q.tile, 2 * q.kb0, 2 * q.kb1, 0, pws[q.slot]});
+    for (const GemmSeg &q : s.segs)
+        segs.push_back(HSeg{q.tile, 2 * q.kb0, 2 * q.kb1, pass == 1 && s.npieces[q.tile] == 1 ? 1 : 0, pws[q.slot]});
     std::vector<int> rows;
     for (const HUnit &u : units) rows.push_back(u.rows);
-    for (size_t u = 0; u < zu.size(); u++) {
-        zu[u].p0 = s.piece0[u];
-        zu[u].np = s.npieces[u];
+    {
+        std::vector<HZUnit> split;   // k_hm_zconv: the units cut into several pieces
+        for (size_t u = 0; u < zu.size(); u++)
+            if (s.npieces[u] > 1) {
+                zu[u].p0 = s.piece0[u];
+                zu[u].np = s.npieces[u];
+                split.push_back(zu[u]);
+            }
+        zu.swap(split);
+        P.nzu = (int)zu.size();
     }
     P.nsegs = (int)segs.size();
     P.ws_floats = (size_t)std::max<long>(off, 4);
@@ -2017,7 +2061,7 @@ int upload_hplan(ucg_ensemble *E, HPlanBufs &P, int ni, int pass)
     ECUDA(cudaMemcpyAsync(P.p0, s.piece0.data(), sizeof(int) * units.size(), cudaMemcpyHostToDevice, E->stream));
     ECUDA(cudaMemcpyAsync(P.np, s.npieces.data(), sizeof(int) * units.size(), cudaMemcpyHostToDevice, E->stream));
     ECUDA(cudaMemcpyAsync(P.rows, rows.data(), sizeof(int) * units.size(), cudaMemcpyHostToDevice, E->stream));
-    if (pass == 1) {
+    if (pass == 1 && !zu.empty()) {
         ECUDA(cudaMalloc(&P.zu, sizeof(HZUnit) * zu.size()));
         ECUDA(cudaMemcpyAsync(P.zu, zu.data(), sizeof(HZUnit) * zu.size(), cudaMemcpyHostToDevice, E->stream));
     }
@@ -2062,10 +2106,12 @@ cudaError_t launch_hier(ucg_ensemble *E, bool klo)
     if (E->h1.nunits > 0) {
         e = launch_hpass(E, E->h1, klo);
         if (e != cudaSuccess) return e;
-        k_hm_zconv<<<E->h1.nunits, 256, 0, E->stream>>>(E->h1.zu, E->h1.pws, E->h1.ws, E->ni);
-        E->launches++;
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
+        if (E->h1.nzu > 0) {
+            k_hm_zconv<<<E->h1.nzu, 256, 0, E->stream>>>(E->h1.zu, E->h1.pws, E->h1.ws, E->ni);
+            E->launches++;
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+        }
     }
     if (E->h2.nunits > 0) e = launch_hpass(E, E->h2, klo);
     return e;
