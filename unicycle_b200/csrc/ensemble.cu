@@ -490,7 +490,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
 // per run of consecutive K-groups.  Rows of a unit beyond its 8-row groups are
 // read by the 128-row MMA from the stage's own buffer and land in accumulator
 // lanes that are never drained.
-constexpr int HKG_STAGE = 8;                  // K-groups per anchor stage (four K-steps of 16)
+constexpr int HKG_STAGE = 8;                  // K-groups per stage (four K-steps of 16); see HTile::KG
 
 template <int NI, bool KLO>
 struct HTile {
