@@ -333,9 +333,17 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
             // producer: per k-block one copy of K per M-tile of the unit and one copy of V
             const uint64_t pol_a = l2_policy(false), pol_b = l2_policy(true);
             long issued = 0;
+            // the next segments' descriptors are loaded ahead (segment two
+            // ahead, its tile one ahead), off the copy issue's critical path
+            GemmSeg s1 = q0 < q1 ? segs[q0] : GemmSeg{0, 0, 0, 0};
+            GemmSeg s2 = q0 + 1 < q1 ? segs[q0 + 1] : s1;
+            GemmTile t1 = q0 < q1 ? tiles[s1.tile] : GemmTile{nullptr, nullptr, nullptr};
             for (int q = q0; q < q1 && !abort_flag; q++) {
-                const GemmSeg sg = segs[q];
-                const GemmTile tl = tiles[sg.tile];
+                const GemmSeg sg = s1;
+                const GemmTile tl = t1;
+                s1 = s2;
+                if (q + 1 < q1) t1 = tiles[s1.tile];
+                if (q + 2 < q1) s2 = segs[q + 2];
                 const bool two = MT == 2 && tl.a1 != nullptr;
                 const uint32_t bytes = (uint32_t)((two ? 2 : 1) * T::A_BYTES + T::B_IMG);
                 for (int kb = sg.kb0; kb < sg.kb1; kb++) {
@@ -603,10 +611,29 @@ __global__ void __launch_bounds__(224, 2) k_hm_contract(const HUnit *__restrict_
             // operand images: the unit's hi (and lo) planes of the stage's K-groups
             const uint64_t pol_a = l2_policy(false);
             long issued = 0;
+            // descriptors loaded ahead: the segment two ahead, its unit one ahead
+            HSeg s1 = q0 < q1 ? segs[q0] : HSeg{0, 0, 0, 0, 0};
+            HSeg s2 = q0 + 1 < q1 ? segs[q0 + 1] : s1;
+            const uint8_t *a1 = nullptr;
+            long lo1 = 0;
+            int g1 = 1;
+            if (q0 < q1) {
+                a1 = units[s1.unit].a;
+                lo1 = units[s1.unit].lo_off;
+                g1 = units[s1.unit].g;
+            }
             for (int q = q0; q < q1 && !abort_flag; q++) {
-                const HSeg sg = segs[q];
-                const HUnit U = units[sg.unit];
-                const uint32_t plane = (uint32_t)U.g * 128u;
+                const HSeg sg = s1;
+                const uint8_t *ua = a1;
+                const long ulo = lo1;
+                const uint32_t plane = (uint32_t)g1 * 128u;
+                s1 = s2;
+                if (q + 1 < q1) {
+                    a1 = units[s1.unit].a;
+                    lo1 = units[s1.unit].lo_off;
+                    g1 = units[s1.unit].g;
+                }
+                if (q + 2 < q1) s2 = segs[q + 2];
                 bool ok = true;
                 for (int kg = sg.kg0; kg < sg.kg1; kg += T::KG) {
                     const int nk = min(T::KG, sg.kg1 - kg);
@@ -620,8 +647,8 @@ __global__ void __launch_bounds__(224, 2) k_hm_contract(const HUnit *__restrict_
                     uint8_t *st = smem + (size_t)s * T::A_STAGE;
                     const uint32_t abytes = (uint32_t)nk * plane;
                     bar_expect_tx(&fullA[s], (KLO ? 2u : 1u) * abytes);
-                    bulk_load_hint(st, U.a + (size_t)kg * plane, abytes, &fullA[s], pol_a);
-                    if (KLO) bulk_load_hint(st + T::A_PLANE, U.a + U.lo_off + (size_t)kg * plane, abytes, &fullA[s], pol_a);
+                    bulk_load_hint(st, ua + (size_t)kg * plane, abytes, &fullA[s], pol_a);
+                    if (KLO) bulk_load_hint(st + T::A_PLANE, ua + ulo + (size_t)kg * plane, abytes, &fullA[s], pol_a);
                     issued++;
                 }
                 if (!ok) break;
@@ -636,14 +663,30 @@ __global__ void __launch_bounds__(224, 2) k_hm_contract(const HUnit *__restrict_
         const uint64_t pol_b = l2_policy(true);
         long issued = 0;
         bool stop = false;
+        // descriptors loaded ahead: the segment two ahead, its unit one ahead
+        HSeg s1 = q0 < q1 ? segs[q0] : HSeg{0, 0, 0, 0, 0};
+        HSeg s2 = q0 + 1 < q1 ? segs[q0 + 1] : s1;
+        const int *x1 = nullptr;
+        const uint8_t *b1 = nullptr;
+        if (q0 < q1) {
+            x1 = units[s1.unit].bidx;
+            b1 = units[s1.unit].b;
+        }
         for (int q = q0; q < q1 && !stop; q++) {
-            const HSeg sg = segs[q];
-            const HUnit U = units[sg.unit];
+            const HSeg sg = s1;
+            const int *ubidx = x1;
+            const uint8_t *ub = b1;
+            s1 = s2;
+            if (q + 1 < q1) {
+                x1 = units[s1.unit].bidx;
+                b1 = units[s1.unit].b;
+            }
+            if (q + 2 < q1) s2 = segs[q + 2];
             for (int kgb = sg.kg0; kgb < sg.kg1 && !stop; kgb += 32 * T::KG) {
                 int my[T::KG];
                 const int kgl = kgb + lane * T::KG;
 #pragma unroll
-                for (int j = 0; j < T::KG; j++) my[j] = kgl + j < sg.kg1 ? __ldg(U.bidx + kgl + j) : 0;
+                for (int j = 0; j < T::KG; j++) my[j] = kgl + j < sg.kg1 ? __ldg(ubidx + kgl + j) : 0;
                 const int nst = min(32, (sg.kg1 - kgb + T::KG - 1) / T::KG);
                 for (int t = 0; t < nst; t++) {
                     const int kg = kgb + t * T::KG;
@@ -670,7 +713,7 @@ __global__ void __launch_bounds__(224, 2) k_hm_contract(const HUnit *__restrict_
                             if (j > nk) break;
                             const bool cont = j < T::KG && j < nk && bi[j] == bi[j - 1] + 1;
                             if (!cont) {
-                                bulk_load_hint(bst + (size_t)rs * T::B_KG, U.b + (size_t)bs * T::B_KG,
+                                bulk_load_hint(bst + (size_t)rs * T::B_KG, ub + (size_t)bs * T::B_KG,
                                                (uint32_t)(j - rs) * T::B_KG, &fullB[s], pol_b);
                                 if (j < T::KG && j < nk) {
                                     rs = j;
@@ -1965,6 +2008,32 @@ Sched sched_weighted(const std::vector<int> &steps, const std::vector<int> &w, i
     return s;
 }
 
+// every segment cut, within its CTA, into pieces of at most SEG_MAX_KB k-blocks:
+// one FP32 tensor-memory accumulator then sums at most 64 SEG_MAX_KB products
+// (16,384 sources), whatever N, and the pieces are added in FP64 by the stage
+// epilogue, which bounds the accumulation error of the contraction.  Measured
+// at N = 20k x 64 (max |T - K V| / (|K| |V|) on 768 rows, ms per attempt): no
+// cap 8.9e-5 / 5.95, 256 k-blocks 4.8e-5 / 6.07, 128 k-blocks 3.1e-5 / 6.21
+constexpr int SEG_MAX_KB = 256;
+
+void cap_segments(Sched &s, int ntiles, int cap = SEG_MAX_KB)
+{
+    std::vector<GemmSeg> segs;
+    std::vector<int> cta(s.cta.size(), 0);
+    for (size_t c = 0; c + 1 < s.cta.size(); c++) {
+        cta[c] = (int)segs.size();
+        for (int q = s.cta[c]; q < s.cta[c + 1]; q++) {
+            const GemmSeg g = s.segs[q];
+            for (int k = g.kb0; k < g.kb1; k += cap)
+                segs.push_back(GemmSeg{g.tile, k, std::min(g.kb1, k + cap), 0});
+        }
+    }
+    cta.back() = (int)segs.size();
+    s.segs.swap(segs);
+    s.cta.swap(cta);
+    number_pieces(s, ntiles);
+}
+
 size_t b_bytes(const EnsGeomHost &g, int ni)
 {
     const int ntl = (g.ninst + ni - 1) / ni;
@@ -2015,6 +2084,7 @@ int upload_hplan(ucg_ensemble *E, HPlanBufs &P, int ni, int pass)
         w.push_back(u.g + 4);      // a K-step's bytes grow with the row groups; its MMAs do not
     }
     Sched s = sched_weighted(steps, w, (8 * ni <= 512 ? 2 : 1) * E->sms);   // HTile<ni, *>::CTAS per SM
+    cap_segments(s, P.nunits, 512);   // 1,024 K-groups = 8,192 K entries per FP32 partial sum
     // partial sums for every piece, except a pass-1 unit's only one, whose
     // drain writes Z directly
     std::vector<long> pws(std::max(1, s.nslots), 0);
@@ -2365,10 +2435,13 @@ int default_ni(ucg_ensemble *E)
 }
 
 // the schedule of a kind for the single-tile (mt 1) or paired (mt 2) units
+
 Sched make_sched(ucg_ensemble *E, int ni, int mt, int kind, int chunk)
 {
     const std::vector<int> tkb = unit_kblocks(E, ni, mt);
-    return kind == UCG_ENS_STREAM_K ? sched_stream_k(tkb, E->sms) : sched_split_lpt(tkb, E->sms, chunk, 2);
+    Sched s = kind == UCG_ENS_STREAM_K ? sched_stream_k(tkb, E->sms) : sched_split_lpt(tkb, E->sms, chunk, 2);
+    cap_segments(s, (int)tkb.size());
+    return s;
 }
 
 int ensure_plan(ucg_ensemble *E)
