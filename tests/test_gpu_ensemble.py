@@ -266,3 +266,32 @@ def test_host_launched_attempts_match_graph(ucg):
     b.close()
     for s in sims:
         s.close()
+
+
+def test_contraction_long_k_range(ucg):
+    """A fault of 8,448 rectangles (16,896 sources = 264 k-blocks of 64 per
+    tile): every plan cuts its segments to at most 256 k-blocks, so one FP32
+    accumulator never sums more than 16,384 products; both forms against FP64
+    on the first 768 rows of K, determinism of each plan."""
+    from unicycle_b200 import _lib, configs
+    c = configs.cfg1(nx=128, nz=66)
+    sim = ucg.Simulation(c["mu"], c["lam"])
+    sim.set_rectangles(*c["mesh"]["rect"])
+    sim.buildG()
+    ninst = 64
+    ens = ucg.Ensemble()
+    ens.add_geometry(sim, ninst)
+    Kr = sim.copy_G(0, 768)
+    rng = np.random.default_rng(9)
+    V = rng.standard_normal((ninst, Kr.shape[1])) * 1e-9
+    mag = np.abs(V) @ np.abs(Kr).T
+    for plan in [(64, _lib.UCG_ENS_STREAM_K, 0), (64, _lib.UCG_ENS_SPLIT_LPT, 0), (32, _lib.UCG_ENS_STREAM_K, 0)]:
+        ens.plan(*plan)
+        T = ens.matvec(0, V)
+        assert np.array_equal(T, ens.matvec(0, V)), plan
+        r3 = np.max(np.abs(T[:, :768] - V @ Kr.T) / mag)
+        r2 = np.max(np.abs(ens.matvec(0, V, terms=2)[:, :768] - V @ Kr.T) / mag)
+        print(plan, f"anchor {r3:.2e}, increment form {r2:.2e}")
+        assert r3 < BOUND and r2 < 5e-3, plan
+    ens.close()
+    sim.close()
