@@ -75,7 +75,9 @@ constexpr int A_HALF = BM * BK * 2;     // one bf16 image of a tile k-block: 16 
 constexpr int A_IMG = 2 * A_HALF;       // hi + lo
 constexpr int MAX_GEOM = 16;
 constexpr int EW_THREADS = 128;         // element-wise kernels: elements per block
-constexpr int ST_THREADS = 256;         // finish kernel: state entries per block
+constexpr int ST_THREADS = 256;         // finish / commit kernels: threads per block
+constexpr int ST_PER = 4;               // state entries per thread (independent loads in flight)
+constexpr int ST_SPAN = ST_THREADS * ST_PER;
 constexpr unsigned long long TIMEOUT_NS = 4000000000ull;
 
 // KLO: the stage also reads the K lo image (three MMAs per k-step); without it
@@ -1155,7 +1157,10 @@ __global__ void __launch_bounds__(EW_THREADS) k_ens_prologue(const EnsArgs *__re
     const bool work = inst_live(c, A->glob) && !(S == 1 && !c->need_stage1);
     const double h = c->h;
     const long base = (long)i * 7 * G.np + 7L * e0;
-    for (int f = threadIdx.x; f < 7 * ne; f += EW_THREADS) {
+#pragma unroll
+    for (int u = 0; u < 7; u++) {
+        const int f = threadIdx.x + u * EW_THREADS;
+        if (f >= 7 * ne) break;
         const long x = base + f;
         double v = 0.0;
         if (S == 1) {
@@ -1279,7 +1284,11 @@ __global__ void __launch_bounds__(EW_THREADS) k_ens_rhs(const EnsArgs *__restric
         return;
     }
     const long base = (long)i * 7 * G.np + 7L * e0;
-    for (int f = threadIdx.x; f < 7 * ne; f += EW_THREADS) sh[f] = ysrc[base + f];
+#pragma unroll
+    for (int u = 0; u < 7; u++) {
+        const int f = threadIdx.x + u * EW_THREADS;
+        if (f < 7 * ne) sh[f] = ysrc[base + f];
+    }
     __syncthreads();
     if (valid) {
         const int e = el;
@@ -1300,7 +1309,11 @@ __global__ void __launch_bounds__(EW_THREADS) k_ens_rhs(const EnsArgs *__restric
         for (int q = 0; q < 7; q++) sh[7 * threadIdx.x + q] = k[q];   // each thread its own slots
     }
     __syncthreads();
-    for (int f = threadIdx.x; f < 7 * ne; f += EW_THREADS) ks[base + f] = sh[f];
+#pragma unroll
+    for (int u = 0; u < 7; u++) {
+        const int f = threadIdx.x + u * EW_THREADS;
+        if (f < 7 * ne) ks[base + f] = sh[f];
+    }
 }
 
 #define E_C1 (37.0 / 378.0)
@@ -1324,28 +1337,32 @@ __global__ void k_ens_finish(const EnsArgs *__restrict__ A)
     InstCtl *c = G.ctl + i;
     if (!inst_live(c, A->glob)) return;        // uniform over the block
     const long len = 7L * G.np;
-    const long j = (long)(local % G.epb_s) * ST_THREADS + threadIdx.x;
+    const long j0 = (long)(local % G.epb_s) * ST_SPAN + threadIdx.x;
     const double h = c->h;
     double mx = 0.0;
     bool bad = false;
-    if (j < len) {
-        const long x = (long)i * len + j;
-        const double k1 = G.k[0][x], k3 = G.k[2][x], k4 = G.k[3][x], k5 = G.k[4][x], k6 = G.k[5][x];
-        double r = __dmul_rn(E_C1, k1);
-        r = __dadd_rn(r, __dmul_rn(E_C3, k3));
-        r = __dadd_rn(r, __dmul_rn(E_C4, k4));
-        r = __dadd_rn(r, __dmul_rn(E_C6, k6));
-        const double yc = __dadd_rn(G.y[x], __dmul_rn(h, r));
-        double er = __dmul_rn(E_DC1, k1);
-        er = __dadd_rn(er, __dmul_rn(E_DC3, k3));
-        er = __dadd_rn(er, __dmul_rn(E_DC4, k4));
-        er = __dadd_rn(er, __dmul_rn(E_DC5, k5));
-        er = __dadd_rn(er, __dmul_rn(E_DC6, k6));
-        er = __dmul_rn(h, er);
-        G.ycand[x] = yc;
-        G.yerr[x] = er;
-        mx = fmax(0.0, fabs(er / G.yscal[x]));
-        bad = !isfinite(yc);
+#pragma unroll
+    for (int u = 0; u < ST_PER; u++) {
+        const long j = j0 + (long)u * ST_THREADS;
+        if (j < len) {
+            const long x = (long)i * len + j;
+            const double k1 = G.k[0][x], k3 = G.k[2][x], k4 = G.k[3][x], k5 = G.k[4][x], k6 = G.k[5][x];
+            double r = __dmul_rn(E_C1, k1);
+            r = __dadd_rn(r, __dmul_rn(E_C3, k3));
+            r = __dadd_rn(r, __dmul_rn(E_C4, k4));
+            r = __dadd_rn(r, __dmul_rn(E_C6, k6));
+            const double yc = __dadd_rn(G.y[x], __dmul_rn(h, r));
+            double er = __dmul_rn(E_DC1, k1);
+            er = __dadd_rn(er, __dmul_rn(E_DC3, k3));
+            er = __dadd_rn(er, __dmul_rn(E_DC4, k4));
+            er = __dadd_rn(er, __dmul_rn(E_DC5, k5));
+            er = __dadd_rn(er, __dmul_rn(E_DC6, k6));
+            er = __dmul_rn(h, er);
+            G.ycand[x] = yc;
+            G.yerr[x] = er;
+            mx = fmax(mx, fabs(er / G.yscal[x]));
+            bad = bad || !isfinite(yc);
+        }
     }
     for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
     bad = __any_sync(0xffffffffu, bad);
@@ -1515,8 +1532,12 @@ __global__ void k_ens_commit(const EnsArgs *__restrict__ A)
     const int i = local / G.epb_s;
     if (i >= G.ninst || !G.ctl[i].pending) return;
     const long len = 7L * G.np;
-    const long j = (long)(local % G.epb_s) * ST_THREADS + threadIdx.x;
-    if (j < len) G.y[(long)i * len + j] = G.ycand[(long)i * len + j];
+    const long j0 = (long)(local % G.epb_s) * ST_SPAN + threadIdx.x;
+#pragma unroll
+    for (int u = 0; u < ST_PER; u++) {
+        const long j = j0 + (long)u * ST_THREADS;
+        if (j < len) G.y[(long)i * len + j] = G.ycand[(long)i * len + j];
+    }
 }
 
 __global__ void k_ens_clear_pending(const EnsArgs *__restrict__ A)
@@ -2376,7 +2397,7 @@ int install_plan(ucg_ensemble *E, int ni, const Sched &s1, const Sched &s2)
         d.epb_e = (g.np + EW_THREADS - 1) / EW_THREADS;
         d.blk_e0 = be;
         be += d.epb_e * g.ninst;
-        d.epb_s = (int)((7L * g.np + ST_THREADS - 1) / ST_THREADS);
+        d.epb_s = (int)((7L * g.np + ST_SPAN - 1) / ST_SPAN);
         d.blk_s0 = bs;
         bs += d.epb_s * g.ninst;
         d.B = g.B;
@@ -2497,7 +2518,7 @@ int build_graph(ucg_ensemble *E)
     int be = 0, bs = 0;
     for (const EnsGeomHost &g : E->geoms) {
         be += g.ninst * ((g.np + EW_THREADS - 1) / EW_THREADS);
-        bs += g.ninst * (int)((7L * g.np + ST_THREADS - 1) / ST_THREADS);
+        bs += g.ninst * (int)((7L * g.np + ST_SPAN - 1) / ST_SPAN);
     }
     cudaGraph_t g;
     ECUDA(cudaGraphCreate(&g, 0));
@@ -2946,7 +2967,7 @@ int run_eager(ucg_ensemble *E)
     int be = 0, bs = 0;
     for (const EnsGeomHost &g : E->geoms) {
         be += g.ninst * ((g.np + EW_THREADS - 1) / EW_THREADS);
-        bs += g.ninst * (int)((7L * g.np + ST_THREADS - 1) / ST_THREADS);
+        bs += g.ninst * (int)((7L * g.np + ST_SPAN - 1) / ST_SPAN);
     }
     k_ens_begin<<<1, 256, 0, E->stream>>>(E->d_args);
     E->launches++;
