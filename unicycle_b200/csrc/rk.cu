@@ -328,15 +328,32 @@ __device__ __forceinline__ void tm_load_v<double>(const double *v, long c, long 
     (void)n;
     vr.x = *reinterpret_cast<const double2 *>(v + c);
 }
+// c is a multiple of the values per thread (4 or 8), so away from the ragged
+// end the thread's values are 16-byte aligned pairs
 template <>
 __device__ __forceinline__ void tm_load_v<__nv_bfloat162>(const double *v, long c, long n, TmV<__nv_bfloat162> &vr)
 {
+    if (c + 4 <= n) {
+        const double2 a = __ldg(reinterpret_cast<const double2 *>(v + c));
+        const double2 b = __ldg(reinterpret_cast<const double2 *>(v + c + 2));
+        vr.x[0] = (float)a.x; vr.x[1] = (float)a.y; vr.x[2] = (float)b.x; vr.x[3] = (float)b.y;
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < 4; q++) vr.x[q] = (c + q < n) ? (float)v[c + q] : 0.0f;
 }
 template <>
 __device__ __forceinline__ void tm_load_v<__nv_bfloat16>(const double *v, long c, long n, TmV<__nv_bfloat16> &vr)
 {
+    if (c + 8 <= n) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const double2 a = __ldg(reinterpret_cast<const double2 *>(v + c + 2 * q));
+            vr.x[2 * q] = (float)a.x;
+            vr.x[2 * q + 1] = (float)a.y;
+        }
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < 8; q++) vr.x[q] = (c + q < n) ? (float)v[c + q] : 0.0f;
 }
@@ -387,7 +404,11 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
     extern __shared__ __align__(128) unsigned char tm_smem[];
     KT *stage = reinterpret_cast<KT *>(tm_smem);
     __shared__ __align__(8) uint64_t full[TM_STAGES], empty[TM_STAGES];
-    __shared__ double red[MV_WARPS][MV_ROWS];
+    // row sums of a block, double-buffered: the few threads that run a
+    // block's epilogue read one buffer while the other warps already
+    // accumulate the next block into the other; the next block's barrier
+    // orders the epilogue before its buffer comes round again
+    __shared__ double red[2][MV_WARPS][MV_ROWS];
     __shared__ int abort_flag;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nblk = pblocks + vblocks;
@@ -444,7 +465,8 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
     double *ks = a.k[S - 1];
     long item = 0;
     const int t = threadIdx.x;
-    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    int rb = 0;
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x, rb ^= 1) {
         long row0; int nrows, e0, nel; bool patch;
         block_rows(blk, row0, nrows, e0, nel, patch);
         Acc acc[MV_ROWS];
@@ -455,17 +477,18 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
             const uint32_t ph = (uint32_t)((item / TM_STAGES) & 1);
             // on a timed-out wait every consumer keeps walking the same item
             // sequence without computing, so all of them reach each named barrier
+            // v does not depend on the stage: its loads are in flight during the wait
+            const int cl = PER * t;
+            const long c = ch * CH + cl;
+            TmV<KT> vr;
+            if (c < n) tm_load_v<KT>(a.v, c, n, vr);
             const bool ready = !abort_flag && mbar_wait(&full[s], ph, &abort_flag);
             if (!ready && !abort_flag) {
                 abort_flag = 1;
                 ctl->status = UCG_E_TIMEOUT;
             }
             const KT *src = stage + (size_t)s * MV_ROWS * CH;
-            const int cl = PER * t;
-            const long c = ch * CH + cl;
             if (ready && c < n) {
-                TmV<KT> vr;
-                tm_load_v<KT>(a.v, c, n, vr);
 #pragma unroll
                 for (int r = 0; r < MV_ROWS; r++)
                     if (r < nrows) tm_accumulate<KT>(src + (size_t)r * CH, cl, vr, acc[r]);
@@ -483,7 +506,7 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
         }
         if (lane == 0) {
 #pragma unroll
-            for (int r = 0; r < MV_ROWS; r++) red[warp][r] = rs[r];
+            for (int r = 0; r < MV_ROWS; r++) red[rb][warp][r] = rs[r];
         }
         consumer_sync();
         if (t < nel && !abort_flag) {
@@ -492,7 +515,7 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
                 double tr[3];
                 for (int c3 = 0; c3 < 3; c3++) {
                     double sum = 0.0;
-                    for (int w = 0; w < MV_WARPS; w++) sum += red[w][3 * q + c3];
+                    for (int w = 0; w < MV_WARPS; w++) sum += red[rb][w][3 * q + c3];
                     tr[c3] = scale ? sum * (double)scale[row0 + 3 * q + c3] : sum;
                     if (a.anchored) {
                         const long row = row0 + 3 * q + c3;
@@ -505,7 +528,7 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
                 const long o = 7L * a.np + 12L * (e0 + q);
                 for (int c6 = 0; c6 < 6; c6++) {
                     double sum = 0.0;
-                    for (int w = 0; w < MV_WARPS; w++) sum += red[w][6 * q + c6];
+                    for (int w = 0; w < MV_WARPS; w++) sum += red[rb][w][6 * q + c6];
                     double sv = scale ? sum * (double)scale[row0 + 6 * q + c6] : sum;
                     if (a.anchored) {
                         const long row = row0 + 6 * q + c6;
@@ -516,7 +539,6 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
                 }
             }
         }
-        consumer_sync();
     }
 }
 
