@@ -171,16 +171,15 @@ __global__ void k_prologue(StageArgs a, Ctl *ctl)
 
 // ---- traction product fused with the right-hand side ----------------------------
 //
-// K (m x n, row-major) times v.  A CTA owns 12 consecutive rows: 4 patches
-// (3 rows each) or 2 volumes (6 rows each).  Its 8 warps sweep interleaved
-// 64-column slices of those 12 rows, so every v element loaded feeds 12 K
-// elements; K is streamed once with 16-byte non-allocating loads.  The 12 row
+// K (m x n, row-major) times v.  A CTA owns blocks of consecutive rows: in FP64
+// 12 rows, 4 patches (3 rows each) or 2 volumes (6 rows each); in the split
+// forms 24.  Its 8 warps sweep interleaved column slices of a block's rows, so
+// every v element loaded feeds all of them; K is streamed once.  The row
 // sums are reduced across lanes and warps, and the elementwise rate-state
 // (ratestate.f90:731-776) or Maxwell (viscouscycles.f90:1072-1080) epilogue of
 // each owned element runs on the reduced values, writing k_s directly.
 
 constexpr int MV_WARPS = 8;
-constexpr int MV_ROWS = 12;
 
 __device__ __forceinline__ double2 ld_stream(const double *p)
 {
@@ -232,9 +231,10 @@ __global__ void k_rhs_t(StageArgs a, const Ctl *ctl, const double *__restrict__ 
 // ---- TMA bulk-copy pipeline ------------------------------------------------------
 //
 // The traction product streams K once per stage evaluation and is bound by HBM
-// bandwidth.  Each persistent CTA (one per SM) owns a sequence of 12-row blocks;
+// bandwidth.  Each persistent CTA (one per SM) owns a sequence of row blocks;
 // a producer warp moves K into shared memory with cp.async.bulk row copies
-// (48 KB per stage, 4 stages in flight, completion counted on mbarriers) while
+// (192 KB in flight: 4 stages of 48 KB in FP64, 2 of 96 KB in the split forms;
+// completion counted on mbarriers) while
 // 8 consumer warps multiply by v and hand the stage back.  Consumer thread
 // t = 32 w + l accumulates columns c = CH k + PER t .. (PER per thread) across
 // chunks, so the per-row summation order is: per-thread fused multiply-adds
@@ -244,8 +244,6 @@ __global__ void k_rhs_t(StageArgs a, const Ctl *ctl, const double *__restrict__ 
 // Every mbarrier wait is bounded (about 4 s of %globaltimer); a wait that runs
 // out records UCG_E_TIMEOUT in the control block and the CTA stops.
 
-constexpr int TM_STAGES = 4;
-constexpr int TM_STAGE_BYTES = MV_ROWS * 512 * 8;   // 48 KB
 constexpr unsigned long long TM_TIMEOUT_NS = 4000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -300,18 +298,27 @@ __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 256;
 
 // element traits: FP64 K (2 columns per thread) or split-BF16 pairs (4 per thread)
 template <class KT> struct TmTraits;
+// ROWS per block: 12 (4 patches or 2 volumes) in FP64; the split forms take
+// 24 rows (8 patches or 4 volumes) in two 96 KB stages, which halves the
+// per-block reduction and epilogue per K byte where a chunk holds 2-4 times
+// more columns
 template <> struct TmTraits<double> {
-    static constexpr int PER = 2, CH = 512;
+    static constexpr int PER = 2, CH = 512, ROWS = 12, STAGES = 4;
     using Acc = double;
 };
 template <> struct TmTraits<__nv_bfloat162> {
-    static constexpr int PER = 4, CH = 1024;
+    static constexpr int PER = 4, CH = 1024, ROWS = 24, STAGES = 2;
     using Acc = float;
 };
 template <> struct TmTraits<__nv_bfloat16> {   // the hi plane alone (anchored stages 2-6)
-    static constexpr int PER = 8, CH = 2048;
+    static constexpr int PER = 8, CH = 2048, ROWS = 24, STAGES = 2;
     using Acc = float;
 };
+template <class KT>
+constexpr size_t tm_smem_bytes()
+{
+    return (size_t)TmTraits<KT>::STAGES * TmTraits<KT>::ROWS * TmTraits<KT>::CH * sizeof(KT);
+}
 
 // the thread's PER values of v for one chunk, loaded once and used for all the
 // rows of the stage; then one row's contribution
@@ -398,23 +405,24 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
 {
     using Tr = TmTraits<KT>;
     using Acc = typename Tr::Acc;
-    constexpr int CH = Tr::CH, PER = Tr::PER;
+    constexpr int CH = Tr::CH, PER = Tr::PER, ROWS = Tr::ROWS, STAGES = Tr::STAGES;
+    constexpr int PB = ROWS / 3, VB = ROWS / 6;   // patches, volumes per block
     if (!ctl_live(ctl)) return;
     if (S == 1 && !ctl->need_stage1) return;
     extern __shared__ __align__(128) unsigned char tm_smem[];
     KT *stage = reinterpret_cast<KT *>(tm_smem);
-    __shared__ __align__(8) uint64_t full[TM_STAGES], empty[TM_STAGES];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
     // row sums of a block, double-buffered: the few threads that run a
     // block's epilogue read one buffer while the other warps already
     // accumulate the next block into the other; the next block's barrier
     // orders the epilogue before its buffer comes round again
-    __shared__ double red[2][MV_WARPS][MV_ROWS];
+    __shared__ double red[2][MV_WARPS][ROWS];
     __shared__ int abort_flag;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nblk = pblocks + vblocks;
     const long nch = (n + CH - 1) / CH;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < TM_STAGES; s++) {
+        for (int s = 0; s < STAGES; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], MV_WARPS);
         }
@@ -426,9 +434,9 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
     auto block_rows = [&](int blk, long &row0, int &nrows, int &e0, int &nel, bool &patch) {
         patch = blk < pblocks;
         if (patch) {
-            e0 = blk * 4; nel = min(4, a.np - e0); row0 = 3L * e0; nrows = 3 * nel;
+            e0 = blk * PB; nel = min(PB, a.np - e0); row0 = 3L * e0; nrows = 3 * nel;
         } else {
-            e0 = (blk - pblocks) * 2; nel = min(2, a.nvol - e0); row0 = 3L * a.np + 6L * e0; nrows = 6 * nel;
+            e0 = (blk - pblocks) * VB; nel = min(VB, a.nvol - e0); row0 = 3L * a.np + 6L * e0; nrows = 6 * nel;
         }
     };
 
@@ -440,8 +448,8 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
                 long row0; int nrows, e0, nel; bool patch;
                 block_rows(blk, row0, nrows, e0, nel, patch);
                 for (long ch = 0; ch < nch; ch++, item++) {
-                    const int s = (int)(item % TM_STAGES);
-                    const uint32_t ph = (uint32_t)((item / TM_STAGES) & 1);
+                    const int s = (int)(item % STAGES);
+                    const uint32_t ph = (uint32_t)((item / STAGES) & 1);
                     if (!mbar_wait(&empty[s], ph ^ 1u, &abort_flag)) {
                         abort_flag = 1;
                         ctl->status = UCG_E_TIMEOUT;
@@ -451,7 +459,7 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
                     const long w = min((long)CH, ldk - c0);
                     const uint32_t rowbytes = (uint32_t)(w * sizeof(KT));
                     mbar_expect_tx(&full[s], rowbytes * nrows);
-                    KT *dst = stage + (size_t)s * MV_ROWS * CH;
+                    KT *dst = stage + (size_t)s * ROWS * CH;
                     for (int r = 0; r < nrows; r++)
                         bulk_g2s(dst + (size_t)r * CH, K + (row0 + r) * ldk + c0, rowbytes, &full[s]);
                 }
@@ -469,12 +477,12 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x, rb ^= 1) {
         long row0; int nrows, e0, nel; bool patch;
         block_rows(blk, row0, nrows, e0, nel, patch);
-        Acc acc[MV_ROWS];
+        Acc acc[ROWS];
 #pragma unroll
-        for (int r = 0; r < MV_ROWS; r++) acc[r] = Acc(0);
+        for (int r = 0; r < ROWS; r++) acc[r] = Acc(0);
         for (long ch = 0; ch < nch; ch++, item++) {
-            const int s = (int)(item % TM_STAGES);
-            const uint32_t ph = (uint32_t)((item / TM_STAGES) & 1);
+            const int s = (int)(item % STAGES);
+            const uint32_t ph = (uint32_t)((item / STAGES) & 1);
             // on a timed-out wait every consumer keeps walking the same item
             // sequence without computing, so all of them reach each named barrier
             // v does not depend on the stage: its loads are in flight during the wait
@@ -487,18 +495,18 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
                 abort_flag = 1;
                 ctl->status = UCG_E_TIMEOUT;
             }
-            const KT *src = stage + (size_t)s * MV_ROWS * CH;
+            const KT *src = stage + (size_t)s * ROWS * CH;
             if (ready && c < n) {
 #pragma unroll
-                for (int r = 0; r < MV_ROWS; r++)
+                for (int r = 0; r < ROWS; r++)
                     if (r < nrows) tm_accumulate<KT>(src + (size_t)r * CH, cl, vr, acc[r]);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
         }
-        double rs[MV_ROWS];
+        double rs[ROWS];
 #pragma unroll
-        for (int r = 0; r < MV_ROWS; r++) {
+        for (int r = 0; r < ROWS; r++) {
             Acc x = acc[r];
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
@@ -506,7 +514,7 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
         }
         if (lane == 0) {
 #pragma unroll
-            for (int r = 0; r < MV_ROWS; r++) red[rb][warp][r] = rs[r];
+            for (int r = 0; r < ROWS; r++) red[rb][warp][r] = rs[r];
         }
         consumer_sync();
         if (t < nel && !abort_flag) {
@@ -786,35 +794,41 @@ void rk_free(ucg_ctx *c)
     c->attempt_graph = nullptr;
 }
 
+// the blocks of ROWS rows (patches first, then volumes) and the grid
+template <class KT>
 static int traction_grid(ucg_ctx *c, int *pb, int *vb)
 {
+    constexpr int PB = TmTraits<KT>::ROWS / 3, VB = TmTraits<KT>::ROWS / 6;
     const int np = c->nr + c->nt;
-    *pb = (np + 3) / 4;
-    *vb = (c->nv + 1) / 2;
+    *pb = (np + PB - 1) / PB;
+    *vb = (c->nv + VB - 1) / VB;
     const int blocks = *pb + *vb;
     const int cap = c->sms;
     return blocks < cap ? blocks : cap;
 }
 
-template <int S>
-static void launch_traction(ucg_ctx *c, const StageArgs &a, int grid, int pb, int vb)
+template <int S, class KT>
+static void launch_traction_t(ucg_ctx *c, const StageArgs &a, const KT *K, long ldk, const float *scale)
 {
-    const int threads = (MV_WARPS + 1) * 32;
-    const size_t smem = (size_t)TM_STAGES * TM_STAGE_BYTES;
+    int pb, vb;
+    const int grid = traction_grid<KT>(c, &pb, &vb);
+    const size_t smem = tm_smem_bytes<KT>();
+    auto kfn = k_traction<S, KT>;
+    cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kfn<<<grid, (MV_WARPS + 1) * 32, smem, c->stream>>>(K, c->n, ldk, scale, a, c->ctl, pb, vb);
+}
+
+template <int S>
+static void launch_traction(ucg_ctx *c, const StageArgs &a)
+{
     if (S > 1 && rk_anchored(c) && c->Khi_plane) {
         // anchored stages multiply the increments by the hi plane alone
-        auto kfn = k_traction<S, __nv_bfloat16>;
-        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kfn<<<grid, threads, smem, c->stream>>>(c->Khi_plane, c->n, c->ldk_split, c->Kscale, a, c->ctl, pb, vb);
+        launch_traction_t<S, __nv_bfloat16>(c, a, c->Khi_plane, c->ldk_split, c->Kscale);
     } else if (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi) {
-        auto kfn = k_traction<S, __nv_bfloat162>;
-        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kfn<<<grid, threads, smem, c->stream>>>(reinterpret_cast<const __nv_bfloat162 *>(c->Khi), c->n,
-                                                c->ldk_split, c->Kscale, a, c->ctl, pb, vb);
+        launch_traction_t<S, __nv_bfloat162>(c, a, reinterpret_cast<const __nv_bfloat162 *>(c->Khi), c->ldk_split,
+                                             c->Kscale);
     } else {
-        auto kfn = k_traction<S, double>;
-        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kfn<<<grid, threads, smem, c->stream>>>(c->K, c->n, c->n, nullptr, a, c->ctl, pb, vb);
+        launch_traction_t<S, double>(c, a, c->K, c->n, nullptr);
     }
 }
 
@@ -833,9 +847,7 @@ static void enqueue_stage(ucg_ctx *c)
         c->launches.count += 1;
         return;
     }
-    int pb, vb;
-    int grid = traction_grid(c, &pb, &vb);
-    launch_traction<S>(c, a, grid, pb, vb);
+    launch_traction<S>(c, a);
     c->launches.count += 1;
 }
 
@@ -907,14 +919,12 @@ int rk_profile_traction(ucg_ctx *c, int reps, double *ms)
     h->status = 0;
     UCG_CUDA(cudaMemcpyAsync(c->ctl, h, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
     StageArgs a = stage_args(c, 2);
-    int pb, vb;
-    const int grid = traction_grid(c, &pb, &vb);
     cudaEvent_t e0, e1;
     UCG_CUDA(cudaEventCreate(&e0));
     UCG_CUDA(cudaEventCreate(&e1));
     UCG_CUDA(cudaEventRecord(e0, c->stream));
     for (int r = 0; r < reps; r++) {
-        launch_traction<2>(c, a, grid, pb, vb);
+        launch_traction<2>(c, a);
     }
     c->launches.count += reps;
     UCG_CUDA(cudaEventRecord(e1, c->stream));
@@ -1087,7 +1097,7 @@ extern "C" int ucg_odefun_noalloc(const double *K, long n, long m, int np, const
     cudaDeviceGetAttribute(&dcount, cudaDevAttrMultiProcessorCount, dev);
     const int pb = (np + 3) / 4;
     const int grid = pb < dcount ? pb : dcount;
-    const size_t smem = (size_t)TM_STAGES * TM_STAGE_BYTES;
+    const size_t smem = tm_smem_bytes<double>();
     auto kfn = k_traction<1, double>;
     if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return UCG_E_CUDA;
