@@ -1,12 +1,16 @@
 // Batched ensembles: many frictional-parameter instances that share a fault
 // geometry march together, so that the traction product of every Runge-Kutta
 // stage becomes one dense contraction T = K V per geometry (K: 3N x 2N receiver
-// x source DOFs, V: 2N x instances) on the tcgen05 tensor cores.
+// x source DOFs, V: 2N x instances) on the tcgen05 tensor cores, or, for a
+// geometry held as a hierarchical matrix, the two-pass contraction described
+// before k_hm_contract.
 //
 // Precision.  K and V are both held as bf16 hi/lo pairs, K with a power-of-two
-// scale per row: K = s (Khi + Klo), V = Vhi + Vlo.  Each k-block issues three
-// MMAs, Khi Vhi + Khi Vlo + Klo Vhi, accumulating in FP32 in tensor memory; the
-// dropped Klo Vlo term and the residuals are of relative size 2^-16.  State,
+// scale per row: K = s (Khi + Klo), V = Vhi + Vlo.  Each 16-source step forms
+// Khi Vhi + Khi Vlo + Klo Vhi, accumulating in FP32 in tensor memory (the V hi
+// and lo images are consecutive rows of one operand, so one MMA of N = 2 NI
+// takes both Khi products into two accumulator halves that the drain adds);
+// the dropped Klo Vlo term and the residuals are of relative size 2^-16.  State,
 // stage combinations, error norm and step control stay FP64 and follow the
 // single-instance integrator (rk.cu) per instance: every instance has its own
 // step size, time, accept/reject decision and counters, and the reference
@@ -37,7 +41,9 @@
 // memory, so that the drain of one segment overlaps the MMAs of the next) to a
 // workspace.  Work is a list of segments (tile, k-range) per CTA, produced on
 // the host by a scheduler that the autotuner picks (stream-K, or split-K with
-// longest-first packing), so geometries of uneven sizes balance across the SMs.
+// longest-first packing), so geometries of uneven sizes balance across the SMs;
+// every segment is then cut to at most 256 k-blocks, which bounds the FP32
+// accumulation of one partial sum whatever N.
 // The partial sums of a tile are added in k order, in FP64, by the stage
 // epilogue kernel: results are deterministic for a given schedule and an
 // instance's column never depends on the other instances.
