@@ -393,6 +393,12 @@ const char *ucg_ens_last_error(ucg_ensemble *ens);
 /* Add a geometry from a context that holds an assembled FP64 matrix (patches
    only), with n_instances instances (1..4096).  The matrix is converted to the
    tensor-core image at the call; the context may be destroyed afterwards.
+   A context that steps on its hierarchical matrix (ucg_build_hmatrix with
+   leaf <= 42, then UCG_PREC_HMATRIX or UCG_PREC_HMATRIX_SPLIT) or holds no
+   dense matrix gives a hierarchical geometry: H is laid out as tensor-core
+   operand images and every stage runs the two-pass hierarchical contraction
+   (UCG_E_UNSUPPORTED for wider leaves).  No reference counterpart (the
+   reference runs one parameter set per job).
    *geometry receives the geometry index. */
 int ucg_ens_add_geometry(ucg_ensemble *ens, ucg_ctx *ctx, int n_instances, int *geometry);
 

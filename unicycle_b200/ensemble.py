@@ -51,7 +51,10 @@ class Ensemble:
             raise UcgError(st, f"{what}: {msg}")
 
     def add_geometry(self, sim, n_instances):
-        """Add the assembled geometry of `sim` (a Simulation) with n_instances instances."""
+        """Add the geometry of `sim` (a Simulation) with n_instances instances: its assembled
+        dense K, or its hierarchical matrix when `sim` steps on it (UCG_PREC_HMATRIX after
+        build_hmatrix, leaf <= 42) or holds no dense K; the hierarchical operand images are
+        built here."""
         g = ctypes.c_int()
         self._check(self.lib.ucg_ens_add_geometry(self.ens, sim.ctx, int(n_instances), ctypes.byref(g)),
                     "add_geometry")
