@@ -1,23 +1,27 @@
 """Benchmark: RK45 (Cash-Karp, NR step control) steps/s and simulated years per
 hour of the 3-D quasi-dynamic boundary-integral model at N = 20,000
-Nikkhoo-Walter triangles (curved megathrust, full reference layout: K is
-60,000 x 40,000, 19.2 GB in FP64).
+Nikkhoo-Walter triangles (curved megathrust, oblique rake, full reference
+layout: K is 60,000 x 40,000, 19.2 GB in FP64).
 
 One "step" is one accepted main-loop iteration of the reference
 (fortran/3d/src/ratestate.f90:307-326): f(y), yscal, RKQSm attempts until one
 is accepted.
 
-Default workload (--workload ensemble): 64 frictional parameter sets of the
-N = 20k model marched together (ucg_ens_*: the traction product of every stage
-is one split-BF16 K V contraction on the tcgen05 tensor cores; per-instance
-FP64 state and step control).  `value` is accepted steps/s summed over the
-instances and GPUs with the state resident in HBM (one CUDA-graph launch);
-`plain_fp64` is the same model as a single FP64 instance (ucg_run), the
-baseline of the speed-up.  --workload plain / split time the single-instance
-FP64 or split-BF16 path as the headline instead; --workload hens the ensemble on
-the hierarchical K alone (no dense K; --nx 200 --nz 200 is N = 80k), and
---workload hmatrix the single instance on it.  `e2e` is the headline metric
-through host arrays, state host->device and device->host every step.
+Default workload (--workload all): the parsed line is the plain FP64 path --
+the reference's algorithm and precision on one instance (ucg_run, state
+resident in HBM) -- so that the reference arm (the same main loop on the host
+cores) measures the same quantity; `e2e` is the same metric through the
+host-array ABI call (ucg_step: state host->device, state and rate back, every
+step).  `chosen_forms` holds the forms measured against it on the same model:
+split-BF16 K (single instance), 64 frictional parameter sets in one ensemble
+(tensor-core K V contraction), the learned step-size proposal, the
+hierarchical K and the ensemble on it, each with its speed-up over the plain
+FP64 path.  --workload ensemble makes the ensemble the parsed line instead;
+--workload plain / split time one single-instance path alone; --workload hens
+the ensemble on the hierarchical K alone (no dense K; --nx 200 --nz 200 is
+N = 80k), --workload hmatrix the single instance on it; --workload cfg4 the
+batched configuration of 4 faults x 64 sets; --workload coupled the
+fault + strain-volume assembly.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload ...]
 Multi-GPU: replicas only (the path runs on one GPU; no inter-GPU collective).
@@ -50,7 +54,8 @@ def parse():
     p.add_argument("--nx", type=int, default=100, help="along-strike cells (2 triangles each per row)")
     p.add_argument("--nz", type=int, default=100, help="down-dip rows")
     p.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16"])
-    p.add_argument("--workload", default="ensemble", choices=["ensemble", "plain", "split", "coupled", "cfg4", "hmatrix", "hens"])
+    p.add_argument("--workload", default="all",
+                   choices=["all", "ensemble", "plain", "split", "coupled", "cfg4", "hmatrix", "hens"])
     p.add_argument("--coupled-size", default="64,64,16,8,8",
                    help="coupled assembly leg: fault nx,nz and volume nx,ny,nz")
     p.add_argument("--sets", type=int, default=N_SETS, help="instances in the ensemble workload")
@@ -58,6 +63,7 @@ def parse():
                    help="launch the ensemble's attempt kernels from the host instead of one graph launch "
                         "(for ncu, which does not follow conditional graph nodes)")
     p.add_argument("--no-learned", action="store_true", help="skip the learned step-size leg")
+    p.add_argument("--no-split", action="store_true", help="skip the single-instance split-BF16 leg")
     p.add_argument("--no-hmatrix", action="store_true", help="skip the hierarchical-matrix leg")
     p.add_argument("--hm-eta", type=float, default=2.0, help="hierarchical matrix: admissibility parameter")
     p.add_argument("--hm-eps", type=float, default=1e-6, help="hierarchical matrix: ACA relative accuracy")
@@ -311,7 +317,7 @@ def run_ours(args, world, rank, local, keep_sim=False, plain_steps=None):
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (ms_mv / 1e3) / 1e9
     # end to end through the host-array ABI call
-    e2e_steps = args.e2e_steps or max(3, steps_req // 3)
+    e2e_steps = args.e2e_steps or max(10, steps_req // 3)
     y_h, t_h, dt_h = y_t.copy(), t_t, dt_t
     torch.cuda.synchronize()
     e0.record(stream)
@@ -622,6 +628,52 @@ def hmatrix_leg(args, local, sim, cfg, plain):
                          "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind}}
 
 
+def split_leg(args, local, sim, cfg, plain):
+    """The single-instance split-BF16 form on the same N = 20k model: K stored
+    as bf16 hi + lo with a per-row scale, anchored stages (stage 1 reads hi and
+    lo, stages 2-6 the hi plane alone); steps/s and simulated years per hour
+    over the same window as the plain FP64 leg, the hi-plane traction launch
+    against the HBM roofline, and the right-hand side's error against FP64."""
+    import torch
+    import unicycle_b200
+    n = cfg["n_patch"]
+    y_probe = sim.get_state()[0]
+    d64, _ = sim.odefun(y_probe)
+    sim.set_precision(unicycle_b200.UCG_PREC_SPLIT_BF16)
+    dsp, _ = sim.odefun(y_probe)
+    idx = np.concatenate([np.arange(q, len(y_probe), 7) for q in (2, 3, 4)])
+    rhs_err = float(np.max(np.abs(dsp[idx] - d64[idx])) / np.max(np.abs(d64[idx])))
+    stream = torch.cuda.ExternalStream(sim.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sim.set_state(cfg["y0"], 0.0, cfg["dt0"])
+    sim.run(1e300, args.spinup + args.warmup)
+    _, t_w, _, _, rej_w = sim.get_state()
+    steps_req = plain["steps"]
+    torch.cuda.synchronize()
+    e0.record(stream)
+    steps = sim.run(1e300, steps_req)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    _, t_t, _, _, rej_t = sim.get_state()
+    ms_mv = sim.profile_traction(reps=10)
+    sim.set_precision(unicycle_b200.UCG_PREC_FP64)
+    alg = 2.0 * (3 * n) * (2 * n) + 4.0 * 3 * n + 8.0 * (2 * n + 3 * n)
+    peak, peak_kind = load_peaks()
+    syh = (t_t - t_w) / YEAR / (el / 3600.0)
+    return {"steps_per_s": steps / el, "ms_per_step": 1e3 * el / steps, "steps": steps,
+            "sim_years_per_hour": syh, "rejected_attempts": rej_t - rej_w,
+            "speedup_vs_plain_fp64": {"steps_per_s": steps / el / plain["value"],
+                                      "sim_years_per_hour": syh / plain["sim_years_per_hour"]
+                                      if plain["sim_years_per_hour"] > 0 else None},
+            "rhs_traction_rate_max_rel_error_vs_fp64": rhs_err,
+            "roofline": {"bound": "hbm", "kernel": "k_traction<S,bf16> (hi plane x velocity increments)",
+                         "ms_per_launch": ms_mv, "bytes_per_launch": alg, "achieved": alg / (ms_mv / 1e3) / 1e9,
+                         "peak": peak, "unit": "GB/s", "frac": alg / (ms_mv / 1e3) / 1e9 / peak,
+                         "peak_source": peak_kind},
+            "dtype": "bf16 hi+lo K, f32 sums, f64 state"}
+
+
 def hier_ensemble_leg(args, local, cfg, sets, y0s, dense, Kr):
     """The headline ensemble with K replaced by its hierarchical approximation
     (a context that never assembles the dense K): the two-pass tcgen05
@@ -758,18 +810,18 @@ def run_hier_ensemble(args, world, rank, local):
     ref = np.stack([sim.hmatrix_matvec(V[i]) for i in range(3)])
     err = float(max(np.linalg.norm(T[i] - ref[i]) / np.linalg.norm(ref[i]) for i in range(3)))
     # end to end: every attempt, all instances' states host->device (pinned) and back
-    e2e_att = max(3, min(10, args.steps // 6))
+    e2e_att = args.e2e_steps or max(10, args.steps // 3)
     pin = torch.empty((args.sets, 7 * n), dtype=torch.float64, pin_memory=True).numpy()
-    y_h, t_h, dt_h, *_r = ens.get_states(0, out=pin)
-    acc_e2e = 0
+    y_h, t_h, dt_h, acc0, *_r = ens.get_states(0, out=pin)
+    acc0 = int(acc0.sum())
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_att):
-        ens.set_states(0, y_h, t_h, dt_h)
+        ens.put_states(0, y_h)
         ens.run(1e300, 1)
         y_h, t_h, dt_h, acc_h, rej_h, st_h = ens.get_states(0, out=pin)
-        acc_e2e += int(acc_h.sum())
     torch.cuda.synchronize()
+    acc_e2e = int(acc_h.sum()) - acc0
     e2e_el = reduce_max(time.perf_counter() - t0, world, args)
     ens.close()
     sim.close()
@@ -891,8 +943,12 @@ def run_ensemble(args, world, rank, local):
     from unicycle_b200 import configs
 
     torch.cuda.set_device(local)
-    plain = run_ours(args, world, rank, local, keep_sim=True, plain_steps=max(10, args.steps // 2))
+    headline_plain = args.workload == "all"
+    plain = run_ours(args, world, rank, local, keep_sim=True,
+                     plain_steps=args.steps if headline_plain else max(10, args.steps // 2))
     sim, plain = plain["_sim"], {k: v for k, v in plain.items() if k != "_sim"}
+    split = split_leg(args, local, sim, configs.cfg2(nx=args.nx, nz=args.nz), plain) \
+        if rank == 0 and not args.no_split else None
     cfg = configs.cfg2(nx=args.nx, nz=args.nz)
     n = cfg["n_patch"]
     sets, y0s = configs.parameter_sets(cfg, args.sets)
@@ -943,18 +999,18 @@ def run_ensemble(args, world, rank, local):
     check2 = float(np.max(np.abs(ens.matvec(0, V, terms=2)[:, :3 * 256] - V @ Kr.T) / mag))
     # end to end: every attempt, all instances' states host->device (pinned host
     # arrays) and back
-    e2e_att = max(3, min(10, args.steps // 6))
+    e2e_att = args.e2e_steps or max(10, args.steps // 3)
     pin = torch.empty((args.sets, 7 * n), dtype=torch.float64, pin_memory=True).numpy()
-    y_h, t_h, dt_h, *_r = ens.get_states(0, out=pin)
-    acc_e2e = 0
+    y_h, t_h, dt_h, acc0, *_r = ens.get_states(0, out=pin)
+    acc0 = int(acc0.sum())
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_att):
-        ens.set_states(0, y_h, t_h, dt_h)
+        ens.put_states(0, y_h)
         ens.run(1e300, 1)
         y_h, t_h, dt_h, acc_h, rej_h, st_h = ens.get_states(0, out=pin)
-        acc_e2e += int(acc_h.sum())
     torch.cuda.synchronize()
+    acc_e2e = int(acc_h.sum()) - acc0
     e2e_elapsed = reduce_max(time.perf_counter() - t0, world, args)
     ens.close()
     tri_ms = sim.assembly_times()[1]
@@ -1014,8 +1070,9 @@ def run_ensemble(args, world, rank, local):
             "autotune": tune_report.strip().splitlines(),
             "e2e": {"value": world * acc_e2e / e2e_elapsed, "unit": "steps/s",
                     "h2d_bytes_per_step": 8 * 7 * n * args.sets, "d2h_bytes_per_step": 8 * 7 * n * args.sets,
-                    "note": "per attempt: ucg_ens_set_states of all instances from pinned host arrays, one "
-                            "attempt (one graph launch), ucg_ens_get_states back; wall clock"},
+                    "attempts": e2e_att,
+                    "note": "per attempt: ucg_ens_put_states of all instances from pinned host arrays (controller "
+                            "state kept), one attempt (one graph launch), ucg_ens_get_states back; wall clock"},
             "contraction_check": {"anchor_max_rel_to_abs_product": check, "anchor_bound": 1e-4,
                                   "increment_max_rel_to_abs_product": check2, "increment_bound": 5e-3,
                                   "rows": 3 * 256},
@@ -1026,8 +1083,41 @@ def run_ensemble(args, world, rank, local):
             "learned_step": learned,
             "hmatrix": hmat,
             "hierarchical_ensemble": hens,
+            "split_bf16": split,
         }
+        if headline_plain:
+            out = headline_line(out, plain)
     sim.close()
+    return out
+
+
+def headline_line(ens_line, plain):
+    """The parsed line: the plain FP64 path (the reference's own precision and
+    algorithm, so its arm measures the same thing), with the chosen forms beside
+    it as extras, each with its speed-up over this plain FP64 path."""
+    ens = {k: v for k, v in ens_line.items() if k not in (
+        "n_gpus", "warmup", "higher_is_better", "scaling", "vs_baseline", "data", "cpu_baseline", "plain_fp64",
+        "assembly", "assembly_families", "learned_step", "hmatrix", "hierarchical_ensemble", "split_bf16")}
+    learned = ens_line.get("learned_step") or {}
+    comb = None
+    l20 = learned.get("megathrust_20k_ensemble")
+    if l20 and plain.get("sim_years_per_hour"):
+        comb = {"sim_years_per_hour": l20["learned"]["sim_years_per_hour"],
+                "speedup_vs_plain_fp64": l20["learned"]["sim_years_per_hour"] / plain["sim_years_per_hour"],
+                "target": 10.0,
+                "what": "split-BF16 K (tensor-core contraction) x 64-instance batching x learned step proposal, "
+                        "simulated years per hour summed over the instances, over the plain FP64 single instance"}
+    out = dict(plain)
+    out.pop("_sim", None)
+    out["chosen_forms"] = {
+        "combined": comb,
+        "ensemble": ens,
+        "split_bf16": ens_line.get("split_bf16"),
+        "learned_step": learned,
+        "hmatrix": ens_line.get("hmatrix"),
+        "hierarchical_ensemble": ens_line.get("hierarchical_ensemble"),
+    }
+    out["assembly_families"] = ens_line.get("assembly_families")
     return out
 
 
@@ -1036,7 +1126,7 @@ def main():
     world, rank, local = dist_init(args)
     if args.impl == "reference":
         out = run_reference(args, world, rank)
-    elif args.workload == "ensemble":
+    elif args.workload in ("all", "ensemble"):
         out = run_ensemble(args, world, rank, local)
     elif args.workload == "cfg4":
         out = run_cfg4(args, world, rank, local)

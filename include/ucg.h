@@ -347,27 +347,43 @@ void *ucg_stream(ucg_ctx *ctx);
    stepped at least once).  No reference counterpart. */
 int ucg_profile_traction(ucg_ctx *ctx, int reps, double *ms);
 
+/* Fault injection for testing the bounded device waits (the reference has no
+   counterpart: its failures end in STOP).  wait_ns > 0 replaces the 4 s limit
+   of the traction product's data waits; hold != 0 makes the product's first
+   CTA issue no copies, so that its consumers wait on data that never comes,
+   give up after wait_ns and the call (ucg_odefun, ucg_step, ucg_run) returns
+   UCG_E_TIMEOUT with the context still usable.  ucg_test_wait_timeout(ctx, 0,
+   0) restores normal operation. */
+int ucg_test_wait_timeout(ucg_ctx *ctx, long wait_ns, int hold);
+
 /* ---- allocation-free right-hand side ------------------------------------- */
 
 /* dydt = f(y) for a fault model held entirely in caller-owned DEVICE memory,
    without any device allocation: for callers that cannot call cudaMalloc at
    this point (an external memory manager owns the device, or an
-   allocation-free real-time loop).  No counterpart in the reference (it is the
-   odefun of fortran/3d/src/ratestate.f90:624-778 without a context).
-   K: m x n row-major traction matrix (m = 3 np, n = 2 np; patches only);
+   allocation-free real-time loop).  No counterpart in the reference; the
+   context-based equivalent is ucg_odefun above.
+   K: m x n row-major traction matrix (m = 3 np, n = 2 np; patches only), its
+   base address 16-byte aligned (its rows are moved by bulk copies);
    y, dydt: 7 np state and rate; per patch Vpl*cos(rake), Vpl*sin(rake), a, b,
-   sig, L, damping.  Work is queued on `stream` (a cudaStream_t, NULL for the
-   default stream) on the current device.  The only working storage is a fixed
-   8 MB array in the library's device image, which bounds n at 2^20 source DOFs
-   (UCG_E_BADARG beyond); every GPU that loads the library holds it until the
-   process exits.  The first call on a device resolves that array's device
-   address and should come before any stream capture.  Calls share the array:
-   calls that overlap on the GPU race and must be ordered by the caller. */
+   sig, L, damping; every double array 8-byte aligned.  UCG_E_BADARG, before
+   anything is queued, for a null or misaligned pointer or inconsistent sizes.
+   Work is queued on `stream` (a cudaStream_t, NULL for the default stream) on
+   the current device; the return value reports only the checks and the
+   launches.  status (optional, caller-owned DEVICE int, may be NULL) receives,
+   in stream order after the result, UCG_OK, UCG_E_NONFINITE (a NaN/Inf state
+   or rate) or UCG_E_TIMEOUT (a bounded device wait gave up: dydt incomplete).
+   The only working storage is a fixed 8 MB array in the library's device
+   image, which bounds n at 2^20 source DOFs (UCG_E_BADARG beyond); every GPU
+   that loads the library holds it until the process exits.  The first call on
+   a device may load the library's device code and should come before any
+   stream capture.  Calls share the array: calls that overlap on the GPU race
+   and must be ordered by the caller. */
 int ucg_odefun_noalloc(const double *K, long n, long m, int np, const double *y,
                        const double *Vpl_cos_rake, const double *Vpl_sin_rake,
                        const double *a, const double *b, const double *sig,
                        const double *L, const double *damping, double *dydt,
-                       void *stream);
+                       void *stream, int *status);
 
 /* ---- batched ensembles (tensor-core traction product) --------------------- */
 
@@ -425,6 +441,23 @@ int ucg_ens_set_states(ucg_ensemble *ens, int geometry, const double *y, const d
                        const double *dt_next);
 int ucg_ens_get_states(ucg_ensemble *ens, int geometry, double *y, double *time, double *dt_next,
                        long *accepted, long *rejected, int *status);
+/* Replace every instance's state vector of a geometry from a host array
+   (n_instances x 7 n_patches) and keep each instance's time, step size,
+   counters and step-size history: a driver that takes the states to the host
+   between runs (ucg_ens_get_states) and hands them back continues exactly as
+   the device-resident loop would.  An instance whose state changed in any bit
+   re-evaluates f(y) and yscal at its next attempt (a new main-loop iteration,
+   fortran/3d/src/ratestate.f90:307-326).  No reference counterpart. */
+int ucg_ens_put_states(ucg_ensemble *ens, int geometry, const double *y);
+
+/* Fault injection for testing the bounded device waits (no reference
+   counterpart).  wait_ns > 0 replaces the 4 s limit of the dense contraction's
+   data waits; hold != 0 makes its first CTA issue no copies, so that the MMA
+   issuer waits on data that never comes and gives up: ucg_ens_run (and
+   ucg_ens_matvec) then return UCG_E_TIMEOUT, the instances' stage kernels skip
+   the attempt, and the ensemble stays usable after ucg_ens_test_wait_timeout(ens,
+   0, 0) and fresh states. */
+int ucg_ens_test_wait_timeout(ucg_ensemble *ens, long wait_ns, int hold);
 
 /* Contraction plan: instance tile width ni (32, 64 or 128 instances per MMA)
    and schedule (UCG_ENS_*; chunk = k-blocks per split for UCG_ENS_SPLIT_LPT,

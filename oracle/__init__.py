@@ -8,6 +8,7 @@ CPU legs of bench.py, never by the unicycle_b200 package.
 import ctypes
 import os
 import subprocess
+import sys
 
 import numpy as np
 
@@ -24,11 +25,22 @@ OKADA_REF32IO = 1
 
 
 def build(ref=True):
-    """Compile liboracle.so (and the reference C into _ref/ when available)."""
+    """Compile liboracle.so, and the reference's Nikkhoo-Walter C into _ref/ when
+    the environment variable UCG_REFERENCE_SRC names the reference's
+    fortran/3d/src directory (there is no default location)."""
     subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
-    src = os.environ.get("UCG_REFERENCE_SRC", "/root/reference/fortran/3d/src")
-    if ref and os.path.isdir(src):
+    src = os.environ.get("UCG_REFERENCE_SRC")
+    if not ref:
+        return
+    if not src:
+        if not os.path.exists(_REF):
+            print("oracle.build: UCG_REFERENCE_SRC is unset; the reference's own C is not compiled "
+                  "(tests that need it use the committed fixtures or skip)", file=sys.stderr)
+        return
+    if os.path.isdir(src):
         subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF_SRC={src}"], check=True)
+    else:
+        print(f"oracle.build: UCG_REFERENCE_SRC={src} is not a directory", file=sys.stderr)
 
 
 def _ptr(a, t=_dp):

@@ -1,0 +1,211 @@
+"""Slip-rate and state histories of every form of the integrator against the
+FP64 oracle's own adaptive run of the reference main loop
+(fortran/3d/src/ratestate.f90:307-326 with RKQSm, fortran/3d/src/ode45.f90:51-108).
+
+Every form takes its own accepted steps, so the histories are compared at the
+form's accepted times: the oracle's value at a time t is one Cash-Karp step of
+size t - t_k from the oracle's last accepted state before t (the fifth-order
+solution, whose local error is below the one the oracle accepted at t_k), not
+an interpolation.  The quantities are the state components log10 V and
+log10 theta; the error is relative on them, max over patches.
+
+Model: a 16 x 8 rectangle fault tilted to 70 deg dip slipping at rake 30 deg
+(no state component is zero by symmetry), rtol 1e-8, the first 1,000 accepted
+steps.  They cover interseismic loading, the nucleation and one slip event
+(peak V about 1e-4 m/s) and its afterslip.  While V is far below the event
+threshold the histories of every form are compared pointwise; during an event
+a pointwise comparison measures the onset timing (V grows e-fold in seconds
+there), so the onset time is compared separately.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NSTEPS = 1000
+V_QUIET = 1.0e-7          # pointwise window: max V below 100 Vpl
+V_EVENT = 1.0e-5          # onset: first accepted step with max V at or above this
+
+
+def _model():
+    from unicycle_b200 import configs
+    return configs.tilt(configs.cfg1(nx=16, nz=8))
+
+
+class _Reference:
+    """The oracle's adaptive run and its values at arbitrary times."""
+
+    def __init__(self, oracle_lib, G, c, nsteps):
+        self.md = oracle_lib.Model(G, c["friction"])
+        y, t, dt = c["y0"].copy(), 0.0, c["dt0"]
+        self.t, self.y = [0.0], [y.copy()]
+        for _ in range(nsteps):
+            rc, t, y, _, dt, _, _ = self.md.step(t, y, dt, c["epsilon"])
+            assert rc == 0
+            self.t.append(t)
+            self.y.append(y.copy())
+        self.t = np.array(self.t)
+
+    def at(self, t):
+        k = int(np.searchsorted(self.t, t, side="right")) - 1
+        assert 0 <= k < len(self.t) - 1, "form ran past the reference window"
+        if self.t[k] == t:
+            return self.y[k]
+        d, _ = self.md.odefun(self.y[k])
+        yo, _ = self.md.rkck(self.y[k], d, t - self.t[k])
+        return yo
+
+
+def _onset(ts, ys):
+    for t, y in zip(ts, ys):
+        if 10.0 ** np.max(y[6::7]) >= V_EVENT:
+            return t
+    return None
+
+
+def _compare(name, ref, ts, ys):
+    quiet = {"v": 0.0, "th": 0.0, "n": 0}
+    whole = {"v": 0.0, "th": 0.0}
+    for t, y in zip(ts, ys):
+        r = ref.at(t)
+        ev = np.max(np.abs(y[6::7] - r[6::7]) / np.abs(r[6::7]))
+        et = np.max(np.abs(y[5::7] - r[5::7]) / np.abs(r[5::7]))
+        whole["v"], whole["th"] = max(whole["v"], ev), max(whole["th"], et)
+        if 10.0 ** np.max(r[6::7]) < V_QUIET:
+            quiet["v"], quiet["th"] = max(quiet["v"], ev), max(quiet["th"], et)
+            quiet["n"] += 1
+    o_ref = _onset(ref.t, ref.y)
+    o = _onset(ts, ys)
+    d_on = abs(o - o_ref) / o_ref if (o is not None and o_ref is not None) else None
+    print(f"{name:>22}: {len(ts)} steps to t = {ts[-1]:.6e} s; quiet window ({quiet['n']} steps) "
+          f"log10 V {quiet['v']:.2e}, log10 theta {quiet['th']:.2e}; whole run {whole['v']:.2e} / "
+          f"{whole['th']:.2e}; onset {o} vs {o_ref} (rel {d_on})")
+    return quiet, whole, d_on
+
+
+def _single(sim, c, nsteps):
+    y, t, dt = c["y0"].copy(), 0.0, c["dt0"]
+    ts, ys = [], []
+    for _ in range(nsteps):
+        t, y, _, dt, _, _ = sim.step(t, y, dt)
+        ts.append(t)
+        ys.append(y.copy())
+    return np.array(ts), ys
+
+
+def _ensemble(ucg, sim, c, nsteps, ninst=4, model=None):
+    """Attempts one at a time; instance 0's state after each acceptance.  All
+    instances carry the same parameters: their histories must be identical."""
+    fr = c["friction"]
+    ens = ucg.Ensemble()
+    ens.add_geometry(sim, ninst)
+    for i in range(ninst):
+        ens.set_friction(0, i, fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
+                         fr["damping"])
+        ens.set_state(0, i, c["y0"], 0.0, c["dt0"])
+    ens.set_tolerance(c["epsilon"])
+    if model is not None:
+        ens.set_step_model(model)
+    ts, ys = [], []
+    last = 0
+    for _ in range(4 * nsteps):
+        ens.run(1e300, 1)
+        y, t, _, acc, _, st = ens.get_states(0)
+        assert np.all(st == 0)
+        if acc[0] > last:
+            last = acc[0]
+            ts.append(t[0])
+            ys.append(y[0].copy())
+            assert np.array_equal(y[0], y[-1])
+            if len(ts) == nsteps:
+                break
+    ens.close()
+    return np.array(ts), ys
+
+
+@pytest.fixture(scope="module")
+def setup(ucg, oracle_lib):
+    from unicycle_b200 import configs
+    c = _model()
+    sim = ucg.Simulation(c["mu"], c["lam"])
+    configs.build(sim, c)
+    sim.set_tolerance(c["epsilon"])
+    G = sim.copy_G()
+    ref = _Reference(oracle_lib, G, c, int(1.6 * NSTEPS))
+    yield c, sim, ref
+    sim.close()
+
+
+def _check(name, ref, ts, ys, quiet_tol, onset_tol):
+    quiet, whole, d_on = _compare(name, ref, ts, ys)
+    assert quiet["n"] > 100
+    assert quiet["v"] <= quiet_tol and quiet["th"] <= quiet_tol, (name, quiet)
+    assert d_on is not None and d_on <= onset_tol, (name, d_on)
+
+
+def test_history_plain_fp64(ucg, setup):
+    c, sim, ref = setup
+    sim.set_precision(ucg.UCG_PREC_FP64)
+    ts, ys = _single(sim, c, NSTEPS)
+    _check("plain FP64", ref, ts, ys, 1e-9, 1e-6)
+
+
+def test_history_split_bf16(ucg, setup):
+    c, sim, ref = setup
+    sim.set_precision(ucg.UCG_PREC_SPLIT_BF16)
+    ts, ys = _single(sim, c, NSTEPS)
+    sim.set_precision(ucg.UCG_PREC_FP64)
+    _check("split-BF16", ref, ts, ys, 1e-6, 1e-5)
+
+
+def test_history_dense_ensemble(ucg, setup):
+    c, sim, ref = setup
+    sim.set_precision(ucg.UCG_PREC_FP64)
+    ts, ys = _ensemble(ucg, sim, c, NSTEPS)
+    _check("ensemble (tensor cores)", ref, ts, ys, 1e-6, 1e-5)
+
+
+def test_history_hmatrix(ucg, setup):
+    c, sim, ref = setup
+    sim.build_hmatrix(eta=2.0, eps=1e-8, leaf=16)
+    for prec, name in ((ucg.UCG_PREC_HMATRIX, "hierarchical FP64"),
+                       (ucg.UCG_PREC_HMATRIX_SPLIT, "hierarchical split")):
+        sim.set_precision(prec)
+        ts, ys = _single(sim, c, NSTEPS)
+        _check(name, ref, ts, ys, 1e-6, 1e-5)
+    sim.set_precision(ucg.UCG_PREC_HMATRIX)
+    ts, ys = _ensemble(ucg, sim, c, NSTEPS)
+    _check("hierarchical ensemble", ref, ts, ys, 1e-6, 1e-5)
+    sim.set_precision(ucg.UCG_PREC_FP64)
+
+
+def test_history_learned_step(ucg, setup):
+    """The learned proposal on the ensemble: the proposal only changes which
+    step is tried; the embedded error estimate still judges it, so the history
+    stays within the same bound of the oracle's."""
+    from unicycle_b200 import configs
+    from unicycle_b200.stepmodel import training_set
+    c, sim, ref = setup
+    sim.set_precision(ucg.UCG_PREC_FP64)
+    cfg, y0s = configs.cfg1_instances(list(range(100, 116)), nx=16, nz=8)
+    s1 = ucg.Simulation(cfg["mu"], cfg["lam"])
+    configs.build(s1, cfg)
+    fr = cfg["friction"]
+    tr = ucg.Ensemble()
+    tr.add_geometry(s1, len(y0s))
+    for i, y0 in enumerate(y0s):
+        tr.set_friction(0, i, fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
+                        fr["damping"])
+        tr.set_state(0, i, y0, 0.0, cfg["dt0"])
+    tr.set_tolerance(cfg["epsilon"])
+    tr.record_traces(200000)
+    tr.run(200 * configs.YEAR, 6000)
+    x, y = training_set(tr.traces())
+    tr.close()
+    s1.close()
+    m = ucg.StepModel(seed=1)
+    m.set_data(x, y)
+    m.train(epochs=20, batch=2048, lr=1e-3)
+    ts, ys = _ensemble(ucg, sim, c, NSTEPS, model=m)
+    m.close()
+    _check("ensemble + learned step", ref, ts, ys, 1e-6, 1e-5)

@@ -104,7 +104,8 @@ SIGNATURES = {
     "ucg_launch_count": (_l, [_vp]),
     "ucg_stream": (_vp, [_vp]),
     "ucg_profile_traction": (_i, [_vp, _i, _dp]),
-    "ucg_odefun_noalloc": (_i, [_vp, _l, _l, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ucg_test_wait_timeout": (_i, [_vp, _l, _i]),
+    "ucg_odefun_noalloc": (_i, [_vp, _l, _l, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ucg_ens_create": (_i, [ctypes.POINTER(_vp), _i]),
     "ucg_ens_destroy": (None, [_vp]),
     "ucg_ens_last_error": (ctypes.c_char_p, [_vp]),
@@ -115,6 +116,8 @@ SIGNATURES = {
     "ucg_ens_get_state": (_i, [_vp, _i, _i, _dp, _dp, _dp, _lp, _lp, _ip]),
     "ucg_ens_set_states": (_i, [_vp, _i, _dp, _dp, _dp]),
     "ucg_ens_get_states": (_i, [_vp, _i, _dp, _dp, _dp, _lp, _lp, _ip]),
+    "ucg_ens_put_states": (_i, [_vp, _i, _dp]),
+    "ucg_ens_test_wait_timeout": (_i, [_vp, _l, _i]),
     "ucg_ens_plan": (_i, [_vp, _i, _i, _i]),
     "ucg_ens_tune": (_i, [_vp, _i, ctypes.c_char_p, _l]),
     "ucg_ens_use_graph": (_i, [_vp, _i]),

@@ -149,6 +149,11 @@ struct EnsGlobal {
     const mlp::Norm *mlp_N;
     float *trace;               // records of TRACE_LEN floats
     unsigned long long trace_cap, trace_n;
+    // fault injection for tests of the bounded waits (ucg_ens_test_wait_timeout):
+    // wait_ns != 0 replaces the 4 s limit of the dense contraction's data waits;
+    // test_hold makes its first CTA issue no copies
+    unsigned long long wait_ns;
+    int test_hold;
 };
 
 // one trace record: the 11 model inputs at an acceptance, then log10 of the
@@ -230,7 +235,8 @@ __device__ __forceinline__ unsigned long long now_ns()
     return t;
 }
 // bounded wait; abort == nullptr waits out the deadline regardless of other threads
-__device__ __forceinline__ bool bar_wait(uint64_t *b, uint32_t parity, volatile int *abort)
+__device__ __forceinline__ bool bar_wait(uint64_t *b, uint32_t parity, volatile int *abort,
+                                         unsigned long long limit = TIMEOUT_NS)
 {
     if (bar_try(b, parity)) return true;
     const unsigned long long t0 = now_ns();
@@ -238,7 +244,7 @@ __device__ __forceinline__ bool bar_wait(uint64_t *b, uint32_t parity, volatile 
         if (bar_try(b, parity)) return true;
         if ((it & 127u) == 0u) {
             if (abort && *abort) return false;
-            if (now_ns() - t0 > TIMEOUT_NS) return false;
+            if (now_ns() - t0 > limit) return false;
         }
     }
 }
@@ -297,8 +303,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16])
 
 template <int NI, bool KLO, int MT>
 __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__restrict__ tiles,
-        const GemmSeg *__restrict__ segs, const int *__restrict__ cta_seg, float *__restrict__ ws, int *err)
+        const GemmSeg *__restrict__ segs, const int *__restrict__ cta_seg, float *__restrict__ ws, EnsGlobal *gl)
 {
+    int *err = &gl->err;
+    const unsigned long long lim = gl->wait_ns ? gl->wait_ns : TIMEOUT_NS;
+    // (test_hold: the first CTA issues no copies, its MMA issuer's wait runs out)
+    const bool hold = gl->test_hold && blockIdx.x == 0;
     using T = Tile<NI, KLO, MT>;
     extern __shared__ unsigned char dyn_smem[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dyn_smem) + 1023) & ~(uintptr_t)1023);
@@ -346,7 +356,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
             GemmSeg s1 = q0 < q1 ? segs[q0] : GemmSeg{0, 0, 0, 0};
             GemmSeg s2 = q0 + 1 < q1 ? segs[q0 + 1] : s1;
             GemmTile t1 = q0 < q1 ? tiles[s1.tile] : GemmTile{nullptr, nullptr, nullptr};
-            for (int q = q0; q < q1 && !abort_flag; q++) {
+            for (int q = q0; q < q1 && !abort_flag && !hold; q++) {
                 const GemmSeg sg = s1;
                 const GemmTile tl = t1;
                 s1 = s2;
@@ -357,7 +367,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                 for (int kb = sg.kb0; kb < sg.kb1; kb++) {
                     const int s = (int)(issued % T::STAGES);
                     const uint32_t ph = (uint32_t)((issued / T::STAGES) & 1);
-                    if (!bar_wait(&empty[s], ph ^ 1u, &abort_flag)) {
+                    if (!bar_wait(&empty[s], ph ^ 1u, &abort_flag, lim)) {
                         if (!abort_flag) fail();
                         break;
                     }
@@ -383,7 +393,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                 const int nt = (MT == 2 && tiles[sg.tile].a1 != nullptr) ? 2 : 1;
                 const int buf = tc & 1;
                 const uint32_t use = (uint32_t)(tc >> 1);
-                if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag)) {
+                if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag, lim)) {
                     if (!abort_flag) fail();
                     break;
                 }
@@ -392,7 +402,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                 for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
                     const int s = (int)(it % T::STAGES);
                     const uint32_t ph = (uint32_t)((it / T::STAGES) & 1);
-                    if (!bar_wait(&full[s], ph, &abort_flag)) {
+                    if (!bar_wait(&full[s], ph, &abort_flag, lim)) {
                         if (!abort_flag) fail();
                         ok = false;
                         break;
@@ -446,7 +456,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
             const int buf = tc & 1;
             const uint32_t use = (uint32_t)(tc >> 1);
             int ok = 0;
-            if (lane == 0) ok = bar_wait(&acc_full[buf], use & 1u, &abort_flag) ? 1 : 0;
+            if (lane == 0) ok = bar_wait(&acc_full[buf], use & 1u, &abort_flag, lim) ? 1 : 0;
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) {
                 if (lane == 0 && !abort_flag) fail();
@@ -1549,6 +1559,23 @@ __global__ void k_ens_commit(const EnsArgs *__restrict__ A)
     }
 }
 
+// ucg_ens_put_states: the staged states (in the candidate vector, unused
+// between launches) replace the instances' states; an instance whose state
+// changed in any bit re-evaluates f(y) and yscal at its next attempt, one
+// handed back the state it had keeps its stage-1 rate, as the device-resident
+// loop would
+__global__ void k_ens_put(double *__restrict__ y, const double *__restrict__ staged, InstCtl *__restrict__ ctl,
+                          long len, long total)
+{
+    for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < total; j += (long)gridDim.x * blockDim.x) {
+        const double v = staged[j];
+        if (__double_as_longlong(v) != __double_as_longlong(y[j])) {
+            y[j] = v;
+            ctl[j / len].need_stage1 = 1;
+        }
+    }
+}
+
 __global__ void k_ens_clear_pending(const EnsArgs *__restrict__ A)
 {
     for (int gi = 0; gi < A->ngeom; gi++) {
@@ -2249,7 +2276,7 @@ template <int NI, bool KLO, int MT>
 cudaError_t launch_contract_t(ucg_ensemble *E, const PlanBufs &P)
 {
     k_bf16x3_contract<NI, KLO, MT><<<E->sms, 192, Tile<NI, KLO, MT>::SMEM, E->stream>>>(P.tiles, P.segs, P.cta,
-                                                                                        P.ws, &E->d_glob->err);
+                                                                                        P.ws, E->d_glob);
     E->launches++;
     return cudaGetLastError();
 }
@@ -2830,6 +2857,37 @@ int ucg_ens_set_states(ucg_ensemble *E, int gi, const double *y, const double *t
         x[i].thmin_key = ~0ull;
     }
     ECUDA(cudaMemcpyAsync(g.ctl, x.data(), sizeof(InstCtl) * g.ninst, cudaMemcpyHostToDevice, E->stream));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    return UCG_OK;
+}
+
+int ucg_ens_test_wait_timeout(ucg_ensemble *E, long wait_ns, int hold)
+{
+    if (!E || wait_ns < 0) return UCG_E_BADARG;
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    E->h_glob->wait_ns = (unsigned long long)wait_ns;
+    E->h_glob->test_hold = hold != 0;
+    E->h_glob->err = 0;
+    ECUDA(cudaMemcpy(&E->d_glob->wait_ns, &E->h_glob->wait_ns, sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    ECUDA(cudaMemcpy(&E->d_glob->test_hold, &E->h_glob->test_hold, sizeof(int), cudaMemcpyHostToDevice));
+    ECUDA(cudaMemcpy(&E->d_glob->err, &E->h_glob->err, sizeof(int), cudaMemcpyHostToDevice));
+    return UCG_OK;
+}
+
+int ucg_ens_put_states(ucg_ensemble *E, int gi, const double *y)
+{
+    if (!E || gi < 0 || gi >= (int)E->geoms.size()) return E ? ebad(E, UCG_E_BADARG, "geometry out of range") : UCG_E_BADARG;
+    if (!y) return ebad(E, UCG_E_BADARG, "null array");
+    EnsGeomHost &g = E->geoms[gi];
+    ECUDA(cudaSetDevice(E->device));
+    const long len = 7L * g.np, total = len * g.ninst;
+    double *staged = g.state + 8 * total;   // the candidate vector: free between launches
+    ECUDA(cudaMemcpyAsync(staged, y, sizeof(double) * total, cudaMemcpyHostToDevice, E->stream));
+    const int blocks = (int)std::min<long>((total + 255) / 256, 4L * 148);
+    ens::k_ens_put<<<blocks, 256, 0, E->stream>>>(g.state, staged, g.ctl, len, total);
+    E->launches++;
+    ECUDA(cudaGetLastError());
     ECUDA(cudaStreamSynchronize(E->stream));
     return UCG_OK;
 }

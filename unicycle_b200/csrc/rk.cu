@@ -276,16 +276,18 @@ __device__ __forceinline__ unsigned long long gtimer()
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     return t;
 }
-// bounded wait: false when the deadline passes or another thread aborted
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort)
+// bounded wait: false when `limit` ns pass or (abort != nullptr) another
+// thread aborted
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort,
+                                          unsigned long long limit = TM_TIMEOUT_NS)
 {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = gtimer();
     for (unsigned it = 1;; it++) {
         if (mbar_try(bar, parity)) return true;
         if ((it & 255u) == 0u) {
-            if (*abort) return false;
-            if (gtimer() - t0 > TM_TIMEOUT_NS) return false;
+            if (abort && *abort) return false;
+            if (gtimer() - t0 > limit) return false;
         }
     }
 }
@@ -440,11 +442,14 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
         }
     };
 
+    const unsigned long long wait_lim = ctl->wait_ns ? ctl->wait_ns : TM_TIMEOUT_NS;
     if (warp == MV_WARPS) {
         // producer: one lane issues the row copies of each (block, chunk) item
         if (lane == 0) {
             long item = 0;
-            for (int blk = blockIdx.x; blk < nblk && !abort_flag; blk += gridDim.x) {
+            // (test_hold: the first CTA issues nothing, its consumers' waits run out)
+            const bool hold = ctl->test_hold && blockIdx.x == 0;
+            for (int blk = blockIdx.x; blk < nblk && !abort_flag && !hold; blk += gridDim.x) {
                 long row0; int nrows, e0, nel; bool patch;
                 block_rows(blk, row0, nrows, e0, nel, patch);
                 for (long ch = 0; ch < nch; ch++, item++) {
@@ -464,6 +469,11 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
                         bulk_g2s(dst + (size_t)r * CH, K + (row0 + r) * ldk + c0, rowbytes, &full[s]);
                 }
             }
+            // items are issued in order, so the last copies into each stage are
+            // those of the last STAGES items: they land before the CTA may exit,
+            // also when the consumers gave up on them (bounded at the normal limit)
+            for (long i = item > STAGES ? item - STAGES : 0; i < item; i++)
+                mbar_wait(&full[i % STAGES], (uint32_t)((i / STAGES) & 1), nullptr);
         }
         return;
     }
@@ -490,7 +500,7 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
             const long c = ch * CH + cl;
             TmV<KT> vr;
             if (c < n) tm_load_v<KT>(a.v, c, n, vr);
-            const bool ready = !abort_flag && mbar_wait(&full[s], ph, &abort_flag);
+            const bool ready = !abort_flag && mbar_wait(&full[s], ph, &abort_flag, wait_lim);
             if (!ready && !abort_flag) {
                 abort_flag = 1;
                 ctl->status = UCG_E_TIMEOUT;
@@ -1010,7 +1020,22 @@ int rk_odefun(ucg_ctx *c)
     UCG_CUDA(cudaGetLastError());
     UCG_CUDA(cudaMemcpyAsync(h, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
     UCG_CUDA(cudaStreamSynchronize(c->stream));
+    if (h->status) return h->status;
     return h->nonfinite ? UCG_E_NONFINITE : UCG_OK;
+}
+
+// fault injection for the tests of the bounded waits
+int rk_test_wait_timeout(ucg_ctx *c, unsigned long long wait_ns, int hold)
+{
+    Ctl *h = c->ctl_host;
+    UCG_CUDA(cudaMemcpyAsync(h, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    h->wait_ns = wait_ns;
+    h->test_hold = hold;
+    h->status = 0;
+    UCG_CUDA(cudaMemcpyAsync(c->ctl, h, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+    UCG_CUDA(cudaStreamSynchronize(c->stream));
+    return UCG_OK;
 }
 
 // ---- allocation-free right-hand side --------------------------------------------
@@ -1034,9 +1059,6 @@ constexpr long NOALLOC_CTL_DOUBLES = (sizeof(Ctl) + sizeof(double) - 1) / sizeof
 
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_MAX_N + NOALLOC_CTL_DOUBLES];
 
-constexpr int NOALLOC_MAX_DEVICES = 64;
-static double *g_noalloc_addr[NOALLOC_MAX_DEVICES];      // device address per device, set once
-
 __global__ void k_noalloc_ctl_reset(Ctl *ctl)
 {
     Ctl z;
@@ -1048,6 +1070,15 @@ __global__ void k_noalloc_ctl_reset(Ctl *ctl)
     *ctl = z;
 }
 
+// the call's outcome into the caller's status word, after the other kernels:
+// a wait that gave up (UCG_E_TIMEOUT), a NaN/Inf met on the way, or UCG_OK
+__global__ void k_noalloc_status(const Ctl *ctl, int *status)
+{
+    *status = ctl->status ? ctl->status : (ctl->nonfinite ? UCG_E_NONFINITE : UCG_OK);
+}
+
+inline bool aligned_to(const void *p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
+
 }  // namespace
 
 }  // namespace ucg
@@ -1055,29 +1086,33 @@ __global__ void k_noalloc_ctl_reset(Ctl *ctl)
 extern "C" int ucg_odefun_noalloc(const double *K, long n, long m, int np, const double *y,
                                   const double *Vpl_cos_rake, const double *Vpl_sin_rake,
                                   const double *a, const double *b, const double *sig, const double *L,
-                                  const double *damping, double *dydt, void *stream)
+                                  const double *damping, double *dydt, void *stream, int *status)
 {
     using namespace ucg;
-    if (!K || !y || !dydt || !Vpl_cos_rake || !Vpl_sin_rake || !a || !b || !sig || !L || !damping)
-        return UCG_E_BADARG;
+    const double *dp[] = {y, dydt, Vpl_cos_rake, Vpl_sin_rake, a, b, sig, L, damping};
+    if (!K) return UCG_E_BADARG;
+    for (const double *p : dp)
+        if (!p || !aligned_to(p, sizeof(double))) return UCG_E_BADARG;
+    // K's rows go to shared memory by bulk copies, whose source must sit on a
+    // 16-byte boundary (n is even, so every row then does)
+    if (!aligned_to(K, 16)) return UCG_E_BADARG;
+    if (status && !aligned_to(status, sizeof(int))) return UCG_E_BADARG;
     if (np <= 0 || n != 2L * np || m != 3L * np) return UCG_E_BADARG;
     if (n > NOALLOC_MAX_N) return UCG_E_BADARG;   // beyond the fixed scratch: 2^20 source DOFs
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return UCG_E_NODEVICE;
-    // set-up, once per device, with that device current: the host-side name of
-    // the array is not a device address, so resolve it here
-    if (!g_noalloc_addr[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return UCG_E_CUDA;
-        g_noalloc_addr[dev] = static_cast<double *>(p);
-    }
-    double *v = g_noalloc_addr[dev];
+    if (cudaGetDevice(&dev) != cudaSuccess) return UCG_E_NODEVICE;
+    // the host-side name of the array is not a device address: resolve it on
+    // every call with the calling device current (no allocation; the first call
+    // on a device may load the module)
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return UCG_E_CUDA;
+    double *v = static_cast<double *>(p);
     Ctl *ctl = reinterpret_cast<Ctl *>(v + NOALLOC_MAX_N);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     StageArgs sa{};
     sa.y = y;
-    sa.ys = const_cast<double *>(y);
+    sa.ys = const_cast<double *>(y);   // stage 1 reads y and writes nothing into it
     for (int j = 0; j < 6; j++) sa.k[j] = dydt;
     sa.v = v;
     sa.fr.vpl_c = const_cast<double *>(Vpl_cos_rake);
@@ -1091,16 +1126,18 @@ extern "C" int ucg_odefun_noalloc(const double *K, long n, long m, int np, const
     sa.nvol = 0;
     sa.len = 7L * np;
 
-    k_noalloc_ctl_reset<<<1, 1, 0, st>>>(ctl);
-    k_prologue<1><<<(np + 127) / 128, 128, 0, st>>>(sa, ctl);
     int dcount = 0;
-    cudaDeviceGetAttribute(&dcount, cudaDevAttrMultiProcessorCount, dev);
-    const int pb = (np + 3) / 4;
-    const int grid = pb < dcount ? pb : dcount;
+    if (cudaDeviceGetAttribute(&dcount, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || dcount <= 0)
+        return UCG_E_CUDA;
     const size_t smem = tm_smem_bytes<double>();
     auto kfn = k_traction<1, double>;
     if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return UCG_E_CUDA;
+    k_noalloc_ctl_reset<<<1, 1, 0, st>>>(ctl);
+    k_prologue<1><<<(np + 127) / 128, 128, 0, st>>>(sa, ctl);
+    const int pb = (np + 3) / 4;
+    const int grid = pb < dcount ? pb : dcount;
     kfn<<<grid, (MV_WARPS + 1) * 32, smem, st>>>(K, n, n, nullptr, sa, ctl, pb, 0);
+    if (status) k_noalloc_status<<<1, 1, 0, st>>>(ctl, status);
     return cudaGetLastError() == cudaSuccess ? UCG_OK : UCG_E_CUDA;
 }

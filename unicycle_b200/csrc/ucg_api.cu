@@ -988,4 +988,14 @@ int ucg_profile_traction(ucg_ctx *c, int reps, double *ms)
     return rk_profile_traction(c, reps, ms);
 }
 
+int ucg_test_wait_timeout(ucg_ctx *c, long wait_ns, int hold)
+{
+    if (!c || wait_ns < 0) return UCG_E_BADARG;
+    int rc = ensure_state(c);
+    if (rc) return rc;
+    UCG_CUDA(cudaSetDevice(c->device));
+    rk_drop_graph(c);   // the captured attempt reads the control block anyway; start clean
+    return rk_test_wait_timeout(c, (unsigned long long)wait_ns, hold != 0);
+}
+
 }  // extern "C"

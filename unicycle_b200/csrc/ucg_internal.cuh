@@ -32,6 +32,12 @@ struct Ctl {
     // the step that reaches it ends exactly on it (clamped marks that attempt)
     double t_stop;
     int stop_on, clamped;
+    // fault injection for tests of the bounded waits (ucg_test_wait_timeout):
+    // wait_ns != 0 replaces the 4 s limit of the traction product's waits;
+    // test_hold makes the product's first CTA issue no copies, so that its
+    // consumers wait on data that never comes and give up
+    unsigned long long wait_ns;
+    int test_hold, pad_;
 };
 
 // Device-side output recorder (the reference's export/exportPoints,
@@ -201,6 +207,7 @@ int assemble_observation(ucg_ctx *c, int okada_mode);   // O for c->obs_x (sets 
 int rk_alloc(ucg_ctx *c);
 void rk_free(ucg_ctx *c);
 int rk_odefun(ucg_ctx *c);                  // k[0] = f(y) on device, sets vmax
+int rk_test_wait_timeout(ucg_ctx *c, unsigned long long wait_ns, int hold);
 int rk_profile_traction(ucg_ctx *c, int reps, double *ms);
 void rk_enqueue_attempt(ucg_ctx *c);        // one Cash-Karp attempt + control
 void rk_enqueue_commit(ucg_ctx *c);         // copy a pending candidate into y

@@ -93,6 +93,21 @@ class Ensemble:
         dn = _d(np.broadcast_to(np.asarray(dt_next, dtype=float), (ninst,)))
         self._check(self.lib.ucg_ens_set_states(self.ens, geometry, _p(y), _p(t), _p(dn)), "set_states")
 
+    def put_states(self, geometry, y):
+        """Replace every instance's state (n_instances, 7 n) and keep its time, step
+        size, counters and step history (ucg_ens_put_states): the states taken by
+        get_states and handed back continue as the device-resident loop would."""
+        ninst = self.geoms[geometry][1]
+        y = _d(y).reshape(ninst, -1)
+        self._check(self.lib.ucg_ens_put_states(self.ens, geometry, _p(y)), "put_states")
+
+    def test_wait_timeout(self, wait_ns=0, hold=False):
+        """Fault injection for tests (ucg_ens_test_wait_timeout): with hold the dense
+        contraction's first CTA issues no copies and its MMA issuer gives up after
+        wait_ns; (0, False) restores normal operation."""
+        self._check(self.lib.ucg_ens_test_wait_timeout(self.ens, int(wait_ns), int(bool(hold))),
+                    "test_wait_timeout")
+
     def get_states(self, geometry, out=None):
         """(y (n_instances, 7 n), time, dt_next, accepted, rejected, status) of all instances."""
         npatch, ninst = self.geoms[geometry][0], self.geoms[geometry][1]

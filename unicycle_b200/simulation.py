@@ -325,6 +325,12 @@ class Simulation:
         """The context's cudaStream_t as an integer handle."""
         return self.lib.ucg_stream(self.ctx)
 
+    def test_wait_timeout(self, wait_ns=0, hold=False):
+        """Fault injection for tests (ucg_test_wait_timeout): with hold the traction
+        product's first CTA issues no copies and its consumers give up after
+        wait_ns; (0, False) restores normal operation."""
+        self._check(self.lib.ucg_test_wait_timeout(self.ctx, int(wait_ns), int(bool(hold))), "test_wait_timeout")
+
     def profile_traction(self, reps=10):
         """Mean device milliseconds of one traction-product launch."""
         ms = ctypes.c_double()
