@@ -84,6 +84,9 @@ def lib():
         L.orc_okada_stress.argtypes = [ctypes.c_int] + [ctypes.c_double] * 15 + [_dp]
         L.orc_nw15_stress.argtypes = [ctypes.c_double] * 3 + [_dp] * 3 + [ctypes.c_double] * 5 + [_dp]
         L.orc_bml17_stress.argtypes = [ctypes.c_double] * 10 + [_dp, ctypes.c_double, ctypes.c_double, _dp]
+        L.orc_bml17_stress_mindlin.argtypes = [ctypes.c_double] * 10 + [_dp, ctypes.c_double, ctypes.c_double, _dp]
+        L.orc_cuboid_grad_mindlin.argtypes = [ctypes.c_double] * 7 + [_dp, ctypes.c_double, ctypes.c_double, _dp]
+        L.orc_mindlin.argtypes = [ctypes.c_double] * 6 + [_dp]
         L.orc_okada_frames.argtypes = [ctypes.c_int] + [_dp] * 9
         L.orc_tri_frames.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _ip, _ip, _ip] + [_dp] * 4
         L.orc_vol_frames.argtypes = [ctypes.c_int] + [_dp] * 8
@@ -172,6 +175,29 @@ def bml17_stress(x, q, L, T, W, theta, eps, G, nu):
     lib().orc_bml17_stress(x[0], x[1], x[2], q[0], q[1], q[2], L, T, W, theta,
                            _ptr(_d(eps)), G, nu, _ptr(sig))
     return sig
+
+
+def bml17_stress_mindlin(x, q, L, T, W, theta, eps, G, nu):
+    """The cuboid's stress by Mindlin's point force integrated over its faces
+    (oracle/mindlin.cc), independent of the Barbot et al. closed forms."""
+    sig = np.zeros(6)
+    lib().orc_bml17_stress_mindlin(x[0], x[1], x[2], q[0], q[1], q[2], L, T, W, theta,
+                                   _ptr(_d(eps)), G, nu, _ptr(sig))
+    return sig
+
+
+def set_volume_route(route):
+    """Strain-volume sources in Mesh.build_g: 0 the closed forms (default), 1
+    Mindlin's point force over the cuboid's faces (independent route)."""
+    lib().orc_set_volume_route(int(route))
+
+
+def mindlin(x, y, z, c, G, nu):
+    """Mindlin's half-space Green's function: u[i, j] at (x, y, z) from a unit
+    force along j at (0, 0, c)."""
+    u = np.zeros(9)
+    lib().orc_mindlin(x, y, z, c, G, nu, _ptr(u))
+    return u.reshape(3, 3)
 
 
 class Mesh:

@@ -54,6 +54,11 @@ static void stress_rot(const double *sv, const double *dv, const double *nv,
     o[5] = -da * dv[0] - db * dv[1] - dc * dv[2];
 }
 
+/* 0: strain volumes by the closed forms (strainvolume.cc); 1: by Mindlin's
+   point force over the cuboid's faces (mindlin.cc), the independent route */
+static int g_volume_route = 0;
+void orc_set_volume_route(int route) { g_volume_route = route; }
+
 /* stress at x due to unit component j of source number src (global source index
    over rect, tri, vol) */
 static void source_stress(const orc_mesh *m, const double *x, long src, int j, double s[6])
@@ -82,8 +87,12 @@ static void source_stress(const orc_mesh *m, const double *x, long src, int j, d
         double eps[6] = {0, 0, 0, 0, 0, 0};
         eps[j] = 1.0;
         double nu = m->lambda / (m->lambda + m->mu) / 2.0;
-        orc_bml17_stress(x[0], x[1], x[2], m->vx[3 * i], m->vx[3 * i + 1], m->vx[3 * i + 2],
-                         m->vL[i], m->vT[i], m->vW[i], m->vstrike[i], eps, m->mu, nu, s);
+        if (g_volume_route == 1)
+            orc_bml17_stress_mindlin(x[0], x[1], x[2], m->vx[3 * i], m->vx[3 * i + 1], m->vx[3 * i + 2],
+                                     m->vL[i], m->vT[i], m->vW[i], m->vstrike[i], eps, m->mu, nu, s);
+        else
+            orc_bml17_stress(x[0], x[1], x[2], m->vx[3 * i], m->vx[3 * i + 1], m->vx[3 * i + 2],
+                             m->vL[i], m->vT[i], m->vW[i], m->vstrike[i], eps, m->mu, nu, s);
     }
 }
 

@@ -56,6 +56,18 @@ void orc_vol_frames(int ns, const double *x, const double *L, const double *W,
                     const double *strike, double *sv, double *dv, double *nv,
                     double *xc);
 
+/* ---- mindlin.cc: the same stress by Mindlin's point force integrated over the
+   cuboid's faces (independent of the closed forms above) ------------------- */
+void orc_bml17_stress_mindlin(double x1, double x2, double x3, double q1, double q2,
+                              double q3, double L, double T, double W, double theta,
+                              const double eps[6], double G, double nu, double sig[6]);
+void orc_cuboid_grad_mindlin(double x1p, double x2p, double x3, double q3, double L,
+                             double T, double W, const double eps[6], double G,
+                             double nu, double grad[9]);
+void orc_mindlin(double x, double y, double z, double c, double G, double nu, double u[9]);
+/* strain-volume sources of orc_build_g / orc_build_o: 0 closed forms, 1 Mindlin route */
+void orc_set_volume_route(int route);
+
 /* ---- greens.c ----------------------------------------------------------- */
 typedef struct {
     int nr, nt, nv;                 /* rectangles, triangles, volumes */

@@ -47,6 +47,28 @@ def test_volume_assembly_vs_oracle(ucg, oracle_lib, small_cfg3):
     sim.close()
 
 
+def test_volume_assembly_vs_mindlin_route(ucg, oracle_lib, small_cfg3):
+    """Volume-source columns against the independent route (Mindlin's point
+    force integrated over each cuboid's faces, oracle/mindlin.cc), which shares
+    no formula with the closed-form integrals the device differentiates."""
+    from unicycle_b200 import configs
+    c = small_cfg3
+    sim = ucg.Simulation(c["mu"], c["lam"], driver="viscouscycles")
+    configs.build_coupled(sim, c)
+    K = sim.copy_G()
+    sim.close()
+    M = oracle_lib.Mesh(c["mu"], c["lam"], rect=c["mesh"]["rect"], vol=c["mesh"]["vol"])
+    oracle_lib.set_volume_route(1)
+    try:
+        G = M.build_g()
+    finally:
+        oracle_lib.set_volume_route(0)
+    nf, nv = c["n_patch"], c["n_vol"]
+    err = _elem_err(K[:, 2 * nf:], G[:, 2 * nf:], [3] * nf + [6] * nv)
+    print(f"device volume columns vs Mindlin route: {err:.2e} of the receiver scale")
+    assert err < 5e-9
+
+
 def test_viscous_odefun_vs_oracle(ucg, oracle_lib, small_cfg3):
     from unicycle_b200 import configs
     c = small_cfg3

@@ -289,3 +289,142 @@ def test_bml17_thin_layer_is_a_dislocation(oracle_lib):
     s_vol = _sv(oracle_lib, x, q, L, T, W, 0.0, np.array([0, e12, 0, 0, 0, 0.0]))
     s_ok = oracle_lib.okada_stress(0, x, q, L, W, 0.0, np.pi / 2, 2 * e12 * T, 0.0, 0.0, MU, 30.0e3)
     assert np.max(np.abs(s_vol - s_ok)) < 5e-3 * np.max(np.abs(s_ok))
+
+
+def test_cfg2_rake_is_oblique_and_marches(oracle_lib):
+    """The megathrust configuration slips at an oblique rake: at exactly 90 deg
+    its strike components are rounding residue and the main loop's relative
+    error norm collapses the step size (fortran/3d/src/ratestate.f90:314-315),
+    at 60 deg the same 200-triangle model marches to its first event."""
+    from unicycle_b200 import configs
+    c = configs.cfg2(nx=10, nz=10)
+    assert abs(np.degrees(c["friction"]["rake"][0]) - configs.CFG2_RAKE_DEG) < 1e-12
+    i1, i2, i3, v = c["mesh"]["tri"]
+    G = oracle_lib.Mesh(c["mu"], c["lam"], tri=(v, i1, i2, i3)).build_g()
+
+    def march(rake_deg, nsteps):
+        fr = dict(c["friction"])
+        fr["rake"] = np.full(c["n_patch"], np.radians(rake_deg))
+        md = oracle_lib.Model(G, fr)
+        y, t, dt, rej = configs.steady_state(np.full(c["n_patch"], 0.9e-9), fr), 0.0, c["dt0"], 0
+        for _ in range(nsteps):
+            rc, t, y, _, dt, _, nr = md.step(t, y, dt, c["epsilon"])
+            assert rc == 0
+            rej += nr
+        return t / configs.YEAR, rej
+
+    t60, rej60 = march(configs.CFG2_RAKE_DEG, 100)
+    t90, rej90 = march(90.0, 100)
+    assert t60 > 1.0 and rej60 <= 5, (t60, rej60)
+    assert t90 < 1e-9 and rej90 > 100, (t90, rej90)
+
+
+# ---- Mindlin's point force and the independent cuboid route -----------------
+
+def _lame(mu, nu):
+    return 2.0 * mu * nu / (1.0 - 2.0 * nu)
+
+
+def test_mindlin_green_function(oracle_lib):
+    """Mindlin's half-space Green's function (oracle/mindlin.cc): Navier's
+    equations away from the source, a traction-free surface, the Kelvin
+    singularity at the source, and reciprocity G_ij(x; xi) = G_ji(xi; x)."""
+    G0, nu = 30.0e3, 0.25
+    lam = _lame(G0, nu)
+    c = 900.0
+
+    def u(p, cc=c):
+        return oracle_lib.mindlin(p[0], p[1], p[2], cc, G0, nu)
+
+    h = 0.5
+
+    def grad(p):
+        g = np.zeros((3, 3, 3))                       # g[i, j, d] = d u_ij / d x_d
+        for d in range(3):
+            e = np.zeros(3)
+            e[d] = h
+            g[:, :, d] = (8 * (u(p + e) - u(p - e)) - (u(p + 2 * e) - u(p - 2 * e))) / (12 * h)
+        return g
+
+    def stress(p):
+        g = grad(p)
+        s = np.zeros((3, 3, 3))                       # s[j][a, b]: force along j
+        for j in range(3):
+            eps = 0.5 * (g[:, j, :] + g[:, j, :].T)
+            s[j] = lam * np.trace(eps) * np.eye(3) + 2 * G0 * eps
+        return s
+
+    rng = np.random.default_rng(4)
+    for _ in range(5):
+        p = np.array([rng.uniform(-2e3, 2e3), rng.uniform(-2e3, 2e3), rng.uniform(200.0, 3e3)])
+        if np.linalg.norm(p - [0, 0, c]) < 300.0:
+            continue
+        # div(stress) = 0: second differences of the stress
+        hh = 2.0
+        div = np.zeros((3, 3))
+        for d in range(3):
+            e = np.zeros(3)
+            e[d] = hh
+            div += ((stress(p + e) - stress(p - e)) / (2 * hh))[:, :, d]
+        scale = np.max(np.abs(stress(p))) / np.linalg.norm(p - [0, 0, c])
+        assert np.max(np.abs(div)) < 1e-5 * scale
+    # traction-free surface: sigma_i3 = 0 at z = 0 (one-sided stencil in z)
+    for _ in range(4):
+        p = np.array([rng.uniform(-3e3, 3e3), rng.uniform(-3e3, 3e3), 0.0])
+        g = np.zeros((3, 3, 3))
+        for d in range(2):
+            e = np.zeros(3)
+            e[d] = h
+            g[:, :, d] = (8 * (u(p + e) - u(p - e)) - (u(p + 2 * e) - u(p - 2 * e))) / (12 * h)
+        f = [u(p + np.array([0, 0, k * h])) for k in range(5)]
+        g[:, :, 2] = (-25 * f[0] + 48 * f[1] - 36 * f[2] + 16 * f[3] - 3 * f[4]) / (12 * h)
+        for j in range(3):
+            eps = 0.5 * (g[:, j, :] + g[:, j, :].T)
+            s = lam * np.trace(eps) * np.eye(3) + 2 * G0 * eps
+            assert np.max(np.abs(s[:, 2])) < 1e-8 * np.max(np.abs(s)) + 1e-14
+    # Kelvin singularity: G - Kelvin stays bounded at the source
+    A = 1.0 / (16.0 * np.pi * G0 * (1.0 - nu))
+    rest = []
+    for r in (1e-1, 1e-3):
+        d = np.array([0.3, -0.5, 0.81]) / np.linalg.norm([0.3, -0.5, 0.81]) * r
+        kel = A * ((3 - 4 * nu) * np.eye(3) / r + np.outer(d, d) / r ** 3)
+        rest.append(u(np.array([0, 0, c]) + d) - kel)
+        assert np.max(np.abs(rest[-1])) < 10.0 * A / c      # the image part is O(1 / depth)
+    assert np.max(np.abs(rest[0] - rest[1])) < 1e-3 * np.max(np.abs(rest[1]))
+    # reciprocity: u_ij(x; xi) = u_ji(xi; x)
+    for _ in range(5):
+        x = rng.uniform([-2e3, -2e3, 100.0], [2e3, 2e3, 3e3])
+        xi = rng.uniform([-2e3, -2e3, 100.0], [2e3, 2e3, 3e3])
+        a = oracle_lib.mindlin(x[0] - xi[0], x[1] - xi[1], x[2], xi[2], G0, nu)
+        b = oracle_lib.mindlin(xi[0] - x[0], xi[1] - x[1], xi[2], x[2], G0, nu)
+        assert np.max(np.abs(a - b.T)) < 1e-12 * np.max(np.abs(a))
+
+
+@pytest.mark.parametrize("region", ["inside", "near", "far", "surface"])
+def test_bml17_closed_forms_match_mindlin_route(oracle_lib, region):
+    """The Barbot et al. closed forms (numerically differentiated, x87) against
+    the independent Mindlin route (point force over the faces, exact
+    derivatives): every eigenstrain component, receivers inside the cuboid,
+    next to it (within 0.3 of its size of a face), far from it and on the free
+    surface.  Measured: 8e-11 inside, 1e-8 near, 7e-11 far, 2e-11 surface."""
+    q = np.array([1000.0, -500.0, 3000.0])
+    L, T, W, th = 2000.0, 1500.0, 1800.0, 0.3
+    ct, st = np.cos(th), np.sin(th)
+    rng = np.random.default_rng({"inside": 1, "near": 2, "far": 3, "surface": 4}[region])
+    tol = {"inside": 1e-9, "near": 5e-8, "far": 1e-9, "surface": 1e-9}[region]
+    for _ in range(6):
+        if region == "inside":
+            f = (rng.uniform(0.1 * L, 0.9 * L), rng.uniform(-0.4 * T, 0.4 * T), rng.uniform(q[2] + 0.1 * W, q[2] + 0.9 * W))
+        elif region == "near":
+            f = (rng.uniform(-0.3 * L, 1.3 * L), rng.choice([-1, 1]) * rng.uniform(0.55 * T, 0.8 * T),
+                 rng.uniform(q[2] - 0.3 * W, q[2] + 1.3 * W))
+        elif region == "far":
+            f = (rng.uniform(-5 * L, 6 * L), rng.uniform(-5 * T, 5 * T), rng.uniform(0.0, q[2] + 5 * W))
+        else:
+            f = (rng.uniform(-3 * L, 4 * L), rng.uniform(-3 * T, 3 * T), 0.0)
+        x = np.array([q[0] + f[0] * ct - f[1] * st, q[1] + f[0] * st + f[1] * ct, f[2]])
+        for k in range(6):
+            eps = np.eye(6)[k] * 1e-6
+            a = oracle_lib.bml17_stress(x, q, L, T, W, th, eps, MU, NU)
+            b = oracle_lib.bml17_stress_mindlin(x, q, L, T, W, th, eps, MU, NU)
+            assert np.max(np.abs(a - b)) <= tol * np.max(np.abs(b)), (region, k, a, b)
