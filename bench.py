@@ -55,7 +55,10 @@ def parse():
     p.add_argument("--nz", type=int, default=100, help="down-dip rows")
     p.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16"])
     p.add_argument("--workload", default="all",
-                   choices=["all", "ensemble", "plain", "split", "coupled", "cfg4", "hmatrix", "hens"])
+                   choices=["all", "ensemble", "plain", "split", "coupled", "cfg3", "cfg4", "hmatrix", "hens"])
+    p.add_argument("--cfg3-size", default="64,64,32,16,16",
+                   help="cfg3 workload: fault nx,nz and volume nx,ny,nz (full size: 4,096 + 8,192)")
+    p.add_argument("--cfg3-steps", type=int, default=2000, help="cfg3 workload: accepted steps per precision")
     p.add_argument("--coupled-size", default="64,64,16,8,8",
                    help="coupled assembly leg: fault nx,nz and volume nx,ny,nz")
     p.add_argument("--sets", type=int, default=N_SETS, help="instances in the ensemble workload")
@@ -393,6 +396,101 @@ def assembly_leg(args, local):
     return {"model": f"{nf} rectangles + {nv} cuboids (K {m} x {n})",
             "okada_rect": {"entries": m * 2 * nf, "ms": rect_ms, "mentries_per_s": m * 2 * nf / rect_ms / 1e3},
             "bml17_vol": {"entries": m * 6 * nv, "ms": vol_ms, "mentries_per_s": m * 6 * nv / vol_ms / 1e3}}
+
+
+def run_cfg3(args, world, rank, local):
+    """The coupled configuration at full size: 4,096 rectangular fault patches and
+    8,192 cuboids (K 61,440 x 57,344, 28 GB in FP64), linear Maxwell volumes,
+    a 5 m uniform coseismic strike slip applied on the device at t = 0 (K u), then
+    postseismic relaxation towards 50 years with the plain FP64 path and with
+    the split-BF16 K (anchored stages).  Assembly is timed per source family
+    (fault columns: fault-fault and fault-volume blocks; volume columns:
+    volume-fault and volume-volume blocks)."""
+    import torch
+    import unicycle_b200
+    from unicycle_b200 import configs
+    torch.cuda.set_device(local)
+    nxf, nzf, nxv, nyv, nzv = (int(v) for v in args.cfg3_size.split(","))
+    c = configs.cfg3(nxf=nxf, nzf=nzf, nxv=nxv, nyv=nyv, nzv=nzv)
+    nf, nv = c["n_patch"], c["n_vol"]
+    sim = unicycle_b200.Simulation(c["mu"], c["lam"], driver="viscouscycles", device=local)
+    t0 = time.perf_counter()
+    configs.build_coupled(sim, c)
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t0
+    rect_ms, _, vol_ms = sim.assembly_times()
+    n, m = sim.dims
+    fam = {"okada_rect_columns": {"entries": m * 2 * nf, "ms": rect_ms, "mentries_per_s": m * 2 * nf / rect_ms / 1e3,
+                                  "blocks": "fault-fault + fault-volume"},
+           "bml17_vol_columns": {"entries": m * 6 * nv, "ms": vol_ms, "mentries_per_s": m * 6 * nv / vol_ms / 1e3,
+                                 "blocks": "volume-fault + volume-volume"},
+           "total_seconds_incl_host": t_build}
+    slip = np.zeros((nf, 2))
+    slip[:, 0] = c["coseismic_slip"]
+    sim.set_state(c["y0"], 0.0, c["dt0"])
+    sim.apply_perturbation(slip=slip)
+    y_pre = sim.get_state()[0]
+    stream = torch.cuda.ExternalStream(sim.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    peak, peak_kind = load_peaks()
+    t_end = c["t_end"]
+    legs = {}
+    for prec in ("fp64", "split_bf16"):
+        sim.set_precision(prec)
+        sim.set_state(y_pre, 0.0, c["dt0"])
+        sim.run(t_end, args.warmup)
+        _, tw, _, aw, rw = sim.get_state()
+        torch.cuda.synchronize()
+        with Clocks(local) as clk:
+            e0.record(stream)
+            steps = sim.run(t_end, args.cfg3_steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        el = e0.elapsed_time(e1) / 1e3
+        y, tt, _, at, rt = sim.get_state()
+        ms_mv = sim.profile_traction(reps=5)
+        if prec == "fp64":
+            alg = 8.0 * m * n + 8.0 * (n + m)
+        else:
+            alg = 2.0 * m * n + 4.0 * m + 8.0 * (n + m)
+        legs[prec] = {"steps": steps, "steps_per_s": steps / el, "ms_per_step": 1e3 * el / max(1, steps),
+                      "sim_years": (tt - tw) / YEAR, "reached_years": tt / YEAR,
+                      "sim_years_per_hour": (tt - tw) / YEAR / (el / 3600.0), "rejected_attempts": rt - rw,
+                      "roofline": {"bound": "hbm", "ms_per_launch": ms_mv, "bytes_per_launch": alg,
+                                   "achieved": alg / (ms_mv / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                                   "frac": alg / (ms_mv / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+                                   "kernel": "k_traction<S,double>" if prec == "fp64" else
+                                   "k_traction<S,bf16> (hi plane x increments)"},
+                      "clocks": clk.summary(), "final_state_finite": bool(np.all(np.isfinite(y)))}
+    # split product error against FP64 on the preloaded state
+    sim.set_precision("fp64")
+    d64, _ = sim.odefun(y_pre)
+    sim.set_precision("split_bf16")
+    dsp, _ = sim.odefun(y_pre)
+    sim.set_precision("fp64")
+    idx_f = np.concatenate([np.arange(q, 7 * nf, 7) for q in (2, 3, 4)])
+    vol = np.arange(7 * nf, len(y_pre)).reshape(-1, 12)[:, 6:].ravel()
+    legs["split_bf16"]["rhs_max_rel_error_vs_fp64"] = {
+        "fault_traction_rates": float(np.max(np.abs(dsp[idx_f] - d64[idx_f])) / np.max(np.abs(d64[idx_f]))),
+        "volume_stress_rates": float(np.max(np.abs(dsp[vol] - d64[vol])) / np.max(np.abs(d64[vol])))}
+    sim.close()
+    if rank != 0:
+        return None
+    p64 = legs["fp64"]
+    return {"metric": "simulated years/hour, coupled fault + strain volumes (plain FP64)",
+            "value": world * p64["sim_years_per_hour"], "unit": "sim-yr/hr", "n_gpus": world,
+            "steps": p64["steps"], "warmup": args.warmup, "ms_per_step": p64["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded cfg3: viscosity log-uniform 1e18-1e20 Pa s)",
+            "config": {"workload": f"{nf} Okada rectangles + {nv} cuboids, linear Maxwell, 5 m coseismic preload, "
+                                   f"relaxation towards {t_end / YEAR:.0f} yr", "K_shape": [m, n],
+                       "K_gb_fp64": 8.0 * m * n / 1e9, "rtol": c["epsilon"],
+                       "l2": "inputs larger than L2 (K %.1f GB)" % (8.0 * m * n / 1e9)},
+            "assembly": fam, "plain_fp64": p64, "split_bf16": legs["split_bf16"],
+            "speedup_split_vs_fp64": {"steps_per_s": legs["split_bf16"]["steps_per_s"] / p64["steps_per_s"],
+                                      "sim_years_per_hour": legs["split_bf16"]["sim_years_per_hour"] /
+                                      max(1e-300, p64["sim_years_per_hour"])},
+            "roofline": p64["roofline"], "clocks": p64["clocks"], "gpu_launches": None}
 
 
 def run_cfg4(args, world, rank, local):
@@ -1130,6 +1228,8 @@ def main():
         out = run_ensemble(args, world, rank, local)
     elif args.workload == "cfg4":
         out = run_cfg4(args, world, rank, local)
+    elif args.workload == "cfg3":
+        out = run_cfg3(args, world, rank, local)
     elif args.workload == "hmatrix":
         out = run_hmatrix(args, world, rank, local)
     elif args.workload == "hens":

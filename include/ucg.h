@@ -450,10 +450,17 @@ int ucg_ens_get_states(ucg_ensemble *ens, int geometry, double *y, double *time,
    fortran/3d/src/ratestate.f90:307-326).  No reference counterpart. */
 int ucg_ens_put_states(ucg_ensemble *ens, int geometry, const double *y);
 
+/* Precision of the stage increments (stages 2-6 contract v_s - v1): terms = 2,
+   the default, Khi (Vhi + Vlo) over pairs of M-tiles (half the matrix bytes of
+   the anchor); terms = 3, the anchor's form Khi Vhi + Khi Vlo + Klo Vhi with
+   its FP32 sums cut into pieces of at most 16,384 sources.  No reference
+   counterpart. */
+int ucg_ens_set_increment_terms(ucg_ensemble *ens, int terms);
+
 /* Fault injection for testing the bounded device waits (no reference
    counterpart).  wait_ns > 0 replaces the 4 s limit of the dense contraction's
-   data waits; hold != 0 makes its first CTA issue no copies, so that the MMA
-   issuer waits on data that never comes and gives up: ucg_ens_run (and
+   data waits; hold != 0 makes the CTA that owns the first work segment issue
+   no copies, so that its MMA issuer waits on data that never comes and gives up: ucg_ens_run (and
    ucg_ens_matvec) then return UCG_E_TIMEOUT, the instances' stage kernels skip
    the attempt, and the ensemble stays usable after ucg_ens_test_wait_timeout(ens,
    0, 0) and fresh states. */

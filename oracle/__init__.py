@@ -186,6 +186,12 @@ def bml17_stress_mindlin(x, q, L, T, W, theta, eps, G, nu):
     return sig
 
 
+def set_dgemv_threads(threads):
+    """odefun's DGEMV over `threads` threads in a plain summation order (timing
+    the CPU baseline); 0 restores the fixed order the parity tests use."""
+    lib().orc_set_dgemv_threads(int(threads))
+
+
 def set_volume_route(route):
     """Strain-volume sources in Mesh.build_g: 0 the closed forms (default), 1
     Mindlin's point force over the cuboid's faces (independent route)."""

@@ -104,6 +104,9 @@ typedef struct {
 } orc_model;
 
 long orc_state_len(const orc_model *md);
+/* odefun's DGEMV: threads > 0 runs the columns over that many threads with a
+   plain summation order (timing the CPU baseline); 0 (default) the fixed order */
+void orc_set_dgemv_threads(int threads);
 /* one DGEMV dot product in the fixed summation order documented in ratestate.c */
 double orc_dot_fixed_order(const double *col, const double *v, long n);
 void orc_init_state(const orc_model *md, double *y);

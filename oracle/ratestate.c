@@ -36,6 +36,11 @@ long orc_state_len(const orc_model *md) { return 7L * md->np + 12L * md->nvol; }
  * multiply-adds; the 32 slots of a group combine by an xor butterfly
  * (distance 16, 8, 4, 2, 1) and the 8 groups are added in order.
  */
+/* > 0: odefun's DGEMV runs over this many threads in a plain summation order
+   (for timing the CPU baseline); 0: the fixed order below (parity) */
+static int g_dgemv_threads = 0;
+void orc_set_dgemv_threads(int threads) { g_dgemv_threads = threads > 0 ? threads : 0; }
+
 double orc_dot_fixed_order(const double *col, const double *v, long n)
 {
     double part[8];
@@ -132,9 +137,31 @@ void orc_odefun(const orc_model *md, const double *y, double *dydt, double *vmax
         for (int k = 0; k < 6; k++) v[2L * md->np + 6L * i + k] = e[k] - md->ebg[6L * i + k];
     }
     /* step 2/3: t = G^T v (DGEMV "T"), column k is contiguous */
-    for (long k = 0; k < m; k++) {
-        if (!md->G) { t[k] = 0.0; continue; }
-        t[k] = orc_dot_fixed_order(md->G + k * n, v, n);
+    if (md->G && g_dgemv_threads > 0) {
+        /* timing mode: the columns over threads, each a plain sequential dot
+           (the reference leaves the order to its BLAS) */
+        const double *G = md->G;
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(g_dgemv_threads) schedule(static)
+#endif
+        for (long k = 0; k < m; k++) {
+            const double *col = G + k * n;
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            long c = 0;
+            for (; c + 4 <= n; c += 4) {
+                s0 += col[c] * v[c];
+                s1 += col[c + 1] * v[c + 1];
+                s2 += col[c + 2] * v[c + 2];
+                s3 += col[c + 3] * v[c + 3];
+            }
+            for (; c < n; c++) s0 += col[c] * v[c];
+            t[k] = (s0 + s1) + (s2 + s3);
+        }
+    } else {
+        for (long k = 0; k < m; k++) {
+            if (!md->G) { t[k] = 0.0; continue; }
+            t[k] = orc_dot_fixed_order(md->G + k * n, v, n);
+        }
     }
     /* step 3/3: remaining state rates */
     for (int i = 0; i < md->np; i++) {

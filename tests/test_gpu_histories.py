@@ -22,7 +22,8 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-NSTEPS = 1000
+NSTEPS = 1000            # the first 1,000 accepted steps ...
+NRUN = 1400              # ... and beyond, so that every form reaches the event
 V_QUIET = 1.0e-7          # pointwise window: max V below 100 Vpl
 V_EVENT = 1.0e-5          # onset: first accepted step with max V at or above this
 
@@ -64,23 +65,32 @@ def _onset(ts, ys):
 
 
 def _compare(name, ref, ts, ys):
-    quiet = {"v": 0.0, "th": 0.0, "n": 0}
-    whole = {"v": 0.0, "th": 0.0}
+    """Errors of log10 V and log10 theta against the oracle at the form's accepted
+    times, max over patches, in windows that end where the oracle's max V first
+    reaches 2, 10 and 100 Vpl (loading, then nucleation: the pointwise window
+    ends before the event because a shift of the onset by a fraction of a
+    second moves V by orders of magnitude there), and over the whole run."""
+    marks = {"2Vpl": 2e-9, "10Vpl": 1e-8, "100Vpl": V_QUIET}
+    t_end = {}
+    for k, vth in marks.items():
+        hit = [t for t, y in zip(ref.t, ref.y) if 10.0 ** np.max(y[6::7]) >= vth]
+        t_end[k] = hit[0] if hit else np.inf
+    win = {k: {"v": 0.0, "th": 0.0, "n": 0} for k in list(marks) + ["whole"]}
     for t, y in zip(ts, ys):
         r = ref.at(t)
         ev = np.max(np.abs(y[6::7] - r[6::7]) / np.abs(r[6::7]))
         et = np.max(np.abs(y[5::7] - r[5::7]) / np.abs(r[5::7]))
-        whole["v"], whole["th"] = max(whole["v"], ev), max(whole["th"], et)
-        if 10.0 ** np.max(r[6::7]) < V_QUIET:
-            quiet["v"], quiet["th"] = max(quiet["v"], ev), max(quiet["th"], et)
-            quiet["n"] += 1
+        for k in win:
+            if k == "whole" or t < t_end[k]:
+                w = win[k]
+                w["v"], w["th"], w["n"] = max(w["v"], ev), max(w["th"], et), w["n"] + 1
     o_ref = _onset(ref.t, ref.y)
     o = _onset(ts, ys)
     d_on = abs(o - o_ref) / o_ref if (o is not None and o_ref is not None) else None
-    print(f"{name:>22}: {len(ts)} steps to t = {ts[-1]:.6e} s; quiet window ({quiet['n']} steps) "
-          f"log10 V {quiet['v']:.2e}, log10 theta {quiet['th']:.2e}; whole run {whole['v']:.2e} / "
-          f"{whole['th']:.2e}; onset {o} vs {o_ref} (rel {d_on})")
-    return quiet, whole, d_on
+    txt = "; ".join(f"{k} ({w['n']}) {w['v']:.1e}/{w['th']:.1e}" for k, w in win.items())
+    print(f"{name:>24}: {len(ts)} steps to t = {ts[-1]:.6e} s; log10 V / log10 theta errors: {txt}; "
+          f"onset rel {d_on}")
+    return win, d_on
 
 
 def _single(sim, c, nsteps):
@@ -131,29 +141,31 @@ def setup(ucg, oracle_lib):
     configs.build(sim, c)
     sim.set_tolerance(c["epsilon"])
     G = sim.copy_G()
-    ref = _Reference(oracle_lib, G, c, int(1.6 * NSTEPS))
+    ref = _Reference(oracle_lib, G, c, 2 * NRUN)
     yield c, sim, ref
     sim.close()
 
 
-def _check(name, ref, ts, ys, quiet_tol, onset_tol):
-    quiet, whole, d_on = _compare(name, ref, ts, ys)
-    assert quiet["n"] > 100
-    assert quiet["v"] <= quiet_tol and quiet["th"] <= quiet_tol, (name, quiet)
-    assert d_on is not None and d_on <= onset_tol, (name, d_on)
+def _check(name, ref, ts, ys, tol, onset_tol, window="10Vpl"):
+    win, d_on = _compare(name, ref, ts, ys)
+    w = win[window]
+    assert w["n"] > 100
+    assert w["v"] <= tol and w["th"] <= tol, (name, window, w)
+    if onset_tol is not None:
+        assert d_on is not None and d_on <= onset_tol, (name, d_on)
 
 
 def test_history_plain_fp64(ucg, setup):
     c, sim, ref = setup
     sim.set_precision(ucg.UCG_PREC_FP64)
-    ts, ys = _single(sim, c, NSTEPS)
+    ts, ys = _single(sim, c, NRUN)
     _check("plain FP64", ref, ts, ys, 1e-9, 1e-6)
 
 
 def test_history_split_bf16(ucg, setup):
     c, sim, ref = setup
     sim.set_precision(ucg.UCG_PREC_SPLIT_BF16)
-    ts, ys = _single(sim, c, NSTEPS)
+    ts, ys = _single(sim, c, NRUN)
     sim.set_precision(ucg.UCG_PREC_FP64)
     _check("split-BF16", ref, ts, ys, 1e-6, 1e-5)
 
@@ -161,7 +173,7 @@ def test_history_split_bf16(ucg, setup):
 def test_history_dense_ensemble(ucg, setup):
     c, sim, ref = setup
     sim.set_precision(ucg.UCG_PREC_FP64)
-    ts, ys = _ensemble(ucg, sim, c, NSTEPS)
+    ts, ys = _ensemble(ucg, sim, c, NRUN)
     _check("ensemble (tensor cores)", ref, ts, ys, 1e-6, 1e-5)
 
 
@@ -171,10 +183,10 @@ def test_history_hmatrix(ucg, setup):
     for prec, name in ((ucg.UCG_PREC_HMATRIX, "hierarchical FP64"),
                        (ucg.UCG_PREC_HMATRIX_SPLIT, "hierarchical split")):
         sim.set_precision(prec)
-        ts, ys = _single(sim, c, NSTEPS)
+        ts, ys = _single(sim, c, NRUN)
         _check(name, ref, ts, ys, 1e-6, 1e-5)
     sim.set_precision(ucg.UCG_PREC_HMATRIX)
-    ts, ys = _ensemble(ucg, sim, c, NSTEPS)
+    ts, ys = _ensemble(ucg, sim, c, NRUN)
     _check("hierarchical ensemble", ref, ts, ys, 1e-6, 1e-5)
     sim.set_precision(ucg.UCG_PREC_FP64)
 
@@ -206,6 +218,6 @@ def test_history_learned_step(ucg, setup):
     m = ucg.StepModel(seed=1)
     m.set_data(x, y)
     m.train(epochs=20, batch=2048, lr=1e-3)
-    ts, ys = _ensemble(ucg, sim, c, NSTEPS, model=m)
+    ts, ys = _ensemble(ucg, sim, c, NRUN, model=m)
     m.close()
     _check("ensemble + learned step", ref, ts, ys, 1e-6, 1e-5)

@@ -151,9 +151,10 @@ struct EnsGlobal {
     unsigned long long trace_cap, trace_n;
     // fault injection for tests of the bounded waits (ucg_ens_test_wait_timeout):
     // wait_ns != 0 replaces the 4 s limit of the dense contraction's data waits;
-    // test_hold makes its first CTA issue no copies
+    // test_hold makes the CTA owning the first segment issue no copies
     unsigned long long wait_ns;
     int test_hold;
+    int inc_full;               // stages 2-6 contracted in the anchor's three-term form
 };
 
 // one trace record: the 11 model inputs at an acceptance, then log10 of the
@@ -307,8 +308,9 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
 {
     int *err = &gl->err;
     const unsigned long long lim = gl->wait_ns ? gl->wait_ns : TIMEOUT_NS;
-    // (test_hold: the first CTA issues no copies, its MMA issuer's wait runs out)
-    const bool hold = gl->test_hold && blockIdx.x == 0;
+    // (test_hold: the CTA that owns the first segment issues no copies, its MMA
+    // issuer's wait runs out; a small plan leaves some CTAs without segments)
+    const bool hold = gl->test_hold && cta_seg[blockIdx.x] == 0 && cta_seg[blockIdx.x + 1] > 0;
     using T = Tile<NI, KLO, MT>;
     extern __shared__ unsigned char dyn_smem[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dyn_smem) + 1023) & ~(uintptr_t)1023);
@@ -1314,7 +1316,7 @@ __global__ void __launch_bounds__(EW_THREADS, 12) k_ens_rhs(const EnsArgs *__res
         double t[3];
         double *t1 = G.t1 + (long)i * 3 * G.np + 3L * e;
         for (int q = 0; q < 3; q++) {
-            const double inc = traction_row(A, G, i, 3L * e + q, S > 1);
+            const double inc = traction_row(A, G, i, 3L * e + q, S > 1 && !A->glob->inc_full);
             if (S == 1) {
                 t1[q] = inc;
                 t[q] = inc;
@@ -1665,6 +1667,7 @@ struct ucg_ensemble {
     EnsGlobal *h_glob = nullptr;   // pinned
     cudaGraphExec_t graph = nullptr;
     bool use_graph = true;     // false: attempts launched one by one from the host
+    bool inc_full = false;     // stage increments: three-term form (Khi Vhi + Khi Vlo + Klo Vhi)
     long launches = 0;
 };
 
@@ -2544,7 +2547,7 @@ template <int S>
 cudaError_t enqueue_stage(ucg_ensemble *E, int be)
 {
     k_ens_prologue<S><<<be, EW_THREADS, 0, E->stream>>>(E->d_args);
-    cudaError_t e = launch_all(E, S == 1);
+    cudaError_t e = launch_all(E, S == 1 || E->inc_full);
     if (e != cudaSuccess) return e;
     k_ens_rhs<S><<<be, EW_THREADS, 0, E->stream>>>(E->d_args);
     E->launches += 2;
@@ -2858,6 +2861,19 @@ int ucg_ens_set_states(ucg_ensemble *E, int gi, const double *y, const double *t
     }
     ECUDA(cudaMemcpyAsync(g.ctl, x.data(), sizeof(InstCtl) * g.ninst, cudaMemcpyHostToDevice, E->stream));
     ECUDA(cudaStreamSynchronize(E->stream));
+    return UCG_OK;
+}
+
+int ucg_ens_set_increment_terms(ucg_ensemble *E, int terms)
+{
+    if (!E || (terms != 2 && terms != 3)) return E ? ebad(E, UCG_E_BADARG, "terms must be 2 or 3") : UCG_E_BADARG;
+    ECUDA(cudaSetDevice(E->device));
+    ECUDA(cudaStreamSynchronize(E->stream));
+    E->inc_full = terms == 3;
+    E->h_glob->inc_full = E->inc_full ? 1 : 0;
+    ECUDA(cudaMemcpy(&E->d_glob->inc_full, &E->h_glob->inc_full, sizeof(int), cudaMemcpyHostToDevice));
+    if (E->graph) cudaGraphExecDestroy(E->graph);   // the launches differ: capture again
+    E->graph = nullptr;
     return UCG_OK;
 }
 

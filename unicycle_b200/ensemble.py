@@ -101,6 +101,11 @@ class Ensemble:
         y = _d(y).reshape(ninst, -1)
         self._check(self.lib.ucg_ens_put_states(self.ens, geometry, _p(y)), "put_states")
 
+    def set_increment_terms(self, terms):
+        """Stage increments in the two-term form Khi (Vhi + Vlo) (2, the default) or
+        the anchor's three-term form (3) (ucg_ens_set_increment_terms)."""
+        self._check(self.lib.ucg_ens_set_increment_terms(self.ens, int(terms)), "set_increment_terms")
+
     def test_wait_timeout(self, wait_ns=0, hold=False):
         """Fault injection for tests (ucg_ens_test_wait_timeout): with hold the dense
         contraction's first CTA issues no copies and its MMA issuer gives up after
