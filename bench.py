@@ -55,7 +55,7 @@ def parse():
     p.add_argument("--nz", type=int, default=100, help="down-dip rows")
     p.add_argument("--precision", default="fp64", choices=["fp64", "split_bf16"])
     p.add_argument("--workload", default="all",
-                   choices=["all", "ensemble", "plain", "split", "coupled", "cfg3", "cfg4", "hmatrix", "hens"])
+                   choices=["all", "ensemble", "plain", "split", "coupled", "cfg1", "cfg3", "cfg4", "hmatrix", "hens"])
     p.add_argument("--cfg3-size", default="64,64,32,16,16",
                    help="cfg3 workload: fault nx,nz and volume nx,ny,nz (full size: 4,096 + 8,192)")
     p.add_argument("--cfg3-steps", type=int, default=2000, help="cfg3 workload: accepted steps per precision")
@@ -396,6 +396,89 @@ def assembly_leg(args, local):
     return {"model": f"{nf} rectangles + {nv} cuboids (K {m} x {n})",
             "okada_rect": {"entries": m * 2 * nf, "ms": rect_ms, "mentries_per_s": m * 2 * nf / rect_ms / 1e3},
             "bml17_vol": {"entries": m * 6 * nv, "ms": vol_ms, "mentries_per_s": m * 6 * nv / vol_ms / 1e3}}
+
+
+def run_cfg1(args, world, rank, local):
+    """The reference's own small configuration run in full: 512 Okada rectangles
+    on a vertical strike-slip fault, 300 simulated years, plain FP64 on the
+    device (ucg_run, the state resident), with accepted / rejected counts."""
+    import torch
+    import unicycle_b200
+    from unicycle_b200 import configs
+    torch.cuda.set_device(local)
+    c = configs.cfg1()
+    sim = unicycle_b200.Simulation(c["mu"], c["lam"], device=local)
+    configs.build(sim, c)
+    sim.set_tolerance(c["epsilon"])
+    sim.set_state(c["y0"], 0.0, c["dt0"])
+    stream = torch.cuda.ExternalStream(sim.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0.record(stream)
+        steps = 0
+        while True:
+            k = sim.run(c["t_end"], 1 << 20)
+            steps += k
+            _, t, _, acc, rej = sim.get_state()
+            if t >= c["t_end"] or k == 0:
+                break
+        e1.record(stream)
+        torch.cuda.synchronize()
+    el = reduce_max(e0.elapsed_time(e1) / 1e3, world, args)
+    sim.close()
+    if rank != 0:
+        return None
+    return {"metric": "RK45 steps/s, cfg1 full run (512 rectangles, 300 yr, plain FP64)", "value": world * acc / el,
+            "unit": "steps/s", "n_gpus": world, "steps": int(acc), "warmup": 0, "ms_per_step": 1e3 * el / acc,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded cfg1: lognormal initial slip rate, seed 1)",
+            "config": {"workload": "cfg1 vertical strike-slip fault, 32 x 16 Okada rectangles, rtol 1e-8, 300 yr, "
+                                   "full run", "rtol": c["epsilon"]},
+            "sim_years": t / YEAR, "sim_years_per_hour": t / YEAR / (el / 3600.0), "accepted": int(acc),
+            "rejected": int(rej), "seconds": el, "clocks": clk.summary()}
+
+
+def run_reference_cfg1(args):
+    """cfg1 in full on the host cores: the oracle restatement of the reference
+    main loop (ratestate.f90:307-326 with RKQSm), its DGEMV over all threads."""
+    import oracle
+    from unicycle_b200 import configs
+    c = configs.cfg1()
+    threads = os.cpu_count() or 1
+    oracle.build(ref=False)
+    t0 = time.perf_counter()
+    G = oracle.build_g_omp(oracle.Mesh(c["mu"], c["lam"], rect=c["mesh"]["rect"]), 0, 3 * c["n_patch"], threads)
+    t_asm = time.perf_counter() - t0
+    oracle.set_dgemv_threads(threads)
+    md = oracle.Model(G, c["friction"])
+    y, t, dt = c["y0"].copy(), 0.0, c["dt0"]
+    acc = rej = 0
+    limit = args.cpu_seconds if args.cpu_seconds > 0 else float("inf")
+    t0 = time.perf_counter()
+    while t < c["t_end"] and time.perf_counter() - t0 < limit:
+        rc, t, y, _, dt, _, nr = md.step(t, y, dt, c["epsilon"])
+        if rc:
+            break
+        acc += 1
+        rej += nr
+    el = time.perf_counter() - t0
+    oracle.set_dgemv_threads(0)
+    full = t >= c["t_end"]
+    rate = acc / el
+    sample = ("full run: 300 simulated years" if full else f"first {t / YEAR:.2f} of 300 simulated years "
+              f"({el:.0f} s cap)") + f", {acc} accepted / {rej} rejected steps; assembly {t_asm:.2f} s"
+    return {"metric": "RK45 steps/s, cfg1 full run (512 rectangles, 300 yr, plain FP64)", "value": rate,
+            "unit": "steps/s", "n_gpus": args.gpus, "steps": acc, "warmup": 0, "ms_per_step": 1e3 / rate,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded cfg1: lognormal initial slip rate, seed 1)", "impl": "reference",
+            "config": {"workload": "cfg1 vertical strike-slip fault, 32 x 16 Okada rectangles, rtol 1e-8, 300 yr, "
+                                   "full run", "rtol": c["epsilon"]},
+            "sim_years": t / YEAR, "sim_years_per_hour": t / YEAR / (el / 3600.0), "accepted": acc, "rejected": rej,
+            "seconds": el,
+            "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def run_cfg3(args, world, rank, local):
@@ -1222,7 +1305,9 @@ def headline_line(ens_line, plain):
 def main():
     args = parse()
     world, rank, local = dist_init(args)
-    if args.impl == "reference":
+    if args.impl == "reference" and args.workload == "cfg1":
+        out = run_reference_cfg1(args) if rank == 0 else None
+    elif args.impl == "reference":
         out = run_reference(args, world, rank)
     elif args.workload in ("all", "ensemble"):
         out = run_ensemble(args, world, rank, local)
@@ -1230,6 +1315,8 @@ def main():
         out = run_cfg4(args, world, rank, local)
     elif args.workload == "cfg3":
         out = run_cfg3(args, world, rank, local)
+    elif args.workload == "cfg1":
+        out = run_cfg1(args, world, rank, local)
     elif args.workload == "hmatrix":
         out = run_hmatrix(args, world, rank, local)
     elif args.workload == "hens":

@@ -113,5 +113,8 @@ def test_learned_proposal_on_held_out_runs(ucg):
     print("onset rel diff", np.abs(ol - op) / op)
     assert np.all(op > 0) and np.all(ol > 0)
     assert np.all(np.abs(ol - op) <= 1e-3 * op)
+    # what the trained network gains: fewer attempts for the same simulated time
+    # (measured 1.16-1.20x on these seeds; the embedded estimate still judges)
+    assert np.sum(ap + rp) >= 1.05 * np.sum(al + rl)
     m.close()
     sim.close()

@@ -113,6 +113,15 @@ struct Tile {
     }
     static constexpr uint32_t IDESC = idesc(NI);
     static constexpr uint32_t IDESC2 = idesc(2 * NI);
+    // KDRAIN: every k-block's products go into a fresh accumulator that the
+    // drain warps add, in FP32 with round-to-nearest, into per-thread register
+    // sums (MT NI of them).  The tensor core's own FP32 accumulation truncates
+    // at every addition; over a whole segment (hundreds of k-blocks) that bias
+    // grows with the segment length and sits in every stage rate, where the
+    // embedded error estimate cannot tell it from truncation error and shrinks
+    // the step.  Drained per k-block it covers 4 MMAs only.  Off where the
+    // register sums would not fit (128 instances x 2 M-tiles).
+    static constexpr bool KDRAIN = MT * NI <= 128;
 };
 
 // byte offset of element (r, k) in a 128-byte-swizzled tile image with 128-byte rows
@@ -300,6 +309,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t r[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 // ---- the contraction ---------------------------------------------------------------
 
 template <int NI, bool KLO, int MT>
@@ -393,15 +412,28 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
             for (int q = q0; q < q1 && !abort_flag; q++, tc++) {
                 const GemmSeg sg = segs[q];
                 const int nt = (MT == 2 && tiles[sg.tile].a1 != nullptr) ? 2 : 1;
-                const int buf = tc & 1;
-                const uint32_t use = (uint32_t)(tc >> 1);
-                if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag, lim)) {
-                    if (!abort_flag) fail();
-                    break;
+                int buf = tc & 1;
+                uint32_t use = (uint32_t)(tc >> 1);
+                if (!T::KDRAIN) {
+                    if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag, lim)) {
+                        if (!abort_flag) fail();
+                        break;
+                    }
+                    tc_fence_after();
                 }
-                tc_fence_after();
                 bool ok = true;
                 for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
+                    if (T::KDRAIN) {
+                        // one accumulator per k-block, alternating between the two sets
+                        buf = (int)(it & 1);
+                        use = (uint32_t)(it >> 1);
+                        if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag, lim)) {
+                            if (!abort_flag) fail();
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                    }
                     const int s = (int)(it % T::STAGES);
                     const uint32_t ph = (uint32_t)((it / T::STAGES) & 1);
                     if (!bar_wait(&full[s], ph, &abort_flag, lim)) {
@@ -415,7 +447,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
 #pragma unroll
                     for (int j = 0; j < BK / 16; j++) {
                         const uint64_t bhi = sw128_desc(b + 32u * j), blo = sw128_desc(b + T::B_HALF + 32u * j);
-                        const uint32_t acc = (kb > sg.kb0 || j > 0) ? 1u : 0u;
+                        const uint32_t acc = ((!T::KDRAIN && kb > sg.kb0) || j > 0) ? 1u : 0u;
 #pragma unroll
                         for (int u = 0; u < MT; u++) {
                             if (u < nt) {
@@ -436,9 +468,10 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                     }
                     issued_any = true;
                     mma_commit(&empty[s]);   // frees the stage once these MMAs have read it
+                    if (T::KDRAIN) mma_commit(&acc_full[buf]);
                 }
                 if (!ok) break;
-                mma_commit(&acc_full[buf]);
+                if (!T::KDRAIN) mma_commit(&acc_full[buf]);
             }
             // no MMA may be in flight when the tensor memory is released
             if (issued_any) {
@@ -447,6 +480,68 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
             }
         }
         __syncwarp();
+    } else if (T::KDRAIN) {
+        // drain per k-block: warp w reads tensor-memory lanes 32 (w mod 4) .. +31
+        // (tile rows) and adds them into its register sums; a segment's sums go
+        // to the workspace when its last k-block is in
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;
+        long it = 0;
+        bool ok = true;
+        for (int q = q0; q < q1 && ok; q++) {
+            const GemmSeg sg = segs[q];
+            const int nt = (MT == 2 && tiles[sg.tile].a1 != nullptr) ? 2 : 1;
+            float sum[MT][NI];
+#pragma unroll
+            for (int u = 0; u < MT; u++)
+#pragma unroll
+                for (int c = 0; c < NI; c++) sum[u][c] = 0.0f;
+            for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
+                const int buf = (int)(it & 1);
+                const uint32_t use = (uint32_t)(it >> 1);
+                int got = 0;
+                if (lane == 0) got = bar_wait(&acc_full[buf], use & 1u, &abort_flag, lim) ? 1 : 0;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) {
+                    if (lane == 0 && !abort_flag) fail();
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+#pragma unroll
+                for (int u = 0; u < MT; u++) {
+                    if (u < nt) {
+                        const uint32_t tbase =
+                            tmem + (uint32_t)((buf * MT + u) * T::ACC_N) + ((uint32_t)(quarter * 32) << 16);
+#pragma unroll
+                        for (int c0 = 0; c0 < NI; c0 += 16) {
+                            uint32_t r[16], r2[16];
+                            tmem_ld16_async(tbase + (uint32_t)c0, r);
+                            if (T::MERGE) tmem_ld16_async(tbase + (uint32_t)(c0 + NI), r2);
+                            tmem_wait_ld();
+#pragma unroll
+                            for (int i = 0; i < 16; i++) {
+                                const float x = T::MERGE ? __fadd_rn(__uint_as_float(r[i]), __uint_as_float(r2[i]))
+                                                         : __uint_as_float(r[i]);
+                                sum[u][c0 + i] = __fadd_rn(sum[u][c0 + i], x);
+                            }
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) bar_arrive(&acc_empty[buf]);
+            }
+            if (!ok) break;
+#pragma unroll
+            for (int u = 0; u < MT; u++) {
+                if (u < nt) {
+                    float *dst = ws + ((size_t)sg.slot * MT + u) * NI * BM + row;
+#pragma unroll
+                    for (int c = 0; c < NI; c++) dst[(size_t)c * BM] = sum[u][c];
+                }
+            }
+        }
     } else {
         // drain: warp w reads tensor-memory lanes 32 (w mod 4) .. +31 = tile rows
         const int quarter = warp & 3;

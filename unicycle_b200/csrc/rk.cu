@@ -308,9 +308,9 @@ template <> struct TmTraits<double> {
     static constexpr int PER = 2, CH = 512, ROWS = 12, STAGES = 4;
     using Acc = double;
 };
-template <> struct TmTraits<__nv_bfloat162> {
+template <> struct TmTraits<float> {   // the anchor of the split form: K/s in FP32, FP64 sums
     static constexpr int PER = 4, CH = 1024, ROWS = 24, STAGES = 2;
-    using Acc = float;
+    using Acc = double;
 };
 template <> struct TmTraits<__nv_bfloat16> {   // the hi plane alone (anchored stages 2-6)
     static constexpr int PER = 8, CH = 2048, ROWS = 24, STAGES = 2;
@@ -326,7 +326,7 @@ constexpr size_t tm_smem_bytes()
 // rows of the stage; then one row's contribution
 template <class KT> struct TmV;
 template <> struct TmV<double> { double2 x; };
-template <> struct TmV<__nv_bfloat162> { float x[4]; };
+template <> struct TmV<float> { double x[4]; };
 template <> struct TmV<__nv_bfloat16> { float x[8]; };
 
 template <class KT>
@@ -340,16 +340,16 @@ __device__ __forceinline__ void tm_load_v<double>(const double *v, long c, long 
 // c is a multiple of the values per thread (4 or 8), so away from the ragged
 // end the thread's values are 16-byte aligned pairs
 template <>
-__device__ __forceinline__ void tm_load_v<__nv_bfloat162>(const double *v, long c, long n, TmV<__nv_bfloat162> &vr)
+__device__ __forceinline__ void tm_load_v<float>(const double *v, long c, long n, TmV<float> &vr)
 {
     if (c + 4 <= n) {
         const double2 a = __ldg(reinterpret_cast<const double2 *>(v + c));
         const double2 b = __ldg(reinterpret_cast<const double2 *>(v + c + 2));
-        vr.x[0] = (float)a.x; vr.x[1] = (float)a.y; vr.x[2] = (float)b.x; vr.x[3] = (float)b.y;
+        vr.x[0] = a.x; vr.x[1] = a.y; vr.x[2] = b.x; vr.x[3] = b.y;
         return;
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) vr.x[q] = (c + q < n) ? (float)v[c + q] : 0.0f;
+    for (int q = 0; q < 4; q++) vr.x[q] = (c + q < n) ? v[c + q] : 0.0;
 }
 template <>
 __device__ __forceinline__ void tm_load_v<__nv_bfloat16>(const double *v, long c, long n, TmV<__nv_bfloat16> &vr)
@@ -377,16 +377,13 @@ __device__ __forceinline__ void tm_accumulate<double>(const double *srow, int cl
     acc = fma(kv.y, vr.x.y, fma(kv.x, vr.x.x, acc));
 }
 template <>
-__device__ __forceinline__ void tm_accumulate<__nv_bfloat162>(const __nv_bfloat162 *srow, int cl,
-                                                              const TmV<__nv_bfloat162> &vr, float &acc)
+__device__ __forceinline__ void tm_accumulate<float>(const float *srow, int cl, const TmV<float> &vr, double &acc)
 {
-    const uint4 raw = *reinterpret_cast<const uint4 *>(srow + cl);
-    const uint32_t w4[4] = {raw.x, raw.y, raw.z, raw.w};
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        acc = fmaf(__uint_as_float(w4[q] << 16), vr.x[q], acc);
-        acc = fmaf(__uint_as_float(w4[q] & 0xffff0000u), vr.x[q], acc);
-    }
+    const float4 kv = *reinterpret_cast<const float4 *>(srow + cl);
+    acc = fma((double)kv.x, vr.x[0], acc);
+    acc = fma((double)kv.y, vr.x[1], acc);
+    acc = fma((double)kv.z, vr.x[2], acc);
+    acc = fma((double)kv.w, vr.x[3], acc);
 }
 template <>
 __device__ __forceinline__ void tm_accumulate<__nv_bfloat16>(const __nv_bfloat16 *srow, int cl,
@@ -712,7 +709,7 @@ __global__ void k_clear_pending(Ctl *ctl) { ctl->pending = 0; }
 
 bool rk_anchored(const ucg_ctx *c)
 {
-    return (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi != nullptr) || c->precision == UCG_PREC_HMATRIX_SPLIT;
+    return (c->precision == UCG_PREC_SPLIT_BF16 && c->Ksp != nullptr) || c->precision == UCG_PREC_HMATRIX_SPLIT;
 }
 
 // the attempt graph holds device addresses of the matrix and parameter arrays;
@@ -834,9 +831,8 @@ static void launch_traction(ucg_ctx *c, const StageArgs &a)
     if (S > 1 && rk_anchored(c) && c->Khi_plane) {
         // anchored stages multiply the increments by the hi plane alone
         launch_traction_t<S, __nv_bfloat16>(c, a, c->Khi_plane, c->ldk_split, c->Kscale);
-    } else if (c->precision == UCG_PREC_SPLIT_BF16 && c->Khi) {
-        launch_traction_t<S, __nv_bfloat162>(c, a, reinterpret_cast<const __nv_bfloat162 *>(c->Khi), c->ldk_split,
-                                             c->Kscale);
+    } else if (c->precision == UCG_PREC_SPLIT_BF16 && c->Ksp) {
+        launch_traction_t<S, float>(c, a, c->Ksp, c->ldk_split, c->Kscale);
     } else {
         launch_traction_t<S, double>(c, a, c->K, c->n, nullptr);
     }

@@ -1,11 +1,14 @@
-// Split-BF16 storage of the traction matrix: K = diag(s) (hi + lo).
-//
-// s_r = max_c |K_rc| (FP32), hi = bf16(K/s), lo = bf16(K/s - hi).  hi carries
-// 8 significant bits and lo the next 8, so each entry keeps about 16 bits
-// (relative error <= 2^-16 of the row maximum).  hi/lo are stored interleaved as
-// one bf16 pair per entry (4 bytes: half the FP64 stream of the traction product),
-// and hi once more as a plane of its own (2 bytes per entry), which the anchored
-// stages 2-6 multiply against the velocity increments.
+// Split storage of the traction matrix for the single-instance split path:
+// K = diag(s) k with a per-row scale s_r = max_c |K_rc| (FP32, rounded up so
+// that |k| <= 1), stored twice:
+//   * the pair plane: k in FP32, i.e. a bf16 hi part (its upper 16 bits) and a
+//     16-bit lo extension of the significand (its lower 16 bits): 4 bytes per
+//     entry, half the FP64 stream, relative error <= 2^-24 per entry.  The
+//     stage-1 anchor of every step reads it and sums in FP64;
+//   * the hi plane: bf16(k) rounded to nearest, 2 bytes per entry (relative
+//     error <= 2^-8), which the anchored stages 2-6 multiply against the
+//     velocity increments.
+#include <cmath>
 #include <cmath>
 #include "ucg_internal.cuh"
 
@@ -33,21 +36,18 @@ __global__ void k_row_absmax(const double *__restrict__ K, long n, float *__rest
 
 // out has row stride ldk >= n; the padding columns hold zeros
 __global__ void k_split(const double *__restrict__ K, long n, long ldk, long total, const float *__restrict__ scale,
-                        __nv_bfloat162 *__restrict__ out, __nv_bfloat16 *__restrict__ out_hi)
+                        float *__restrict__ out, __nv_bfloat16 *__restrict__ out_hi)
 {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const long r = i / ldk, cc = i - r * ldk;
         if (cc >= n) {
-            out[i] = __halves2bfloat162(__double2bfloat16(0.0), __double2bfloat16(0.0));
+            out[i] = 0.0f;
             out_hi[i] = __double2bfloat16(0.0);
             continue;
         }
         const double x = K[r * n + cc] / (double)scale[r];
-        const __nv_bfloat16 hi = __double2bfloat16(x);
-        const double rem = x - (double)__bfloat162float(hi);
-        const __nv_bfloat16 lo = __double2bfloat16(rem);
-        out[i] = __halves2bfloat162(hi, lo);
-        out_hi[i] = hi;
+        out[i] = __double2float_rn(x);
+        out_hi[i] = __double2bfloat16(x);
     }
 }
 
@@ -58,15 +58,14 @@ int split_bf16_build(ucg_ctx *c)
     UCG_CUDA(cudaSetDevice(c->device));
     c->ldk_split = (c->n + 7) / 8 * 8;
     const long total = c->ldk_split * c->m;
-    cudaError_t e = cudaMalloc(&c->Khi, sizeof(__nv_bfloat162) * (size_t)total);
-    if (e != cudaSuccess) { c->Khi = nullptr; return cuda_fail(c, e, "cudaMalloc(split K)"); }
+    cudaError_t e = cudaMalloc(&c->Ksp, sizeof(float) * (size_t)total);
+    if (e != cudaSuccess) { c->Ksp = nullptr; return cuda_fail(c, e, "cudaMalloc(split K)"); }
     e = cudaMalloc(&c->Khi_plane, sizeof(__nv_bfloat16) * (size_t)total);
     if (e != cudaSuccess) { c->Khi_plane = nullptr; return cuda_fail(c, e, "cudaMalloc(split K hi plane)"); }
     UCG_CUDA(cudaMalloc(&c->Kscale, sizeof(float) * (size_t)c->m));
     k_row_absmax<<<(unsigned)c->m, 256, 0, c->stream>>>(c->K, c->n, c->Kscale);
     const int grid = c->sms * 16;
-    k_split<<<grid, 256, 0, c->stream>>>(c->K, c->n, c->ldk_split, total, c->Kscale,
-                                         reinterpret_cast<__nv_bfloat162 *>(c->Khi), c->Khi_plane);
+    k_split<<<grid, 256, 0, c->stream>>>(c->K, c->n, c->ldk_split, total, c->Kscale, c->Ksp, c->Khi_plane);
     c->launches.count += 2;
     UCG_CUDA(cudaGetLastError());
     UCG_CUDA(cudaStreamSynchronize(c->stream));
@@ -79,13 +78,12 @@ int split_bf16_build(ucg_ctx *c)
 
 void split_bf16_free(ucg_ctx *c)
 {
-    if (c->Khi || c->Kscale) rk_drop_graph(c);
-    if (c->Khi) cudaFree(c->Khi);
+    if (c->Ksp || c->Kscale) rk_drop_graph(c);
+    if (c->Ksp) cudaFree(c->Ksp);
     if (c->Khi_plane) cudaFree(c->Khi_plane);
     if (c->Kscale) cudaFree(c->Kscale);
-    c->Khi = nullptr;
+    c->Ksp = nullptr;
     c->Khi_plane = nullptr;
-    c->Klo = nullptr;
     c->Kscale = nullptr;
 }
 

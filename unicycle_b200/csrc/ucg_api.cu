@@ -341,7 +341,7 @@ int ucg_set_precision(ucg_ctx *c, int precision)
     if (precision == UCG_PREC_FP64 && c->assembled && !c->K)
         return set_err(c, UCG_E_STATE, "FP64 matrix was released; re-assemble");
     c->precision = precision;
-    if (precision == UCG_PREC_SPLIT_BF16 && c->assembled && !c->Khi) return split_bf16_build(c);
+    if (precision == UCG_PREC_SPLIT_BF16 && c->assembled && !c->Ksp) return split_bf16_build(c);
     return UCG_OK;
 }
 
@@ -349,7 +349,7 @@ int ucg_keep_fp64(ucg_ctx *c, int keep)
 {
     if (!c) return UCG_E_BADARG;
     c->keep_fp64 = keep != 0;
-    if (!c->keep_fp64 && c->Khi && c->K) {
+    if (!c->keep_fp64 && c->Ksp && c->K) {
         rk_drop_graph(c);
         cudaStreamSynchronize(c->stream);
         cudaFree(c->K);

@@ -139,7 +139,7 @@ struct ucg_ctx {
     double asm_ms[3] = {0.0, 0.0, 0.0};   // device time of the last assembly: rect, tri, vol sources
     int precision = UCG_PREC_FP64;
     bool keep_fp64 = true;
-    __nv_bfloat16 *Khi = nullptr, *Klo = nullptr;   // Khi: interleaved (hi, lo) pairs
+    float *Ksp = nullptr;                            // K/s in FP32: bf16 hi bits + 16-bit lo extension
     __nv_bfloat16 *Khi_plane = nullptr;              // hi alone, same row stride
     float *Kscale = nullptr;   // per row
     long ldk_split = 0;        // row stride of the split matrix (n padded to a multiple of 8)
