@@ -78,9 +78,10 @@ def parse():
     p.add_argument("--trace-attempts", type=int, default=16000, help="attempts of the trace-recording runs")
     p.add_argument("--learned-eval-years", type=float, default=15.0,
                    help="simulated years of the held-out comparison (0: train only, no comparison)")
-    p.add_argument("--spinup", type=int, default=20,
+    p.add_argument("--spinup", type=int, default=200,
                    help="untimed accepted steps (plain) / attempts (ensemble) before warm-up, past the start-up "
-                        "transient of the step size")
+                        "transient of the step size (from dt0 = 1 ms the step grows at most 5x per step and "
+                        "settles after about 100 steps at N = 20k)")
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU sample length")
     return p.parse_args()

@@ -2,17 +2,20 @@
 inputs, its determinism and column independence, and ensemble Runge-Kutta
 attempts against the single-instance FP64 integrator (which the oracle pins).
 
-Error bound of the contraction: K and V are each split into bf16 hi + lo with
-unit roundoff 2^-8 per part, so every product carries a relative error of at
-most about 3 * 2^-16 (the dropped lo*lo term and both residuals), plus FP32
-accumulation; the test asks |T - K V| <= 1e-4 (|K| |V|) entry by entry.
+Error bound of the contraction: K and V are each held as fp16 hi + 2^-11 lo
+pairs with a power-of-two scale per 128 x 64 block of K and per 64-source
+block of each instance's V, so every product carries a relative error of about
+2^-21 (both residuals; the dropped lo*lo term is 2^-44) for entries above
+2^-14 of their block's largest, and every k-block's FP32 partial sum is added
+into register sums with round-to-nearest; the test asks
+|T - K V| <= 1e-5 (|K| |V|) entry by entry.
 """
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-BOUND = 1.0e-4
+BOUND = 1.0e-5
 
 
 def _small_cfg(shapes=((16, 8), (24, 8)), n_sets=40, seed=11):
@@ -67,10 +70,10 @@ def test_contraction_matches_fp64(ucg):
         T = ens.matvec(gi, V)
         worst.append(_check_contraction(K, V, T))
     print("max |T - KV| / (|K||V|):", worst)
-    # the increments' form reads K hi only: error up to the bf16 unit roundoff 2^-8
+    # the increments' form reads K hi only: error up to the fp16 unit roundoff 2^-11
     K = sims[0].copy_G()
     V = rng.standard_normal((len(cfg["geoms"][0]["sets"]), K.shape[1]))
-    r2 = _check_contraction(K, V, ens.matvec(0, V, terms=2), bound=5e-3)
+    r2 = _check_contraction(K, V, ens.matvec(0, V, terms=2), bound=1e-3)
     print("two-term form: max |T - KV| / (|K||V|):", r2)
     for s in sims:
         s.close()
@@ -86,7 +89,10 @@ def test_contraction_plans_deterministic_and_column_independent(ucg):
     rng = np.random.default_rng(6)
     V = rng.standard_normal((70, K.shape[1]))
     plans = [(64, _lib.UCG_ENS_STREAM_K, 0), (64, _lib.UCG_ENS_SPLIT_LPT, 4), (32, _lib.UCG_ENS_SPLIT_LPT, 0),
-             (128, _lib.UCG_ENS_STREAM_K, 0), (128, _lib.UCG_ENS_SPLIT_LPT, 2)]
+             (32, _lib.UCG_ENS_STREAM_K, 0)]
+    # 128-instance tiles are for hierarchical geometries only
+    with pytest.raises(ucg.UcgError):
+        ens.plan(128, _lib.UCG_ENS_STREAM_K, 0)
     results = []
     for ni, kind, chunk in plans:
         ens.plan(ni, kind, chunk)

@@ -103,7 +103,7 @@ def _single(sim, c, nsteps):
     return np.array(ts), ys
 
 
-def _ensemble(ucg, sim, c, nsteps, ninst=4, model=None):
+def _ensemble(ucg, sim, c, nsteps, ninst=4, model=None, terms=None):
     """Attempts one at a time; instance 0's state after each acceptance.  All
     instances carry the same parameters: their histories must be identical."""
     fr = c["friction"]
@@ -114,6 +114,8 @@ def _ensemble(ucg, sim, c, nsteps, ninst=4, model=None):
                          fr["damping"])
         ens.set_state(0, i, c["y0"], 0.0, c["dt0"])
     ens.set_tolerance(c["epsilon"])
+    if terms is not None:
+        ens.set_increment_terms(terms)
     if model is not None:
         ens.set_step_model(model)
     ts, ys = [], []
@@ -162,19 +164,21 @@ def test_history_plain_fp64(ucg, setup):
     _check("plain FP64", ref, ts, ys, 1e-9, 1e-6)
 
 
-def test_history_split_bf16(ucg, setup):
+@pytest.mark.parametrize("form", ["split_pair", "split_bf16"])
+def test_history_split(ucg, setup, form):
     c, sim, ref = setup
-    sim.set_precision(ucg.UCG_PREC_SPLIT_BF16)
+    sim.set_precision(form)
     ts, ys = _single(sim, c, NRUN)
     sim.set_precision(ucg.UCG_PREC_FP64)
-    _check("split-BF16", ref, ts, ys, 1e-6, 1e-5)
+    _check(form, ref, ts, ys, 1e-6, 1e-5)
 
 
-def test_history_dense_ensemble(ucg, setup):
+@pytest.mark.parametrize("terms", [3, 2])
+def test_history_dense_ensemble(ucg, setup, terms):
     c, sim, ref = setup
     sim.set_precision(ucg.UCG_PREC_FP64)
-    ts, ys = _ensemble(ucg, sim, c, NRUN)
-    _check("ensemble (tensor cores)", ref, ts, ys, 1e-6, 1e-5)
+    ts, ys = _ensemble(ucg, sim, c, NRUN, terms=terms)
+    _check(f"ensemble (tensor cores, {terms} terms)", ref, ts, ys, 1e-6, 1e-5)
 
 
 def test_history_hmatrix(ucg, setup):

@@ -6,7 +6,8 @@ boundary-integral hot path behind a C ABI (include/ucg.h, libucg.so).
 from . import configs  # noqa: F401  (pure numpy; no device needed)
 from ._lib import UcgError, load  # noqa: F401
 from ._lib import (UCG_OKADA_FP64, UCG_OKADA_REF32IO, UCG_PREC_FP64,  # noqa: F401
-                   UCG_PREC_HMATRIX, UCG_PREC_HMATRIX_SPLIT, UCG_PREC_SPLIT_BF16)
+                   UCG_PREC_HMATRIX, UCG_PREC_HMATRIX_SPLIT, UCG_PREC_SPLIT_BF16,
+                   UCG_PREC_SPLIT_PAIR)
 from .simulation import Simulation  # noqa: F401
 from .ensemble import Ensemble  # noqa: F401
 from .stepmodel import StepModel  # noqa: F401

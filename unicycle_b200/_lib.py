@@ -24,6 +24,7 @@ UCG_OKADA_FP64 = 0
 UCG_OKADA_REF32IO = 1
 UCG_PREC_FP64 = 0
 UCG_PREC_SPLIT_BF16 = 1
+UCG_PREC_SPLIT_PAIR = 4
 UCG_PREC_HMATRIX = 2
 UCG_PREC_HMATRIX_SPLIT = 3
 UCG_DRIVER_RATESTATE = 0

@@ -79,6 +79,7 @@ constexpr int BM = 128;                 // K rows per tile (MMA M)
 constexpr int BK = 64;                  // sources per k-block (one 128-byte bf16 row)
 constexpr int A_HALF = BM * BK * 2;     // one bf16 image of a tile k-block: 16 KB
 constexpr int A_IMG = 2 * A_HALF;       // hi + lo
+constexpr float LO_SCALE = 2048.0f, LO_UNSCALE = 1.0f / 2048.0f;   // dense images: lo = 2^11 residual
 constexpr int MAX_GEOM = 16;
 constexpr int EW_THREADS = 128;         // element-wise kernels: elements per block
 constexpr int ST_THREADS = 256;         // finish / commit kernels: threads per block
@@ -105,14 +106,18 @@ struct Tile {
     static constexpr bool MERGE = 2 * MT * 2 * NI <= 512;
     static constexpr int ACC_N = MERGE ? 2 * NI : NI;
     static constexpr uint32_t TMEM_COLS = 2 * MT * ACC_N; // two sets of MT FP32 accumulators
-    // instruction descriptor: F32 accumulator, bf16 A and B, both K-major,
+    // instruction descriptor: F32 accumulator, A and B fp16 (format 0; the
+    // dense images) or bf16 (format 1; the hierarchical images), both K-major,
     // N (bits 17-22, N/8), M = 128 (bits 24-28, M/16)
-    static constexpr uint32_t idesc(int n)
+    static constexpr uint32_t idesc(int n, bool bf16)
     {
-        return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+        return (1u << 4) | (bf16 ? (1u << 7) | (1u << 10) : 0u) | ((uint32_t)(n >> 3) << 17) |
+               ((uint32_t)(BM >> 4) << 24);
     }
-    static constexpr uint32_t IDESC = idesc(NI);
-    static constexpr uint32_t IDESC2 = idesc(2 * NI);
+    static constexpr uint32_t IDESC = idesc(NI, false);
+    static constexpr uint32_t IDESC2 = idesc(2 * NI, false);
+    static constexpr uint32_t IDESC_BF = idesc(NI, true);
+    static constexpr uint32_t IDESC2_BF = idesc(2 * NI, true);
     // KDRAIN: every k-block's products go into a fresh accumulator that the
     // drain warps add, in FP32 with round-to-nearest, into per-thread register
     // sums (MT NI of them).  The tensor core's own FP32 accumulation truncates
@@ -121,7 +126,9 @@ struct Tile {
     // embedded error estimate cannot tell it from truncation error and shrinks
     // the step.  Drained per k-block it covers 4 MMAs only.  Off where the
     // register sums would not fit (128 instances x 2 M-tiles).
-    static constexpr bool KDRAIN = MT * NI <= 128;
+    static constexpr bool KDRAIN = true;
+    static constexpr int NCOL = MT == 2 ? NI : NI / 2;   // register sums per drain thread
+    static_assert(MERGE, "the drain adds the hi and 2^-11 halves of a merged accumulator");
 };
 
 // byte offset of element (r, k) in a 128-byte-swizzled tile image with 128-byte rows
@@ -178,6 +185,7 @@ struct GeomDev {
     int blk_e0, epb_e;          // element-wise grid: first block, blocks per instance
     int blk_s0, epb_s;          // state-wise grid
     uint8_t *B;                 // V images [ntile][kblock][hi | lo]
+    float *vscale;              // dense: V image scale per [ntile][kblock][instance of the tile]
     const float *rscale;        // per K row (mtiles * 128)
     double *y, *ys, *k[6], *ycand, *yerr, *yscal;           // [ninst][7 np]
     double *v1, *t1;            // stage-1 anchor: [ninst][2 np] velocities, [ninst][3 np] tractions
@@ -211,6 +219,8 @@ struct GemmTile {
     const uint8_t *a;           // K images of k-block 0 of the (first) M-tile
     const uint8_t *a1;          // the second M-tile's, or null
     const uint8_t *b;           // V images of k-block 0 of this instance tile
+    const float *ks, *ks1;      // K image scale per k-block of the (first, second) M-tile
+    const float *vs;            // V image scales of k-block 0 of this instance tile ([kblock][ni])
 };
 struct GemmSeg {
     int tile, kb0, kb1, slot;
@@ -317,12 +327,18 @@ __device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t r[16])
                    "=r"(r[15])
                  : "r"(taddr));
 }
+__device__ __forceinline__ void tmem_ld8_async(uint32_t taddr, uint32_t r[8])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+}
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // ---- the contraction ---------------------------------------------------------------
 
 template <int NI, bool KLO, int MT>
-__global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__restrict__ tiles,
+__global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__restrict__ tiles,
         const GemmSeg *__restrict__ segs, const int *__restrict__ cta_seg, float *__restrict__ ws, EnsGlobal *gl)
 {
     int *err = &gl->err;
@@ -346,7 +362,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
         }
         for (int b = 0; b < 2; b++) {
             bar_init(&acc_full[b], 1);
-            bar_init(&acc_empty[b], 4);
+            bar_init(&acc_empty[b], 8);   // both drain warpgroups
         }
         bar_init(&drain, 1);
         abort_flag = 0;
@@ -376,7 +392,7 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
             // ahead, its tile one ahead), off the copy issue's critical path
             GemmSeg s1 = q0 < q1 ? segs[q0] : GemmSeg{0, 0, 0, 0};
             GemmSeg s2 = q0 + 1 < q1 ? segs[q0 + 1] : s1;
-            GemmTile t1 = q0 < q1 ? tiles[s1.tile] : GemmTile{nullptr, nullptr, nullptr};
+            GemmTile t1 = q0 < q1 ? tiles[s1.tile] : GemmTile{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
             for (int q = q0; q < q1 && !abort_flag && !hold; q++) {
                 const GemmSeg sg = s1;
                 const GemmTile tl = t1;
@@ -455,9 +471,13 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                                 const uint32_t au = a + (uint32_t)(u * T::A_BYTES);
                                 const uint64_t ahi = sw128_desc(au + 32u * j);
                                 if (T::MERGE) {
-                                    // rows 0..NI-1 of the B operand are Vhi, NI..2NI-1 Vlo
+                                    // rows 0..NI-1 of the B operand are Vhi, NI..2NI-1 Vlo:
+                                    // columns 0..NI-1 take Khi Vhi, NI..2NI-1 the products
+                                    // that carry 2^-11 (Khi Vlo, and in the anchor Klo Vhi)
                                     mma_bf16(d, ahi, bhi, T::IDESC2, acc);
-                                    if (KLO) mma_bf16(d, sw128_desc(au + A_HALF + 32u * j), bhi, T::IDESC, 1u);
+                                    if (KLO)
+                                        mma_bf16(d + (uint32_t)NI, sw128_desc(au + A_HALF + 32u * j), bhi, T::IDESC,
+                                                 1u);
                                 } else {
                                     mma_bf16(d, ahi, bhi, T::IDESC, acc);
                                     mma_bf16(d, ahi, blo, T::IDESC, 1u);
@@ -480,22 +500,29 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
             }
         }
         __syncwarp();
-    } else if (T::KDRAIN) {
-        // drain per k-block: warp w reads tensor-memory lanes 32 (w mod 4) .. +31
-        // (tile rows) and adds them into its register sums; a segment's sums go
-        // to the workspace when its last k-block is in
+    } else {
+        // drain per k-block, two warpgroups (warps 2-5 and 6-9): warp w reads
+        // tensor-memory lanes 32 (w mod 4) .. +31 (tile rows); with two M-tiles a
+        // group takes one tile, with one M-tile half of its instance columns.
+        // Every k-block's partial sums (hi products + 2^-11 lo products, times
+        // the K block and V block scales) are added in FP64 registers; a
+        // segment's sums go to the workspace when its last k-block is in
         const int quarter = warp & 3;
+        const int grp = (warp - 2) >> 2;
         const int row = quarter * 32 + lane;
+        constexpr int NC = T::NCOL;                   // columns per thread
+        const int u = (MT == 2) ? grp : 0;            // the M-tile this group drains
+        const int cbase = (MT == 2) ? 0 : grp * NC;   // its first instance column
         long it = 0;
         bool ok = true;
         for (int q = q0; q < q1 && ok; q++) {
             const GemmSeg sg = segs[q];
             const int nt = (MT == 2 && tiles[sg.tile].a1 != nullptr) ? 2 : 1;
-            float sum[MT][NI];
+            const bool mine = u < nt;                 // a pair's missing second tile: wait and release only
+            double sum[NC];
 #pragma unroll
-            for (int u = 0; u < MT; u++)
-#pragma unroll
-                for (int c = 0; c < NI; c++) sum[u][c] = 0.0f;
+            for (int c = 0; c < NC; c++) sum[c] = 0.0;
+            const GemmTile tl = tiles[sg.tile];
             for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
                 const int buf = (int)(it & 1);
                 const uint32_t use = (uint32_t)(it >> 1);
@@ -508,23 +535,23 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                     break;
                 }
                 tc_fence_after();
+                if (mine) {
+                    const double sk = (double)(u == 0 ? tl.ks : tl.ks1)[kb];
+                    const float *vs = tl.vs + (size_t)kb * NI + cbase;
+                    const uint32_t tbase = tmem + (uint32_t)((buf * MT + u) * T::ACC_N + cbase) +
+                                           ((uint32_t)(quarter * 32) << 16);
 #pragma unroll
-                for (int u = 0; u < MT; u++) {
-                    if (u < nt) {
-                        const uint32_t tbase =
-                            tmem + (uint32_t)((buf * MT + u) * T::ACC_N) + ((uint32_t)(quarter * 32) << 16);
+                    for (int c0 = 0; c0 < NC; c0 += 8) {
+                        uint32_t r[8], r2[8];
+                        tmem_ld8_async(tbase + (uint32_t)c0, r);
+                        tmem_ld8_async(tbase + (uint32_t)(c0 + NI), r2);
+                        tmem_wait_ld();
 #pragma unroll
-                        for (int c0 = 0; c0 < NI; c0 += 16) {
-                            uint32_t r[16], r2[16];
-                            tmem_ld16_async(tbase + (uint32_t)c0, r);
-                            if (T::MERGE) tmem_ld16_async(tbase + (uint32_t)(c0 + NI), r2);
-                            tmem_wait_ld();
-#pragma unroll
-                            for (int i = 0; i < 16; i++) {
-                                const float x = T::MERGE ? __fadd_rn(__uint_as_float(r[i]), __uint_as_float(r2[i]))
-                                                         : __uint_as_float(r[i]);
-                                sum[u][c0 + i] = __fadd_rn(sum[u][c0 + i], x);
-                            }
+                        for (int i = 0; i < 8; i++) {
+                            // hi products + 2^-11 lo products (exact in FP64), times the block scales
+                            const double x = (double)__uint_as_float(r[i]) +
+                                             (double)__uint_as_float(r2[i]) * (double)LO_UNSCALE;
+                            sum[c0 + i] = fma(x, sk * (double)__ldg(vs + c0 + i), sum[c0 + i]);
                         }
                     }
                 }
@@ -533,56 +560,11 @@ __global__ void __launch_bounds__(192, 1) k_bf16x3_contract(const GemmTile *__re
                 if (lane == 0) bar_arrive(&acc_empty[buf]);
             }
             if (!ok) break;
+            if (mine) {
+                float *dst = ws + ((size_t)sg.slot * MT + u) * NI * BM + (size_t)cbase * BM + row;
 #pragma unroll
-            for (int u = 0; u < MT; u++) {
-                if (u < nt) {
-                    float *dst = ws + ((size_t)sg.slot * MT + u) * NI * BM + row;
-#pragma unroll
-                    for (int c = 0; c < NI; c++) dst[(size_t)c * BM] = sum[u][c];
-                }
+                for (int c = 0; c < NC; c++) dst[(size_t)c * BM] = (float)sum[c];
             }
-        }
-    } else {
-        // drain: warp w reads tensor-memory lanes 32 (w mod 4) .. +31 = tile rows
-        const int quarter = warp & 3;
-        const int row = quarter * 32 + lane;
-        int tc = 0;
-        for (int q = q0; q < q1; q++, tc++) {
-            const GemmSeg sg = segs[q];
-            const int nt = (MT == 2 && tiles[sg.tile].a1 != nullptr) ? 2 : 1;
-            const int buf = tc & 1;
-            const uint32_t use = (uint32_t)(tc >> 1);
-            int ok = 0;
-            if (lane == 0) ok = bar_wait(&acc_full[buf], use & 1u, &abort_flag, lim) ? 1 : 0;
-            ok = __shfl_sync(0xffffffffu, ok, 0);
-            if (!ok) {
-                if (lane == 0 && !abort_flag) fail();
-                break;
-            }
-            tc_fence_after();
-            for (int u = 0; u < nt; u++) {
-                float *dst = ws + ((size_t)sg.slot * MT + u) * NI * BM + row;
-                const uint32_t tbase =
-                    tmem + (uint32_t)((buf * MT + u) * T::ACC_N) + ((uint32_t)(quarter * 32) << 16);
-#pragma unroll
-                for (int c0 = 0; c0 < NI; c0 += 16) {
-                    uint32_t r[16];
-                    tmem_ld16(tbase + (uint32_t)c0, r);
-                    if (T::MERGE) {
-                        uint32_t r2[16];
-                        tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
-#pragma unroll
-                        for (int i = 0; i < 16; i++)
-                            dst[(size_t)(c0 + i) * BM] = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < 16; i++) dst[(size_t)(c0 + i) * BM] = __uint_as_float(r[i]);
-                    }
-                }
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) bar_arrive(&acc_empty[buf]);
         }
     }
 
@@ -642,8 +624,8 @@ struct HTile {
     // K-groups together (they are consecutive 8-row groups); the drain adds
     // the accumulator's two halves
     static constexpr uint32_t TMEM_COLS = 4 * NI;
-    static constexpr uint32_t IDESC = Tile<NI, false, 1>::IDESC;
-    static constexpr uint32_t IDESC2 = Tile<NI, false, 1>::IDESC2;
+    static constexpr uint32_t IDESC = Tile<NI, false, 1>::IDESC_BF;
+    static constexpr uint32_t IDESC2 = Tile<NI, false, 1>::IDESC2_BF;
 };
 
 struct HUnit {                  // one M-tile of one pass for one instance tile
@@ -1077,9 +1059,54 @@ __global__ void k_row_scale(const double *__restrict__ K, long m, long n, long r
     }
 }
 
+// Dense operand images are fp16 pairs with one power-of-two scale per image
+// block (a 128-row x 64-source K block, or the 64 sources of one instance's V
+// k-block): x = s (hi + 2^-11 lo) with hi = fp16(x / s) and lo the rounded
+// residual scaled by 2^11, so that it stays a normal fp16 number: 22
+// significant bits for every entry above 2^-14 of its block's largest (an
+// absolute 2^-25 of that below).  The MMAs run on the hi and lo images as
+// they are; the drain applies 2^-11 to the lo products and the two block
+// scales to every k-block's partial sums before adding them up.
+__device__ __forceinline__ float pow2_at_least(double m)
+{
+    if (!(m > 0.0)) return 1.0f;
+    int e;
+    frexp(m, &e);                 // m = f 2^e, 0.5 <= f < 1
+    return ldexpf(1.0f, e);       // >= m
+}
+
+__device__ __forceinline__ void split16(double x, __half &hi, __half &lo)
+{
+    hi = __double2half(x);
+    lo = __double2half((x - (double)__half2float(hi)) * (double)LO_SCALE);
+}
+
+// the scale of one 128 x 64 block of K with its rows divided by their row
+// scales (one CTA per block): rows far smaller than others of the same tile
+// (a traction component that vanishes by symmetry) keep their own precision
+__global__ void k_block_scale(const double *__restrict__ K, long m, long n, int kblocks,
+                              const float *__restrict__ rscale, float *__restrict__ ks)
+{
+    const int mt = blockIdx.x / kblocks, kb = blockIdx.x % kblocks;
+    double mx = 0.0;
+    for (int t = threadIdx.x; t < BM * BK; t += blockDim.x) {
+        const long r = (long)mt * BM + t / BK, c = (long)kb * BK + t % BK;
+        if (r < m && c < n) mx = fmax(mx, fabs(K[r * n + c]) / (double)rscale[r]);
+    }
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    __shared__ double wm[32];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t = fmax(t, wm[w]);
+        ks[blockIdx.x] = pow2_at_least(t);
+    }
+}
+
 // one thread per (row, 8 sources): 8 doubles in, 16 bytes of hi and of lo out
 __global__ void k_pack_k(const double *__restrict__ K, long m, long n, int kblocks, long rows_pad,
-                         const float *__restrict__ scale, uint8_t *__restrict__ img)
+                         const float *__restrict__ rscale, const float *__restrict__ ks, uint8_t *__restrict__ img)
 {
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     const long per_row = (long)kblocks * (BK / 8);
@@ -1088,50 +1115,66 @@ __global__ void k_pack_k(const double *__restrict__ K, long m, long n, int kbloc
     const int c8 = (int)(t % per_row);
     const int kb = c8 / (BK / 8), kk = (c8 % (BK / 8)) * 8;
     const long c0 = (long)kb * BK + kk;
-    const double inv = 1.0 / (double)scale[r];
+    const long mt = r / BM;
+    const double inv = 1.0 / ((double)rscale[r] * (double)ks[mt * kblocks + kb]);
     uint32_t hi[4], lo[4];
 #pragma unroll
     for (int j = 0; j < 8; j += 2) {
         const double x0 = (r < m && c0 + j < n) ? K[r * n + c0 + j] * inv : 0.0;
         const double x1 = (r < m && c0 + j + 1 < n) ? K[r * n + c0 + j + 1] * inv : 0.0;
-        const __nv_bfloat16 h0 = __double2bfloat16(x0), h1 = __double2bfloat16(x1);
-        const __nv_bfloat16 l0 = __double2bfloat16(x0 - (double)__bfloat162float(h0));
-        const __nv_bfloat16 l1 = __double2bfloat16(x1 - (double)__bfloat162float(h1));
-        hi[j / 2] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-        lo[j / 2] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+        __half h0, h1, l0, l1;
+        split16(x0, h0, l0);
+        split16(x1, h1, l1);
+        hi[j / 2] = (uint32_t)__half_as_ushort(h0) | ((uint32_t)__half_as_ushort(h1) << 16);
+        lo[j / 2] = (uint32_t)__half_as_ushort(l0) | ((uint32_t)__half_as_ushort(l1) << 16);
     }
-    const long mt = r / BM;
     const int rr = (int)(r % BM);
     uint8_t *base = img + ((size_t)mt * kblocks + kb) * A_IMG + sw128(rr, kk);
     *reinterpret_cast<uint4 *>(base) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
     *reinterpret_cast<uint4 *>(base + A_HALF) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
 }
 
-// write the source pair (c, c+1), c even, of instance i into the V images
-__device__ __forceinline__ void put_v(uint8_t *B, int ni, int kblocks, int i, long c, double v0, double v1)
+// write the source pair (c, c+1), c even, of instance i into the V images with
+// the scale s of its k-block
+__device__ __forceinline__ void put_v(uint8_t *B, int ni, int kblocks, int i, long c, double v0, double v1, float s)
 {
     const int nt = i / ni, rr = i % ni;
     const int kb = (int)(c / BK), kk = (int)(c % BK);
     const size_t bimg = (size_t)2 * ni * BK * 2;
     uint8_t *base = B + ((size_t)nt * kblocks + kb) * bimg + sw128(rr, kk);
-    const __nv_bfloat16 h0 = __double2bfloat16(v0), h1 = __double2bfloat16(v1);
-    const __nv_bfloat16 l0 = __double2bfloat16(v0 - (double)__bfloat162float(h0));
-    const __nv_bfloat16 l1 = __double2bfloat16(v1 - (double)__bfloat162float(h1));
-    *reinterpret_cast<__nv_bfloat162 *>(base) = __halves2bfloat162(h0, h1);
-    *reinterpret_cast<__nv_bfloat162 *>(base + (size_t)ni * BK * 2) = __halves2bfloat162(l0, l1);
+    const double inv = 1.0 / (double)s;
+    __half h0, h1, l0, l1;
+    split16(v0 * inv, h0, l0);
+    split16(v1 * inv, h1, l1);
+    *reinterpret_cast<__half2 *>(base) = __halves2half2(h0, h1);
+    *reinterpret_cast<__half2 *>(base + (size_t)ni * BK * 2) = __halves2half2(l0, l1);
 }
 
-// dense V (instance-major, ninst x n) into the images of one geometry
-__global__ void k_pack_v_dense(uint8_t *B, int ni, int kblocks, int ninst, long n, const double *__restrict__ V)
+// the k-block scale of 32 consecutive source pairs held by the lanes of a
+// warp (lanes without a pair pass 0): the largest magnitude rounded up to a
+// power of two, the same on every lane
+__device__ __forceinline__ float warp_block_scale(double v0, double v1)
 {
-    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    const long pairs = (n + 1) / 2;
-    if (t >= (long)ninst * pairs) return;
-    const int i = (int)(t / pairs);
-    const long c = 2 * (t % pairs);
-    const double v0 = V[(long)i * n + c];
+    double m = fmax(fabs(v0), fabs(v1));
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    return pow2_at_least(m);
+}
+
+// dense V (instance-major, ninst x n) into the images of one geometry: one warp
+// per (instance, k-block), lane j the source pair j of the k-block
+__global__ void k_pack_v_dense(uint8_t *B, float *vscale, int ni, int kblocks, int ninst, long n,
+                               const double *__restrict__ V)
+{
+    const long w = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= (long)ninst * kblocks) return;     // uniform over the warp
+    const int i = (int)(w / kblocks), kb = (int)(w % kblocks);
+    const long c = (long)kb * BK + 2 * lane;
+    const double v0 = (c < n) ? V[(long)i * n + c] : 0.0;
     const double v1 = (c + 1 < n) ? V[(long)i * n + c + 1] : 0.0;
-    put_v(B, ni, kblocks, i, c, v0, v1);
+    const float s = warp_block_scale(v0, v1);
+    if (lane == 0) vscale[((size_t)(i / ni) * kblocks + kb) * ni + i % ni] = s;
+    put_v(B, ni, kblocks, i, c, v0, v1, s);
 }
 
 // row r of instance i from the partial sums, added in k order: `paired`
@@ -1288,9 +1331,9 @@ __global__ void __launch_bounds__(EW_THREADS) k_ens_prologue(const EnsArgs *__re
     }
     __syncthreads();
     unsigned long long vkey = 0ull, tkey = ~0ull;   // max V and min log10 theta of this element (stage 1)
+    double v0 = 0.0, v1 = 0.0;
     if (valid) {
         const double *yy = sh + 7 * threadIdx.x;
-        double v0 = 0.0, v1 = 0.0;
         if (work) {
             const double rake = atan2(yy[3], yy[2]);
             const double vel = exp(yy[6] * E_LG10);
@@ -1313,10 +1356,16 @@ __global__ void __launch_bounds__(EW_THREADS) k_ens_prologue(const EnsArgs *__re
                 v1 = v1 - G.v1[2 * pe + 1];
             }
         }
-        if (G.hier)
-            put_x(G.B + (size_t)(i / A->ni) * G.hbtile, A->ni, i % A->ni, G.hxpos[e], v0, v1);
-        else
-            put_v(G.B, A->ni, G.kblocks, i, 2L * e, v0, v1);
+        if (G.hier) put_x(G.B + (size_t)(i / A->ni) * G.hbtile, A->ni, i % A->ni, G.hxpos[e], v0, v1);
+    }
+    if (!G.hier) {
+        // a warp holds the 32 elements (64 sources) of one k-block: its scale,
+        // then every element's pair of sources
+        const float sv = warp_block_scale(v0, v1);
+        const int ew = e0 + (threadIdx.x & ~31);          // the warp's first element
+        if ((threadIdx.x & 31) == 0 && ew < G.np)
+            G.vscale[((size_t)(i / A->ni) * G.kblocks + ew / 32) * A->ni + i % A->ni] = sv;
+        if (valid) put_v(G.B, A->ni, G.kblocks, i, 2L * e, v0, v1, sv);
     }
     if (S == 1) {
         // the block's elements belong to one instance: reduce over the warp,
@@ -1696,6 +1745,8 @@ struct EnsGeomHost {
     long m = 0, n = 0;
     uint8_t *A = nullptr;      // K images
     float *rscale = nullptr;
+    float *kscale = nullptr;   // dense: K image scale per [mtile][kblock]
+    float *vscale = nullptr;   // dense: V image scale per [ntile][kblock][ni]
     double *state = nullptr;   // 12 vectors of ninst * 7 np
     double *anchor = nullptr;  // v1 (ninst * 2 np) then t1 (ninst * 3 np)
     double *par = nullptr;     // 7 vectors of ninst * np
@@ -2359,7 +2410,7 @@ cudaError_t prepare_contract(int ni)
     switch (ni) {
     case 32: e = prepare_contract_t<32>(); break;
     case 64: e = prepare_contract_t<64>(); break;
-    case 128: e = prepare_contract_t<128>(); break;
+    case 128: e = cudaSuccess; break;   // hierarchical geometries only: no dense contraction
     default: return cudaErrorInvalidValue;
     }
     if (e != cudaSuccess) return e;
@@ -2373,7 +2424,7 @@ cudaError_t prepare_contract(int ni)
 template <int NI, bool KLO, int MT>
 cudaError_t launch_contract_t(ucg_ensemble *E, const PlanBufs &P)
 {
-    k_bf16x3_contract<NI, KLO, MT><<<E->sms, 192, Tile<NI, KLO, MT>::SMEM, E->stream>>>(P.tiles, P.segs, P.cta,
+    k_bf16x3_contract<NI, KLO, MT><<<E->sms, 320, Tile<NI, KLO, MT>::SMEM, E->stream>>>(P.tiles, P.segs, P.cta,
                                                                                         P.ws, E->d_glob);
     E->launches++;
     return cudaGetLastError();
@@ -2387,8 +2438,7 @@ cudaError_t launch_contract(ucg_ensemble *E, bool klo = true)
     switch (E->ni) {
     case 32: return klo ? launch_contract_t<32, true, 1>(E, E->p1) : launch_contract_t<32, false, 2>(E, E->p2);
     case 64: return klo ? launch_contract_t<64, true, 1>(E, E->p1) : launch_contract_t<64, false, 2>(E, E->p2);
-    case 128: return klo ? launch_contract_t<128, true, 1>(E, E->p1) : launch_contract_t<128, false, 2>(E, E->p2);
-    default: return cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;   // 128-instance tiles: hierarchical geometries only
     }
 }
 
@@ -2440,10 +2490,18 @@ int ensure_b(ucg_ensemble *E, int ni)
     for (EnsGeomHost &g : E->geoms) {
         if (g.B && g.b_ni == ni) continue;
         if (g.B) cudaFree(g.B);
+        if (g.vscale) cudaFree(g.vscale);
         g.B = nullptr;
+        g.vscale = nullptr;
         const size_t bytes = b_bytes(g, ni);
         ECUDA(cudaMalloc(&g.B, bytes));
         ECUDA(cudaMemsetAsync(g.B, 0, bytes, E->stream));
+        if (!g.hier) {
+            // padding instances of the last tile keep zero images and zero scales
+            const size_t vb = sizeof(float) * (size_t)((g.ninst + ni - 1) / ni) * g.kblocks * ni;
+            ECUDA(cudaMalloc(&g.vscale, vb));
+            ECUDA(cudaMemsetAsync(g.vscale, 0, vb, E->stream));
+        }
         g.b_ni = ni;
     }
     return UCG_OK;
@@ -2460,7 +2518,11 @@ int upload_plan(ucg_ensemble *E, PlanBufs &P, int ni, int mt, const Sched &s)
                 units.push_back(GemmTile{g.A + (size_t)t * g.kblocks * A_IMG,
                                          (mt == 2 && t + 1 < g.mtiles) ? g.A + (size_t)(t + 1) * g.kblocks * A_IMG
                                                                        : nullptr,
-                                         g.B + (size_t)nt * g.kblocks * (size_t)(2 * ni * BK * 2)});
+                                         g.B + (size_t)nt * g.kblocks * (size_t)(2 * ni * BK * 2),
+                                         g.kscale + (size_t)t * g.kblocks,
+                                         (mt == 2 && t + 1 < g.mtiles) ? g.kscale + (size_t)(t + 1) * g.kblocks
+                                                                       : nullptr,
+                                         g.vscale + (size_t)nt * g.kblocks * ni});
     }
     P.nunits = (int)units.size();
     P.nsegs = (int)s.segs.size();
@@ -2535,6 +2597,7 @@ int install_plan(ucg_ensemble *E, int ni, const Sched &s1, const Sched &s2)
         d.blk_s0 = bs;
         bs += d.epb_s * g.ninst;
         d.B = g.B;
+        d.vscale = g.vscale;
         d.rscale = g.rscale;
         const long len = (long)g.ninst * 7 * g.np;
         double *v = g.state;
@@ -2582,11 +2645,21 @@ int install_plan(ucg_ensemble *E, int ni, const Sched &s1, const Sched &s2)
     return UCG_OK;
 }
 
+bool has_dense(const ucg_ensemble *E)
+{
+    for (const EnsGeomHost &g : E->geoms)
+        if (!g.hier) return true;
+    return false;
+}
+
+// instance tile width: 128 only for hierarchical-only ensembles (the dense
+// contraction's per-k-block drain keeps 2 x 64 register sums per thread)
 int default_ni(ucg_ensemble *E)
 {
     int mx = 1;
     for (const EnsGeomHost &g : E->geoms) mx = std::max(mx, g.ninst);
-    return mx <= 32 ? 32 : (mx <= 64 ? 64 : 128);
+    const int ni = mx <= 32 ? 32 : (mx <= 64 ? 64 : 128);
+    return (ni == 128 && has_dense(E)) ? 64 : ni;
 }
 
 // the schedule of a kind for the single-tile (mt 1) or paired (mt 2) units
@@ -2762,7 +2835,7 @@ void ucg_ens_destroy(ucg_ensemble *E)
     if (E->stream) cudaStreamSynchronize(E->stream);
     free_plan(E);
     for (EnsGeomHost &g : E->geoms) {
-        void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl, g.B, g.hA, g.hbidx, g.hperm, g.hinv,
+        void *ptrs[] = {g.A, g.rscale, g.kscale, g.vscale, g.state, g.anchor, g.par, g.ctl, g.B, g.hA, g.hbidx, g.hperm, g.hinv,
                         g.hxpos, g.hrow, g.hzdst};
         for (void *p : ptrs)
             if (p) cudaFree(p);
@@ -2819,6 +2892,7 @@ int ucg_ens_add_geometry(ucg_ensemble *E, ucg_ctx *c, int n_instances, int *geom
     } else {
         e = cudaMalloc(&g.A, aimg);
         if (e == cudaSuccess) e = cudaMalloc(&g.rscale, sizeof(float) * rows_pad);
+        if (e == cudaSuccess) e = cudaMalloc(&g.kscale, sizeof(float) * (size_t)g.mtiles * g.kblocks);
     }
     if (e == cudaSuccess) e = cudaMalloc(&g.state, sizeof(double) * 12 * len);
     if (e == cudaSuccess) e = cudaMalloc(&g.anchor, sizeof(double) * 5L * g.ninst * g.np);
@@ -2837,16 +2911,20 @@ int ucg_ens_add_geometry(ucg_ensemble *E, ucg_ctx *c, int n_instances, int *geom
         e = cudaMemcpy(g.ctl, ctl.data(), sizeof(InstCtl) * g.ninst, cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess && !hier) {
+        // K = diag(row scale) (block scale) (hi + 2^-11 lo): the contraction's
+        // drain applies the block scales, the stage epilogue the row scales
         k_row_scale<<<(unsigned)((rows_pad + 7) / 8), 256, 0, E->stream>>>(c->K, g.m, g.n, rows_pad, g.rscale);
+        k_block_scale<<<(unsigned)(g.mtiles * g.kblocks), 256, 0, E->stream>>>(c->K, g.m, g.n, g.kblocks, g.rscale,
+                                                                              g.kscale);
         const long work = rows_pad * (long)g.kblocks * (BK / 8);
         k_pack_k<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(c->K, g.m, g.n, g.kblocks, rows_pad,
-                                                                       g.rscale, g.A);
-        E->launches += 2;
+                                                                       g.rscale, g.kscale, g.A);
+        E->launches += 3;
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
     if (e != cudaSuccess) {
-        void *ptrs[] = {g.A, g.rscale, g.state, g.anchor, g.par, g.ctl, g.hA, g.hbidx, g.hperm, g.hinv, g.hxpos, g.hrow,
+        void *ptrs[] = {g.A, g.rscale, g.kscale, g.state, g.anchor, g.par, g.ctl, g.hA, g.hbidx, g.hperm, g.hinv, g.hxpos, g.hrow,
                         g.hzdst};
         for (void *p : ptrs)
             if (p) cudaFree(p);
@@ -3029,6 +3107,8 @@ int ucg_ens_plan(ucg_ensemble *E, int ni, int schedule, int chunk)
     if (!E) return UCG_E_BADARG;
     if (E->geoms.empty()) return ebad(E, UCG_E_STATE, "ensemble has no geometry");
     if (ni != 32 && ni != 64 && ni != 128) return ebad(E, UCG_E_BADARG, "ni must be 32, 64 or 128");
+    if (ni == 128 && has_dense(E))
+        return ebad(E, UCG_E_UNSUPPORTED, "ni 128 is for hierarchical geometries only");
     if (schedule != UCG_ENS_STREAM_K && schedule != UCG_ENS_SPLIT_LPT) return ebad(E, UCG_E_BADARG, "unknown schedule");
     ECUDA(cudaSetDevice(E->device));
     ECUDA(cudaStreamSynchronize(E->stream));
@@ -3045,7 +3125,7 @@ int ucg_ens_tune(ucg_ensemble *E, int reps, char *report, long report_len)
     int maxinst = 1;
     for (const EnsGeomHost &g : E->geoms) maxinst = std::max(maxinst, g.ninst);
     std::vector<int> nis = {default_ni(E)};
-    if (maxinst > 64 && nis[0] != 64) nis.push_back(64);
+    if (maxinst > 64 && nis[0] != 64) nis.push_back(64);   // (default 128: hierarchical only)
     std::string rep;
     // the anchor's schedule (single tiles) and the increments' (pairs) are chosen
     // independently; an attempt costs one anchor and five increment contractions
@@ -3112,9 +3192,9 @@ int ucg_ens_matvec(ucg_ensemble *E, int gi, const double *V, double *T, int term
             const long work = (long)g.ninst * g.np;
             k_pack_x_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(E->d_args, gi, dV);
         } else {
-            const long work = (long)g.ninst * ((g.n + 1) / 2);
-            k_pack_v_dense<<<(unsigned)((work + 255) / 256), 256, 0, E->stream>>>(g.B, E->ni, g.kblocks, g.ninst,
-                                                                                 g.n, dV);
+            const long warps = (long)g.ninst * g.kblocks;
+            k_pack_v_dense<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, E->stream>>>(g.B, g.vscale, E->ni,
+                                                                                       g.kblocks, g.ninst, g.n, dV);
         }
         e = cudaGetLastError();
     }

@@ -312,9 +312,9 @@ template <> struct TmTraits<float> {   // the anchor of the split form: K/s in F
     static constexpr int PER = 4, CH = 1024, ROWS = 24, STAGES = 2;
     using Acc = double;
 };
-template <> struct TmTraits<__nv_bfloat16> {   // the hi plane alone (anchored stages 2-6)
+template <> struct TmTraits<__half> {   // the fp16 plane (anchored stages 2-6), FP64 sums
     static constexpr int PER = 8, CH = 2048, ROWS = 24, STAGES = 2;
-    using Acc = float;
+    using Acc = double;
 };
 template <class KT>
 constexpr size_t tm_smem_bytes()
@@ -327,7 +327,7 @@ constexpr size_t tm_smem_bytes()
 template <class KT> struct TmV;
 template <> struct TmV<double> { double2 x; };
 template <> struct TmV<float> { double x[4]; };
-template <> struct TmV<__nv_bfloat16> { float x[8]; };
+template <> struct TmV<__half> { double x[8]; };
 
 template <class KT>
 __device__ __forceinline__ void tm_load_v(const double *v, long c, long n, TmV<KT> &vr);
@@ -352,19 +352,19 @@ __device__ __forceinline__ void tm_load_v<float>(const double *v, long c, long n
     for (int q = 0; q < 4; q++) vr.x[q] = (c + q < n) ? v[c + q] : 0.0;
 }
 template <>
-__device__ __forceinline__ void tm_load_v<__nv_bfloat16>(const double *v, long c, long n, TmV<__nv_bfloat16> &vr)
+__device__ __forceinline__ void tm_load_v<__half>(const double *v, long c, long n, TmV<__half> &vr)
 {
     if (c + 8 <= n) {
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const double2 a = __ldg(reinterpret_cast<const double2 *>(v + c + 2 * q));
-            vr.x[2 * q] = (float)a.x;
-            vr.x[2 * q + 1] = (float)a.y;
+            vr.x[2 * q] = a.x;
+            vr.x[2 * q + 1] = a.y;
         }
         return;
     }
 #pragma unroll
-    for (int q = 0; q < 8; q++) vr.x[q] = (c + q < n) ? (float)v[c + q] : 0.0f;
+    for (int q = 0; q < 8; q++) vr.x[q] = (c + q < n) ? v[c + q] : 0.0;
 }
 
 template <class KT>
@@ -386,15 +386,15 @@ __device__ __forceinline__ void tm_accumulate<float>(const float *srow, int cl, 
     acc = fma((double)kv.w, vr.x[3], acc);
 }
 template <>
-__device__ __forceinline__ void tm_accumulate<__nv_bfloat16>(const __nv_bfloat16 *srow, int cl,
-                                                             const TmV<__nv_bfloat16> &vr, float &acc)
+__device__ __forceinline__ void tm_accumulate<__half>(const __half *srow, int cl, const TmV<__half> &vr, double &acc)
 {
     const uint4 raw = *reinterpret_cast<const uint4 *>(srow + cl);
     const uint32_t w4[4] = {raw.x, raw.y, raw.z, raw.w};
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        acc = fmaf(__uint_as_float(w4[q] << 16), vr.x[2 * q], acc);
-        acc = fmaf(__uint_as_float(w4[q] & 0xffff0000u), vr.x[2 * q + 1], acc);
+        const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w4[q]));
+        acc = fma((double)f.x, vr.x[2 * q], acc);
+        acc = fma((double)f.y, vr.x[2 * q + 1], acc);
     }
 }
 
@@ -709,7 +709,8 @@ __global__ void k_clear_pending(Ctl *ctl) { ctl->pending = 0; }
 
 bool rk_anchored(const ucg_ctx *c)
 {
-    return (c->precision == UCG_PREC_SPLIT_BF16 && c->Ksp != nullptr) || c->precision == UCG_PREC_HMATRIX_SPLIT;
+    return ((c->precision == UCG_PREC_SPLIT_BF16 || c->precision == UCG_PREC_SPLIT_PAIR) && c->Ksp != nullptr) ||
+           c->precision == UCG_PREC_HMATRIX_SPLIT;
 }
 
 // the attempt graph holds device addresses of the matrix and parameter arrays;
@@ -828,10 +829,10 @@ static void launch_traction_t(ucg_ctx *c, const StageArgs &a, const KT *K, long 
 template <int S>
 static void launch_traction(ucg_ctx *c, const StageArgs &a)
 {
-    if (S > 1 && rk_anchored(c) && c->Khi_plane) {
-        // anchored stages multiply the increments by the hi plane alone
-        launch_traction_t<S, __nv_bfloat16>(c, a, c->Khi_plane, c->ldk_split, c->Kscale);
-    } else if (c->precision == UCG_PREC_SPLIT_BF16 && c->Ksp) {
+    if (S > 1 && c->precision == UCG_PREC_SPLIT_BF16 && rk_anchored(c) && c->Khi_plane) {
+        // anchored stages multiply the increments by the fp16 plane
+        launch_traction_t<S, __half>(c, a, c->Khi_plane, c->ldk_split, c->Kscale);
+    } else if ((c->precision == UCG_PREC_SPLIT_BF16 || c->precision == UCG_PREC_SPLIT_PAIR) && c->Ksp) {
         launch_traction_t<S, float>(c, a, c->Ksp, c->ldk_split, c->Kscale);
     } else {
         launch_traction_t<S, double>(c, a, c->K, c->n, nullptr);

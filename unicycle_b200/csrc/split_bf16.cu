@@ -5,8 +5,9 @@
 //     16-bit lo extension of the significand (its lower 16 bits): 4 bytes per
 //     entry, half the FP64 stream, relative error <= 2^-24 per entry.  The
 //     stage-1 anchor of every step reads it and sums in FP64;
-//   * the hi plane: bf16(k) rounded to nearest, 2 bytes per entry (relative
-//     error <= 2^-8), which the anchored stages 2-6 multiply against the
+//   * the increment plane: fp16(k) rounded to nearest, 2 bytes per entry
+//     (relative error <= 2^-11 down to 2^-14 of the row maximum, an absolute
+//     2^-25 of it below), which the anchored stages 2-6 multiply against the
 //     velocity increments.
 #include <cmath>
 #include <cmath>
@@ -36,18 +37,18 @@ __global__ void k_row_absmax(const double *__restrict__ K, long n, float *__rest
 
 // out has row stride ldk >= n; the padding columns hold zeros
 __global__ void k_split(const double *__restrict__ K, long n, long ldk, long total, const float *__restrict__ scale,
-                        float *__restrict__ out, __nv_bfloat16 *__restrict__ out_hi)
+                        float *__restrict__ out, __half *__restrict__ out_hi)
 {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const long r = i / ldk, cc = i - r * ldk;
         if (cc >= n) {
             out[i] = 0.0f;
-            out_hi[i] = __double2bfloat16(0.0);
+            out_hi[i] = __float2half_rn(0.0f);
             continue;
         }
         const double x = K[r * n + cc] / (double)scale[r];
         out[i] = __double2float_rn(x);
-        out_hi[i] = __double2bfloat16(x);
+        out_hi[i] = __double2half(x);
     }
 }
 
@@ -60,7 +61,7 @@ int split_bf16_build(ucg_ctx *c)
     const long total = c->ldk_split * c->m;
     cudaError_t e = cudaMalloc(&c->Ksp, sizeof(float) * (size_t)total);
     if (e != cudaSuccess) { c->Ksp = nullptr; return cuda_fail(c, e, "cudaMalloc(split K)"); }
-    e = cudaMalloc(&c->Khi_plane, sizeof(__nv_bfloat16) * (size_t)total);
+    e = cudaMalloc(&c->Khi_plane, sizeof(__half) * (size_t)total);
     if (e != cudaSuccess) { c->Khi_plane = nullptr; return cuda_fail(c, e, "cudaMalloc(split K hi plane)"); }
     UCG_CUDA(cudaMalloc(&c->Kscale, sizeof(float) * (size_t)c->m));
     k_row_absmax<<<(unsigned)c->m, 256, 0, c->stream>>>(c->K, c->n, c->Kscale);

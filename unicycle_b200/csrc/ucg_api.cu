@@ -287,7 +287,7 @@ int ucg_assemble(ucg_ctx *c, int okada_mode)
     split_bf16_free(c);
     int rc = assemble_matrix(c, okada_mode);
     if (rc) return rc;
-    if (c->precision == UCG_PREC_SPLIT_BF16) return split_bf16_build(c);
+    if (c->precision == UCG_PREC_SPLIT_BF16 || c->precision == UCG_PREC_SPLIT_PAIR) return split_bf16_build(c);
     return UCG_OK;
 }
 
@@ -325,7 +325,8 @@ int ucg_copy_G(ucg_ctx *c, double *G, long ld, long k0, long k1)
 int ucg_set_precision(ucg_ctx *c, int precision)
 {
     if (!c) return UCG_E_BADARG;
-    if (precision != UCG_PREC_FP64 && precision != UCG_PREC_SPLIT_BF16 && precision != UCG_PREC_HMATRIX &&
+    if (precision != UCG_PREC_FP64 && precision != UCG_PREC_SPLIT_BF16 && precision != UCG_PREC_SPLIT_PAIR &&
+        precision != UCG_PREC_HMATRIX &&
         precision != UCG_PREC_HMATRIX_SPLIT)
         return bad(c, "precision");
     if (precision == UCG_PREC_HMATRIX || precision == UCG_PREC_HMATRIX_SPLIT) {
@@ -341,7 +342,8 @@ int ucg_set_precision(ucg_ctx *c, int precision)
     if (precision == UCG_PREC_FP64 && c->assembled && !c->K)
         return set_err(c, UCG_E_STATE, "FP64 matrix was released; re-assemble");
     c->precision = precision;
-    if (precision == UCG_PREC_SPLIT_BF16 && c->assembled && !c->Ksp) return split_bf16_build(c);
+    if ((precision == UCG_PREC_SPLIT_BF16 || precision == UCG_PREC_SPLIT_PAIR) && c->assembled && !c->Ksp)
+        return split_bf16_build(c);
     return UCG_OK;
 }
 

@@ -140,7 +140,7 @@ struct ucg_ctx {
     int precision = UCG_PREC_FP64;
     bool keep_fp64 = true;
     float *Ksp = nullptr;                            // K/s in FP32: bf16 hi bits + 16-bit lo extension
-    __nv_bfloat16 *Khi_plane = nullptr;              // hi alone, same row stride
+    __half *Khi_plane = nullptr;                     // fp16 of K/s (stage increments), same row stride
     float *Kscale = nullptr;   // per row
     long ldk_split = 0;        // row stride of the split matrix (n padded to a multiple of 8)
 

@@ -160,7 +160,8 @@ class Simulation:
         return out
 
     def set_precision(self, precision):
-        p = {"fp64": _lib.UCG_PREC_FP64, "split_bf16": _lib.UCG_PREC_SPLIT_BF16}.get(precision, precision)
+        p = {"fp64": _lib.UCG_PREC_FP64, "split_bf16": _lib.UCG_PREC_SPLIT_BF16,
+             "split_pair": _lib.UCG_PREC_SPLIT_PAIR}.get(precision, precision)
         self._check(self.lib.ucg_set_precision(self.ctx, p), "set_precision")
 
     def keep_fp64(self, keep):
