@@ -67,6 +67,9 @@ def parse():
                         "(for ncu, which does not follow conditional graph nodes)")
     p.add_argument("--no-learned", action="store_true", help="skip the learned step-size leg")
     p.add_argument("--no-split", action="store_true", help="skip the single-instance split-BF16 leg")
+    p.add_argument("--ens-terms", type=int, default=3, choices=[2, 3],
+                   help="ensemble stage increments: 3 (the anchor form, histories within 1e-6 of FP64) or 2 "
+                        "(K hi only, half the bytes)")
     p.add_argument("--no-hmatrix", action="store_true", help="skip the hierarchical-matrix leg")
     p.add_argument("--hm-eta", type=float, default=2.0, help="hierarchical matrix: admissibility parameter")
     p.add_argument("--hm-eps", type=float, default=1e-6, help="hierarchical matrix: ACA relative accuracy")
@@ -963,6 +966,7 @@ def run_hier_ensemble(args, world, rank, local):
                          fr["damping"])
         ens.set_state(0, i, y0, 0.0, cfg["dt0"])
     ens.set_tolerance(cfg["epsilon"])
+    ens.set_increment_terms(args.ens_terms)
     if args.ens_eager:
         ens.use_graph(False)
     stream = torch.cuda.ExternalStream(ens.stream, device=local)
@@ -1117,6 +1121,31 @@ def run_hmatrix(args, world, rank, local):
             "gpu_launches": int(launches), "clocks": clk.summary(), "cpu_baseline": None}
 
 
+def ens_roofline(args, ms_a, ms_c, a_bytes, a_flops, c_bytes, c_flops, peak, peak_kind, tpeak, tpeak_kind):
+    """Roofline of the ensemble's dominant kernel: the three-term contraction,
+    which runs every stage with the default increment form, or the two-term
+    increment contraction (5 of 6 stages) with --ens-terms 2; the other form
+    beside it."""
+    full = {"kernel": "k_bf16x3_contract<64,true,1> (tcgen05 Khi Vhi + 2^-11 (Khi Vlo + Klo Vhi), per-k-block "
+                      "drains; every stage)" if args.ens_terms == 3 else
+                      "k_bf16x3_contract<64,true,1> (stage 1)",
+            "ms_per_launch": ms_a, "bytes_per_launch": a_bytes, "achieved": a_bytes / (ms_a / 1e3) / 1e9,
+            "frac": a_bytes / (ms_a / 1e3) / 1e9 / peak, "tensor_tflops": a_flops / (ms_a / 1e3) / 1e12,
+            "traffic": load_traffic("k_bf16x3_contract")}
+    two = {"kernel": "k_bf16x3_contract<64,false,2> (tcgen05 Khi (Vhi + 2^-11 Vlo); stages 2-6 with --ens-terms 2)",
+           "ms_per_launch": ms_c, "bytes_per_launch": c_bytes, "achieved": c_bytes / (ms_c / 1e3) / 1e9,
+           "frac": c_bytes / (ms_c / 1e3) / 1e9 / peak, "tensor_tflops": c_flops / (ms_c / 1e3) / 1e12,
+           "traffic": load_traffic("k_bf16x3_contract_increment")}
+    main, other = (full, two) if args.ens_terms == 3 else (two, full)
+    flops = a_flops if args.ens_terms == 3 else c_flops
+    ms = main["ms_per_launch"]
+    return {"bound": "hbm", "achieved": main["achieved"], "peak": peak, "unit": "GB/s", "frac": main["frac"],
+            "traffic": main["traffic"], "kernel": main["kernel"], "ms_per_launch": ms, "peak_source": peak_kind,
+            "bytes_per_launch": main["bytes_per_launch"], "tensor_tflops": flops / (ms / 1e3) / 1e12,
+            "tensor_peak_tflops": tpeak, "tensor_frac": flops / (ms / 1e3) / 1e12 / tpeak,
+            "tensor_peak_source": tpeak_kind, "other_form": other}
+
+
 def run_ensemble(args, world, rank, local):
     """Headline: args.sets frictional parameter sets of the N = 20k model in one
     ensemble, beside the same model as one plain FP64 instance."""
@@ -1237,18 +1266,8 @@ def run_ensemble(args, world, rank, local):
             "plain_fp64": {k: plain[k] for k in ("value", "unit", "ms_per_step", "sim_years_per_hour",
                                                  "rejected_attempts", "roofline", "e2e", "gpu_launches")},
             "assembly": plain["assembly"],
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": load_traffic("k_bf16x3_contract_increment"),
-                         "kernel": "k_bf16x3_contract<64,false> (tcgen05 Khi Vhi + Khi Vlo, FP32 accumulators; "
-                                   "stages 2-6)",
-                         "ms_per_launch": ms_c, "peak_source": peak_kind, "bytes_per_launch": c_bytes,
-                         "tensor_tflops": c_flops / (ms_c / 1e3) / 1e12, "tensor_peak_tflops": tpeak,
-                         "tensor_frac": c_flops / (ms_c / 1e3) / 1e12 / tpeak, "tensor_peak_source": tpeak_kind,
-                         "anchor": {"kernel": "k_bf16x3_contract<64,true> (+ Klo Vhi; stage 1)", "ms_per_launch": ms_a,
-                                    "bytes_per_launch": a_bytes, "achieved": a_bytes / (ms_a / 1e3) / 1e9,
-                                    "frac": a_bytes / (ms_a / 1e3) / 1e9 / peak,
-                                    "tensor_tflops": a_flops / (ms_a / 1e3) / 1e12,
-                                    "traffic": load_traffic("k_bf16x3_contract")}},
+            "roofline": ens_roofline(args, ms_a, ms_c, a_bytes, a_flops, c_bytes, c_flops, peak, peak_kind, tpeak,
+                                     tpeak_kind),
             "autotune": tune_report.strip().splitlines(),
             "e2e": {"value": world * acc_e2e / e2e_elapsed, "unit": "steps/s",
                     "h2d_bytes_per_step": 8 * 7 * n * args.sets, "d2h_bytes_per_step": 8 * 7 * n * args.sets,

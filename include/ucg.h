@@ -48,8 +48,9 @@ typedef struct ucg_ctx ucg_ctx;
 #define UCG_PREC_SPLIT_PAIR  4  /* the same split pair for every stage (half of the FP64 bytes),
                                    anchored, FP64 sums: the accurate split form */
 #define UCG_PREC_HMATRIX     2  /* hierarchical approximation of K (ucg_build_hmatrix), FP64 */
-#define UCG_PREC_HMATRIX_SPLIT 3  /* the same stored as bf16 hi + lo, anchored stages (hi alone for
-                                     the stage increments), FP64 sums */
+#define UCG_PREC_HMATRIX_SPLIT 3  /* the same stored as the FP32 value of every entry in two 16-bit
+                                     planes (bf16 hi, lo extension): half the FP64 bytes for every
+                                     stage, anchored stages, FP64 sums */
 
 /* driver conventions (ucg_create flags) */
 #define UCG_DRIVER_RATESTATE      0  /* fortran/3d/src/ratestate.f90     */
@@ -455,10 +456,11 @@ int ucg_ens_get_states(ucg_ensemble *ens, int geometry, double *y, double *time,
    fortran/3d/src/ratestate.f90:307-326).  No reference counterpart. */
 int ucg_ens_put_states(ucg_ensemble *ens, int geometry, const double *y);
 
-/* Precision of the stage increments (stages 2-6 contract v_s - v1): terms = 2,
-   the default, Khi (Vhi + Vlo) over pairs of M-tiles (half the matrix bytes of
-   the anchor); terms = 3, the anchor's form Khi Vhi + Khi Vlo + Klo Vhi with
-   its FP32 sums cut into pieces of at most 16,384 sources.  No reference
+/* Precision of the stage increments (stages 2-6 contract v_s - v1): terms = 3,
+   the default, the anchor's form Khi Vhi + 2^-11 (Khi Vlo + Klo Vhi), which
+   keeps slip-rate histories within 1e-6 of the FP64 integrator's; terms = 2,
+   Khi (Vhi + Vlo) over pairs of M-tiles, half the matrix bytes and fp16
+   precision of K (about 2e-5 on the same histories).  No reference
    counterpart. */
 int ucg_ens_set_increment_terms(ucg_ensemble *ens, int terms);
 

@@ -128,6 +128,8 @@ struct Tile {
     // register sums would not fit (128 instances x 2 M-tiles).
     static constexpr bool KDRAIN = true;
     static constexpr int NCOL = MT == 2 ? NI : NI / 2;   // register sums per drain thread
+    static constexpr bool TWO_LEVEL = NCOL <= 32;          // FP32 over FOLD k-blocks, then FP64
+    static constexpr int FOLD = 8;
     static_assert(MERGE, "the drain adds the hi and 2^-11 halves of a merged accumulator");
 };
 
@@ -519,9 +521,15 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
             const GemmSeg sg = segs[q];
             const int nt = (MT == 2 && tiles[sg.tile].a1 != nullptr) ? 2 : 1;
             const bool mine = u < nt;                 // a pair's missing second tile: wait and release only
-            double sum[NC];
+            // FP32 sums over up to FOLD k-blocks, folded into FP64 sums (with one
+            // M-tile per group; the two-tile increments keep FP32 sums, their K
+            // hi truncation dominates)
+            float part[NC];
+            double sum[T::TWO_LEVEL ? NC : 1];
 #pragma unroll
-            for (int c = 0; c < NC; c++) sum[c] = 0.0;
+            for (int c = 0; c < NC; c++) part[c] = 0.0f;
+#pragma unroll
+            for (int c = 0; c < (T::TWO_LEVEL ? NC : 1); c++) sum[c] = 0.0;
             const GemmTile tl = tiles[sg.tile];
             for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
                 const int buf = (int)(it & 1);
@@ -536,7 +544,7 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
                 }
                 tc_fence_after();
                 if (mine) {
-                    const double sk = (double)(u == 0 ? tl.ks : tl.ks1)[kb];
+                    const float sk = (u == 0 ? tl.ks : tl.ks1)[kb];
                     const float *vs = tl.vs + (size_t)kb * NI + cbase;
                     const uint32_t tbase = tmem + (uint32_t)((buf * MT + u) * T::ACC_N + cbase) +
                                            ((uint32_t)(quarter * 32) << 16);
@@ -548,10 +556,17 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
                         tmem_wait_ld();
 #pragma unroll
                         for (int i = 0; i < 8; i++) {
-                            // hi products + 2^-11 lo products (exact in FP64), times the block scales
-                            const double x = (double)__uint_as_float(r[i]) +
-                                             (double)__uint_as_float(r2[i]) * (double)LO_UNSCALE;
-                            sum[c0 + i] = fma(x, sk * (double)__ldg(vs + c0 + i), sum[c0 + i]);
+                            // hi products + 2^-11 lo products, times the block scales (powers of
+                            // two: exact)
+                            const float x = __fmaf_rn(__uint_as_float(r2[i]), LO_UNSCALE, __uint_as_float(r[i]));
+                            part[c0 + i] = __fmaf_rn(x, sk * __ldg(vs + c0 + i), part[c0 + i]);
+                        }
+                    }
+                    if (T::TWO_LEVEL && ((kb - sg.kb0) % T::FOLD == T::FOLD - 1 || kb == sg.kb1 - 1)) {
+#pragma unroll
+                        for (int c = 0; c < NC; c++) {
+                            sum[T::TWO_LEVEL ? c : 0] += (double)part[c];
+                            part[c] = 0.0f;
                         }
                     }
                 }
@@ -563,7 +578,8 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
             if (mine) {
                 float *dst = ws + ((size_t)sg.slot * MT + u) * NI * BM + (size_t)cbase * BM + row;
 #pragma unroll
-                for (int c = 0; c < NC; c++) dst[(size_t)c * BM] = (float)sum[c];
+                for (int c = 0; c < NC; c++)
+                    dst[(size_t)c * BM] = T::TWO_LEVEL ? (float)sum[T::TWO_LEVEL ? c : 0] : part[c];
             }
         }
     }
@@ -1813,7 +1829,7 @@ struct ucg_ensemble {
     EnsGlobal *h_glob = nullptr;   // pinned
     cudaGraphExec_t graph = nullptr;
     bool use_graph = true;     // false: attempts launched one by one from the host
-    bool inc_full = false;     // stage increments: three-term form (Khi Vhi + Khi Vlo + Klo Vhi)
+    bool inc_full = true;      // stage increments: three-term form (Khi Vhi + Khi Vlo + Klo Vhi)
     long launches = 0;
 };
 
@@ -2819,6 +2835,7 @@ int ucg_ens_create(ucg_ensemble **out, int device)
     }
     cudaDeviceGetAttribute(&E->sms, cudaDevAttrMultiProcessorCount, device);
     memset(E->h_glob, 0, sizeof(EnsGlobal));
+    E->h_glob->inc_full = E->inc_full ? 1 : 0;
     E->h_glob->epsilon = E->epsilon;
     E->h_glob->hmax = E->hmax;
     E->h_glob->ev_on = 1.0e-3;

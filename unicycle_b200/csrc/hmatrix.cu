@@ -508,22 +508,31 @@ __global__ void __launch_bounds__(128) k_hm_rows(const HLeafTerm *__restrict__ t
     part[(long)blockIdx.x * rows_max + i] = (a0 + a1) + (a2 + a3);
 }
 
-// ---- split (bf16 hi + lo) form ---------------------------------------------------------
+// ---- split (hi + lo) form ---------------------------------------------------------------
 //
-// Every stored value x is kept as hi = bf16(x) and lo = bf16(x - hi) (relative
-// error ~2^-16).  The anchored Runge-Kutta stages read hi and lo for the stage-1
-// product and hi alone for the stage increments (2 bytes per value), as the
-// dense split-BF16 path does.
+// Every stored value x is kept as its FP32 rounding split into two 16-bit
+// planes: hi, the upper half (a bf16 number: sign, exponent, 7 significand
+// bits) and lo, the lower 16 significand bits.  hi and lo together give the
+// FP32 value exactly (relative error <= 2^-24); the anchored Runge-Kutta
+// stages read both for every stage (4 bytes per value, half the FP64 stream)
+// and sum in FP64.
+
+__device__ __forceinline__ void split32(double v, __nv_bfloat16 &hi, __nv_bfloat16 &lo)
+{
+    const uint32_t b = __float_as_uint(__double2float_rn(v));
+    hi = __ushort_as_bfloat16((unsigned short)(b >> 16));
+    lo = __ushort_as_bfloat16((unsigned short)(b & 0xffffu));
+}
+__device__ __forceinline__ float join32(__nv_bfloat16 hi, __nv_bfloat16 lo)
+{
+    return __uint_as_float(((uint32_t)__bfloat16_as_ushort(hi) << 16) | (uint32_t)__bfloat16_as_ushort(lo));
+}
 
 __global__ void k_split_flat(const double *__restrict__ x, long n, __nv_bfloat16 *__restrict__ hi,
                              __nv_bfloat16 *__restrict__ lo)
 {
-    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-        const double v = x[t];
-        const __nv_bfloat16 h = __double2bfloat16(v);
-        hi[t] = h;
-        lo[t] = __double2bfloat16(v - (double)__bfloat162float(h));
-    }
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
+        split32(x[t], hi[t], lo[t]);
 }
 
 struct SplitJob {
@@ -535,12 +544,7 @@ __global__ void k_split_jobs(const SplitJob *__restrict__ jobs, __nv_bfloat16 *_
                              __nv_bfloat16 *__restrict__ lo)
 {
     const SplitJob J = jobs[blockIdx.x];
-    for (long t = threadIdx.x; t < J.n; t += blockDim.x) {
-        const double v = J.src[t];
-        const __nv_bfloat16 h = __double2bfloat16(v);
-        hi[J.dst + t] = h;
-        lo[J.dst + t] = __double2bfloat16(v - (double)__bfloat162float(h));
-    }
+    for (long t = threadIdx.x; t < J.n; t += blockDim.x) split32(J.src[t], hi[J.dst + t], lo[J.dst + t]);
 }
 
 template <bool LO>
@@ -559,13 +563,15 @@ __global__ void k_hm_z_split(const HLowRank *__restrict__ lr, const int2 *__rest
     const double2 *x = reinterpret_cast<const double2 *>(xp + 2L * b.s0);
     double s0 = 0.0, s1 = 0.0;
     for (int j = lane; j < (b.n >> 1); j += 32) {
-        const float2 a = __bfloat1622float2(h2[j]);
         const double2 xx = x[j];
-        double a0 = a.x, a1 = a.y;
+        double a0, a1;
         if (LO) {
-            const float2 c = __bfloat1622float2(l2[j]);
-            a0 += c.x;
-            a1 += c.y;
+            a0 = join32(h2[j].x, l2[j].x);
+            a1 = join32(h2[j].y, l2[j].y);
+        } else {
+            const float2 a = __bfloat1622float2(h2[j]);
+            a0 = a.x;
+            a1 = a.y;
         }
         s0 = fma(a0, xx.x, s0);
         s1 = fma(a1, xx.y, s1);
@@ -623,9 +629,8 @@ __global__ void __launch_bounds__(128) k_hm_rows_split(const HLeafTerm *__restri
         const double *x = (T.xsel ? z : xp) + T.xoff;
         const __nv_bfloat16 *col = sb + off + i;
         auto val = [&](int j) -> double {
-            double v = (double)__bfloat162float(col[(long)j * rows]);
-            if (LO) v += (double)__bfloat162float(col[nel + (long)j * rows]);
-            return v;
+            if (LO) return (double)join32(col[(long)j * rows], col[nel + (long)j * rows]);
+            return (double)__bfloat162float(col[(long)j * rows]);
         };
         int j = 0;
         for (; j + 3 < T.cols; j += 4) {
@@ -1054,7 +1059,7 @@ void hmatrix_apply(ucg_ctx *c, const double *v, double *t)
     c->launches.count += 3;
 }
 
-// hi / lo bf16 copies of the panels and of V (once; kept with the matrix)
+// hi / lo planes of the FP32 copies of the panels and of V (once; kept with the matrix)
 int hmatrix_split_build(ucg_ctx *c)
 {
     HMat *h = c->hm;

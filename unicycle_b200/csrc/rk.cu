@@ -849,7 +849,7 @@ static void enqueue_stage(ucg_ctx *c)
     if (c->precision == UCG_PREC_HMATRIX || c->precision == UCG_PREC_HMATRIX_SPLIT) {
         double *t = hmatrix_t(c);
         if (c->precision == UCG_PREC_HMATRIX) hmatrix_apply(c, c->st.v, t);
-        else hmatrix_apply_split(c, c->st.v, t, S == 1);   // anchor: hi + lo; increments: hi
+        else hmatrix_apply_split(c, c->st.v, t, true);     // every stage on the FP32 planes (hi + lo)
         k_rhs_t<S><<<(c->nr + c->nt + 127) / 128, 128, 0, c->stream>>>(a, c->ctl, t);
         c->launches.count += 1;
         return;
