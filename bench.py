@@ -814,49 +814,59 @@ def hmatrix_leg(args, local, sim, cfg, plain):
 
 
 def split_leg(args, local, sim, cfg, plain):
-    """The single-instance split-BF16 form on the same N = 20k model: K stored
-    as bf16 hi + lo with a per-row scale, anchored stages (stage 1 reads hi and
-    lo, stages 2-6 the hi plane alone); steps/s and simulated years per hour
-    over the same window as the plain FP64 leg, the hi-plane traction launch
-    against the HBM roofline, and the right-hand side's error against FP64."""
+    """The single-instance split forms on the same N = 20k model, K = diag(s) k:
+    split_bf16 anchors every step on the FP32 pair plane of k and contracts the
+    stage increments against an fp16 plane (a quarter of the FP64 bytes at
+    stages 2-6); split_pair uses the pair plane for every stage (half of the FP64
+    bytes; histories within 1e-6 of FP64).  Steps/s and simulated years per hour
+    over the same window as the plain FP64 leg, the traction launch against the
+    HBM roofline, and the right-hand side's error against FP64."""
     import torch
     import unicycle_b200
     n = cfg["n_patch"]
     y_probe = sim.get_state()[0]
     d64, _ = sim.odefun(y_probe)
-    sim.set_precision(unicycle_b200.UCG_PREC_SPLIT_BF16)
-    dsp, _ = sim.odefun(y_probe)
     idx = np.concatenate([np.arange(q, len(y_probe), 7) for q in (2, 3, 4)])
-    rhs_err = float(np.max(np.abs(dsp[idx] - d64[idx])) / np.max(np.abs(d64[idx])))
     stream = torch.cuda.ExternalStream(sim.stream, device=local)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    sim.set_state(cfg["y0"], 0.0, cfg["dt0"])
-    sim.run(1e300, args.spinup + args.warmup)
-    _, t_w, _, _, rej_w = sim.get_state()
-    steps_req = plain["steps"]
-    torch.cuda.synchronize()
-    e0.record(stream)
-    steps = sim.run(1e300, steps_req)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    el = e0.elapsed_time(e1) / 1e3
-    _, t_t, _, _, rej_t = sim.get_state()
-    ms_mv = sim.profile_traction(reps=10)
-    sim.set_precision(unicycle_b200.UCG_PREC_FP64)
-    alg = 2.0 * (3 * n) * (2 * n) + 4.0 * 3 * n + 8.0 * (2 * n + 3 * n)
     peak, peak_kind = load_peaks()
-    syh = (t_t - t_w) / YEAR / (el / 3600.0)
-    return {"steps_per_s": steps / el, "ms_per_step": 1e3 * el / steps, "steps": steps,
-            "sim_years_per_hour": syh, "rejected_attempts": rej_t - rej_w,
-            "speedup_vs_plain_fp64": {"steps_per_s": steps / el / plain["value"],
-                                      "sim_years_per_hour": syh / plain["sim_years_per_hour"]
-                                      if plain["sim_years_per_hour"] > 0 else None},
-            "rhs_traction_rate_max_rel_error_vs_fp64": rhs_err,
-            "roofline": {"bound": "hbm", "kernel": "k_traction<S,bf16> (hi plane x velocity increments)",
-                         "ms_per_launch": ms_mv, "bytes_per_launch": alg, "achieved": alg / (ms_mv / 1e3) / 1e9,
-                         "peak": peak, "unit": "GB/s", "frac": alg / (ms_mv / 1e3) / 1e9 / peak,
-                         "peak_source": peak_kind},
-            "dtype": "bf16 hi+lo K, f32 sums, f64 state"}
+    out = {}
+    for form in ("split_bf16", "split_pair"):
+        sim.set_precision(form)
+        dsp, _ = sim.odefun(y_probe)
+        rhs_err = float(np.max(np.abs(dsp[idx] - d64[idx])) / np.max(np.abs(d64[idx])))
+        sim.set_state(cfg["y0"], 0.0, cfg["dt0"])
+        sim.run(1e300, args.spinup + args.warmup)
+        _, t_w, _, _, rej_w = sim.get_state()
+        steps_req = plain["steps"]
+        torch.cuda.synchronize()
+        e0.record(stream)
+        steps = sim.run(1e300, steps_req)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        el = e0.elapsed_time(e1) / 1e3
+        _, t_t, _, _, rej_t = sim.get_state()
+        ms_mv = sim.profile_traction(reps=10)   # a stage-2 launch: the increment plane (bf16) or the pair plane
+        if form == "split_bf16":
+            alg = 2.0 * (3 * n) * (2 * n) + 4.0 * 3 * n + 8.0 * (2 * n + 3 * n)
+            kern = "k_traction<S,__half> (fp16 increment plane x velocity increments, FP64 sums)"
+        else:
+            alg = 4.0 * (3 * n) * (2 * n) + 4.0 * 3 * n + 8.0 * (2 * n + 3 * n)
+            kern = "k_traction<S,float> (FP32 pair plane, FP64 sums)"
+        syh = (t_t - t_w) / YEAR / (el / 3600.0)
+        out[form] = {"steps_per_s": steps / el, "ms_per_step": 1e3 * el / steps, "steps": steps,
+                     "sim_years_per_hour": syh, "rejected_attempts": rej_t - rej_w,
+                     "speedup_vs_plain_fp64": {"steps_per_s": steps / el / plain["value"],
+                                               "sim_years_per_hour": syh / plain["sim_years_per_hour"]
+                                               if plain["sim_years_per_hour"] > 0 else None},
+                     "rhs_traction_rate_max_rel_error_vs_fp64": rhs_err,
+                     "roofline": {"bound": "hbm", "kernel": kern, "ms_per_launch": ms_mv, "bytes_per_launch": alg,
+                                  "achieved": alg / (ms_mv / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                                  "frac": alg / (ms_mv / 1e3) / 1e9 / peak, "peak_source": peak_kind}}
+    sim.set_precision(unicycle_b200.UCG_PREC_FP64)
+    out["split_bf16"]["dtype"] = "FP32 pair anchor, fp16 increments, FP64 sums, f64 state"
+    out["split_pair"]["dtype"] = "FP32 pair every stage, FP64 sums, f64 state"
+    return out
 
 
 def hier_ensemble_leg(args, local, cfg, sets, y0s, dense, Kr):

@@ -534,6 +534,19 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
             for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
                 const int buf = (int)(it & 1);
                 const uint32_t use = (uint32_t)(it >> 1);
+                // this k-block's scales do not depend on the MMAs: their loads are
+                // in flight while the accumulator is awaited
+                constexpr int NV = T::TWO_LEVEL ? NC / 4 : 1;
+                float4 vv[NV];
+                float sk = 1.0f;
+                if (mine) {
+                    sk = (u == 0 ? tl.ks : tl.ks1)[kb];
+                    if (T::TWO_LEVEL) {
+                        const float4 *vs4 = reinterpret_cast<const float4 *>(tl.vs + (size_t)kb * NI + cbase);
+#pragma unroll
+                        for (int q4 = 0; q4 < NV; q4++) vv[q4] = __ldg(vs4 + q4);
+                    }
+                }
                 int got = 0;
                 if (lane == 0) got = bar_wait(&acc_full[buf], use & 1u, &abort_flag, lim) ? 1 : 0;
                 got = __shfl_sync(0xffffffffu, got, 0);
@@ -544,7 +557,6 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
                 }
                 tc_fence_after();
                 if (mine) {
-                    const float sk = (u == 0 ? tl.ks : tl.ks1)[kb];
                     const float *vs = tl.vs + (size_t)kb * NI + cbase;
                     const uint32_t tbase = tmem + (uint32_t)((buf * MT + u) * T::ACC_N + cbase) +
                                            ((uint32_t)(quarter * 32) << 16);
@@ -558,8 +570,16 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
                         for (int i = 0; i < 8; i++) {
                             // hi products + 2^-11 lo products, times the block scales (powers of
                             // two: exact)
+                            const int c = c0 + i;
+                            float sv;
+                            if (T::TWO_LEVEL) {
+                                const float4 q = vv[(c >> 2) < NV ? (c >> 2) : 0];
+                                sv = (c & 3) == 0 ? q.x : (c & 3) == 1 ? q.y : (c & 3) == 2 ? q.z : q.w;
+                            } else {
+                                sv = __ldg(vs + c);
+                            }
                             const float x = __fmaf_rn(__uint_as_float(r2[i]), LO_UNSCALE, __uint_as_float(r[i]));
-                            part[c0 + i] = __fmaf_rn(x, sk * __ldg(vs + c0 + i), part[c0 + i]);
+                            part[c] = __fmaf_rn(x, sk * sv, part[c]);
                         }
                     }
                     if (T::TWO_LEVEL && ((kb - sg.kb0) % T::FOLD == T::FOLD - 1 || kb == sg.kb1 - 1)) {
