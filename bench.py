@@ -383,6 +383,53 @@ def load_tensor_peak():
     return 1590.0, "fallback"
 
 
+def fp64_peak_tflops(local):
+    """Measured FP64 throughput of this GPU: the best of three cuBLAS DGEMMs of
+    8,192^3 (2 n^3 flops), the denominator of the assembly kernels' FP64 fraction."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=f"cuda:{local}")
+    b = torch.randn(n, n, dtype=torch.float64, device=f"cuda:{local}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e300
+    torch.matmul(a, b)
+    for _ in range(3):
+        torch.cuda.synchronize()
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def load_flops(name):
+    """FP64 flops per K entry of an assembly kernel family, counted by ncu
+    (dadd + dmul + 2 dfma thread instructions per entry), or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_flops.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f).get(name)
+    return None
+
+
+def add_fp64_fractions(fam, peak_tf):
+    """flops per entry and FP64 fraction of each assembly family."""
+    for key, name in (("okada_rect", "okada_rect"), ("bml17_vol", "bml17_vol"), ("nikkhoo_tri", "nikkhoo_tri")):
+        if key in fam and isinstance(fam[key], dict):
+            fpe = load_flops(name)
+            fam[key]["flops_per_entry"] = fpe
+            if fpe:
+                tf = fpe * fam[key]["mentries_per_s"] * 1e6 / 1e12
+                fam[key]["fp64_tflops"] = tf
+                fam[key]["fp64_frac"] = tf / peak_tf
+    fam["fp64_peak_tflops"] = peak_tf
+    fam["fp64_peak_source"] = "measured: cuBLAS DGEMM 8192^3, best of 3 (torch.matmul float64)"
+    return fam
+
+
 def assembly_leg(args, local):
     """Green's-function assembly per source family on a coupled fault + volume
     model (cfg3 geometry, reduced wedge): device time of the rectangle and the
@@ -1238,6 +1285,7 @@ def run_ensemble(args, world, rank, local):
     families = assembly_leg(args, local) if rank == 0 else None
     if families:
         families["nikkhoo_tri"] = {"entries": 6 * n * n, "ms": tri_ms, "mentries_per_s": 6 * n * n / tri_ms / 1e3}
+        families = add_fp64_fractions(families, fp64_peak_tflops(local))
     hens = None
     if rank == 0 and not args.no_hier_ensemble:
         hens = hier_ensemble_leg(args, local, cfg, sets, y0s,
