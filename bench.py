@@ -406,8 +406,9 @@ def fp64_peak_tflops(local):
 
 
 def load_flops(name):
-    """FP64 flops per K entry of an assembly kernel family, counted by ncu
-    (dadd + dmul + 2 dfma thread instructions per entry), or None."""
+    """FP64 flops per (receiver, source) pair of an assembly kernel family by
+    receiver kind, counted by ncu (dadd + dmul + 2 dfma thread instructions),
+    or None."""
     path = os.path.join(ROOT, "profiles", "ncu_flops.json")
     if os.path.exists(path):
         with open(path) as f:
@@ -415,18 +416,29 @@ def load_flops(name):
     return None
 
 
-def add_fp64_fractions(fam, peak_tf):
+def family_fp64(entry, family, peak_tf):
+    """flops per entry and FP64 fraction of one assembly family entry (its
+    `pairs` by receiver kind times the counted flops per pair)."""
+    per_pair = load_flops(family)
+    pairs = entry.get("pairs", {})
+    if per_pair and pairs and all(k in per_pair for k in pairs):
+        flops = sum(per_pair[k] * v for k, v in pairs.items())
+        tf = flops / (entry["ms"] * 1e-3) / 1e12
+        entry.update({"flops_per_entry": flops / entry["entries"], "fp64_tflops": tf, "fp64_frac": tf / peak_tf})
+    else:
+        entry["flops_per_entry"] = None
+    return entry
+
+
+def add_fp64_fractions(fam, peak_tf, names=None):
     """flops per entry and FP64 fraction of each assembly family."""
-    for key, name in (("okada_rect", "okada_rect"), ("bml17_vol", "bml17_vol"), ("nikkhoo_tri", "nikkhoo_tri")):
+    names = names or {"okada_rect": "okada_rect", "bml17_vol": "bml17_vol", "nikkhoo_tri": "nikkhoo_tri"}
+    for key, family in names.items():
         if key in fam and isinstance(fam[key], dict):
-            fpe = load_flops(name)
-            fam[key]["flops_per_entry"] = fpe
-            if fpe:
-                tf = fpe * fam[key]["mentries_per_s"] * 1e6 / 1e12
-                fam[key]["fp64_tflops"] = tf
-                fam[key]["fp64_frac"] = tf / peak_tf
+            family_fp64(fam[key], family, peak_tf)
     fam["fp64_peak_tflops"] = peak_tf
     fam["fp64_peak_source"] = "measured: cuBLAS DGEMM 8192^3, best of 3 (torch.matmul float64)"
+    fam["flops_source"] = "ncu-counted FP64 flops per pair, profiles/ncu_flops.json"
     return fam
 
 
@@ -445,8 +457,10 @@ def assembly_leg(args, local):
     nf, nv = c["n_patch"], c["n_vol"]
     sim.close()
     return {"model": f"{nf} rectangles + {nv} cuboids (K {m} x {n})",
-            "okada_rect": {"entries": m * 2 * nf, "ms": rect_ms, "mentries_per_s": m * 2 * nf / rect_ms / 1e3},
-            "bml17_vol": {"entries": m * 6 * nv, "ms": vol_ms, "mentries_per_s": m * 6 * nv / vol_ms / 1e3}}
+            "okada_rect": {"entries": m * 2 * nf, "ms": rect_ms, "mentries_per_s": m * 2 * nf / rect_ms / 1e3,
+                           "pairs": {"fault_receiver": nf * nf, "volume_receiver": nv * nf}},
+            "bml17_vol": {"entries": m * 6 * nv, "ms": vol_ms, "mentries_per_s": m * 6 * nv / vol_ms / 1e3,
+                          "pairs": {"fault_receiver": nf * nv, "volume_receiver": nv * nv}}}
 
 
 def run_cfg1(args, world, rank, local):
@@ -555,10 +569,14 @@ def run_cfg3(args, world, rank, local):
     rect_ms, _, vol_ms = sim.assembly_times()
     n, m = sim.dims
     fam = {"okada_rect_columns": {"entries": m * 2 * nf, "ms": rect_ms, "mentries_per_s": m * 2 * nf / rect_ms / 1e3,
-                                  "blocks": "fault-fault + fault-volume"},
+                                  "blocks": "fault-fault + fault-volume",
+                                  "pairs": {"fault_receiver": nf * nf, "volume_receiver": nv * nf}},
            "bml17_vol_columns": {"entries": m * 6 * nv, "ms": vol_ms, "mentries_per_s": m * 6 * nv / vol_ms / 1e3,
-                                 "blocks": "volume-fault + volume-volume"},
+                                 "blocks": "volume-fault + volume-volume",
+                                 "pairs": {"fault_receiver": nf * nv, "volume_receiver": nv * nv}},
            "total_seconds_incl_host": t_build}
+    fam = add_fp64_fractions(fam, fp64_peak_tflops(local),
+                             {"okada_rect_columns": "okada_rect", "bml17_vol_columns": "bml17_vol"})
     slip = np.zeros((nf, 2))
     slip[:, 0] = c["coseismic_slip"]
     sim.set_state(c["y0"], 0.0, c["dt0"])
@@ -1284,7 +1302,8 @@ def run_ensemble(args, world, rank, local):
     tri_ms = sim.assembly_times()[1]
     families = assembly_leg(args, local) if rank == 0 else None
     if families:
-        families["nikkhoo_tri"] = {"entries": 6 * n * n, "ms": tri_ms, "mentries_per_s": 6 * n * n / tri_ms / 1e3}
+        families["nikkhoo_tri"] = {"entries": 6 * n * n, "ms": tri_ms, "mentries_per_s": 6 * n * n / tri_ms / 1e3,
+                                   "pairs": {"fault_receiver": n * n}}
         families = add_fp64_fractions(families, fp64_peak_tflops(local))
     hens = None
     if rank == 0 and not args.no_hier_ensemble:
@@ -1405,6 +1424,7 @@ def main():
         fam = assembly_leg(args, local) if rank == 0 else None
         out = None
         if rank == 0:
+            fam = add_fp64_fractions(fam, fp64_peak_tflops(local))
             tot_e = fam["okada_rect"]["entries"] + fam["bml17_vol"]["entries"]
             tot_ms = fam["okada_rect"]["ms"] + fam["bml17_vol"]["ms"]
             out = {"metric": "GF assembly Mentries/s (coupled fault + volume)", "value": tot_e / tot_ms / 1e3,

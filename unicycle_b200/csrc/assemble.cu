@@ -539,6 +539,17 @@ int assemble_matrix(ucg_ctx *c, int okada_mode)
     cudaEvent_t ev[6];
     for (cudaEvent_t &e : ev) UCG_CUDA(cudaEventCreate(&e));
     for (double &t : c->asm_ms) t = 0.0;
+    // load the kernels' code before the first event: under lazy module loading
+    // a first launch would otherwise count the load in its family's time
+    cudaFuncAttributes fa;
+    if (c->nr) UCG_CUDA(okada_mode == UCG_OKADA_REF32IO ? cudaFuncGetAttributes(&fa, k_assemble_rect<true>)
+                                                        : cudaFuncGetAttributes(&fa, k_assemble_rect<false>));
+    if (c->nt) {
+        UCG_CUDA(cudaFuncGetAttributes(&fa, k_assemble_tri<0>));
+        UCG_CUDA(cudaFuncGetAttributes(&fa, k_assemble_tri<1>));
+        UCG_CUDA(cudaFuncGetAttributes(&fa, k_assemble_tri<2>));
+    }
+    if (c->nv) UCG_CUDA(cudaFuncGetAttributes(&fa, k_assemble_vol));
     if (c->nr) {
         std::vector<double> s;
         build_rect_sources(c, okada_mode, s);
