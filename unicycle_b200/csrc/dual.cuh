@@ -90,6 +90,18 @@ __device__ __forceinline__ Dd datan2_g(Dd y, Dd x)
               (x.v * y.z - y.v * x.z) * r};
 }
 
+// square root and its reciprocal from one square root and one division
+__device__ __forceinline__ void dsqrt_inv(Dd a, Dd &s, Dd &is)
+{
+    const double q = sqrt(a.v), r = 1.0 / q, h = 0.5 * r, g = -r * r * h;
+    s = Dd{q, h * a.x, h * a.y, h * a.z};
+    is = Dd{r, g * a.x, g * a.y, g * a.z};
+}
+// gradient-only logarithm of a, given ia = 1 / a (already formed)
+__device__ __forceinline__ Dd dlog_gi(Dd a, Dd ia) { return Dd{0.0, ia.v * a.x, ia.v * a.y, ia.v * a.z}; }
+// gradient-only arctangent of n / d: (d n' - n d') / (n^2 + d^2), one division
+__device__ __forceinline__ Dd datan_q_g(Dd n, Dd d) { return datan2_g(n, d); }
+
 // Single-direction dual: a value and one directional derivative.  Evaluating a
 // field once per coordinate direction with these keeps half the live state of
 // the three-direction type, which matters for the longest expressions.
@@ -137,6 +149,18 @@ __device__ __forceinline__ Dd1 dsqrt(Dd1 a)
 __device__ __forceinline__ Dd1 dlog_g(Dd1 a) { return Dd1{0.0, a.d / a.v}; }
 __device__ __forceinline__ Dd1 datan_g(Dd1 a) { return Dd1{0.0, a.d / (1.0 + a.v * a.v)}; }
 
+__device__ __forceinline__ void dsqrt_inv(Dd1 a, Dd1 &s, Dd1 &is)
+{
+    const double q = sqrt(a.v), r = 1.0 / q, h = 0.5 * r * a.d;
+    s = Dd1{q, h};
+    is = Dd1{r, -r * r * h};
+}
+__device__ __forceinline__ Dd1 dlog_gi(Dd1 a, Dd1 ia) { return Dd1{0.0, ia.v * a.d}; }
+__device__ __forceinline__ Dd1 datan_q_g(Dd1 n, Dd1 d)
+{
+    return Dd1{0.0, (d.v * n.d - n.v * d.d) / (n.v * n.v + d.v * d.v)};
+}
+
 // Plain value: the same closed forms evaluated for the displacement itself
 // (observation-point displacements).  The "gradient-only" forms of the dual
 // types above skip the value of a logarithm or arctangent; for this type the
@@ -164,5 +188,16 @@ __device__ __forceinline__ Dv dsqrt(Dv a) { return Dv{sqrt(a.v)}; }
 __device__ __forceinline__ Dv dlog_g(Dv a) { return Dv{log(a.v)}; }
 __device__ __forceinline__ Dv datan_g(Dv a) { return Dv{atan(a.v)}; }
 __device__ __forceinline__ Dv datan2_g(Dv y, Dv x) { return Dv{atan2(y.v, x.v)}; }
+
+// the value forms: the square root and its reciprocal, the logarithm itself,
+// and the arctangent of the quotient as written (not atan2: the value keeps
+// the closed form's branch)
+__device__ __forceinline__ void dsqrt_inv(Dv a, Dv &s, Dv &is)
+{
+    s = Dv{sqrt(a.v)};
+    is = Dv{1.0 / s.v};
+}
+__device__ __forceinline__ Dv dlog_gi(Dv a, Dv) { return Dv{log(a.v)}; }
+__device__ __forceinline__ Dv datan_q_g(Dv n, Dv d) { return Dv{atan(n.v / d.v)}; }
 
 }  // namespace ucg

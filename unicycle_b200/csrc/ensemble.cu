@@ -105,7 +105,10 @@ struct Tile {
     // accumulate into one NI-column accumulator instead
     static constexpr bool MERGE = 2 * MT * 2 * NI <= 512;
     static constexpr int ACC_N = MERGE ? 2 * NI : NI;
-    static constexpr uint32_t TMEM_COLS = 2 * MT * ACC_N; // two sets of MT FP32 accumulators
+    // sets of MT FP32 accumulators in flight between the MMA issuer and the
+    // drain: four where the 512 tensor-memory columns hold them, else two
+    static constexpr int NACC = 4 * MT * ACC_N <= 512 ? 4 : 2;
+    static constexpr uint32_t TMEM_COLS = NACC * MT * ACC_N;
     // instruction descriptor: F32 accumulator, A and B fp16 (format 0; the
     // dense images) or bf16 (format 1; the hierarchical images), both K-major,
     // N (bits 17-22, N/8), M = 128 (bits 24-28, M/16)
@@ -351,7 +354,8 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
     using T = Tile<NI, KLO, MT>;
     extern __shared__ unsigned char dyn_smem[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dyn_smem) + 1023) & ~(uintptr_t)1023);
-    __shared__ __align__(8) uint64_t full[T::STAGES], empty[T::STAGES], acc_full[2], acc_empty[2], drain;
+    __shared__ __align__(8) uint64_t full[T::STAGES], empty[T::STAGES], acc_full[T::NACC], acc_empty[T::NACC],
+        drain;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -362,7 +366,7 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
             bar_init(&full[s], 1);
             bar_init(&empty[s], 1);
         }
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < T::NACC; b++) {
             bar_init(&acc_full[b], 1);
             bar_init(&acc_empty[b], 8);   // both drain warpgroups
         }
@@ -430,8 +434,8 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
             for (int q = q0; q < q1 && !abort_flag; q++, tc++) {
                 const GemmSeg sg = segs[q];
                 const int nt = (MT == 2 && tiles[sg.tile].a1 != nullptr) ? 2 : 1;
-                int buf = tc & 1;
-                uint32_t use = (uint32_t)(tc >> 1);
+                int buf = tc % T::NACC;
+                uint32_t use = (uint32_t)(tc / T::NACC);
                 if (!T::KDRAIN) {
                     if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag, lim)) {
                         if (!abort_flag) fail();
@@ -442,9 +446,9 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
                 bool ok = true;
                 for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
                     if (T::KDRAIN) {
-                        // one accumulator per k-block, alternating between the two sets
-                        buf = (int)(it & 1);
-                        use = (uint32_t)(it >> 1);
+                        // one accumulator per k-block, taking the NACC sets in turn
+                        buf = (int)(it % T::NACC);
+                        use = (uint32_t)(it / T::NACC);
                         if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag, lim)) {
                             if (!abort_flag) fail();
                             ok = false;
@@ -531,22 +535,28 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
 #pragma unroll
             for (int c = 0; c < (T::TWO_LEVEL ? NC : 1); c++) sum[c] = 0.0;
             const GemmTile tl = tiles[sg.tile];
-            for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
-                const int buf = (int)(it & 1);
-                const uint32_t use = (uint32_t)(it >> 1);
-                // this k-block's scales do not depend on the MMAs: their loads are
-                // in flight while the accumulator is awaited
-                constexpr int NV = T::TWO_LEVEL ? NC / 4 : 1;
-                float4 vv[NV];
-                float sk = 1.0f;
-                if (mine) {
-                    sk = (u == 0 ? tl.ks : tl.ks1)[kb];
-                    if (T::TWO_LEVEL) {
-                        const float4 *vs4 = reinterpret_cast<const float4 *>(tl.vs + (size_t)kb * NI + cbase);
+            // the k-block's scales: the tile's K block scale and, per lane, the V
+            // block scale of its instance columns cbase + lane + 32 j, both
+            // loaded one k-block ahead (their latency would otherwise sit in
+            // every k-block once the drain is the busy side) and the lane's
+            // product broadcast to the warp by shuffles
+            constexpr int NL = (NC + 31) / 32;       // instance columns per lane
+            const float *ksu = u == 0 ? tl.ks : tl.ks1;
+            auto load_scales = [&](int k, float *dst) {
+                const float skk = ksu[k];
 #pragma unroll
-                        for (int q4 = 0; q4 < NV; q4++) vv[q4] = __ldg(vs4 + q4);
-                    }
-                }
+                for (int j = 0; j < NL; j++)
+                    dst[j] = (32 * j + lane < NC) ? skk * __ldg(tl.vs + (size_t)k * NI + cbase + 32 * j + lane) : 0.0f;
+            };
+            float nxt[NL];
+            if (mine && sg.kb0 < sg.kb1) load_scales(sg.kb0, nxt);
+            for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
+                const int buf = (int)(it % T::NACC);
+                const uint32_t use = (uint32_t)(it / T::NACC);
+                float skv[NL];
+#pragma unroll
+                for (int j = 0; j < NL; j++) skv[j] = nxt[j];
+                if (mine && kb + 1 < sg.kb1) load_scales(kb + 1, nxt);
                 int got = 0;
                 if (lane == 0) got = bar_wait(&acc_full[buf], use & 1u, &abort_flag, lim) ? 1 : 0;
                 got = __shfl_sync(0xffffffffu, got, 0);
@@ -556,30 +566,35 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
                     break;
                 }
                 tc_fence_after();
+                // the accumulator goes back to the MMA issuer as soon as the last
+                // batch of its columns is in registers, before that batch is added
+                auto release = [&]() {
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) bar_arrive(&acc_empty[buf]);
+                };
                 if (mine) {
-                    const float *vs = tl.vs + (size_t)kb * NI + cbase;
                     const uint32_t tbase = tmem + (uint32_t)((buf * MT + u) * T::ACC_N + cbase) +
                                            ((uint32_t)(quarter * 32) << 16);
+                    constexpr int LB = NC < 32 ? NC : 32;     // columns per batch of loads
 #pragma unroll
-                    for (int c0 = 0; c0 < NC; c0 += 8) {
-                        uint32_t r[8], r2[8];
-                        tmem_ld8_async(tbase + (uint32_t)c0, r);
-                        tmem_ld8_async(tbase + (uint32_t)(c0 + NI), r2);
+                    for (int c0 = 0; c0 < NC; c0 += LB) {
+                        uint32_t r[LB], r2[LB];
+#pragma unroll
+                        for (int c = 0; c < LB; c += 8) {
+                            tmem_ld8_async(tbase + (uint32_t)(c0 + c), r + c);
+                            tmem_ld8_async(tbase + (uint32_t)(c0 + c + NI), r2 + c);
+                        }
                         tmem_wait_ld();
+                        if (c0 + LB >= NC) release();
 #pragma unroll
-                        for (int i = 0; i < 8; i++) {
+                        for (int i = 0; i < LB; i++) {
                             // hi products + 2^-11 lo products, times the block scales (powers of
                             // two: exact)
                             const int c = c0 + i;
-                            float sv;
-                            if (T::TWO_LEVEL) {
-                                const float4 q = vv[(c >> 2) < NV ? (c >> 2) : 0];
-                                sv = (c & 3) == 0 ? q.x : (c & 3) == 1 ? q.y : (c & 3) == 2 ? q.z : q.w;
-                            } else {
-                                sv = __ldg(vs + c);
-                            }
+                            const float sc = __shfl_sync(0xffffffffu, skv[c >> 5], c & 31);
                             const float x = __fmaf_rn(__uint_as_float(r2[i]), LO_UNSCALE, __uint_as_float(r[i]));
-                            part[c] = __fmaf_rn(x, sk * sv, part[c]);
+                            part[c] = __fmaf_rn(x, sc, part[c]);
                         }
                     }
                     if (T::TWO_LEVEL && ((kb - sg.kb0) % T::FOLD == T::FOLD - 1 || kb == sg.kb1 - 1)) {
@@ -589,10 +604,9 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
                             part[c] = 0.0f;
                         }
                     }
+                } else {
+                    release();
                 }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) bar_arrive(&acc_empty[buf]);
             }
             if (!ok) break;
             if (mine) {

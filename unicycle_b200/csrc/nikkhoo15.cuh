@@ -242,10 +242,11 @@ __device__ inline void nw_angdis(T x, T y, T z, double cosA, double sinA, double
     T z1 = a10 * ty + a11 * tz;
     T eta = y1 * cosA - z1 * sinA;
     T zeta = y1 * sinA + z1 * cosA;
-    T r = dsqrt(x * x + y1 * y1 + z1 * z1);
+    T r, ir;
+    dsqrt_inv(x * x + y1 * y1 + z1 * z1, r, ir);
     T rmz = r - z1, rmzeta = r - zeta;
-    T irz = rcp(rmz), irze = rcp(rmzeta), ir = rcp(r);
-    T lz = dlog_g(rmz), lzeta = dlog_g(rmzeta);
+    T irz = rcp(rmz), irze = rcp(rmzeta);
+    T lz = dlog_gi(rmz, irz), lzeta = dlog_gi(rmzeta, irze);
     const double k = 1.0 / 8.0 / 3.141592653589793 / (1.0 - nu);
     const double n12 = 1.0 - 2.0 * nu;
     T x2 = x * x;
@@ -325,13 +326,18 @@ __device__ inline void nw_fsc(Dd y1, Dd y2, Dd y3, double sinB, double cosB, dou
     Dd y3b = y3 + 2.0 * a;
     Dd z1b = y1 * cosB + y3b * sinB;
     Dd z3b = -y1 * sinB + y3b * cosB;
-    Dd rb = dsqrt(y1 * y1 + y2 * y2 + y3b * y3b);
-    Dd Fib = 2.0 * datan_g(-y2 / (-(rb + y3b) * coth + y1));
+    // divisions are the costliest FP64 operations here: rb and 1 / rb come from
+    // one square root and one division, the logarithms' gradients reuse the
+    // reciprocals, and the quotients by cos(beta) multiply by its reciprocal
+    Dd rb, irb;
+    dsqrt_inv(y1 * y1 + y2 * y2 + y3b * y3b, rb, irb);
+    Dd Fib = 2.0 * datan_q_g(-y2, -(rb + y3b) * coth + y1);
     const double n12 = 1.0 - 2.0 * nu, n1 = 1.0 - nu, cot2 = cotB * cotB;
     const double k = 1.0 / 4.0 / 3.141592653589793 / n1;
+    const double icB = 1.0 / cosB;
     Dd ry = rb + y3b, rz = rb + z3b, w = rb * cosB + y3b, ya = y3b - a;
-    Dd iry = rcp(ry), irz = rcp(rz), irb = rcp(rb);
-    Dd lry = dlog_g(ry), lrz = dlog_g(rz);
+    Dd iry = rcp(ry), irz = rcp(rz);
+    Dd lry = dlog_gi(ry, iry), lrz = dlog_gi(rz, irz);
     Dd irb2 = irb * irb, irb3 = irb2 * irb;
     Dd cpa = cosB + a * irb;
     Dd rsy = rb * sinB - y1;
@@ -369,18 +375,18 @@ __device__ inline void nw_fsc(Dd y1, Dd y2, Dd y3, double sinB, double cosB, dou
     {
         const Dd e21 = n12 * ((2.0 * n1 * cot2 + nu) * lry - (2.0 * n1 * cot2 + 1.0) * cosB * lrz)
            + n12 * iry * (-n12 * y1 * cotB + nu * y3b - a + a * y1 * cotB * irb + y1 * y1 * iry * (nu + a * irb))
-           - n12 * cotB * irz * (z1b * cosB - a * rsy * irb / cosB) - a * y1 * ya * cotB * irb3
+           - n12 * cotB * irz * (z1b * cosB - a * rsy * irb * icB) - a * y1 * ya * cotB * irb3
            + ya * iry * (2.0 * nu + irb * (n12 * y1 * cotB + a) - y1 * y1 * irb * iry * (2.0 * nu + a * irb) - a * y1 * y1 * irb3)
-           + ya * cotB * irz * (-cosB * sinB + a * y1 * y3b * irb3 / cosB
-                                + rsy * irb * (2.0 * n1 * cosB - w * irz * (1.0 + a * irb / cosB)));
+           + ya * cotB * irz * (-cosB * sinB + a * y1 * y3b * irb3 * icB
+                                + rsy * irb * (2.0 * n1 * cosB - w * irz * (1.0 + a * irb * icB)));
         oS[0] = oS[0] + b[1] * e21;
         oD[0] = oD[0] + b[4] * e21;
     }
     {
         const Dd e22 = 2.0 * n1 * n12 * Fib * cot2 + n12 * y2 * iry * (-(n12 - a * irb) * cotB + y1 * iry * (nu + a * irb))
-           - n12 * y2 * cotB * irz * (1.0 + a * irb / cosB) - a * y2 * ya * cotB * irb3
+           - n12 * y2 * cotB * irz * (1.0 + a * irb * icB) - a * y2 * ya * cotB * irb3
            + y2 * ya * irb * iry * (n12 * cotB - 2.0 * nu * y1 * iry - a * y1 * irb * (irb + iry))
-           + y2 * ya * cotB * irb * irz * (-2.0 * n1 * cosB + w * irz * (1.0 + a * irb / cosB) + a * y3b * irb2 / cosB);
+           + y2 * ya * cotB * irb * irz * (-2.0 * n1 * cosB + w * irz * (1.0 + a * irb * icB) + a * y3b * irb2 * icB);
         oS[1] = oS[1] + b[1] * e22;
         oD[1] = oD[1] + b[4] * e22;
     }
