@@ -43,8 +43,9 @@ typedef struct ucg_ctx ucg_ctx;
 #define UCG_PREC_FP64        0  /* K in binary64, FP64 matvec (the plain method) */
 #define UCG_PREC_SPLIT_BF16  1  /* K = diag(s) k, s a per-row scale: stage 1 (the anchor) reads the
                                    split pair of k (bf16 hi + a 16-bit lo extension, together the
-                                   FP32 value), stages 2-6 the velocity increments against an fp16
-                                   plane of k (a quarter of the FP64 bytes); FP64 sums */
+                                   FP32 value, FP64 sums), stages 2-6 the velocity increments in
+                                   FP32 against an fp16 plane of k (a quarter of the FP64 bytes):
+                                   FP32 products over 8 entries, their sums added in FP64 */
 #define UCG_PREC_SPLIT_PAIR  4  /* the same split pair for every stage (half of the FP64 bytes),
                                    anchored, FP64 sums: the accurate split form */
 #define UCG_PREC_HMATRIX     2  /* hierarchical approximation of K (ucg_build_hmatrix), FP64 */

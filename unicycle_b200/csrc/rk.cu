@@ -312,8 +312,8 @@ template <> struct TmTraits<float> {   // the anchor of the split form: K/s in F
     static constexpr int PER = 4, CH = 1024, ROWS = 24, STAGES = 2;
     using Acc = double;
 };
-template <> struct TmTraits<__half> {   // the fp16 plane (anchored stages 2-6), FP64 sums
-    static constexpr int PER = 8, CH = 2048, ROWS = 24, STAGES = 2;
+template <> struct TmTraits<__half> {   // the fp16 plane (anchored stages 2-6): FP32 products
+    static constexpr int PER = 8, CH = 2048, ROWS = 24, STAGES = 2;   // and 8-term sums, FP64 across
     using Acc = double;
 };
 template <class KT>
@@ -327,7 +327,7 @@ constexpr size_t tm_smem_bytes()
 template <class KT> struct TmV;
 template <> struct TmV<double> { double2 x; };
 template <> struct TmV<float> { double x[4]; };
-template <> struct TmV<__half> { double x[8]; };
+template <> struct TmV<__half> { float x[8]; };   // v in FP32: the plane itself carries 2^-12
 
 template <class KT>
 __device__ __forceinline__ void tm_load_v(const double *v, long c, long n, TmV<KT> &vr);
@@ -358,13 +358,13 @@ __device__ __forceinline__ void tm_load_v<__half>(const double *v, long c, long 
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const double2 a = __ldg(reinterpret_cast<const double2 *>(v + c + 2 * q));
-            vr.x[2 * q] = a.x;
-            vr.x[2 * q + 1] = a.y;
+            vr.x[2 * q] = __double2float_rn(a.x);
+            vr.x[2 * q + 1] = __double2float_rn(a.y);
         }
         return;
     }
 #pragma unroll
-    for (int q = 0; q < 8; q++) vr.x[q] = (c + q < n) ? v[c + q] : 0.0;
+    for (int q = 0; q < 8; q++) vr.x[q] = (c + q < n) ? __double2float_rn(v[c + q]) : 0.0f;
 }
 
 template <class KT>
@@ -385,17 +385,22 @@ __device__ __forceinline__ void tm_accumulate<float>(const float *srow, int cl, 
     acc = fma((double)kv.z, vr.x[2], acc);
     acc = fma((double)kv.w, vr.x[3], acc);
 }
+// the thread's 8 products of the row in FP32 (each rounded once, 2^-24: far
+// below the plane's own 2^-12), their sum added to the FP64 row sum: one
+// conversion to FP64 per 8 entries instead of one per entry
 template <>
 __device__ __forceinline__ void tm_accumulate<__half>(const __half *srow, int cl, const TmV<__half> &vr, double &acc)
 {
     const uint4 raw = *reinterpret_cast<const uint4 *>(srow + cl);
     const uint32_t w4[4] = {raw.x, raw.y, raw.z, raw.w};
+    float p = 0.0f;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w4[q]));
-        acc = fma((double)f.x, vr.x[2 * q], acc);
-        acc = fma((double)f.y, vr.x[2 * q + 1], acc);
+        p = __fmaf_rn(f.x, vr.x[2 * q], p);
+        p = __fmaf_rn(f.y, vr.x[2 * q + 1], p);
     }
+    acc += (double)p;
 }
 
 template <int S, class KT>
