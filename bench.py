@@ -864,8 +864,9 @@ def hmatrix_leg(args, local, sim, cfg, plain):
     split = {"steps_per_s": steps_s / el_s, "ms_per_step": 1e3 * el_s / steps_s,
              "speedup_vs_plain_fp64_steps": steps_s / el_s / plain["value"],
              "sim_years_per_hour": (ts_t - ts_w) / YEAR / (el_s / 3600.0),
-             "bytes_stage1": info["bytes"] / 2, "bytes_increments": info["bytes"] / 4,
-             "note": "bf16 hi + lo of every stored value; stage 1 reads both, stages 2-6 the hi copy alone"}
+             "bytes_per_stage": info["bytes"] / 2,
+             "note": "the FP32 value of every stored entry in two 16-bit planes (bf16 hi bits + 16-bit lo "
+                     "extension), read by every stage (anchored stages, FP64 sums)"}
     return {"eta": args.hm_eta, "eps": args.hm_eps, "leaf": args.hm_leaf, "build_seconds": build_s,
             "blocks_dense": info["n_dense"], "blocks_lowrank": info["n_lowrank"], "max_rank": info["max_rank"],
             "bytes": info["bytes"], "compression_vs_dense_fp64": info["compression"],
