@@ -541,27 +541,30 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
             for (int c = 0; c < (T::TWO_LEVEL ? NC : 1); c++) sum[c] = 0.0;
             const GemmTile tl = tiles[sg.tile];
             // the k-block's scales: the tile's K block scale and, per lane, the V
-            // block scale of its instance columns cbase + lane + 32 j, both
-            // loaded one k-block ahead (their latency would otherwise sit in
-            // every k-block once the drain is the busy side) and the lane's
-            // product broadcast to the warp by shuffles
+            // block scale of its instance columns cbase + lane + 32 j, loaded one
+            // k-block ahead and multiplied only when used (a product formed at
+            // the load would wait out the L2 latency in every k-block once the
+            // drain is the busy side), the lane's product broadcast to the warp
+            // by shuffles
             constexpr int NL = (NC + 31) / 32;       // instance columns per lane
             const float *ksu = u == 0 ? tl.ks : tl.ks1;
-            auto load_scales = [&](int k, float *dst) {
-                const float skk = ksu[k];
+            float nk = 0.0f, nv[NL];
+            auto load_scales = [&](int k) {
+                nk = ksu[k];
 #pragma unroll
                 for (int j = 0; j < NL; j++)
-                    dst[j] = (32 * j + lane < NC) ? skk * __ldg(tl.vs + (size_t)k * NI + cbase + 32 * j + lane) : 0.0f;
+                    nv[j] = (32 * j + lane < NC) ? __ldg(tl.vs + (size_t)k * NI + cbase + 32 * j + lane) : 0.0f;
             };
-            float nxt[NL];
-            if (mine && sg.kb0 < sg.kb1) load_scales(sg.kb0, nxt);
+#pragma unroll
+            for (int j = 0; j < NL; j++) nv[j] = 0.0f;
+            if (mine && sg.kb0 < sg.kb1) load_scales(sg.kb0);
             for (int kb = sg.kb0; kb < sg.kb1; kb++, it++) {
                 const int buf = (int)(it % T::NACC);
                 const uint32_t use = (uint32_t)(it / T::NACC);
                 float skv[NL];
 #pragma unroll
-                for (int j = 0; j < NL; j++) skv[j] = nxt[j];
-                if (mine && kb + 1 < sg.kb1) load_scales(kb + 1, nxt);
+                for (int j = 0; j < NL; j++) skv[j] = nk * nv[j];
+                if (mine && kb + 1 < sg.kb1) load_scales(kb + 1);
                 int got = 0;
                 if (lane == 0) got = bar_wait(&acc_full[buf], use & 1u, &abort_flag, lim) ? 1 : 0;
                 got = __shfl_sync(0xffffffffu, got, 0);

@@ -328,6 +328,10 @@ template <class KT> struct TmV;
 template <> struct TmV<double> { double2 x; };
 template <> struct TmV<float> { double x[4]; };
 template <> struct TmV<__half> { float x[8]; };   // v in FP32: the plane itself carries 2^-12
+// v as loaded (one chunk ahead): the fp16 form keeps the doubles and converts
+// them when the chunk is used, so that no instruction waits on the loads early
+template <class KT> struct TmVRaw { TmV<KT> v; };
+template <> struct TmVRaw<__half> { double x[8]; };
 
 template <class KT>
 __device__ __forceinline__ void tm_load_v(const double *v, long c, long n, TmV<KT> &vr);
@@ -351,20 +355,37 @@ __device__ __forceinline__ void tm_load_v<float>(const double *v, long c, long n
 #pragma unroll
     for (int q = 0; q < 4; q++) vr.x[q] = (c + q < n) ? v[c + q] : 0.0;
 }
+// the raw loads of one chunk's v (every form) and their conversion when used
+template <class KT>
+__device__ __forceinline__ void tm_load_raw(const double *v, long c, long n, TmVRaw<KT> &raw)
+{
+    tm_load_v<KT>(v, c, n, raw.v);
+}
 template <>
-__device__ __forceinline__ void tm_load_v<__half>(const double *v, long c, long n, TmV<__half> &vr)
+__device__ __forceinline__ void tm_load_raw<__half>(const double *v, long c, long n, TmVRaw<__half> &raw)
 {
     if (c + 8 <= n) {
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const double2 a = __ldg(reinterpret_cast<const double2 *>(v + c + 2 * q));
-            vr.x[2 * q] = __double2float_rn(a.x);
-            vr.x[2 * q + 1] = __double2float_rn(a.y);
+            raw.x[2 * q] = a.x;
+            raw.x[2 * q + 1] = a.y;
         }
         return;
     }
 #pragma unroll
-    for (int q = 0; q < 8; q++) vr.x[q] = (c + q < n) ? __double2float_rn(v[c + q]) : 0.0f;
+    for (int q = 0; q < 8; q++) raw.x[q] = (c + q < n) ? v[c + q] : 0.0;
+}
+template <class KT>
+__device__ __forceinline__ void tm_cook(const TmVRaw<KT> &raw, TmV<KT> &vr)
+{
+    vr = raw.v;
+}
+template <>
+__device__ __forceinline__ void tm_cook<__half>(const TmVRaw<__half> &raw, TmV<__half> &vr)
+{
+#pragma unroll
+    for (int q = 0; q < 8; q++) vr.x[q] = __double2float_rn(raw.x[q]);
 }
 
 template <class KT>
@@ -492,16 +513,20 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
         Acc acc[ROWS];
 #pragma unroll
         for (int r = 0; r < ROWS; r++) acc[r] = Acc(0);
+        // v does not depend on the stage: each chunk's values are loaded one
+        // chunk ahead, so their latency overlaps the previous chunk's products
+        const int cl = PER * t;
+        TmVRaw<KT> vn;
+        if (cl < n) tm_load_raw<KT>(a.v, cl, n, vn);
         for (long ch = 0; ch < nch; ch++, item++) {
             const int s = (int)(item % STAGES);
             const uint32_t ph = (uint32_t)((item / STAGES) & 1);
             // on a timed-out wait every consumer keeps walking the same item
             // sequence without computing, so all of them reach each named barrier
-            // v does not depend on the stage: its loads are in flight during the wait
-            const int cl = PER * t;
             const long c = ch * CH + cl;
             TmV<KT> vr;
-            if (c < n) tm_load_v<KT>(a.v, c, n, vr);
+            if (c < n) tm_cook<KT>(vn, vr);
+            if (c + CH < n) tm_load_raw<KT>(a.v, c + CH, n, vn);
             const bool ready = !abort_flag && mbar_wait(&full[s], ph, &abort_flag, wait_lim);
             if (!ready && !abort_flag) {
                 abort_flag = 1;
