@@ -26,6 +26,7 @@
 // instead of dominating it on components whose state and rate are near zero,
 // which at rtol 1e-8 would reject nearly every attempt.  The FP64 path keeps
 // the reference's plain form.
+#include <utility>
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -71,6 +72,36 @@ struct StageArgs {
 
 __device__ __forceinline__ bool ctl_live(const Ctl *c) { return c->active && c->status == 0; }
 
+// Programmatic dependent launch.  The kernels of an attempt are launched with
+// programmatic stream serialization: each may be scheduled while its
+// predecessor in the stream still runs, waits here (griddepcontrol.wait) until
+// that predecessor has completed and its writes are visible, and at once lets
+// its own successor be scheduled.  So the launch latency of every kernel of an
+// attempt overlaps the previous kernel instead of adding to it (it dominates
+// at small N).  Without a programmatic predecessor the wait returns at once.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 __device__ __forceinline__ void atomic_max_pos(unsigned long long *p, double x)
 {
     // non-negative doubles order like their bit patterns
@@ -95,6 +126,7 @@ __device__ __forceinline__ double stage_comb(const StageArgs &a, long i, double 
 template <int S>
 __global__ void k_prologue(StageArgs a, Ctl *ctl)
 {
+    pdl_enter();
     if (!ctl_live(ctl)) return;
     if (S == 1 && !ctl->need_stage1) return;
     const double h = ctl->h;
@@ -432,6 +464,7 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
     using Acc = typename Tr::Acc;
     constexpr int CH = Tr::CH, PER = Tr::PER, ROWS = Tr::ROWS, STAGES = Tr::STAGES;
     constexpr int PB = ROWS / 3, VB = ROWS / 6;   // patches, volumes per block
+    pdl_enter();
     if (!ctl_live(ctl)) return;
     if (S == 1 && !ctl->need_stage1) return;
     extern __shared__ __align__(128) unsigned char tm_smem[];
@@ -591,6 +624,7 @@ __global__ void __launch_bounds__((MV_WARPS + 1) * 32, 1) k_traction(const KT *_
 
 __global__ void k_finish(StageArgs a, Ctl *ctl)
 {
+    pdl_enter();
     if (!ctl_live(ctl)) return;
     const double h = ctl->h;
     double mx = 0.0;
@@ -630,6 +664,7 @@ __global__ void k_finish(StageArgs a, Ctl *ctl)
 
 __global__ void k_control(Ctl *ctl)
 {
+    pdl_enter();
     if (!ctl_live(ctl)) return;
     const double SAFETY = 0.7, PGROW = -0.2, PSHRNK = -0.15, ERRCON = 1.89e-4;
     double errmax = __longlong_as_double((long long)ctl->errbits);
@@ -679,6 +714,7 @@ __global__ void k_control(Ctl *ctl)
 // one output record at the start of a step (after stage 1: y and its rate k1)
 __global__ void k_record(StageArgs a, const Ctl *ctl, Rec *rec)
 {
+    pdl_enter();
     if (!rec->enabled || !ctl_live(ctl) || !ctl->need_stage1) return;
     const long long step = ctl->accepted - rec->base;
     if (step < 0 || step % rec->every) return;
@@ -727,13 +763,18 @@ __global__ void k_record(StageArgs a, const Ctl *ctl, Rec *rec)
 
 __global__ void k_commit(StageArgs a, const Ctl *ctl)
 {
+    pdl_enter();
     if (!ctl->pending) return;
     double *y = const_cast<double *>(a.y);
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < a.len; i += (long)gridDim.x * blockDim.x)
         y[i] = a.ycand[i];
 }
 
-__global__ void k_clear_pending(Ctl *ctl) { ctl->pending = 0; }
+__global__ void k_clear_pending(Ctl *ctl)
+{
+    pdl_enter();
+    ctl->pending = 0;
+}
 
 // ---- host side -----------------------------------------------------------------
 
@@ -853,7 +894,7 @@ static void launch_traction_t(ucg_ctx *c, const StageArgs &a, const KT *K, long 
     const size_t smem = tm_smem_bytes<KT>();
     auto kfn = k_traction<S, KT>;
     cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kfn<<<grid, (MV_WARPS + 1) * 32, smem, c->stream>>>(K, c->n, ldk, scale, a, c->ctl, pb, vb);
+    launch_pdl(kfn, dim3(grid), dim3((MV_WARPS + 1) * 32), smem, c->stream, K, c->n, ldk, scale, a, c->ctl, pb, vb);
 }
 
 template <int S>
@@ -874,7 +915,7 @@ static void enqueue_stage(ucg_ctx *c)
 {
     const int ne = c->nr + c->nt + c->nv;
     StageArgs a = stage_args(c, S);
-    k_prologue<S><<<(ne + 127) / 128, 128, 0, c->stream>>>(a, c->ctl);
+    launch_pdl(k_prologue<S>, dim3((ne + 127) / 128), dim3(128), 0, c->stream, a, c->ctl);
     c->launches.count += 1;
     if (c->precision == UCG_PREC_HMATRIX || c->precision == UCG_PREC_HMATRIX_SPLIT) {
         double *t = hmatrix_t(c);
@@ -893,7 +934,7 @@ static void enqueue_attempt_raw(ucg_ctx *c)
     enqueue_stage<1>(c);
     // the recorder joins the attempt (and its graph) only while recording is on
     if (c->rec_host.enabled) {
-        k_record<<<c->sms, 256, 0, c->stream>>>(stage_args(c, 1), c->ctl, c->rec);
+        launch_pdl(k_record, dim3(c->sms), dim3(256), 0, c->stream, stage_args(c, 1), c->ctl, c->rec);
         c->launches.count += 1;
     }
     enqueue_stage<2>(c);
@@ -903,8 +944,8 @@ static void enqueue_attempt_raw(ucg_ctx *c)
     enqueue_stage<6>(c);
     StageArgs a = stage_args(c, 6);
     const int fin_grid = (int)((c->state_len + 255) / 256 < (long)c->sms * 4 ? (c->state_len + 255) / 256 : c->sms * 4);
-    k_finish<<<fin_grid > 0 ? fin_grid : 1, 256, 0, c->stream>>>(a, c->ctl);
-    k_control<<<1, 1, 0, c->stream>>>(c->ctl);
+    launch_pdl(k_finish, dim3(fin_grid > 0 ? fin_grid : 1), dim3(256), 0, c->stream, a, c->ctl);
+    launch_pdl(k_control, dim3(1), dim3(1), 0, c->stream, c->ctl);
     c->launches.count += 2;
 }
 
@@ -938,8 +979,8 @@ void rk_enqueue_attempt(ucg_ctx *c)
 void rk_enqueue_commit(ucg_ctx *c)
 {
     StageArgs a = stage_args(c, 1);
-    k_commit<<<(int)((c->state_len + 255) / 256), 256, 0, c->stream>>>(a, c->ctl);
-    k_clear_pending<<<1, 1, 0, c->stream>>>(c->ctl);
+    launch_pdl(k_commit, dim3((unsigned)((c->state_len + 255) / 256)), dim3(256), 0, c->stream, a, c->ctl);
+    launch_pdl(k_clear_pending, dim3(1), dim3(1), 0, c->stream, c->ctl);
     c->launches.count += 2;
 }
 
