@@ -1598,25 +1598,25 @@ __global__ void k_ens_finish(const EnsArgs *__restrict__ A)
 // RKQSm decision per instance (ode45.f90:77-106) and the loop condition.  With a
 // step-size model, the instances that accepted in this attempt are collected per
 // chunk of blockDim.x instances and each warp evaluates the model for one of
-// them from a shared-memory copy of its weights.
-constexpr int CTL_THREADS = 256;
+// them (weights read from global memory).
+constexpr int CTL_THREADS = 512;    // 16 warps: up to 16 model evaluations in one round
 
 __global__ void __launch_bounds__(CTL_THREADS) k_ens_control(const EnsArgs *__restrict__ A,
                                                                cudaGraphConditionalHandle cond, int in_graph)
 {
     EnsGlobal *gl = A->glob;
     const double SAFETY = 0.7, PGROW = -0.2, PSHRNK = -0.15, ERRCON = 1.89e-4;
-    __shared__ __half wt[mlp::NPARAM + 1];
     __shared__ mlp::Norm norm;
     __shared__ float feat[CTL_THREADS][mlp::NIN];
     __shared__ InstCtl *who[CTL_THREADS];
     __shared__ int nwho;
     __shared__ int wsum[CTL_THREADS / 32];
+    // the model's weights are read where they are (global memory, cached): a copy
+    // into shared memory at every launch costs more than the few evaluations
+    // of one attempt read
     const bool model = gl->mlp_P != nullptr;
-    if (model) {
-        for (int p = threadIdx.x; p < mlp::NPARAM; p += blockDim.x) wt[p] = gl->mlp_P[p];
-        if (threadIdx.x == 0) norm = *gl->mlp_N;
-    }
+    const __half *wt = gl->mlp_P;
+    if (model && threadIdx.x == 0) norm = *gl->mlp_N;
     const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     int live = 0;
     for (int gi = 0; gi < A->ngeom; gi++) {
