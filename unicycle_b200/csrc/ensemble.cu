@@ -1461,10 +1461,9 @@ __device__ __forceinline__ void ens_rate(const double *yy, const double t[3], do
 }
 
 // traction rates from the contraction and the rate-state right-hand side
-// (ratestate.f90:731-776 per instance).  Dense geometries stage the block's
-// contiguous state range and rate range through shared memory (coalesced);
-// a hierarchical geometry walks its elements in the permuted order, so that
-// consecutive threads read consecutive rows of a leaf's partial sums.
+// (ratestate.f90:731-776 per instance).  The block's contiguous state range and
+// rate range go through shared memory (coalesced); a hierarchical geometry
+// gathers each element's partial sums from the cluster order.
 // 12 blocks per SM (40 registers, a few spilled): the kernel waits on memory,
 // and more resident warps hide it better than fewer that spill nothing
 // (measured at N = 20k x 64: 5.96 ms per attempt against 6.08 at 80 registers)
@@ -1485,27 +1484,6 @@ __global__ void __launch_bounds__(EW_THREADS, 12) k_ens_rhs(const EnsArgs *__res
     const bool valid = threadIdx.x < ne;
     const double *ysrc = (S == 1) ? G.y : G.ys;
     double *ks = G.k[S - 1];
-    if (G.hier) {
-        if (!valid) return;
-        const int e = G.hperm[el];
-        double t[3];
-        double *t1 = G.t1 + (long)i * 3 * G.np + 3L * e;
-        for (int q = 0; q < 3; q++) {
-            const double inc = traction_row_h(A, G, i, el, q);
-            if (S == 1) {
-                t1[q] = inc;
-                t[q] = inc;
-            } else {
-                t[q] = t1[q] + inc;
-            }
-        }
-        const long o = (long)i * 7 * G.np + 7L * e;
-        const long pe = (long)i * G.np + e;
-        double k[7];
-        ens_rate(ysrc + o, t, G.L[pe], G.b[pe], G.sig[pe], G.a[pe], G.damping[pe], k);
-        for (int q = 0; q < 7; q++) ks[o + q] = k[q];
-        return;
-    }
     const long base = (long)i * 7 * G.np + 7L * e0;
 #pragma unroll
     for (int u = 0; u < 7; u++) {
@@ -1517,8 +1495,13 @@ __global__ void __launch_bounds__(EW_THREADS, 12) k_ens_rhs(const EnsArgs *__res
         const int e = el;
         double t[3];
         double *t1 = G.t1 + (long)i * 3 * G.np + 3L * e;
+        // a hierarchical geometry's partial sums lie in the cluster order: the
+        // element's permuted position finds them (a gather of a few floats per
+        // row, while the state and the rate stay coalesced)
+        const int ph = G.hier ? G.hinv[e] : 0;
         for (int q = 0; q < 3; q++) {
-            const double inc = traction_row(A, G, i, 3L * e + q, S > 1 && !A->glob->inc_full);
+            const double inc = G.hier ? traction_row_h(A, G, i, ph, q)
+                                      : traction_row(A, G, i, 3L * e + q, S > 1 && !A->glob->inc_full);
             if (S == 1) {
                 t1[q] = inc;
                 t[q] = inc;
