@@ -533,7 +533,7 @@ int ucg_ens_profile_contract(ucg_ensemble *ens, int reps, double *ms_anchor, dou
    device by the library's own forward/backward kernels on traces that the
    ensemble integrator records.  In use, the proposal (limited to 0.2..10 times
    the accepted step) replaces RKQSm's hnext; the embedded error estimate still
-   judges the attempt, and a rejected proposal is shrunk by the plain RKQSm
+   accepts or rejects the attempt, and a rejected proposal is shrunk by the plain RKQSm
    rule (fortran/3d/src/ode45.f90:79-84).  No reference counterpart. */
 typedef struct ucg_mlp ucg_mlp;
 

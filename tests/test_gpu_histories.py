@@ -219,7 +219,7 @@ def test_history_hierarchical_ensemble(ucg, hsetup):
 
 def test_history_learned_step(ucg, setup):
     """The learned proposal on the ensemble: the proposal only changes which
-    step is tried; the embedded error estimate still judges it, so the history
+    step is tried; the embedded error estimate still accepts or rejects it, so the history
     stays within the same bound of the oracle's."""
     from unicycle_b200 import configs
     from unicycle_b200.stepmodel import training_set

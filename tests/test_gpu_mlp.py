@@ -60,7 +60,7 @@ def _first_onsets(ens, ninst):
 def test_learned_proposal_on_held_out_runs(ucg):
     """Traces from 64 seeded runs of a small cfg1 fault train the model; 8
     held-out seeds then run to past their first earthquake with the plain
-    controller and with the learned proposal.  The judge keeps the physics:
+    controller and with the learned proposal.  The error estimate keeps the physics:
     event onsets agree within 1e-3 relative; the attempts, rejected fraction
     and simulated time per attempt of both are printed."""
     from unicycle_b200 import configs

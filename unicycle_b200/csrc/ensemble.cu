@@ -14,7 +14,7 @@
 // stage combinations, error norm and step control stay FP64 and follow the
 // single-instance integrator (rk.cu) per instance: every instance has its own
 // step size, time, accept/reject decision and counters, and the reference
-// RKQSm controller (fortran/3d/src/ode45.f90:51-108) judges each of them.
+// RKQSm controller (fortran/3d/src/ode45.f90:51-108) accepts or rejects each attempt.
 //
 // Anchored stages.  The contraction's rounding (about 1e-5 of |K| |v|) would
 // otherwise enter the embedded error estimate h sum_i dc_i k_i directly: for

@@ -7,8 +7,8 @@
 //   log10 max(errmax, 1e-12) of the step just accepted (errmax = max|yerr/yscal|/epsilon).
 // Inputs are standardised with the training set's means and deviations, which
 // travel with the weights.  Weights and activations are FP16, sums are FP32;
-// training keeps FP32 master weights (mlp.cu).  The embedded error estimate stays
-// the judge: a proposal is only the first try of the next step, and a rejected
+// training keeps FP32 master weights (mlp.cu).  The embedded error estimate still
+// decides: a proposal is only the first try of the next step, and a rejected
 // proposal is shrunk by the plain RKQSm rule.
 #pragma once
 #include <cuda_fp16.h>

@@ -5,7 +5,7 @@ log10 of the next Runge-Kutta step from the integrator's own recent history.
 It is trained on the device by the library's own kernels on traces that the
 ensemble integrator records (`Ensemble.record_traces`), and used by the
 ensemble controller (`Ensemble.set_step_model`).  The embedded error estimate
-stays the judge: a rejected proposal is shrunk by the plain RKQSm rule
+still decides: a rejected proposal is shrunk by the plain RKQSm rule
 (fortran/3d/src/ode45.f90:79-84).
 """
 import ctypes
