@@ -155,6 +155,35 @@ def test_odefun_matches_oracle(ucg, oracle_lib, cfg1_small):
     sim.close()
 
 
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("split_pair", 3e-7), ("split_bf16", 3e-7)])
+def test_odefun_at_size_matches_oracle(ucg, oracle_lib, precision, tol):
+    """2,000 triangles (K 6,000 x 4,000): the traction kernel walks 8 column
+    chunks per row block and several row blocks per CTA (every FP64 path of the
+    small model above has one or two); the oracle evaluates the right-hand side
+    on the device's own K.  The split planes carry K/s in FP32 (a stage-1
+    right-hand side reads the pair plane): measured 5.5e-16 (FP64) and 2.5e-8 (split)
+    of the column scale."""
+    from unicycle_b200 import configs
+    c = configs.cfg2(nx=25, nz=40)
+    sim = _sim(ucg, c)
+    K = sim.copy_G()
+    assert K.shape == (6000, 4000)
+    md = oracle_lib.Model(K, c["friction"])
+    sim.set_precision(precision)
+    rng = np.random.default_rng(5)
+    n = c["n_patch"]
+    y = c["y0"].copy()
+    y[6::7] += rng.normal(0, 1.0, n)
+    y[5::7] += rng.normal(0, 0.5, n)
+    dy, _ = sim.odefun(y)
+    ref, _ = md.odefun(y)
+    sim.set_precision(ucg.UCG_PREC_FP64)
+    err = np.abs(dy - ref).reshape(n, 7) / _odefun_scales(ref, n)
+    print(f"{precision}: max error {err.max():.2e} of the column scale")
+    assert err.max() < tol, err.max(axis=0)
+    sim.close()
+
+
 def test_rk_attempt_matches_oracle(ucg, oracle_lib, cfg1_small):
     """One Cash-Karp attempt from identical (y, dydt, h): the accepted candidate
     matches the oracle's RKCKm to 1e-12 in the physical components (tolerance
