@@ -232,7 +232,7 @@ def test_history_within_reference_envelope(ucg, oracle_lib):
     envelope is below that."""
     from unicycle_b200 import configs
     c = _oblique(configs.cfg1(nx=16, nz=8))
-    nsteps = 400
+    nsteps = 1000
     sim = _sim(ucg, c)
     G = sim.copy_G()
 
