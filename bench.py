@@ -77,6 +77,9 @@ def parse():
     p.add_argument("--hm-ens-leaf", type=int, default=40,
                    help="hierarchical ensemble: patches per cluster leaf (at most 42: a row leaf is one 128-row tile)")
     p.add_argument("--no-hier-ensemble", action="store_true", help="skip the hierarchical-ensemble leg")
+    p.add_argument("--hier-planes", type=int, default=3, choices=[2, 3],
+                   help="hierarchical ensemble: bf16 planes of the operand images, 3 (24 bits, histories within "
+                        "1e-6 of FP64) or 2 (16 bits, two thirds of the bytes)")
     p.add_argument("--trace-runs", type=int, default=64, help="seeded cfg1 runs that record training traces")
     p.add_argument("--trace-attempts", type=int, default=16000, help="attempts of the trace-recording runs")
     p.add_argument("--learned-eval-years", type=float, default=15.0,
@@ -956,6 +959,7 @@ def hier_ensemble_leg(args, local, cfg, sets, y0s, dense, Kr):
     info = sim.hmatrix_info()
     sim.set_precision(unicycle_b200.UCG_PREC_HMATRIX)
     ens = unicycle_b200.Ensemble(device=local)
+    ens.set_hier_planes(args.hier_planes)
     t0 = time.perf_counter()
     ens.add_geometry(sim, args.sets)
     images_s = time.perf_counter() - t0
@@ -964,6 +968,7 @@ def hier_ensemble_leg(args, local, cfg, sets, y0s, dense, Kr):
                          fr["damping"])
         ens.set_state(0, i, y0, 0.0, cfg["dt0"])
     ens.set_tolerance(cfg["epsilon"])
+    ens.set_increment_terms(args.ens_terms)
     stream = torch.cuda.ExternalStream(ens.stream, device=local)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ens.run(1e300, args.spinup + args.warmup)
@@ -993,7 +998,8 @@ def hier_ensemble_leg(args, local, cfg, sets, y0s, dense, Kr):
     e_k = float(np.max(np.abs(T[:, :Kr.shape[0]] - V @ Kr.T) / mag))
     ens.close()
     sim.close()
-    out = {"leaf": args.hm_ens_leaf, "eta": args.hm_eta, "eps": args.hm_eps, "hmatrix_build_seconds": build_s,
+    out = {"leaf": args.hm_ens_leaf, "eta": args.hm_eta, "eps": args.hm_eps, "planes": args.hier_planes,
+           "hmatrix_build_seconds": build_s,
            "images_seconds": images_s, "hmatrix_fp64_bytes": info["bytes"], "image_bytes": img,
            "steps_per_s": acc / el, "ms_per_attempt": 1e3 * el / attempts, "accepted_steps": acc,
            "rejected_attempts": rej,
@@ -1004,14 +1010,21 @@ def hier_ensemble_leg(args, local, cfg, sets, y0s, dense, Kr):
            "rel_l2_error_vs_fp64_hmatrix": {"anchor": e_h, "increment_form": e_h2},
            "max_rel_to_abs_product_vs_dense_K_rows_0_767": e_k}
     if img:
-        inc = img / 2
-        out["roofline"] = {"bound": "hbm", "kernel": "k_hm_contract<64,false> x2 + k_hm_zconv (increment form; "
-                                                    "operand hi planes)", "bytes_per_launch": inc,
-                           "achieved": inc / (ms_c / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                           "frac": inc / (ms_c / 1e3) / 1e9 / peak, "peak_source": peak_kind,
-                           "anchor": {"bytes_per_launch": img, "achieved": img / (ms_a / 1e3) / 1e9,
-                                      "frac": img / (ms_a / 1e3) / 1e9 / peak}}
+        out["roofline"] = hier_roofline(args, img, ms_a, ms_c, peak, peak_kind)
     return out
+
+
+def hier_roofline(args, img, ms_a, ms_c, peak, peak_kind):
+    """The hierarchical contraction in the form every stage of the run takes:
+    all planes of the operand images (three planes, or two with the anchor's
+    form at every stage), else the hi planes of the two-term increments."""
+    full = args.hier_planes == 3 or args.ens_terms == 3
+    byt, ms = (img, ms_a) if full else (img / 2, ms_c)
+    kern = (f"k_hm_contract<64,true,{args.hier_planes}> x2 + k_hm_zconv (every operand plane)" if full else
+            "k_hm_contract<64,false,2> x2 + k_hm_zconv (increment form; operand hi planes)")
+    return {"bound": "hbm", "kernel": kern, "ms_per_launch": ms, "bytes_per_launch": byt,
+            "achieved": byt / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+            "frac": byt / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None}
 
 
 def run_hier_ensemble(args, world, rank, local):
@@ -1036,6 +1049,7 @@ def run_hier_ensemble(args, world, rank, local):
     info = sim.hmatrix_info()
     sim.set_precision(unicycle_b200.UCG_PREC_HMATRIX)
     ens = unicycle_b200.Ensemble(device=local)
+    ens.set_hier_planes(args.hier_planes)
     t0 = time.perf_counter()
     ens.add_geometry(sim, args.sets)
     images_s = time.perf_counter() - t0
@@ -1091,14 +1105,15 @@ def run_hier_ensemble(args, world, rank, local):
     sim.close()
     if rank != 0:
         return None
-    inc = img / 2
     return {"metric": f"RK45 steps/s at N={n}, {args.sets}-instance ensemble on the hierarchical K (aggregate)",
             "value": world * acc / el_max, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * el_max / attempts, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3/f32 product, f64 state",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": f"bf16 x {args.hier_planes} planes / f32 product, f64 state",
             "data": "synthetic (seeded cfg2 curved megathrust; Dc redrawn per parameter set)",
             "config": {"workload": f"megathrust {n} Nikkhoo-Walter triangles x {args.sets} frictional parameter "
                                    "sets, one ensemble, hierarchical K only", "n_triangles": n,
+                       "planes": args.hier_planes,
                        "instances": args.sets, "K_shape": [m, nn], "dense_fp64_bytes": 8.0 * m * nn,
                        "step": "one attempt of every instance (timed steps = attempts)",
                        "parallelism": f"replicas x{world}", "rtol": cfg["epsilon"],
@@ -1109,13 +1124,7 @@ def run_hier_ensemble(args, world, rank, local):
                         "eps": args.hm_eps, "leaf": args.hm_ens_leaf,
                         **{k: info[k] for k in ("n_dense", "n_lowrank", "max_rank", "bytes", "compression")}},
             "rel_l2_error_vs_fp64_hmatrix": err,
-            "roofline": {"bound": "hbm", "kernel": "k_hm_contract<64,false> x2 + k_hm_zconv (increment form; "
-                                                   "operand hi planes)", "ms_per_launch": ms_c,
-                         "bytes_per_launch": inc, "achieved": inc / (ms_c / 1e3) / 1e9, "peak": peak,
-                         "unit": "GB/s", "frac": inc / (ms_c / 1e3) / 1e9 / peak, "peak_source": peak_kind,
-                         "traffic": None,
-                         "anchor": {"ms_per_launch": ms_a, "bytes_per_launch": img,
-                                    "achieved": img / (ms_a / 1e3) / 1e9, "frac": img / (ms_a / 1e3) / 1e9 / peak}},
+            "roofline": hier_roofline(args, img, ms_a, ms_c, peak, peak_kind),
             "e2e": {"value": world * acc_e2e / e2e_el, "unit": "steps/s",
                     "h2d_bytes_per_step": 8 * 7 * n * args.sets, "d2h_bytes_per_step": 8 * 7 * n * args.sets},
             "gpu_launches": int(attempts * 32 + 3), "clocks": clk.summary(), "cpu_baseline": None}

@@ -465,6 +465,16 @@ int ucg_ens_put_states(ucg_ensemble *ens, int geometry, const double *y);
    counterpart. */
 int ucg_ens_set_increment_terms(ucg_ensemble *ens, int terms);
 
+/* Operand precision of the hierarchical geometries' tensor-core contraction,
+   fixed before the first hierarchical geometry is added (UCG_E_STATE after):
+   planes = 3, the default, keeps every image (the low-rank factors, the dense
+   leaf blocks, the slip rates and the intermediate Z) as three bf16 planes
+   (hi, mid, lo: 24 significant bits) and forms the six products of weight
+   2^-16 and above; planes = 2 keeps hi and lo (16 bits: about 2e-5 on slip-rate
+   histories), two thirds of the bytes, and allows 128-instance tiles.  No
+   reference counterpart. */
+int ucg_ens_set_hier_planes(ucg_ensemble *ens, int planes);
+
 /* Fault injection for testing the bounded device waits (no reference
    counterpart).  wait_ns > 0 replaces the 4 s limit of the dense contraction's
    data waits; hold != 0 makes the CTA that owns the first work segment issue

@@ -103,11 +103,13 @@ def _single(sim, c, nsteps):
     return np.array(ts), ys
 
 
-def _ensemble(ucg, sim, c, nsteps, ninst=4, model=None, terms=None):
+def _ensemble(ucg, sim, c, nsteps, ninst=4, model=None, terms=None, planes=None):
     """Attempts one at a time; instance 0's state after each acceptance.  All
     instances carry the same parameters: their histories must be identical."""
     fr = c["friction"]
     ens = ucg.Ensemble()
+    if planes is not None:
+        ens.set_hier_planes(planes)
     ens.add_geometry(sim, ninst)
     for i in range(ninst):
         ens.set_friction(0, i, fr["Vpl"], fr["rake"], fr["mu0"], fr["sig"], fr["a"], fr["b"], fr["L"], fr["Vo"],
@@ -207,14 +209,16 @@ def test_history_hmatrix_split(ucg, hsetup):
     _check("hierarchical split", ref, ts, ys, 1e-6, 1e-5)
 
 
-def test_history_hierarchical_ensemble(ucg, hsetup):
-    """The ensemble on the hierarchical K keeps its operand images in bf16 hi + lo
-    (16 significant bits) with FP32 tensor-core sums over runs of up to 8,192
-    entries: measured 1.8e-5 in the 10 Vpl window, held to 3e-5."""
+# three planes (the default): bf16 hi + mid + lo images (24 bits) and a fresh
+# tensor-memory accumulator every 64 entries, added in FP32 registers; two
+# planes: hi + lo images (16 bits), one accumulator per run of up to 8,192
+# entries, held to their measured 1.8e-5
+@pytest.mark.parametrize("planes,tol", [(3, 1e-6), (2, 3e-5)])
+def test_history_hierarchical_ensemble(ucg, hsetup, planes, tol):
     c, sim, ref = hsetup
     sim.set_precision(ucg.UCG_PREC_HMATRIX)
-    ts, ys = _ensemble(ucg, sim, c, NRUN)
-    _check("hierarchical ensemble", ref, ts, ys, 3e-5, 1e-5)
+    ts, ys = _ensemble(ucg, sim, c, NRUN, planes=planes)
+    _check(f"hierarchical ensemble ({planes} planes)", ref, ts, ys, tol, 1e-5)
 
 
 def test_history_learned_step(ucg, setup):

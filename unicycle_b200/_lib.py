@@ -120,6 +120,7 @@ SIGNATURES = {
     "ucg_ens_put_states": (_i, [_vp, _i, _dp]),
     "ucg_ens_test_wait_timeout": (_i, [_vp, _l, _i]),
     "ucg_ens_set_increment_terms": (_i, [_vp, _i]),
+    "ucg_ens_set_hier_planes": (_i, [_vp, _i]),
     "ucg_ens_plan": (_i, [_vp, _i, _i, _i]),
     "ucg_ens_tune": (_i, [_vp, _i, ctypes.c_char_p, _l]),
     "ucg_ens_use_graph": (_i, [_vp, _i]),

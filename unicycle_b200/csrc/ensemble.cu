@@ -202,7 +202,7 @@ struct GeomDev {
     const double *vpl_c, *vpl_s, *a, *b, *sig, *L, *damping; // [ninst][np]
     InstCtl *ctl;               // [ninst]
     // hierarchical K (hier != 0): B is the B space of the hierarchical contraction
-    int hier, hleaves, hunit0, hpad;
+    int hier, hleaves, hunit0, hpl;    // hpl: bf16 planes of the hierarchical images (2 or 3)
     size_t hbtile;              // bytes of one instance tile's B space
     const int *hperm;           // permuted position -> element
     const int *hinv;            // element -> permuted position
@@ -646,44 +646,69 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
 // Operands are stored in the K-major core-matrix layout without swizzle: a
 // K-group is 8 consecutive K entries (16 bytes of bf16), an 8-row group of one
 // K-group is one 128-byte core matrix, and an image is [K-group][row group] per
-// plane (hi, then lo).  Granularity 8 along K lets a row leaf's K range
+// plane (hi, then lo, or hi, mid, lo).  Granularity 8 along K lets a row leaf's K range
 // concatenate pieces of any length multiple of 8 (leaf columns, ranks) and the
 // B operand of every K-group be fetched from wherever its instances' values
 // live (X: the permuted sources; Z: pass 1's output), merged into one bulk copy
 // per run of consecutive K-groups.  Rows of a unit beyond its 8-row groups are
 // read by the 128-row MMA from the stage's own buffer and land in accumulator
 // lanes that are never drained.
+constexpr int HSUB_KG3 = 8;                  // three planes: K-groups per fresh accumulator (64 entries)
 constexpr int HKG_STAGE = 8;                  // K-groups per stage (four K-steps of 16); see HTile::KG
 
-template <int NI, bool KLO>
+// tensor-memory columns of a hierarchical CTA: two accumulators of PL NI
+// columns, rounded up to the power of two that tcgen05.alloc takes
+constexpr int hm_cols(int ni, int pl)
+{
+    return 2 * pl * ni <= 32 ? 32 : 2 * pl * ni <= 64 ? 64 : 2 * pl * ni <= 128 ? 128 : 2 * pl * ni <= 256 ? 256 : 512;
+}
+// CTAs per SM: two when their tensor memory fits the SM's 512 columns; two
+// independent pipelines per SM hide the per-stage issue latency that bounds
+// one (measured: 20 % less time per launch)
+constexpr int hm_ctas(int ni, int pl) { return 2 * hm_cols(ni, pl) <= 512 ? 2 : 1; }
+
+// PL planes of bf16 per operand value: 2 (hi, lo: 16 significant bits) or 3
+// (hi, mid, lo: 24 bits, an FP32 value exactly)
+template <int NI, bool KLO, int PL>
 struct HTile {
-    static constexpr int B_KG = 2 * NI * 16;              // hi + lo of one K-group for NI instances
-    // CTAS per SM: two when their tensor memory (4 NI columns each) fits the
-    // SM's 512 columns; two independent pipelines per SM hide the per-stage
-    // issue latency that bounds one (measured: 20 % less time per launch)
-    static constexpr int CTAS = 8 * NI <= 512 ? 2 : 1;
+    static_assert(PL == 2 || (PL == 3 && KLO && NI <= 64), "planes");
+    static constexpr int B_KG = PL * NI * 16;             // every plane of one K-group for NI instances
+    static constexpr int CTAS = hm_ctas(NI, PL);
     static constexpr int BUDGET = CTAS == 2 ? 104 * 1024 : 208 * 1024;
     // two rings: the operand images stream from HBM and need many bytes in
     // flight; the B K-groups come from L2 and need few
     // K-groups per stage: 8, or 16 for the increments (hi planes) of a lone
-    // CTA: fewer, larger stages where the stage is cheap and room allows
-    static constexpr int KG = (KLO || CTAS == 2) ? HKG_STAGE : 2 * HKG_STAGE;
+    // CTA: fewer, larger stages where the stage is cheap and room allows; 4
+    // for three planes in two CTAs
+    static constexpr int KG = (PL == 3 && CTAS == 2) ? HKG_STAGE / 2 : (KLO || CTAS == 2) ? HKG_STAGE : 2 * HKG_STAGE;
     static constexpr int A_PLANE = KG * 16 * 128;          // one plane of a stage for 16 row groups
-    static constexpr int A_STAGE = KLO ? 2 * A_PLANE : A_PLANE;
+    static constexpr int A_STAGE = KLO ? PL * A_PLANE : A_PLANE;
     static constexpr int B_STAGE = KG * B_KG;
     static constexpr int SB_FIT = (BUDGET - A_STAGE) / B_STAGE;
-    static constexpr int SB_CAP = (KLO && CTAS == 2) ? 2 : 3;
+    static constexpr int SB_CAP = (KLO && (CTAS == 2 || PL == 3)) ? 2 : 3;
     static constexpr int SB = SB_FIT < SB_CAP ? SB_FIT : SB_CAP;
     static constexpr int SA_FIT = (BUDGET - SB * B_STAGE) / A_STAGE;
     static constexpr int SA = SA_FIT < 12 ? SA_FIT : 12;
     static constexpr int SMEM = SA * A_STAGE + SB * B_STAGE + 1024;   // + 1024 for the alignment
     static_assert(SA >= 2 && SB >= 1 && SMEM * CTAS <= 227 * 1024, "hierarchical contraction rings");
-    // one MMA of N = 2 NI per K-step reads the hi and lo planes of the B
-    // K-groups together (they are consecutive 8-row groups); the drain adds
-    // the accumulator's two halves
-    static constexpr uint32_t TMEM_COLS = 4 * NI;
-    static constexpr uint32_t IDESC = Tile<NI, false, 1>::IDESC_BF;
-    static constexpr uint32_t IDESC2 = Tile<NI, false, 1>::IDESC2_BF;
+    // one MMA of N = PL NI per K-step reads every plane of the B K-groups
+    // together (they are consecutive 8-row groups) into PL NI-column parts of
+    // one accumulator; the drain adds the parts.  Two planes: Ahi [Bhi; Blo]
+    // and Alo Bhi.  Three: Ahi [Bhi; Bmid; Blo], Amid [Bhi; Bmid] and Alo Bhi,
+    // every product of weight 2^-16 and above (the three left out are below
+    // 2^-24 of the value)
+    static constexpr int ACC = PL * NI;                    // columns of one accumulator
+    // three planes: a fresh accumulator every SUB_KG K-groups (64 entries),
+    // which the drain adds into FP32 register sums with round-to-nearest; the
+    // tensor core's own accumulation truncates at each K-step, a bias that
+    // grows with the run (two planes: one accumulator per segment, their
+    // 16-bit images outweigh it)
+    static constexpr int SUB_KG = PL == 3 ? HSUB_KG3 : 0;
+    static_assert(SUB_KG == 0 || (SUB_KG % KG == 0 && SUB_KG % 2 == 0), "sub-segments of whole stages");
+    static constexpr uint32_t TMEM_COLS = hm_cols(NI, PL);
+    static constexpr uint32_t IDESC = Tile<NI, false, 1>::idesc(NI, true);
+    static constexpr uint32_t IDESC2 = Tile<NI, false, 1>::idesc(2 * NI, true);
+    static constexpr uint32_t IDESC3 = Tile<NI, false, 1>::idesc(PL * NI, true);
 };
 
 struct HUnit {                  // one M-tile of one pass for one instance tile
@@ -710,15 +735,15 @@ __device__ __forceinline__ uint64_t cm_desc(uint32_t saddr, uint32_t lbo, uint32
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1u << 46);
 }
 
-template <int NI, bool KLO>
-__global__ void __launch_bounds__(224, 2) k_hm_contract(const HUnit *__restrict__ units,
+template <int NI, bool KLO, int PL>
+__global__ void __launch_bounds__(224, hm_ctas(NI, PL)) k_hm_contract(const HUnit *__restrict__ units,
         const HSeg *__restrict__ segs, const int *__restrict__ cta_seg, float *__restrict__ ws, int *err)
 {
     // warp 0: operand-image producer; warp 1: MMA issue; warps 2-5: drain
     // (tensor-memory lane quarter = warp mod 4); warp 6: B producer.  Both
-    // producers walk the same sequence of stages (segments in order, eight
+    // producers walk the same sequence of stages (segments in order, KG
     // K-groups at a time), each into its own ring.
-    using T = HTile<NI, KLO>;
+    using T = HTile<NI, KLO, PL>;
     extern __shared__ unsigned char dyn_smem[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dyn_smem) + 1023) & ~(uintptr_t)1023);
     uint8_t *bring = smem + (size_t)T::SA * T::A_STAGE;
@@ -801,9 +826,13 @@ __global__ void __launch_bounds__(224, 2) k_hm_contract(const HUnit *__restrict_
                     }
                     uint8_t *st = smem + (size_t)s * T::A_STAGE;
                     const uint32_t abytes = (uint32_t)nk * plane;
-                    bar_expect_tx(&fullA[s], (KLO ? 2u : 1u) * abytes);
+                    bar_expect_tx(&fullA[s], (KLO ? (uint32_t)PL : 1u) * abytes);
                     bulk_load_hint(st, ua + (size_t)kg * plane, abytes, &fullA[s], pol_a);
-                    if (KLO) bulk_load_hint(st + T::A_PLANE, ua + ulo + (size_t)kg * plane, abytes, &fullA[s], pol_a);
+                    if (KLO)
+#pragma unroll
+                        for (int p = 1; p < PL; p++)
+                            bulk_load_hint(st + p * T::A_PLANE, ua + p * ulo + (size_t)kg * plane, abytes, &fullA[s],
+                                           pol_a);
                     issued++;
                 }
                 if (!ok) break;
@@ -890,44 +919,59 @@ __global__ void __launch_bounds__(224, 2) k_hm_contract(const HUnit *__restrict_
             long it = 0;
             int tc = 0;
             bool issued_any = false;
-            for (int q = q0; q < q1 && !abort_flag; q++, tc++) {
+            for (int q = q0; q < q1 && !abort_flag; q++) {
                 const HSeg sg = segs[q];
                 const uint32_t plane = (uint32_t)units[sg.unit].g * 128u;
-                const int buf = tc & 1;
-                const uint32_t use = (uint32_t)(tc >> 1);
-                if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag)) {
-                    if (!abort_flag) fail();
-                    break;
-                }
-                tc_fence_after();
                 bool ok = true;
-                const uint32_t d = tmem + (uint32_t)(buf * 2 * NI);
-                for (int kg = sg.kg0; kg < sg.kg1; kg += T::KG, it++) {
-                    const int nk = min(T::KG, sg.kg1 - kg);
-                    const int sa = (int)(it % T::SA), sb = (int)(it % T::SB);
-                    if (!bar_wait(&fullA[sa], (uint32_t)((it / T::SA) & 1), &abort_flag) ||
-                        !bar_wait(&fullB[sb], (uint32_t)((it / T::SB) & 1), &abort_flag)) {
+                const int span = T::SUB_KG ? T::SUB_KG : sg.kg1 - sg.kg0;
+                for (int k0 = sg.kg0; k0 < sg.kg1 && ok; k0 += span, tc++) {
+                    const int k1 = min(sg.kg1, k0 + span);
+                    const int buf = tc & 1;
+                    const uint32_t use = (uint32_t)(tc >> 1);
+                    if (!bar_wait(&acc_empty[buf], (use & 1u) ^ 1u, &abort_flag)) {
                         if (!abort_flag) fail();
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t a = s_addr(smem + (size_t)sa * T::A_STAGE);
-                    const uint32_t b = s_addr(bring + (size_t)sb * T::B_STAGE);
-                    for (int j = 0; j < nk / 2; j++) {
-                        const uint32_t ao = (uint32_t)(2 * j) * plane, bo = (uint32_t)(2 * j) * T::B_KG;
-                        const uint64_t ahi = cm_desc(a + ao, plane, 128u);
-                        const uint64_t bhl = cm_desc(b + bo, T::B_KG, 128u);   // hi rows, then lo rows
-                        const uint32_t acc = (kg > sg.kg0 || j > 0) ? 1u : 0u;
-                        mma_bf16(d, ahi, bhl, T::IDESC2, acc);
-                        if (KLO) mma_bf16(d, cm_desc(a + T::A_PLANE + ao, plane, 128u), bhl, T::IDESC, 1u);
+                    const uint32_t d = tmem + (uint32_t)(buf * T::ACC);
+                    for (int kg = k0; kg < k1; kg += T::KG, it++) {
+                        const int nk = min(T::KG, sg.kg1 - kg);
+                        const int sa = (int)(it % T::SA), sb = (int)(it % T::SB);
+                        if (!bar_wait(&fullA[sa], (uint32_t)((it / T::SA) & 1), &abort_flag) ||
+                            !bar_wait(&fullB[sb], (uint32_t)((it / T::SB) & 1), &abort_flag)) {
+                            if (!abort_flag) fail();
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t a = s_addr(smem + (size_t)sa * T::A_STAGE);
+                        const uint32_t b = s_addr(bring + (size_t)sb * T::B_STAGE);
+                        for (int j = 0; j < nk / 2; j++) {
+                            const uint32_t ao = (uint32_t)(2 * j) * plane, bo = (uint32_t)(2 * j) * T::B_KG;
+                            const uint64_t ahi = cm_desc(a + ao, plane, 128u);
+                            const uint64_t bhl = cm_desc(b + bo, T::B_KG, 128u);   // hi rows, then the other planes'
+                            const uint32_t acc = (kg > k0 || j > 0) ? 1u : 0u;
+                            mma_bf16(d, ahi, bhl, T::IDESC3, acc);
+                            if (PL == 3) {
+                                // each product into the part of its weight: Amid [Bhi; Bmid]
+                                // into parts 1-2, Alo Bhi into part 2, so that part 0 takes
+                                // one addition per K-step
+                                mma_bf16(d + (uint32_t)NI, cm_desc(a + T::A_PLANE + ao, plane, 128u), bhl, T::IDESC2,
+                                         1u);
+                                mma_bf16(d + (uint32_t)(2 * NI), cm_desc(a + 2 * T::A_PLANE + ao, plane, 128u), bhl,
+                                         T::IDESC, 1u);
+                            } else if (KLO) {
+                                mma_bf16(d, cm_desc(a + T::A_PLANE + ao, plane, 128u), bhl, T::IDESC, 1u);
+                            }
+                        }
+                        issued_any = true;
+                        mma_commit(&emptyA[sa]);   // each frees its slot once these MMAs have read it
+                        mma_commit(&emptyB[sb]);
                     }
-                    issued_any = true;
-                    mma_commit(&emptyA[sa]);   // each frees its slot once these MMAs have read it
-                    mma_commit(&emptyB[sb]);
+                    if (!ok) break;
+                    mma_commit(&acc_full[buf]);
                 }
-                if (!ok) break;
-                mma_commit(&acc_full[buf]);
             }
             if (issued_any) {
                 mma_commit(&drain);
@@ -941,63 +985,169 @@ __global__ void __launch_bounds__(224, 2) k_hm_contract(const HUnit *__restrict_
         const int quarter = warp & 3;
         const int row = quarter * 32 + lane;
         int tc = 0;
-        for (int q = q0; q < q1; q++, tc++) {
-            const HSeg sg = segs[q];
-            const int rows = units[sg.unit].rows;
-            const int buf = tc & 1;
-            const uint32_t use = (uint32_t)(tc >> 1);
-            int ok = 0;
-            if (lane == 0) ok = bar_wait(&acc_full[buf], use & 1u, &abort_flag) ? 1 : 0;
-            ok = __shfl_sync(0xffffffffu, ok, 0);
-            if (!ok) {
-                if (lane == 0 && !abort_flag) fail();
-                break;
-            }
-            tc_fence_after();
-            const uint32_t tbase = tmem + (uint32_t)(buf * 2 * NI) + ((uint32_t)(quarter * 32) << 16);
-            if (sg.direct) {
-                // the whole K range of a pass-1 unit: Z = the sum, split into
-                // bf16 hi and lo at its B-space slot (rank entry row, instance)
-                uint8_t *zb = nullptr;
-                if (row < rows) {
-                    const HUnit &U = units[sg.unit];
-                    zb = const_cast<uint8_t *>(U.b) + (size_t)U.zdst[row >> 3] * (2 * NI * 16) + (size_t)(row & 7) * 2;
+        if constexpr (T::SUB_KG == 0) {
+            // two planes: one accumulator per segment
+            for (int q = q0; q < q1; q++, tc++) {
+                const HSeg sg = segs[q];
+                const int rows = units[sg.unit].rows;
+                const int buf = tc & 1;
+                const uint32_t use = (uint32_t)(tc >> 1);
+                int ok = 0;
+                if (lane == 0) ok = bar_wait(&acc_full[buf], use & 1u, &abort_flag) ? 1 : 0;
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) {
+                    if (lane == 0 && !abort_flag) fail();
+                    break;
                 }
-#pragma unroll
-                for (int c0 = 0; c0 < NI; c0 += 16) {
-                    uint32_t r[16], r2[16];
-                    tmem_ld16(tbase + (uint32_t)c0, r);
-                    tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
+                tc_fence_after();
+                const uint32_t tbase = tmem + (uint32_t)(buf * T::ACC) + ((uint32_t)(quarter * 32) << 16);
+                if (sg.direct) {
+                    // the whole K range of a pass-1 unit: Z = the sum, split into
+                    // bf16 hi and lo at its B-space slot (rank entry row, instance)
+                    uint8_t *zb = nullptr;
                     if (row < rows) {
+                        const HUnit &U = units[sg.unit];
+                        zb = const_cast<uint8_t *>(U.b) + (size_t)U.zdst[row >> 3] * T::B_KG + (size_t)(row & 7) * 2;
+                    }
 #pragma unroll
-                        for (int i = 0; i < 16; i++) {
-                            const float z = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
-                            const __nv_bfloat16 h = __float2bfloat16_rn(z);
-                            const __nv_bfloat16 l = __float2bfloat16_rn(z - __bfloat162float(h));
-                            const int inst = c0 + i;
-                            uint8_t *pz = zb + (size_t)(inst >> 3) * 128 + (size_t)(inst & 7) * 16;
-                            *reinterpret_cast<__nv_bfloat16 *>(pz) = h;
-                            *reinterpret_cast<__nv_bfloat16 *>(pz + NI * 16) = l;
+                    for (int c0 = 0; c0 < NI; c0 += 16) {
+                        uint32_t r[16], r2[16];
+                        tmem_ld16(tbase + (uint32_t)c0, r);
+                        tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
+                        if (row < rows) {
+#pragma unroll
+                            for (int i = 0; i < 16; i++) {
+                                const float z = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
+                                const __nv_bfloat16 h = __float2bfloat16_rn(z);
+                                const __nv_bfloat16 l = __float2bfloat16_rn(z - __bfloat162float(h));
+                                const int inst = c0 + i;
+                                uint8_t *pz = zb + (size_t)(inst >> 3) * 128 + (size_t)(inst & 7) * 16;
+                                *reinterpret_cast<__nv_bfloat16 *>(pz) = h;
+                                *reinterpret_cast<__nv_bfloat16 *>(pz + NI * 16) = l;
+                            }
+                        }
+                    }
+                } else {
+                    float *dst = ws + sg.ws + row;
+#pragma unroll
+                    for (int c0 = 0; c0 < NI; c0 += 16) {
+                        uint32_t r[16], r2[16];
+                        tmem_ld16(tbase + (uint32_t)c0, r);
+                        tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
+                        if (row < rows) {
+#pragma unroll
+                            for (int i = 0; i < 16; i++)
+                                dst[(size_t)(c0 + i) * rows] = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
                         }
                     }
                 }
-            } else {
-                float *dst = ws + sg.ws + row;
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) bar_arrive(&acc_empty[buf]);
+            }
+        } else {
+            // three planes: a fresh accumulator every SUB_KG K-groups, added
+            // into FP32 register sums that the segment's end writes out
+            for (int q = q0; q < q1; q++) {
+                const HSeg sg = segs[q];
+                const int rows = units[sg.unit].rows;
+                // 16 instances' values of this row out: a pass-1 unit with its
+                // whole K range writes Z, split into PL bf16 planes, at its B-space
+                // slot (rank entry row, instance); the others their partial sums
+                auto put16 = [&](int c0, const float *z) {
+                    if (row >= rows) return;
+                    if (sg.direct) {
+                        const HUnit &U = units[sg.unit];
+                        uint8_t *zb = const_cast<uint8_t *>(U.b) + (size_t)U.zdst[row >> 3] * T::B_KG + (size_t)(row & 7) * 2;
 #pragma unroll
-                for (int c0 = 0; c0 < NI; c0 += 16) {
-                    uint32_t r[16], r2[16];
-                    tmem_ld16(tbase + (uint32_t)c0, r);
-                    tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
-                    if (row < rows) {
+                        for (int i = 0; i < 16; i++) {
+                            const int inst = c0 + i;
+                            uint8_t *pz = zb + (size_t)(inst >> 3) * 128 + (size_t)(inst & 7) * 16;
+                            float x = z[i];
 #pragma unroll
-                        for (int i = 0; i < 16; i++)
-                            dst[(size_t)(c0 + i) * rows] = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
+                            for (int p = 0; p < PL; p++) {
+                                // each plane the rest rounded to bf16 (the differences are exact)
+                                const __nv_bfloat16 h = __float2bfloat16_rn(x);
+                                *reinterpret_cast<__nv_bfloat16 *>(pz + (size_t)p * NI * 16) = h;
+                                x = x - __bfloat162float(h);
+                            }
+                        }
+                    } else {
+                        float *dst = ws + sg.ws + row;
+#pragma unroll
+                        for (int i = 0; i < 16; i++) dst[(size_t)(c0 + i) * rows] = z[i];
                     }
+                };
+                const int span = T::SUB_KG ? T::SUB_KG : sg.kg1 - sg.kg0;
+                const int nsub = span > 0 ? (sg.kg1 - sg.kg0 + span - 1) / span : 0;
+                float sum[T::SUB_KG ? NI : 1];
+#pragma unroll
+                for (int c = 0; c < (T::SUB_KG ? NI : 1); c++) sum[c] = 0.0f;
+                bool ok = true;
+#pragma unroll 1
+                for (int sub = 0; sub < nsub; sub++, tc++) {
+                    const int buf = tc & 1;
+                    const uint32_t use = (uint32_t)(tc >> 1);
+                    int got = 0;
+                    if (lane == 0) got = bar_wait(&acc_full[buf], use & 1u, &abort_flag) ? 1 : 0;
+                    got = __shfl_sync(0xffffffffu, got, 0);
+                    if (!got) {
+                        if (lane == 0 && !abort_flag) fail();
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t tbase = tmem + (uint32_t)(buf * T::ACC) + ((uint32_t)(quarter * 32) << 16);
+                    // the sum of the accumulator's PL parts for 16 instances, the
+                    // small parts first
+                    auto load16 = [&](int c0, float *z) {
+                        uint32_t r[16], r2[16];
+                        tmem_ld16(tbase + (uint32_t)c0, r);
+                        tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
+                        if constexpr (PL == 3) {
+                            uint32_t r3[16];
+                            tmem_ld16(tbase + (uint32_t)(c0 + 2 * NI), r3);
+#pragma unroll
+                            for (int i = 0; i < 16; i++)
+                                z[i] = __uint_as_float(r[i]) + (__uint_as_float(r2[i]) + __uint_as_float(r3[i]));
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < 16; i++) z[i] = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
+                        }
+                    };
+                    if constexpr (T::SUB_KG > 0) {
+#pragma unroll
+                        for (int c0 = 0; c0 < NI; c0 += 16) {
+                            float z[16];
+                            load16(c0, z);
+#pragma unroll
+                            for (int i = 0; i < 16; i++) sum[c0 + i] += z[i];
+                        }
+                    } else if (sg.direct) {
+#pragma unroll
+                        for (int c0 = 0; c0 < NI; c0 += 16) {
+                            float z[16];
+                            load16(c0, z);
+                            put16(c0, z);
+                        }
+                    } else {
+#pragma unroll
+                        for (int c0 = 0; c0 < NI; c0 += 16) {
+                            float z[16];
+                            load16(c0, z);
+                            put16(c0, z);
+                        }
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) bar_arrive(&acc_empty[buf]);
+                }
+                if (!ok) break;
+                if constexpr (T::SUB_KG > 0) {
+#pragma unroll
+                    for (int c0 = 0; c0 < NI; c0 += 16) put16(c0, sum + c0);
                 }
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) bar_arrive(&acc_empty[buf]);
         }
     }
 
@@ -1010,50 +1160,70 @@ __global__ void __launch_bounds__(224, 2) k_hm_contract(const HUnit *__restrict_
     }
 }
 
+// the bf16 planes of an FP64 value: each plane the rest rounded to nearest
+// (the differences are exact in FP64)
+template <int PL>
+__device__ __forceinline__ void split_planes(double x, __nv_bfloat16 (&p)[PL])
+{
+#pragma unroll
+    for (int j = 0; j < PL; j++) {
+        p[j] = __double2bfloat16(x);
+        x = x - (double)__bfloat162float(p[j]);
+    }
+}
+
 // one K-group of an operand image from FP64 values: value(row r, slot k) =
 // src[k][(r - row0) stride] for rows row0 .. row0 + nrows - 1, zero where src[k]
-// is null; one thread per row writes its 16 bytes of hi and of lo
+// is null; one thread per row writes its 16 bytes of every plane
 struct HPackJob {
-    uint8_t *dst;               // the K-group's hi plane; lo at dst + lo_off
+    uint8_t *dst;               // the K-group's hi plane; the next planes lo_off bytes apart
     long lo_off;
     long stride;
     int row0, nrows;
     const double *src[8];
 };
 
+template <int PL>
 __global__ void k_hm_pack(const HPackJob *__restrict__ jobs)
 {
     const HPackJob J = jobs[blockIdx.x];
     const int t = threadIdx.x;
     if (t >= J.nrows) return;
     const int r = J.row0 + t;
-    uint32_t hi[4], lo[4];
+    uint32_t w[PL][4];
 #pragma unroll
     for (int k = 0; k < 8; k += 2) {
-        const double x0 = J.src[k] ? J.src[k][(long)t * J.stride] : 0.0;
-        const double x1 = J.src[k + 1] ? J.src[k + 1][(long)t * J.stride] : 0.0;
-        const __nv_bfloat16 h0 = __double2bfloat16(x0), h1 = __double2bfloat16(x1);
-        const __nv_bfloat16 l0 = __double2bfloat16(x0 - (double)__bfloat162float(h0));
-        const __nv_bfloat16 l1 = __double2bfloat16(x1 - (double)__bfloat162float(h1));
-        hi[k / 2] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-        lo[k / 2] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+        __nv_bfloat16 a[PL], b[PL];
+        split_planes<PL>(J.src[k] ? J.src[k][(long)t * J.stride] : 0.0, a);
+        split_planes<PL>(J.src[k + 1] ? J.src[k + 1][(long)t * J.stride] : 0.0, b);
+#pragma unroll
+        for (int p = 0; p < PL; p++)
+            w[p][k / 2] = (uint32_t)__bfloat16_as_ushort(a[p]) | ((uint32_t)__bfloat16_as_ushort(b[p]) << 16);
     }
-    uint8_t *p = J.dst + (size_t)(r >> 3) * 128 + (size_t)(r & 7) * 16;
-    *reinterpret_cast<uint4 *>(p) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-    *reinterpret_cast<uint4 *>(p + J.lo_off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    uint8_t *q = J.dst + (size_t)(r >> 3) * 128 + (size_t)(r & 7) * 16;
+#pragma unroll
+    for (int p = 0; p < PL; p++)
+        *reinterpret_cast<uint4 *>(q + p * J.lo_off) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
 }
 
 // a B-space entry (instance rr of a tile, slot `pos` = 8 K-group + k, k even) and
-// the next slot from two FP64 values, split into hi and lo
-__device__ __forceinline__ void put_x(uint8_t *Bt, int ni, int rr, int pos, double v0, double v1)
+// the next slot from two FP64 values, split into pl planes (2 or 3)
+__device__ __forceinline__ void put_x(uint8_t *Bt, int ni, int pl, int rr, int pos, double v0, double v1)
 {
-    uint8_t *base = Bt + (size_t)(pos >> 3) * (2 * ni * 16) + (size_t)(rr >> 3) * 128 + (size_t)(rr & 7) * 16 +
+    uint8_t *base = Bt + (size_t)(pos >> 3) * (pl * ni * 16) + (size_t)(rr >> 3) * 128 + (size_t)(rr & 7) * 16 +
                     (size_t)(pos & 7) * 2;
-    const __nv_bfloat16 h0 = __double2bfloat16(v0), h1 = __double2bfloat16(v1);
-    const __nv_bfloat16 l0 = __double2bfloat16(v0 - (double)__bfloat162float(h0));
-    const __nv_bfloat16 l1 = __double2bfloat16(v1 - (double)__bfloat162float(h1));
-    *reinterpret_cast<__nv_bfloat162 *>(base) = __halves2bfloat162(h0, h1);
-    *reinterpret_cast<__nv_bfloat162 *>(base + (size_t)ni * 16) = __halves2bfloat162(l0, l1);
+    __nv_bfloat16 a[3], b[3];
+    if (pl == 3) {
+        split_planes<3>(v0, a);
+        split_planes<3>(v1, b);
+    } else {
+        __nv_bfloat16 a2[2], b2[2];
+        split_planes<2>(v0, a2);
+        split_planes<2>(v1, b2);
+        a[0] = a2[0], a[1] = a2[1], b[0] = b2[0], b[1] = b2[1];
+    }
+    for (int p = 0; p < pl; p++)
+        *reinterpret_cast<__nv_bfloat162 *>(base + (size_t)p * ni * 16) = __halves2bfloat162(a[p], b[p]);
 }
 
 // pass 1's output into the B space for the units cut into several pieces (the
@@ -1066,6 +1236,7 @@ struct HZUnit {
     int g, rows, p0, np, pad;
 };
 
+template <int PL>
 __global__ void k_hm_zconv(const HZUnit *__restrict__ zu, const long *__restrict__ pws,
                            const float *__restrict__ ws, int ni)
 {
@@ -1079,18 +1250,20 @@ __global__ void k_hm_zconv(const HZUnit *__restrict__ zu, const long *__restrict
             z[0] += a.x; z[1] += a.y; z[2] += a.z; z[3] += a.w;
             z[4] += b.x; z[5] += b.y; z[6] += b.z; z[7] += b.w;
         }
-        uint32_t hi[4], lo[4];
+        uint32_t wd[PL][4];
 #pragma unroll
         for (int k = 0; k < 8; k += 2) {
-            const __nv_bfloat16 h0 = __double2bfloat16(z[k]), h1 = __double2bfloat16(z[k + 1]);
-            const __nv_bfloat16 l0 = __double2bfloat16(z[k] - (double)__bfloat162float(h0));
-            const __nv_bfloat16 l1 = __double2bfloat16(z[k + 1] - (double)__bfloat162float(h1));
-            hi[k / 2] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-            lo[k / 2] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+            __nv_bfloat16 a[PL], b[PL];
+            split_planes<PL>(z[k], a);
+            split_planes<PL>(z[k + 1], b);
+#pragma unroll
+            for (int p = 0; p < PL; p++)
+                wd[p][k / 2] = (uint32_t)__bfloat16_as_ushort(a[p]) | ((uint32_t)__bfloat16_as_ushort(b[p]) << 16);
         }
-        uint8_t *p = U.b + (size_t)U.zdst[grp] * (2 * ni * 16) + (size_t)(i >> 3) * 128 + (size_t)(i & 7) * 16;
-        *reinterpret_cast<uint4 *>(p) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-        *reinterpret_cast<uint4 *>(p + (size_t)ni * 16) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        uint8_t *q = U.b + (size_t)U.zdst[grp] * (PL * ni * 16) + (size_t)(i >> 3) * 128 + (size_t)(i & 7) * 16;
+#pragma unroll
+        for (int p = 0; p < PL; p++)
+            *reinterpret_cast<uint4 *>(q + (size_t)p * ni * 16) = make_uint4(wd[p][0], wd[p][1], wd[p][2], wd[p][3]);
     }
 }
 
@@ -1296,7 +1469,7 @@ __global__ void k_pack_x_dense(const EnsArgs *A, int gi, const double *__restric
     if (t >= (long)G.ninst * G.np) return;
     const int i = (int)(t / G.np), e = (int)(t % G.np);
     const double *v = V + (long)i * 2 * G.np + 2L * e;
-    put_x(G.B + (size_t)(i / A->ni) * G.hbtile, A->ni, i % A->ni, G.hxpos[e], v[0], v[1]);
+    put_x(G.B + (size_t)(i / A->ni) * G.hbtile, A->ni, G.hpl, i % A->ni, G.hxpos[e], v[0], v[1]);
 }
 
 // T (instance-major, ninst x m) of geometry gi from the workspace
@@ -1414,7 +1587,7 @@ __global__ void __launch_bounds__(EW_THREADS) k_ens_prologue(const EnsArgs *__re
                 v1 = v1 - G.v1[2 * pe + 1];
             }
         }
-        if (G.hier) put_x(G.B + (size_t)(i / A->ni) * G.hbtile, A->ni, i % A->ni, G.hxpos[e], v0, v1);
+        if (G.hier) put_x(G.B + (size_t)(i / A->ni) * G.hbtile, A->ni, G.hpl, i % A->ni, G.hxpos[e], v0, v1);
     }
     if (!G.hier) {
         // a warp holds the 32 elements (64 sources) of one k-block: its scale,
@@ -1796,6 +1969,7 @@ struct EnsGeomHost {
     int b_ni = 0;
     // hierarchical K: operand images of both passes and the maps of the B space
     bool hier = false;
+    int hpl = 2;               // bf16 planes of its images and B space
     struct HU {                // a unit of one pass, without its instance tile
         long a_off, lo_off, bidx_off;
         long zdst_off;         // pass 1: offset of its 8-row groups' Z destinations
@@ -1855,6 +2029,7 @@ struct ucg_ensemble {
     cudaGraphExec_t graph = nullptr;
     bool use_graph = true;     // false: attempts launched one by one from the host
     bool inc_full = true;      // stage increments: three-term form (Khi Vhi + Khi Vlo + Klo Vhi)
+    int hplanes = 3;           // bf16 planes of the hierarchical geometries' images (2 or 3)
     long launches = 0;
 };
 
@@ -1984,7 +2159,7 @@ int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
                     jobs.push_back(J);
                 }
             }
-            a_off += 2 * u.lo_off;
+            a_off += g.hpl * u.lo_off;
             g.hu1.push_back(u);
             g.h_kg1 += nke;
         }
@@ -2063,7 +2238,7 @@ int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
             jobs.push_back(J);
         }
         if (nk & 1) bidx.push_back(zero_kg);
-        a_off += 2 * u.lo_off;
+        a_off += g.hpl * u.lo_off;
         g.hu2.push_back(u);
         g.h_kg2 += nke;
     }
@@ -2105,7 +2280,10 @@ int build_hgeom(ucg_ensemble *E, const ucg::HLayout &L, EnsGeomHost &g)
         for (size_t j = j0; j < j0 + nb; j++) jobs[j].dst = g.hA + dst_off[j];
         cudaError_t e = cudaMemcpyAsync(jd, jobs.data() + j0, sizeof(HPackJob) * nb, cudaMemcpyHostToDevice, E->stream);
         if (e == cudaSuccess) {
-            k_hm_pack<<<(unsigned)nb, 128, 0, E->stream>>>(jd);
+            if (g.hpl == 3)
+                k_hm_pack<3><<<(unsigned)nb, 128, 0, E->stream>>>(jd);
+            else
+                k_hm_pack<2><<<(unsigned)nb, 128, 0, E->stream>>>(jd);
             E->launches++;
             e = cudaGetLastError();
         }
@@ -2284,7 +2462,7 @@ void cap_segments(Sched &s, int ntiles, int cap = SEG_MAX_KB)
 size_t b_bytes(const EnsGeomHost &g, int ni)
 {
     const int ntl = (g.ninst + ni - 1) / ni;
-    if (g.hier) return (size_t)ntl * g.nbkg * (size_t)(2 * ni * 16);
+    if (g.hier) return (size_t)ntl * g.nbkg * (size_t)(g.hpl * ni * 16);
     return (size_t)ntl * g.kblocks * (size_t)(2 * ni * BK * 2);
 }
 
@@ -2306,7 +2484,7 @@ int upload_hplan(ucg_ensemble *E, HPlanBufs &P, int ni, int pass)
     for (const EnsGeomHost &g : E->geoms) {
         if (!g.hier) continue;
         const int ntl = (g.ninst + ni - 1) / ni;
-        const size_t bt = (size_t)g.nbkg * 2 * ni * 16;
+        const size_t bt = (size_t)g.nbkg * g.hpl * ni * 16;
         for (int nt = 0; nt < ntl; nt++)
             for (const EnsGeomHost::HU &h : (pass == 1 ? g.hu1 : g.hu2)) {
                 HUnit u;
@@ -2330,8 +2508,11 @@ int upload_hplan(ucg_ensemble *E, HPlanBufs &P, int ni, int pass)
         steps.push_back(u.nkg / 2);
         w.push_back(u.g + 4);      // a K-step's bytes grow with the row groups; its MMAs do not
     }
-    Sched s = sched_weighted(steps, w, (8 * ni <= 512 ? 2 : 1) * E->sms);   // HTile<ni, *>::CTAS per SM
-    cap_segments(s, P.nunits, 512);   // 1,024 K-groups = 8,192 K entries per FP32 partial sum
+    Sched s = sched_weighted(steps, w, hm_ctas(ni, E->hplanes) * E->sms);   // HTile<ni, *, planes>::CTAS per SM
+    // 512 K-steps (8,192 K entries) per FP32 partial sum (three planes: of
+    // register sums over fresh 64-entry accumulators; measured as accurate
+    // as runs of 1,024 entries, and 7 % faster per attempt)
+    cap_segments(s, P.nunits, 512);
     // partial sums for every piece, except a pass-1 unit's only one, whose
     // drain writes Z directly
     std::vector<long> pws(std::max(1, s.nslots), 0);
@@ -2387,31 +2568,48 @@ int upload_hplan(ucg_ensemble *E, HPlanBufs &P, int ni, int pass)
     return UCG_OK;
 }
 
-template <int NI>
-cudaError_t prepare_hcontract_t()
+template <int NI, bool KLO, int PL>
+cudaError_t prepare_hcontract_one()
 {
-    cudaError_t e = cudaFuncSetAttribute(k_hm_contract<NI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         HTile<NI, true>::SMEM);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_hm_contract<NI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                HTile<NI, false>::SMEM);
+    return cudaFuncSetAttribute(k_hm_contract<NI, KLO, PL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                HTile<NI, KLO, PL>::SMEM);
 }
 
-template <int NI, bool KLO>
+template <int NI>
+cudaError_t prepare_hcontract_t(int planes)
+{
+    if constexpr (NI <= 64)
+        if (planes == 3) return prepare_hcontract_one<NI, true, 3>();
+    cudaError_t e = prepare_hcontract_one<NI, true, 2>();
+    if (e != cudaSuccess) return e;
+    return prepare_hcontract_one<NI, false, 2>();
+}
+
+template <int NI, bool KLO, int PL>
 cudaError_t launch_hpass_t(ucg_ensemble *E, const HPlanBufs &P)
 {
-    k_hm_contract<NI, KLO><<<HTile<NI, KLO>::CTAS * E->sms, 224, HTile<NI, KLO>::SMEM, E->stream>>>(P.units, P.segs, P.cta, P.ws,
-                                                                            &E->d_glob->err);
+    using T = HTile<NI, KLO, PL>;
+    k_hm_contract<NI, KLO, PL><<<T::CTAS * E->sms, 224, T::SMEM, E->stream>>>(P.units, P.segs, P.cta, P.ws,
+                                                                           &E->d_glob->err);
     E->launches++;
     return cudaGetLastError();
 }
 
+// three planes: every stage in the one form (the increments' two-term option
+// is a form of the dense contraction and of the two-plane images)
 cudaError_t launch_hpass(ucg_ensemble *E, const HPlanBufs &P, bool klo)
 {
+    if (E->hplanes == 3) {
+        switch (E->ni) {
+        case 32: return launch_hpass_t<32, true, 3>(E, P);
+        case 64: return launch_hpass_t<64, true, 3>(E, P);
+        default: return cudaErrorInvalidValue;
+        }
+    }
     switch (E->ni) {
-    case 32: return klo ? launch_hpass_t<32, true>(E, P) : launch_hpass_t<32, false>(E, P);
-    case 64: return klo ? launch_hpass_t<64, true>(E, P) : launch_hpass_t<64, false>(E, P);
-    case 128: return klo ? launch_hpass_t<128, true>(E, P) : launch_hpass_t<128, false>(E, P);
+    case 32: return klo ? launch_hpass_t<32, true, 2>(E, P) : launch_hpass_t<32, false, 2>(E, P);
+    case 64: return klo ? launch_hpass_t<64, true, 2>(E, P) : launch_hpass_t<64, false, 2>(E, P);
+    case 128: return klo ? launch_hpass_t<128, true, 2>(E, P) : launch_hpass_t<128, false, 2>(E, P);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -2424,7 +2622,10 @@ cudaError_t launch_hier(ucg_ensemble *E, bool klo)
         e = launch_hpass(E, E->h1, klo);
         if (e != cudaSuccess) return e;
         if (E->h1.nzu > 0) {
-            k_hm_zconv<<<E->h1.nzu, 256, 0, E->stream>>>(E->h1.zu, E->h1.pws, E->h1.ws, E->ni);
+            if (E->hplanes == 3)
+                k_hm_zconv<3><<<E->h1.nzu, 256, 0, E->stream>>>(E->h1.zu, E->h1.pws, E->h1.ws, E->ni);
+            else
+                k_hm_zconv<2><<<E->h1.nzu, 256, 0, E->stream>>>(E->h1.zu, E->h1.pws, E->h1.ws, E->ni);
             E->launches++;
             e = cudaGetLastError();
             if (e != cudaSuccess) return e;
@@ -2445,7 +2646,7 @@ cudaError_t prepare_contract_t()
                                 Tile<NI, false, 2>::SMEM);
 }
 
-cudaError_t prepare_contract(int ni)
+cudaError_t prepare_contract(int ni, int planes)
 {
     cudaError_t e;
     switch (ni) {
@@ -2456,9 +2657,9 @@ cudaError_t prepare_contract(int ni)
     }
     if (e != cudaSuccess) return e;
     switch (ni) {
-    case 32: return prepare_hcontract_t<32>();
-    case 64: return prepare_hcontract_t<64>();
-    default: return prepare_hcontract_t<128>();
+    case 32: return prepare_hcontract_t<32>(planes);
+    case 64: return prepare_hcontract_t<64>(planes);
+    default: return prepare_hcontract_t<128>(planes);
     }
 }
 
@@ -2595,7 +2796,7 @@ int install_plan(ucg_ensemble *E, int ni, const Sched &s1, const Sched &s2)
     free_plan(E);
     int st = ensure_b(E, ni);
     if (st) return st;
-    ECUDA(prepare_contract(ni));
+    ECUDA(prepare_contract(ni, E->hplanes));
     E->ni = ni;
     if ((st = upload_plan(E, E->p1, ni, 1, s1)) || (st = upload_plan(E, E->p2, ni, 2, s2))) return st;
     if ((st = upload_hplan(E, E->h1, ni, 1)) || (st = upload_hplan(E, E->h2, ni, 2))) return st;
@@ -2619,7 +2820,8 @@ int install_plan(ucg_ensemble *E, int ni, const Sched &s1, const Sched &s2)
             d.hleaves = g.hleaves;
             d.hunit0 = hunit0;
             hunit0 += ntl * g.hleaves;
-            d.hbtile = (size_t)g.nbkg * 2 * ni * 16;
+            d.hbtile = (size_t)g.nbkg * g.hpl * ni * 16;
+            d.hpl = g.hpl;
             d.hperm = g.hperm;
             d.hinv = g.hinv;
             d.hrow = g.hrow;
@@ -2693,14 +2895,16 @@ bool has_dense(const ucg_ensemble *E)
     return false;
 }
 
-// instance tile width: 128 only for hierarchical-only ensembles (the dense
-// contraction's per-k-block drain keeps 2 x 64 register sums per thread)
+// instance tile width: 128 only for hierarchical-only ensembles of two-plane
+// images (the dense contraction's per-k-block drain keeps 2 x 64 register
+// sums per thread; three planes of 128 instances are 384 accumulator columns,
+// two of which do not fit the tensor memory)
 int default_ni(ucg_ensemble *E)
 {
     int mx = 1;
     for (const EnsGeomHost &g : E->geoms) mx = std::max(mx, g.ninst);
     const int ni = mx <= 32 ? 32 : (mx <= 64 ? 64 : 128);
-    return (ni == 128 && has_dense(E)) ? 64 : ni;
+    return (ni == 128 && (has_dense(E) || E->hplanes == 3)) ? 64 : ni;
 }
 
 // the schedule of a kind for the single-tile (mt 1) or paired (mt 2) units
@@ -2921,6 +3125,7 @@ int ucg_ens_add_geometry(ucg_ensemble *E, ucg_ctx *c, int n_instances, int *geom
     if (hier) {
         ucg::HLayout L;
         ucg::hmatrix_layout(c, &L);
+        g.hpl = E->hplanes;
         int st = build_hgeom(E, L, g);
         if (st) {
             void *ptrs[] = {g.hA, g.hbidx, g.hperm, g.hinv, g.hxpos, g.hrow, g.hzdst};
@@ -3079,6 +3284,16 @@ int ucg_ens_set_states(ucg_ensemble *E, int gi, const double *y, const double *t
     return UCG_OK;
 }
 
+int ucg_ens_set_hier_planes(ucg_ensemble *E, int planes)
+{
+    if (!E || (planes != 2 && planes != 3)) return E ? ebad(E, UCG_E_BADARG, "planes must be 2 or 3") : UCG_E_BADARG;
+    for (const EnsGeomHost &g : E->geoms)
+        if (g.hier && g.hpl != planes)
+            return ebad(E, UCG_E_STATE, "the planes are fixed once a hierarchical geometry is added");
+    E->hplanes = planes;
+    return UCG_OK;
+}
+
 int ucg_ens_set_increment_terms(ucg_ensemble *E, int terms)
 {
     if (!E || (terms != 2 && terms != 3)) return E ? ebad(E, UCG_E_BADARG, "terms must be 2 or 3") : UCG_E_BADARG;
@@ -3151,6 +3366,8 @@ int ucg_ens_plan(ucg_ensemble *E, int ni, int schedule, int chunk)
     if (ni != 32 && ni != 64 && ni != 128) return ebad(E, UCG_E_BADARG, "ni must be 32, 64 or 128");
     if (ni == 128 && has_dense(E))
         return ebad(E, UCG_E_UNSUPPORTED, "ni 128 is for hierarchical geometries only");
+    if (ni == 128 && E->hplanes == 3)
+        return ebad(E, UCG_E_UNSUPPORTED, "ni 128 takes two-plane hierarchical images only");
     if (schedule != UCG_ENS_STREAM_K && schedule != UCG_ENS_SPLIT_LPT) return ebad(E, UCG_E_BADARG, "unknown schedule");
     ECUDA(cudaSetDevice(E->device));
     ECUDA(cudaStreamSynchronize(E->stream));

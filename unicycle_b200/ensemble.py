@@ -102,9 +102,15 @@ class Ensemble:
         self._check(self.lib.ucg_ens_put_states(self.ens, geometry, _p(y)), "put_states")
 
     def set_increment_terms(self, terms):
-        """Stage increments in the two-term form Khi (Vhi + Vlo) (2, the default) or
-        the anchor's three-term form (3) (ucg_ens_set_increment_terms)."""
+        """Stage increments in the anchor's three-term form (3, the default) or the
+        two-term form Khi (Vhi + Vlo) (2) (ucg_ens_set_increment_terms)."""
         self._check(self.lib.ucg_ens_set_increment_terms(self.ens, int(terms)), "set_increment_terms")
+
+    def set_hier_planes(self, planes):
+        """bf16 planes of the hierarchical geometries' operand images: 3 (24 bits,
+        the default) or 2 (16 bits); before the first hierarchical geometry is
+        added (ucg_ens_set_hier_planes)."""
+        self._check(self.lib.ucg_ens_set_hier_planes(self.ens, int(planes)), "set_hier_planes")
 
     def test_wait_timeout(self, wait_ns=0, hold=False):
         """Fault injection for tests (ucg_ens_test_wait_timeout): with hold the dense
