@@ -656,12 +656,9 @@ __global__ void __launch_bounds__(320, 1) k_bf16x3_contract(const GemmTile *__re
 constexpr int HSUB_KG3 = 8;                  // three planes: K-groups per fresh accumulator (64 entries)
 constexpr int HKG_STAGE = 8;                  // K-groups per stage (four K-steps of 16); see HTile::KG
 
-// tensor-memory columns of a hierarchical CTA: two accumulators of PL NI
-// columns, rounded up to the power of two that tcgen05.alloc takes
-constexpr int hm_cols(int ni, int pl)
-{
-    return 2 * pl * ni <= 32 ? 32 : 2 * pl * ni <= 64 ? 64 : 2 * pl * ni <= 128 ? 128 : 2 * pl * ni <= 256 ? 256 : 512;
-}
+// tensor-memory columns of a hierarchical CTA: two accumulators of two NI-column
+// parts (every plane count), a power of two as tcgen05.alloc takes
+constexpr int hm_cols(int ni, int) { return 4 * ni; }
 // CTAs per SM: two when their tensor memory fits the SM's 512 columns; two
 // independent pipelines per SM hide the per-stage issue latency that bounds
 // one (measured: 20 % less time per launch)
@@ -691,13 +688,15 @@ struct HTile {
     static constexpr int SA = SA_FIT < 12 ? SA_FIT : 12;
     static constexpr int SMEM = SA * A_STAGE + SB * B_STAGE + 1024;   // + 1024 for the alignment
     static_assert(SA >= 2 && SB >= 1 && SMEM * CTAS <= 227 * 1024, "hierarchical contraction rings");
-    // one MMA of N = PL NI per K-step reads every plane of the B K-groups
-    // together (they are consecutive 8-row groups) into PL NI-column parts of
-    // one accumulator; the drain adds the parts.  Two planes: Ahi [Bhi; Blo]
-    // and Alo Bhi.  Three: Ahi [Bhi; Bmid; Blo], Amid [Bhi; Bmid] and Alo Bhi,
-    // every product of weight 2^-16 and above (the three left out are below
-    // 2^-24 of the value)
-    static constexpr int ACC = PL * NI;                    // columns of one accumulator
+    // an accumulator has two NI-column parts, which the drain adds.  Two
+    // planes: one MMA of N = 2 NI per K-step reads the hi and lo planes of the
+    // B K-groups together (consecutive 8-row groups): Ahi [Bhi; Blo], then Alo
+    // Bhi into part 0.  Three planes: the six products of weight 2^-16 and above
+    // (the three left out are below 2^-24 of the value), Ahi [Bhi; Bmid] with
+    // N = 2 NI, then Ahi Blo, Amid Bhi, Amid Bmid and Alo Bhi into part 1, so
+    // that part 0 takes one tensor-core addition per K-step and part 1, 2^-8 of
+    // it, keeps the small products to 2^-31 of the value
+    static constexpr int ACC = 2 * NI;                     // columns of one accumulator
     // three planes: a fresh accumulator every SUB_KG K-groups (64 entries),
     // which the drain adds into FP32 register sums with round-to-nearest; the
     // tensor core's own accumulation truncates at each K-step, a bias that
@@ -708,7 +707,6 @@ struct HTile {
     static constexpr uint32_t TMEM_COLS = hm_cols(NI, PL);
     static constexpr uint32_t IDESC = Tile<NI, false, 1>::idesc(NI, true);
     static constexpr uint32_t IDESC2 = Tile<NI, false, 1>::idesc(2 * NI, true);
-    static constexpr uint32_t IDESC3 = Tile<NI, false, 1>::idesc(PL * NI, true);
 };
 
 struct HUnit {                  // one M-tile of one pass for one instance tile
@@ -952,15 +950,15 @@ __global__ void __launch_bounds__(224, hm_ctas(NI, PL)) k_hm_contract(const HUni
                             const uint64_t ahi = cm_desc(a + ao, plane, 128u);
                             const uint64_t bhl = cm_desc(b + bo, T::B_KG, 128u);   // hi rows, then the other planes'
                             const uint32_t acc = (kg > k0 || j > 0) ? 1u : 0u;
-                            mma_bf16(d, ahi, bhl, T::IDESC3, acc);
+                            mma_bf16(d, ahi, bhl, T::IDESC2, acc);
                             if (PL == 3) {
-                                // each product into the part of its weight: Amid [Bhi; Bmid]
-                                // into parts 1-2, Alo Bhi into part 2, so that part 0 takes
-                                // one addition per K-step
-                                mma_bf16(d + (uint32_t)NI, cm_desc(a + T::A_PLANE + ao, plane, 128u), bhl, T::IDESC2,
-                                         1u);
-                                mma_bf16(d + (uint32_t)(2 * NI), cm_desc(a + 2 * T::A_PLANE + ao, plane, 128u), bhl,
-                                         T::IDESC, 1u);
+                                const uint32_t d1 = d + (uint32_t)NI;
+                                const uint64_t amid = cm_desc(a + T::A_PLANE + ao, plane, 128u);
+                                const uint64_t bmid = cm_desc(b + bo + NI * 16, T::B_KG, 128u);
+                                mma_bf16(d1, ahi, cm_desc(b + bo + 2 * NI * 16, T::B_KG, 128u), T::IDESC, 1u);
+                                mma_bf16(d1, amid, bhl, T::IDESC, 1u);
+                                mma_bf16(d1, amid, bmid, T::IDESC, 1u);
+                                mma_bf16(d1, cm_desc(a + 2 * T::A_PLANE + ao, plane, 128u), bhl, T::IDESC, 1u);
                             } else if (KLO) {
                                 mma_bf16(d, cm_desc(a + T::A_PLANE + ao, plane, 128u), bhl, T::IDESC, 1u);
                             }
@@ -1104,16 +1102,8 @@ __global__ void __launch_bounds__(224, hm_ctas(NI, PL)) k_hm_contract(const HUni
                         uint32_t r[16], r2[16];
                         tmem_ld16(tbase + (uint32_t)c0, r);
                         tmem_ld16(tbase + (uint32_t)(c0 + NI), r2);
-                        if constexpr (PL == 3) {
-                            uint32_t r3[16];
-                            tmem_ld16(tbase + (uint32_t)(c0 + 2 * NI), r3);
 #pragma unroll
-                            for (int i = 0; i < 16; i++)
-                                z[i] = __uint_as_float(r[i]) + (__uint_as_float(r2[i]) + __uint_as_float(r3[i]));
-                        } else {
-#pragma unroll
-                            for (int i = 0; i < 16; i++) z[i] = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
-                        }
+                        for (int i = 0; i < 16; i++) z[i] = __uint_as_float(r[i]) + __uint_as_float(r2[i]);
                     };
                     if constexpr (T::SUB_KG > 0) {
 #pragma unroll
@@ -2896,9 +2886,8 @@ bool has_dense(const ucg_ensemble *E)
 }
 
 // instance tile width: 128 only for hierarchical-only ensembles of two-plane
-// images (the dense contraction's per-k-block drain keeps 2 x 64 register
-// sums per thread; three planes of 128 instances are 384 accumulator columns,
-// two of which do not fit the tensor memory)
+// images (the dense contraction's per-k-block drain, and the three-plane
+// hierarchical one, keep a register sum per instance of the tile and thread)
 int default_ni(ucg_ensemble *E)
 {
     int mx = 1;
