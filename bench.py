@@ -1024,7 +1024,9 @@ def hier_roofline(args, img, ms_a, ms_c, peak, peak_kind):
             "k_hm_contract<64,false,2> x2 + k_hm_zconv (increment form; operand hi planes)")
     return {"bound": "hbm", "kernel": kern, "ms_per_launch": ms, "bytes_per_launch": byt,
             "achieved": byt / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-            "frac": byt / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None}
+            "frac": byt / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+            "traffic": load_traffic("k_hm_contract_3planes") if args.hier_planes == 3 and args.nx * args.nz == 10000
+            else None}
 
 
 def run_hier_ensemble(args, world, rank, local):
