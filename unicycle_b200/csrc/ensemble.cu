@@ -5,12 +5,17 @@
 // geometry held as a hierarchical matrix, the two-pass contraction described
 // before k_hm_contract.
 //
-// Precision.  K and V are both held as bf16 hi/lo pairs, K with a power-of-two
-// scale per row: K = s (Khi + Klo), V = Vhi + Vlo.  Each 16-source step forms
-// Khi Vhi + Khi Vlo + Klo Vhi, accumulating in FP32 in tensor memory (the V hi
-// and lo images are consecutive rows of one operand, so one MMA of N = 2 NI
-// takes both Khi products into two accumulator halves that the drain adds);
-// the dropped Klo Vlo term and the residuals are of relative size 2^-16.  State,
+// Precision.  A dense geometry's K and V are both held as fp16 hi/lo pairs,
+// the lo image the residual times 2^11, with power-of-two scales per K row, per
+// 128-row x 64-source K-block and per 64-source V-block (the scales keep every
+// value inside fp16's range).  Each 16-source step forms Khi Vhi + 2^-11 (Khi
+// Vlo + Klo Vhi) in FP32 in tensor memory (the V hi and lo images are
+// consecutive rows of one operand, so one MMA of N = 2 NI takes both Khi
+// products into two accumulator halves that the drain adds); every 64-source
+// k-block goes into a fresh accumulator that the drain scales and adds into
+// FP32, then FP64, register sums.  The dropped Klo Vlo term and the residuals
+// are of relative size 2^-21.  A hierarchical geometry holds its images as two
+// or three bf16 planes (k_hm_contract).  State,
 // stage combinations, error norm and step control stay FP64 and follow the
 // single-instance integrator (rk.cu) per instance: every instance has its own
 // step size, time, accept/reject decision and counters, and the reference
@@ -81,8 +86,8 @@ namespace ucg {
 namespace ens {
 
 constexpr int BM = 128;                 // K rows per tile (MMA M)
-constexpr int BK = 64;                  // sources per k-block (one 128-byte bf16 row)
-constexpr int A_HALF = BM * BK * 2;     // one bf16 image of a tile k-block: 16 KB
+constexpr int BK = 64;                  // sources per k-block (one 128-byte row of 16-bit values)
+constexpr int A_HALF = BM * BK * 2;     // one 16-bit image of a tile k-block: 16 KB
 constexpr int A_IMG = 2 * A_HALF;       // hi + lo
 constexpr float LO_SCALE = 2048.0f, LO_UNSCALE = 1.0f / 2048.0f;   // dense images: lo = 2^11 residual
 constexpr int MAX_GEOM = 16;
